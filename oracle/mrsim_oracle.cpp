@@ -1,0 +1,1719 @@
+// mrsim_oracle.cpp — TEST INFRASTRUCTURE ONLY.  A CPU FP64 restatement of the reference crate's
+// 2D EPI k-space path (Rust `mrsim-acq`, which cannot be compiled in this image: no Rust
+// toolchain).  It is the parity checker for the CUDA library and the timed CPU baseline.  Only
+// `tests/`, `__graft_entry__.smoke()` and `bench.py`'s CPU-baseline / reference arm may load it;
+// the product library never links or calls it.
+//
+// Pinning: `oracle_golden_*` regenerates the reference's golden record
+// (tests/golden_baseline.rs:28-126) and the tests compare it bit for bit with the reference's
+// committed fixtures (tests/fixtures/p4_baseline/default/*.bin, copied to tests/golden/).
+//
+// Build rule: -O2 -ffp-contract=off -fno-fast-math, glibc libm — Rust never fuses multiply-adds
+// and calls the platform libm for sin/cos/exp/ln, so every expression below keeps the reference's
+// operation order.  Each function cites the reference file:line it restates.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <stdexcept>
+#include <atomic>
+#include <mutex>
+#include <thread>
+#include <functional>
+
+#include "../include/mrsim_acq.h"
+
+namespace {
+
+constexpr double TAU = 6.283185307179586;  // std::f64::consts::TAU
+constexpr double PI = 3.141592653589793;
+
+// ---- complex helper: `C` kspace.rs:29-55 ----
+struct Cx {
+  double re, im;
+};
+inline Cx cadd(Cx a, Cx b) { return {a.re + b.re, a.im + b.im}; }
+inline Cx cmul(Cx a, Cx o) { return {a.re * o.re - a.im * o.im, a.re * o.im + a.im * o.re}; }
+inline Cx cscale(Cx a, double s) { return {a.re * s, a.im * s}; }
+inline double cabs_(Cx a) { return std::sqrt(a.re * a.re + a.im * a.im); }
+inline Cx ccis(double th) { return {std::cos(th), std::sin(th)}; }
+const Cx CZERO = {0.0, 0.0};
+
+// ---- `Rng` kspace.rs:59-77 (SplitMix64 + Box-Muller) ----
+struct Rng {
+  uint64_t s;
+  explicit Rng(uint64_t seed) : s(seed) {}
+  uint64_t next_u64() {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  }
+  double unit() { return ((double)(next_u64() >> 11) + 0.5) / (double)(1ull << 53); }
+  double gauss() {
+    double u1 = unit();
+    double u2 = unit();
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(TAU * u2);
+  }
+};
+
+struct Fail : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+// Dynamic-schedule parallel loop over [0, n) on `threads` std::threads (the reference's rayon
+// `par` feature parallelises the same loops; results do not depend on the thread count).
+void parallel_for(size_t n, int threads, const std::function<void(size_t)>& body) {
+  if (threads <= 1 || n <= 1) {
+    for (size_t i = 0; i < n; ++i) body(i);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::mutex mu;
+  std::string err;
+  auto worker = [&] {
+    for (;;) {
+      size_t i = next.fetch_add(1);
+      if (i >= n) return;
+      try {
+        body(i);
+      } catch (std::exception& e) {
+        std::lock_guard<std::mutex> lk(mu);
+        err = e.what();
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads && (size_t)t < n; ++t) pool.emplace_back(worker);
+  for (auto& t : pool) t.join();
+  if (!err.empty()) throw Fail(err);
+}
+
+// ---- `SingleShotEpi` readout.rs:23-69 ----
+struct Epi {
+  size_t kx_max, ky_max;
+  double t_line, t_echo;
+  bool reverse_phase;
+  double dt() const { return t_line / (double)kx_max; }
+  double half_read_time() const { return (double)(kx_max * ky_max) * dt() / 2.0; }
+  void kspace_index(size_t tick, size_t& kx, size_t& ky) const {
+    size_t x = tick % kx_max;
+    size_t y = tick / kx_max;
+    if (!reverse_phase) {
+      y = ky_max - 1 - y;
+      if (y % 2 == 1) x = kx_max - x - 1;
+    } else if (y % 2 == 1) {
+      x = kx_max - x - 1;
+    }
+    kx = x;
+    ky = y;
+  }
+  double time_from_max_echo(size_t tick) const { return dt() * ((double)tick + 0.5) - half_read_time(); }
+  double time_from_prep_gradient(size_t tick) const { return (double)tick * dt() + dt() / 2.0; }
+  double time_from_rf(size_t tick) const { return t_echo + time_from_max_echo(tick); }
+};
+
+// ---- `pf_skipped_lines` kspace.rs:110-116 ----
+size_t pf_skipped_lines(size_t ny, const mrsim_acquisition& a) {
+  if (a.partial_fourier < 1.0 && a.pf_mode == MRSIM_PF_SCANNER) {
+    size_t keep = (size_t)std::round((double)ny * a.partial_fourier);
+    return ny - std::min(keep, ny);
+  }
+  return 0;
+}
+
+// ---- `LineTiming` kspace.rs:271-325 ----
+struct LineTiming {
+  std::vector<double> t_ms, trf_ms, tread_ms;
+  std::vector<int8_t> polarity;
+};
+
+LineTiming line_timing_for(const mrsim_acquisition& a, size_t nx, size_t ny) {
+  Epi epi{nx, ny, a.t_line, a.t_echo, a.reverse_phase != 0};
+  LineTiming lt;
+  lt.t_ms.assign(ny, 0.0);
+  lt.trf_ms.assign(ny, 0.0);
+  lt.tread_ms.assign(ny, 0.0);
+  size_t xs = nx / 2;
+  for (size_t tick = 0; tick < nx * ny; ++tick) {
+    size_t kx, ky;
+    epi.kspace_index(tick, kx, ky);
+    if (kx == xs) {
+      lt.t_ms[ky] = epi.time_from_max_echo(tick);
+      lt.trf_ms[ky] = epi.time_from_rf(tick);
+      lt.tread_ms[ky] = epi.time_from_prep_gradient(tick);
+    }
+  }
+  lt.polarity.resize(ny);
+  for (size_t k = 0; k < ny; ++k) lt.polarity[k] = (k % 2 == 1) ? -1 : 1;
+  double offset = (double)pf_skipped_lines(ny, a) * a.t_line;
+  if (offset > 0.0)
+    for (auto& v : lt.tread_ms) v -= offset;
+  return lt;
+}
+
+// ---- `sampling_mask` kspace.rs:546-588 ----
+std::vector<uint8_t> sampling_mask(size_t nx, size_t ny, const mrsim_acquisition& a) {
+  size_t ys = ny / 2;
+  size_t accel = std::max<int64_t>(a.accel, 1);
+  std::vector<uint8_t> m(nx * ny, 0);
+  size_t keep_n = (size_t)std::round((double)ny * a.partial_fourier);
+  for (size_t kyi = 0; kyi < ny; ++kyi) {
+    if (a.partial_fourier < 1.0 && a.pf_mode == MRSIM_PF_SCANNER) {
+      bool skip = a.reverse_phase ? (kyi < ny - keep_n) : (kyi >= keep_n);
+      if (skip) continue;
+    } else if (a.partial_fourier < 1.0 && a.pf_mode == MRSIM_PF_CONTIGUOUS) {
+      bool skip = a.reverse_phase ? (kyi >= keep_n) : (kyi < ny - keep_n);
+      if (skip) continue;
+    } else if (a.partial_fourier < 1.0) {
+      bool skip;
+      if (a.reverse_phase)
+        skip = (double)kyi > std::ceil((double)ny * a.partial_fourier);
+      else
+        skip = (double)kyi < std::floor((double)ny * (1.0 - a.partial_fourier)) && (kyi > 0 || ny % 2 == 1);
+      if (skip) continue;
+    }
+    bool acquired = accel <= 1 || kyi % accel == ys % accel;
+    if (!acquired) continue;
+    for (size_t kxi = 0; kxi < nx; ++kxi) m[kxi + nx * kyi] = 1;
+  }
+  return m;
+}
+
+std::vector<uint8_t> acquired_lines(size_t ny, const mrsim_acquisition& a) { return sampling_mask(1, ny, a); }
+
+// ---- `validate_acquisition_timing` kspace.rs:411-431 ----
+void validate_acquisition_timing(const mrsim_acquisition& a, size_t nx, size_t ny) {
+  LineTiming lt = line_timing_for(a, nx, ny);
+  auto mask = sampling_mask(nx, ny, a);
+  double worst = INFINITY;
+  for (size_t ky = 0; ky < ny; ++ky)
+    if (mask[ky * nx] && lt.trf_ms[ky] < worst) worst = lt.trf_ms[ky];
+  if (worst <= 0.0) {
+    char buf[512];
+    snprintf(buf, sizeof buf,
+             "trf = %.3f ms <= 0 on an acquired line: the readout starts before the excitation. Raise "
+             "t_echo above %.3f ms or shorten t_line. Partial Fourier helps only in Scanner mode (it skips "
+             "the first lines); the Fiberfox and Contiguous modes drop lines this trajectory reads last.",
+             worst, a.t_echo - worst);
+    throw Fail(buf);
+  }
+}
+
+// ---- `coil_sensitivity` kspace.rs:226-237 ----
+double coil_sensitivity(size_t coil, size_t n_coils, double x, double y, size_t nx, size_t ny) {
+  if (n_coils <= 1) return 1.0;
+  double cx = (double)nx / 2.0, cy = (double)ny / 2.0;
+  double r = 0.6 * (double)std::max(nx, ny);
+  double ang = TAU * (double)coil / (double)n_coils;
+  double px = cx + r * std::cos(ang), py = cy + r * std::sin(ang);
+  double dx = x - px, dy = y - py;
+  double d2 = dx * dx + dy * dy;
+  double sigma = 0.9 * (double)std::max(nx, ny);
+  return std::exp(-d2 / (2.0 * sigma * sigma)) + 0.15;
+}
+
+// ---- `KspaceWindow::at` kspace.rs:140-161 ----
+double window_at(const mrsim_acquisition& a, double kx, double ky) {
+  double r = 2.0 * std::sqrt(kx * kx + ky * ky);
+  switch (a.window_kind) {
+    case MRSIM_WINDOW_NONE:
+      return 1.0;
+    case MRSIM_WINDOW_HANN:
+      return r >= 1.0 ? 0.0 : 0.5 * (1.0 + std::cos(PI * r));
+    case MRSIM_WINDOW_TUKEY: {
+      double al = std::min(std::max(a.window_a, 0.0), 1.0);
+      if (r <= 1.0 - al) return 1.0;
+      if (r >= 1.0) return 0.0;
+      return 0.5 * (1.0 + std::cos(PI * (r - (1.0 - al)) / std::max(al, 1e-12)));
+    }
+    case MRSIM_WINDOW_FERMI:
+      return 1.0 / (1.0 + std::exp((r - a.window_a) / std::max(a.window_b, 1e-12)));
+  }
+  return 1.0;
+}
+
+bool eddy_enabled(const mrsim_acquisition& a, const mrsim_slice_input& inp) {
+  return a.eddy_strength != 0.0 && inp.has_eddy_drive;
+}
+
+// T2 accessors (`T2Slice` kspace.rs:380-386)
+inline double t2_value(const mrsim_t2& t, size_t i) { return t.is_map ? (double)t.map[i] : (double)t.value; }
+
+// ---- `XStage` (default build, twiddle tables) kspace.rs:1052-1140 ----
+struct XStage {
+  size_t snx, nx;
+  std::vector<Cx> tw[2];
+  XStage(size_t snx_, size_t nx_, size_t xs, size_t sxs, double xoff, double ghost) : snx(snx_), nx(nx_) {
+    double c = (double)sxs + xoff;
+    double gh[2] = {ghost, -ghost};
+    for (int p = 0; p < 2; ++p) {
+      tw[p].reserve(snx * nx);
+      for (size_t kxi = 0; kxi < nx; ++kxi) {
+        double kx_norm = ((double)kxi - (double)xs + gh[p]) / (double)snx;
+        for (size_t x = 0; x < snx; ++x) {
+          double ph = TAU * kx_norm * ((double)x - c);
+          tw[p].push_back({std::cos(ph), std::sin(ph)});
+        }
+      }
+    }
+  }
+  void run(const double* g_re, const double* g_im, double ghost_shift, Cx* out) const {
+    int pol = ghost_shift < 0.0 ? 1 : 0;
+    const std::vector<Cx>& t = tw[pol];
+    for (size_t kxi = 0; kxi < nx; ++kxi) {
+      const Cx* row = &t[snx * kxi];
+      double ar = 0.0, ai = 0.0;
+      for (size_t x = 0; x < snx; ++x) {
+        double tr = row[x].re, ti = row[x].im;
+        ar += g_re[x] * tr - g_im[x] * ti;
+        ai += g_re[x] * ti + g_im[x] * tr;
+      }
+      out[kxi] = {ar, ai};
+    }
+  }
+};
+
+// ---- `build_coil_kspace_timed` kspace.rs:607-1042 (default build: rotor y-stage) ----
+std::vector<Cx> build_coil_kspace_timed(const mrsim_slice_input& inp, const mrsim_acquisition& acq, size_t coil,
+                                        size_t ncoils, const LineTiming& timing, const double* log_amp) {
+  size_t snx = inp.sim[0], sny = inp.sim[1], nx = inp.acq_matrix[0], ny = inp.acq_matrix[1];
+  if (!(snx % nx == 0 && sny % ny == 0)) throw Fail("sim grid must be an integer multiple of the acquired matrix");
+  if (!(timing.t_ms.size() == ny && timing.trf_ms.size() == ny && timing.tread_ms.size() == ny &&
+        timing.polarity.size() == ny))
+    throw Fail("line-timing table must have one entry per phase-encode line");
+  size_t z = inp.z, nz = inp.nz;
+  size_t ncomp = inp.ncomp;
+  const double* t_ms = timing.t_ms.data();
+  const double* trf_ms = timing.trf_ms.data();
+  const double* tread_ms = timing.tread_ms.data();
+  double gradient[3] = {0.0, 0.0, 0.0};
+  if (inp.has_eddy_drive)
+    for (int i = 0; i < 3; ++i) gradient[i] = inp.eddy_drive[i];
+  bool do_eddy = eddy_enabled(acq, inp);
+  bool do_eddy_phase = acq.eddy_phase != 0.0 && inp.has_eddy_drive;
+  size_t xs = nx / 2, ys = ny / 2, zs = nz / 2;
+  size_t ox = snx / nx, oy = sny / ny;
+  size_t sxs = ox * xs, sys = oy * ys;
+  double xoff = ((double)ox - 1.0) / 2.0, yoff = ((double)oy - 1.0) / 2.0;
+  size_t nvox = snx * sny;
+  auto mask = sampling_mask(nx, ny, acq);
+
+  const size_t REANCHOR = 32;
+  double zc = (double)z - (double)zs;
+  double zc_c = (double)z - ((double)nz - 1.0) / 2.0;
+  std::vector<double> amp(nvox), phi0(nvox), rate(nvox);
+  for (size_t y = 0; y < sny; ++y) {
+    for (size_t x = 0; x < snx; ++x) {
+      size_t i = x + snx * y;
+      double xa = ((double)x - xoff) / (double)ox, ya = ((double)y - yoff) / (double)oy;
+      amp[i] = acq.signal_scale * coil_sensitivity(coil, ncoils, xa, ya, nx, ny);
+      double xc = ((double)x - (double)sxs - xoff) / (double)ox;
+      double yc = ((double)y - (double)sys - yoff) / (double)oy;
+      double p0 = inp.phase0 ? inp.phase0[i] : 0.0;
+      if (do_eddy_phase) p0 += acq.eddy_phase * (gradient[0] * xc + gradient[1] * yc + gradient[2] * zc_c);
+      if (acq.echo == MRSIM_ECHO_GRADIENT && acq.do_distortions)
+        p0 += TAU * (double)inp.fmap[i] * (acq.t_echo / 1000.0);
+      phi0[i] = p0;
+      rate[i] = acq.do_distortions ? (double)inp.fmap[i] : 0.0;
+    }
+  }
+  auto xc_of = [&](size_t x) { return ((double)x - (double)sxs - xoff) / (double)ox; };
+  auto yc_of = [&](size_t y) { return ((double)y - (double)sys - yoff) / (double)oy; };
+  auto ky_norm_of = [&](size_t kyi) { return ((double)kyi - (double)ys) / (double)sny; };
+
+  std::vector<double> st_re(nvox, 0.0), st_im(nvox, 0.0);
+  auto set_state = [&](size_t kyi) {
+    double t = t_ms[kyi] / 1000.0;
+    double kyn = ky_norm_of(kyi);
+    for (size_t y = 0; y < sny; ++y) {
+      double yy = (double)y - (double)sys - yoff;
+      for (size_t x = 0; x < snx; ++x) {
+        size_t i = x + snx * y;
+        double ph = phi0[i] + TAU * (rate[i] * t + kyn * yy);
+        st_re[i] = amp[i] * std::cos(ph);
+        st_im[i] = amp[i] * std::sin(ph);
+      }
+    }
+  };
+  struct Rotor {
+    size_t k0, k1;
+    double dt, dkyn;
+    std::vector<double> re, im;
+  };
+  std::vector<Rotor> rotors;
+
+  bool uniform = true;
+  for (size_t c = 0; c < ncomp; ++c) uniform = uniform && !inp.t2[c].is_map;
+  if (inp.t_inhom)
+    for (size_t c = 0; c < ncomp; ++c) uniform = uniform && !inp.t_inhom[c].is_map;
+  uniform = uniform && log_amp == nullptr;
+
+  std::vector<double> rel(ncomp, 1.0);
+  std::vector<double> ex_re(snx, 1.0), ex_im(snx, 0.0), ey_re(sny, 1.0), ey_im(sny, 0.0);
+  std::vector<double> g_re(snx, 0.0), g_im(snx, 0.0);
+  XStage xstage(snx, nx, xs, sxs, xoff, acq.ghost_offset);
+
+  std::vector<Cx> kspace(nx * ny, CZERO);
+  bool have_prev = false;
+  size_t prev = 0;
+  size_t since_anchor = 0;
+  for (size_t kyi = 0; kyi < ny; ++kyi) {
+    if (!mask[nx * kyi]) continue;
+    double t = t_ms[kyi] / 1000.0;
+    double trf = trf_ms[kyi];
+    if (have_prev && since_anchor < REANCHOR) {
+      size_t p = prev;
+      size_t k0 = kyi - p, k1 = p % 2;
+      double dt = t - t_ms[p] / 1000.0;
+      double dkyn = ky_norm_of(kyi) - ky_norm_of(p);
+      size_t idx = rotors.size();
+      for (size_t r = 0; r < rotors.size(); ++r)
+        if (rotors[r].k0 == k0 && rotors[r].k1 == k1) {
+          idx = r;
+          break;
+        }
+      if (idx == rotors.size()) {
+        Rotor R{k0, k1, dt, dkyn, std::vector<double>(nvox), std::vector<double>(nvox)};
+        for (size_t y = 0; y < sny; ++y) {
+          double yy = (double)y - (double)sys - yoff;
+          for (size_t x = 0; x < snx; ++x) {
+            size_t i = x + snx * y;
+            double ph = TAU * (rate[i] * dt + dkyn * yy);
+            R.re[i] = std::cos(ph);
+            R.im[i] = std::sin(ph);
+          }
+        }
+        rotors.push_back(std::move(R));
+      }
+      const Rotor& r = rotors[idx];
+      if (std::fabs(r.dt - dt) <= 1e-12 * std::max(std::fabs(dt), 1e-300) && r.dkyn == dkyn) {
+        for (size_t i = 0; i < nvox; ++i) {
+          double a = st_re[i], b = st_im[i];
+          st_re[i] = a * r.re[i] - b * r.im[i];
+          st_im[i] = a * r.im[i] + b * r.re[i];
+        }
+        since_anchor += 1;
+      } else {
+        set_state(kyi);
+        since_anchor = 0;
+      }
+    } else {
+      set_state(kyi);
+      since_anchor = 0;
+    }
+    prev = kyi;
+    have_prev = true;
+
+    if (uniform) {
+      for (size_t c = 0; c < ncomp; ++c) {
+        if (acq.do_relaxation) {
+          double t2c = (double)inp.t2[c].value;
+          double tic = inp.t_inhom ? (double)inp.t_inhom[c].value : acq.t_inhom;
+          if (acq.echo == MRSIM_ECHO_SPIN)
+            rel[c] = std::exp(-trf / t2c - std::fabs(t) * 1000.0 / tic);
+          else
+            rel[c] = std::exp(-trf / t2c - trf / tic);
+        } else {
+          rel[c] = 1.0;
+        }
+      }
+    }
+    double ez_re = 1.0, ez_im = 0.0;
+    if (do_eddy) {
+      double eddy_decay = std::exp(-tread_ms[kyi] / acq.eddy_tau) * t;
+      for (size_t x = 0; x < snx; ++x) {
+        double xc = xc_of(x);
+        double ph = TAU * (acq.eddy_strength * gradient[0] * xc + acq.eddy_quad * gradient[0] * xc * xc) * eddy_decay;
+        ex_re[x] = std::cos(ph);
+        ex_im[x] = std::sin(ph);
+      }
+      for (size_t y = 0; y < sny; ++y) {
+        double yc = yc_of(y);
+        double ph = TAU * (acq.eddy_strength * gradient[1] * yc + acq.eddy_quad * gradient[1] * yc * yc) * eddy_decay;
+        ey_re[y] = std::cos(ph);
+        ey_im[y] = std::sin(ph);
+      }
+      double ph = TAU * (acq.eddy_strength * gradient[2] * zc + acq.eddy_quad * gradient[2] * zc * zc) * eddy_decay;
+      ez_re = std::cos(ph);
+      ez_im = std::sin(ph);
+    }
+    std::fill(g_re.begin(), g_re.end(), 0.0);
+    std::fill(g_im.begin(), g_im.end(), 0.0);
+    for (size_t y = 0; y < sny; ++y) {
+      size_t row = snx * y;
+      double eyr = ey_re[y], eyi = ey_im[y];
+      for (size_t x = 0; x < snx; ++x) {
+        size_t i = row + x;
+        double w = 0.0;
+        for (size_t c = 0; c < ncomp; ++c) {
+          double r;
+          if (uniform) {
+            r = rel[c];
+          } else if (acq.do_relaxation) {
+            double t2c = t2_value(inp.t2[c], i);
+            double tic = inp.t_inhom ? t2_value(inp.t_inhom[c], i) : acq.t_inhom;
+            bool spin = acq.echo == MRSIM_ECHO_SPIN;
+            if (!log_amp)
+              r = spin ? std::exp(-trf / t2c - std::fabs(t) * 1000.0 / tic) : std::exp(-trf / t2c - trf / tic);
+            else
+              r = spin ? std::exp(log_amp[i] - trf / t2c - std::fabs(t) * 1000.0 / tic)
+                       : std::exp(log_amp[i] - trf / t2c - trf / tic);
+          } else {
+            r = 1.0;
+          }
+          w += r * (double)inp.compartments[c][i];
+        }
+        double sr = st_re[i], si = st_im[i];
+        double mr, mi;
+        if (do_eddy) {
+          mr = sr * eyr - si * eyi;
+          mi = sr * eyi + si * eyr;
+        } else {
+          mr = sr;
+          mi = si;
+        }
+        g_re[x] += w * mr;
+        g_im[x] += w * mi;
+      }
+    }
+    if (do_eddy) {
+      for (size_t x = 0; x < snx; ++x) {
+        double a = g_re[x], b = g_im[x];
+        double fr = ex_re[x] * ez_re - ex_im[x] * ez_im, fi = ex_re[x] * ez_im + ex_im[x] * ez_re;
+        g_re[x] = a * fr - b * fi;
+        g_im[x] = a * fi + b * fr;
+      }
+    }
+    double ghost_shift = timing.polarity[kyi] < 0 ? -acq.ghost_offset : acq.ghost_offset;
+    xstage.run(g_re.data(), g_im.data(), ghost_shift, &kspace[nx * kyi]);
+  }
+  double n_inv = 1.0 / (double)nvox;
+  for (auto& k : kspace) {
+    k.re *= n_inv;
+    k.im *= n_inv;
+  }
+  // spikes kspace.rs:997-1019
+  if (acq.n_spikes > 0) {
+    Cx peak = CZERO;
+    double peak_mag = 0.0;
+    for (auto& k : kspace) {
+      double m = cabs_(k);
+      if (m > peak_mag) {
+        peak_mag = m;
+        peak = k;
+      }
+    }
+    Cx spike = cscale(peak, acq.spike_amplitude);
+    std::vector<size_t> acquired;
+    for (size_t i = 0; i < nx * ny; ++i)
+      if (mask[i]) acquired.push_back(i);
+    if (!acquired.empty()) {
+      Rng rng(inp.slice_seed ^ 0xA5A5123456789ABCull);
+      for (int64_t s = 0; s < acq.n_spikes; ++s) {
+        size_t pick = acquired[(size_t)(rng.next_u64() % (uint64_t)acquired.size())];
+        kspace[pick] = spike;
+      }
+    }
+  }
+  // noise kspace.rs:1021-1039
+  if (acq.noise_variance > 0.0) {
+    Rng rng((inp.slice_seed ^ ((uint64_t)coil * 0x9E3779B9ull)) | 1ull);
+    double sigma = std::sqrt(acq.noise_variance / (double)(nx * ny));
+    for (size_t i = 0; i < nx * ny; ++i) {
+      if (mask[i]) {
+        kspace[i].re += rng.gauss() * sigma;
+        kspace[i].im += rng.gauss() * sigma;
+      }
+    }
+  }
+  return kspace;
+}
+
+std::vector<Cx> build_coil_kspace(const mrsim_slice_input& inp, const mrsim_acquisition& acq, size_t coil,
+                                  size_t ncoils) {
+  return build_coil_kspace_timed(inp, acq, coil, ncoils,
+                                 line_timing_for(acq, inp.acq_matrix[0], inp.acq_matrix[1]), nullptr);
+}
+
+std::vector<std::vector<Cx>> build_coil_kspaces(const mrsim_slice_input& inp, const mrsim_acquisition& acq) {
+  size_t nc = std::max<int64_t>(acq.n_coils, 1);
+  std::vector<std::vector<Cx>> out;
+  for (size_t c = 0; c < nc; ++c) out.push_back(build_coil_kspace(inp, acq, c, nc));
+  return out;
+}
+
+// ---- literal per-line sum, `reference_coil_kspace` kspace.rs:2225-2406 (test oracle) ----
+std::vector<Cx> reference_coil_kspace(const mrsim_slice_input& inp, const mrsim_acquisition& acq, size_t coil,
+                                      size_t ncoils) {
+  size_t snx = inp.sim[0], sny = inp.sim[1], nx = inp.acq_matrix[0], ny = inp.acq_matrix[1];
+  if (!(snx % nx == 0 && sny % ny == 0)) throw Fail("sim grid must be an integer multiple of the acquired matrix");
+  size_t z = inp.z;
+  Epi epi{nx, ny, acq.t_line, acq.t_echo, acq.reverse_phase != 0};
+  std::vector<double> t_ms(ny, 0.0), trf_ms(ny, 0.0), tread_ms(ny, 0.0);
+  for (size_t tick = 0; tick < nx * ny; ++tick) {
+    size_t kx, ky;
+    epi.kspace_index(tick, kx, ky);
+    if (kx == nx / 2) {
+      t_ms[ky] = epi.time_from_max_echo(tick);
+      trf_ms[ky] = epi.time_from_rf(tick);
+      tread_ms[ky] = epi.time_from_prep_gradient(tick);
+    }
+  }
+  double skip = (double)pf_skipped_lines(ny, acq) * acq.t_line;
+  for (auto& v : tread_ms) v -= skip;
+  double gradient[3] = {0, 0, 0};
+  if (inp.has_eddy_drive)
+    for (int i = 0; i < 3; ++i) gradient[i] = inp.eddy_drive[i];
+  bool do_eddy = eddy_enabled(acq, inp);
+  bool do_eddy_phase = acq.eddy_phase != 0.0 && inp.has_eddy_drive;
+  size_t xs = nx / 2, ys = ny / 2, zs = inp.nz / 2;
+  size_t ox = snx / nx, oy = sny / ny;
+  size_t sxs = ox * xs, sys = oy * ys;
+  double xoff = ((double)ox - 1.0) / 2.0, yoff = ((double)oy - 1.0) / 2.0;
+  auto mask = sampling_mask(nx, ny, acq);
+  std::vector<Cx> kspace(nx * ny, CZERO);
+  double n_inv = 1.0 / (double)(snx * sny);
+  std::vector<Cx> modimg(snx * sny);
+  std::vector<Cx> g(snx);
+  for (size_t kyi = 0; kyi < ny; ++kyi) {
+    if (!mask[nx * kyi]) continue;
+    double t = t_ms[kyi] / 1000.0;
+    double trf = trf_ms[kyi];
+    double ky_norm = ((double)kyi - (double)ys) / (double)sny;
+    double ghost_shift = (kyi % 2 == 1) ? -acq.ghost_offset : acq.ghost_offset;
+    double eddy_decay = do_eddy ? std::exp(-tread_ms[kyi] / acq.eddy_tau) * t : 0.0;
+    for (size_t y = 0; y < sny; ++y) {
+      for (size_t x = 0; x < snx; ++x) {
+        size_t i = x + snx * y;
+        double f_real = 0.0;
+        for (size_t c = 0; c < (size_t)inp.ncomp; ++c) {
+          double v = (double)inp.compartments[c][i];
+          if (acq.do_relaxation) {
+            double t2c = t2_value(inp.t2[c], i);
+            double tic = inp.t_inhom ? t2_value(inp.t_inhom[c], i) : acq.t_inhom;
+            double inhom_ms = acq.echo == MRSIM_ECHO_SPIN ? std::fabs(t) * 1000.0 : trf;
+            v *= std::exp(-trf / t2c - inhom_ms / tic);
+          }
+          f_real += v;
+        }
+        double xa = ((double)x - xoff) / (double)ox, ya = ((double)y - yoff) / (double)oy;
+        f_real *= acq.signal_scale * coil_sensitivity(coil, ncoils, xa, ya, nx, ny);
+        double t_b0 = acq.echo == MRSIM_ECHO_SPIN ? t : t + acq.t_echo / 1000.0;
+        double phi = acq.do_distortions ? (double)inp.fmap[i] * t_b0 : 0.0;
+        double phi0 = inp.phase0 ? inp.phase0[i] : 0.0;
+        if (do_eddy || do_eddy_phase) {
+          double xc = ((double)x - (double)sxs - xoff) / (double)ox;
+          double yc = ((double)y - (double)sys - yoff) / (double)oy;
+          double zc = (double)z - (double)zs;
+          if (do_eddy) {
+            double lin = gradient[0] * xc + gradient[1] * yc + gradient[2] * zc;
+            double quad = gradient[0] * xc * xc + gradient[1] * yc * yc + gradient[2] * zc * zc;
+            phi += (acq.eddy_strength * lin + acq.eddy_quad * quad) * eddy_decay;
+          }
+          if (do_eddy_phase) {
+            double zc_c = (double)z - ((double)inp.nz - 1.0) / 2.0;
+            phi0 += acq.eddy_phase * (gradient[0] * xc + gradient[1] * yc + gradient[2] * zc_c);
+          }
+        }
+        modimg[i] = cscale(ccis(TAU * phi + phi0), f_real);
+      }
+    }
+    for (size_t x = 0; x < snx; ++x) {
+      Cx acc = CZERO;
+      for (size_t y = 0; y < sny; ++y) {
+        Cx ph = ccis(TAU * ky_norm * ((double)y - (double)sys - yoff));
+        acc = cadd(acc, cmul(modimg[x + snx * y], ph));
+      }
+      g[x] = acc;
+    }
+    for (size_t kxi = 0; kxi < nx; ++kxi) {
+      double kx_norm = ((double)kxi - (double)xs + ghost_shift) / (double)snx;
+      Cx acc = CZERO;
+      for (size_t x = 0; x < snx; ++x)
+        acc = cadd(acc, cmul(g[x], ccis(TAU * kx_norm * ((double)x - (double)sxs - xoff))));
+      kspace[kxi + nx * kyi] = cscale(acc, n_inv);
+    }
+  }
+  return kspace;
+}
+
+// ---- `inverse_2d` kspace.rs:1428-1453 ----
+std::vector<Cx> inverse_2d(const std::vector<Cx>& k, size_t nx, size_t ny, size_t xs, size_t ys) {
+  std::vector<Cx> h(nx * ny, CZERO), out(nx * ny, CZERO);
+  for (size_t kxi = 0; kxi < nx; ++kxi)
+    for (size_t y = 0; y < ny; ++y) {
+      Cx acc = CZERO;
+      for (size_t kyi = 0; kyi < ny; ++kyi) {
+        double ky_norm = ((double)kyi - (double)ys) / (double)ny;
+        acc = cadd(acc, cmul(k[kxi + nx * kyi], ccis(-TAU * ky_norm * ((double)y - (double)ys))));
+      }
+      h[kxi + nx * y] = acc;
+    }
+  for (size_t y = 0; y < ny; ++y)
+    for (size_t x = 0; x < nx; ++x) {
+      Cx acc = CZERO;
+      for (size_t kxi = 0; kxi < nx; ++kxi) {
+        double kx_norm = ((double)kxi - (double)xs) / (double)nx;
+        acc = cadd(acc, cmul(h[kxi + nx * y], ccis(-TAU * kx_norm * ((double)x - (double)xs))));
+      }
+      out[x + nx * y] = acc;
+    }
+  return out;
+}
+
+// ---- `solve_hermitian` kspace.rs:1457-1491 ----
+std::vector<Cx> solve_hermitian(std::vector<std::vector<Cx>> h, std::vector<Cx> b) {
+  size_t n = b.size();
+  auto recip = [](Cx d) -> Cx {
+    double m2 = d.re * d.re + d.im * d.im;
+    if (m2 < 1e-18) return CZERO;
+    return {d.re / m2, -d.im / m2};
+  };
+  for (size_t col = 0; col < n; ++col) {
+    size_t piv = col;
+    double best = cabs_(h[col][col]);
+    for (size_t r = col + 1; r < n; ++r) {
+      double m = cabs_(h[r][col]);
+      if (m > best) {
+        best = m;
+        piv = r;
+      }
+    }
+    std::swap(h[col], h[piv]);
+    std::swap(b[col], b[piv]);
+    Cx dinv = recip(h[col][col]);
+    for (size_t r = col + 1; r < n; ++r) {
+      Cx f = cmul(h[r][col], dinv);
+      for (size_t c = col; c < n; ++c) {
+        Cx s = cmul(f, h[col][c]);
+        h[r][c] = cadd(h[r][c], cscale(s, -1.0));
+      }
+      Cx sb = cmul(f, b[col]);
+      b[r] = cadd(b[r], cscale(sb, -1.0));
+    }
+  }
+  std::vector<Cx> x(n, CZERO);
+  for (size_t col = n; col-- > 0;) {
+    Cx s = b[col];
+    for (size_t c = col + 1; c < n; ++c) s = cadd(s, cscale(cmul(h[col][c], x[c]), -1.0));
+    x[col] = cmul(s, recip(h[col][col]));
+  }
+  return x;
+}
+
+// ---- `GrappaKernel` kspace.rs:1508-1633 ----
+const int64_t GRAPPA_DKX[3] = {-1, 0, 1};
+const double GRAPPA_LAMBDA = 1e-3;
+
+void grappa_feature(const std::vector<std::vector<Cx>>& coil, size_t nx, size_t s0, size_t s1, size_t kx,
+                    std::vector<Cx>& f) {
+  size_t nc = coil.size();
+  f.assign(6 * nc, CZERO);
+  size_t sl[2] = {s0, s1};
+  for (size_t li = 0; li < 2; ++li)
+    for (size_t ki = 0; ki < 3; ++ki) {
+      int64_t v = ((int64_t)kx + GRAPPA_DKX[ki]) % (int64_t)nx;
+      if (v < 0) v += (int64_t)nx;
+      for (size_t ci = 0; ci < nc; ++ci) f[(li * 3 + ki) * nc + ci] = coil[ci][(size_t)v + nx * sl[li]];
+    }
+}
+
+struct GrappaKernel {
+  size_t accel = 1;
+  std::vector<std::vector<std::vector<Cx>>> weights;  // [d-1][out coil][feature]
+};
+
+GrappaKernel grappa_fit(const std::vector<std::vector<Cx>>& coil, size_t nx, size_t ny, size_t accel, size_t acs_lines,
+                        const std::vector<uint8_t>& lines) {
+  if (lines.size() != ny) throw Fail("one acquired-line flag per PE line");
+  size_t nc = coil.size();
+  size_t ys = ny / 2;
+  size_t nfeat = 6 * nc;
+  int64_t acs_half = (int64_t)(acs_lines / 2);
+  size_t acs_lo = (size_t)std::max<int64_t>((int64_t)ys - acs_half, 0);
+  size_t acs_hi = std::min<size_t>((size_t)((int64_t)ys + acs_half), ny - 1);
+  GrappaKernel K;
+  K.accel = accel;
+  std::vector<Cx> f;
+  for (size_t d = 1; d < accel; ++d) {
+    std::vector<std::vector<Cx>> aha(nfeat, std::vector<Cx>(nfeat, CZERO));
+    std::vector<std::vector<Cx>> ahb(nc, std::vector<Cx>(nfeat, CZERO));
+    for (size_t b = acs_lo; b < acs_hi; ++b) {
+      size_t s0 = b, s1 = b + accel, tgt = b + d;
+      if (s1 > acs_hi || tgt > acs_hi || !(lines[s0] && lines[s1] && lines[tgt])) continue;
+      for (size_t kx = 0; kx < nx; ++kx) {
+        grappa_feature(coil, nx, s0, s1, kx, f);
+        for (size_t i = 0; i < nfeat; ++i) {
+          Cx fic = {f[i].re, -f[i].im};
+          for (size_t j = 0; j < nfeat; ++j) aha[i][j] = cadd(aha[i][j], cmul(fic, f[j]));
+          for (size_t co = 0; co < nc; ++co) ahb[co][i] = cadd(ahb[co][i], cmul(fic, coil[co][kx + nx * tgt]));
+        }
+      }
+    }
+    double sum = -0.0;
+    for (size_t i = 0; i < nfeat; ++i) sum = sum + aha[i][i].re;
+    double mean_diag = sum / (double)nfeat;
+    if (mean_diag <= 0.0) {
+      K.weights.push_back(std::vector<std::vector<Cx>>(nc, std::vector<Cx>(nfeat, CZERO)));
+      continue;
+    }
+    double s = 1.0 / mean_diag;
+    for (size_t i = 0; i < nfeat; ++i) {
+      for (auto& x : aha[i]) x = cscale(x, s);
+      aha[i][i].re += GRAPPA_LAMBDA;
+    }
+    for (auto& bb : ahb)
+      for (auto& x : bb) x = cscale(x, s);
+    std::vector<std::vector<Cx>> w;
+    for (size_t co = 0; co < nc; ++co) w.push_back(solve_hermitian(aha, ahb[co]));
+    K.weights.push_back(std::move(w));
+  }
+  return K;
+}
+
+void grappa_apply(const GrappaKernel& K, std::vector<std::vector<Cx>>& coil, size_t nx, size_t ny,
+                  const std::vector<uint8_t>& acquired) {
+  if (acquired.size() != ny) throw Fail("one acquired-line flag per PE line");
+  size_t ys = ny / 2;
+  size_t accel = K.accel, nc = coil.size();
+  std::vector<Cx> f;
+  for (size_t di = 0; di < K.weights.size(); ++di) {
+    size_t d = di + 1;
+    const auto& weights = K.weights[di];
+    if (weights.size() != nc) throw Fail("the GRAPPA kernel was fitted for another coil count");
+    for (size_t ky = 0; ky < ny; ++ky) {
+      int64_t r = ((int64_t)ky - (int64_t)ys) % (int64_t)accel;
+      if (r < 0) r += (int64_t)accel;
+      if (r != (int64_t)d || ky < d || ky + accel - d >= ny) continue;
+      size_t s0 = ky - d, s1 = ky - d + accel;
+      if (!(acquired[s0] && acquired[s1])) continue;
+      for (size_t kx = 0; kx < nx; ++kx) {
+        grappa_feature(coil, nx, s0, s1, kx, f);
+        for (size_t co = 0; co < nc; ++co) {
+          Cx v = CZERO;
+          for (size_t i = 0; i < f.size(); ++i) v = cadd(v, cmul(weights[co][i], f[i]));
+          coil[co][kx + nx * ky] = v;
+        }
+      }
+    }
+  }
+}
+
+const uint64_t SEED_SALT_GRAPPA_CAL = 0x47525043414Cull;
+
+// `grappa_reference_kernel` kspace.rs:1253-1262
+GrappaKernel grappa_reference_kernel(const mrsim_slice_input& inp, const mrsim_acquisition& acq) {
+  mrsim_slice_input ref = inp;
+  ref.has_eddy_drive = 0;
+  ref.has_prep_drive = 0;
+  mrsim_acquisition acq_ref = acq;
+  acq_ref.accel = 1;
+  acq_ref.n_spikes = 0;
+  auto coils = build_coil_kspaces(ref, acq_ref);
+  return grappa_fit(coils, inp.acq_matrix[0], inp.acq_matrix[1], (size_t)acq.accel, (size_t)acq.acs_lines,
+                    acquired_lines(inp.acq_matrix[1], acq_ref));
+}
+
+// ---- `reconstruct_coils_full` kspace.rs:1301-1378 ----
+struct SliceRecon {
+  std::vector<std::vector<Cx>> acquired, reconstructed, coil_images;
+  std::vector<std::vector<double>> sensitivities;
+  std::vector<Cx> combined;
+  std::vector<uint8_t> mask;
+};
+
+SliceRecon reconstruct_coils_full(std::vector<std::vector<Cx>> coil_kspace, const mrsim_acquisition& acq, size_t nx,
+                                  size_t ny, bool cap_acq, bool cap_rec, bool cap_img, const GrappaKernel* kernel) {
+  size_t xs = nx / 2, ys = ny / 2;
+  size_t ncoils = std::max<int64_t>(acq.n_coils, 1);
+  size_t accel = std::max<int64_t>(acq.accel, 1);
+  if (coil_kspace.size() != ncoils) throw Fail("one k-space per coil");
+  SliceRecon R;
+  if (cap_acq) R.acquired = coil_kspace;
+  if (accel > 1) {
+    if (!kernel) throw Fail("an accelerated slice needs its GRAPPA kernel (fitted on a reference scan)");
+    if (kernel->accel != accel) throw Fail("the GRAPPA kernel was fitted for another acceleration");
+    grappa_apply(*kernel, coil_kspace, nx, ny, acquired_lines(ny, acq));
+  }
+  if (acq.window_kind != MRSIM_WINDOW_NONE) {
+    for (auto& ks : coil_kspace)
+      for (size_t kyi = 0; kyi < ny; ++kyi)
+        for (size_t kxi = 0; kxi < nx; ++kxi) {
+          double kx = ((double)kxi - (double)xs) / (double)nx;
+          double ky = ((double)kyi - (double)ys) / (double)ny;
+          double w = window_at(acq, kx, ky);
+          Cx& k = ks[kxi + nx * kyi];
+          k.re *= w;
+          k.im *= w;
+        }
+  }
+  if (cap_rec) R.reconstructed = coil_kspace;
+  R.sensitivities.resize(ncoils);
+  for (size_t coil = 0; coil < ncoils; ++coil) {
+    R.sensitivities[coil].resize(nx * ny);
+    for (size_t i = 0; i < nx * ny; ++i)
+      R.sensitivities[coil][i] = coil_sensitivity(coil, ncoils, (double)(i % nx), (double)(i / nx), nx, ny);
+  }
+  std::vector<Cx> wsum(nx * ny, CZERO);
+  std::vector<double> ssum(nx * ny, 0.0);
+  for (size_t coil = 0; coil < ncoils; ++coil) {
+    auto img = inverse_2d(coil_kspace[coil], nx, ny, xs, ys);
+    for (size_t i = 0; i < nx * ny; ++i) {
+      double s = R.sensitivities[coil][i];
+      wsum[i] = cadd(wsum[i], cscale(img[i], s));
+      ssum[i] += s * s;
+    }
+    if (cap_img) R.coil_images.push_back(std::move(img));
+  }
+  R.combined.resize(nx * ny);
+  for (size_t i = 0; i < nx * ny; ++i) {
+    double s = std::max(ssum[i], 1e-12);
+    R.combined[i] = {wsum[i].re / s, wsum[i].im / s};
+  }
+  R.mask = sampling_mask(nx, ny, acq);
+  return R;
+}
+
+// `simulate_slice_with` kspace.rs:1271-1284
+SliceRecon simulate_slice_with(const mrsim_slice_input& inp, const mrsim_acquisition& acq, bool ca, bool cr, bool ci,
+                               const GrappaKernel* kernel) {
+  GrappaKernel own;
+  if (!kernel && acq.accel > 1) {
+    mrsim_slice_input salted = inp;
+    salted.slice_seed = inp.slice_seed ^ SEED_SALT_GRAPPA_CAL;
+    own = grappa_reference_kernel(salted, acq);
+    kernel = &own;
+  }
+  return reconstruct_coils_full(build_coil_kspaces(inp, acq), acq, inp.acq_matrix[0], inp.acq_matrix[1], ca, cr, ci,
+                                kernel);
+}
+
+// ---- object phase: `PhaseModel` phase.rs:48-205, `phase_slice` kspace.rs:1156-1180 ----
+struct Shot {
+  double q[3] = {0, 0, 0}, dx[3] = {0, 0, 0}, rot[3] = {0, 0, 0};
+};
+
+double shot_at(const Shot& s, const double r[3]) {
+  double c[3] = {s.rot[1] * r[2] - s.rot[2] * r[1], s.rot[2] * r[0] - s.rot[0] * r[2],
+                 s.rot[0] * r[1] - s.rot[1] * r[0]};
+  double sum = -0.0;
+  for (int i = 0; i < 3; ++i) sum = sum + s.q[i] * (s.dx[i] + c[i]);
+  return sum;
+}
+
+Shot prep_shot(const mrsim_phase_model& p, double magnitude, const double dir[3], size_t volume, size_t slice_group,
+               uint64_t seed) {
+  Shot s;
+  double n = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+  if (magnitude <= 0.0 || n < 1e-12) return s;
+  double sc = p.c_q * std::sqrt(magnitude) / n;
+  for (int i = 0; i < 3; ++i) s.q[i] = dir[i] * sc;
+  Rng rng(seed ^ ((uint64_t)volume * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)slice_group * 0xBF58476D1CE4E5B9ull));
+  for (int i = 0; i < 3; ++i) s.dx[i] = rng.gauss() * p.sigma_dx;
+  for (int i = 0; i < 3; ++i) s.rot[i] = rng.gauss() * p.sigma_rot;
+  return s;
+}
+
+double model_at(const mrsim_phase_model& m, const double r[3], const Shot& s) {
+  const double* c = m.background;
+  double x = r[0], y = r[1], z = r[2];
+  double bg = c[0] + c[1] * x + c[2] * y + c[3] * z + c[4] * x * x + c[5] * y * y + c[6] * z * z + c[7] * x * y +
+              c[8] * x * z + c[9] * y * z;
+  return m.global + bg + shot_at(s, r);
+}
+
+std::vector<double> phase_slice(const mrsim_phase_model& m, const Shot& s, size_t snx, size_t sny, size_t o, size_t z,
+                                size_t nz) {
+  double sxs = (double)snx / 2.0, sys = (double)sny / 2.0;
+  double off = ((double)o - 1.0) / 2.0;
+  double zc = (double)z - (double)nz / 2.0;
+  std::vector<double> v(snx * sny);
+  for (size_t y = 0; y < sny; ++y)
+    for (size_t x = 0; x < snx; ++x) {
+      double r[3] = {((double)x - sxs - off) / (double)o, ((double)y - sys - off) / (double)o, zc};
+      v[x + snx * y] = model_at(m, r, s);
+    }
+  return v;
+}
+
+// ---- series: `acquire_volumes_complex` kspace.rs:1851-2125 ----
+uint64_t grappa_cal_slice_seed(size_t z, uint64_t seed) {
+  return ((uint64_t)z * 0x9E37ull) ^ seed ^ SEED_SALT_GRAPPA_CAL;
+}
+
+void validate_t2_volumes(const char* what, const mrsim_t2* vols, size_t ncomp, size_t nvox) {
+  (void)nvox;
+  for (size_t c = 0; c < ncomp; ++c) {
+    if (!vols[c].is_map) continue;
+    for (size_t i = 0; i < nvox; ++i) {
+      float v = vols[c].map[i];
+      if (std::isnan(v) || v <= 0.0f) {
+        char buf[256];
+        snprintf(buf, sizeof buf, "%s map for compartment %zu: T2 map value %g at index %zu is not strictly positive",
+                 what, c, (double)v, i);
+        throw Fail(buf);
+      }
+    }
+  }
+}
+
+struct SeriesOut {
+  std::vector<float> re, im;
+  // capture
+  std::vector<float> acquired, reconstructed, coil_images, combined, sensitivities;
+  std::vector<uint8_t> mask;
+};
+
+SeriesOut acquire_volumes_complex(const mrsim_acquisition_input& in, const mrsim_acquisition& acq,
+                                  const mrsim_acquisition_options* opts, uint64_t excitation_seed,
+                                  uint64_t receiver_seed, int threads) {
+  mrsim_acquisition_options dflt;
+  memset(&dflt, 0, sizeof dflt);
+  if (!opts) opts = &dflt;
+  size_t snx = in.sim_dims[0], sny = in.sim_dims[1], nz = in.sim_dims[2];
+  size_t nx = in.acq_dims[0], ny = in.acq_dims[1], nzo = in.acq_dims[2];
+  size_t nv = in.n_volumes;
+  if (nz != nzo) throw Fail("slice count must match; z is never oversampled");
+  if (!(snx % nx == 0 && sny % ny == 0)) throw Fail("sim grid must be an integer multiple of the acquired matrix");
+  size_t o = snx / nx;
+  if (o != sny / ny) throw Fail("oversampling must match on both axes");
+  size_t nvox_sim = snx * sny * nz, nvox_acq = nx * ny * nz;
+  size_t ncomp = in.ncomp;
+  validate_t2_volumes("T2", in.t2, ncomp, nvox_sim);
+  if (in.t_inhom) validate_t2_volumes("T2'", in.t_inhom, ncomp, nvox_sim);
+  if (!opts->t_echo_per_volume) {
+    validate_acquisition_timing(acq, nx, ny);
+  } else {
+    for (size_t g = 0; g < nv; ++g) {
+      mrsim_acquisition a = acq;
+      a.t_echo = opts->t_echo_per_volume[g];
+      try {
+        validate_acquisition_timing(a, nx, ny);
+      } catch (Fail& e) {
+        throw Fail("volume " + std::to_string(g) + ": " + e.what());
+      }
+    }
+  }
+  size_t nz_full = opts->nz_full > 0 ? (size_t)opts->nz_full : nz;
+  if (opts->slice_z)
+    for (size_t zl = 0; zl < nz; ++zl)
+      if ((size_t)opts->slice_z[zl] >= nz_full)
+        throw Fail("slice_z entries must be below nz_full " + std::to_string(nz_full));
+  auto global_z = [&](size_t zl) { return opts->slice_z ? (size_t)opts->slice_z[zl] : zl; };
+  std::vector<size_t> captured;
+  for (int64_t i = 0; i < opts->n_kspace_slices; ++i) {
+    if ((size_t)opts->kspace_slices[i] >= nz)
+      throw Fail("kspace_slices index " + std::to_string(opts->kspace_slices[i]) + " out of range for " +
+                 std::to_string(nz) + " slices");
+    captured.push_back((size_t)opts->kspace_slices[i]);
+  }
+  auto slice_t2 = [&](const mrsim_t2* vols, size_t zl) {
+    std::vector<mrsim_t2> s(ncomp);
+    for (size_t c = 0; c < ncomp; ++c) {
+      s[c] = vols[c];
+      if (vols[c].is_map) s[c].map = vols[c].map + zl * snx * sny;
+    }
+    return s;
+  };
+  // GRAPPA kernels: one per distinct TE per slice, kspace.rs:1906-1968
+  std::vector<double> tes;
+  if (opts->t_echo_per_volume)
+    tes.assign(opts->t_echo_per_volume, opts->t_echo_per_volume + nv);
+  else
+    tes.push_back(acq.t_echo);
+  std::sort(tes.begin(), tes.end());
+  tes.erase(std::unique(tes.begin(), tes.end(),
+                        [](double a, double b) {
+                          uint64_t x, y;
+                          memcpy(&x, &a, 8);
+                          memcpy(&y, &b, 8);
+                          return x == y;
+                        }),
+            tes.end());
+  std::vector<std::pair<double, std::vector<GrappaKernel>>> kernels;
+  if (std::max<int64_t>(acq.accel, 1) > 1 && nv > 0) {
+    std::vector<std::vector<float>> owned;
+    std::vector<const float*> cal(ncomp);
+    uint64_t cal_seed;
+    if (opts->has_grappa_calibration) {
+      for (size_t c = 0; c < ncomp; ++c) cal[c] = opts->grappa_calibration_images[c];
+      cal_seed = opts->grappa_calibration_seed;
+    } else {
+      owned.resize(ncomp);
+      for (size_t c = 0; c < ncomp; ++c) {
+        owned[c].resize(nvox_sim);
+        for (size_t v = 0; v < nvox_sim; ++v) owned[c][v] = in.images[c][v * nv + 0];
+        cal[c] = owned[c].data();
+      }
+      cal_seed = receiver_seed;
+    }
+    Shot no_shot;
+    for (double te : tes) {
+      mrsim_acquisition acq_cal = acq;
+      acq_cal.t_echo = te;
+      std::vector<GrappaKernel> ks(nz);
+      parallel_for(nz, threads, [&](size_t zl) {
+        size_t z = global_z(zl);
+        std::vector<const float*> refs(ncomp);
+        for (size_t c = 0; c < ncomp; ++c) refs[c] = cal[c] + snx * sny * zl;
+        auto t2s = slice_t2(in.t2, zl);
+        std::vector<mrsim_t2> tis;
+        if (in.t_inhom) tis = slice_t2(in.t_inhom, zl);
+        auto phi = phase_slice(*in.phase, no_shot, snx, sny, o, z, nz_full);
+        mrsim_slice_input si;
+        memset(&si, 0, sizeof si);
+        si.compartments = refs.data();
+        si.ncomp = ncomp;
+        si.t2 = t2s.data();
+        si.t_inhom = in.t_inhom ? tis.data() : nullptr;
+        si.fmap = in.fmap + snx * sny * zl;
+        si.phase0 = phi.data();
+        si.sim[0] = snx;
+        si.sim[1] = sny;
+        si.acq_matrix[0] = nx;
+        si.acq_matrix[1] = ny;
+        si.z = z;
+        si.nz = nz_full;
+        si.slice_seed = grappa_cal_slice_seed(z, cal_seed);
+        ks[zl] = grappa_reference_kernel(si, acq_cal);
+      });
+      kernels.emplace_back(te, std::move(ks));
+    }
+  }
+  auto kernel_at = [&](double te, size_t zl) -> const GrappaKernel* {
+    for (auto& kv : kernels) {
+      uint64_t a, b;
+      memcpy(&a, &kv.first, 8);
+      memcpy(&b, &te, 8);
+      if (a == b) return zl < kv.second.size() ? &kv.second[zl] : nullptr;
+    }
+    return nullptr;
+  };
+
+  SeriesOut out;
+  out.re.assign(nvox_acq * nv, 0.0f);
+  out.im.assign(nvox_acq * nv, 0.0f);
+  size_t ncoils = std::max<int64_t>(acq.n_coils, 1);
+  size_t nsl = captured.size();
+  size_t per = nx * ny;
+  if (nsl) {
+    if (opts->capture_acquired) out.acquired.assign(nv * nsl * ncoils * per * 2, 0.0f);
+    if (opts->capture_reconstructed) out.reconstructed.assign(nv * nsl * ncoils * per * 2, 0.0f);
+    if (opts->capture_coil_images) out.coil_images.assign(nv * nsl * ncoils * per * 2, 0.0f);
+    out.combined.assign(nv * nsl * per * 2, 0.0f);
+  }
+  std::mutex mu;
+  parallel_for(nv, threads, [&](size_t g) {
+    {
+      mrsim_acquisition acq_g = acq;
+      if (opts->t_echo_per_volume) acq_g.t_echo = opts->t_echo_per_volume[g];
+      std::vector<std::vector<float>> cslices(ncomp, std::vector<float>(snx * sny));
+      std::vector<float> fslice(snx * sny);
+      for (size_t zl = 0; zl < nz; ++zl) {
+        size_t z = global_z(zl);
+        for (size_t y = 0; y < sny; ++y)
+          for (size_t x = 0; x < snx; ++x) {
+            size_t vox = x + snx * (y + sny * zl);
+            for (size_t c = 0; c < ncomp; ++c) cslices[c][x + snx * y] = in.images[c][vox * nv + g];
+            fslice[x + snx * y] = in.fmap[vox];
+          }
+        std::vector<const float*> refs(ncomp);
+        for (size_t c = 0; c < ncomp; ++c) refs[c] = cslices[c].data();
+        auto t2s = slice_t2(in.t2, zl);
+        std::vector<mrsim_t2> tis;
+        if (in.t_inhom) tis = slice_t2(in.t_inhom, zl);
+        Shot shot;
+        bool has_prep = in.prep_drive_set && in.prep_drive_set[g];
+        if (in.phase->has_prep && has_prep)
+          shot = prep_shot(*in.phase, in.prep_drive[4 * g], &in.prep_drive[4 * g + 1], g, z, excitation_seed);
+        auto phi = phase_slice(*in.phase, shot, snx, sny, o, z, nz_full);
+        uint64_t slice_seed = (((uint64_t)g * 0x1000001ull) + (uint64_t)z) * 0x9E37ull ^ receiver_seed;
+        size_t cap_pos = nsl;
+        for (size_t i = 0; i < nsl; ++i)
+          if (captured[i] == zl) {
+            cap_pos = i;
+            break;
+          }
+        bool want = cap_pos < nsl;
+        mrsim_slice_input si;
+        memset(&si, 0, sizeof si);
+        si.compartments = refs.data();
+        si.ncomp = ncomp;
+        si.t2 = t2s.data();
+        si.t_inhom = in.t_inhom ? tis.data() : nullptr;
+        si.fmap = fslice.data();
+        si.phase0 = phi.data();
+        si.sim[0] = snx;
+        si.sim[1] = sny;
+        si.acq_matrix[0] = nx;
+        si.acq_matrix[1] = ny;
+        si.z = z;
+        si.nz = nz_full;
+        bool has_eddy = in.eddy_drive_set && in.eddy_drive_set[g];
+        si.has_eddy_drive = has_eddy;
+        if (has_eddy)
+          for (int i = 0; i < 3; ++i) si.eddy_drive[i] = in.eddy_drive[3 * g + i];
+        si.has_prep_drive = has_prep;
+        if (has_prep) {
+          si.prep_magnitude = in.prep_drive[4 * g];
+          for (int i = 0; i < 3; ++i) si.prep_direction[i] = in.prep_drive[4 * g + 1 + i];
+        }
+        si.slice_seed = slice_seed;
+        const GrappaKernel* K = kernel_at(acq_g.t_echo, zl);
+        SliceRecon r = simulate_slice_with(si, acq_g, want && opts->capture_acquired,
+                                           want && opts->capture_reconstructed, want && opts->capture_coil_images,
+                                           K);
+        for (size_t y = 0; y < ny; ++y)
+          for (size_t x = 0; x < nx; ++x) {
+            Cx c = r.combined[x + nx * y];
+            float re = (float)c.re, im = (float)c.im;
+            size_t vox = x + nx * (y + ny * zl);
+            if (in.noise_sigma) {
+              double sd = (double)in.noise_sigma[vox];
+              if (sd > 0.0) {
+                size_t vox_g = x + nx * (y + ny * z);
+                Rng rng((receiver_seed ^ ((uint64_t)g * 0x9E3779B97F4A7C15ull) ^
+                         ((uint64_t)vox_g * 0xBF58476D1CE4E5B9ull)) |
+                        1ull);
+                re += (float)(rng.gauss() * sd);
+                im += (float)(rng.gauss() * sd);
+              }
+            }
+            out.re[vox * nv + g] = re;
+            out.im[vox * nv + g] = im;
+          }
+        if (want) {
+          size_t base = (g * nsl + cap_pos);
+          auto put = [&](std::vector<float>& dst, const std::vector<std::vector<Cx>>& src) {
+            for (size_t c = 0; c < ncoils; ++c)
+              for (size_t i = 0; i < per; ++i) {
+                dst[((base * ncoils + c) * per + i) * 2] = (float)src[c][i].re;
+                dst[((base * ncoils + c) * per + i) * 2 + 1] = (float)src[c][i].im;
+              }
+          };
+          if (opts->capture_acquired) put(out.acquired, r.acquired);
+          if (opts->capture_reconstructed) put(out.reconstructed, r.reconstructed);
+          if (opts->capture_coil_images) put(out.coil_images, r.coil_images);
+          for (size_t i = 0; i < per; ++i) {
+            out.combined[(base * per + i) * 2] = (float)r.combined[i].re;
+            out.combined[(base * per + i) * 2 + 1] = (float)r.combined[i].im;
+          }
+          if (g == 0) {
+            std::lock_guard<std::mutex> lk(mu);
+            {
+              out.mask = r.mask;
+              out.sensitivities.resize(ncoils * per);
+              for (size_t c = 0; c < ncoils; ++c)
+                for (size_t i = 0; i < per; ++i) out.sensitivities[c * per + i] = (float)r.sensitivities[c][i];
+            }
+          }
+        }
+      }
+    }
+  });
+  return out;
+}
+
+// ---- golden record: tests/golden_baseline.rs:28-126 ----
+struct GoldenCase {
+  std::string name;
+  std::vector<uint32_t> bits;
+};
+
+mrsim_acquisition acq_default() {
+  mrsim_acquisition a;
+  memset(&a, 0, sizeof a);
+  a.t_line = 1.0;
+  a.t_echo = 90.0;
+  a.t_inhom = 50.0;
+  a.signal_scale = 100.0;
+  a.reverse_phase = 0;
+  a.do_distortions = 1;
+  a.do_relaxation = 1;
+  a.noise_variance = 0.0;
+  a.partial_fourier = 1.0;
+  a.pf_mode = MRSIM_PF_FIBERFOX;
+  a.ghost_offset = 0.0;
+  a.eddy_strength = 0.0;
+  a.eddy_quad = 0.0;
+  a.eddy_phase = 0.0;
+  a.eddy_tau = 70.0;
+  a.n_spikes = 0;
+  a.spike_amplitude = 1.0;
+  a.window_kind = MRSIM_WINDOW_NONE;
+  a.n_coils = 1;
+  a.accel = 1;
+  a.acs_lines = 24;
+  a.seed = 0;
+  a.echo = MRSIM_ECHO_SPIN;
+  return a;
+}
+
+uint32_t f32bits(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  return u;
+}
+
+std::vector<GoldenCase> golden_outputs() {
+  std::vector<GoldenCase> out;
+  Rng rng(0xC0FFEE);
+  const size_t geo[3][3] = {{17, 70, 2}, {16, 40, 1}, {8, 9, 3}};
+  for (auto& gm : geo) {
+    size_t nx = gm[0], ny = gm[1], o = gm[2];
+    size_t snx = nx * o, sny = ny * o, n = snx * sny;
+    std::vector<std::vector<float>> comps(3, std::vector<float>(n));
+    for (size_t c = 0; c < 3; ++c)
+      for (size_t i = 0; i < n; ++i) {
+        double x = (double)(i % snx) / (double)snx, y = (double)(i / snx) / (double)sny;
+        double a = x - 0.5, b = y - 0.45;
+        double blob = std::exp(-((a * a + b * b) / (0.03 * (double)(c + 1))));
+        comps[c][i] = (float)(blob + 0.05 * rng.unit());
+      }
+    std::vector<float> fmap(n);
+    for (size_t i = 0; i < n; ++i) {
+      double x = (double)(i % snx) / (double)snx, y = (double)(i / snx) / (double)sny;
+      fmap[i] = (float)(300.0 * (std::sin(3.0 * x) * std::cos(2.0 * y + 1.0)) + 20.0 * rng.unit());
+    }
+    std::vector<double> phase0(n);
+    for (size_t i = 0; i < n; ++i) phase0[i] = TAU * rng.unit();
+    std::vector<float> t2map(n), timap(n);
+    for (size_t i = 0; i < n; ++i) {
+      t2map[i] = (float)(60.0 + 80.0 * ((double)(i % snx) / (double)snx));
+      timap[i] = (float)(30.0 + 40.0 * ((double)(i / snx) / (double)sny));
+    }
+    mrsim_acquisition full = acq_default();
+    full.do_distortions = 1;
+    full.do_relaxation = 1;
+    full.signal_scale = 100.0;
+    mrsim_t2 uniform[3] = {{nullptr, 70.0f, 0}, {nullptr, 100.0f, 0}, {nullptr, 2000.0f, 0}};
+    mrsim_t2 mapped[3] = {{t2map.data(), 0.0f, 1}, {nullptr, 100.0f, 0}, {t2map.data(), 0.0f, 1}};
+    mrsim_t2 ti_mapped[3] = {{timap.data(), 0.0f, 1}, {nullptr, 45.0f, 0}, {timap.data(), 0.0f, 1}};
+    struct Case {
+      const char* name;
+      mrsim_acquisition a;
+      bool has_eddy;
+      double eddy[3];
+      bool maps;
+    };
+    std::vector<Case> cases;
+    auto mk = [&](const char* name) {
+      Case c;
+      c.name = name;
+      c.a = full;
+      c.has_eddy = false;
+      c.eddy[0] = c.eddy[1] = c.eddy[2] = 0;
+      c.maps = false;
+      return c;
+    };
+    {
+      Case c = mk("clean");
+      c.a.do_distortions = 0;
+      c.a.do_relaxation = 0;
+      cases.push_back(c);
+    }
+    cases.push_back(mk("distortion+relaxation"));
+    {
+      Case c = mk("reverse");
+      c.a.reverse_phase = 1;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("ghost");
+      c.a.ghost_offset = 0.015;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("eddy-poly");
+      c.a.eddy_strength = 3.0;
+      c.a.eddy_quad = 0.4;
+      c.a.eddy_tau = 70.0;
+      c.has_eddy = true;
+      c.eddy[0] = 0.3;
+      c.eddy[1] = -0.8;
+      c.eddy[2] = 0.5;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("eddy-phase");
+      c.a.eddy_phase = 0.2;
+      c.has_eddy = true;
+      c.eddy[0] = 0.6;
+      c.eddy[1] = 0.6;
+      c.eddy[2] = 0.5;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("pf-fiberfox");
+      c.a.partial_fourier = 0.75;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("pf-contiguous-reverse");
+      c.a.partial_fourier = 0.75;
+      c.a.pf_mode = MRSIM_PF_CONTIGUOUS;
+      c.a.reverse_phase = 1;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("grappa-coils");
+      c.a.accel = 2;
+      c.a.acs_lines = 6;
+      c.a.n_coils = 4;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("grappa3");
+      c.a.accel = 3;
+      c.a.acs_lines = 8;
+      c.a.n_coils = 4;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("everything");
+      c.a.ghost_offset = 0.02;
+      c.a.eddy_strength = 2.0;
+      c.a.eddy_quad = 0.3;
+      c.a.eddy_phase = 0.1;
+      c.a.partial_fourier = 0.8;
+      c.a.accel = 2;
+      c.a.acs_lines = 8;
+      c.a.n_coils = 3;
+      c.has_eddy = true;
+      c.eddy[0] = 0.5;
+      c.eddy[1] = 0.5;
+      c.eddy[2] = 0.7;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("maps");
+      c.maps = true;
+      cases.push_back(c);
+    }
+    {
+      Case c = mk("maps-coils-noise");
+      c.a.n_coils = 3;
+      c.a.noise_variance = 4.0;
+      c.maps = true;
+      cases.push_back(c);
+    }
+    std::vector<const float*> refs = {comps[0].data(), comps[1].data(), comps[2].data()};
+    for (auto& cs : cases) {
+      mrsim_slice_input si;
+      memset(&si, 0, sizeof si);
+      si.compartments = refs.data();
+      si.ncomp = 3;
+      si.t2 = cs.maps ? mapped : uniform;
+      si.t_inhom = cs.maps ? ti_mapped : nullptr;
+      si.fmap = fmap.data();
+      si.phase0 = phase0.data();
+      si.sim[0] = snx;
+      si.sim[1] = sny;
+      si.acq_matrix[0] = nx;
+      si.acq_matrix[1] = ny;
+      si.z = 3;
+      si.nz = 9;
+      si.has_eddy_drive = cs.has_eddy;
+      for (int i = 0; i < 3; ++i) si.eddy_drive[i] = cs.eddy[i];
+      si.slice_seed = 7;
+      SliceRecon r = simulate_slice_with(si, cs.a, false, false, false, nullptr);
+      GoldenCase g;
+      g.name = "slice-" + std::to_string(nx) + "x" + std::to_string(ny) + "o" + std::to_string(o) + "-" + cs.name;
+      for (auto& c : r.combined) {
+        g.bits.push_back(f32bits((float)c.re));
+        g.bits.push_back(f32bits((float)c.im));
+      }
+      out.push_back(std::move(g));
+    }
+  }
+  // the two series cases
+  {
+    size_t nx = 16, ny = 16, nz = 3, o = 2, nv = 4;
+    size_t snx = nx * o, sny = ny * o, nsim = snx * sny * nz;
+    Rng r2(0xBA5E);
+    std::vector<std::vector<float>> images(2);
+    for (size_t c = 0; c < 2; ++c) {
+      std::vector<float> byv(nsim * nv);
+      for (size_t i = 0; i < nsim * nv; ++i) {
+        size_t v = i / nsim, vox = i % nsim;
+        double x = (double)(vox % snx) / (double)snx, y = (double)((vox / snx) % sny) / (double)sny;
+        double a = x - 0.5, b = y - 0.5;
+        double blob = std::exp(-((a * a + b * b) / 0.05));
+        byv[i] = (float)((1.0 + 0.1 * (double)c + 0.01 * (double)v) * blob + 0.02 * r2.unit());
+      }
+      images[c].resize(nsim * nv);
+      for (size_t g = 0; g < nv; ++g)
+        for (size_t vox = 0; vox < nsim; ++vox) images[c][vox * nv + g] = byv[g * nsim + vox];
+    }
+    std::vector<float> fmap(nsim), t2map(nsim);
+    for (size_t i = 0; i < nsim; ++i) {
+      fmap[i] = (float)(40.0 * ((double)(i % snx) / (double)snx - 0.5));
+      t2map[i] = (float)(50.0 + (double)(i % 7) * 10.0);
+    }
+    mrsim_acquisition a = acq_default();
+    a.n_coils = 3;
+    a.accel = 2;
+    a.acs_lines = 6;
+    a.noise_variance = 2.0;
+    a.signal_scale = 100.0;
+    a.t_echo = 30.0;
+    a.t_line = 0.5;
+    mrsim_phase_model pm;
+    memset(&pm, 0, sizeof pm);
+    pm.background[1] = 0.13;
+    pm.background[2] = 0.10;
+    pm.background[3] = 0.02;
+    pm.has_prep = 1;
+    pm.c_q = 0.0425;
+    pm.sigma_dx = 1.0;
+    pm.sigma_rot = 2.0e-3;
+    mrsim_t2 tu[2] = {{nullptr, 80.0f, 0}, {nullptr, 160.0f, 0}};
+    mrsim_t2 tm[2] = {{t2map.data(), 0.0f, 1}, {nullptr, 160.0f, 0}};
+    const char* names[2] = {"series-uniform", "series-mapped"};
+    std::vector<const float*> imgs = {images[0].data(), images[1].data()};
+    for (int k = 0; k < 2; ++k) {
+      mrsim_acquisition_input in;
+      memset(&in, 0, sizeof in);
+      in.sim_dims[0] = snx;
+      in.sim_dims[1] = sny;
+      in.sim_dims[2] = nz;
+      in.acq_dims[0] = nx;
+      in.acq_dims[1] = ny;
+      in.acq_dims[2] = nz;
+      in.n_volumes = nv;
+      in.ncomp = 2;
+      in.images = imgs.data();
+      in.t2 = k == 0 ? tu : tm;
+      in.fmap = fmap.data();
+      in.phase = &pm;
+      in.seed = 42;
+      SeriesOut so = acquire_volumes_complex(in, a, nullptr, 42, 42, 1);
+      GoldenCase g;
+      g.name = names[k];
+      size_t nn = so.re.size();
+      std::vector<uint32_t> mag(nn), ph(nn);
+      for (size_t i = 0; i < nn; ++i) {
+        float re = so.re[i], im = so.im[i];
+        mag[i] = f32bits(std::sqrt(re * re + im * im));
+        ph[i] = f32bits(std::atan2(im, re));
+      }
+      g.bits = mag;
+      g.bits.insert(g.bits.end(), ph.begin(), ph.end());
+      out.push_back(std::move(g));
+    }
+  }
+  return out;
+}
+
+thread_local std::string g_err;
+std::vector<GoldenCase>* g_golden = nullptr;
+
+template <class F>
+int guard(F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return 1;
+  }
+}
+
+void put_cx(const std::vector<Cx>& v, double* out) {
+  for (size_t i = 0; i < v.size(); ++i) {
+    out[2 * i] = v[i].re;
+    out[2 * i + 1] = v[i].im;
+  }
+}
+
+LineTiming timing_from(const mrsim_acquisition& acq, size_t nx, size_t ny, const double* t, const double* trf,
+                       const double* tread, const int8_t* pol) {
+  if (!t) return line_timing_for(acq, nx, ny);
+  LineTiming lt;
+  lt.t_ms.assign(t, t + ny);
+  lt.trf_ms.assign(trf, trf + ny);
+  lt.tread_ms.assign(tread, tread + ny);
+  lt.polarity.assign(pol, pol + ny);
+  return lt;
+}
+
+}  // namespace
+
+// ============================ C ABI for the test harness ===================================
+extern "C" {
+
+const char* oracle_last_error(void) { return g_err.c_str(); }
+
+int oracle_acquisition_default(mrsim_acquisition* a) {
+  *a = acq_default();
+  return 0;
+}
+
+int oracle_sampling_mask(int64_t nx, int64_t ny, const mrsim_acquisition* acq, uint8_t* mask) {
+  auto m = sampling_mask(nx, ny, *acq);
+  memcpy(mask, m.data(), m.size());
+  return 0;
+}
+
+int64_t oracle_pf_skipped_lines(int64_t ny, const mrsim_acquisition* acq) { return pf_skipped_lines(ny, *acq); }
+
+int oracle_line_timing(const mrsim_acquisition* acq, int64_t nx, int64_t ny, double* t, double* trf, double* tread,
+                       int8_t* pol) {
+  auto lt = line_timing_for(*acq, nx, ny);
+  memcpy(t, lt.t_ms.data(), ny * 8);
+  memcpy(trf, lt.trf_ms.data(), ny * 8);
+  memcpy(tread, lt.tread_ms.data(), ny * 8);
+  memcpy(pol, lt.polarity.data(), ny);
+  return 0;
+}
+
+int oracle_epi_order(const mrsim_acquisition* acq, int64_t nx, int64_t ny, int64_t* order) {
+  Epi epi{(size_t)nx, (size_t)ny, acq->t_line, acq->t_echo, acq->reverse_phase != 0};
+  for (int64_t line = 0; line < ny; ++line) {
+    size_t kx, ky;
+    epi.kspace_index(line * nx, kx, ky);
+    order[line] = ky;
+  }
+  return 0;
+}
+
+int oracle_validate_acquisition_timing(const mrsim_acquisition* acq, int64_t nx, int64_t ny) {
+  return guard([&] { validate_acquisition_timing(*acq, nx, ny); });
+}
+
+double oracle_coil_sensitivity(int64_t coil, int64_t n_coils, double x, double y, int64_t nx, int64_t ny) {
+  return coil_sensitivity(coil, n_coils, x, y, nx, ny);
+}
+
+double oracle_window_at(const mrsim_acquisition* acq, double kx, double ky) { return window_at(*acq, kx, ky); }
+
+// build_coil_kspace_timed for one coil (spikes and noise included).
+int oracle_build_coil_kspace(const mrsim_slice_input* inp, const mrsim_acquisition* acq, int64_t coil, int64_t ncoils,
+                             const double* t, const double* trf, const double* tread, const int8_t* pol,
+                             const double* log_amp, double* out) {
+  return guard([&] {
+    auto lt = timing_from(*acq, inp->acq_matrix[0], inp->acq_matrix[1], t, trf, tread, pol);
+    put_cx(build_coil_kspace_timed(*inp, *acq, coil, ncoils, lt, log_amp), out);
+  });
+}
+
+// the literal sum (no spikes/noise)
+int oracle_reference_coil_kspace(const mrsim_slice_input* inp, const mrsim_acquisition* acq, int64_t coil,
+                                 int64_t ncoils, double* out) {
+  return guard([&] { put_cx(reference_coil_kspace(*inp, *acq, coil, ncoils), out); });
+}
+
+int oracle_inverse_2d(const double* k, int64_t nx, int64_t ny, double* out) {
+  std::vector<Cx> v(nx * ny);
+  for (int64_t i = 0; i < nx * ny; ++i) v[i] = {k[2 * i], k[2 * i + 1]};
+  put_cx(inverse_2d(v, nx, ny, nx / 2, ny / 2), out);
+  return 0;
+}
+
+// simulate_slice_full: combined (f64 pairs), optional captures (n_coils*nx*ny pairs each).
+int oracle_simulate_slice_full(const mrsim_slice_input* inp, const mrsim_acquisition* acq, double* combined,
+                               double* acquired, double* reconstructed, double* coil_images, double* sens) {
+  return guard([&] {
+    SliceRecon r = simulate_slice_with(*inp, *acq, acquired != nullptr, reconstructed != nullptr,
+                                       coil_images != nullptr, nullptr);
+    put_cx(r.combined, combined);
+    size_t per = r.combined.size();
+    for (size_t c = 0; c < r.acquired.size(); ++c) put_cx(r.acquired[c], acquired + 2 * per * c);
+    for (size_t c = 0; c < r.reconstructed.size(); ++c) put_cx(r.reconstructed[c], reconstructed + 2 * per * c);
+    for (size_t c = 0; c < r.coil_images.size(); ++c) put_cx(r.coil_images[c], coil_images + 2 * per * c);
+    if (sens)
+      for (size_t c = 0; c < r.sensitivities.size(); ++c)
+        memcpy(sens + per * c, r.sensitivities[c].data(), per * 8);
+  });
+}
+
+int oracle_simulate_slice(const mrsim_slice_input* inp, const mrsim_acquisition* acq, float* out) {
+  return guard([&] {
+    SliceRecon r = simulate_slice_with(*inp, *acq, false, false, false, nullptr);
+    for (size_t i = 0; i < r.combined.size(); ++i) {
+      out[2 * i] = (float)r.combined[i].re;
+      out[2 * i + 1] = (float)r.combined[i].im;
+    }
+  });
+}
+
+// GRAPPA fit on given coil k-spaces; weights out: (accel-1)*nc*6nc complex pairs.
+int oracle_grappa_fit(const double* coils, int64_t nc, int64_t nx, int64_t ny, int64_t accel, int64_t acs_lines,
+                      const uint8_t* lines, double* weights) {
+  return guard([&] {
+    std::vector<std::vector<Cx>> cv(nc, std::vector<Cx>(nx * ny));
+    for (int64_t c = 0; c < nc; ++c)
+      for (int64_t i = 0; i < nx * ny; ++i) cv[c][i] = {coils[2 * (c * nx * ny + i)], coils[2 * (c * nx * ny + i) + 1]};
+    std::vector<uint8_t> l(lines, lines + ny);
+    GrappaKernel K = grappa_fit(cv, nx, ny, accel, acs_lines, l);
+    size_t p = 0;
+    for (auto& d : K.weights)
+      for (auto& co : d)
+        for (auto& w : co) {
+          weights[p++] = w.re;
+          weights[p++] = w.im;
+        }
+  });
+}
+
+int oracle_acquire_volumes_complex(const mrsim_acquisition_input* in, const mrsim_acquisition* acq,
+                                   const mrsim_acquisition_options* opts, uint64_t excitation_seed,
+                                   uint64_t receiver_seed, int threads, mrsim_acquisition_output* out) {
+  return guard([&] {
+    SeriesOut so = acquire_volumes_complex(*in, *acq, opts, excitation_seed, receiver_seed, threads);
+    memcpy(out->re, so.re.data(), so.re.size() * 4);
+    memcpy(out->im, so.im.data(), so.im.size() * 4);
+    if (out->acquired && !so.acquired.empty()) memcpy(out->acquired, so.acquired.data(), so.acquired.size() * 4);
+    if (out->reconstructed && !so.reconstructed.empty())
+      memcpy(out->reconstructed, so.reconstructed.data(), so.reconstructed.size() * 4);
+    if (out->coil_images && !so.coil_images.empty())
+      memcpy(out->coil_images, so.coil_images.data(), so.coil_images.size() * 4);
+    if (out->combined && !so.combined.empty()) memcpy(out->combined, so.combined.data(), so.combined.size() * 4);
+    if (out->mask && !so.mask.empty()) memcpy(out->mask, so.mask.data(), so.mask.size());
+    if (out->sensitivities && !so.sensitivities.empty())
+      memcpy(out->sensitivities, so.sensitivities.data(), so.sensitivities.size() * 4);
+  });
+}
+
+// `echo_salt` kspace.rs:2130
+uint64_t oracle_echo_salt(uint64_t e) { return e * 0xD1B54A32D192ED03ull; }
+
+// `phase_slice` with an optional prep shot
+int oracle_phase_slice(const mrsim_phase_model* m, int32_t has_shot, double magnitude, const double* dir,
+                       int64_t volume, uint64_t seed, int64_t snx, int64_t sny, int64_t o, int64_t z, int64_t nz,
+                       double* out) {
+  Shot s;
+  if (has_shot && m->has_prep) s = prep_shot(*m, magnitude, dir, volume, z, seed);
+  auto v = phase_slice(*m, s, snx, sny, o, z, nz);
+  memcpy(out, v.data(), v.size() * 8);
+  return 0;
+}
+
+uint64_t oracle_rng_next(uint64_t seed, int64_t n, uint64_t* out) {
+  Rng r(seed);
+  for (int64_t i = 0; i < n; ++i) out[i] = r.next_u64();
+  return r.s;
+}
+
+int oracle_golden_count(void) {
+  if (!g_golden) g_golden = new std::vector<GoldenCase>(golden_outputs());
+  return (int)g_golden->size();
+}
+
+const char* oracle_golden_name(int i) {
+  oracle_golden_count();
+  return (*g_golden)[i].name.c_str();
+}
+
+int64_t oracle_golden_output(int i, uint32_t* out, int64_t cap) {
+  oracle_golden_count();
+  auto& b = (*g_golden)[i].bits;
+  if (out && cap >= (int64_t)b.size()) memcpy(out, b.data(), b.size() * 4);
+  return (int64_t)b.size();
+}
+
+}  // extern "C"
