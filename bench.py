@@ -1,0 +1,346 @@
+"""Benchmark of the exact-DFT k-space forward + adjoint on B200 (one JSON line on rank 0).
+
+Workload: the batched 2D EPI series — scan 64x64 on a 128x128 sim grid, 30 slices, 40 volumes
+with seeded rigid motion, 3 compartments (T2 80/250/30 ms, T2' 40/60/20 ms), 8 ring coils,
+GRAPPA R=2 sampling, partial Fourier 6/8 (Scanner), ghost 0.05, echoes TE 15/35/55 ms.
+Synthetic seeded data of that shape (no dataset exists for it).  A step is one forward over
+every (volume, slice, echo, coil) plus one adjoint/VJP (complex images, fieldmap and R2
+gradients) of the k-space it produced.  Metric: acquired k-space samples per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference's CPU algorithm (the FP64 C++ restatement in oracle/, the
+reference crate being Rust and unbuildable here) on the host cores, on a bounded sample of the
+same workload.  Under torchrun each rank runs its own copy of the series (weak scaling, no
+collective on the data path); rank 0 prints the max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "exact-DFT k-space samples/s (fwd+adjoint)"
+WORKLOAD = dict(name="epi-series-64x64-sim128-z30-v40-c3-q8-r2-pf0.75-te3", nx=64, ny=64, o=2, nz=30, nv=40,
+                ncomp=3, n_coils=8, echoes=(15.0, 35.0, 55.0))
+
+
+def make_acquisition():
+    from mrsim_acq_b200.api import Acquisition, KspaceWindow, PartialFourierMode
+    return Acquisition(n_coils=WORKLOAD["n_coils"], accel=2, acs_lines=24, partial_fourier=0.75,
+                       pf_mode=PartialFourierMode.Scanner, t_line=0.5, t_echo=30.0, ghost_offset=0.05,
+                       window=KspaceWindow.hann(), signal_scale=100.0)
+
+
+def make_inputs(seed=1):
+    """Seeded synthetic series: a 10-ellipse phantom split into 3 compartments, a per-volume
+    rigid motion (rotation <= 2 deg, translation <= 2 mm at 3.4 mm voxels) evaluated analytically,
+    and a fieldmap of 3 Gaussian blobs (+-60 Hz, sigma 8-20 px).  Layouts are the reference's."""
+    from mrsim_acq_b200.api import T2
+    W = WORKLOAD
+    nx, ny, o, nz, nv, nc = W["nx"], W["ny"], W["o"], W["nz"], W["nv"], W["ncomp"]
+    snx, sny = nx * o, ny * o
+    rng = np.random.default_rng(seed)
+    ell = []
+    for k in range(10):
+        ell.append(dict(cx=rng.uniform(0.3, 0.7), cy=rng.uniform(0.3, 0.7), a=rng.uniform(0.05, 0.25),
+                        b=rng.uniform(0.05, 0.25), th=rng.uniform(0, np.pi), mag=rng.uniform(0.2, 1.0), comp=k % nc))
+    ys, xs = np.meshgrid((np.arange(sny) + 0.5) / sny, (np.arange(snx) + 0.5) / snx, indexing="ij")
+    images = np.zeros((nc, nz, sny, snx, nv), np.float32)
+    vox_mm = 3.4
+    for g in range(nv):
+        rot = np.deg2rad(rng.uniform(-2, 2))
+        tx, ty = rng.uniform(-2, 2, 2) / (vox_mm * nx)
+        cr, sr = np.cos(rot), np.sin(rot)
+        X = cr * (xs - 0.5) - sr * (ys - 0.5) + 0.5 - tx
+        Y = sr * (xs - 0.5) + cr * (ys - 0.5) + 0.5 - ty
+        for z in range(nz):
+            zf = (z - nz / 2) / nz
+            for e in ell:
+                scale = math.sqrt(max(0.0, 1.0 - (zf / 0.6) ** 2))
+                if scale <= 0:
+                    continue
+                c, s = np.cos(e["th"]), np.sin(e["th"])
+                u = (c * (X - e["cx"]) + s * (Y - e["cy"])) / (e["a"] * scale)
+                v = (-s * (X - e["cx"]) + c * (Y - e["cy"])) / (e["b"] * scale)
+                images[e["comp"], z, :, :, g] += np.float32(e["mag"]) * (u * u + v * v <= 1.0)
+    imgs = [np.ascontiguousarray(images[c]).reshape(-1) for c in range(nc)]  # vox*nv + g
+    fmap = np.zeros((nz, sny, snx), np.float32)
+    zz = np.arange(nz)[:, None, None]
+    for _ in range(3):
+        amp, sig = rng.uniform(-60, 60), rng.uniform(8, 20) * o
+        cx, cy, cz = rng.uniform(0.3, 0.7) * snx, rng.uniform(0.3, 0.7) * sny, rng.uniform(0.2, 0.8) * nz
+        fmap += (amp * np.exp(-(((xs * snx - cx) ** 2 + (ys * sny - cy) ** 2) / (2 * sig * sig)
+                                + (zz - cz) ** 2 / (2 * (nz / 3) ** 2)))).astype(np.float32)
+    t2 = [T2.uniform(80.0), T2.uniform(250.0), T2.uniform(30.0)]
+    ti = [T2.uniform(40.0), T2.uniform(60.0), T2.uniform(20.0)]
+    return dict(sim_dims=(snx, sny, nz), acq_dims=(nx, ny, nz), n_volumes=nv, images=imgs, t2=t2, t_inhom=ti,
+                fmap=fmap.reshape(-1))
+
+
+class Clocks:
+    """nvidia-smi clock and throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait()
+        self.f.close()
+        rows = [r.split(", ") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4) if "Active" in r[5 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def algorithmic_flops(op_units, n_lines, snx, sny, nx, ncoils, ncomp):
+    """Per launch over all units: the canonical per-(slice, volume, echo) work of the exact DFT,
+    y-stage 4*Q*C*snx*sny*ny_acq and x-stage 8*Q*snx*nx*ny_acq, summed over echoes (n_lines is
+    every echo's acquired lines of one unit)."""
+    y = 4.0 * ncoils * ncomp * snx * sny * n_lines * op_units
+    x = 8.0 * ncoils * snx * nx * n_lines * op_units
+    return y, x
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from mrsim_acq_b200 import api
+    torch.cuda.set_device(local_rank)
+    ctx = api.Context(local_rank)
+    acq = make_acquisition()
+    inp = make_inputs(seed=1 + rank)
+    from mrsim_acq_b200.api import EpiOperator, PhaseModel
+    op = EpiOperator(inp["sim_dims"], inp["acq_dims"], inp["n_volumes"], inp["t2"], inp["fmap"], acq,
+                     images=inp["images"], echo_times_ms=WORKLOAD["echoes"], t_inhom=inp["t_inhom"],
+                     phase=PhaseModel.hbcd_like(), seed=42, grads=3, ctx=ctx)
+    samples = op.samples
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    snx, sny, nz = inp["sim_dims"]
+    nx, ny, _ = inp["acq_dims"]
+    units = inp["n_volumes"] * nz
+    n_lines = samples // (units * acq.n_coils * nx)
+    fy, fx = algorithmic_flops(units, n_lines, snx, sny, nx, acq.n_coils, WORKLOAD["ncomp"])
+
+    def step(evs=None):
+        for i in range(5):
+            if evs is not None:
+                evs[i].record(stream)
+            op.stage(i)
+        if evs is not None:
+            evs[5].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    t_begin = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(args.steps)]
+    t_begin.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    t_end.record(stream)
+    t_end.synchronize()
+    ctx.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    total_ms = t_begin.elapsed_time(t_end)
+    stage_ms = np.array([[evs[k][i].elapsed_time(evs[k][i + 1]) for i in range(5)] for k in range(args.steps)])
+    stage_avg = stage_ms.mean(axis=0)
+    ms = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(ms, op=torch.distributed.ReduceOp.MAX)
+    ms_step = float(ms.item()) / args.steps
+
+    # end to end through the host-buffer C ABI call (pinned host memory)
+    shp = op.shapes()
+    pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()  # noqa: E731
+    host_imgs = []
+    for a in inp["images"]:
+        h = pin(a.shape, torch.float32)
+        h[...] = a
+        host_imgs.append(h)
+    out = {"kspace": pin(shp["kspace"] + (2,), torch.float32).view(np.complex64)[..., 0],
+           "comp_grad": pin(shp["comp_grad"] + (2,), torch.float32).view(np.complex64)[..., 0],
+           "fmap_grad": pin(shp["fmap_grad"], torch.float32), "r2_grad": pin(shp["r2_grad"], torch.float32)}
+    e2e_steps = max(2, min(args.steps, 5))
+    for _ in range(2):
+        op.apply_host(host_imgs, out)
+    if world > 1:
+        torch.distributed.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        op.apply_host(host_imgs, out)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1) / e2e_steps], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
+    h2d = sum(a.nbytes for a in host_imgs)
+    d2h = sum(v.nbytes for v in out.values() if v is not None)
+
+    fp32 = ctx.probe_fp32_tflops()
+    pk, pk_kind = peaks()
+    # dominant kernel: the larger of the forward / adjoint y-stages
+    dom = 1 if stage_avg[1] >= stage_avg[4] else 4
+    achieved = fy / (stage_avg[dom] * 1e-3) / 1e12
+    res = {
+        "metric": METRIC, "value": samples * world / (ms_step * 1e-3), "unit": "samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "sim_grid": [snx, sny], "acq_matrix": [nx, ny], "slices": nz,
+                   "volumes": inp["n_volumes"], "echoes": list(WORKLOAD["echoes"]), "compartments": WORKLOAD["ncomp"],
+                   "coils": acq.n_coils, "accel": acq.accel, "partial_fourier": acq.partial_fourier,
+                   "samples_per_step_per_gpu": samples, "parallelism": f"weak x{world} (independent series)",
+                   "l2": "inputs (236 MB images) larger than L2; no flush"},
+        "e2e": {"value": samples * world / (float(e2e_ms.item()) * 1e-3), "unit": "samples/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "call": "mrsim_epi_operator_apply_host (host images in, k-space and gradients out)"},
+        "roofline": {"bound": "fp32", "kernel": ["statics", "forward_ystage", "forward_xstage", "adjoint_xstage",
+                                                 "adjoint_ystage"][dom],
+                     "achieved": achieved, "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
+                     "peak_source": "measured live: register FMA loop on this GPU (no FP32 entry in MEASURED_PEAKS.json)",
+                     "algorithmic_flops_per_launch": fy, "traffic": None,
+                     "stage_ms": dict(zip(["statics", "forward_ystage", "forward_xstage", "adjoint_xstage",
+                                           "adjoint_ystage"], [round(float(v), 4) for v in stage_avg]))},
+        "gpu_launches": 5 * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res["cpu_baseline"] = cpu_baseline(acq, inp, sample_volumes=1, sample_slices=args.cpu_slices)
+    return res, op, ctx
+
+
+def cpu_baseline(acq, inp, sample_volumes=1, sample_slices=8, threads=None):
+    """The oracle (FP64 restatement of the reference's rotor forward, plus its FP64 transpose) on
+    the host cores, forward + adjoint over a bounded sample of the same workload."""
+    from oracle import oracle
+    threads = threads or os.cpu_count() or 1
+    snx, sny, nz = inp["sim_dims"]
+    nx, ny, _ = inp["acq_dims"]
+    nv = inp["n_volumes"]
+    # the sample: `sample_volumes` volumes x `sample_slices` slices, every echo and coil
+    vol = np.stack([a.reshape(nz, sny, snx, nv)[:sample_slices, :, :, :sample_volumes] for a in inp["images"]])
+    imgs = [np.ascontiguousarray(vol[c]).reshape(-1) for c in range(vol.shape[0])]
+    fmap = inp["fmap"].reshape(nz, sny, snx)[:sample_slices].reshape(-1)
+    sim = (snx, sny, sample_slices)
+    acqd = (nx, ny, sample_slices)
+    from mrsim_acq_b200.api import PhaseModel
+    kw = dict(t_inhom=inp["t_inhom"], phase=PhaseModel.hbcd_like(), seed=42, nz_full=nz)
+    t0 = time.perf_counter()
+    k = oracle.series_forward(sim, acqd, sample_volumes, imgs, inp["t2"], fmap, acq, echo_times_ms=WORKLOAD["echoes"],
+                              threads=threads, **kw)
+    oracle.series_adjoint(sim, acqd, sample_volumes, imgs, inp["t2"], fmap, acq, k, echo_times_ms=WORKLOAD["echoes"],
+                          threads=threads, **kw)
+    dt = time.perf_counter() - t0
+    rows = int(oracle.sampling_mask(nx, ny, acq)[:, 0].sum())
+    samples = sample_volumes * sample_slices * acq.n_coils * len(WORKLOAD["echoes"]) * rows * nx
+    return {"value": samples / dt, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"{sample_volumes} volume x {sample_slices} slices x {len(WORKLOAD['echoes'])} echoes x "
+                      f"{acq.n_coils} coils ({samples} samples), forward + adjoint, FP64, {dt:.2f} s"}
+
+
+def run_reference(args):
+    acq = make_acquisition()
+    inp = make_inputs(seed=1)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline(acq, inp, sample_volumes=1, sample_slices=1, threads=threads)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(acq, inp, sample_volumes=1, sample_slices=args.ref_slices, threads=threads))
+    wall = time.perf_counter() - t0
+    v = float(np.median([r["value"] for r in vals]))
+    cb = dict(vals[0])
+    cb["value"] = v
+    return {"metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD["name"], "note": "each step is a bounded sample of the series "
+                       "(1 volume x %d slices, every echo and coil) on the host cores" % args.ref_slices},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-slices", type=int, default=30)
+    ap.add_argument("--ref-slices", type=int, default=30)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res, op, ctx = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    op.close()
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

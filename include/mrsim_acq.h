@@ -197,12 +197,6 @@ int mrsim_validate_acquisition_timing(const mrsim_acquisition* acq, int64_t nx, 
 int mrsim_epi_order(const mrsim_acquisition* acq, int64_t nx, int64_t ny, int64_t* order);
 
 /* ---- per-slice entry points (host buffers) ---------------------------------------------- */
-/* `simulate_slice` kspace.rs:1229-1235: out = nx*ny (re, im) f32 pairs. */
-int mrsim_simulate_slice(mrsim_context* ctx, const mrsim_slice_input* inp,
-                         const mrsim_acquisition* acq, float* out);
-/* `simulate_slice_kspace` kspace.rs:1144-1149: coil 0's acquired k-space, nx*ny (re, im) f64. */
-int mrsim_simulate_slice_kspace(mrsim_context* ctx, const mrsim_slice_input* inp,
-                                const mrsim_acquisition* acq, double* out);
 /* `build_coil_kspace_timed` kspace.rs:607-1042 for every coil of one slice, timing from
  * `LineTiming::for_acquisition` unless t_ms.. are given (each ny long, or all NULL); log_amp is
  * the 3D voxel-mode log-amplitude (snx*sny) or NULL.  out = n_coils*nx*ny (re, im) f64. */
@@ -211,85 +205,62 @@ int mrsim_build_coil_kspaces(mrsim_context* ctx, const mrsim_slice_input* inp,
                              const double* trf_ms, const double* tread_ms,
                              const int8_t* polarity, const double* log_amp, double* out);
 
-/* ---- series entry points (host buffers) ------------------------------------------------- */
-/* `simulate_acquisition_complex` kspace.rs:1803-1808. */
-int mrsim_simulate_acquisition_complex(mrsim_context* ctx, const mrsim_acquisition_input* inp,
-                                       const mrsim_acquisition* acq,
-                                       const mrsim_acquisition_options* opts,
-                                       mrsim_acquisition_output* out);
-/* `simulate_acquisition_oversampled` kspace.rs:1687-1714: magnitude and phase (f32). */
-int mrsim_simulate_acquisition_oversampled(mrsim_context* ctx, const mrsim_acquisition_input* inp,
-                                           const mrsim_acquisition* acq, float* mag, float* phase);
-/* `simulate_acquisition_echoes` kspace.rs:2152-2174: images_per_echo[e] holds echo e's ncomp
- * image arrays; mag/phase are n_echoes arrays of nx*ny*nz*n_volumes. */
-int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisition_input* inp,
-                                      const float* const* const* images_per_echo,
-                                      const mrsim_acquisition* acq, const double* echo_times_ms,
-                                      int64_t n_echoes, float* const* mag, float* const* phase);
-
-/* ---- the batched forward / adjoint operator pair (device buffers) ------------------------ */
+/* ---- the batched forward / adjoint operator of a 2D EPI series --------------------------- */
 /*
- * A batch is a list of independent units (one slice of one volume read at one echo), each with
- * its own geometry, so one launch covers uneven matrix sizes.  All pointers are DEVICE pointers.
- * The forward is `build_coil_kspace_timed` (kspace.rs:607-1042) before spikes and noise:
- *   s_q[kx,ky] = (1/nvox) sum_x tw(kx,x) sum_y amp_q(x,y) e^{i2pi a(x,y)} E(x,y,ky)
- *                sum_c rel_c(x,y,ky) m_c(x,y)
- * with E = e^{i2pi(rate*t(ky) + (ky-ys)(y-c)/sny)} times the eddy polynomial factors.
- * The adjoint is its Hermitian transpose with respect to complex compartment images and, on
- * request, the vector-Jacobian products with respect to the fieldmap (Hz) and each compartment's
- * R2 = 1/T2 (1/ms).  The reference has no adjoint; its oracle is the FP64 transpose and central
- * finite differences.
+ * The series' forward model `build_coil_kspace_timed` (kspace.rs:607-1042, without spikes and
+ * noise) over every volume, slice, echo and coil in one batch, and its adjoint.  A unit is one
+ * slice of one volume; its line list holds every echo's acquired lines, so the echoes of a
+ * volume share one pass over its voxels and the adjoint sums over them.  For each unit
+ *   k_q[e][ky][kx] = (1/nvox) sum_{x,y} tw(kx,x) amp_q(x,y) e^{i2pi theta(x,y,ky,e)}
+ *                    sum_c rel_c(x,y,ky,e) m_c(x,y)
+ * and the adjoint applied to the k-space buffer r writes
+ *   comp_grad_c(x,y) = (A^H r)_c(x,y)                      (complex, per compartment)
+ *   fmap_grad(x,y)   = dL/d fmap(x,y)    for L = sum |r|^2 with r = A m - d (Hz^-1 units)
+ *   r2_grad_c(x,y)   = dL/d R2_c(x,y),   R2 = 1/T2 in 1/ms.
+ * The reference has no adjoint; its oracle is the FP64 transpose plus finite differences.
+ *
+ * Device layouts (all owned by the operator; see mrsim_epi_operator_buffers):
+ *   images    [g][z][c][sny][snx] f32            fmap  [z][sny][snx] f32
+ *   kspace    [g][z][coil][echo][ny][nx] complex (re, im) f32; un-acquired rows stay zero
+ *   comp_grad [g][z][c][sny][snx] complex        fmap_grad [g][z][sny][snx]
+ *   r2_grad   [g][z][c][sny][snx]
+ * The images of every echo are the same (callers that decay them per echo use one operator per
+ * echo).  `in->images` may be NULL at creation; `in->fmap`, T2/T2' maps, drives and the phase
+ * model are read at creation.  `grads` bit 0 = fmap_grad, bit 1 = r2_grad.
  */
-typedef struct mrsim_epi_unit {
-  /* geometry */
-  int32_t snx, sny, nx, ny;
-  int32_t ncomp, ncoils, coil0, n_lines; /* coils coil0..coil0+ncoils-1 of ncoils_total     */
-  int32_t ncoils_total;                  /* ring size for coil_sensitivity                 */
-  int32_t z, nz;                         /* eddy z-terms                                   */
-  int32_t flags;                         /* MRSIM_UNIT_* bits                              */
-  /* device inputs */
-  const float* comp;          /* ncomp planes of snx*sny (real) — or 2*ncomp (re,im) if  */
-                              /* MRSIM_UNIT_COMPLEX_M                                     */
-  const float* fmap;          /* snx*sny, Hz                                              */
-  const float* phase_turns;   /* snx*sny static phase / (2 pi), or NULL                   */
-  const float* t2_map;        /* ncomp planes (ms), only for MAPS units; or NULL           */
-  const float* ti_map;        /* ncomp planes (ms), only for MAPS units; or NULL           */
-  const float* log_amp;       /* snx*sny or NULL                                          */
-  const float* lines;         /* n_lines records of MRSIM_LINE_FLOATS floats (see below)  */
-  /* scalars */
-  float t2_uniform[4];        /* per compartment (ms) for uniform compartments             */
-  float ti_uniform[4];
-  float signal_scale;
-  float eddy_strength, eddy_quad, eddy_tau;
-  float eddy_drive[3];
-  float ghost_offset;
-  /* device output (forward) / input (adjoint): ncoils*ny*nx (re, im) */
-  float* kspace;
-  /* adjoint outputs (device): comp_grad ncomp*snx*sny (re,im); fmap_grad, r2_grad ncomp*snx*sny */
-  float* comp_grad;
-  float* fmap_grad;
-  float* r2_grad;
-} mrsim_epi_unit;
+typedef struct mrsim_epi_operator mrsim_epi_operator;
 
-/* unit flags */
-#define MRSIM_UNIT_RELAX      1   /* do_relaxation                                           */
-#define MRSIM_UNIT_MAPS       2   /* per-voxel relaxation (a T2/T2' map or log_amp present)   */
-#define MRSIM_UNIT_GRADIENT   4   /* gradient echo: T2' decays from the RF                   */
-#define MRSIM_UNIT_EDDY       8   /* gradient-model eddy polynomial on                       */
-#define MRSIM_UNIT_COMPLEX_M 16   /* compartments are complex (re, im interleaved planes)     */
-#define MRSIM_UNIT_WANT_FMAP_GRAD 32
-#define MRSIM_UNIT_WANT_R2_GRAD   64
-#define MRSIM_UNIT_DISTORT  128   /* do_distortions (rate = fmap)                            */
-
-/* A line record: ky index, t (s, hi and lo split), |t|*1000 (ms), trf (ms), tread (ms),
- * polarity (+1/-1). */
-#define MRSIM_LINE_FLOATS 8
-
-/* Forward over every unit of the batch (device pointers, asynchronous on the context stream).
- * `units` is a host array of n_units descriptors. */
-int mrsim_epi_forward(mrsim_context* ctx, const mrsim_epi_unit* units, int64_t n_units);
-/* Adjoint / VJP over every unit (reads unit.kspace, writes comp_grad and the requested grads). */
-int mrsim_epi_adjoint(mrsim_context* ctx, const mrsim_epi_unit* units, int64_t n_units);
+int mrsim_epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_input* in,
+                              const mrsim_acquisition* acq, const double* echo_times_ms,
+                              int64_t n_echoes, const int64_t* slice_z, int64_t nz_full,
+                              int32_t grads, mrsim_epi_operator** out);
+int mrsim_epi_operator_destroy(mrsim_epi_operator* op);
+/* Acquired k-space samples one forward produces (every coil, echo, slice and volume). */
+int64_t mrsim_epi_operator_samples(const mrsim_epi_operator* op);
+/* Device pointers of the operator's buffers (any argument may be NULL). */
+int mrsim_epi_operator_buffers(mrsim_epi_operator* op, float** images, float** kspace,
+                               float** comp_grad, float** fmap_grad, float** r2_grad);
+/* Copy host images (reference layout: ncomp arrays of vox*n_volumes + g) to the device. */
+int mrsim_epi_operator_upload_images(mrsim_epi_operator* op, const float* const* images);
+/* Asynchronous on the context stream: statics + forward into the k-space buffer. */
+int mrsim_epi_operator_forward(mrsim_epi_operator* op);
+/* Asynchronous: adjoint / VJP of the k-space buffer's current contents. */
+int mrsim_epi_operator_adjoint(mrsim_epi_operator* op);
+/* One stage of the pair, asynchronous, for per-kernel timing: 0 statics (static phase),
+ * 1 forward y-stage, 2 forward x-stage, 3 adjoint x-stage, 4 adjoint y-stage. */
+int mrsim_epi_operator_stage(mrsim_epi_operator* op, int32_t stage);
+/* FP32 FMA throughput of the context's device (TFLOP/s, a register-resident FMA loop): the
+ * denominator of the exact path's roofline, measured because no table of peaks carries it. */
+int mrsim_probe_fp32_tflops(mrsim_context* ctx, double* tflops);
+/* Synchronous, host buffers: the adjoint / VJP of the given k-space (residual) r, layout of the
+ * k-space buffer, (re, im) f32.  Any output may be NULL. */
+int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace, float* comp_grad,
+                                    float* fmap_grad, float* r2_grad);
+/* Synchronous, host buffers: upload images, forward, copy k-space to the host, adjoint of that
+ * k-space (the residual of zero data), copy the gradients to the host.  Any output may be NULL. */
+int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images,
+                                  float* kspace, float* comp_grad, float* fmap_grad,
+                                  float* r2_grad);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,10 @@
+"""B200-native k-space acquisition path of mrsim-acq: CUDA kernels for sm_100a behind a C ABI.
+
+`api` mirrors the reference crate's names (Acquisition, SliceInput, T2, PhaseModel,
+sampling_mask, LineTiming, build_coil_kspaces, EpiOperator); `abi` is the ctypes layer over
+include/mrsim_acq.h; `build` compiles libmrsim_acq_cuda.so in-tree.
+"""
+from .abi import LibraryMissing, MrsimError, lib  # noqa: F401
+from .api import (Acquisition, Context, EchoFormation, EpiOperator, KspaceWindow, LineTiming,  # noqa: F401
+                  PartialFourierMode, PhaseModel, SliceInput, T2, build_coil_kspaces, default_context,
+                  epi_order, pf_skipped_lines, sampling_mask, simulate_slice_kspace, validate_acquisition_timing)

@@ -1,0 +1,174 @@
+"""ctypes mirror of include/mrsim_acq.h and the loader of libmrsim_acq_cuda.so.
+
+The structures here are the C ABI's, field for field.  The library is loaded from this package
+directory (it is built in-tree by `build.py`); there is no CPU fallback: loading fails loudly if
+the shared object is missing, and every compute entry point needs a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libmrsim_acq_cuda.so"
+
+c_f32p = C.POINTER(C.c_float)
+c_f64p = C.POINTER(C.c_double)
+
+
+class Acquisition_(C.Structure):
+    """`mrsim_acquisition` — `Acquisition` (reference kspace.rs:166-197)."""
+
+    _fields_ = [
+        ("t_line", C.c_double), ("t_echo", C.c_double), ("t_inhom", C.c_double), ("signal_scale", C.c_double),
+        ("reverse_phase", C.c_int32), ("do_distortions", C.c_int32), ("do_relaxation", C.c_int32),
+        ("pf_mode", C.c_int32),
+        ("noise_variance", C.c_double), ("partial_fourier", C.c_double), ("ghost_offset", C.c_double),
+        ("eddy_strength", C.c_double), ("eddy_quad", C.c_double), ("eddy_phase", C.c_double),
+        ("eddy_tau", C.c_double), ("n_spikes", C.c_int64), ("spike_amplitude", C.c_double),
+        ("window_kind", C.c_int32), ("echo", C.c_int32), ("window_a", C.c_double), ("window_b", C.c_double),
+        ("n_coils", C.c_int64), ("accel", C.c_int64), ("acs_lines", C.c_int64), ("seed", C.c_uint64),
+    ]
+
+
+class T2_(C.Structure):
+    """`mrsim_t2` — `T2Slice` / `T2Volume` (kspace.rs:380-393)."""
+
+    _fields_ = [("map", c_f32p), ("value", C.c_float), ("is_map", C.c_int32)]
+
+
+class SliceInput_(C.Structure):
+    """`mrsim_slice_input` — `SliceInput` (kspace.rs:458-496)."""
+
+    _fields_ = [
+        ("compartments", C.POINTER(c_f32p)), ("ncomp", C.c_int64), ("t2", C.POINTER(T2_)),
+        ("t_inhom", C.POINTER(T2_)), ("fmap", c_f32p), ("phase0", c_f64p), ("sim", C.c_int64 * 2),
+        ("acq_matrix", C.c_int64 * 2), ("z", C.c_int64), ("nz", C.c_int64), ("has_eddy_drive", C.c_int32),
+        ("has_prep_drive", C.c_int32), ("eddy_drive", C.c_double * 3), ("prep_magnitude", C.c_double),
+        ("prep_direction", C.c_double * 3), ("slice_seed", C.c_uint64),
+    ]
+
+
+class PhaseModel_(C.Structure):
+    """`mrsim_phase_model` — `PhaseModel` (phase.rs:130-205)."""
+
+    _fields_ = [
+        ("global_", C.c_double), ("background", C.c_double * 10), ("has_prep", C.c_int32),
+        ("reserved", C.c_int32), ("c_q", C.c_double), ("sigma_dx", C.c_double), ("sigma_rot", C.c_double),
+    ]
+
+
+class AcquisitionInput_(C.Structure):
+    """`mrsim_acquisition_input` — `AcquisitionInput` (kspace.rs:1720-1740)."""
+
+    _fields_ = [
+        ("sim_dims", C.c_int64 * 3), ("acq_dims", C.c_int64 * 3), ("n_volumes", C.c_int64), ("ncomp", C.c_int64),
+        ("images", C.POINTER(c_f32p)), ("t2", C.POINTER(T2_)), ("fmap", c_f32p), ("t_inhom", C.POINTER(T2_)),
+        ("eddy_drive_set", C.POINTER(C.c_int32)), ("eddy_drive", c_f64p),
+        ("prep_drive_set", C.POINTER(C.c_int32)), ("prep_drive", c_f64p),
+        ("phase", C.POINTER(PhaseModel_)), ("seed", C.c_uint64), ("noise_sigma", c_f32p),
+    ]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_int64, C.c_int64, C.c_void_p)
+
+
+class AcquisitionOptions_(C.Structure):
+    """`mrsim_acquisition_options` — `AcquisitionOptions` (kspace.rs:1744-1762)."""
+
+    _fields_ = [
+        ("slice_z", C.POINTER(C.c_int64)), ("nz_full", C.c_int64), ("kspace_slices", C.POINTER(C.c_int64)),
+        ("n_kspace_slices", C.c_int64), ("capture_acquired", C.c_int32), ("capture_reconstructed", C.c_int32),
+        ("capture_coil_images", C.c_int32), ("has_grappa_calibration", C.c_int32),
+        ("t_echo_per_volume", c_f64p), ("progress", PROGRESS_FN), ("progress_user", C.c_void_p),
+        ("grappa_calibration_images", C.POINTER(c_f32p)), ("grappa_calibration_seed", C.c_uint64),
+    ]
+
+
+class AcquisitionOutput_(C.Structure):
+    """`mrsim_acquisition_output` — `AcquisitionOutput` + `KspaceCapture` (kspace.rs:1767-1797)."""
+
+    _fields_ = [
+        ("re", c_f32p), ("im", c_f32p), ("mask", C.POINTER(C.c_uint8)), ("sensitivities", c_f32p),
+        ("acquired", c_f32p), ("reconstructed", c_f32p), ("coil_images", c_f32p), ("combined", c_f32p),
+    ]
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def _declare(lib):
+    P = C.c_void_p
+    sigs = {
+        "mrsim_abi_version": (C.c_int, []),
+        "mrsim_last_error": (C.c_char_p, []),
+        "mrsim_acquisition_default": (C.c_int, [C.POINTER(Acquisition_)]),
+        "mrsim_phase_model_hbcd_like": (C.c_int, [C.POINTER(PhaseModel_)]),
+        "mrsim_phase_model_none": (C.c_int, [C.POINTER(PhaseModel_)]),
+        "mrsim_context_create": (C.c_int, [C.c_int, C.POINTER(P)]),
+        "mrsim_context_destroy": (C.c_int, [P]),
+        "mrsim_context_stream": (P, [P]),
+        "mrsim_context_synchronize": (C.c_int, [P]),
+        "mrsim_sampling_mask": (C.c_int, [C.c_int64, C.c_int64, C.POINTER(Acquisition_), C.POINTER(C.c_uint8)]),
+        "mrsim_pf_skipped_lines": (C.c_int64, [C.c_int64, C.POINTER(Acquisition_)]),
+        "mrsim_line_timing": (C.c_int, [C.POINTER(Acquisition_), C.c_int64, C.c_int64, c_f64p, c_f64p, c_f64p,
+                                        C.POINTER(C.c_int8)]),
+        "mrsim_validate_acquisition_timing": (C.c_int, [C.POINTER(Acquisition_), C.c_int64, C.c_int64]),
+        "mrsim_epi_order": (C.c_int, [C.POINTER(Acquisition_), C.c_int64, C.c_int64, C.POINTER(C.c_int64)]),
+        "mrsim_build_coil_kspaces": (C.c_int, [P, C.POINTER(SliceInput_), C.POINTER(Acquisition_), c_f64p, c_f64p,
+                                               c_f64p, C.POINTER(C.c_int8), c_f64p, c_f64p]),
+        "mrsim_epi_operator_create": (C.c_int, [P, C.POINTER(AcquisitionInput_), C.POINTER(Acquisition_), c_f64p,
+                                                C.c_int64, C.POINTER(C.c_int64), C.c_int64, C.c_int32,
+                                                C.POINTER(P)]),
+        "mrsim_epi_operator_destroy": (C.c_int, [P]),
+        "mrsim_epi_operator_samples": (C.c_int64, [P]),
+        "mrsim_epi_operator_buffers": (C.c_int, [P] + [C.POINTER(c_f32p)] * 5),
+        "mrsim_epi_operator_upload_images": (C.c_int, [P, C.POINTER(c_f32p)]),
+        "mrsim_epi_operator_forward": (C.c_int, [P]),
+        "mrsim_epi_operator_adjoint": (C.c_int, [P]),
+        "mrsim_epi_operator_stage": (C.c_int, [P, C.c_int32]),
+        "mrsim_probe_fp32_tflops": (C.c_int, [P, C.POINTER(C.c_double)]),
+        "mrsim_epi_operator_adjoint_host": (C.c_int, [P, c_f32p, c_f32p, c_f32p, c_f32p]),
+        "mrsim_epi_operator_apply_host": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def lib():
+    """The loaded library (raises LibraryMissing if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise LibraryMissing(f"{LIB_PATH} is missing: run `python mrsim_acq_b200/build.py` "
+                                 "(the k-space path has no CPU fallback)")
+        _lib = _declare(C.CDLL(str(LIB_PATH)))
+    return _lib
+
+
+class MrsimError(RuntimeError):
+    """A non-zero status from the library; the message is the reference's panic text."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def check(status: int):
+    if status != 0:
+        raise MrsimError(status, lib().mrsim_last_error().decode())
+    return status
+
+
+def declared_symbols() -> list[str]:
+    """Every function name include/mrsim_acq.h declares (parsed from the header)."""
+    import re
+    text = (HERE.parent / "include" / "mrsim_acq.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(mrsim_\w+)\s*\(", text, re.M)))

@@ -1,0 +1,323 @@
+// abi.cpp — the extern "C" entry points of libmrsim_acq_cuda.so (declared in include/mrsim_acq.h).
+// Each converts C++ exceptions into a status code plus a thread-local message.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+
+#include "driver.h"
+#include "host_tables.h"
+#include "mrsim_internal.h"
+
+namespace {
+thread_local std::string g_last_error;
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return MRSIM_OK;
+  } catch (const mrsim::Error& e) {
+    g_last_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return MRSIM_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return MRSIM_ERR_INVALID;
+  }
+}
+
+void need(const void* p, const char* what) {
+  if (!p) mrsim::fail(std::string(what) + " is NULL");
+}
+
+// Runs `f` on the context's device with the context locked.
+template <class F>
+int on_ctx(mrsim_context* ctx, F&& f) {
+  return guarded([&] {
+    need(ctx, "context");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    MRSIM_CUDA(cudaSetDevice(ctx->device));
+    f();
+  });
+}
+}  // namespace
+
+struct mrsim_epi_operator {
+  mrsim::EpiOperator* impl;
+};
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+int mrsim_abi_version(void) { return MRSIM_ABI_VERSION; }
+const char* mrsim_last_error(void) { return g_last_error.c_str(); }
+
+int mrsim_acquisition_default(mrsim_acquisition* acq) {
+  return guarded([&] {
+    need(acq, "acq");
+    *acq = mrsim::acquisition_default();
+  });
+}
+
+int mrsim_phase_model_hbcd_like(mrsim_phase_model* out) {  // phase.rs:187-195
+  return guarded([&] {
+    need(out, "out");
+    std::memset(out, 0, sizeof *out);
+    out->background[1] = 0.13;
+    out->background[2] = 0.10;
+    out->background[3] = 0.02;
+    out->has_prep = 1;
+    out->c_q = 0.0425;
+    out->sigma_dx = 1.0;
+    out->sigma_rot = 2.0e-3;
+  });
+}
+
+int mrsim_phase_model_none(mrsim_phase_model* out) {  // phase.rs:197-205
+  return guarded([&] {
+    need(out, "out");
+    std::memset(out, 0, sizeof *out);
+    out->has_prep = 1;
+  });
+}
+
+int mrsim_context_create(int device, mrsim_context** out) {
+  return guarded([&] {
+    need(out, "out");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+      cudaGetLastError();
+      throw mrsim::Error(MRSIM_ERR_NOGPU, "no CUDA device: this library runs on the GPU only");
+    }
+    if (device < 0 || device >= n) mrsim::fail("device index out of range");
+    auto* ctx = new mrsim_context();
+    ctx->device = device;
+    try {
+      MRSIM_CUDA(cudaSetDevice(device));
+      MRSIM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    } catch (...) {
+      delete ctx;
+      throw;
+    }
+    *out = ctx;
+  });
+}
+
+int mrsim_context_destroy(mrsim_context* ctx) {
+  return guarded([&] {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& b : ctx->ws)
+      if (b.p) cudaFree(b.p);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+  });
+}
+
+void* mrsim_context_stream(mrsim_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int mrsim_context_synchronize(mrsim_context* ctx) {
+  return on_ctx(ctx, [&] { MRSIM_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+int mrsim_sampling_mask(int64_t nx, int64_t ny, const mrsim_acquisition* acq, uint8_t* mask) {
+  return guarded([&] {
+    need(acq, "acq");
+    need(mask, "mask");
+    auto m = mrsim::sampling_mask((size_t)nx, (size_t)ny, *acq);
+    std::memcpy(mask, m.data(), m.size());
+  });
+}
+
+int64_t mrsim_pf_skipped_lines(int64_t ny, const mrsim_acquisition* acq) {
+  return acq ? (int64_t)mrsim::pf_skipped_lines((size_t)ny, *acq) : -1;
+}
+
+int mrsim_line_timing(const mrsim_acquisition* acq, int64_t nx, int64_t ny, double* t_ms, double* trf_ms,
+                      double* tread_ms, int8_t* polarity) {
+  return guarded([&] {
+    need(acq, "acq");
+    auto lt = mrsim::line_timing(*acq, (size_t)nx, (size_t)ny);
+    if (t_ms) std::memcpy(t_ms, lt.t_ms.data(), (size_t)ny * 8);
+    if (trf_ms) std::memcpy(trf_ms, lt.trf_ms.data(), (size_t)ny * 8);
+    if (tread_ms) std::memcpy(tread_ms, lt.tread_ms.data(), (size_t)ny * 8);
+    if (polarity) std::memcpy(polarity, lt.polarity.data(), (size_t)ny);
+  });
+}
+
+int mrsim_validate_acquisition_timing(const mrsim_acquisition* acq, int64_t nx, int64_t ny) {
+  return guarded([&] {
+    need(acq, "acq");
+    mrsim::validate_acquisition_timing(*acq, (size_t)nx, (size_t)ny);
+  });
+}
+
+int mrsim_epi_order(const mrsim_acquisition* acq, int64_t nx, int64_t ny, int64_t* order) {
+  return guarded([&] {
+    need(acq, "acq");
+    need(order, "order");
+    auto o = mrsim::epi_order(*acq, (size_t)nx, (size_t)ny);
+    std::memcpy(order, o.data(), o.size() * 8);
+  });
+}
+
+int mrsim_build_coil_kspaces(mrsim_context* ctx, const mrsim_slice_input* inp, const mrsim_acquisition* acq,
+                             const double* t_ms, const double* trf_ms, const double* tread_ms, const int8_t* polarity,
+                             const double* log_amp, double* out) {
+  return on_ctx(ctx, [&] {
+    need(inp, "inp");
+    need(acq, "acq");
+    need(out, "out");
+    if (t_ms && !(trf_ms && tread_ms && polarity))
+      mrsim::fail("line-timing table must have one entry per phase-encode line");
+    auto k = mrsim::slice_forward(ctx, *inp, *acq, t_ms, trf_ms, tread_ms, polarity, log_amp);
+    for (size_t i = 0; i < k.size(); ++i) {
+      out[2 * i] = (double)k[i].x;
+      out[2 * i + 1] = (double)k[i].y;
+    }
+  });
+}
+
+int mrsim_epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_input* in, const mrsim_acquisition* acq,
+                              const double* echo_times_ms, int64_t n_echoes, const int64_t* slice_z, int64_t nz_full,
+                              int32_t grads, mrsim_epi_operator** out) {
+  return on_ctx(ctx, [&] {
+    need(in, "in");
+    need(acq, "acq");
+    need(out, "out");
+    need(in->fmap, "fmap");
+    need(in->t2, "t2");
+    auto* op = new mrsim_epi_operator();
+    try {
+      op->impl = mrsim::epi_operator_create(ctx, *in, *acq, echo_times_ms, n_echoes, slice_z, nz_full, grads);
+    } catch (...) {
+      delete op;
+      throw;
+    }
+    *out = op;
+  });
+}
+
+int mrsim_epi_operator_destroy(mrsim_epi_operator* op) {
+  return guarded([&] {
+    if (!op) return;
+    if (op->impl) {
+      mrsim_context* ctx = op->impl->ctx;
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      cudaSetDevice(ctx->device);
+      cudaStreamSynchronize(ctx->stream);
+      delete op->impl;
+    }
+    delete op;
+  });
+}
+
+int64_t mrsim_epi_operator_samples(const mrsim_epi_operator* op) {
+  return op && op->impl ? op->impl->samples_per_step : -1;
+}
+
+int mrsim_epi_operator_buffers(mrsim_epi_operator* op, float** images, float** kspace, float** comp_grad,
+                               float** fmap_grad, float** r2_grad) {
+  return guarded([&] {
+    need(op, "operator");
+    auto* o = op->impl;
+    if (images) *images = o->d_images;
+    if (kspace) *kspace = (float*)o->d_kspace;
+    if (comp_grad) *comp_grad = (float*)o->d_comp_grad;
+    if (fmap_grad) *fmap_grad = o->d_fmap_grad;
+    if (r2_grad) *r2_grad = o->d_r2_grad;
+  });
+}
+
+int mrsim_epi_operator_upload_images(mrsim_epi_operator* op, const float* const* images) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    need(images, "images");
+    mrsim::upload_series_images(op->impl, images);
+  });
+}
+
+int mrsim_epi_operator_forward(mrsim_epi_operator* op) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] { mrsim::epi_operator_forward(op->impl); });
+}
+
+int mrsim_epi_operator_adjoint(mrsim_epi_operator* op) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] { mrsim::epi_operator_adjoint(op->impl); });
+}
+
+int mrsim_epi_operator_stage(mrsim_epi_operator* op, int32_t stage) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    const mrsim::EpiPlan* p = op->impl->plan.get();
+    cudaStream_t st = op->impl->ctx->stream;
+    switch (stage) {
+      case 0: mrsim::epi_plan_statics(p, st); break;
+      case 1: mrsim::epi_plan_forward_ystage(p, st); break;
+      case 2: mrsim::epi_plan_forward_xstage(p, st); break;
+      case 3: mrsim::epi_plan_adjoint_xstage(p, st); break;
+      case 4: mrsim::epi_plan_adjoint_ystage(p, st); break;
+      default: mrsim::fail("stage must be 0..4");
+    }
+  });
+}
+
+int mrsim_probe_fp32_tflops(mrsim_context* ctx, double* tflops) {
+  return on_ctx(ctx, [&] {
+    need(tflops, "tflops");
+    *tflops = mrsim::probe_fp32_tflops(ctx->stream);
+  });
+}
+
+int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace, float* comp_grad, float* fmap_grad,
+                                    float* r2_grad) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    need(kspace, "kspace");
+    auto* o = op->impl;
+    cudaStream_t st = o->ctx->stream;
+    const size_t plane = (size_t)o->snx * o->sny, nunits = (size_t)o->nv * o->nz;
+    MRSIM_CUDA(cudaMemcpyAsync(o->d_kspace, kspace, o->kspace_elems * sizeof(float2), cudaMemcpyHostToDevice, st));
+    mrsim::epi_operator_adjoint(o);
+    if (comp_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(comp_grad, o->d_comp_grad, nunits * o->ncomp * plane * sizeof(float2),
+                                 cudaMemcpyDeviceToHost, st));
+    if (fmap_grad && o->d_fmap_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(fmap_grad, o->d_fmap_grad, nunits * plane * 4, cudaMemcpyDeviceToHost, st));
+    if (r2_grad && o->d_r2_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(r2_grad, o->d_r2_grad, nunits * o->ncomp * plane * 4, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images, float* kspace, float* comp_grad,
+                                  float* fmap_grad, float* r2_grad) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    auto* o = op->impl;
+    cudaStream_t st = o->ctx->stream;
+    const size_t plane = (size_t)o->snx * o->sny, nunits = (size_t)o->nv * o->nz;
+    if (images) mrsim::upload_series_images(o, images);
+    mrsim::epi_operator_forward(o);
+    if (kspace)
+      MRSIM_CUDA(cudaMemcpyAsync(kspace, o->d_kspace, o->kspace_elems * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    mrsim::epi_operator_adjoint(o);
+    if (comp_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(comp_grad, o->d_comp_grad, nunits * o->ncomp * plane * sizeof(float2),
+                                 cudaMemcpyDeviceToHost, st));
+    if (fmap_grad && o->d_fmap_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(fmap_grad, o->d_fmap_grad, nunits * plane * 4, cudaMemcpyDeviceToHost, st));
+    if (r2_grad && o->d_r2_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(r2_grad, o->d_r2_grad, nunits * o->ncomp * plane * 4, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,565 @@
+// driver.cpp — host orchestration of the B200 k-space library: context, geometry and line
+// tables, the batched forward/adjoint operator of a 2D EPI series, and the per-slice forward.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <tuple>
+
+#include "driver.h"
+#include "host_tables.h"
+#include "mrsim_internal.h"
+#include "noise_kernels.h"
+
+namespace mrsim {
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(MRSIM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+void* workspace(mrsim_context* ctx, int slot, size_t bytes) {
+  if ((int)ctx->ws.size() <= slot) ctx->ws.resize(slot + 1);
+  DeviceBuffer& b = ctx->ws[slot];
+  if (b.n < bytes) {
+    if (b.p) MRSIM_CUDA(cudaFree(b.p));
+    b.p = nullptr;
+    b.n = 0;
+    MRSIM_CUDA(cudaMalloc(&b.p, bytes));
+    b.n = bytes;
+  }
+  return b.p;
+}
+
+// ---- device memory owned by an object --------------------------------------------------------
+void* DevArena::alloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  MRSIM_CUDA(cudaMalloc(&p, bytes));
+  ptrs.push_back(p);
+  return p;
+}
+void* DevArena::upload(const void* src, size_t bytes, cudaStream_t st) {
+  void* p = alloc(bytes);
+  if (bytes) MRSIM_CUDA(cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, st));
+  return p;
+}
+DevArena::~DevArena() {
+  for (void* p : ptrs) cudaFree(p);
+}
+
+// ---- geometry tables -----------------------------------------------------------------------
+// ex/ey: the two factors of the Gaussian ring coil sensitivity (`coil_sensitivity`
+// kspace.rs:226-237) on the sim grid in acquired-voxel units (xa = (x - xoff)/o); tw: the x-stage
+// twiddles e^{i2pi (kx - xs + gh)(x - sxs - xoff)/snx} for gh = +ghost, -ghost (`XStage::new`,
+// kspace.rs:1069-1110), with the k.r part from the exact integer index (kx-xs)(2(x-sxs)-(o-1))
+// mod 2 snx, stored [pol][x][kx] then transposed [pol][kx][x].
+GeoTab build_geo(DevArena& arena, int snx, int sny, int nx, int ny, int ncoils, double ghost, cudaStream_t st) {
+  const int ox = snx / nx, oy = sny / ny;
+  const double xoff = (ox - 1.0) / 2.0, yoff = (oy - 1.0) / 2.0;
+  const int xs = nx / 2, sxs = ox * xs;
+  std::vector<float> ex((size_t)ncoils * snx), ey((size_t)ncoils * sny);
+  const double sigma = 0.9 * (double)std::max(nx, ny);
+  const double r = 0.6 * (double)std::max(nx, ny);
+  for (int q = 0; q < ncoils; ++q) {
+    if (ncoils <= 1) {
+      for (int x = 0; x < snx; ++x) ex[x] = 1.f;
+      for (int y = 0; y < sny; ++y) ey[y] = 1.f;
+      continue;
+    }
+    const double ang = kTau * (double)q / (double)ncoils;
+    const double px = nx / 2.0 + r * std::cos(ang), py = ny / 2.0 + r * std::sin(ang);
+    for (int x = 0; x < snx; ++x) {
+      double d = ((double)x - xoff) / ox - px;
+      ex[(size_t)q * snx + x] = (float)std::exp(-(d * d) / (2.0 * sigma * sigma));
+    }
+    for (int y = 0; y < sny; ++y) {
+      double d = ((double)y - yoff) / oy - py;
+      ey[(size_t)q * sny + y] = (float)std::exp(-(d * d) / (2.0 * sigma * sigma));
+    }
+  }
+  std::vector<float2> tw((size_t)4 * snx * nx);
+  const double c = (double)sxs + xoff;
+  const long long m2 = 2LL * snx;
+  for (int pol = 0; pol < 2; ++pol) {
+    const double gh = pol == 0 ? ghost : -ghost;
+    for (int x = 0; x < snx; ++x) {
+      const long long X = 2LL * (x - sxs) - (ox - 1);
+      const double gramp = gh * ((double)x - c) / (double)snx;
+      for (int kx = 0; kx < nx; ++kx) {
+        long long K = kx - xs;
+        double turns = (double)((K * X) % m2) / (double)m2 + gramp;
+        turns -= std::rint(turns);
+        double ph = kTau * turns;
+        float2 v = make_float2((float)std::cos(ph), (float)std::sin(ph));
+        tw[(size_t)pol * snx * nx + (size_t)x * nx + kx] = v;
+        tw[(size_t)(2 + pol) * snx * nx + (size_t)kx * snx + x] = v;
+      }
+    }
+  }
+  GeoTab g;
+  g.ex = (const float*)arena.upload(ex.data(), ex.size() * 4, st);
+  g.ey = (const float*)arena.upload(ey.data(), ey.size() * 4, st);
+  g.tw = (const float2*)arena.upload(tw.data(), tw.size() * sizeof(float2), st);
+  g.coil_off = ncoils <= 1 ? 0.f : 0.15f;
+  return g;
+}
+
+// ---- line records --------------------------------------------------------------------------
+// One echo's acquired lines, in ky order (the reference loops kyi = 0..ny and skips rows the
+// sampling mask drops, kspace.rs:843-846), with the per-line factors of kspace.rs:847-903.
+void append_lines(std::vector<LineRec>& out, const mrsim_acquisition& acq, const LineTimingTab& lt, int nx, int ny,
+                  int echo, bool eddy, bool uniform, int ncomp, const float* t2u, const float* tiu) {
+  auto mask = sampling_mask(nx, ny, acq);
+  for (int ky = 0; ky < ny; ++ky) {
+    if (!mask[(size_t)nx * ky]) continue;
+    LineRec L;
+    std::memset(&L, 0, sizeof L);
+    L.ky = ky;
+    L.row = echo * ny + ky;
+    L.pol = lt.polarity[ky] < 0 ? -1 : 1;
+    const double t = lt.t_ms[ky] / 1000.0;
+    const double trf = lt.trf_ms[ky];
+    const bool spin = acq.echo == MRSIM_ECHO_SPIN;
+    const double tb0 = spin ? t : t + acq.t_echo / 1000.0;
+    L.t_hi = (float)tb0;
+    L.t_lo = (float)(tb0 - (double)L.t_hi);
+    L.t_s = (float)tb0;
+    const double inh = spin ? std::fabs(t) * 1000.0 : trf;
+    L.inhom_ms = (float)inh;
+    L.trf_ms = (float)trf;
+    L.decay = eddy ? (float)(std::exp(-lt.tread_ms[ky] / acq.eddy_tau) * t) : 0.f;
+    for (int c = 0; c < kMaxComp; ++c) {
+      double rel = 1.0;
+      if (c < ncomp && uniform && acq.do_relaxation) rel = std::exp(-trf / (double)t2u[c] - inh / (double)tiu[c]);
+      L.rel[c] = (float)rel;
+    }
+    out.push_back(L);
+  }
+}
+
+// ---- per-slice forward (`build_coil_kspace_timed` for every coil + spikes + noise) ---------
+std::vector<float2> slice_forward(mrsim_context* ctx, const mrsim_slice_input& inp, const mrsim_acquisition& acq,
+                                  const double* t_ms, const double* trf_ms, const double* tread_ms,
+                                  const int8_t* polarity, const double* log_amp) {
+  const int snx = (int)inp.sim[0], sny = (int)inp.sim[1], nx = (int)inp.acq_matrix[0], ny = (int)inp.acq_matrix[1];
+  if (snx <= 0 || sny <= 0 || nx <= 0 || ny <= 0) fail("empty simulation grid or acquired matrix");
+  if (!(snx % nx == 0 && sny % ny == 0)) fail("sim grid must be an integer multiple of the acquired matrix");
+  const int ncomp = (int)inp.ncomp;
+  if (ncomp > kMaxComp) fail("more than 8 compartments");
+  const int ncoils = (int)std::max<int64_t>(acq.n_coils, 1);
+  if (ncoils > kMaxCoils) fail("more than 64 coils");
+  const size_t plane = (size_t)snx * sny;
+  cudaStream_t st = ctx->stream;
+  DevArena A;
+
+  LineTimingTab lt;
+  if (t_ms) {
+    lt.t_ms.assign(t_ms, t_ms + ny);
+    lt.trf_ms.assign(trf_ms, trf_ms + ny);
+    lt.tread_ms.assign(tread_ms, tread_ms + ny);
+    lt.polarity.assign(polarity, polarity + ny);
+  } else {
+    lt = line_timing(acq, nx, ny);
+  }
+  bool uniform = log_amp == nullptr;
+  for (int c = 0; c < ncomp; ++c) uniform = uniform && !inp.t2[c].is_map;
+  if (inp.t_inhom)
+    for (int c = 0; c < ncomp; ++c) uniform = uniform && !inp.t_inhom[c].is_map;
+  const bool maps = !uniform && acq.do_relaxation;
+  const bool eddy = acq.eddy_strength != 0.0 && inp.has_eddy_drive;
+  const bool eddy_phase = acq.eddy_phase != 0.0 && inp.has_eddy_drive;
+  float t2u[kMaxComp], tiu[kMaxComp];
+  for (int c = 0; c < kMaxComp; ++c) {
+    t2u[c] = c < ncomp ? inp.t2[c].value : 1.f;
+    tiu[c] = c < ncomp ? (inp.t_inhom ? inp.t_inhom[c].value : (float)acq.t_inhom) : 1.f;
+  }
+  std::vector<LineRec> lines;
+  append_lines(lines, acq, lt, nx, ny, 0, eddy, uniform, ncomp, t2u, tiu);
+  if (ncomp > 0 && uniform && acq.do_relaxation && !inp.t_inhom) {
+    // `t_inhom: None` reads Acquisition::t_inhom as f64 — recompute rel at full precision
+    for (auto& L : lines)
+      for (int c = 0; c < ncomp; ++c) {
+        double t = lt.t_ms[L.ky] / 1000.0, trf = lt.trf_ms[L.ky];
+        double inh = acq.echo == MRSIM_ECHO_SPIN ? std::fabs(t) * 1000.0 : trf;
+        L.rel[c] = (float)std::exp(-trf / (double)t2u[c] - inh / acq.t_inhom);
+      }
+  }
+
+  // inputs
+  std::vector<float> comp(std::max<size_t>(1, (size_t)ncomp * plane));
+  for (int c = 0; c < ncomp; ++c) std::memcpy(&comp[(size_t)c * plane], inp.compartments[c], plane * 4);
+  float* d_comp = (float*)A.upload(comp.data(), comp.size() * 4, st);
+  float* d_fmap = (float*)A.upload(inp.fmap, plane * 4, st);
+  const double* d_phase0 = inp.phase0 ? (const double*)A.upload(inp.phase0, plane * 8, st) : nullptr;
+  float* d_t2 = nullptr;
+  float* d_ti = nullptr;
+  float* d_la = nullptr;
+  if (maps) {
+    bool any_t2 = false, any_ti = false;
+    for (int c = 0; c < ncomp; ++c) {
+      any_t2 = any_t2 || inp.t2[c].is_map;
+      any_ti = any_ti || (inp.t_inhom && inp.t_inhom[c].is_map);
+    }
+    if (any_t2) {
+      std::vector<float> m((size_t)ncomp * plane);
+      for (int c = 0; c < ncomp; ++c)
+        for (size_t i = 0; i < plane; ++i) m[(size_t)c * plane + i] = inp.t2[c].is_map ? inp.t2[c].map[i] : inp.t2[c].value;
+      d_t2 = (float*)A.upload(m.data(), m.size() * 4, st);
+    }
+    if (any_ti) {
+      std::vector<float> m((size_t)ncomp * plane);
+      for (int c = 0; c < ncomp; ++c)
+        for (size_t i = 0; i < plane; ++i)
+          m[(size_t)c * plane + i] = inp.t_inhom[c].is_map ? inp.t_inhom[c].map[i] : inp.t_inhom[c].value;
+      d_ti = (float*)A.upload(m.data(), m.size() * 4, st);
+    }
+    if (log_amp) {
+      std::vector<float> m(plane);
+      for (size_t i = 0; i < plane; ++i) m[i] = (float)log_amp[i];
+      d_la = (float*)A.upload(m.data(), m.size() * 4, st);
+    }
+  }
+  GeoTab geo = build_geo(A, snx, sny, nx, ny, ncoils, acq.ghost_offset, st);
+  const LineRec* d_lines = (const LineRec*)A.upload(lines.data(), std::max<size_t>(1, lines.size()) * sizeof(LineRec), st);
+  float* d_phase = (float*)A.alloc(plane * 4);
+  float2* d_g = (float2*)A.alloc(std::max<size_t>(1, (size_t)ncoils * lines.size() * snx) * sizeof(float2));
+  float2* d_k = (float2*)A.alloc((size_t)ncoils * nx * ny * sizeof(float2));
+  MRSIM_CUDA(cudaMemsetAsync(d_k, 0, (size_t)ncoils * nx * ny * sizeof(float2), st));
+
+  StaticDesc sd;
+  std::memset(&sd, 0, sizeof sd);
+  sd.snx = snx;
+  sd.sny = sny;
+  sd.nx = nx;
+  sd.ny = ny;
+  sd.o = snx / nx;
+  sd.z = (int)inp.z;
+  sd.nz_full = (int)inp.nz;
+  sd.flags = 1 | (eddy_phase ? 2 : 0);
+  sd.phase0 = d_phase0;
+  double grad[3] = {0, 0, 0};
+  if (inp.has_eddy_drive)
+    for (int i = 0; i < 3; ++i) grad[i] = inp.eddy_drive[i];
+  for (int i = 0; i < 3; ++i) sd.eddy_phase_coef[i] = acq.eddy_phase * grad[i];
+  sd.zc_c = (double)inp.z - ((double)inp.nz - 1.0) / 2.0;
+  sd.out = d_phase;
+  if (!d_phase0) {
+    // no explicit phase: zero phase model
+    sd.flags &= ~1;
+  }
+
+  UnitDesc u;
+  std::memset(&u, 0, sizeof u);
+  u.snx = snx;
+  u.sny = sny;
+  u.nx = nx;
+  u.ny = ny;
+  u.ncomp = ncomp;
+  u.ncoils = ncoils;
+  u.n_lines = (int)lines.size();
+  u.n_rows = ny;
+  u.flags = (acq.do_relaxation ? UF_RELAX : 0) | (maps ? UF_MAPS : 0) | (eddy ? UF_EDDY : 0) |
+            (acq.do_distortions ? UF_DISTORT : 0) | (acq.echo == MRSIM_ECHO_GRADIENT ? UF_GRADIENT : 0);
+  u.z = (int)inp.z;
+  u.nz = (int)inp.nz;
+  u.comp_stride = (long long)plane;
+  u.map_stride = (long long)plane;
+  u.comp = d_comp;
+  u.fmap = d_fmap;
+  u.phase = d_phase;
+  u.t2map = d_t2;
+  u.timap = d_ti;
+  u.log_amp = d_la;
+  u.lines = d_lines;
+  u.geo = geo;
+  u.signal_scale = (float)acq.signal_scale;
+  for (int c = 0; c < kMaxComp; ++c) {
+    u.t2u[c] = t2u[c];
+    u.tiu[c] = tiu[c];
+  }
+  if (eddy) {
+    const int zs = (int)inp.nz / 2;
+    const double zc = (double)inp.z - (double)zs;
+    u.eddy_cx = (float)(acq.eddy_strength * grad[0]);
+    u.eddy_qx = (float)(acq.eddy_quad * grad[0]);
+    u.eddy_cy = (float)(acq.eddy_strength * grad[1]);
+    u.eddy_qy = (float)(acq.eddy_quad * grad[1]);
+    u.eddy_z = (float)(acq.eddy_strength * grad[2] * zc + acq.eddy_quad * grad[2] * zc * zc);
+  }
+  u.kspace = d_k;
+  u.g = d_g;
+
+  std::unique_ptr<EpiPlan> plan(epi_plan_create(&u, 1, &sd, 1));
+  epi_plan_statics(plan.get(), st);
+  if (!lines.empty()) epi_plan_forward(plan.get(), st);
+
+  // spikes and noise per coil
+  const bool do_spikes = acq.n_spikes > 0;
+  const bool do_noise = acq.noise_variance > 0.0;
+  if ((do_spikes || do_noise) && !lines.empty()) {
+    std::vector<int> rows;
+    for (auto& L : lines) rows.push_back(L.ky);
+    std::vector<int> picks;
+    if (do_spikes) {
+      auto mask = sampling_mask(nx, ny, acq);
+      std::vector<int> acquired;
+      for (int i = 0; i < nx * ny; ++i)
+        if (mask[i]) acquired.push_back(i);
+      Rng rng(inp.slice_seed ^ 0xA5A5123456789ABCull);
+      for (int64_t s = 0; s < acq.n_spikes; ++s)
+        picks.push_back(acquired[(size_t)(rng.next_u64() % (uint64_t)acquired.size())]);
+    }
+    const int* d_rows = (const int*)A.upload(rows.data(), rows.size() * 4, st);
+    const int* d_picks = picks.empty() ? nullptr : (const int*)A.upload(picks.data(), picks.size() * 4, st);
+    std::vector<NoiseJob> jobs(ncoils);
+    for (int q = 0; q < ncoils; ++q) {
+      NoiseJob& J = jobs[q];
+      std::memset(&J, 0, sizeof J);
+      J.k = d_k + (size_t)q * nx * ny;
+      J.rows = d_rows;
+      J.picks = d_picks;
+      J.n_rows = (int)rows.size();
+      J.nx = nx;
+      J.n_picks = (int)picks.size();
+      J.seed = (inp.slice_seed ^ ((uint64_t)q * 0x9E3779B9ull)) | 1ull;
+      J.sigma = do_noise ? std::sqrt(acq.noise_variance / (double)((size_t)nx * ny)) : 0.0;
+      J.spike_amplitude = acq.spike_amplitude;
+    }
+    const NoiseJob* d_jobs = (const NoiseJob*)A.upload(jobs.data(), jobs.size() * sizeof(NoiseJob), st);
+    auto* d_keys = (unsigned long long*)A.alloc(sizeof(unsigned long long) * ncoils);
+    launch_noise_jobs(d_jobs, ncoils, do_spikes, do_noise, (int)rows.size() * nx, d_keys, st);
+    MRSIM_CUDA(cudaGetLastError());
+  }
+  std::vector<float2> out((size_t)ncoils * nx * ny);
+  MRSIM_CUDA(cudaMemcpyAsync(out.data(), d_k, out.size() * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+  return out;
+}
+
+// =============================================================================================
+// The batched forward/adjoint operator of a 2D EPI series.
+EpiOperator::~EpiOperator() {}
+
+static void validate_series(const mrsim_acquisition_input& in, const mrsim_acquisition& acq) {
+  const int64_t snx = in.sim_dims[0], sny = in.sim_dims[1], nz = in.sim_dims[2];
+  const int64_t nx = in.acq_dims[0], ny = in.acq_dims[1], nzo = in.acq_dims[2];
+  if (nz != nzo) fail("slice count must match; z is never oversampled");
+  if (nx <= 0 || ny <= 0 || snx <= 0 || sny <= 0) fail("empty simulation grid or acquired matrix");
+  if (!(snx % nx == 0 && sny % ny == 0)) fail("sim grid must be an integer multiple of the acquired matrix");
+  if (snx / nx != sny / ny) fail("oversampling must match on both axes");
+  if (in.ncomp > kMaxComp) fail("more than 8 compartments");
+  if (std::max<int64_t>(acq.n_coils, 1) > kMaxCoils) fail("more than 64 coils");
+  (void)acq;
+}
+
+EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_input& in, const mrsim_acquisition& acq,
+                                 const double* echo_times_ms, int64_t n_echoes, const int64_t* slice_z,
+                                 int64_t nz_full_in, int grads) {
+  validate_series(in, acq);
+  std::unique_ptr<EpiOperator> op(new EpiOperator());
+  op->ctx = ctx;
+  cudaStream_t st = ctx->stream;
+  const int snx = (int)in.sim_dims[0], sny = (int)in.sim_dims[1], nz = (int)in.sim_dims[2];
+  const int nx = (int)in.acq_dims[0], ny = (int)in.acq_dims[1];
+  const int nv = (int)in.n_volumes, ncomp = (int)in.ncomp;
+  const int ncoils = (int)std::max<int64_t>(acq.n_coils, 1);
+  const int nz_full = nz_full_in > 0 ? (int)nz_full_in : nz;
+  std::vector<double> tes;
+  if (echo_times_ms && n_echoes > 0)
+    tes.assign(echo_times_ms, echo_times_ms + n_echoes);
+  else
+    tes.push_back(acq.t_echo);
+  const int ne = (int)tes.size();
+  op->snx = snx;
+  op->sny = sny;
+  op->nx = nx;
+  op->ny = ny;
+  op->nz = nz;
+  op->nv = nv;
+  op->ncomp = ncomp;
+  op->ncoils = ncoils;
+  op->n_echoes = ne;
+  const size_t plane = (size_t)snx * sny;
+
+  bool uniform = true;
+  for (int c = 0; c < ncomp; ++c) uniform = uniform && !in.t2[c].is_map;
+  if (in.t_inhom)
+    for (int c = 0; c < ncomp; ++c) uniform = uniform && !in.t_inhom[c].is_map;
+  const bool maps = !uniform && acq.do_relaxation;
+  float t2u[kMaxComp], tiu[kMaxComp];
+  for (int c = 0; c < kMaxComp; ++c) {
+    t2u[c] = c < ncomp ? in.t2[c].value : 1.f;
+    tiu[c] = c < ncomp ? (in.t_inhom ? in.t_inhom[c].value : (float)acq.t_inhom) : 1.f;
+  }
+  // eddy is per volume; lines are built with decay for the eddy case (decay is only read when a
+  // unit has UF_EDDY, so one line table serves every volume)
+  const bool any_eddy = acq.eddy_strength != 0.0 && in.eddy_drive_set &&
+                        std::any_of(in.eddy_drive_set, in.eddy_drive_set + nv, [](int32_t v) { return v != 0; });
+  std::vector<LineRec> lines;
+  for (int e = 0; e < ne; ++e) {
+    mrsim_acquisition a = acq;
+    a.t_echo = tes[e];
+    validate_acquisition_timing(a, nx, ny);
+    LineTimingTab lt = line_timing(a, nx, ny);
+    size_t before = lines.size();
+    append_lines(lines, a, lt, nx, ny, e, any_eddy, uniform, ncomp, t2u, tiu);
+    if (uniform && acq.do_relaxation && !in.t_inhom)
+      for (size_t k = before; k < lines.size(); ++k) {
+        LineRec& L = lines[k];
+        double t = lt.t_ms[L.ky] / 1000.0, trf = lt.trf_ms[L.ky];
+        double inh = a.echo == MRSIM_ECHO_SPIN ? std::fabs(t) * 1000.0 : trf;
+        for (int c = 0; c < ncomp; ++c) L.rel[c] = (float)std::exp(-trf / (double)t2u[c] - inh / a.t_inhom);
+      }
+  }
+  op->n_lines = (int)lines.size();
+  op->samples_per_step = (int64_t)nv * nz * ncoils * (int64_t)lines.size() * nx;
+
+  DevArena& A = op->arena;
+  op->d_images = (float*)A.alloc((size_t)nv * nz * ncomp * plane * 4);
+  op->d_fmap = (float*)A.upload(in.fmap, (size_t)nz * plane * 4, st);
+  if (maps) {
+    bool any_t2 = false, any_ti = false;
+    for (int c = 0; c < ncomp; ++c) {
+      any_t2 = any_t2 || in.t2[c].is_map;
+      any_ti = any_ti || (in.t_inhom && in.t_inhom[c].is_map);
+    }
+    auto build = [&](const mrsim_t2* v) {
+      std::vector<float> m((size_t)ncomp * nz * plane);
+      for (int c = 0; c < ncomp; ++c)
+        for (size_t i = 0; i < (size_t)nz * plane; ++i) m[(size_t)c * nz * plane + i] = v[c].is_map ? v[c].map[i] : v[c].value;
+      return (float*)A.upload(m.data(), m.size() * 4, st);
+    };
+    if (any_t2) op->d_t2 = build(in.t2);
+    if (any_ti) op->d_ti = build(in.t_inhom);
+  }
+  op->geo = build_geo(A, snx, sny, nx, ny, ncoils, acq.ghost_offset, st);
+  op->d_lines = (LineRec*)A.upload(lines.data(), std::max<size_t>(1, lines.size()) * sizeof(LineRec), st);
+  const size_t nunits = (size_t)nv * nz;
+  op->d_phase = (float*)A.alloc(nunits * plane * 4);
+  op->d_g = (float2*)A.alloc(std::max<size_t>(1, nunits * ncoils * lines.size() * snx) * sizeof(float2));
+  op->kspace_elems = nunits * ncoils * ne * (size_t)ny * nx;
+  op->d_kspace = (float2*)A.alloc(op->kspace_elems * sizeof(float2));
+  MRSIM_CUDA(cudaMemsetAsync(op->d_kspace, 0, op->kspace_elems * sizeof(float2), st));
+  op->d_comp_grad = (float2*)A.alloc(nunits * ncomp * plane * sizeof(float2));
+  op->want_fmap = (grads & 1) != 0;
+  op->want_r2 = (grads & 2) != 0;
+  op->d_fmap_grad = op->want_fmap ? (float*)A.alloc(nunits * plane * 4) : nullptr;
+  op->d_r2_grad = op->want_r2 ? (float*)A.alloc(nunits * ncomp * plane * 4) : nullptr;
+
+  std::vector<UnitDesc> units(nunits);
+  std::vector<StaticDesc> statics(nunits);
+  for (int g = 0; g < nv; ++g) {
+    const bool has_eddy = in.eddy_drive_set && in.eddy_drive_set[g];
+    const bool eddy = acq.eddy_strength != 0.0 && has_eddy;
+    const bool eddy_phase = acq.eddy_phase != 0.0 && has_eddy;
+    double grad[3] = {0, 0, 0};
+    if (has_eddy)
+      for (int i = 0; i < 3; ++i) grad[i] = in.eddy_drive[3 * g + i];
+    for (int zl = 0; zl < nz; ++zl) {
+      const int z = slice_z ? (int)slice_z[zl] : zl;
+      const size_t ui = (size_t)g * nz + zl;
+      UnitDesc& u = units[ui];
+      std::memset(&u, 0, sizeof u);
+      u.snx = snx;
+      u.sny = sny;
+      u.nx = nx;
+      u.ny = ny;
+      u.ncomp = ncomp;
+      u.ncoils = ncoils;
+      u.n_lines = (int)lines.size();
+      u.n_rows = ne * ny;
+      u.flags = (acq.do_relaxation ? UF_RELAX : 0) | (maps ? UF_MAPS : 0) | (eddy ? UF_EDDY : 0) |
+                (acq.do_distortions ? UF_DISTORT : 0) | (acq.echo == MRSIM_ECHO_GRADIENT ? UF_GRADIENT : 0) |
+                (op->want_fmap ? UF_WANT_FMAP_GRAD : 0) | (op->want_r2 ? UF_WANT_R2_GRAD : 0);
+      u.z = z;
+      u.nz = nz_full;
+      u.comp_stride = (long long)plane;
+      u.map_stride = (long long)nz * plane;
+      u.comp = op->d_images + ui * ncomp * plane;
+      u.fmap = op->d_fmap + (size_t)zl * plane;
+      u.phase = op->d_phase + ui * plane;
+      u.t2map = op->d_t2 ? op->d_t2 + (size_t)zl * plane : nullptr;
+      u.timap = op->d_ti ? op->d_ti + (size_t)zl * plane : nullptr;
+      u.lines = op->d_lines;
+      u.geo = op->geo;
+      u.signal_scale = (float)acq.signal_scale;
+      for (int c = 0; c < kMaxComp; ++c) {
+        u.t2u[c] = t2u[c];
+        u.tiu[c] = tiu[c];
+      }
+      if (eddy) {
+        const double zc = (double)z - (double)(nz_full / 2);
+        u.eddy_cx = (float)(acq.eddy_strength * grad[0]);
+        u.eddy_qx = (float)(acq.eddy_quad * grad[0]);
+        u.eddy_cy = (float)(acq.eddy_strength * grad[1]);
+        u.eddy_qy = (float)(acq.eddy_quad * grad[1]);
+        u.eddy_z = (float)(acq.eddy_strength * grad[2] * zc + acq.eddy_quad * grad[2] * zc * zc);
+      }
+      u.kspace = op->d_kspace + ui * (size_t)ncoils * ne * ny * nx;
+      u.g = op->d_g + ui * (size_t)ncoils * lines.size() * snx;
+      u.comp_grad = op->d_comp_grad + ui * ncomp * plane;
+      u.fmap_grad = op->d_fmap_grad ? op->d_fmap_grad + ui * plane : nullptr;
+      u.r2_grad = op->d_r2_grad ? op->d_r2_grad + ui * ncomp * plane : nullptr;
+
+      StaticDesc& sd = statics[ui];
+      std::memset(&sd, 0, sizeof sd);
+      sd.snx = snx;
+      sd.sny = sny;
+      sd.nx = nx;
+      sd.ny = ny;
+      sd.o = snx / nx;
+      sd.z = z;
+      sd.nz_full = nz_full;
+      sd.flags = eddy_phase ? 2 : 0;
+      if (in.phase) {
+        sd.global = in.phase->global;
+        for (int k = 0; k < 10; ++k) sd.bg[k] = in.phase->background[k];
+        const bool has_prep = in.prep_drive_set && in.prep_drive_set[g];
+        if (in.phase->has_prep && has_prep) {
+          ShotParams sp = prep_shot(*in.phase, in.prep_drive[4 * g], &in.prep_drive[4 * g + 1], g, z, in.seed);
+          for (int k = 0; k < 3; ++k) {
+            sd.shot_q[k] = sp.q[k];
+            sd.shot_dx[k] = sp.dx[k];
+            sd.shot_rot[k] = sp.rot[k];
+          }
+        }
+      }
+      for (int i = 0; i < 3; ++i) sd.eddy_phase_coef[i] = acq.eddy_phase * grad[i];
+      sd.zc_c = (double)z - ((double)nz_full - 1.0) / 2.0;
+      sd.out = op->d_phase + ui * plane;
+    }
+  }
+  op->plan.reset(epi_plan_create(units.data(), (int)units.size(), statics.data(), (int)statics.size()));
+  if (in.images) upload_series_images(op.get(), in.images);
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+  return op.release();
+}
+
+// Reference layout (per compartment, vox*nv + g with vox = x + snx*(y + sny*z)) to the
+// operator's unit-major layout [g][z][c][y][x], on the device.
+void upload_series_images(EpiOperator* op, const float* const* host_images) {
+  cudaStream_t st = op->ctx->stream;
+  const size_t plane = (size_t)op->snx * op->sny;
+  const size_t per_comp = (size_t)op->nz * plane * op->nv;
+  float* staging = (float*)workspace(op->ctx, 20, per_comp * op->ncomp * 4);
+  for (int c = 0; c < op->ncomp; ++c)
+    MRSIM_CUDA(cudaMemcpyAsync(staging + (size_t)c * per_comp, host_images[c], per_comp * 4, cudaMemcpyHostToDevice, st));
+  launch_series_transpose(staging, op->d_images, op->ncomp, op->nv, op->nz, (int)plane, st);
+}
+
+void epi_operator_forward(EpiOperator* op) {
+  cudaStream_t st = op->ctx->stream;
+  epi_plan_statics(op->plan.get(), st);
+  epi_plan_forward(op->plan.get(), st);
+}
+
+void epi_operator_adjoint(EpiOperator* op) { epi_plan_adjoint(op->plan.get(), op->ctx->stream); }
+
+}  // namespace mrsim

@@ -1,0 +1,71 @@
+// driver.h — host orchestration objects (see driver.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "mrsim_internal.h"
+
+namespace mrsim {
+
+// Device allocations owned by one object, freed together.
+struct DevArena {
+  std::vector<void*> ptrs;
+  void* alloc(size_t bytes);
+  void* upload(const void* src, size_t bytes, cudaStream_t st);
+  DevArena() = default;
+  DevArena(const DevArena&) = delete;
+  DevArena& operator=(const DevArena&) = delete;
+  ~DevArena();
+};
+
+GeoTab build_geo(DevArena& arena, int snx, int sny, int nx, int ny, int ncoils, double ghost, cudaStream_t st);
+
+// `build_coil_kspace_timed` (kspace.rs:607-1042) for every coil of one slice, on the device;
+// returns n_coils*ny*nx complex samples (FP32) with spikes and noise.
+std::vector<float2> slice_forward(mrsim_context* ctx, const mrsim_slice_input& inp, const mrsim_acquisition& acq,
+                                  const double* t_ms, const double* trf_ms, const double* tread_ms,
+                                  const int8_t* polarity, const double* log_amp);
+
+// The forward/adjoint operator of a whole 2D EPI series: units (volume, slice) with every
+// echo's acquired lines.  Device layouts:
+//   images    [g][z][c][sny][snx]            fmap [z][sny][snx]
+//   kspace    [g][z][coil][echo][ny][nx]     complex
+//   comp_grad [g][z][c][sny][snx]            complex (A^H applied to the k-space buffer)
+//   fmap_grad [g][z][sny][snx],  r2_grad [g][z][c][sny][snx]
+struct EpiOperator {
+  mrsim_context* ctx = nullptr;
+  int snx = 0, sny = 0, nx = 0, ny = 0, nz = 0, nv = 0, ncomp = 0, ncoils = 0, n_echoes = 0, n_lines = 0;
+  int64_t samples_per_step = 0;
+  size_t kspace_elems = 0;
+  bool want_fmap = false, want_r2 = false;
+  DevArena arena;
+  float* d_images = nullptr;
+  float* d_fmap = nullptr;
+  float* d_t2 = nullptr;
+  float* d_ti = nullptr;
+  LineRec* d_lines = nullptr;
+  GeoTab geo{};
+  float* d_phase = nullptr;
+  float2* d_g = nullptr;
+  float2* d_kspace = nullptr;
+  float2* d_comp_grad = nullptr;
+  float* d_fmap_grad = nullptr;
+  float* d_r2_grad = nullptr;
+  std::unique_ptr<EpiPlan> plan;
+  ~EpiOperator();
+};
+
+EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_input& in, const mrsim_acquisition& acq,
+                                 const double* echo_times_ms, int64_t n_echoes, const int64_t* slice_z,
+                                 int64_t nz_full, int grads);
+void upload_series_images(EpiOperator* op, const float* const* host_images);
+void epi_operator_forward(EpiOperator* op);
+void epi_operator_adjoint(EpiOperator* op);
+
+// misc_kernels.cu
+void launch_series_transpose(const float* staging, float* out, int ncomp, int nv, int nz, int plane, cudaStream_t st);
+
+}  // namespace mrsim

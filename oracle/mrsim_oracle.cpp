@@ -1218,6 +1218,298 @@ SeriesOut acquire_volumes_complex(const mrsim_acquisition_input& in, const mrsim
   return out;
 }
 
+// ---- the series operator pair (no reference counterpart for the adjoint) ----
+// Forward: for every (volume g, slice z, echo e, coil q) the noiseless, spike-free
+// `build_coil_kspace_timed` (kspace.rs:607-1042) of the series' slice input (kspace.rs:1985-2030
+// for the slice input, `echo_times` as in `simulate_acquisition_echoes` kspace.rs:2152).
+// Adjoint: the FP64 transpose of that forward with respect to complex compartment images, plus
+// dL/dfmap and dL/dR2_c for L = sum |k|^2 (the k-space passed in is the residual).  It uses the
+// same factoring as the forward: x-stage twiddles, and per-voxel states advanced line to line by
+// memoised rotors re-anchored to the closed form every 32 lines (kspace.rs:848-884).
+struct SeriesSlice {
+  std::vector<std::vector<float>> comps;
+  std::vector<const float*> refs;
+  std::vector<float> fmap;
+  std::vector<double> phi;
+  std::vector<mrsim_t2> t2s, tis;
+  mrsim_slice_input si;
+};
+
+SeriesSlice series_slice(const mrsim_acquisition_input& in, size_t g, size_t zl, size_t nz_full, const int64_t* slice_z,
+                         uint64_t seed) {
+  size_t snx = in.sim_dims[0], sny = in.sim_dims[1], nz = in.sim_dims[2];
+  size_t nv = in.n_volumes, ncomp = in.ncomp, o = snx / in.acq_dims[0];
+  size_t z = slice_z ? (size_t)slice_z[zl] : zl;
+  SeriesSlice S;
+  S.comps.assign(ncomp, std::vector<float>(snx * sny));
+  S.fmap.resize(snx * sny);
+  for (size_t p = 0; p < snx * sny; ++p) {
+    size_t vox = p + snx * sny * zl;
+    for (size_t c = 0; c < ncomp; ++c) S.comps[c][p] = in.images[c][vox * nv + g];
+    S.fmap[p] = in.fmap[vox];
+  }
+  for (auto& c : S.comps) S.refs.push_back(c.data());
+  S.t2s.resize(ncomp);
+  for (size_t c = 0; c < ncomp; ++c) {
+    S.t2s[c] = in.t2[c];
+    if (in.t2[c].is_map) S.t2s[c].map = in.t2[c].map + zl * snx * sny;
+  }
+  if (in.t_inhom) {
+    S.tis.resize(ncomp);
+    for (size_t c = 0; c < ncomp; ++c) {
+      S.tis[c] = in.t_inhom[c];
+      if (in.t_inhom[c].is_map) S.tis[c].map = in.t_inhom[c].map + zl * snx * sny;
+    }
+  }
+  Shot shot;
+  bool has_prep = in.prep_drive_set && in.prep_drive_set[g];
+  if (in.phase && in.phase->has_prep && has_prep)
+    shot = prep_shot(*in.phase, in.prep_drive[4 * g], &in.prep_drive[4 * g + 1], g, z, seed);
+  mrsim_phase_model zero;
+  memset(&zero, 0, sizeof zero);
+  S.phi = phase_slice(in.phase ? *in.phase : zero, shot, snx, sny, o, z, nz_full);
+  (void)nz;
+  memset(&S.si, 0, sizeof S.si);
+  S.si.compartments = S.refs.data();
+  S.si.ncomp = ncomp;
+  S.si.t2 = S.t2s.data();
+  S.si.t_inhom = in.t_inhom ? S.tis.data() : nullptr;
+  S.si.fmap = S.fmap.data();
+  S.si.phase0 = S.phi.data();
+  S.si.sim[0] = snx;
+  S.si.sim[1] = sny;
+  S.si.acq_matrix[0] = in.acq_dims[0];
+  S.si.acq_matrix[1] = in.acq_dims[1];
+  S.si.z = z;
+  S.si.nz = nz_full;
+  bool has_eddy = in.eddy_drive_set && in.eddy_drive_set[g];
+  S.si.has_eddy_drive = has_eddy;
+  if (has_eddy)
+    for (int i = 0; i < 3; ++i) S.si.eddy_drive[i] = in.eddy_drive[3 * g + i];
+  return S;
+}
+
+void series_forward(const mrsim_acquisition_input& in, const mrsim_acquisition& acq0, const double* tes, size_t ne,
+                    const int64_t* slice_z, size_t nz_full, int threads, double* out) {
+  size_t nx = in.acq_dims[0], ny = in.acq_dims[1], nz = in.sim_dims[2], nv = in.n_volumes;
+  size_t nc = std::max<int64_t>(acq0.n_coils, 1);
+  if (nz_full == 0) nz_full = nz;
+  parallel_for(nv * nz, threads, [&](size_t u) {
+    size_t g = u / nz, zl = u % nz;
+    SeriesSlice S = series_slice(in, g, zl, nz_full, slice_z, in.seed);
+    for (size_t e = 0; e < ne; ++e) {
+      mrsim_acquisition a = acq0;
+      a.t_echo = tes ? tes[e] : acq0.t_echo;
+      a.noise_variance = 0.0;
+      a.n_spikes = 0;
+      LineTiming lt = line_timing_for(a, nx, ny);
+      for (size_t q = 0; q < nc; ++q) {
+        auto k = build_coil_kspace_timed(S.si, a, q, nc, lt, nullptr);
+        double* dst = out + 2 * (((u * nc + q) * ne + e) * ny * nx);
+        for (size_t i = 0; i < nx * ny; ++i) {
+          dst[2 * i] = k[i].re;
+          dst[2 * i + 1] = k[i].im;
+        }
+      }
+    }
+  });
+}
+
+// Adjoint of one (unit, echo, coil): accumulates into cg [c][p] (complex), U, V [c][p] (complex).
+void unit_adjoint(const mrsim_slice_input& inp, const mrsim_acquisition& acq, size_t coil, size_t ncoils,
+                  const LineTiming& timing, const double* r, std::vector<Cx>& cg, std::vector<Cx>& U,
+                  std::vector<Cx>& V) {
+  size_t snx = inp.sim[0], sny = inp.sim[1], nx = inp.acq_matrix[0], ny = inp.acq_matrix[1];
+  size_t ncomp = inp.ncomp, nvox = snx * sny;
+  size_t z = inp.z, nz = inp.nz;
+  double gradient[3] = {0, 0, 0};
+  if (inp.has_eddy_drive)
+    for (int i = 0; i < 3; ++i) gradient[i] = inp.eddy_drive[i];
+  bool do_eddy = eddy_enabled(acq, inp);
+  bool do_eddy_phase = acq.eddy_phase != 0.0 && inp.has_eddy_drive;
+  size_t xs = nx / 2, ys = ny / 2, zs = nz / 2;
+  size_t ox = snx / nx, oy = sny / ny, sxs = ox * xs, sys = oy * ys;
+  double xoff = ((double)ox - 1.0) / 2.0, yoff = ((double)oy - 1.0) / 2.0;
+  auto mask = sampling_mask(nx, ny, acq);
+  double zc = (double)z - (double)zs, zc_c = (double)z - ((double)nz - 1.0) / 2.0;
+  std::vector<double> amp(nvox), phi0(nvox), rate(nvox);
+  for (size_t y = 0; y < sny; ++y)
+    for (size_t x = 0; x < snx; ++x) {
+      size_t i = x + snx * y;
+      amp[i] = acq.signal_scale *
+               coil_sensitivity(coil, ncoils, ((double)x - xoff) / (double)ox, ((double)y - yoff) / (double)oy, nx, ny);
+      double xc = ((double)x - (double)sxs - xoff) / (double)ox, yc = ((double)y - (double)sys - yoff) / (double)oy;
+      double p0 = inp.phase0 ? inp.phase0[i] : 0.0;
+      if (do_eddy_phase) p0 += acq.eddy_phase * (gradient[0] * xc + gradient[1] * yc + gradient[2] * zc_c);
+      if (acq.echo == MRSIM_ECHO_GRADIENT && acq.do_distortions) p0 += TAU * (double)inp.fmap[i] * (acq.t_echo / 1000.0);
+      phi0[i] = p0;
+      rate[i] = acq.do_distortions ? (double)inp.fmap[i] : 0.0;
+    }
+  XStage xst(snx, nx, xs, sxs, xoff, acq.ghost_offset);
+  double n_inv = 1.0 / (double)nvox;
+  std::vector<Cx> h(snx);
+  std::vector<Cx> st(nvox);
+  auto set_state = [&](size_t kyi) {
+    double t = timing.t_ms[kyi] / 1000.0;
+    double kyn = ((double)kyi - (double)ys) / (double)sny;
+    for (size_t y = 0; y < sny; ++y) {
+      double yy = (double)y - (double)sys - yoff;
+      for (size_t x = 0; x < snx; ++x) {
+        size_t i = x + snx * y;
+        double ph = phi0[i] + TAU * (rate[i] * t + kyn * yy);
+        st[i] = {amp[i] * std::cos(ph), amp[i] * std::sin(ph)};
+      }
+    }
+  };
+  struct ARotor {
+    size_t k0, k1;
+    double dt, dkyn;
+    std::vector<Cx> rot;
+  };
+  std::vector<ARotor> rotors;
+  bool have_prev = false;
+  size_t prev = 0, since_anchor = 0;
+  bool rel_uniform = true;
+  for (size_t c = 0; c < ncomp; ++c) rel_uniform = rel_uniform && !inp.t2[c].is_map;
+  if (inp.t_inhom)
+    for (size_t c = 0; c < ncomp; ++c) rel_uniform = rel_uniform && !inp.t_inhom[c].is_map;
+  for (size_t kyi = 0; kyi < ny; ++kyi) {
+    if (!mask[nx * kyi]) continue;
+    double t = timing.t_ms[kyi] / 1000.0, trf = timing.trf_ms[kyi];
+    double tph = acq.echo == MRSIM_ECHO_SPIN ? t : t + acq.t_echo / 1000.0;
+    double kyn = ((double)kyi - (double)ys) / (double)sny;
+    double ghost_shift = timing.polarity[kyi] < 0 ? -acq.ghost_offset : acq.ghost_offset;
+    const std::vector<Cx>& tw = xst.tw[ghost_shift < 0.0 ? 1 : 0];
+    double eddy_decay = do_eddy ? std::exp(-timing.tread_ms[kyi] / acq.eddy_tau) * t : 0.0;
+    // x-adjoint: h[x] = (1/N) conj(E(x)) sum_kx conj(tw[kx][x]) r[kx]
+    for (size_t x = 0; x < snx; ++x) {
+      double ar = 0.0, ai = 0.0;
+      for (size_t kx = 0; kx < nx; ++kx) {
+        Cx w = tw[snx * kx + x];
+        double rr = r[2 * (kx + nx * kyi)], ri = r[2 * (kx + nx * kyi) + 1];
+        ar += w.re * rr + w.im * ri;
+        ai += w.re * ri - w.im * rr;
+      }
+      Cx v = {ar * n_inv, ai * n_inv};
+      if (do_eddy) {
+        double xc = ((double)x - (double)sxs - xoff) / (double)ox;
+        double ph = TAU * ((acq.eddy_strength * gradient[0] * xc + acq.eddy_quad * gradient[0] * xc * xc) +
+                           (acq.eddy_strength * gradient[2] * zc + acq.eddy_quad * gradient[2] * zc * zc)) *
+                    eddy_decay;
+        v = cmul(v, Cx{std::cos(ph), -std::sin(ph)});
+      }
+      h[x] = v;
+    }
+    // advance the per-voxel state amp*e^{i(phi0 + 2pi(rate t + kyn yy))} to this line: closed form
+    // on the first line and every REANCHOR lines, else a memoised rotor (kspace.rs:848-884)
+    if (have_prev && since_anchor < 32) {
+      size_t p = prev, k0 = kyi - p, k1 = p % 2;
+      double dt = t - timing.t_ms[p] / 1000.0;
+      double dkyn = kyn - (((double)p - (double)ys) / (double)sny);
+      size_t idx = rotors.size();
+      for (size_t rr = 0; rr < rotors.size(); ++rr)
+        if (rotors[rr].k0 == k0 && rotors[rr].k1 == k1) {
+          idx = rr;
+          break;
+        }
+      if (idx == rotors.size()) {
+        ARotor R{k0, k1, dt, dkyn, std::vector<Cx>(nvox)};
+        for (size_t y = 0; y < sny; ++y) {
+          double yy = (double)y - (double)sys - yoff;
+          for (size_t x = 0; x < snx; ++x) {
+            size_t i = x + snx * y;
+            double ph = TAU * (rate[i] * dt + dkyn * yy);
+            R.rot[i] = {std::cos(ph), std::sin(ph)};
+          }
+        }
+        rotors.push_back(std::move(R));
+      }
+      const ARotor& R = rotors[idx];
+      if (std::fabs(R.dt - dt) <= 1e-12 * std::max(std::fabs(dt), 1e-300) && R.dkyn == dkyn) {
+        for (size_t i = 0; i < nvox; ++i) st[i] = cmul(st[i], R.rot[i]);
+        since_anchor += 1;
+      } else {
+        set_state(kyi);
+        since_anchor = 0;
+      }
+    } else {
+      set_state(kyi);
+      since_anchor = 0;
+    }
+    prev = kyi;
+    have_prev = true;
+    bool uniform = rel_uniform;
+    std::vector<double> rl(ncomp, 1.0);
+    if (uniform && acq.do_relaxation)
+      for (size_t c = 0; c < ncomp; ++c) {
+        double tic = inp.t_inhom ? (double)inp.t_inhom[c].value : acq.t_inhom;
+        double inh = acq.echo == MRSIM_ECHO_SPIN ? std::fabs(t) * 1000.0 : trf;
+        rl[c] = std::exp(-trf / (double)inp.t2[c].value - inh / tic);
+      }
+    for (size_t y = 0; y < sny; ++y) {
+      Cx eyc = {1.0, 0.0};
+      if (do_eddy) {
+        double yc = ((double)y - (double)sys - yoff) / (double)oy;
+        double eyph = TAU * (acq.eddy_strength * gradient[1] * yc + acq.eddy_quad * gradient[1] * yc * yc) * eddy_decay;
+        eyc = {std::cos(eyph), std::sin(eyph)};
+      }
+      for (size_t x = 0; x < snx; ++x) {
+        size_t i = x + snx * y;
+        Cx sv = do_eddy ? cmul(st[i], eyc) : st[i];
+        // Z = conj(state) h
+        Cx Z = cmul(Cx{sv.re, -sv.im}, h[x]);
+        for (size_t c = 0; c < ncomp; ++c) {
+          double r_ = rl[c];
+          if (!uniform && acq.do_relaxation) {
+            double t2c = t2_value(inp.t2[c], i);
+            double tic = inp.t_inhom ? t2_value(inp.t_inhom[c], i) : acq.t_inhom;
+            double inh = acq.echo == MRSIM_ECHO_SPIN ? std::fabs(t) * 1000.0 : trf;
+            r_ = std::exp(-trf / t2c - inh / tic);
+          }
+          size_t k = c * nvox + i;
+          cg[k] = cadd(cg[k], cscale(Z, r_));
+          U[k] = cadd(U[k], cscale(Z, r_ * tph));
+          V[k] = cadd(V[k], cscale(Z, r_ * trf));
+        }
+      }
+    }
+  }
+}
+
+void series_adjoint(const mrsim_acquisition_input& in, const mrsim_acquisition& acq0, const double* tes, size_t ne,
+                    const int64_t* slice_z, size_t nz_full, int threads, const double* kspace, double* comp_grad,
+                    double* fmap_grad, double* r2_grad) {
+  size_t snx = in.sim_dims[0], sny = in.sim_dims[1], nx = in.acq_dims[0], ny = in.acq_dims[1], nz = in.sim_dims[2];
+  size_t nv = in.n_volumes, ncomp = in.ncomp, nvox = snx * sny;
+  size_t nc = std::max<int64_t>(acq0.n_coils, 1);
+  if (nz_full == 0) nz_full = nz;
+  parallel_for(nv * nz, threads, [&](size_t u) {
+    size_t g = u / nz, zl = u % nz;
+    SeriesSlice S = series_slice(in, g, zl, nz_full, slice_z, in.seed);
+    std::vector<Cx> cg(ncomp * nvox, CZERO), U(ncomp * nvox, CZERO), V(ncomp * nvox, CZERO);
+    for (size_t e = 0; e < ne; ++e) {
+      mrsim_acquisition a = acq0;
+      a.t_echo = tes ? tes[e] : acq0.t_echo;
+      LineTiming lt = line_timing_for(a, nx, ny);
+      for (size_t q = 0; q < nc; ++q)
+        unit_adjoint(S.si, a, q, nc, lt, kspace + 2 * (((u * nc + q) * ne + e) * ny * nx), cg, U, V);
+    }
+    for (size_t c = 0; c < ncomp; ++c)
+      for (size_t p = 0; p < nvox; ++p) {
+        size_t k = c * nvox + p;
+        comp_grad[2 * (u * ncomp * nvox + k)] = cg[k].re;
+        comp_grad[2 * (u * ncomp * nvox + k) + 1] = cg[k].im;
+        if (r2_grad) r2_grad[u * ncomp * nvox + k] = -2.0 * (double)S.comps[c][p] * V[k].re;
+      }
+    if (fmap_grad)
+      for (size_t p = 0; p < nvox; ++p) {
+        double fg = 0.0;
+        for (size_t c = 0; c < ncomp; ++c) fg += (double)S.comps[c][p] * U[c * nvox + p].im;
+        fmap_grad[u * nvox + p] = acq0.do_distortions ? 2.0 * TAU * fg : 0.0;
+      }
+  });
+}
+
 // ---- golden record: tests/golden_baseline.rs:28-126 ----
 struct GoldenCase {
   std::string name;
@@ -1697,6 +1989,20 @@ uint64_t oracle_rng_next(uint64_t seed, int64_t n, uint64_t* out) {
   Rng r(seed);
   for (int64_t i = 0; i < n; ++i) out[i] = r.next_u64();
   return r.s;
+}
+
+// The series operator pair: kspace [g][z][coil][echo][ny][nx] complex128; grads [g][z][c][p].
+int oracle_series_forward(const mrsim_acquisition_input* in, const mrsim_acquisition* acq, const double* tes,
+                          int64_t ne, const int64_t* slice_z, int64_t nz_full, int threads, double* out) {
+  return guard([&] { series_forward(*in, *acq, tes, ne > 0 ? ne : 1, slice_z, nz_full, threads, out); });
+}
+
+int oracle_series_adjoint(const mrsim_acquisition_input* in, const mrsim_acquisition* acq, const double* tes,
+                          int64_t ne, const int64_t* slice_z, int64_t nz_full, int threads, const double* kspace,
+                          double* comp_grad, double* fmap_grad, double* r2_grad) {
+  return guard([&] {
+    series_adjoint(*in, *acq, tes, ne > 0 ? ne : 1, slice_z, nz_full, threads, kspace, comp_grad, fmap_grad, r2_grad);
+  });
 }
 
 int oracle_golden_count(void) {

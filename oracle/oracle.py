@@ -1,0 +1,295 @@
+"""TEST INFRASTRUCTURE ONLY — ctypes binding of the FP64 oracle (liboracle, mrsim_oracle.cpp).
+
+The oracle is a CPU restatement of the reference crate's 2D EPI k-space path, pinned bit for bit
+to the reference's golden record.  Only the tests, `__graft_entry__.smoke()` and `bench.py`'s
+CPU-baseline / reference arm load it, as the checker and the timed CPU baseline; the product
+library (mrsim_acq_b200) never imports, links or calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+import subprocess
+from typing import Optional, Sequence
+
+import numpy as np
+
+from mrsim_acq_b200 import abi
+from mrsim_acq_b200.api import Acquisition, PhaseModel, SliceInput, T2, _Keep, slice_input_c
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB = HERE / "libmrsim_oracle.so"
+_lib = None
+
+
+def build() -> pathlib.Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        P = C.POINTER
+        L.oracle_last_error.restype = C.c_char_p
+        L.oracle_golden_name.restype = C.c_char_p
+        L.oracle_golden_output.restype = C.c_int64
+        L.oracle_golden_output.argtypes = [C.c_int, P(C.c_uint32), C.c_int64]
+        L.oracle_build_coil_kspace.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), C.c_int64, C.c_int64,
+                                               abi.c_f64p, abi.c_f64p, abi.c_f64p, P(C.c_int8), abi.c_f64p, abi.c_f64p]
+        L.oracle_reference_coil_kspace.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), C.c_int64, C.c_int64,
+                                                   abi.c_f64p]
+        L.oracle_simulate_slice.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), abi.c_f32p]
+        L.oracle_simulate_slice_full.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_)] + [abi.c_f64p] * 5
+        L.oracle_series_forward.argtypes = [P(abi.AcquisitionInput_), P(abi.Acquisition_), abi.c_f64p, C.c_int64,
+                                            P(C.c_int64), C.c_int64, C.c_int, abi.c_f64p]
+        L.oracle_series_adjoint.argtypes = [P(abi.AcquisitionInput_), P(abi.Acquisition_), abi.c_f64p, C.c_int64,
+                                            P(C.c_int64), C.c_int64, C.c_int, abi.c_f64p, abi.c_f64p, abi.c_f64p,
+                                            abi.c_f64p]
+        L.oracle_acquire_volumes_complex.argtypes = [P(abi.AcquisitionInput_), P(abi.Acquisition_),
+                                                     P(abi.AcquisitionOptions_), C.c_uint64, C.c_uint64, C.c_int,
+                                                     P(abi.AcquisitionOutput_)]
+        L.oracle_sampling_mask.argtypes = [C.c_int64, C.c_int64, P(abi.Acquisition_), P(C.c_uint8)]
+        L.oracle_pf_skipped_lines.restype = C.c_int64
+        L.oracle_pf_skipped_lines.argtypes = [C.c_int64, P(abi.Acquisition_)]
+        L.oracle_line_timing.argtypes = [P(abi.Acquisition_), C.c_int64, C.c_int64, abi.c_f64p, abi.c_f64p,
+                                         abi.c_f64p, P(C.c_int8)]
+        L.oracle_epi_order.argtypes = [P(abi.Acquisition_), C.c_int64, C.c_int64, P(C.c_int64)]
+        L.oracle_validate_acquisition_timing.argtypes = [P(abi.Acquisition_), C.c_int64, C.c_int64]
+        L.oracle_inverse_2d.argtypes = [abi.c_f64p, C.c_int64, C.c_int64, abi.c_f64p]
+        L.oracle_rng_next.restype = C.c_uint64
+        L.oracle_rng_next.argtypes = [C.c_uint64, C.c_int64, P(C.c_uint64)]
+        L.oracle_echo_salt.restype = C.c_uint64
+        L.oracle_echo_salt.argtypes = [C.c_uint64]
+        L.oracle_coil_sensitivity.restype = C.c_double
+        L.oracle_coil_sensitivity.argtypes = [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int64, C.c_int64]
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != 0:
+        raise RuntimeError(lib().oracle_last_error().decode())
+
+
+# ---- golden record -----------------------------------------------------------------------------
+def golden_outputs() -> list[tuple[str, np.ndarray]]:
+    """The reference's golden record regenerated by the oracle: (name, uint32 bit patterns)."""
+    L = lib()
+    out = []
+    for i in range(L.oracle_golden_count()):
+        name = L.oracle_golden_name(i).decode()
+        n = L.oracle_golden_output(i, None, 0)
+        buf = np.zeros(n, np.uint32)
+        L.oracle_golden_output(i, buf.ctypes.data_as(C.POINTER(C.c_uint32)), n)
+        out.append((name, buf))
+    return out
+
+
+# ---- tables --------------------------------------------------------------------------------------
+def sampling_mask(nx, ny, acq: Acquisition) -> np.ndarray:
+    m = np.zeros(nx * ny, np.uint8)
+    _check(lib().oracle_sampling_mask(nx, ny, C.byref(acq.to_c()), m.ctypes.data_as(C.POINTER(C.c_uint8))))
+    return m.reshape(ny, nx).astype(bool)
+
+
+def line_timing(acq: Acquisition, nx, ny):
+    t, trf, tread = (np.zeros(ny) for _ in range(3))
+    pol = np.zeros(ny, np.int8)
+    _check(lib().oracle_line_timing(C.byref(acq.to_c()), nx, ny, t.ctypes.data_as(abi.c_f64p),
+                                    trf.ctypes.data_as(abi.c_f64p), tread.ctypes.data_as(abi.c_f64p),
+                                    pol.ctypes.data_as(C.POINTER(C.c_int8))))
+    return t, trf, tread, pol
+
+
+# ---- per slice ---------------------------------------------------------------------------------
+def build_coil_kspace(inp: SliceInput, acq: Acquisition, coil: int, ncoils: int, timing=None,
+                      log_amp=None) -> np.ndarray:
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    nx, ny = inp.acq_matrix
+    out = np.zeros(nx * ny * 2)
+    t = [None] * 4
+    if timing is not None:
+        t = [keep.f64(timing.t_ms), keep.f64(timing.trf_ms), keep.f64(timing.tread_ms)]
+        pol = np.ascontiguousarray(timing.polarity, np.int8)
+        keep.append(pol)
+        t.append(pol.ctypes.data_as(C.POINTER(C.c_int8)))
+    la = keep.f64(np.ravel(log_amp)) if log_amp is not None else None
+    _check(lib().oracle_build_coil_kspace(C.byref(s), C.byref(acq.to_c()), coil, ncoils, t[0], t[1], t[2], t[3], la,
+                                          out.ctypes.data_as(abi.c_f64p)))
+    return out.view(np.complex128).reshape(ny, nx)
+
+
+def reference_coil_kspace(inp: SliceInput, acq: Acquisition, coil: int, ncoils: int) -> np.ndarray:
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    nx, ny = inp.acq_matrix
+    out = np.zeros(nx * ny * 2)
+    _check(lib().oracle_reference_coil_kspace(C.byref(s), C.byref(acq.to_c()), coil, ncoils,
+                                              out.ctypes.data_as(abi.c_f64p)))
+    return out.view(np.complex128).reshape(ny, nx)
+
+
+def simulate_slice(inp: SliceInput, acq: Acquisition) -> np.ndarray:
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    nx, ny = inp.acq_matrix
+    out = np.zeros(nx * ny * 2, np.float32)
+    _check(lib().oracle_simulate_slice(C.byref(s), C.byref(acq.to_c()), out.ctypes.data_as(abi.c_f32p)))
+    return out.view(np.complex64).reshape(ny, nx)
+
+
+def simulate_slice_full(inp: SliceInput, acq: Acquisition, capture=True) -> dict:
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    nx, ny = inp.acq_matrix
+    nc = max(acq.n_coils, 1)
+    comb = np.zeros(nx * ny * 2)
+    bufs = {k: np.zeros(nc * nx * ny * 2) for k in ("acquired", "reconstructed", "coil_images")} if capture else {}
+    sens = np.zeros(nc * nx * ny)
+
+    def p(a):
+        return a.ctypes.data_as(abi.c_f64p) if a is not None else None
+
+    _check(lib().oracle_simulate_slice_full(C.byref(s), C.byref(acq.to_c()), p(comb), p(bufs.get("acquired")),
+                                            p(bufs.get("reconstructed")), p(bufs.get("coil_images")), p(sens)))
+    out = {"combined": comb.view(np.complex128).reshape(ny, nx), "sensitivities": sens.reshape(nc, ny, nx)}
+    for k, v in bufs.items():
+        out[k] = v.view(np.complex128).reshape(nc, ny, nx)
+    return out
+
+
+# ---- series --------------------------------------------------------------------------------------
+def _series_input(keep: _Keep, sim_dims, acq_dims, n_volumes, images, t2, fmap, t_inhom=None, eddy_drive=None,
+                  prep_drive=None, phase: Optional[PhaseModel] = None, seed=0, noise_sigma=None):
+    inp = abi.AcquisitionInput_()
+    for i in range(3):
+        inp.sim_dims[i] = sim_dims[i]
+        inp.acq_dims[i] = acq_dims[i]
+    inp.n_volumes = n_volumes
+    inp.ncomp = len(t2)
+    inp.images = keep.ptrs([np.ravel(a) for a in images])
+    inp.t2 = keep.t2s(t2)
+    inp.t_inhom = keep.t2s(t_inhom) if t_inhom is not None else None
+    inp.fmap = keep.f32(np.ravel(fmap))
+    if eddy_drive is not None:
+        flags = np.array([d is not None for d in eddy_drive], np.int32)
+        vals = np.array([d if d is not None else (0.0, 0.0, 0.0) for d in eddy_drive], np.float64)
+        keep += [flags, vals]
+        inp.eddy_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        inp.eddy_drive = vals.ctypes.data_as(abi.c_f64p)
+    if prep_drive is not None:
+        flags = np.array([d is not None for d in prep_drive], np.int32)
+        vals = np.array([(d[0], *d[1]) if d is not None else (0, 0, 0, 0) for d in prep_drive], np.float64)
+        keep += [flags, vals]
+        inp.prep_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        inp.prep_drive = vals.ctypes.data_as(abi.c_f64p)
+    ph = (phase or PhaseModel.none()).to_c()
+    keep.append(ph)
+    inp.phase = C.pointer(ph)
+    inp.seed = int(seed)
+    if noise_sigma is not None:
+        inp.noise_sigma = keep.f32(np.ravel(noise_sigma))
+    return inp
+
+
+def series_forward(sim_dims, acq_dims, n_volumes, images, t2, fmap, acq: Acquisition, echo_times_ms=None,
+                   threads=1, slice_z=None, nz_full=0, **kw) -> np.ndarray:
+    keep = _Keep()
+    inp = _series_input(keep, sim_dims, acq_dims, n_volumes, images, t2, fmap, **kw)
+    ne = len(echo_times_ms) if echo_times_ms is not None else 1
+    tes = keep.f64(echo_times_ms) if echo_times_ms is not None else None
+    nx, ny, nz = acq_dims
+    nc = max(acq.n_coils, 1)
+    out = np.zeros(n_volumes * nz * nc * ne * ny * nx * 2)
+    sz = None
+    if slice_z is not None:
+        a = np.ascontiguousarray(slice_z, np.int64)
+        keep.append(a)
+        sz = a.ctypes.data_as(C.POINTER(C.c_int64))
+    _check(lib().oracle_series_forward(C.byref(inp), C.byref(acq.to_c()), tes, ne, sz, nz_full, threads,
+                                       out.ctypes.data_as(abi.c_f64p)))
+    return out.view(np.complex128).reshape(n_volumes, nz, nc, ne, ny, nx)
+
+
+def series_adjoint(sim_dims, acq_dims, n_volumes, images, t2, fmap, acq: Acquisition, kspace, echo_times_ms=None,
+                   threads=1, slice_z=None, nz_full=0, **kw) -> dict:
+    keep = _Keep()
+    inp = _series_input(keep, sim_dims, acq_dims, n_volumes, images, t2, fmap, **kw)
+    ne = len(echo_times_ms) if echo_times_ms is not None else 1
+    tes = keep.f64(echo_times_ms) if echo_times_ms is not None else None
+    snx, sny, nz = sim_dims
+    nc = len(t2)
+    k = np.ascontiguousarray(kspace, np.complex128)
+    cg = np.zeros(n_volumes * nz * nc * sny * snx * 2)
+    fg = np.zeros(n_volumes * nz * sny * snx)
+    rg = np.zeros(n_volumes * nz * nc * sny * snx)
+    sz = None
+    if slice_z is not None:
+        a = np.ascontiguousarray(slice_z, np.int64)
+        keep.append(a)
+        sz = a.ctypes.data_as(C.POINTER(C.c_int64))
+    _check(lib().oracle_series_adjoint(C.byref(inp), C.byref(acq.to_c()), tes, ne, sz, nz_full, threads,
+                                       k.ctypes.data_as(abi.c_f64p), cg.ctypes.data_as(abi.c_f64p),
+                                       fg.ctypes.data_as(abi.c_f64p), rg.ctypes.data_as(abi.c_f64p)))
+    return {"comp_grad": cg.view(np.complex128).reshape(n_volumes, nz, nc, sny, snx),
+            "fmap_grad": fg.reshape(n_volumes, nz, sny, snx), "r2_grad": rg.reshape(n_volumes, nz, nc, sny, snx)}
+
+
+def acquire_volumes_complex(sim_dims, acq_dims, n_volumes, images, t2, fmap, acq: Acquisition, excitation_seed,
+                            receiver_seed, threads=1, options: Optional[dict] = None, **kw) -> dict:
+    keep = _Keep()
+    inp = _series_input(keep, sim_dims, acq_dims, n_volumes, images, t2, fmap, seed=receiver_seed, **kw)
+    o = abi.AcquisitionOptions_()
+    options = options or {}
+    nx, ny, nz = acq_dims
+    if options.get("t_echo_per_volume") is not None:
+        o.t_echo_per_volume = keep.f64(options["t_echo_per_volume"])
+    if options.get("slice_z") is not None:
+        a = np.ascontiguousarray(options["slice_z"], np.int64)
+        keep.append(a)
+        o.slice_z = a.ctypes.data_as(C.POINTER(C.c_int64))
+    o.nz_full = int(options.get("nz_full", 0))
+    caps = options.get("kspace_slices")
+    nsl = 0
+    if caps is not None:
+        a = np.ascontiguousarray(caps, np.int64)
+        keep.append(a)
+        o.kspace_slices = a.ctypes.data_as(C.POINTER(C.c_int64))
+        o.n_kspace_slices = nsl = len(caps)
+        o.capture_acquired = int(options.get("acquired", False))
+        o.capture_reconstructed = int(options.get("reconstructed", False))
+        o.capture_coil_images = int(options.get("coil_images", False))
+    if options.get("grappa_calibration") is not None:
+        cal_images, cal_seed = options["grappa_calibration"]
+        o.has_grappa_calibration = 1
+        o.grappa_calibration_images = keep.ptrs([np.ravel(a) for a in cal_images])
+        o.grappa_calibration_seed = int(cal_seed)
+    nvox = nx * ny * nz
+    nc = max(acq.n_coils, 1)
+    re = np.zeros(nvox * n_volumes, np.float32)
+    im = np.zeros(nvox * n_volumes, np.float32)
+    out = abi.AcquisitionOutput_()
+    out.re = re.ctypes.data_as(abi.c_f32p)
+    out.im = im.ctypes.data_as(abi.c_f32p)
+    cap = {}
+    if nsl:
+        for key in ("acquired", "reconstructed", "coil_images"):
+            if options.get(key):
+                cap[key] = np.zeros(n_volumes * nsl * nc * nx * ny * 2, np.float32)
+                setattr(out, key, cap[key].ctypes.data_as(abi.c_f32p))
+        cap["combined"] = np.zeros(n_volumes * nsl * nx * ny * 2, np.float32)
+        out.combined = cap["combined"].ctypes.data_as(abi.c_f32p)
+        cap["mask"] = np.zeros(nx * ny, np.uint8)
+        out.mask = cap["mask"].ctypes.data_as(C.POINTER(C.c_uint8))
+        cap["sensitivities"] = np.zeros(nc * nx * ny, np.float32)
+        out.sensitivities = cap["sensitivities"].ctypes.data_as(abi.c_f32p)
+    _check(lib().oracle_acquire_volumes_complex(C.byref(inp), C.byref(acq.to_c()), C.byref(o), excitation_seed,
+                                                receiver_seed, threads, C.byref(out)))
+    res = {"re": re, "im": im}
+    res.update(cap)
+    return res

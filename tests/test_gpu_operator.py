@@ -1,0 +1,96 @@
+"""GPU parity of the batched series operator pair: the forward over every (volume, slice, echo,
+coil) and its adjoint / VJP (no reference counterpart; checked against the FP64 transpose, the
+dot-product identity and central finite differences)."""
+import numpy as np
+import pytest
+
+from mrsim_acq_b200 import api
+from mrsim_acq_b200.api import Acquisition, PartialFourierMode, PhaseModel
+from oracle import oracle
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def rel_l2(a, b):
+    n = np.linalg.norm(np.ravel(b))
+    return np.linalg.norm(np.ravel(a - b)) / (n if n > 0 else 1.0)
+
+
+def _setup(maps=False, eddy=True, gradient=False, nv=2, nz=2, ncomp=3, coils=4):
+    s = cases.series_case(nv=nv, nz=nz, ncomp=ncomp, maps=maps)
+    acq = Acquisition(n_coils=coils, accel=2, partial_fourier=0.75, pf_mode=PartialFourierMode.Scanner, t_line=0.5,
+                      t_echo=30.0, ghost_offset=0.02, eddy_strength=2.0 if eddy else 0.0, eddy_quad=0.3,
+                      eddy_phase=0.1 if eddy else 0.0)
+    if gradient:
+        acq = acq.replace(echo=api.EchoFormation.Gradient)
+    tes = [15.0, 35.0, 55.0]
+    kw = dict(t_inhom=s["t_inhom"], eddy_drive=[(0.5, -0.4, 0.7) if g % 2 == 0 else None for g in range(nv)],
+              prep_drive=[(1000.0, (0.6, 0.8, 0.0))] * nv, phase=PhaseModel.hbcd_like(), seed=42)
+    return s, acq, tes, kw
+
+
+@pytest.mark.parametrize("maps,eddy,gradient", [(False, False, False), (False, True, False), (True, True, False),
+                                                (False, True, True)])
+def test_series_forward_and_adjoint_match_the_oracle(maps, eddy, gradient, gpu_ctx):
+    s, acq, tes, kw = _setup(maps, eddy, gradient)
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], s["n_volumes"], s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
+    out = op.apply_host(None)
+    want = oracle.series_forward(s["sim_dims"], s["acq_dims"], s["n_volumes"], s["images"], s["t2"], s["fmap"], acq,
+                                 echo_times_ms=tes, **kw)
+    assert out["kspace"].shape == want.shape
+    assert rel_l2(out["kspace"], want) <= TOL, rel_l2(out["kspace"], want)
+    adj = oracle.series_adjoint(s["sim_dims"], s["acq_dims"], s["n_volumes"], s["images"], s["t2"], s["fmap"], acq,
+                                out["kspace"].astype(np.complex128), echo_times_ms=tes, **kw)
+    for key in ("comp_grad", "fmap_grad", "r2_grad"):
+        e = rel_l2(out[key], adj[key])
+        assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
+
+
+def test_adjoint_identity(gpu_ctx):
+    """<A x, y> = <x, A^H y> with the GPU forward and adjoint (x the real images, y random k-space
+    on the acquired samples)."""
+    s, acq, tes, kw = _setup()
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], s["n_volumes"], s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=0, ctx=gpu_ctx, **kw)
+    Ax = op.apply_host(None)["kspace"].astype(np.complex128)
+    rng = np.random.default_rng(3)
+    y = (rng.standard_normal(Ax.shape) + 1j * rng.standard_normal(Ax.shape)) * (Ax != 0)
+    cg = op.adjoint_host(y.astype(np.complex64))["comp_grad"].astype(np.complex128)
+    snx, sny, nz = s["sim_dims"]
+    nv, nc = s["n_volumes"], len(s["t2"])
+    x = np.stack([s["images"][c].reshape(nz, sny, snx, nv) for c in range(nc)])  # [c][z][y][x][g]
+    x = np.transpose(x, (4, 1, 0, 2, 3))  # [g][z][c][y][x]
+    lhs = np.vdot(y, Ax)                # <A x, y> conj convention: sum conj(y) Ax
+    rhs = np.vdot(cg, x)                # sum conj(A^H y) x
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs), (lhs, rhs)
+
+
+def test_fieldmap_and_r2_vjp_match_central_differences(gpu_ctx):
+    """dL/dfmap and dL/dR2 at seeded voxels against central differences of the FP64 oracle
+    forward, L = sum |A(m, fmap, R2)|^2 (h = 1e-3 Hz and a relative 1e-3 step in T2)."""
+    s, acq, tes, kw = _setup(eddy=False, nv=1, nz=1)
+    acq = acq.replace(n_coils=2)
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], 1, s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
+    out = op.apply_host(None)
+    snx, sny, _ = s["sim_dims"]
+    rng = np.random.default_rng(11)
+    vox = rng.choice(snx * sny, 6, replace=False)
+
+    def loss(fmap):
+        k = oracle.series_forward(s["sim_dims"], s["acq_dims"], 1, s["images"], s["t2"], fmap, acq,
+                                  echo_times_ms=tes, **kw)
+        return float(np.sum(np.abs(k) ** 2))
+
+    h = 1e-3
+    f0 = s["fmap"].astype(np.float64)
+    for v in vox:
+        fp, fm = f0.copy(), f0.copy()
+        fp[v] += h
+        fm[v] -= h
+        fd = (loss(fp.astype(np.float32)) - loss(fm.astype(np.float32))) / (fp[v].astype(np.float32) - fm[v].astype(np.float32))
+        g = out["fmap_grad"].reshape(-1)[v]
+        assert abs(g - fd) <= 2e-3 * max(abs(fd), 1e-3 * np.abs(out["fmap_grad"]).max()), (v, g, fd)
