@@ -120,7 +120,7 @@ class Clocks:
         sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4) if "Active" in r[5 + i]})
+        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4) if r[5 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
 
@@ -208,8 +208,8 @@ def run_ours(args, rank, world, local_rank):
     out = {"kspace": pin(shp["kspace"] + (2,), torch.float32).view(np.complex64)[..., 0],
            "comp_grad": pin(shp["comp_grad"] + (2,), torch.float32).view(np.complex64)[..., 0],
            "fmap_grad": pin(shp["fmap_grad"], torch.float32), "r2_grad": pin(shp["r2_grad"], torch.float32)}
-    e2e_steps = max(2, min(args.steps, 5))
-    for _ in range(2):
+    e2e_steps = 0 if args.no_e2e else max(2, min(args.steps, 5))
+    for _ in range(2 if e2e_steps else 0):
         op.apply_host(host_imgs, out)
     if world > 1:
         torch.distributed.barrier()
@@ -220,7 +220,7 @@ def run_ours(args, rank, world, local_rank):
         op.apply_host(host_imgs, out)
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1) / e2e_steps], dtype=torch.float64, device="cuda")
+    e2e_ms = torch.tensor([e0.elapsed_time(e1) / max(e2e_steps, 1)], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
     h2d = sum(a.nbytes for a in host_imgs)
@@ -254,7 +254,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res["cpu_baseline"] = cpu_baseline(acq, inp, sample_volumes=1, sample_slices=args.cpu_slices)
+        res["cpu_baseline"] = cpu_baseline(acq, inp, sample_volumes=args.cpu_volumes, sample_slices=args.cpu_slices)
     return res, op, ctx
 
 
@@ -317,9 +317,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-slices", type=int, default=30)
+    ap.add_argument("--cpu-volumes", type=int, default=3)
     ap.add_argument("--ref-slices", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--volumes", type=int, default=0, help="override the volume count (smaller profiling case)")
     args = ap.parse_args()
+    if args.volumes > 0:
+        WORKLOAD["nv"] = args.volumes
+        WORKLOAD["name"] = WORKLOAD["name"].replace("-v40-", f"-v{args.volumes}-")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
