@@ -205,6 +205,23 @@ int mrsim_build_coil_kspaces(mrsim_context* ctx, const mrsim_slice_input* inp,
                              const double* trf_ms, const double* tread_ms,
                              const int8_t* polarity, const double* log_amp, double* out);
 
+/* No counterpart in the reference: a forward that allocates no device memory.  For callers that
+ * may not call cudaMalloc while they run (a host whose device memory is all in its own pool or
+ * arena, a pipeline that pre-allocates at start-up so no call can stall or fail on allocation).
+ * Computes what mrsim_build_coil_kspaces computes with noise_variance = 0 and n_spikes = 0, for
+ * uniform T2/T2' (no maps, no log-amplitude), into `kspace` (DEVICE, n_coils*ny*nx (re, im) f32).
+ * `inp` is a host struct whose data pointers are DEVICE pointers: the compartment planes
+ * contiguous (plane c at compartments[0] + c*snx*sny), fmap, and phase0 (f64) or NULL.  `stream`
+ * is a cudaStream_t (NULL: the legacy default stream) of the current device; the call returns
+ * when the output is complete.  Intermediates live in static device arrays of ~7.6 MiB held by
+ * every GPU that loads the library until exit; limits: n_coils*acquired_lines*snx <= 524288,
+ * snx*sny <= 262144, snx*nx <= 65536, n_coils*max(snx,sny) <= 32768, acquired lines <= 1024 —
+ * larger inputs fail with MRSIM_ERR_INVALID.  The first call on a device looks up the arrays'
+ * addresses (cudaGetSymbolAddress, that device current); make it before any stream capture.
+ * Calls share the arrays: calls that overlap on the GPU race and must be serialised. */
+int mrsim_build_coil_kspaces_noalloc(const mrsim_slice_input* inp, const mrsim_acquisition* acq,
+                                     void* stream, float* kspace);
+
 /* ---- the batched forward / adjoint operator of a 2D EPI series --------------------------- */
 /*
  * The series' forward model `build_coil_kspace_timed` (kspace.rs:607-1042, without spikes and

@@ -183,6 +183,16 @@ int mrsim_build_coil_kspaces(mrsim_context* ctx, const mrsim_slice_input* inp, c
   });
 }
 
+int mrsim_build_coil_kspaces_noalloc(const mrsim_slice_input* inp, const mrsim_acquisition* acq, void* stream,
+                                     float* kspace) {
+  return guarded([&] {
+    need(inp, "inp");
+    need(acq, "acq");
+    need(kspace, "kspace");
+    mrsim::build_coil_kspaces_noalloc(*inp, *acq, (float2*)kspace, (cudaStream_t)stream);
+  });
+}
+
 int mrsim_epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_input* in, const mrsim_acquisition* acq,
                               const double* echo_times_ms, int64_t n_echoes, const int64_t* slice_z, int64_t nz_full,
                               int32_t grads, mrsim_epi_operator** out) {

@@ -65,6 +65,10 @@ void upload_series_images(EpiOperator* op, const float* const* host_images);
 void epi_operator_forward(EpiOperator* op);
 void epi_operator_adjoint(EpiOperator* op);
 
+// noalloc.cu: the forward of one slice with every intermediate in static device arrays.
+void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquisition& acq, float2* out,
+                                cudaStream_t st);
+
 // misc_kernels.cu
 void launch_series_transpose(const float* staging, float* out, int ncomp, int nv, int nz, int plane, cudaStream_t st);
 
