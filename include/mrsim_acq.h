@@ -205,6 +205,41 @@ int mrsim_build_coil_kspaces(mrsim_context* ctx, const mrsim_slice_input* inp,
                              const double* trf_ms, const double* tread_ms,
                              const int8_t* polarity, const double* log_amp, double* out);
 
+/* `simulate_slice` kspace.rs:1229-1235: GRAPPA (a lone slice fits its kernel on a reference scan
+ * of itself), window, inverse DFT, Roemer combine.  out = nx*ny (re, im) f32 pairs. */
+int mrsim_simulate_slice(mrsim_context* ctx, const mrsim_slice_input* inp,
+                         const mrsim_acquisition* acq, float* out);
+/* `simulate_slice_full` kspace.rs:1241-1284 with the `SliceCapture` intermediates (kspace.rs:1184-
+ * 1224); combined = nx*ny (re, im) f32; acquired, reconstructed, coil_images = n_coils*nx*ny (re,
+ * im) f32; sensitivities = n_coils*nx*ny f32; mask = nx*ny bytes.  Captures may be NULL. */
+int mrsim_simulate_slice_full(mrsim_context* ctx, const mrsim_slice_input* inp,
+                              const mrsim_acquisition* acq, float* combined, float* acquired,
+                              float* reconstructed, float* coil_images, float* sensitivities,
+                              uint8_t* mask);
+/* `simulate_slice_kspace` kspace.rs:1144-1149: coil 0's acquired k-space, nx*ny (re, im) f64. */
+int mrsim_simulate_slice_kspace(mrsim_context* ctx, const mrsim_slice_input* inp,
+                                const mrsim_acquisition* acq, double* out);
+
+/* ---- series entry points (host buffers) ------------------------------------------------- */
+/* `simulate_acquisition_complex` kspace.rs:1803-1808. */
+int mrsim_simulate_acquisition_complex(mrsim_context* ctx, const mrsim_acquisition_input* inp,
+                                       const mrsim_acquisition* acq,
+                                       const mrsim_acquisition_options* opts,
+                                       mrsim_acquisition_output* out);
+/* `simulate_acquisition_oversampled` kspace.rs:1687-1714: magnitude and phase (f32). */
+int mrsim_simulate_acquisition_oversampled(mrsim_context* ctx, const mrsim_acquisition_input* inp,
+                                           const mrsim_acquisition* acq, float* mag, float* phase);
+/* `simulate_acquisition_echoes` kspace.rs:2152-2174: images_per_echo[e] holds echo e's ncomp
+ * image arrays; grappa_calibration_images[e] (ncomp single volumes) and _seeds[e] are each echo's
+ * `GrappaCalibration` or NULL; mag/phase are n_echoes arrays of nx*ny*nz*n_volumes. */
+int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisition_input* inp,
+                                      const float* const* const* images_per_echo,
+                                      const mrsim_acquisition* acq, const double* echo_times_ms,
+                                      int64_t n_echoes,
+                                      const float* const* const* grappa_calibration_images,
+                                      const uint64_t* grappa_calibration_seeds, float* const* mag,
+                                      float* const* phase);
+
 /* No counterpart in the reference: a forward that allocates no device memory.  For callers that
  * may not call cudaMalloc while they run (a host whose device memory is all in its own pool or
  * arena, a pipeline that pre-allocates at start-up so no call can stall or fail on allocation).

@@ -121,6 +121,20 @@ def _declare(lib):
         "mrsim_epi_order": (C.c_int, [C.POINTER(Acquisition_), C.c_int64, C.c_int64, C.POINTER(C.c_int64)]),
         "mrsim_build_coil_kspaces": (C.c_int, [P, C.POINTER(SliceInput_), C.POINTER(Acquisition_), c_f64p, c_f64p,
                                                c_f64p, C.POINTER(C.c_int8), c_f64p, c_f64p]),
+        "mrsim_simulate_slice": (C.c_int, [P, C.POINTER(SliceInput_), C.POINTER(Acquisition_), c_f32p]),
+        "mrsim_simulate_slice_full": (C.c_int, [P, C.POINTER(SliceInput_), C.POINTER(Acquisition_), c_f32p, c_f32p,
+                                                c_f32p, c_f32p, c_f32p, C.POINTER(C.c_uint8)]),
+        "mrsim_simulate_slice_kspace": (C.c_int, [P, C.POINTER(SliceInput_), C.POINTER(Acquisition_), c_f64p]),
+        "mrsim_simulate_acquisition_complex": (C.c_int, [P, C.POINTER(AcquisitionInput_), C.POINTER(Acquisition_),
+                                                         C.POINTER(AcquisitionOptions_),
+                                                         C.POINTER(AcquisitionOutput_)]),
+        "mrsim_simulate_acquisition_oversampled": (C.c_int, [P, C.POINTER(AcquisitionInput_),
+                                                             C.POINTER(Acquisition_), c_f32p, c_f32p]),
+        "mrsim_simulate_acquisition_echoes": (C.c_int, [P, C.POINTER(AcquisitionInput_),
+                                                        C.POINTER(C.POINTER(c_f32p)), C.POINTER(Acquisition_),
+                                                        c_f64p, C.c_int64, C.POINTER(C.POINTER(c_f32p)),
+                                                        C.POINTER(C.c_uint64), C.POINTER(c_f32p),
+                                                        C.POINTER(c_f32p)]),
         "mrsim_build_coil_kspaces_noalloc": (C.c_int, [C.POINTER(SliceInput_), C.POINTER(Acquisition_), P, c_f32p]),
         "mrsim_epi_operator_create": (C.c_int, [P, C.POINTER(AcquisitionInput_), C.POINTER(Acquisition_), c_f64p,
                                                 C.c_int64, C.POINTER(C.c_int64), C.c_int64, C.c_int32,

@@ -219,6 +219,103 @@ def slice_input_c(inp: SliceInput, keep: _Keep) -> abi.SliceInput_:
     return s
 
 
+@dataclasses.dataclass
+class AcquisitionInput:
+    """`AcquisitionInput` (kspace.rs:1720-1740).  Images: one array per compartment on the sim grid,
+    layout (x + snx*(y + sny*z))*n_volumes + g."""
+
+    sim_dims: tuple
+    acq_dims: tuple
+    n_volumes: int
+    images: Sequence[np.ndarray]
+    t2: Sequence[T2]
+    fmap: np.ndarray
+    t_inhom: Optional[Sequence[T2]] = None
+    eddy_drive: Optional[Sequence] = None
+    prep_drive: Optional[Sequence] = None
+    phase: PhaseModel = dataclasses.field(default_factory=PhaseModel.none)
+    seed: int = 0
+    noise_sigma: Optional[np.ndarray] = None
+
+
+@dataclasses.dataclass
+class AcquisitionOptions:
+    """`AcquisitionOptions` (kspace.rs:1744-1762) with `SliceCapture` flags (kspace.rs:1184)."""
+
+    slice_z: Optional[Sequence[int]] = None
+    nz_full: int = 0
+    kspace_slices: Optional[Sequence[int]] = None
+    acquired: bool = False
+    reconstructed: bool = False
+    coil_images: bool = False
+    t_echo_per_volume: Optional[Sequence[float]] = None
+    progress: Optional[object] = None
+    grappa_calibration: Optional[tuple] = None  # (images per compartment, seed)
+
+
+def acquisition_input_c(inp: AcquisitionInput, keep: _Keep, with_images: bool = True) -> abi.AcquisitionInput_:
+    c = abi.AcquisitionInput_()
+    for i in range(3):
+        c.sim_dims[i] = inp.sim_dims[i]
+        c.acq_dims[i] = inp.acq_dims[i]
+    c.n_volumes = inp.n_volumes
+    c.ncomp = len(inp.t2)
+    if with_images and inp.images is not None:
+        c.images = keep.ptrs([np.ravel(a) for a in inp.images])
+    c.t2 = keep.t2s(inp.t2)
+    c.t_inhom = keep.t2s(inp.t_inhom) if inp.t_inhom is not None else None
+    c.fmap = keep.f32(np.ravel(inp.fmap))
+    if inp.eddy_drive is not None:
+        flags = np.array([d is not None for d in inp.eddy_drive], np.int32)
+        vals = np.array([d if d is not None else (0.0, 0.0, 0.0) for d in inp.eddy_drive], np.float64)
+        keep += [flags, vals]
+        c.eddy_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        c.eddy_drive = vals.ctypes.data_as(abi.c_f64p)
+    if inp.prep_drive is not None:
+        flags = np.array([d is not None for d in inp.prep_drive], np.int32)
+        vals = np.array([(d[0], *d[1]) if d is not None else (0, 0, 0, 0) for d in inp.prep_drive], np.float64)
+        keep += [flags, vals]
+        c.prep_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        c.prep_drive = vals.ctypes.data_as(abi.c_f64p)
+    ph = (inp.phase or PhaseModel.none()).to_c()
+    keep.append(ph)
+    c.phase = C.pointer(ph)
+    c.seed = int(inp.seed) & 0xFFFFFFFFFFFFFFFF
+    if inp.noise_sigma is not None:
+        c.noise_sigma = keep.f32(np.ravel(inp.noise_sigma))
+    return c
+
+
+def acquisition_options_c(o: Optional[AcquisitionOptions], keep: _Keep) -> abi.AcquisitionOptions_:
+    c = abi.AcquisitionOptions_()
+    if o is None:
+        return c
+    if o.slice_z is not None:
+        a = np.ascontiguousarray(o.slice_z, np.int64)
+        keep.append(a)
+        c.slice_z = a.ctypes.data_as(C.POINTER(C.c_int64))
+    c.nz_full = int(o.nz_full)
+    if o.kspace_slices is not None:
+        a = np.ascontiguousarray(o.kspace_slices, np.int64)
+        keep.append(a)
+        c.kspace_slices = a.ctypes.data_as(C.POINTER(C.c_int64))
+        c.n_kspace_slices = len(o.kspace_slices)
+        c.capture_acquired, c.capture_reconstructed, c.capture_coil_images = (int(o.acquired), int(o.reconstructed),
+                                                                              int(o.coil_images))
+    if o.t_echo_per_volume is not None:
+        c.t_echo_per_volume = keep.f64(o.t_echo_per_volume)
+    if o.progress is not None:
+        cb = abi.PROGRESS_FN(lambda done, total, user: o.progress(done, total))
+        keep.append(cb)
+        c.progress = cb
+    if o.grappa_calibration is not None:
+        imgs, seed = o.grappa_calibration
+        c.has_grappa_calibration = 1
+        c.grappa_calibration_images = keep.ptrs([np.ravel(a) for a in imgs])
+        c.grappa_calibration_seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    return c
+
+
 # ---- host tables -------------------------------------------------------------------------------
 def sampling_mask(nx: int, ny: int, acq: Acquisition) -> np.ndarray:
     """`sampling_mask` (kspace.rs:546): bool mask, layout kx + nx*ky (returned as [ny, nx])."""
@@ -332,6 +429,124 @@ def build_coil_kspaces(inp: SliceInput, acq: Acquisition, timing: Optional[LineT
 def simulate_slice_kspace(inp: SliceInput, acq: Acquisition, ctx: Optional[Context] = None) -> np.ndarray:
     """`simulate_slice_kspace` (kspace.rs:1144): coil 0's acquired k-space [ny, nx]."""
     return build_coil_kspaces(inp, acq, ctx=ctx)[0]
+
+
+def simulate_slice(inp: SliceInput, acq: Acquisition, ctx: Optional[Context] = None) -> np.ndarray:
+    """`simulate_slice` (kspace.rs:1229): the Roemer-combined image [ny, nx] complex64 (f32 pairs)."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    nx, ny = inp.acq_matrix
+    out = np.zeros(nx * ny * 2, np.float32)
+    check(lib().mrsim_simulate_slice(ctx.handle, C.byref(s), C.byref(acq.to_c()), out.ctypes.data_as(abi.c_f32p)))
+    return out.view(np.complex64).reshape(ny, nx)
+
+
+def simulate_slice_full(inp: SliceInput, acq: Acquisition, capture: bool = True,
+                        ctx: Optional[Context] = None) -> dict:
+    """`simulate_slice_full` (kspace.rs:1241) with every `SliceCapture` intermediate."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    nx, ny = inp.acq_matrix
+    nc = max(int(acq.n_coils), 1)
+    comb = np.zeros(nx * ny * 2, np.float32)
+    bufs = {k: np.zeros(nc * nx * ny * 2, np.float32) for k in ("acquired", "reconstructed", "coil_images")} \
+        if capture else {}
+    sens = np.zeros(nc * nx * ny, np.float32)
+    mask = np.zeros(nx * ny, np.uint8)
+
+    def p(a):
+        return a.ctypes.data_as(abi.c_f32p) if a is not None else None
+
+    check(lib().mrsim_simulate_slice_full(ctx.handle, C.byref(s), C.byref(acq.to_c()), p(comb),
+                                          p(bufs.get("acquired")), p(bufs.get("reconstructed")),
+                                          p(bufs.get("coil_images")), p(sens),
+                                          mask.ctypes.data_as(C.POINTER(C.c_uint8))))
+    out = {"combined": comb.view(np.complex64).reshape(ny, nx), "sensitivities": sens.reshape(nc, ny, nx),
+           "mask": mask.reshape(ny, nx).astype(bool)}
+    for k, v in bufs.items():
+        out[k] = v.view(np.complex64).reshape(nc, ny, nx)
+    return out
+
+
+def simulate_acquisition_complex(inp: AcquisitionInput, acq: Acquisition,
+                                 opts: Optional[AcquisitionOptions] = None, ctx: Optional[Context] = None) -> dict:
+    """`simulate_acquisition_complex` (kspace.rs:1803): re and im in the layout vox*n_volumes + g,
+    plus the k-space capture of `opts.kspace_slices` ([vol, slice, coil, ky, kx] complex64)."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    ci = acquisition_input_c(inp, keep)
+    co = acquisition_options_c(opts, keep)
+    nx, ny, nz = inp.acq_dims
+    nv = inp.n_volumes
+    nc = max(int(acq.n_coils), 1)
+    n = nx * ny * nz * nv
+    re, im = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    o = abi.AcquisitionOutput_()
+    o.re, o.im = re.ctypes.data_as(abi.c_f32p), im.ctypes.data_as(abi.c_f32p)
+    res = {"re": re, "im": im}
+    nsl = len(opts.kspace_slices) if opts is not None and opts.kspace_slices is not None else 0
+    if nsl:
+        for key in ("acquired", "reconstructed", "coil_images"):
+            if getattr(opts, key):
+                res[key] = np.zeros((nv, nsl, nc, ny, nx), np.complex64)
+                setattr(o, key, C.cast(res[key].ctypes.data, abi.c_f32p))
+        res["combined"] = np.zeros((nv, nsl, ny, nx), np.complex64)
+        o.combined = C.cast(res["combined"].ctypes.data, abi.c_f32p)
+        res["mask"] = np.zeros((ny, nx), np.uint8)
+        o.mask = res["mask"].ctypes.data_as(C.POINTER(C.c_uint8))
+        res["sensitivities"] = np.zeros((nc, ny, nx), np.float32)
+        o.sensitivities = res["sensitivities"].ctypes.data_as(abi.c_f32p)
+    check(lib().mrsim_simulate_acquisition_complex(ctx.handle, C.byref(ci), C.byref(acq.to_c()),
+                                                   C.byref(co) if opts is not None else None, C.byref(o)))
+    if "mask" in res:
+        res["mask"] = res["mask"].astype(bool)
+    return res
+
+
+def simulate_acquisition_oversampled(inp: AcquisitionInput, acq: Acquisition, ctx: Optional[Context] = None):
+    """`simulate_acquisition_oversampled` (kspace.rs:1687): (magnitude, phase), f32."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    ci = acquisition_input_c(inp, keep)
+    nx, ny, nz = inp.acq_dims
+    n = nx * ny * nz * inp.n_volumes
+    mag, ph = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    check(lib().mrsim_simulate_acquisition_oversampled(ctx.handle, C.byref(ci), C.byref(acq.to_c()),
+                                                       mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
+    return mag, ph
+
+
+def simulate_acquisition_echoes(inp: AcquisitionInput, images_per_echo: Sequence[Sequence[np.ndarray]],
+                                acq: Acquisition, echo_times_ms: Sequence[float],
+                                grappa_calibration: Optional[Sequence[tuple]] = None, ctx: Optional[Context] = None):
+    """`simulate_acquisition_echoes` (kspace.rs:2152): [(magnitude, phase)] per echo."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    ci = acquisition_input_c(inp, keep, with_images=False)
+    ne = len(echo_times_ms)
+    ipe = (C.POINTER(abi.c_f32p) * max(ne, 1))()
+    for e, imgs in enumerate(images_per_echo):
+        ipe[e] = keep.ptrs([np.ravel(a) for a in imgs])
+    cal, seeds = None, None
+    if grappa_calibration is not None:
+        cal = (C.POINTER(abi.c_f32p) * ne)()
+        sd = np.zeros(ne, np.uint64)
+        for e, (imgs, seed) in enumerate(grappa_calibration):
+            cal[e] = keep.ptrs([np.ravel(a) for a in imgs])
+            sd[e] = seed
+        keep += [cal, sd]
+        seeds = sd.ctypes.data_as(C.POINTER(C.c_uint64))
+    nx, ny, nz = inp.acq_dims
+    n = nx * ny * nz * inp.n_volumes
+    mags = [np.zeros(n, np.float32) for _ in range(ne)]
+    phs = [np.zeros(n, np.float32) for _ in range(ne)]
+    mp = (abi.c_f32p * max(ne, 1))(*[m.ctypes.data_as(abi.c_f32p) for m in mags])
+    pp = (abi.c_f32p * max(ne, 1))(*[p.ctypes.data_as(abi.c_f32p) for p in phs])
+    check(lib().mrsim_simulate_acquisition_echoes(ctx.handle, C.byref(ci), ipe, C.byref(acq.to_c()),
+                                                  keep.f64(echo_times_ms), ne, cal, seeds, mp, pp))
+    return list(zip(mags, phs))
 
 
 # ---- the series forward/adjoint operator ----------------------------------------------------------

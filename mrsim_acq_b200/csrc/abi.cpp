@@ -2,12 +2,15 @@
 // Each converts C++ exceptions into a status code plus a thread-local message.
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 
 #include "driver.h"
 #include "host_tables.h"
 #include "mrsim_internal.h"
+#include "series.h"
 
 namespace {
 thread_local std::string g_last_error;
@@ -31,6 +34,18 @@ int guarded(F&& f) {
 
 void need(const void* p, const char* what) {
   if (!p) mrsim::fail(std::string(what) + " is NULL");
+}
+
+void check_slice_input(const mrsim_slice_input& inp, const mrsim_acquisition& acq) {
+  if (inp.sim[0] <= 0 || inp.sim[1] <= 0 || inp.acq_matrix[0] <= 0 || inp.acq_matrix[1] <= 0)
+    mrsim::fail("empty simulation grid or acquired matrix");
+  if (!(inp.sim[0] % inp.acq_matrix[0] == 0 && inp.sim[1] % inp.acq_matrix[1] == 0))
+    mrsim::fail("sim grid must be an integer multiple of the acquired matrix");
+  if (inp.ncomp > mrsim::kMaxComp) mrsim::fail("more than 8 compartments");
+  if (inp.ncomp > 0 && !inp.compartments) mrsim::fail("compartments is NULL");
+  if (!inp.t2 && inp.ncomp > 0) mrsim::fail("t2 is NULL");
+  if (!inp.fmap) mrsim::fail("fmap is NULL");
+  if (std::max<int64_t>(acq.n_coils, 1) > mrsim::kMaxCoils) mrsim::fail("more than 64 coils");
 }
 
 // Runs `f` on the context's device with the context locked.
@@ -175,10 +190,159 @@ int mrsim_build_coil_kspaces(mrsim_context* ctx, const mrsim_slice_input* inp, c
     need(out, "out");
     if (t_ms && !(trf_ms && tread_ms && polarity))
       mrsim::fail("line-timing table must have one entry per phase-encode line");
-    auto k = mrsim::slice_forward(ctx, *inp, *acq, t_ms, trf_ms, tread_ms, polarity, log_amp);
+    mrsim::LineTimingTab lt;
+    const int64_t ny = inp->acq_matrix[1];
+    if (t_ms) {
+      lt.t_ms.assign(t_ms, t_ms + ny);
+      lt.trf_ms.assign(trf_ms, trf_ms + ny);
+      lt.tread_ms.assign(tread_ms, tread_ms + ny);
+      lt.polarity.assign(polarity, polarity + ny);
+    }
+    check_slice_input(*inp, *acq);
+    auto k = mrsim::slice_forward2(ctx, *inp, *acq, t_ms ? &lt : nullptr, log_amp);
     for (size_t i = 0; i < k.size(); ++i) {
       out[2 * i] = (double)k[i].x;
       out[2 * i + 1] = (double)k[i].y;
+    }
+  });
+}
+
+int mrsim_simulate_slice(mrsim_context* ctx, const mrsim_slice_input* inp, const mrsim_acquisition* acq,
+                         float* out) {
+  return on_ctx(ctx, [&] {
+    need(inp, "inp");
+    need(acq, "acq");
+    need(out, "out");
+    check_slice_input(*inp, *acq);
+    mrsim::SliceOutputs so;
+    so.combined = (float2*)out;
+    mrsim::simulate_slice_full(ctx, *inp, *acq, so);
+  });
+}
+
+int mrsim_simulate_slice_full(mrsim_context* ctx, const mrsim_slice_input* inp, const mrsim_acquisition* acq,
+                              float* combined, float* acquired, float* reconstructed, float* coil_images,
+                              float* sensitivities, uint8_t* mask) {
+  return on_ctx(ctx, [&] {
+    need(inp, "inp");
+    need(acq, "acq");
+    need(combined, "combined");
+    check_slice_input(*inp, *acq);
+    mrsim::SliceOutputs so;
+    so.combined = (float2*)combined;
+    so.acquired = (float2*)acquired;
+    so.reconstructed = (float2*)reconstructed;
+    so.coil_images = (float2*)coil_images;
+    so.sensitivities = sensitivities;
+    so.mask = mask;
+    mrsim::simulate_slice_full(ctx, *inp, *acq, so);
+  });
+}
+
+int mrsim_simulate_slice_kspace(mrsim_context* ctx, const mrsim_slice_input* inp, const mrsim_acquisition* acq,
+                                double* out) {
+  return on_ctx(ctx, [&] {
+    need(inp, "inp");
+    need(acq, "acq");
+    need(out, "out");
+    check_slice_input(*inp, *acq);
+    auto k = mrsim::slice_forward2(ctx, *inp, *acq, nullptr, nullptr);
+    const size_t per = (size_t)inp->acq_matrix[0] * inp->acq_matrix[1];
+    for (size_t i = 0; i < per; ++i) {
+      out[2 * i] = (double)k[i].x;
+      out[2 * i + 1] = (double)k[i].y;
+    }
+  });
+}
+
+static void check_series_input(const mrsim_acquisition_input* in, const mrsim_acquisition* acq) {
+  need(in, "in");
+  need(acq, "acq");
+  if (in->ncomp > 0) {
+    need(in->images, "images");
+    need(in->t2, "t2");
+  }
+  need(in->phase, "phase");
+}
+
+int mrsim_simulate_acquisition_complex(mrsim_context* ctx, const mrsim_acquisition_input* in,
+                                       const mrsim_acquisition* acq, const mrsim_acquisition_options* opts,
+                                       mrsim_acquisition_output* out) {
+  return on_ctx(ctx, [&] {
+    check_series_input(in, acq);
+    need(out, "out");
+    need(out->re, "out->re");
+    need(out->im, "out->im");
+    mrsim::acquire_series(ctx, *in, *acq, opts, in->seed, in->seed, in->images, *out);
+  });
+}
+
+// magnitude and phase in f32 (`acquire_volumes`, kspace.rs:1827-1846)
+static void mag_phase(const std::vector<float>& re, const std::vector<float>& im, float* mag, float* ph) {
+  for (size_t i = 0; i < re.size(); ++i) {
+    const float r = re[i], m = im[i];
+    mag[i] = std::sqrt(r * r + m * m);
+    ph[i] = std::atan2(m, r);
+  }
+}
+
+int mrsim_simulate_acquisition_oversampled(mrsim_context* ctx, const mrsim_acquisition_input* in,
+                                           const mrsim_acquisition* acq, float* mag, float* phase) {
+  return on_ctx(ctx, [&] {
+    check_series_input(in, acq);
+    need(mag, "mag");
+    need(phase, "phase");
+    const size_t n = (size_t)in->acq_dims[0] * in->acq_dims[1] * in->acq_dims[2] * in->n_volumes;
+    std::vector<float> re(n), im(n);
+    mrsim_acquisition_output out;
+    std::memset(&out, 0, sizeof out);
+    out.re = re.data();
+    out.im = im.data();
+    mrsim::acquire_series(ctx, *in, *acq, nullptr, in->seed, in->seed, in->images, out);
+    mag_phase(re, im, mag, phase);
+  });
+}
+
+int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisition_input* in,
+                                      const float* const* const* images_per_echo, const mrsim_acquisition* acq,
+                                      const double* echo_times_ms, int64_t n_echoes,
+                                      const float* const* const* grappa_calibration_images,
+                                      const uint64_t* grappa_calibration_seeds, float* const* mag,
+                                      float* const* phase) {
+  return on_ctx(ctx, [&] {
+    check_series_input(in, acq);
+    need(images_per_echo, "images_per_echo");
+    need(echo_times_ms, "echo_times_ms");
+    need(mag, "mag");
+    need(phase, "phase");
+    // `simulate_acquisition_echoes` kspace.rs:2152-2215
+    for (int64_t e = 0; e + 1 < n_echoes; ++e)
+      if (!(echo_times_ms[e] < echo_times_ms[e + 1])) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf, "echo times must increase strictly: echo %lld at %g ms, echo %lld at %g ms",
+                      (long long)e, echo_times_ms[e], (long long)(e + 1), echo_times_ms[e + 1]);
+        mrsim::fail(buf);
+      }
+    if (n_echoes <= 0) mrsim::fail("simulate_acquisition_echoes needs at least one echo");
+    const size_t n = (size_t)in->acq_dims[0] * in->acq_dims[1] * in->acq_dims[2] * in->n_volumes;
+    std::vector<float> re(n), im(n);
+    for (int64_t e = 0; e < n_echoes; ++e) {
+      mrsim_acquisition acq_e = *acq;
+      acq_e.t_echo = echo_times_ms[e];
+      mrsim_acquisition_options opts;
+      std::memset(&opts, 0, sizeof opts);
+      if (grappa_calibration_images) {
+        opts.has_grappa_calibration = 1;
+        opts.grappa_calibration_images = grappa_calibration_images[e];
+        opts.grappa_calibration_seed = grappa_calibration_seeds ? grappa_calibration_seeds[e] : in->seed;
+      }
+      mrsim_acquisition_output out;
+      std::memset(&out, 0, sizeof out);
+      out.re = re.data();
+      out.im = im.data();
+      mrsim::acquire_series(ctx, *in, acq_e, &opts, in->seed, in->seed ^ mrsim::echo_salt((uint64_t)e),
+                            images_per_echo[e], out);
+      mag_phase(re, im, mag[e], phase[e]);
     }
   });
 }

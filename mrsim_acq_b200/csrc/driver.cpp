@@ -144,205 +144,6 @@ void append_lines(std::vector<LineRec>& out, const mrsim_acquisition& acq, const
   }
 }
 
-// ---- per-slice forward (`build_coil_kspace_timed` for every coil + spikes + noise) ---------
-std::vector<float2> slice_forward(mrsim_context* ctx, const mrsim_slice_input& inp, const mrsim_acquisition& acq,
-                                  const double* t_ms, const double* trf_ms, const double* tread_ms,
-                                  const int8_t* polarity, const double* log_amp) {
-  const int snx = (int)inp.sim[0], sny = (int)inp.sim[1], nx = (int)inp.acq_matrix[0], ny = (int)inp.acq_matrix[1];
-  if (snx <= 0 || sny <= 0 || nx <= 0 || ny <= 0) fail("empty simulation grid or acquired matrix");
-  if (!(snx % nx == 0 && sny % ny == 0)) fail("sim grid must be an integer multiple of the acquired matrix");
-  const int ncomp = (int)inp.ncomp;
-  if (ncomp > kMaxComp) fail("more than 8 compartments");
-  const int ncoils = (int)std::max<int64_t>(acq.n_coils, 1);
-  if (ncoils > kMaxCoils) fail("more than 64 coils");
-  const size_t plane = (size_t)snx * sny;
-  cudaStream_t st = ctx->stream;
-  DevArena A;
-
-  LineTimingTab lt;
-  if (t_ms) {
-    lt.t_ms.assign(t_ms, t_ms + ny);
-    lt.trf_ms.assign(trf_ms, trf_ms + ny);
-    lt.tread_ms.assign(tread_ms, tread_ms + ny);
-    lt.polarity.assign(polarity, polarity + ny);
-  } else {
-    lt = line_timing(acq, nx, ny);
-  }
-  bool uniform = log_amp == nullptr;
-  for (int c = 0; c < ncomp; ++c) uniform = uniform && !inp.t2[c].is_map;
-  if (inp.t_inhom)
-    for (int c = 0; c < ncomp; ++c) uniform = uniform && !inp.t_inhom[c].is_map;
-  const bool maps = !uniform && acq.do_relaxation;
-  const bool eddy = acq.eddy_strength != 0.0 && inp.has_eddy_drive;
-  const bool eddy_phase = acq.eddy_phase != 0.0 && inp.has_eddy_drive;
-  float t2u[kMaxComp], tiu[kMaxComp];
-  for (int c = 0; c < kMaxComp; ++c) {
-    t2u[c] = c < ncomp ? inp.t2[c].value : 1.f;
-    tiu[c] = c < ncomp ? (inp.t_inhom ? inp.t_inhom[c].value : (float)acq.t_inhom) : 1.f;
-  }
-  std::vector<LineRec> lines;
-  append_lines(lines, acq, lt, nx, ny, 0, eddy, uniform, ncomp, t2u, tiu);
-  if (ncomp > 0 && uniform && acq.do_relaxation && !inp.t_inhom) {
-    // `t_inhom: None` reads Acquisition::t_inhom as f64 — recompute rel at full precision
-    for (auto& L : lines)
-      for (int c = 0; c < ncomp; ++c) {
-        double t = lt.t_ms[L.ky] / 1000.0, trf = lt.trf_ms[L.ky];
-        double inh = acq.echo == MRSIM_ECHO_SPIN ? std::fabs(t) * 1000.0 : trf;
-        L.rel[c] = (float)std::exp(-trf / (double)t2u[c] - inh / acq.t_inhom);
-      }
-  }
-
-  // inputs
-  std::vector<float> comp(std::max<size_t>(1, (size_t)ncomp * plane));
-  for (int c = 0; c < ncomp; ++c) std::memcpy(&comp[(size_t)c * plane], inp.compartments[c], plane * 4);
-  float* d_comp = (float*)A.upload(comp.data(), comp.size() * 4, st);
-  float* d_fmap = (float*)A.upload(inp.fmap, plane * 4, st);
-  const double* d_phase0 = inp.phase0 ? (const double*)A.upload(inp.phase0, plane * 8, st) : nullptr;
-  float* d_t2 = nullptr;
-  float* d_ti = nullptr;
-  float* d_la = nullptr;
-  if (maps) {
-    bool any_t2 = false, any_ti = false;
-    for (int c = 0; c < ncomp; ++c) {
-      any_t2 = any_t2 || inp.t2[c].is_map;
-      any_ti = any_ti || (inp.t_inhom && inp.t_inhom[c].is_map);
-    }
-    if (any_t2) {
-      std::vector<float> m((size_t)ncomp * plane);
-      for (int c = 0; c < ncomp; ++c)
-        for (size_t i = 0; i < plane; ++i) m[(size_t)c * plane + i] = inp.t2[c].is_map ? inp.t2[c].map[i] : inp.t2[c].value;
-      d_t2 = (float*)A.upload(m.data(), m.size() * 4, st);
-    }
-    if (any_ti) {
-      std::vector<float> m((size_t)ncomp * plane);
-      for (int c = 0; c < ncomp; ++c)
-        for (size_t i = 0; i < plane; ++i)
-          m[(size_t)c * plane + i] = inp.t_inhom[c].is_map ? inp.t_inhom[c].map[i] : inp.t_inhom[c].value;
-      d_ti = (float*)A.upload(m.data(), m.size() * 4, st);
-    }
-    if (log_amp) {
-      std::vector<float> m(plane);
-      for (size_t i = 0; i < plane; ++i) m[i] = (float)log_amp[i];
-      d_la = (float*)A.upload(m.data(), m.size() * 4, st);
-    }
-  }
-  GeoTab geo = build_geo(A, snx, sny, nx, ny, ncoils, acq.ghost_offset, st);
-  const LineRec* d_lines = (const LineRec*)A.upload(lines.data(), std::max<size_t>(1, lines.size()) * sizeof(LineRec), st);
-  float* d_phase = (float*)A.alloc(plane * 4);
-  float2* d_g = (float2*)A.alloc(std::max<size_t>(1, (size_t)ncoils * lines.size() * snx) * sizeof(float2));
-  float2* d_k = (float2*)A.alloc((size_t)ncoils * nx * ny * sizeof(float2));
-  MRSIM_CUDA(cudaMemsetAsync(d_k, 0, (size_t)ncoils * nx * ny * sizeof(float2), st));
-
-  StaticDesc sd;
-  std::memset(&sd, 0, sizeof sd);
-  sd.snx = snx;
-  sd.sny = sny;
-  sd.nx = nx;
-  sd.ny = ny;
-  sd.o = snx / nx;
-  sd.z = (int)inp.z;
-  sd.nz_full = (int)inp.nz;
-  sd.flags = 1 | (eddy_phase ? 2 : 0);
-  sd.phase0 = d_phase0;
-  double grad[3] = {0, 0, 0};
-  if (inp.has_eddy_drive)
-    for (int i = 0; i < 3; ++i) grad[i] = inp.eddy_drive[i];
-  for (int i = 0; i < 3; ++i) sd.eddy_phase_coef[i] = acq.eddy_phase * grad[i];
-  sd.zc_c = (double)inp.z - ((double)inp.nz - 1.0) / 2.0;
-  sd.out = d_phase;
-  if (!d_phase0) {
-    // no explicit phase: zero phase model
-    sd.flags &= ~1;
-  }
-
-  UnitDesc u;
-  std::memset(&u, 0, sizeof u);
-  u.snx = snx;
-  u.sny = sny;
-  u.nx = nx;
-  u.ny = ny;
-  u.ncomp = ncomp;
-  u.ncoils = ncoils;
-  u.n_lines = (int)lines.size();
-  u.n_rows = ny;
-  u.flags = (acq.do_relaxation ? UF_RELAX : 0) | (maps ? UF_MAPS : 0) | (eddy ? UF_EDDY : 0) |
-            (acq.do_distortions ? UF_DISTORT : 0) | (acq.echo == MRSIM_ECHO_GRADIENT ? UF_GRADIENT : 0);
-  u.z = (int)inp.z;
-  u.nz = (int)inp.nz;
-  u.comp_stride = (long long)plane;
-  u.map_stride = (long long)plane;
-  u.comp = d_comp;
-  u.fmap = d_fmap;
-  u.phase = d_phase;
-  u.t2map = d_t2;
-  u.timap = d_ti;
-  u.log_amp = d_la;
-  u.lines = d_lines;
-  u.geo = geo;
-  u.signal_scale = (float)acq.signal_scale;
-  for (int c = 0; c < kMaxComp; ++c) {
-    u.t2u[c] = t2u[c];
-    u.tiu[c] = tiu[c];
-  }
-  if (eddy) {
-    const int zs = (int)inp.nz / 2;
-    const double zc = (double)inp.z - (double)zs;
-    u.eddy_cx = (float)(acq.eddy_strength * grad[0]);
-    u.eddy_qx = (float)(acq.eddy_quad * grad[0]);
-    u.eddy_cy = (float)(acq.eddy_strength * grad[1]);
-    u.eddy_qy = (float)(acq.eddy_quad * grad[1]);
-    u.eddy_z = (float)(acq.eddy_strength * grad[2] * zc + acq.eddy_quad * grad[2] * zc * zc);
-  }
-  u.kspace = d_k;
-  u.g = d_g;
-
-  std::unique_ptr<EpiPlan> plan(epi_plan_create(&u, 1, &sd, 1));
-  epi_plan_statics(plan.get(), st);
-  if (!lines.empty()) epi_plan_forward(plan.get(), st);
-
-  // spikes and noise per coil
-  const bool do_spikes = acq.n_spikes > 0;
-  const bool do_noise = acq.noise_variance > 0.0;
-  if ((do_spikes || do_noise) && !lines.empty()) {
-    std::vector<int> rows;
-    for (auto& L : lines) rows.push_back(L.ky);
-    std::vector<int> picks;
-    if (do_spikes) {
-      auto mask = sampling_mask(nx, ny, acq);
-      std::vector<int> acquired;
-      for (int i = 0; i < nx * ny; ++i)
-        if (mask[i]) acquired.push_back(i);
-      Rng rng(inp.slice_seed ^ 0xA5A5123456789ABCull);
-      for (int64_t s = 0; s < acq.n_spikes; ++s)
-        picks.push_back(acquired[(size_t)(rng.next_u64() % (uint64_t)acquired.size())]);
-    }
-    const int* d_rows = (const int*)A.upload(rows.data(), rows.size() * 4, st);
-    const int* d_picks = picks.empty() ? nullptr : (const int*)A.upload(picks.data(), picks.size() * 4, st);
-    std::vector<NoiseJob> jobs(ncoils);
-    for (int q = 0; q < ncoils; ++q) {
-      NoiseJob& J = jobs[q];
-      std::memset(&J, 0, sizeof J);
-      J.k = d_k + (size_t)q * nx * ny;
-      J.rows = d_rows;
-      J.picks = d_picks;
-      J.n_rows = (int)rows.size();
-      J.nx = nx;
-      J.n_picks = (int)picks.size();
-      J.seed = (inp.slice_seed ^ ((uint64_t)q * 0x9E3779B9ull)) | 1ull;
-      J.sigma = do_noise ? std::sqrt(acq.noise_variance / (double)((size_t)nx * ny)) : 0.0;
-      J.spike_amplitude = acq.spike_amplitude;
-    }
-    const NoiseJob* d_jobs = (const NoiseJob*)A.upload(jobs.data(), jobs.size() * sizeof(NoiseJob), st);
-    auto* d_keys = (unsigned long long*)A.alloc(sizeof(unsigned long long) * ncoils);
-    launch_noise_jobs(d_jobs, ncoils, do_spikes, do_noise, (int)rows.size() * nx, d_keys, st);
-    MRSIM_CUDA(cudaGetLastError());
-  }
-  std::vector<float2> out((size_t)ncoils * nx * ny);
-  MRSIM_CUDA(cudaMemcpyAsync(out.data(), d_k, out.size() * sizeof(float2), cudaMemcpyDeviceToHost, st));
-  MRSIM_CUDA(cudaStreamSynchronize(st));
-  return out;
-}
-
 // =============================================================================================
 // The batched forward/adjoint operator of a 2D EPI series.
 EpiOperator::~EpiOperator() {}

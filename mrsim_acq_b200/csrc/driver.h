@@ -23,12 +23,6 @@ struct DevArena {
 
 GeoTab build_geo(DevArena& arena, int snx, int sny, int nx, int ny, int ncoils, double ghost, cudaStream_t st);
 
-// `build_coil_kspace_timed` (kspace.rs:607-1042) for every coil of one slice, on the device;
-// returns n_coils*ny*nx complex samples (FP32) with spikes and noise.
-std::vector<float2> slice_forward(mrsim_context* ctx, const mrsim_slice_input& inp, const mrsim_acquisition& acq,
-                                  const double* t_ms, const double* trf_ms, const double* tread_ms,
-                                  const int8_t* polarity, const double* log_amp);
-
 // The forward/adjoint operator of a whole 2D EPI series: units (volume, slice) with every
 // echo's acquired lines.  Device layouts:
 //   images    [g][z][c][sny][snx]            fmap [z][sny][snx]

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include "driver.h"
+#include "series.h"
 
 namespace mrsim {
 
@@ -21,6 +22,46 @@ __global__ void series_transpose_kernel(const float* __restrict__ in, float* __r
     for (int g = 0; g < nv; ++g) out[(((size_t)g * nz + z) * ncomp + c) * plane + p] = src[g];
   }
 }
+__device__ __forceinline__ double unit_of(uint64_t seed, uint64_t k) {
+  uint64_t z = seed + (k + 1ull) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+// One thread per (volume, slice, y, x) of a chunk of volumes [g0, g1).
+__global__ void series_output_kernel(const float2* __restrict__ comb, const float* __restrict__ sigma,
+                                     float* __restrict__ re, float* __restrict__ im, int g0, int g1, int nv, int nz,
+                                     int nx, int ny, const int* __restrict__ zmap, uint64_t seed) {
+  const long long per = (long long)nx * ny;
+  const long long total = (long long)(g1 - g0) * nz * per;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int g = g0 + (int)(t / (nz * per));
+    const int zl = (int)((t / per) % nz);
+    const long long p = t % per;
+    const float2 c = comb[t];
+    float r = c.x, i = c.y;
+    const long long vox = p + per * zl;
+    if (sigma) {
+      const double sd = (double)sigma[vox];
+      if (sd > 0.0) {
+        const long long vox_g = p + per * zmap[zl];
+        const uint64_t s = (seed ^ ((uint64_t)g * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)vox_g * 0xBF58476D1CE4E5B9ull)) |
+                           1ull;
+        const double tau = 6.283185307179586;
+        const double n1 = sqrt(-2.0 * log(unit_of(s, 0))) * cos(tau * unit_of(s, 1));
+        const double n2 = sqrt(-2.0 * log(unit_of(s, 2))) * cos(tau * unit_of(s, 3));
+        r += (float)(n1 * sd);
+        i += (float)(n2 * sd);
+      }
+    }
+    re[vox * nv + g] = r;
+    im[vox * nv + g] = i;
+  }
+}
+
 // Independent FMA chains per thread, all operands in registers: the FP32 pipe's throughput.
 __global__ void __launch_bounds__(256) fma_probe_kernel(float* out, int iters, float a, float b) {
   float v[16];
@@ -59,6 +100,15 @@ double probe_fp32_tflops(cudaStream_t st) {
   cudaFree(out);
   const double flops = 5.0 * blocks * 256.0 * iters * 16.0 * 2.0;
   return flops / (ms * 1e-3) / 1e12;
+}
+
+void launch_series_output(const float2* combined, const float* sigma, float* re, float* im, int g0, int g1, int nv,
+                          int nz, int nx, int ny, const int* zmap, uint64_t receiver_seed, cudaStream_t st) {
+  const long long total = (long long)(g1 - g0) * nz * nx * ny;
+  if (total <= 0) return;
+  int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  series_output_kernel<<<blocks, 256, 0, st>>>(combined, sigma, re, im, g0, g1, nv, nz, nx, ny, zmap, receiver_seed);
+  MRSIM_CUDA(cudaGetLastError());
 }
 
 void launch_series_transpose(const float* staging, float* out, int ncomp, int nv, int nz, int plane, cudaStream_t st) {

@@ -165,3 +165,34 @@ def series_case(nx=16, ny=16, nz=2, o=2, nv=2, ncomp=3, seed=5, maps=False):
         t2 = [T2.of_map((60.0 + 40.0 * x).astype(np.float32))] + t2[1:]
     return dict(sim_dims=(snx, sny, nz), acq_dims=(nx, ny, nz), n_volumes=nv, images=imgs, t2=t2, t_inhom=ti,
                 fmap=fmap)
+
+
+def golden_series_inputs():
+    """The series cases of golden_baseline.rs:90-124: (name, AcquisitionInput, Acquisition)."""
+    from mrsim_acq_b200.api import AcquisitionInput, PhaseModel
+    nx, ny, nz, o, nv = 16, 16, 3, 2, 4
+    snx, sny = nx * o, ny * o
+    nsim = snx * sny * nz
+    rng = Rng(0xBA5E)
+    images = []
+    for c in range(2):
+        i = np.arange(nsim * nv)
+        v = i // nsim
+        vox = i % nsim
+        x = (vox % snx) / snx
+        y = ((vox // snx) % sny) / sny
+        blob = np.exp(-(((x - 0.5) * (x - 0.5) + (y - 0.5) * (y - 0.5)) / 0.05))
+        u = np.array([rng.unit() for _ in range(nsim * nv)])
+        by_volume = ((1.0 + 0.1 * c + 0.01 * v) * blob + 0.02 * u).astype(np.float32)
+        images.append(np.ascontiguousarray(by_volume.reshape(nv, nsim).T).reshape(-1))  # vox*nv + g
+    idx = np.arange(nsim)
+    fmap = (40.0 * ((idx % snx) / snx - 0.5)).astype(np.float32)
+    t2map = (50.0 + (idx % 7) * 10.0).astype(np.float32)
+    acq = Acquisition(n_coils=3, accel=2, acs_lines=6, noise_variance=2.0, signal_scale=100.0, t_echo=30.0, t_line=0.5)
+    out = []
+    for name, t2 in (("series-uniform", [T2.uniform(80.0), T2.uniform(160.0)]),
+                     ("series-mapped", [T2.of_map(t2map), T2.uniform(160.0)])):
+        inp = AcquisitionInput(sim_dims=(snx, sny, nz), acq_dims=(nx, ny, nz), n_volumes=nv, images=images, t2=t2,
+                               fmap=fmap, phase=PhaseModel.hbcd_like(), seed=42)
+        out.append((name, inp, acq))
+    return out
