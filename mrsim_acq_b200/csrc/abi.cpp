@@ -255,11 +255,12 @@ int mrsim_simulate_slice_kspace(mrsim_context* ctx, const mrsim_slice_input* inp
   });
 }
 
-static void check_series_input(const mrsim_acquisition_input* in, const mrsim_acquisition* acq) {
+static void check_series_input(const mrsim_acquisition_input* in, const mrsim_acquisition* acq,
+                               bool images = true) {
   need(in, "in");
   need(acq, "acq");
   if (in->ncomp > 0) {
-    need(in->images, "images");
+    if (images) need(in->images, "images");
     need(in->t2, "t2");
   }
   need(in->phase, "phase");
@@ -310,7 +311,7 @@ int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisitio
                                       const uint64_t* grappa_calibration_seeds, float* const* mag,
                                       float* const* phase) {
   return on_ctx(ctx, [&] {
-    check_series_input(in, acq);
+    check_series_input(in, acq, false);
     need(images_per_echo, "images_per_echo");
     need(echo_times_ms, "echo_times_ms");
     need(mag, "mag");

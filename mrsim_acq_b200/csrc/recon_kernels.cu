@@ -296,6 +296,7 @@ __global__ void __launch_bounds__(256) recon_combine_kernel(const ReconJob* __re
 
 __global__ void window_copy_kernel(const ReconJob* __restrict__ jobs) {
   const ReconJob& J = jobs[blockIdx.y];
+  if (!J.reconstructed) return;  // only the captured slices keep their reconstructed k-space
   const int n = J.nc * J.nx * J.ny;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     float2 v = J.k[e];

@@ -148,7 +148,7 @@ def test_progress_counts_every_volume(gpu_ctx):
 def test_invalid_inputs_fail_with_the_reference_messages(gpu_ctx):
     inp, acq = _series(nv=1, nz=1)
     with pytest.raises(MrsimError, match="trf = .* ms <= 0 on an acquired line"):
-        api.simulate_acquisition_complex(inp, acq.replace(t_echo=5.0), ctx=gpu_ctx)
+        api.simulate_acquisition_complex(inp, acq.replace(t_echo=1.0), ctx=gpu_ctx)
     bad = AcquisitionInput(**{**inp.__dict__, "t2": [T2.of_map(np.zeros(32 * 32, np.float32)), inp.t2[1]]})
     with pytest.raises(MrsimError, match="T2 map for compartment 0: T2 map value 0 at index 0 is not strictly positive"):
         api.simulate_acquisition_complex(bad, acq, ctx=gpu_ctx)
