@@ -248,7 +248,7 @@ int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisitio
  * `inp` is a host struct whose data pointers are DEVICE pointers: the compartment planes
  * contiguous (plane c at compartments[0] + c*snx*sny), fmap, and phase0 (f64) or NULL.  `stream`
  * is a cudaStream_t (NULL: the legacy default stream) of the current device; the call returns
- * when the output is complete.  Intermediates live in static device arrays of ~7.6 MiB held by
+ * when the output is complete.  Intermediates live in static device arrays of ~7.8 MiB held by
  * every GPU that loads the library until exit; limits: n_coils*acquired_lines*snx <= 524288,
  * snx*sny <= 262144, snx*nx <= 65536, n_coils*max(snx,sny) <= 32768, acquired lines <= 1024 —
  * larger inputs fail with MRSIM_ERR_INVALID.  The first call on a device looks up the arrays'

@@ -25,6 +25,9 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <cstring>
+#include <map>
+
 #include "mrsim_internal.h"
 
 namespace mrsim {
@@ -33,13 +36,18 @@ namespace {
 
 constexpr float kTwoPiF = 6.28318530717958647692f;
 
-__device__ __forceinline__ float frac_turn(float v) { return v - rintf(v); }
+// Round to the nearest integer on the FP32 pipe (|v| < 2^22): adding and subtracting 1.5*2^23
+// leaves v rounded to an integer; exact for the turn reductions below.
+__device__ __forceinline__ float round_fadd(float v) {
+  return __fadd_rn(__fadd_rn(v, 12582912.0f), -12582912.0f);
+}
+__device__ __forceinline__ float frac_turn(float v) { return __fadd_rn(v, -round_fadd(v)); }
 
 // Phase of voxel value f (Hz) at line time t = t_hi + t_lo (s), in turns, reduced.
 __device__ __forceinline__ float ft_turns(float f, float t_hi, float t_lo) {
   float p = f * t_hi;
   float e = fmaf(f, t_hi, -p);      // exact error of the product
-  float r = p - rintf(p);           // exact
+  float r = __fadd_rn(p, -round_fadd(p));  // exact
   return r + fmaf(f, t_lo, e);
 }
 
@@ -90,36 +98,39 @@ struct Tile {
 };
 
 template <int T, int QG, int NC, bool MAPS>
-__global__ void __launch_bounds__(128) ystage_kernel(const UnitDesc* __restrict__ units,
-                                                     const Tile* __restrict__ tiles) {
-  extern __shared__ float smem[];
+__global__ void __launch_bounds__(128, 4) ystage_kernel(const UnitDesc* __restrict__ units,
+                                                        const Tile* __restrict__ tiles) {
+  // A CTA of 128 threads: one column each, T lines x QG coils per thread.
+  constexpr int LG = 1;
+  constexpr int TL = LG * T;  // lines per CTA
+  static_assert(T == 4, "the phase table is read as float4");
+  extern __shared__ __align__(16) float smem[];
   const Tile tl = tiles[blockIdx.x];
   const UnitDesc& u = units[tl.unit];
   const int snx = u.snx, sny = u.sny;
   const int ncomp = u.ncomp;
-  float* Bt = smem;                 // [sny][T] phase terms per (row, line)
-  float* Ey = smem + sny * T;       // [QG][sny]
-  __shared__ float rel_s[T][kMaxComp];
-  __shared__ float tinh_s[T], trf_s[T];
-  __shared__ float thi_s[T], tlo_s[T];
+  float* Bt = smem;                 // [sny][TL] phase terms per (row, line)
+  float* Ey = smem + sny * TL;      // [sny][QGP] (QGP = QG rounded up to 4)
+  constexpr int QGP = (QG + 3) / 4 * 4;
+  __shared__ float rel_s[TL][kMaxComp];
+  __shared__ float tinh_s[TL], trf_s[TL];
+  __shared__ float thi_s[TL], tlo_s[TL];
 
-  const int nl = min(T, u.n_lines - tl.line0);
+  const int nl = min(TL, u.n_lines - tl.line0);
   const int ys = u.ny / 2;
   const int oy = sny / u.ny;
   const int sys = oy * ys;
-  // per-CTA tables
-  for (int idx = threadIdx.x; idx < sny * T; idx += blockDim.x) {
-    int y = idx / T, j = idx % T;
+  for (int idx = threadIdx.x; idx < sny * TL; idx += blockDim.x) {
+    const int y = idx / TL, j = idx % TL;
     float v = 0.f;
     if (j < nl) {
       const LineRec& L = u.lines[tl.line0 + j];
-      long long K = L.ky - ys;
-      long long Y = 2LL * (y - sys) - (oy - 1);
-      long long m2 = 2LL * sny;
-      long long r = (K * Y) % m2;
-      double tv = (double)r / (double)m2;
+      const long long K = L.ky - ys;
+      const long long Y = 2LL * (y - sys) - (oy - 1);
+      const long long m2 = 2LL * sny;
+      double tv = (double)((K * Y) % m2) / (double)m2;
       if (u.flags & UF_EDDY) {
-        double yc = ((double)y - sys - (oy - 1) / 2.0) / oy;
+        const double yc = ((double)y - sys - (oy - 1) / 2.0) / oy;
         tv += ((double)u.eddy_cy * yc + (double)u.eddy_qy * yc * yc) * (double)L.decay;
       }
       tv -= rint(tv);
@@ -127,13 +138,13 @@ __global__ void __launch_bounds__(128) ystage_kernel(const UnitDesc* __restrict_
     }
     Bt[idx] = v;
   }
-  for (int idx = threadIdx.x; idx < QG * sny; idx += blockDim.x) {
-    int qq = idx / sny, y = idx % sny;
-    int q = tl.q0 + qq;
-    Ey[idx] = q < u.ncoils ? u.geo.ey[(size_t)q * sny + y] : 0.f;
+  for (int idx = threadIdx.x; idx < QGP * sny; idx += blockDim.x) {
+    const int y = idx / QGP, qq = idx % QGP;
+    const int q = tl.q0 + qq;
+    Ey[idx] = (qq < QG && q < u.ncoils) ? u.geo.ey[(size_t)q * sny + y] : 0.f;
   }
-  if (threadIdx.x < T) {
-    int j = threadIdx.x;
+  if (threadIdx.x < TL) {
+    const int j = threadIdx.x;
     if (j < nl) {
       const LineRec& L = u.lines[tl.line0 + j];
       thi_s[j] = L.t_hi;
@@ -148,21 +159,25 @@ __global__ void __launch_bounds__(128) ystage_kernel(const UnitDesc* __restrict_
   }
   __syncthreads();
 
-  const int x = tl.x0 + threadIdx.x;
+  const int col = threadIdx.x & 127, lg = threadIdx.x >> 7;
+  const int jb = lg * T;  // this thread's first line within the CTA
+  const int x = tl.x0 + col;
   const bool xok = x < snx;
   const int xs_ = xok ? x : 0;
   float exq[QG];
   const float off = u.geo.coil_off;
 #pragma unroll
   for (int qq = 0; qq < QG; ++qq) {
-    int q = tl.q0 + qq;
+    const int q = tl.q0 + qq;
     exq[qq] = (xok && q < u.ncoils) ? u.geo.ex[(size_t)q * snx + x] : 0.f;
   }
-  float thi[T], tlo[T];
+  float thi[T], tlo[T], relr[T][NC];
 #pragma unroll
   for (int j = 0; j < T; ++j) {
-    thi[j] = thi_s[j];
-    tlo[j] = tlo_s[j];
+    thi[j] = thi_s[jb + j];
+    tlo[j] = tlo_s[jb + j];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) relr[j][c] = rel_s[jb + j][c];
   }
   float2 acc[T][QG];
 #pragma unroll
@@ -174,35 +189,57 @@ __global__ void __launch_bounds__(128) ystage_kernel(const UnitDesc* __restrict_
   const float* __restrict__ comp = u.comp;
   const float* __restrict__ fmap = u.fmap;
   const float* __restrict__ phase = u.phase;
+  // row y's inputs, prefetched one row ahead
+  float na = 0.f, nf = 0.f, nm[NC];
+  {
+    const int i = xs_;
+    na = phase ? __ldg(phase + i) : 0.f;
+    nf = distort ? __ldg(fmap + i) : 0.f;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) nm[c] = c < ncomp ? __ldg(comp + (size_t)c * u.comp_stride + i) : 0.f;
+  }
   for (int y = 0; y < sny; ++y) {
     const int i = xs_ + snx * y;
-    const float a = phase ? __ldg(phase + i) : 0.f;
-    const float f = distort ? __ldg(fmap + i) : 0.f;
+    const float a = na, f = nf;
     float m[NC];
-    float r2[NC], r2i[NC];
-    float la = 0.f;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      m[c] = 0.f;
-      r2[c] = 0.f;
-      r2i[c] = 0.f;
-      if (c < ncomp) {
-        m[c] = __ldg(comp + (size_t)c * u.comp_stride + i);
-        if (MAPS) {
-          float t2 = u.t2map ? __ldg(u.t2map + (size_t)c * u.map_stride + i) : u.t2u[c];
-          float ti = u.timap ? __ldg(u.timap + (size_t)c * u.map_stride + i) : u.tiu[c];
-          r2[c] = 1.0f / t2;
-          r2i[c] = 1.0f / ti;
+    for (int c = 0; c < NC; ++c) m[c] = nm[c];
+    if (y + 1 < sny) {
+      const int i1 = i + snx;
+      na = phase ? __ldg(phase + i1) : 0.f;
+      nf = distort ? __ldg(fmap + i1) : 0.f;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) nm[c] = c < ncomp ? __ldg(comp + (size_t)c * u.comp_stride + i1) : 0.f;
+    }
+    float r2[MAPS ? NC : 1], r2i[MAPS ? NC : 1];
+    float la = 0.f;
+    if (MAPS) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        r2[MAPS ? c : 0] = r2i[MAPS ? c : 0] = 0.f;
+        if (c < ncomp) {
+          const float t2 = u.t2map ? __ldg(u.t2map + (size_t)c * u.map_stride + i) : u.t2u[c];
+          const float ti = u.timap ? __ldg(u.timap + (size_t)c * u.map_stride + i) : u.tiu[c];
+          r2[MAPS ? c : 0] = 1.0f / t2;
+          r2i[MAPS ? c : 0] = 1.0f / ti;
         }
       }
+      if (u.log_amp) la = __ldg(u.log_amp + i);
     }
-    if (MAPS && u.log_amp) la = __ldg(u.log_amp + i);
     float amp[QG];
 #pragma unroll
-    for (int qq = 0; qq < QG; ++qq) amp[qq] = fmaf(exq[qq], Ey[qq * sny + y], off);
+    for (int q4 = 0; q4 < QGP; q4 += 4) {
+      const float4 e4 = *reinterpret_cast<const float4*>(Ey + y * QGP + q4);
+      const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (q4 + k < QG) amp[q4 + k] = fmaf(exq[q4 + k], ev[k], off);
+    }
+    const float4 b4 = *reinterpret_cast<const float4*>(Bt + y * TL + jb);
+    const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
     for (int j = 0; j < T; ++j) {
-      float th = a + Bt[y * T + j] + ft_turns(f, thi[j], tlo[j]);
+      float th = a + bt[j] + ft_turns(f, thi[j], tlo[j]);
       th = frac_turn(th);
       float sn, cs;
       __sincosf(kTwoPiF * th, &sn, &cs);
@@ -212,9 +249,9 @@ __global__ void __launch_bounds__(128) ystage_kernel(const UnitDesc* __restrict_
         if (c < ncomp) {
           float r;
           if (MAPS)
-            r = __expf(la - trf_s[j] * r2[c] - tinh_s[j] * r2i[c]);
+            r = __expf(la - trf_s[jb + j] * r2[MAPS ? c : 0] - tinh_s[jb + j] * r2i[MAPS ? c : 0]);
           else
-            r = rel_s[j][c];
+            r = relr[j][c];
           W = fmaf(r, m[c], W);
         }
       }
@@ -230,176 +267,86 @@ __global__ void __launch_bounds__(128) ystage_kernel(const UnitDesc* __restrict_
   const float s = u.signal_scale;
 #pragma unroll
   for (int qq = 0; qq < QG; ++qq) {
-    int q = tl.q0 + qq;
+    const int q = tl.q0 + qq;
     if (q >= u.ncoils) break;
 #pragma unroll
     for (int j = 0; j < T; ++j) {
-      if (j < nl) {
-        float2 v = make_float2(acc[j][qq].x * s, acc[j][qq].y * s);
-        u.g[((size_t)q * u.n_lines + tl.line0 + j) * snx + x] = v;
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------------------------
-// x-stage: k[q][row][kx] = (1/nvox) sum_x g[q][j][x] E_j(x) tw_pol(kx,x), for 8 lines per CTA.
-constexpr int XR = 8;
-
-__global__ void __launch_bounds__(128) xstage_kernel(const UnitDesc* __restrict__ units,
-                                                     const int4* __restrict__ tiles) {
-  extern __shared__ float2 gs[];  // [XR][snx]
-  const int4 tl = tiles[blockIdx.x];  // unit, q, line0
-  const UnitDesc& u = units[tl.x];
-  const int snx = u.snx, nx = u.nx, q = tl.y, line0 = tl.z;
-  const int nl = min(XR, u.n_lines - line0);
-  const int ox = snx / nx, sxs = ox * (nx / 2);
-  const float xoff = (ox - 1.0f) / 2.0f;
-  for (int idx = threadIdx.x; idx < XR * snx; idx += blockDim.x) {
-    int j = idx / snx, x = idx % snx;
-    float2 v = make_float2(0.f, 0.f);
-    if (j < nl) {
-      v = u.g[((size_t)q * u.n_lines + line0 + j) * snx + x];
-      if (u.flags & UF_EDDY) {
-        const LineRec& L = u.lines[line0 + j];
-        double xc = ((double)x - sxs - xoff) / ox;
-        double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)L.decay;
-        tv -= rint(tv);
-        float sn, cs;
-        __sincosf(kTwoPiF * (float)tv, &sn, &cs);
-        v = make_float2(v.x * cs - v.y * sn, v.x * sn + v.y * cs);
-      }
-    }
-    gs[idx] = v;
-  }
-  __shared__ int pol_s[XR];
-  __shared__ int row_s[XR];
-  if (threadIdx.x < XR) {
-    int j = threadIdx.x;
-    pol_s[j] = j < nl ? (u.lines[line0 + j].pol < 0 ? 1 : 0) : 0;
-    row_s[j] = j < nl ? u.lines[line0 + j].row : 0;
-  }
-  __syncthreads();
-  const float inv_n = 1.0f / (float)(snx * u.sny);
-  const float2* tw0 = u.geo.tw;
-  const float2* tw1 = u.geo.tw + (size_t)snx * nx;
-  for (int kx = threadIdx.x; kx < nx; kx += blockDim.x) {
-    float2 acc[XR];
-#pragma unroll
-    for (int j = 0; j < XR; ++j) acc[j] = make_float2(0.f, 0.f);
-    for (int x = 0; x < snx; ++x) {
-      const float2 a0 = __ldg(tw0 + (size_t)x * nx + kx);
-      const float2 a1 = __ldg(tw1 + (size_t)x * nx + kx);
-#pragma unroll
-      for (int j = 0; j < XR; ++j) {
-        const float2 t = pol_s[j] ? a1 : a0;
-        const float2 gv = gs[j * snx + x];
-        acc[j].x = fmaf(gv.x, t.x, fmaf(-gv.y, t.y, acc[j].x));
-        acc[j].y = fmaf(gv.x, t.y, fmaf(gv.y, t.x, acc[j].y));
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < XR; ++j)
-      if (j < nl)
-        u.kspace[((size_t)q * u.n_rows + row_s[j]) * nx + kx] = make_float2(acc[j].x * inv_n, acc[j].y * inv_n);
-  }
-}
-
-// ---------------------------------------------------------------------------------------------
-// x-adjoint: h[q][j][x] = (1/nvox) conj(E_j(x)) sum_kx conj(tw_pol(kx,x)) r[q][row_j][kx].
-__global__ void __launch_bounds__(128) xadjoint_kernel(const UnitDesc* __restrict__ units,
-                                                       const int4* __restrict__ tiles) {
-  extern __shared__ float2 rs[];  // [XR][nx]
-  const int4 tl = tiles[blockIdx.x];
-  const UnitDesc& u = units[tl.x];
-  const int snx = u.snx, nx = u.nx, q = tl.y, line0 = tl.z;
-  const int nl = min(XR, u.n_lines - line0);
-  const int ox = snx / nx, sxs = ox * (nx / 2);
-  const float xoff = (ox - 1.0f) / 2.0f;
-  __shared__ int pol_s[XR];
-  __shared__ float dec_s[XR];
-  if (threadIdx.x < XR) {
-    int j = threadIdx.x;
-    pol_s[j] = j < nl ? (u.lines[line0 + j].pol < 0 ? 1 : 0) : 0;
-    dec_s[j] = j < nl ? u.lines[line0 + j].decay : 0.f;
-  }
-  for (int idx = threadIdx.x; idx < XR * nx; idx += blockDim.x) {
-    int j = idx / nx, kx = idx % nx;
-    float2 v = make_float2(0.f, 0.f);
-    if (j < nl) v = u.kspace[((size_t)q * u.n_rows + u.lines[line0 + j].row) * nx + kx];
-    rs[idx] = v;
-  }
-  __syncthreads();
-  const float inv_n = 1.0f / (float)(snx * u.sny);
-  // transposed twiddles follow the forward tables: [pol][kx][x]
-  const float2* tt0 = u.geo.tw + (size_t)2 * snx * nx;
-  const float2* tt1 = tt0 + (size_t)snx * nx;
-  for (int x = threadIdx.x; x < snx; x += blockDim.x) {
-    float2 acc[XR];
-#pragma unroll
-    for (int j = 0; j < XR; ++j) acc[j] = make_float2(0.f, 0.f);
-    for (int kx = 0; kx < nx; ++kx) {
-      const float2 a0 = __ldg(tt0 + (size_t)kx * snx + x);
-      const float2 a1 = __ldg(tt1 + (size_t)kx * snx + x);
-#pragma unroll
-      for (int j = 0; j < XR; ++j) {
-        const float2 t = pol_s[j] ? a1 : a0;
-        const float2 r = rs[j * nx + kx];
-        // conj(t) * r
-        acc[j].x = fmaf(t.x, r.x, fmaf(t.y, r.y, acc[j].x));
-        acc[j].y = fmaf(t.x, r.y, fmaf(-t.y, r.x, acc[j].y));
-      }
-    }
-    double xc = ((double)x - sxs - xoff) / ox;
-#pragma unroll
-    for (int j = 0; j < XR; ++j) {
-      if (j >= nl) continue;
-      float2 v = make_float2(acc[j].x * inv_n, acc[j].y * inv_n);
-      if (u.flags & UF_EDDY) {
-        double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)dec_s[j];
-        tv -= rint(tv);
-        float sn, cs;
-        __sincosf(kTwoPiF * (float)tv, &sn, &cs);
-        // multiply by conj(E) = (cs, -sn)
-        v = make_float2(v.x * cs + v.y * sn, v.y * cs - v.x * sn);
-      }
-      u.g[((size_t)q * u.n_lines + line0 + j) * snx + x] = v;
+      if (jb + j < nl)
+        u.g[((size_t)q * u.n_lines + tl.line0 + jb + j) * snx + x] = make_float2(acc[j][qq].x * s, acc[j][qq].y * s);
     }
   }
 }
 
 // ---------------------------------------------------------------------------------------------
 // y-adjoint: per voxel, over every line j and coil q:
-//   H_j = s * sum_q amp_q h_q[j][x];  Z_j = conj(e^{i2pi theta_j}) H_j
-//   comp_grad_c = sum_j rel_cj Z_j            (A^H r, complex)
-//   fmap_grad   = -4 pi Im( sum_c m_c conj(sum_j t_j rel_cj Z_j) )      (dL/df, Hz)
-//   r2_grad_c   = -2 Re( m_c conj(sum_j trf_j rel_cj Z_j) )             (dL/dR2_c, ms)
-// One thread per column x and TY consecutive rows.
+//   H_j = s * sum_q (ex_q ey_q + off) h_q[j][x];   Z_j = conj(e^{i2pi theta_j}) H_j
+//   comp_grad_c = sum_j rel_cj Z_j                          (A^H r, complex)
+//   fmap_grad   = 4 pi sum_c m_c Im(sum_j t_j rel_cj Z_j)   (dL/dfmap, L = sum |r|^2)
+//   r2_grad_c   = -2 m_c Re(sum_j trf_j rel_cj Z_j)         (dL/dR2_c)
+// A CTA of 128 threads covers 128 columns x TY rows (one column each).  The line table sits in
+// shared memory; h arrives by cp.async in double-buffered chunks of JC lines x every coil.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// The number of lines per h chunk for `ncoils` coils (16 coil-lines per chunk, at least one line).
+__host__ __device__ __forceinline__ int adjoint_chunk_lines(int ncoils) { return ncoils >= 16 ? 1 : 16 / ncoils; }
+
 template <int TY, int NC, bool MAPS, bool GRADS>
 __global__ void __launch_bounds__(128) yadjoint_kernel(const UnitDesc* __restrict__ units,
                                                        const int4* __restrict__ tiles) {
-  extern __shared__ float smem[];
+  extern __shared__ __align__(16) float smem[];
+  static_assert(TY == 4, "the row tables are read as float4");
+  constexpr int ROWS = TY;
   const int4 tl = tiles[blockIdx.x];  // unit, y0, x0
   const UnitDesc& u = units[tl.x];
   const int snx = u.snx, sny = u.sny, ncomp = u.ncomp, nlines = u.n_lines, ncoils = u.ncoils;
   const int y0 = tl.y;
-  float* Bt = smem;                      // [nlines][TY]
-  float* Ey = smem + nlines * TY;        // [ncoils][TY]
+  const int JC = adjoint_chunk_lines(ncoils);
+  // shared layout: h buffers (2 x JC x ncoils x 128 float2), then floats
+  float2* hbuf = reinterpret_cast<float2*>(smem);
+  float* Bt = reinterpret_cast<float*>(hbuf + 2 * JC * ncoils * 128);  // [nlines][ROWS]
+  float* Ey = Bt + nlines * ROWS;                                        // [ncoils][ROWS]
+  float* Ex = Ey + ncoils * ROWS;                                        // [ncoils][128], scale folded
+  float* Lt = Ex + ncoils * 128;                                         // [nlines][LF] line table
+  constexpr int LF = 5 + NC;  // t_hi, t_lo, trf, inhom, t_phase, rel[NC]
   const int ys = u.ny / 2;
   const int oy = sny / u.ny;
   const int sys = oy * ys;
-  for (int idx = threadIdx.x; idx < nlines * TY; idx += blockDim.x) {
-    int j = idx / TY, ty = idx % TY;
-    int y = y0 + ty;
+  const int col = threadIdx.x;
+  const int x = tl.z + col;
+  const bool xok = x < snx;
+  const float2* __restrict__ hcol = u.g + (xok ? x : 0);
+  const size_t qstride = (size_t)nlines * snx;
+  // the first h chunk is in flight while the tables fill
+  auto issue_chunk = [&](int c, int buf) {
+    const int j0 = c * JC;
+    for (int jj = 0; jj < JC; ++jj) {
+      const int j = j0 + jj;
+      if (j >= nlines) break;
+      for (int q = 0; q < ncoils; ++q)
+        cp_async8(hbuf + ((size_t)(buf * JC + jj) * ncoils + q) * 128 + col, hcol + q * qstride + (size_t)j * snx);
+    }
+    cp_async_commit();
+  };
+  const int nchunks = (nlines + JC - 1) / JC;
+  if (nchunks > 0) issue_chunk(0, 0);
+  for (int idx = threadIdx.x; idx < nlines * ROWS; idx += blockDim.x) {
+    const int j = idx / ROWS, r = idx % ROWS;
+    const int y = y0 + r;
     float v = 0.f;
     if (y < sny) {
       const LineRec& L = u.lines[j];
-      long long K = L.ky - ys;
-      long long Y = 2LL * (y - sys) - (oy - 1);
-      long long m2 = 2LL * sny;
+      const long long K = L.ky - ys;
+      const long long Y = 2LL * (y - sys) - (oy - 1);
+      const long long m2 = 2LL * sny;
       double tv = (double)((K * Y) % m2) / (double)m2;
       if (u.flags & UF_EDDY) {
-        double yc = ((double)y - sys - (oy - 1) / 2.0) / oy;
+        const double yc = ((double)y - sys - (oy - 1) / 2.0) / oy;
         tv += ((double)u.eddy_cy * yc + (double)u.eddy_qy * yc * yc) * (double)L.decay;
       }
       tv -= rint(tv);
@@ -407,116 +354,266 @@ __global__ void __launch_bounds__(128) yadjoint_kernel(const UnitDesc* __restric
     }
     Bt[idx] = v;
   }
-  for (int idx = threadIdx.x; idx < ncoils * TY; idx += blockDim.x) {
-    int q = idx / TY, ty = idx % TY;
-    int y = y0 + ty;
+  for (int idx = threadIdx.x; idx < ncoils * ROWS; idx += blockDim.x) {
+    const int q = idx / ROWS, r = idx % ROWS;
+    const int y = y0 + r;
     Ey[idx] = y < sny ? u.geo.ey[(size_t)q * sny + y] : 0.f;
   }
+  for (int idx = threadIdx.x; idx < ncoils * 128; idx += blockDim.x) {
+    const int q = idx / 128, c = idx % 128;
+    const int xx = tl.z + c;
+    Ex[idx] = xx < snx ? u.signal_scale * u.geo.ex[(size_t)q * snx + xx] : 0.f;
+  }
+  for (int j = threadIdx.x; j < nlines; j += blockDim.x) {
+    const LineRec& L = u.lines[j];
+    float* e = Lt + j * LF;
+    e[0] = L.t_hi;
+    e[1] = L.t_lo;
+    e[2] = L.trf_ms;
+    e[3] = L.inhom_ms;
+    e[4] = L.t_hi + L.t_lo;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) e[5 + c] = L.rel[c];
+  }
   __syncthreads();
-  const int x = tl.z + threadIdx.x;
-  if (x >= snx) return;
+  const bool active = xok && y0 < sny;
   const bool distort = (u.flags & UF_DISTORT) != 0;
-  float a[TY], f[TY], m[TY][NC], r2[TY][NC], r2i[TY][NC], la[TY];
+  float a[TY], f[TY], r2[TY][MAPS ? NC : 1], r2i[TY][MAPS ? NC : 1], la[TY];
 #pragma unroll
   for (int ty = 0; ty < TY; ++ty) {
-    int y = min(y0 + ty, sny - 1);
-    int i = x + snx * y;
-    a[ty] = u.phase ? u.phase[i] : 0.f;
-    f[ty] = distort ? u.fmap[i] : 0.f;
-    la[ty] = (MAPS && u.log_amp) ? u.log_amp[i] : 0.f;
+    const int y = min(y0 + ty, sny - 1);
+    const int i = (xok ? x : 0) + snx * y;
+    a[ty] = u.phase ? __ldg(u.phase + i) : 0.f;
+    f[ty] = distort ? __ldg(u.fmap + i) : 0.f;
+    la[ty] = (MAPS && u.log_amp) ? __ldg(u.log_amp + i) : 0.f;
+    if (MAPS) {
 #pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      m[ty][c] = (GRADS && c < ncomp) ? u.comp[(size_t)c * u.comp_stride + i] : 0.f;
-      r2[ty][c] = r2i[ty][c] = 0.f;
-      if (MAPS && c < ncomp) {
-        float t2 = u.t2map ? u.t2map[(size_t)c * u.map_stride + i] : u.t2u[c];
-        float ti = u.timap ? u.timap[(size_t)c * u.map_stride + i] : u.tiu[c];
-        r2[ty][c] = 1.0f / t2;
-        r2i[ty][c] = 1.0f / ti;
+      for (int c = 0; c < NC; ++c) {
+        r2[ty][MAPS ? c : 0] = r2i[ty][MAPS ? c : 0] = 0.f;
+        if (c < ncomp) {
+          const float t2 = u.t2map ? __ldg(u.t2map + (size_t)c * u.map_stride + i) : u.t2u[c];
+          const float ti = u.timap ? __ldg(u.timap + (size_t)c * u.map_stride + i) : u.tiu[c];
+          r2[ty][MAPS ? c : 0] = 1.0f / t2;
+          r2i[ty][MAPS ? c : 0] = 1.0f / ti;
+        }
       }
     }
   }
-  float2 cg[TY][NC], U[TY][GRADS ? NC : 1], V[TY][GRADS ? NC : 1];
+  float2 cg[TY][NC];
+  float Uy[TY][GRADS ? NC : 1], Vx[TY][GRADS ? NC : 1];
 #pragma unroll
   for (int ty = 0; ty < TY; ++ty)
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       cg[ty][c] = make_float2(0.f, 0.f);
-      if (GRADS) U[ty][GRADS ? c : 0] = V[ty][GRADS ? c : 0] = make_float2(0.f, 0.f);
+      if (GRADS) Uy[ty][GRADS ? c : 0] = Vx[ty][GRADS ? c : 0] = 0.f;
     }
-  const float off = u.geo.coil_off;
-  const float s = u.signal_scale;
-  for (int j = 0; j < nlines; ++j) {
-    const LineRec& L = u.lines[j];
-    const float thi = L.t_hi, tlo = L.t_lo, trf = L.trf_ms, tinh = L.inhom_ms;
-    const float tph = L.t_hi + L.t_lo;
-    float rel[NC];
+  const float soff = u.signal_scale * u.geo.coil_off;
+  for (int c = 0; c < nchunks; ++c) {
+    const int buf = c & 1;
+    if (c + 1 < nchunks) {
+      issue_chunk(c + 1, buf ^ 1);
+      cp_async_wait1();
+    } else {
+      cp_async_wait0();
+    }
+    // each thread reads back only its own column, which it copied itself: no barrier needed
+    const int j0 = c * JC;
+    const int jn = min(JC, nlines - j0);
+    for (int jj = 0; jj < jn; ++jj) {
+      const int j = j0 + jj;
+      const float* e = Lt + j * LF;
+      const float thi = e[0], tlo = e[1], trf = e[2], tinh = e[3], tph = e[4];
+      float2 H[TY];
+      float hsr = 0.f, hsi = 0.f;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) rel[c] = L.rel[c];
-    float2 H[TY];
+      for (int ty = 0; ty < TY; ++ty) H[ty] = make_float2(0.f, 0.f);
+      const float2* hb = hbuf + (size_t)(buf * JC + jj) * ncoils * 128 + col;
+#pragma unroll 4
+      for (int q = 0; q < ncoils; ++q) {
+        const float2 h = hb[q * 128];
+        const float ex = Ex[q * 128 + col];
+        hsr += h.x;
+        hsi += h.y;
+        const float ur = ex * h.x, ui = ex * h.y;
+        const float4 e4 = *reinterpret_cast<const float4*>(Ey + q * ROWS);
+        const float ey[4] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
-    for (int ty = 0; ty < TY; ++ty) H[ty] = make_float2(0.f, 0.f);
-    const float2* hp = u.g + (size_t)j * snx + x;
-    for (int q = 0; q < ncoils; ++q) {
-      const float2 h = __ldg(hp + (size_t)q * nlines * snx);
-      const float exq = __ldg(u.geo.ex + (size_t)q * snx + x);
+        for (int ty = 0; ty < TY; ++ty) {
+          H[ty].x = fmaf(ey[ty], ur, H[ty].x);
+          H[ty].y = fmaf(ey[ty], ui, H[ty].y);
+        }
+      }
+      const float4 b4 = *reinterpret_cast<const float4*>(Bt + j * ROWS);
+      const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
       for (int ty = 0; ty < TY; ++ty) {
-        float amp = fmaf(exq, Ey[q * TY + ty], off);
-        H[ty].x = fmaf(amp, h.x, H[ty].x);
-        H[ty].y = fmaf(amp, h.y, H[ty].y);
-      }
-    }
+        const float hr = fmaf(soff, hsr, H[ty].x), hi = fmaf(soff, hsi, H[ty].y);
+        float th = a[ty] + bt[ty] + ft_turns(f[ty], thi, tlo);
+        th = frac_turn(th);
+        float sn, cs;
+        __sincosf(kTwoPiF * th, &sn, &cs);
+        const float zr = fmaf(cs, hr, sn * hi);  // Z = conj(P) * H
+        const float zi = fmaf(cs, hi, -sn * hr);
 #pragma unroll
-    for (int ty = 0; ty < TY; ++ty) {
-      float th = a[ty] + Bt[j * TY + ty] + ft_turns(f[ty], thi, tlo);
-      th = frac_turn(th);
-      float sn, cs;
-      __sincosf(kTwoPiF * th, &sn, &cs);
-      // Z = conj(P) * H * s
-      const float zr = s * (cs * H[ty].x + sn * H[ty].y);
-      const float zi = s * (cs * H[ty].y - sn * H[ty].x);
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        if (c < ncomp) {
-          float r;
-          if (MAPS)
-            r = __expf(la[ty] - trf * r2[ty][c] - tinh * r2i[ty][c]);
-          else
-            r = rel[c];
-          cg[ty][c].x = fmaf(r, zr, cg[ty][c].x);
-          cg[ty][c].y = fmaf(r, zi, cg[ty][c].y);
-          if (GRADS) {
-            const int cc = GRADS ? c : 0;
-            float rt = r * tph, rr = r * trf;
-            U[ty][cc].x = fmaf(rt, zr, U[ty][cc].x);
-            U[ty][cc].y = fmaf(rt, zi, U[ty][cc].y);
-            V[ty][cc].x = fmaf(rr, zr, V[ty][cc].x);
-            V[ty][cc].y = fmaf(rr, zi, V[ty][cc].y);
+        for (int cc = 0; cc < NC; ++cc) {
+          if (cc < ncomp) {
+            float r;
+            if (MAPS)
+              r = __expf(la[ty] - trf * r2[ty][MAPS ? cc : 0] - tinh * r2i[ty][MAPS ? cc : 0]);
+            else
+              r = e[5 + cc];
+            cg[ty][cc].x = fmaf(r, zr, cg[ty][cc].x);
+            cg[ty][cc].y = fmaf(r, zi, cg[ty][cc].y);
+            if (GRADS) {
+              Uy[ty][GRADS ? cc : 0] = fmaf(r * tph, zi, Uy[ty][GRADS ? cc : 0]);
+              Vx[ty][GRADS ? cc : 0] = fmaf(r * trf, zr, Vx[ty][GRADS ? cc : 0]);
+            }
           }
         }
       }
     }
   }
+  if (!active) return;
   const size_t plane = (size_t)snx * sny;
 #pragma unroll
   for (int ty = 0; ty < TY; ++ty) {
-    int y = y0 + ty;
+    const int y = y0 + ty;
     if (y >= sny) break;
-    size_t i = (size_t)x + (size_t)snx * y;
+    const size_t i = (size_t)x + (size_t)snx * y;
     float fg = 0.f;
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       if (c >= ncomp) break;
       u.comp_grad[c * plane + i] = cg[ty][c];
       if (GRADS) {
-        const int cc = GRADS ? c : 0;
-        // Im(m conj(U)) with m real = -m * U.y
-        fg += m[ty][c] * U[ty][cc].y;
-        if (u.r2_grad) u.r2_grad[c * plane + i] = -2.0f * m[ty][c] * V[ty][cc].x;
+        const float m = __ldg(u.comp + (size_t)c * u.comp_stride + i);
+        fg = fmaf(m, Uy[ty][GRADS ? c : 0], fg);
+        if (u.r2_grad) u.r2_grad[c * plane + i] = -2.0f * m * Vx[ty][GRADS ? c : 0];
       }
     }
-    if (GRADS && u.fmap_grad) u.fmap_grad[i] = 4.0f * 3.14159265358979f * fg * (distort ? 1.f : 0.f);
+    if (GRADS && u.fmap_grad) u.fmap_grad[i] = distort ? 4.0f * 3.14159265358979f * fg : 0.f;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// x-stage as a register-tiled complex GEMM.  A tile is up to 32 rows (lines of ONE readout polarity
+// x coils) by 64 output columns; K runs over the contraction in chunks of 32 staged in shared memory.
+//   forward : out[q][row_j][kx] = (1/nvox) sum_x  g[q][j][x] E_j(x)        tw_pol[x][kx]
+//   adjoint : h[q][j][x]        = (1/nvox) conj(E_j(x)) sum_kx conj(tw_pol[x][kx]) r[q][row_j][kx]
+// Each of 256 threads owns 4 rows x 2 columns.
+template <bool ADJ>
+__global__ void __launch_bounds__(256) xgemm_kernel(const UnitDesc* __restrict__ units,
+                                                    const XTile* __restrict__ tiles) {
+  __shared__ float2 As[32][33];   // [row][k]
+  __shared__ float2 Bs[32][64];   // [k][col]
+  __shared__ int lrow[32], lline[32], lq[32];
+  __shared__ float ldec[32];
+  const XTile& T = tiles[blockIdx.x];
+  const UnitDesc& u = units[T.unit];
+  const int snx = u.snx, nx = u.nx;
+  const int K = ADJ ? nx : snx;       // contraction length
+  const int N = ADJ ? snx : nx;       // output columns
+  const int nrows = T.nl * T.nq;
+  const int ox = snx / nx, sxs = ox * (nx / 2);
+  const double xoff = (ox - 1.0) / 2.0;
+  const bool eddy = (u.flags & UF_EDDY) != 0;
+  if (threadIdx.x < 32) {
+    const int r = threadIdx.x;
+    if (r < nrows) {
+      const int jj = r / T.nq, qq = r % T.nq;
+      const LineRec& L = u.lines[T.line[jj]];
+      lrow[r] = L.row;
+      lline[r] = T.line[jj];
+      lq[r] = T.q0 + qq;
+      ldec[r] = L.decay;
+    } else {
+      lrow[r] = 0;
+      lline[r] = 0;
+      lq[r] = -1;
+      ldec[r] = 0.f;
+    }
+  }
+  __syncthreads();
+  // the twiddles of this tile's polarity: forward [x][kx], adjoint [kx][x] (transposed table)
+  const float2* tw = u.geo.tw + (size_t)(ADJ ? 2 + T.pol : T.pol) * snx * nx;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 row groups of 4
+  float2 acc[4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
+  for (int k0 = 0; k0 < K; k0 += 32) {
+    // stage A: 32 rows x 32 k
+    for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+      const int r = e >> 5, kk = e & 31, k = k0 + kk;
+      float2 v = make_float2(0.f, 0.f);
+      if (lq[r] >= 0 && k < K) {
+        if (!ADJ) {
+          v = u.g[((size_t)lq[r] * u.n_lines + lline[r]) * snx + k];
+          if (eddy) {
+            const double xc = ((double)k - sxs - xoff) / ox;
+            double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)ldec[r];
+            tv -= rint(tv);
+            float sn, cs;
+            __sincosf(kTwoPiF * (float)tv, &sn, &cs);
+            v = make_float2(v.x * cs - v.y * sn, v.x * sn + v.y * cs);
+          }
+        } else {
+          v = u.kspace[((size_t)lq[r] * u.n_rows + lrow[r]) * nx + k];
+        }
+      }
+      As[r][kk] = v;
+    }
+    // stage B: 32 k x 64 columns
+    for (int e = threadIdx.x; e < 32 * 64; e += 256) {
+      const int kk = e >> 6, c = e & 63, k = k0 + kk, col = T.col0 + c;
+      Bs[kk][c] = (k < K && col < N) ? __ldg(tw + (size_t)k * N + col) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < 32; ++kk) {
+      const float2 b0 = Bs[kk][tx], b1 = Bs[kk][tx + 32];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 a = As[ty * 4 + i][kk];
+        if (!ADJ) {
+          acc[i][0].x = fmaf(a.x, b0.x, fmaf(-a.y, b0.y, acc[i][0].x));
+          acc[i][0].y = fmaf(a.x, b0.y, fmaf(a.y, b0.x, acc[i][0].y));
+          acc[i][1].x = fmaf(a.x, b1.x, fmaf(-a.y, b1.y, acc[i][1].x));
+          acc[i][1].y = fmaf(a.x, b1.y, fmaf(a.y, b1.x, acc[i][1].y));
+        } else {  // a * conj(b)
+          acc[i][0].x = fmaf(a.x, b0.x, fmaf(a.y, b0.y, acc[i][0].x));
+          acc[i][0].y = fmaf(a.y, b0.x, fmaf(-a.x, b0.y, acc[i][0].y));
+          acc[i][1].x = fmaf(a.x, b1.x, fmaf(a.y, b1.y, acc[i][1].x));
+          acc[i][1].y = fmaf(a.y, b1.x, fmaf(-a.x, b1.y, acc[i][1].y));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const float inv_n = 1.0f / (float)(snx * u.sny);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = ty * 4 + i;
+    if (lq[r] < 0) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int col = T.col0 + tx + 32 * h;
+      if (col >= N) continue;
+      float2 v = make_float2(acc[i][h].x * inv_n, acc[i][h].y * inv_n);
+      if (!ADJ) {
+        u.kspace[((size_t)lq[r] * u.n_rows + lrow[r]) * nx + col] = v;
+      } else {
+        if (eddy) {
+          const double xc = ((double)col - sxs - xoff) / ox;
+          double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)ldec[r];
+          tv -= rint(tv);
+          float sn, cs;
+          __sincosf(kTwoPiF * (float)tv, &sn, &cs);
+          v = make_float2(v.x * cs + v.y * sn, v.y * cs - v.x * sn);
+        }
+        u.g[((size_t)lq[r] * u.n_lines + lline[r]) * snx + col] = v;
+      }
+    }
   }
 }
 
@@ -528,6 +625,32 @@ void set_smem(K kernel, size_t bytes) {
 }  // namespace
 
 // ---- plans and launchers ----------------------------------------------------------------------
+void append_xtiles(std::vector<XTile>& out, const UnitDesc& u, int unit_index, const LineRec* lines, int dir) {
+  const int nl = u.n_lines, nc = u.ncoils;
+  const int N = dir == 0 ? u.nx : u.snx;
+  const int nq = std::min(nc, 32);
+  const int lines_per_tile = std::max(1, 32 / nq);
+  for (int pol = 0; pol < 2; ++pol) {
+    std::vector<int> group;
+    for (int l = 0; l < nl; ++l)
+      if ((lines[l].pol < 0 ? 1 : 0) == pol) group.push_back(l);
+    for (size_t g0 = 0; g0 < group.size(); g0 += lines_per_tile)
+      for (int q0 = 0; q0 < nc; q0 += nq)
+        for (int c0 = 0; c0 < N; c0 += 64) {
+          XTile t;
+          std::memset(&t, 0, sizeof t);
+          t.unit = unit_index;
+          t.q0 = q0;
+          t.nq = std::min(nq, nc - q0);
+          t.nl = (int)std::min<size_t>(lines_per_tile, group.size() - g0);
+          t.col0 = c0;
+          t.pol = pol;
+          for (int k = 0; k < t.nl; ++k) t.line[k] = group[g0 + k];
+          out.push_back(t);
+        }
+  }
+}
+
 namespace {
 constexpr int kT = 4;
 constexpr int kTY = 4;
@@ -566,6 +689,8 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       if (hu[i].ncoils > kMaxCoils) fail("more than 64 coils");
     }
     p->max_coils = max_coils;
+    for (int i = 0; i < n; ++i)
+      p->max_hchunk = std::max(p->max_hchunk, adjoint_chunk_lines(hu[i].ncoils) * hu[i].ncoils);
     int max_comp = 0;
     for (int i = 0; i < n; ++i) max_comp = std::max(max_comp, hu[i].ncomp);
     p->nc = max_comp <= 1 ? 1 : max_comp <= 2 ? 2 : max_comp <= 3 ? 3 : max_comp <= 4 ? 4 : 8;
@@ -581,12 +706,24 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->n_ytiles[pass] = (int)tiles.size();
       p->d_ytiles[pass] = (int4*)dev_upload(p, tiles.data(), sizeof(int4) * tiles.size());
     }
-    std::vector<int4> xt;
-    for (int i = 0; i < n; ++i)
-      for (int q = 0; q < hu[i].ncoils; ++q)
-        for (int l = 0; l < hu[i].n_lines; l += XR) xt.push_back(make_int4(i, q, l, 0));
-    p->n_xtiles = (int)xt.size();
-    p->d_xtiles = (int4*)dev_upload(p, xt.data(), sizeof(int4) * xt.size());
+    // x-stage GEMM tiles, from host copies of the line tables (one copy per distinct table)
+    std::map<const LineRec*, std::vector<LineRec>> host_lines;
+    for (int dir = 0; dir < 2; ++dir) {
+      std::vector<XTile> xt;
+      for (int i = 0; i < n; ++i) {
+        const int nl = hu[i].n_lines;
+        if (nl == 0) continue;
+        auto it = host_lines.find(hu[i].lines);
+        if (it == host_lines.end()) {
+          std::vector<LineRec> L(nl);
+          MRSIM_CUDA(cudaMemcpy(L.data(), hu[i].lines, sizeof(LineRec) * nl, cudaMemcpyDeviceToHost));
+          it = host_lines.emplace(hu[i].lines, std::move(L)).first;
+        }
+        append_xtiles(xt, hu[i], i, it->second.data(), dir);
+      }
+      p->n_gtiles[dir] = (int)xt.size();
+      p->d_gtiles[dir] = dev_upload(p, xt.data(), sizeof(XTile) * xt.size());
+    }
     for (int pass = 0; pass < 4; ++pass) {
       bool maps = pass & 1, grads = pass & 2;
       std::vector<int4> yt;
@@ -629,7 +766,7 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
     if (p->n_ytiles[pass] == 0) continue;
     const bool maps = pass == 1;
     const int QG = p->qg, NCv = p->nc;
-    const size_t sm = sizeof(float) * (size_t)p->max_sny * (kT + QG);
+    const size_t sm = sizeof(float) * (size_t)p->max_sny * (kT + (QG + 3) / 4 * 4);
     bool launched = false;
 #define MRSIM_Y(QGV, NCV, M)                                                            \
   if (QG == QGV && NCv == NCV && maps == M) {                                           \
@@ -650,19 +787,15 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
 }
 
 void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st) {
-  if (p->n_xtiles) {
-    size_t sm = sizeof(float2) * XR * p->max_snx;
-    set_smem(xstage_kernel, sm);
-    xstage_kernel<<<(unsigned)p->n_xtiles, 128, sm, st>>>(p->d_units, p->d_xtiles);
+  if (p->n_gtiles[0]) {
+    xgemm_kernel<false><<<(unsigned)p->n_gtiles[0], 256, 0, st>>>(p->d_units, (const XTile*)p->d_gtiles[0]);
     MRSIM_CUDA(cudaGetLastError());
   }
 }
 
 void epi_plan_adjoint_xstage(const EpiPlan* p, cudaStream_t st) {
-  if (p->n_xtiles) {
-    size_t sm = sizeof(float2) * XR * p->max_nx;
-    set_smem(xadjoint_kernel, sm);
-    xadjoint_kernel<<<(unsigned)p->n_xtiles, 128, sm, st>>>(p->d_units, p->d_xtiles);
+  if (p->n_gtiles[1]) {
+    xgemm_kernel<true><<<(unsigned)p->n_gtiles[1], 256, 0, st>>>(p->d_units, (const XTile*)p->d_gtiles[1]);
     MRSIM_CUDA(cudaGetLastError());
   }
 }
@@ -672,7 +805,9 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st) {
     if (p->n_atiles[pass] == 0) continue;
     const bool maps = pass & 1, grads = (pass & 2) != 0;
     const int NCv = p->nc;
-    size_t sm = sizeof(float) * (size_t)kTY * (p->max_lines + p->max_coils);
+    size_t sm = sizeof(float2) * (size_t)2 * p->max_hchunk * 128 +
+                sizeof(float) * ((size_t)kTY * (p->max_lines + p->max_coils) + 128 * (size_t)p->max_coils +
+                                 (size_t)p->max_lines * (5 + NCv));
     bool launched = false;
 #define MRSIM_A(NCV, M, G)                                                              \
   if (NCv == NCV && maps == M && grads == G) {                                          \

@@ -87,6 +87,13 @@ enum : int {
   UF_DISTORT = 128,
 };
 
+// A tile of the x-stage GEMM: up to 32 rows (lines of one readout polarity x coils) by 64 output
+// columns of one unit.
+struct XTile {
+  int unit, q0, nq, nl, col0, pol, pad0, pad1;
+  int line[32];
+};
+
 // Per-unit static phase inputs for the statics kernel.
 struct StaticDesc {
   int snx, sny, nx, ny, o, z, nz_full, flags;  // flags: 1 = phase from phase0, 2 = eddy phase
@@ -132,16 +139,19 @@ struct EpiPlan {
   UnitDesc* d_units = nullptr;
   StaticDesc* d_statics = nullptr;
   int max_static_n = 0, max_sny = 0, max_snx = 0, max_nx = 0, max_lines = 0, max_coils = 0, qg = 1, nc = 1;
+  int max_hchunk = 0;  // max over units of (adjoint h chunk lines x coils)
   int4* d_ytiles[2] = {nullptr, nullptr};
   int n_ytiles[2] = {0, 0};
-  int4* d_xtiles = nullptr;
-  int n_xtiles = 0;
+  void* d_gtiles[2] = {nullptr, nullptr};  // x-stage GEMM tiles: forward, adjoint
+  int n_gtiles[2] = {0, 0};
   int4* d_atiles[4] = {nullptr, nullptr, nullptr, nullptr};
   int n_atiles[4] = {0, 0, 0, 0};
   std::vector<void*> allocs;
   ~EpiPlan();
 };
 EpiPlan* epi_plan_create(const UnitDesc* units, int n, const StaticDesc* statics, int ns);
+// The x-stage tiles of one unit (dir 0 forward, 1 adjoint); `lines` is a host copy of its table.
+void append_xtiles(std::vector<XTile>& out, const UnitDesc& u, int unit_index, const LineRec* lines, int dir);
 void epi_plan_statics(const EpiPlan* p, cudaStream_t st);
 void epi_plan_forward(const EpiPlan* p, cudaStream_t st);
 void epi_plan_adjoint(const EpiPlan* p, cudaStream_t st);

@@ -11,7 +11,7 @@
 // device pointers for the inputs and the output.
 //
 // Costs and rules:
-//  - every GPU that loads the library holds these arrays (about 7.6 MiB) until the process exits;
+//  - every GPU that loads the library holds these arrays (about 7.8 MiB) until the process exits;
 //  - the sizes are capped (see the limits below); larger slices are rejected with an error;
 //  - the first call on a device resolves the arrays' device addresses with cudaGetSymbolAddress
 //    (with that device current) and caches them; make that first call before any stream capture;
@@ -38,6 +38,7 @@ constexpr size_t kNaTw = size_t(1) << 18;       // float2: 4 * snx * nx
 constexpr size_t kNaAxis = size_t(1) << 15;     // float: ncoils * snx, ncoils * sny
 constexpr size_t kNaLines = 1024;
 constexpr size_t kNaTiles = 8192;
+constexpr size_t kNaXTiles = 2048;
 
 static __device__ __align__(256) float2 na_scratch[kNaScratch];
 static __device__ __align__(256) float na_phase[kNaPlane];
@@ -48,7 +49,7 @@ static __device__ __align__(256) LineRec na_lines[kNaLines];
 static __device__ __align__(256) UnitDesc na_unit[1];
 static __device__ __align__(256) StaticDesc na_static[1];
 static __device__ __align__(256) int4 na_ytiles[kNaTiles];
-static __device__ __align__(256) int4 na_xtiles[kNaTiles];
+static __device__ __align__(256) XTile na_xtiles[kNaXTiles];
 
 struct NaAddrs {
   float2* scratch = nullptr;
@@ -60,7 +61,7 @@ struct NaAddrs {
   UnitDesc* unit = nullptr;
   StaticDesc* statics = nullptr;
   int4* ytiles = nullptr;
-  int4* xtiles = nullptr;
+  XTile* xtiles = nullptr;
   bool ready = false;
 };
 
@@ -93,7 +94,7 @@ const NaAddrs& addresses(int device) {
     MRSIM_CUDA(cudaGetSymbolAddress(&p, na_ytiles));
     a.ytiles = (int4*)p;
     MRSIM_CUDA(cudaGetSymbolAddress(&p, na_xtiles));
-    a.xtiles = (int4*)p;
+    a.xtiles = (XTile*)p;
     a.ready = true;
   }
   return a;
@@ -291,19 +292,20 @@ void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquis
   plan.max_coils = ncoils;
   plan.nc = ncomp <= 1 ? 1 : ncomp <= 2 ? 2 : ncomp <= 3 ? 3 : ncomp <= 4 ? 4 : 8;
   plan.qg = ncoils <= 1 ? 1 : ncoils <= 2 ? 2 : ncoils <= 4 ? 4 : 8;
-  std::vector<int4> yt, xt;
-  for (int l = 0; l < (int)nl; l += 4)
+  std::vector<int4> yt;
+  std::vector<XTile> xt;
+  for (int l = 0; l < (int)nl; l += 4)  // the y-stage covers 4 lines per CTA
     for (int x0 = 0; x0 < snx; x0 += 128)
       for (int q0 = 0; q0 < ncoils; q0 += plan.qg) yt.push_back(make_int4(0, l, x0, q0));
-  for (int q = 0; q < ncoils; ++q)
-    for (int l = 0; l < (int)nl; l += 8) xt.push_back(make_int4(0, q, l, 0));
-  if (yt.size() > kNaTiles || xt.size() > kNaTiles) too_big("the tile lists", std::max(yt.size(), xt.size()), kNaTiles);
+  append_xtiles(xt, u, 0, lines.data(), 0);
+  if (yt.size() > kNaTiles) too_big("the y-stage tile list", yt.size(), kNaTiles);
+  if (xt.size() > kNaXTiles) too_big("the x-stage tile list", xt.size(), kNaXTiles);
   if (!yt.empty()) MRSIM_CUDA(cudaMemcpyAsync(A.ytiles, yt.data(), yt.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-  if (!xt.empty()) MRSIM_CUDA(cudaMemcpyAsync(A.xtiles, xt.data(), xt.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  if (!xt.empty()) MRSIM_CUDA(cudaMemcpyAsync(A.xtiles, xt.data(), xt.size() * sizeof(XTile), cudaMemcpyHostToDevice, st));
   plan.d_ytiles[0] = A.ytiles;
   plan.n_ytiles[0] = (int)yt.size();
-  plan.d_xtiles = A.xtiles;
-  plan.n_xtiles = (int)xt.size();
+  plan.d_gtiles[0] = A.xtiles;
+  plan.n_gtiles[0] = (int)xt.size();
 
   MRSIM_CUDA(cudaMemsetAsync(out, 0, sizeof(float2) * (size_t)ncoils * nx * ny, st));
   epi_plan_statics(&plan, st);
