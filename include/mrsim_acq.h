@@ -314,6 +314,75 @@ int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* im
                                   float* kspace, float* comp_grad, float* fmap_grad,
                                   float* r2_grad);
 
+/* ---- the stack-of-spirals path: host plans ------------------------------------------------ */
+/* `spiral_tau_c` (readout.rs:564-596): the constant-angular-velocity centre region (ms). */
+int mrsim_spiral_tau_c(int64_t nx, int64_t interleaves, double readout_ms, double dwell_ms,
+                       double radial_oversampling, double* tau_c_ms);
+
+typedef struct mrsim_spiral_info {
+  int64_t samples;     /* per interleaf: floor(T / dwell) */
+  int64_t interleaves;
+  double k_max, n_turns, tau_c_ms;
+} mrsim_spiral_info;
+
+/* `spiral_trajectory` (readout.rs:597-620).  Fills `info`; with k / tau_ms non-NULL also writes
+ * k [interleaf][sample][2] (cycles/FOV) and tau_ms [sample] ((j + 1/2) dwell) when
+ * `capacity` >= samples per interleaf.  Errors carry the reference's messages. */
+int mrsim_spiral_trajectory(int64_t nx, int64_t ny, int64_t interleaves, double readout_ms,
+                            double dwell_ms, double radial_oversampling, int64_t capacity,
+                            double* k, double* tau_ms, mrsim_spiral_info* info);
+
+typedef struct mrsim_tseg_info {
+  int64_t l, m;      /* segments, Chebyshev degree */
+  double b_sum;      /* max over samples of sum_l |b_l| */
+  double grid_err;   /* max residual on the rate grid */
+  double bound;      /* certified bound (< 1e-7) */
+} mrsim_tseg_info;
+
+/* `tseg::plan` (tseg.rs:230-289) over the rate rectangle d (1/ms) x f (Hz).  With tau_l / b
+ * non-NULL and l_capacity >= L: tau_l [L] (ms) and b [n_tau][L][2] (re, im). */
+int mrsim_tseg_plan(const double* tau_ms, int64_t n_tau, double t_ms, const double d[2],
+                    const double f[2], int64_t l_capacity, double* tau_l, double* b,
+                    mrsim_tseg_info* info);
+
+/* `epg_cpmg` (epg.rs:101-125): ln A_e for e = 1..n_echoes of a CPMG train. */
+int mrsim_epg_cpmg(int64_t n_echoes, double esp_ms, double refocusing_deg, double t1_ms,
+                   double t2_ms, double* ln_amp);
+
+/* ---- the stack-of-spirals path: device NUFFT pair and spiral forwards ---------------------- */
+/* Kernel width of the exponential-of-semicircle NUFFT at tolerance tol (nufft.rs:165). */
+int mrsim_nufft_kernel_width(double tol);
+
+/* `Nufft2::type1` (nufft.rs:225-256) on the device, host buffers: periods n, modes m_lo ..
+ * m_lo + m_out per axis (inside [-n/2, n/2]), points u [npts][2] (period-n coordinates),
+ * weights [npts] (re, im) f32, sign +1 / -1; modes [m_out1][m_out0] (re, im) f32. */
+int mrsim_nufft2_type1(mrsim_context* ctx, const int64_t n[2], const int64_t m_lo[2],
+                       const int64_t m_out[2], double tol, const double* u, int64_t npts,
+                       const float* weights, int32_t sign, float* modes);
+/* `Nufft2::type2` (nufft.rs:259-292): values at the points from modes in type 1's layout. */
+int mrsim_nufft2_type2(mrsim_context* ctx, const int64_t n[2], const int64_t m_lo[2],
+                       const int64_t m_out[2], double tol, const float* modes, const double* u,
+                       int64_t npts, int32_t sign, float* out);
+
+/* `spiral_kspace_exact` (spiral.rs:107-137) on the device: one slice and coil at frequencies
+ * k [npts][2] (cycles/FOV) sampled tau_ms [npts] after the echo; log_amp per sim voxel or NULL.
+ * Up to 4 compartments.  out [npts] (re, im) f32. */
+int mrsim_spiral_kspace_exact(mrsim_context* ctx, const mrsim_slice_input* inp,
+                              const mrsim_acquisition* acq, int64_t coil, int64_t ncoils,
+                              const double* k, const double* tau_ms, int64_t npts,
+                              const double* log_amp, float* out);
+
+/* `SegmentedForward::new` + `apply` with `segment_inputs` (spiral.rs:83-103, 154-201): the
+ * time-segmented type-2 NUFFT forward of a one-compartment slice.  Sample j sits at
+ * tau_ms[tau_idx[j]]; the plan is certified over d (1/ms) x f (Hz) on [0, t_ms];
+ * decay_inside = voxel mode.  `info` (may be NULL) receives the plan's figures. */
+int mrsim_spiral_segmented_forward(mrsim_context* ctx, const mrsim_slice_input* inp,
+                                   const mrsim_acquisition* acq, int64_t coil, int64_t ncoils,
+                                   const double* k, const int64_t* tau_idx, int64_t npts,
+                                   const double* tau_ms, int64_t n_tau, double t_ms,
+                                   const double d[2], const double f[2], const double* log_amp,
+                                   int32_t decay_inside, float* out, mrsim_tseg_info* info);
+
 #ifdef __cplusplus
 }
 #endif

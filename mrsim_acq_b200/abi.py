@@ -94,6 +94,20 @@ class AcquisitionOutput_(C.Structure):
     ]
 
 
+class SpiralInfo_(C.Structure):
+    """`mrsim_spiral_info` — the scalars of `SpiralTrajectory` (readout.rs:463-560)."""
+
+    _fields_ = [("samples", C.c_int64), ("interleaves", C.c_int64), ("k_max", C.c_double),
+                ("n_turns", C.c_double), ("tau_c_ms", C.c_double)]
+
+
+class TsegInfo_(C.Structure):
+    """`mrsim_tseg_info` — the scalars of `TsegPlan` (tseg.rs:60-75)."""
+
+    _fields_ = [("l", C.c_int64), ("m", C.c_int64), ("b_sum", C.c_double), ("grid_err", C.c_double),
+                ("bound", C.c_double)]
+
+
 class LibraryMissing(RuntimeError):
     pass
 
@@ -149,6 +163,23 @@ def _declare(lib):
         "mrsim_probe_fp32_tflops": (C.c_int, [P, C.POINTER(C.c_double)]),
         "mrsim_epi_operator_adjoint_host": (C.c_int, [P, c_f32p, c_f32p, c_f32p, c_f32p]),
         "mrsim_epi_operator_apply_host": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
+        "mrsim_spiral_tau_c": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, c_f64p]),
+        "mrsim_spiral_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                              C.c_int64, c_f64p, c_f64p, C.POINTER(SpiralInfo_)]),
+        "mrsim_tseg_plan": (C.c_int, [c_f64p, C.c_int64, C.c_double, c_f64p, c_f64p, C.c_int64, c_f64p, c_f64p,
+                                      C.POINTER(TsegInfo_)]),
+        "mrsim_epg_cpmg": (C.c_int, [C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, c_f64p]),
+        "mrsim_nufft_kernel_width": (C.c_int, [C.c_double]),
+        "mrsim_nufft2_type1": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                         C.c_double, c_f64p, C.c_int64, c_f32p, C.c_int32, c_f32p]),
+        "mrsim_nufft2_type2": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                         C.c_double, c_f32p, c_f64p, C.c_int64, C.c_int32, c_f32p]),
+        "mrsim_spiral_kspace_exact": (C.c_int, [P, C.POINTER(SliceInput_), C.POINTER(Acquisition_), C.c_int64,
+                                                C.c_int64, c_f64p, c_f64p, C.c_int64, c_f64p, c_f32p]),
+        "mrsim_spiral_segmented_forward": (C.c_int, [P, C.POINTER(SliceInput_), C.POINTER(Acquisition_), C.c_int64,
+                                                     C.c_int64, c_f64p, C.POINTER(C.c_int64), C.c_int64, c_f64p,
+                                                     C.c_int64, C.c_double, c_f64p, c_f64p, c_f64p, C.c_int32,
+                                                     c_f32p, C.POINTER(TsegInfo_)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -11,6 +11,8 @@
 #include "host_tables.h"
 #include "mrsim_internal.h"
 #include "series.h"
+#include "spiral.h"
+#include "spiral_host.h"
 
 namespace {
 thread_local std::string g_last_error;
@@ -491,6 +493,155 @@ int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* im
     if (r2_grad && o->d_r2_grad)
       MRSIM_CUDA(cudaMemcpyAsync(r2_grad, o->d_r2_grad, nunits * o->ncomp * plane * 4, cudaMemcpyDeviceToHost, st));
     MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+
+// ---- stack-of-spirals path ------------------------------------------------------------------------
+int mrsim_spiral_tau_c(int64_t nx, int64_t interleaves, double readout_ms, double dwell_ms, double radial_oversampling,
+                       double* tau_c_ms) {
+  return guarded([&] {
+    need(tau_c_ms, "tau_c_ms");
+    *tau_c_ms = mrsim::spiral_tau_c((int)nx, (int)interleaves, readout_ms, dwell_ms, radial_oversampling);
+  });
+}
+
+int mrsim_spiral_trajectory(int64_t nx, int64_t ny, int64_t interleaves, double readout_ms, double dwell_ms,
+                            double radial_oversampling, int64_t capacity, double* k, double* tau_ms,
+                            mrsim_spiral_info* info) {
+  return guarded([&] {
+    need(info, "info");
+    mrsim::SpiralTraj tr =
+        mrsim::spiral_trajectory((int)nx, (int)ny, (int)interleaves, readout_ms, dwell_ms, radial_oversampling);
+    info->samples = (int64_t)tr.tau_ms.size();
+    info->interleaves = tr.interleaves;
+    info->k_max = tr.k_max;
+    info->n_turns = tr.n_turns;
+    info->tau_c_ms = tr.tau_c_ms;
+    if (!k && !tau_ms) return;
+    if (capacity < info->samples) mrsim::fail("sample capacity below the samples per interleaf");
+    if (tau_ms) std::memcpy(tau_ms, tr.tau_ms.data(), tr.tau_ms.size() * 8);
+    if (k) std::memcpy(k, tr.k.data(), tr.k.size() * 8);
+  });
+}
+
+int mrsim_tseg_plan(const double* tau_ms, int64_t n_tau, double t_ms, const double d[2], const double f[2],
+                    int64_t l_capacity, double* tau_l, double* b, mrsim_tseg_info* info) {
+  return guarded([&] {
+    need(d, "d");
+    need(f, "f");
+    need(info, "info");
+    if (n_tau > 0) need(tau_ms, "tau_ms");
+    std::vector<double> tau(tau_ms, tau_ms + std::max<int64_t>(0, n_tau));
+    mrsim::TsegPlan p = mrsim::tseg_plan(tau, t_ms, d, f);
+    info->l = p.l;
+    info->m = p.m;
+    info->b_sum = p.b_sum;
+    info->grid_err = p.grid_err;
+    info->bound = p.bound;
+    if (!tau_l && !b) return;
+    if (l_capacity < p.l) mrsim::fail("segment capacity below the plan's L");
+    if (tau_l) std::memcpy(tau_l, p.tau_l.data(), p.tau_l.size() * 8);
+    if (b) std::memcpy(b, p.b.data(), p.b.size() * 8);
+  });
+}
+
+int mrsim_epg_cpmg(int64_t n_echoes, double esp_ms, double refocusing_deg, double t1_ms, double t2_ms,
+                   double* ln_amp) {
+  return guarded([&] {
+    if (n_echoes < 0) mrsim::fail("negative echo count");
+    if (n_echoes > 0) need(ln_amp, "ln_amp");
+    auto v = mrsim::epg_cpmg((int)n_echoes, esp_ms, refocusing_deg, t1_ms, t2_ms);
+    if (n_echoes > 0) std::memcpy(ln_amp, v.data(), v.size() * 8);
+  });
+}
+
+int mrsim_nufft_kernel_width(double tol) { return mrsim::nufft_width(tol); }
+
+static void check_nufft(const int64_t n[2], const int64_t m_lo[2], const int64_t m_out[2], int64_t npts, int sign) {
+  need(n, "n");
+  need(m_lo, "m_lo");
+  need(m_out, "m_out");
+  for (int a = 0; a < 2; ++a)
+    if (n[a] <= 0 || n[a] > 8192) mrsim::fail("NUFFT period must be in 1..8192");
+  if (npts < 0 || npts > ((int64_t)1 << 30)) mrsim::fail("NUFFT point count out of range");
+  if (sign != 1 && sign != -1) mrsim::fail("NUFFT sign must be +1 or -1");
+}
+
+int mrsim_nufft2_type1(mrsim_context* ctx, const int64_t n[2], const int64_t m_lo[2], const int64_t m_out[2],
+                       double tol, const double* u, int64_t npts, const float* weights, int32_t sign, float* modes) {
+  return on_ctx(ctx, [&] {
+    check_nufft(n, m_lo, m_out, npts, sign);
+    need(modes, "modes");
+    if (npts > 0) {
+      need(u, "u");
+      need(weights, "weights");
+    }
+    mrsim::nufft2_host(ctx, 1, (int)n[0], (int)n[1], (int)m_lo[0], (int)m_lo[1], (int)m_out[0], (int)m_out[1], tol, u,
+                       (int)npts, weights, sign, modes);
+  });
+}
+
+int mrsim_nufft2_type2(mrsim_context* ctx, const int64_t n[2], const int64_t m_lo[2], const int64_t m_out[2],
+                       double tol, const float* modes, const double* u, int64_t npts, int32_t sign, float* out) {
+  return on_ctx(ctx, [&] {
+    check_nufft(n, m_lo, m_out, npts, sign);
+    need(modes, "modes");
+    if (npts > 0) {
+      need(u, "u");
+      need(out, "out");
+    }
+    mrsim::nufft2_host(ctx, 2, (int)n[0], (int)n[1], (int)m_lo[0], (int)m_lo[1], (int)m_out[0], (int)m_out[1], tol, u,
+                       (int)npts, modes, sign, out);
+  });
+}
+
+int mrsim_spiral_kspace_exact(mrsim_context* ctx, const mrsim_slice_input* inp, const mrsim_acquisition* acq,
+                              int64_t coil, int64_t ncoils, const double* k, const double* tau_ms, int64_t npts,
+                              const double* log_amp, float* out) {
+  return on_ctx(ctx, [&] {
+    need(inp, "inp");
+    need(acq, "acq");
+    check_slice_input(*inp, *acq);
+    if (npts < 0) mrsim::fail("negative sample count");
+    if (npts > 0) {
+      need(k, "k");
+      need(tau_ms, "tau_ms");
+      need(out, "out");
+    }
+    if (coil < 0 || coil >= std::max<int64_t>(ncoils, 1)) mrsim::fail("coil index out of range");
+    mrsim::spiral_exact_host(ctx, *inp, *acq, (int)coil, (int)ncoils, k, tau_ms, (int)npts, log_amp, out);
+  });
+}
+
+int mrsim_spiral_segmented_forward(mrsim_context* ctx, const mrsim_slice_input* inp, const mrsim_acquisition* acq,
+                                   int64_t coil, int64_t ncoils, const double* k, const int64_t* tau_idx,
+                                   int64_t npts, const double* tau_ms, int64_t n_tau, double t_ms, const double d[2],
+                                   const double f[2], const double* log_amp, int32_t decay_inside, float* out,
+                                   mrsim_tseg_info* info) {
+  return on_ctx(ctx, [&] {
+    need(inp, "inp");
+    need(acq, "acq");
+    need(d, "d");
+    need(f, "f");
+    check_slice_input(*inp, *acq);
+    if (npts < 0 || n_tau < 0) mrsim::fail("negative sample count");
+    if (npts > 0) {
+      need(k, "k");
+      need(tau_idx, "tau_idx");
+      need(out, "out");
+    }
+    if (n_tau > 0) need(tau_ms, "tau_ms");
+    if (coil < 0 || coil >= std::max<int64_t>(ncoils, 1)) mrsim::fail("coil index out of range");
+    auto r = mrsim::spiral_segmented_host(ctx, *inp, *acq, (int)coil, (int)ncoils, k, tau_idx, (int)npts, tau_ms,
+                                          (int)n_tau, t_ms, d, f, log_amp, decay_inside != 0, out);
+    if (info) {
+      info->l = r.l;
+      info->m = r.m;
+      info->bound = r.bound;
+      info->b_sum = r.b_sum;
+      info->grid_err = r.grid_err;
+    }
   });
 }
 

@@ -1,0 +1,346 @@
+// nufft_kernels.cu — the 2D NUFFT pair of the stack-of-spirals path on the device (reference
+// `Nufft2`, nufft.rs:125-299): exponential-of-semicircle kernel exp(beta (sqrt(1 - z^2) - 1)),
+// beta = 2.30 w, w = ceil(-log10 tol) + 1 clamped to 2..16, oversampling 2, deapodization by the
+// kernel's sampled transform.  Type 1 spreads (FP32 atomics), type 2 interpolates; the fine-grid
+// FFT is a shared-memory radix-2 kernel (a direct DFT for lengths that are not powers of two).
+// Point positions and kernel offsets are formed in FP64 (the kernel is steep: an FP32 position
+// would cost ~1e-5 of relative accuracy); the taps and sums are FP32.
+//
+// Also the spiral forwards (spiral.rs): the exact sum over voxels at each sample and the
+// time-segmented combination of L type-2 transforms.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <algorithm>
+
+#include "nufft.h"
+
+namespace mrsim {
+
+namespace {
+
+__device__ __forceinline__ int wrap(int m, int n) {
+  m %= n;
+  return m < 0 ? m + n : m;
+}
+
+// First fine cell and the w taps of coordinate u (period n) on a fine grid of nf = 2n cells.
+__device__ __forceinline__ int es_taps(double u, int nf, int w, float beta, float* k) {
+  const double half = 0.5 * w;
+  double p = fmod(2.0 * u, (double)nf);
+  if (p < 0.0) p += nf;
+  const int m0 = (int)floor(p - half) + 1;
+  const float ih = (float)(1.0 / half);
+#pragma unroll 4
+  for (int i = 0; i < w; ++i) {
+    const float z = (float)((double)(m0 + i) - p) * ih;
+    k[i] = fabsf(z) < 1.0f ? __expf(beta * (sqrtf(1.0f - z * z) - 1.0f)) : 0.0f;
+  }
+  return m0;
+}
+
+constexpr int kWMax = 16;
+
+__global__ void place_kernel(const NufftGrid g, const float2* __restrict__ modes, float2* __restrict__ grid, int batch,
+                             size_t mode_stride, size_t grid_stride, const float* __restrict__ scale) {
+  const int b = blockIdx.y;
+  const int nmodes = g.m_out0 * g.m_out1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nmodes; e += gridDim.x * blockDim.x) {
+    const int j0 = e % g.m_out0, j1 = e / g.m_out0;
+    const int b0 = wrap(g.m_lo0 + j0, g.nf0), b1 = wrap(g.m_lo1 + j1, g.nf1);
+    float2 v = modes[b * mode_stride + e];
+    float s = g.corr0[j0] * g.corr1[j1];
+    if (scale) s *= scale[b];
+    grid[b * grid_stride + (size_t)b0 + (size_t)g.nf0 * b1] = make_float2(v.x * s, v.y * s);
+  }
+}
+
+__global__ void extract_kernel(const NufftGrid g, const float2* __restrict__ grid, float2* __restrict__ modes,
+                               size_t grid_stride, size_t mode_stride) {
+  const int b = blockIdx.y;
+  const int nmodes = g.m_out0 * g.m_out1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nmodes; e += gridDim.x * blockDim.x) {
+    const int j0 = e % g.m_out0, j1 = e / g.m_out0;
+    const int b0 = wrap(g.m_lo0 + j0, g.nf0), b1 = wrap(g.m_lo1 + j1, g.nf1);
+    const float2 v = grid[b * grid_stride + (size_t)b0 + (size_t)g.nf0 * b1];
+    const float s = g.corr0[j0] * g.corr1[j1];
+    modes[b * mode_stride + e] = make_float2(v.x * s, v.y * s);
+  }
+}
+
+// One CTA per line of length n (power of two): stride between elements `es`, between lines
+// `ls`; lines = blockIdx.x within batch item blockIdx.y (batch stride `bs`).
+__global__ void fft_pow2_kernel(float2* __restrict__ data, int n, int logn, size_t es, size_t ls, size_t bs,
+                                const float2* __restrict__ tw, int sign) {
+  extern __shared__ float2 buf[];
+  float2* base = data + blockIdx.y * bs + blockIdx.x * ls;
+  // bit-reversed load
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int r = __brev(i) >> (32 - logn);
+    buf[r] = base[(size_t)i * es];
+  }
+  __syncthreads();
+  for (int s = 1; s <= logn; ++s) {
+    const int m = 1 << s, h = m >> 1;
+    for (int t = threadIdx.x; t < n / 2; t += blockDim.x) {
+      const int grp = t / h, pos = t % h;
+      const int i0 = grp * m + pos, i1 = i0 + h;
+      float2 w = tw[(size_t)pos * (n / m)];  // e^{-i 2 pi pos / m}
+      if (sign > 0) w.y = -w.y;
+      const float2 a = buf[i0], b = buf[i1];
+      const float2 bw = make_float2(b.x * w.x - b.y * w.y, b.x * w.y + b.y * w.x);
+      buf[i0] = make_float2(a.x + bw.x, a.y + bw.y);
+      buf[i1] = make_float2(a.x - bw.x, a.y - bw.y);
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) base[(size_t)i * es] = buf[i];
+}
+
+// Direct DFT of one line (any n), e^{sign i 2 pi j k / n}.
+__global__ void dft_line_kernel(float2* __restrict__ data, int n, size_t es, size_t ls, size_t bs,
+                                const float2* __restrict__ tw, int sign) {
+  extern __shared__ float2 buf[];
+  float2* base = data + blockIdx.y * bs + blockIdx.x * ls;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = base[(size_t)i * es];
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    float ar = 0.f, ai = 0.f;
+    for (int j = 0; j < n; ++j) {
+      float2 w = tw[((long long)j * k) % n];
+      if (sign > 0) w.y = -w.y;
+      const float2 a = buf[j];
+      ar = fmaf(a.x, w.x, fmaf(-a.y, w.y, ar));
+      ai = fmaf(a.x, w.y, fmaf(a.y, w.x, ai));
+    }
+    base[(size_t)k * es] = make_float2(ar, ai);  // inputs are in shared memory: no hazard
+  }
+}
+
+// Type 2: out[j] = sum over the w x w taps of grid, for each point of each batch item.
+__global__ void interp_kernel(const NufftGrid g, const float2* __restrict__ grid, const double* __restrict__ u, int npts,
+                              float2* __restrict__ out, size_t grid_stride, size_t out_stride) {
+  const int b = blockIdx.y;
+  const float2* G = grid + b * grid_stride;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npts; j += gridDim.x * blockDim.x) {
+    float k0[kWMax], k1[kWMax];
+    const int a0 = es_taps(u[2 * j], g.nf0, g.w, g.beta, k0);
+    const int a1 = es_taps(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
+    float re = 0.f, im = 0.f;
+    for (int i1 = 0; i1 < g.w; ++i1) {
+      const int c1 = wrap(a1 + i1, g.nf1);
+      const float2* row = G + (size_t)g.nf0 * c1;
+      float rr = 0.f, ri = 0.f;
+      for (int i0 = 0; i0 < g.w; ++i0) {
+        const float2 v = __ldg(row + wrap(a0 + i0, g.nf0));
+        rr = fmaf(v.x, k0[i0], rr);
+        ri = fmaf(v.y, k0[i0], ri);
+      }
+      re = fmaf(rr, k1[i1], re);
+      im = fmaf(ri, k1[i1], im);
+    }
+    out[b * out_stride + j] = make_float2(re, im);
+  }
+}
+
+// Type 1 spreading: grid += w_j * taps (FP32 atomics).
+__global__ void spread_kernel(const NufftGrid g, float2* __restrict__ grid, const double* __restrict__ u, int npts,
+                              const float2* __restrict__ wts, size_t grid_stride, size_t w_stride) {
+  const int b = blockIdx.y;
+  float2* G = grid + b * grid_stride;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npts; j += gridDim.x * blockDim.x) {
+    float k0[kWMax], k1[kWMax];
+    const int a0 = es_taps(u[2 * j], g.nf0, g.w, g.beta, k0);
+    const int a1 = es_taps(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
+    const float2 wv = wts[b * w_stride + j];
+    for (int i1 = 0; i1 < g.w; ++i1) {
+      const int c1 = wrap(a1 + i1, g.nf1);
+      float* row = reinterpret_cast<float*>(G + (size_t)g.nf0 * c1);
+      const float wr = wv.x * k1[i1], wi = wv.y * k1[i1];
+      for (int i0 = 0; i0 < g.w; ++i0) {
+        const int c0 = wrap(a0 + i0, g.nf0);
+        atomicAdd(row + 2 * c0, wr * k0[i0]);
+        atomicAdd(row + 2 * c0 + 1, wi * k0[i0]);
+      }
+    }
+  }
+}
+
+// ---- spiral forwards ---------------------------------------------------------------------------
+// The exact sum (`spiral_kspace_exact`, spiral.rs:107-137): one thread per sample, voxels staged
+// in shared memory in tiles; the k.r + f tau phase in FP64 (nonuniform k), reduced to turns.
+constexpr int kTileVox = 256;
+
+__global__ void __launch_bounds__(256) spiral_exact_kernel(const SpiralExactArgs a) {
+  __shared__ double sx[kTileVox], sy[kTileVox];
+  __shared__ float sr[kTileVox], sph[kTileVox], samp[kTileVox];
+  __shared__ float sm[kTileVox][4];
+  __shared__ float sd[kTileVox][4];
+  __shared__ float sla[kTileVox];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = j < a.npts;
+  double kx = 0, ky = 0;
+  float tau = 0.f;
+  if (ok) {
+    kx = a.k[2 * j] / a.nx;
+    ky = a.k[2 * j + 1] / a.ny;
+    tau = (float)a.tau_ms[j];
+  }
+  const double taus = ok ? a.tau_ms[j] / 1000.0 : 0.0;
+  float re = 0.f, im = 0.f;
+  const int nvox = a.snx * a.sny;
+  for (int v0 = 0; v0 < nvox; v0 += kTileVox) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < kTileVox; t += blockDim.x) {
+      const int i = v0 + t;
+      if (i < nvox) {
+        const int x = i % a.snx, y = i / a.snx;
+        sx[t] = ((double)x - a.sxs - a.xoff) / a.ox;
+        sy[t] = ((double)y - a.sys - a.yoff) / a.oy;
+        sr[t] = a.rate ? a.rate[i] : 0.f;
+        sph[t] = a.phase_turns ? a.phase_turns[i] : 0.f;
+        samp[t] = a.amp[i];
+        sla[t] = a.log_amp ? a.log_amp[i] : 0.f;
+        for (int c = 0; c < 4; ++c) {
+          sm[t][c] = c < a.ncomp ? a.comp[(size_t)c * nvox + i] : 0.f;
+          sd[t][c] = (a.decay && c < a.ncomp) ? a.decay[(size_t)c * nvox + i] : 0.f;
+        }
+      } else {
+        samp[t] = 0.f;
+        sla[t] = 0.f;
+        for (int c = 0; c < 4; ++c) sm[t][c] = sd[t][c] = 0.f;
+        sx[t] = sy[t] = 0.0;
+        sr[t] = sph[t] = 0.f;
+      }
+    }
+    __syncthreads();
+    if (!ok) continue;
+    const int nt = min(kTileVox, nvox - v0);
+    for (int t = 0; t < nt; ++t) {
+      // w = sum_c m_c exp(ln A - tau d_c) under relaxation, sum_c m_c otherwise (spiral.rs:75-80)
+      float w = 0.f;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        if (c < a.ncomp) {
+          const float e = a.relax ? __expf(sla[t] - tau * sd[t][c]) : 1.f;
+          w = fmaf(sm[t][c], e, w);
+        }
+      }
+      if (w == 0.f) continue;
+      double th = kx * sx[t] + ky * sy[t] + (double)sr[t] * taus;
+      th -= rint(th);
+      float thf = (float)th + sph[t];
+      thf -= rintf(thf);
+      float sn, cs;
+      sincospif(2.0f * thf, &sn, &cs);
+      const float amp = samp[t] * w;
+      re = fmaf(amp, cs, re);
+      im = fmaf(amp, sn, im);
+    }
+  }
+  if (ok) a.out[j] = make_float2(re * a.inv_nvox, im * a.inv_nvox);
+}
+
+// Segment images: img_l(r) = x(r) e^{rate(r) tau_l} for every segment l (spiral.rs:174-201).
+__global__ void segment_images_kernel(const float2* __restrict__ x, const float2* __restrict__ rate, int nvox,
+                                      const double* __restrict__ tau_l, int L, float2* __restrict__ out) {
+  const int l = blockIdx.y;
+  const double tl = tau_l[l];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nvox; i += gridDim.x * blockDim.x) {
+    const float2 r = rate[i];
+    const float mag = __expf(r.x * (float)tl);
+    double th = (double)r.y * tl / 6.283185307179586;
+    th -= rint(th);
+    float sn, cs;
+    sincospif(2.0f * (float)th, &sn, &cs);
+    const float2 v = x[i];
+    const float er = mag * cs, ei = mag * sn;
+    out[(size_t)l * nvox + i] = make_float2(v.x * er - v.y * ei, v.x * ei + v.y * er);
+  }
+}
+
+// out_j = stat_j * sum_l b[tau_idx_j][l] * seg[l][j]
+__global__ void segment_combine_kernel(const float2* __restrict__ seg, int npts, int L, const int* __restrict__ tau_idx,
+                                       const double* __restrict__ b, const float2* __restrict__ stat,
+                                       float2* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npts; j += gridDim.x * blockDim.x) {
+    const double* bj = b + (size_t)tau_idx[j] * L * 2;
+    float re = 0.f, im = 0.f;
+    for (int l = 0; l < L; ++l) {
+      const float2 v = seg[(size_t)l * npts + j];
+      const float br = (float)bj[2 * l], bi = (float)bj[2 * l + 1];
+      re = fmaf(br, v.x, fmaf(-bi, v.y, re));
+      im = fmaf(br, v.y, fmaf(bi, v.x, im));
+    }
+    const float2 s = stat[j];
+    out[j] = make_float2(re * s.x - im * s.y, re * s.y + im * s.x);
+  }
+}
+
+}  // namespace
+
+// ---- launchers ------------------------------------------------------------------------------------
+void nufft_fft2(const NufftGrid& g, float2* grid, int batch, int sign, cudaStream_t st) {
+  const size_t gs = (size_t)g.nf0 * g.nf1;
+  // rows (axis 0, contiguous), then columns (axis 1, stride nf0)
+  for (int axis = 0; axis < 2; ++axis) {
+    const int n = axis == 0 ? g.nf0 : g.nf1;
+    const int lines = axis == 0 ? g.nf1 : g.nf0;
+    const size_t es = axis == 0 ? 1 : (size_t)g.nf0;
+    const size_t ls = axis == 0 ? (size_t)g.nf0 : 1;
+    const float2* tw = axis == 0 ? g.tw0 : g.tw1;
+    const int threads = std::min(256, std::max(32, n / 2));
+    dim3 grid_dim(lines, batch);
+    const size_t smem = sizeof(float2) * n;  // n <= 16384: at most 128 KiB
+    if ((n & (n - 1)) == 0) {
+      int logn = 0;
+      while ((1 << logn) < n) ++logn;
+      if (smem > 48 * 1024)
+        cudaFuncSetAttribute(fft_pow2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      fft_pow2_kernel<<<grid_dim, threads, smem, st>>>(grid, n, logn, es, ls, gs, tw, sign);
+    } else {
+      if (smem > 48 * 1024)
+        cudaFuncSetAttribute(dft_line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      dft_line_kernel<<<grid_dim, std::min(256, n), smem, st>>>(grid, n, es, ls, gs, tw, sign);
+    }
+  }
+}
+
+void nufft_type2(const NufftGrid& g, const float2* modes, int batch, size_t mode_stride, const double* u, int npts,
+                 float2* out, size_t out_stride, float2* work, int sign, const float* scale, cudaStream_t st) {
+  const size_t gs = (size_t)g.nf0 * g.nf1;
+  cudaMemsetAsync(work, 0, gs * batch * sizeof(float2), st);
+  dim3 pg((g.m_out0 * g.m_out1 + 255) / 256, batch);
+  place_kernel<<<pg, 256, 0, st>>>(g, modes, work, batch, mode_stride, gs, scale);
+  nufft_fft2(g, work, batch, sign, st);
+  dim3 ig(std::max(1, std::min((npts + 127) / 128, 4096)), batch);
+  interp_kernel<<<ig, 128, 0, st>>>(g, work, u, npts, out, gs, out_stride);
+}
+
+void nufft_type1(const NufftGrid& g, const double* u, int npts, const float2* wts, int batch, size_t w_stride,
+                 float2* modes, size_t mode_stride, float2* work, int sign, cudaStream_t st) {
+  const size_t gs = (size_t)g.nf0 * g.nf1;
+  cudaMemsetAsync(work, 0, gs * batch * sizeof(float2), st);
+  dim3 sg(std::max(1, std::min((npts + 127) / 128, 4096)), batch);
+  spread_kernel<<<sg, 128, 0, st>>>(g, work, u, npts, wts, gs, w_stride);
+  nufft_fft2(g, work, batch, sign, st);
+  dim3 eg((g.m_out0 * g.m_out1 + 255) / 256, batch);
+  extract_kernel<<<eg, 256, 0, st>>>(g, work, modes, gs, mode_stride);
+}
+
+void spiral_exact(const SpiralExactArgs& a, cudaStream_t st) {
+  spiral_exact_kernel<<<(a.npts + 255) / 256, 256, 0, st>>>(a);
+}
+
+void segment_images(const float2* x, const float2* rate, int nvox, const double* tau_l, int L, float2* out,
+                    cudaStream_t st) {
+  dim3 g((nvox + 255) / 256, L);
+  segment_images_kernel<<<g, 256, 0, st>>>(x, rate, nvox, tau_l, L, out);
+}
+
+void segment_combine(const float2* seg, int npts, int L, const int* tau_idx, const double* b, const float2* stat,
+                     float2* out, cudaStream_t st) {
+  segment_combine_kernel<<<(npts + 255) / 256, 256, 0, st>>>(seg, npts, L, tau_idx, b, stat, out);
+}
+
+}  // namespace mrsim

@@ -1,6 +1,7 @@
 // mrsim_oracle.cpp — TEST INFRASTRUCTURE ONLY.  A CPU FP64 restatement of the reference crate's
-// 2D EPI k-space path (Rust `mrsim-acq`, which cannot be compiled in this image: no Rust
-// toolchain).  It is the parity checker for the CUDA library and the timed CPU baseline.  Only
+// 2D EPI k-space path and of its stack-of-spirals pieces (the 2D NUFFT pair, the exact and
+// time-segmented spiral forwards) — Rust `mrsim-acq`, which cannot be compiled in this image: no
+// Rust toolchain.  It is the parity checker for the CUDA library and the timed CPU baseline.  Only
 // `tests/`, `__graft_entry__.smoke()` and `bench.py`'s CPU-baseline / reference arm may load it;
 // the product library never links or calls it.
 //
@@ -1801,6 +1802,233 @@ std::vector<GoldenCase> golden_outputs() {
   return out;
 }
 
+
+// ============================ stack-of-spirals path =========================================
+// `Nufft2` nufft.rs:125-299, FP64.  The fine-grid transform is a separable direct DFT (the
+// reference calls rustfft; a DFT is the same linear map, within rounding).
+struct Nufft2O {
+  size_t n[2], nf[2], w;
+  double beta;
+  int64_t m_lo[2];
+  size_t m_out[2];
+  std::vector<double> corr[2];
+  Nufft2O(const int64_t* n_, const int64_t* m_lo_, const int64_t* m_out_, double tol) {
+    for (int a = 0; a < 2; ++a) {
+      if (!(m_out_[a] > 0 && m_lo_[a] >= -(n_[a] / 2) && m_lo_[a] + m_out_[a] - 1 <= n_[a] / 2))
+        throw Fail("mode band must sit inside the coarse Nyquist band");
+      n[a] = (size_t)n_[a];
+      nf[a] = 2 * n[a];
+      m_lo[a] = m_lo_[a];
+      m_out[a] = (size_t)m_out_[a];
+    }
+    w = (size_t)std::min(16.0, std::max(2.0, std::ceil(-std::log10(tol)) + 1.0));
+    beta = 2.30 * (double)w;
+    for (int a = 0; a < 2; ++a) {  // `deapodization` nufft.rs:113-123
+      double half = (double)w / 2.0;
+      for (size_t j = 0; j < m_out[a]; ++j) {
+        double k = (double)(m_lo[a] + (int64_t)j);
+        double s = psi(0.0);
+        for (double m = 1.0; m < half; m += 1.0) s += 2.0 * psi(m / half) * std::cos(TAU * k * m / (double)nf[a]);
+        corr[a].push_back(1.0 / s);
+      }
+    }
+  }
+  double psi(double z) const { return std::fabs(z) < 1.0 ? std::exp(beta * (std::sqrt(1.0 - z * z) - 1.0)) : 0.0; }
+  int64_t kernel(int a, double u, double* k) const {  // nufft.rs:196-205
+    double half = (double)w / 2.0;
+    double p = std::fmod(2.0 * u, (double)nf[a]);
+    if (p < 0.0) p += (double)nf[a];
+    if (p >= (double)nf[a]) p -= (double)nf[a];
+    int64_t m0 = (int64_t)std::floor(p - half) + 1;
+    for (size_t i = 0; i < w; ++i) k[i] = psi(((double)m0 + (double)i - p) / half);
+    return m0;
+  }
+  static size_t wrap(int64_t m, size_t n) {
+    int64_t r = m % (int64_t)n;
+    return (size_t)(r < 0 ? r + (int64_t)n : r);
+  }
+  void dft2(std::vector<Cx>& g, int sign) const {  // nufft.rs:209-229
+    for (int a = 0; a < 2; ++a) {
+      size_t len = nf[a], lines = nf[1 - a];
+      std::vector<Cx> tw(len), line(len), out(len);
+      for (size_t k = 0; k < len; ++k) tw[k] = ccis((double)sign * TAU * (double)k / (double)len);
+      for (size_t l = 0; l < lines; ++l) {
+        for (size_t i = 0; i < len; ++i) line[i] = a == 0 ? g[i + nf[0] * l] : g[l + nf[0] * i];
+        for (size_t k = 0; k < len; ++k) {
+          Cx acc{0.0, 0.0};
+          for (size_t j = 0; j < len; ++j) acc = cadd(acc, cmul(line[j], tw[(j * k) % len]));
+          out[k] = acc;
+        }
+        for (size_t i = 0; i < len; ++i) (a == 0 ? g[i + nf[0] * l] : g[l + nf[0] * i]) = out[i];
+      }
+    }
+  }
+  std::vector<Cx> type1(const double* u, size_t npts, const Cx* wts, int sign) const {  // nufft.rs:236-262
+    std::vector<Cx> g(nf[0] * nf[1], Cx{0.0, 0.0});
+    std::vector<double> k0(w), k1(w);
+    for (size_t j = 0; j < npts; ++j) {
+      int64_t a0 = kernel(0, u[2 * j], k0.data()), a1 = kernel(1, u[2 * j + 1], k1.data());
+      for (size_t i1 = 0; i1 < w; ++i1) {
+        size_t c1 = wrap(a1 + (int64_t)i1, nf[1]);
+        for (size_t i0 = 0; i0 < w; ++i0) {
+          size_t c0 = wrap(a0 + (int64_t)i0, nf[0]);
+          double v = k0[i0] * k1[i1];
+          g[c0 + nf[0] * c1].re += wts[j].re * v;
+          g[c0 + nf[0] * c1].im += wts[j].im * v;
+        }
+      }
+    }
+    dft2(g, sign);
+    std::vector<Cx> out;
+    for (size_t j1 = 0; j1 < m_out[1]; ++j1)
+      for (size_t j0 = 0; j0 < m_out[0]; ++j0) {
+        size_t b0 = wrap(m_lo[0] + (int64_t)j0, nf[0]), b1 = wrap(m_lo[1] + (int64_t)j1, nf[1]);
+        out.push_back(cscale(g[b0 + nf[0] * b1], corr[0][j0] * corr[1][j1]));
+      }
+    return out;
+  }
+  std::vector<Cx> type2(const Cx* c, const double* u, size_t npts, int sign) const {  // nufft.rs:265-292
+    std::vector<Cx> g(nf[0] * nf[1], Cx{0.0, 0.0});
+    for (size_t j1 = 0; j1 < m_out[1]; ++j1)
+      for (size_t j0 = 0; j0 < m_out[0]; ++j0) {
+        size_t b0 = wrap(m_lo[0] + (int64_t)j0, nf[0]), b1 = wrap(m_lo[1] + (int64_t)j1, nf[1]);
+        g[b0 + nf[0] * b1] = cscale(c[j0 + m_out[0] * j1], corr[0][j0] * corr[1][j1]);
+      }
+    dft2(g, sign);
+    std::vector<Cx> out(npts);
+    std::vector<double> k0(w), k1(w);
+    for (size_t j = 0; j < npts; ++j) {
+      int64_t a0 = kernel(0, u[2 * j], k0.data()), a1 = kernel(1, u[2 * j + 1], k1.data());
+      double re = 0.0, im = 0.0;
+      for (size_t i1 = 0; i1 < w; ++i1) {
+        size_t c1 = wrap(a1 + (int64_t)i1, nf[1]);
+        for (size_t i0 = 0; i0 < w; ++i0) {
+          size_t c0 = wrap(a0 + (int64_t)i0, nf[0]);
+          double v = k0[i0] * k1[i1];
+          re += g[c0 + nf[0] * c1].re * v;
+          im += g[c0 + nf[0] * c1].im * v;
+        }
+      }
+      out[j] = {re, im};
+    }
+    return out;
+  }
+};
+
+// The literal sums the reference pins `Nufft2` against (nufft.rs:370-445).
+std::vector<Cx> nufft2_direct(int type, const int64_t* n, const int64_t* m_lo, const int64_t* m_out, const double* u,
+                              size_t npts, const Cx* in, int sign) {
+  size_t nm = (size_t)(m_out[0] * m_out[1]);
+  std::vector<Cx> out(type == 1 ? nm : npts, Cx{0.0, 0.0});
+  for (size_t j = 0; j < npts; ++j)
+    for (int64_t j1 = 0; j1 < m_out[1]; ++j1)
+      for (int64_t j0 = 0; j0 < m_out[0]; ++j0) {
+        double m0 = (double)(m_lo[0] + j0), m1 = (double)(m_lo[1] + j1);
+        Cx e = ccis((double)sign * TAU * (u[2 * j] * m0 / (double)n[0] + u[2 * j + 1] * m1 / (double)n[1]));
+        size_t mi = (size_t)(j0 + m_out[0] * j1);
+        if (type == 1)
+          out[mi] = cadd(out[mi], cmul(in[j], e));
+        else
+          out[j] = cadd(out[j], cmul(in[mi], e));
+      }
+  return out;
+}
+
+// `statics`, `decay_rate`, `spiral_kspace_exact` spiral.rs:33-137.
+double spiral_decay_rate(const mrsim_slice_input& inp, const mrsim_acquisition& acq, size_t c, size_t i) {
+  double t2 = t2_value(inp.t2[c], i);
+  double tp = inp.t_inhom ? t2_value(inp.t_inhom[c], i) : acq.t_inhom;
+  return 1.0 / t2 + 1.0 / tp;
+}
+
+std::vector<Cx> spiral_kspace_exact(const mrsim_slice_input& inp, const mrsim_acquisition& acq, size_t coil,
+                                    size_t ncoils, const double* k, const double* tau, size_t npts,
+                                    const double* log_amp) {
+  size_t snx = inp.sim[0], sny = inp.sim[1], nx = inp.acq_matrix[0], ny = inp.acq_matrix[1];
+  if (!(snx % nx == 0 && sny % ny == 0)) throw Fail("sim grid must be an integer multiple of the acquired matrix");
+  if (acq.echo != MRSIM_ECHO_SPIN) throw Fail("the spiral train is a spin-echo train");
+  size_t ox = snx / nx, oy = sny / ny, sxs = ox * (nx / 2), sys = oy * (ny / 2);
+  double xoff = ((double)ox - 1.0) / 2.0, yoff = ((double)oy - 1.0) / 2.0;
+  size_t n = snx * sny;
+  std::vector<double> amp(n), phi0(n), xc(n), yc(n), rate(n);
+  for (size_t y = 0; y < sny; ++y)
+    for (size_t x = 0; x < snx; ++x) {
+      size_t i = x + snx * y;
+      double xa = ((double)x - xoff) / (double)ox, ya = ((double)y - yoff) / (double)oy;
+      amp[i] = acq.signal_scale * coil_sensitivity(coil, ncoils, xa, ya, nx, ny);
+      xc[i] = ((double)x - (double)sxs - xoff) / (double)ox;
+      yc[i] = ((double)y - (double)sys - yoff) / (double)oy;
+      phi0[i] = inp.phase0 ? inp.phase0[i] : 0.0;
+      rate[i] = acq.do_distortions ? (double)inp.fmap[i] : 0.0;
+    }
+  std::vector<Cx> out(npts);
+  for (size_t j = 0; j < npts; ++j) {
+    Cx acc{0.0, 0.0};
+    for (size_t i = 0; i < n; ++i) {
+      double w = 0.0;
+      for (size_t c = 0; c < (size_t)inp.ncomp; ++c) {
+        double m = (double)inp.compartments[c][i];
+        if (m != 0.0) {
+          double dec = acq.do_relaxation
+                           ? std::exp((log_amp ? log_amp[i] : 0.0) - tau[j] * spiral_decay_rate(inp, acq, c, i))
+                           : 1.0;
+          w += m * dec;
+        }
+      }
+      if (w == 0.0) continue;
+      double ph = phi0[i] + TAU * (rate[i] * tau[j] / 1000.0 + k[2 * j] * xc[i] / (double)nx +
+                                   k[2 * j + 1] * yc[i] / (double)ny);
+      double a = amp[i] * w;
+      acc = cadd(acc, Cx{a * std::cos(ph), a * std::sin(ph)});
+    }
+    out[j] = cscale(acc, 1.0 / (double)n);
+  }
+  return out;
+}
+
+// `SegmentedForward::apply` with `segment_inputs` (spiral.rs:83-103, 174-201), the L type-2
+// transforms taken as exact sums, for a given plan (tau_l, b).
+std::vector<Cx> spiral_segmented(const mrsim_slice_input& inp, const mrsim_acquisition& acq, size_t coil,
+                                 size_t ncoils, const double* k, const int64_t* tau_idx, size_t npts,
+                                 const double* tau_l, size_t L, const double* b, const double* log_amp,
+                                 bool decay_inside) {
+  size_t snx = inp.sim[0], sny = inp.sim[1], nx = inp.acq_matrix[0], ny = inp.acq_matrix[1];
+  size_t ox = snx / nx, oy = sny / ny, sxs = ox * (nx / 2), sys = oy * (ny / 2);
+  double xoff = ((double)ox - 1.0) / 2.0, yoff = ((double)oy - 1.0) / 2.0;
+  size_t n = snx * sny;
+  std::vector<Cx> x(n);
+  std::vector<double> rd(n), rw(n);
+  for (size_t yy = 0; yy < sny; ++yy)
+    for (size_t xx = 0; xx < snx; ++xx) {
+      size_t i = xx + snx * yy;
+      double xa = ((double)xx - xoff) / (double)ox, ya = ((double)yy - yoff) / (double)oy;
+      double a = acq.signal_scale * coil_sensitivity(coil, ncoils, xa, ya, nx, ny) * (double)inp.compartments[0][i];
+      double d = 0.0;
+      if (decay_inside && acq.do_relaxation) {
+        a *= log_amp ? std::exp(log_amp[i]) : 1.0;
+        d = spiral_decay_rate(inp, acq, 0, i);
+      }
+      x[i] = cscale(ccis(inp.phase0 ? inp.phase0[i] : 0.0), a);
+      rd[i] = -d;
+      rw[i] = TAU * (acq.do_distortions ? (double)inp.fmap[i] : 0.0) / 1000.0;
+    }
+  int64_t nn[2] = {(int64_t)snx, (int64_t)sny}, lo[2] = {-(int64_t)sxs, -(int64_t)sys}, mo[2] = {(int64_t)snx, (int64_t)sny};
+  std::vector<Cx> out(npts, Cx{0.0, 0.0}), seg(n);
+  for (size_t l = 0; l < L; ++l) {
+    for (size_t i = 0; i < n; ++i) seg[i] = cmul(x[i], cscale(ccis(rw[i] * tau_l[l]), std::exp(rd[i] * tau_l[l])));
+    std::vector<Cx> ks = nufft2_direct(2, nn, lo, mo, k, npts, seg.data(), 1);
+    for (size_t j = 0; j < npts; ++j) {
+      Cx bl{b[2 * ((size_t)tau_idx[j] * L + l)], b[2 * ((size_t)tau_idx[j] * L + l) + 1]};
+      out[j] = cadd(out[j], cmul(bl, ks[j]));
+    }
+  }
+  for (size_t j = 0; j < npts; ++j) {
+    Cx st = cscale(ccis(-TAU * (k[2 * j] * xoff / (double)snx + k[2 * j + 1] * yoff / (double)sny)), 1.0 / (double)n);
+    out[j] = cmul(out[j], st);
+  }
+  return out;
+}
+
 thread_local std::string g_err;
 std::vector<GoldenCase>* g_golden = nullptr;
 
@@ -2020,6 +2248,39 @@ int64_t oracle_golden_output(int i, uint32_t* out, int64_t cap) {
   auto& b = (*g_golden)[i].bits;
   if (out && cap >= (int64_t)b.size()) memcpy(out, b.data(), b.size() * 4);
   return (int64_t)b.size();
+}
+
+
+int oracle_nufft2(int32_t type, const int64_t* n, const int64_t* m_lo, const int64_t* m_out, double tol,
+                  const double* u, int64_t npts, const double* in, int32_t sign, double* out) {
+  return guard([&] {
+    Nufft2O f(n, m_lo, m_out, tol);
+    std::vector<Cx> r = type == 1 ? f.type1(u, (size_t)npts, reinterpret_cast<const Cx*>(in), sign)
+                                  : f.type2(reinterpret_cast<const Cx*>(in), u, (size_t)npts, sign);
+    put_cx(r, out);
+  });
+}
+
+int oracle_nufft2_direct(int32_t type, const int64_t* n, const int64_t* m_lo, const int64_t* m_out, const double* u,
+                         int64_t npts, const double* in, int32_t sign, double* out) {
+  return guard([&] { put_cx(nufft2_direct(type, n, m_lo, m_out, u, (size_t)npts, reinterpret_cast<const Cx*>(in), sign), out); });
+}
+
+int oracle_spiral_kspace_exact(const mrsim_slice_input* inp, const mrsim_acquisition* acq, int64_t coil, int64_t ncoils,
+                               const double* k, const double* tau, int64_t npts, const double* log_amp, double* out) {
+  return guard([&] {
+    put_cx(spiral_kspace_exact(*inp, *acq, (size_t)coil, (size_t)ncoils, k, tau, (size_t)npts, log_amp), out);
+  });
+}
+
+int oracle_spiral_segmented(const mrsim_slice_input* inp, const mrsim_acquisition* acq, int64_t coil, int64_t ncoils,
+                            const double* k, const int64_t* tau_idx, int64_t npts, const double* tau_l, int64_t L,
+                            const double* b, const double* log_amp, int32_t decay_inside, double* out) {
+  return guard([&] {
+    put_cx(spiral_segmented(*inp, *acq, (size_t)coil, (size_t)ncoils, k, tau_idx, (size_t)npts, tau_l, (size_t)L, b,
+                            log_amp, decay_inside != 0),
+           out);
+  });
 }
 
 }  // extern "C"

@@ -66,6 +66,16 @@ def lib():
         L.oracle_echo_salt.argtypes = [C.c_uint64]
         L.oracle_coil_sensitivity.restype = C.c_double
         L.oracle_coil_sensitivity.argtypes = [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int64, C.c_int64]
+        i64p = P(C.c_int64)
+        L.oracle_nufft2.argtypes = [C.c_int32, i64p, i64p, i64p, C.c_double, abi.c_f64p, C.c_int64, abi.c_f64p,
+                                    C.c_int32, abi.c_f64p]
+        L.oracle_nufft2_direct.argtypes = [C.c_int32, i64p, i64p, i64p, abi.c_f64p, C.c_int64, abi.c_f64p,
+                                           C.c_int32, abi.c_f64p]
+        L.oracle_spiral_kspace_exact.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), C.c_int64, C.c_int64,
+                                                 abi.c_f64p, abi.c_f64p, C.c_int64, abi.c_f64p, abi.c_f64p]
+        L.oracle_spiral_segmented.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), C.c_int64, C.c_int64,
+                                              abi.c_f64p, i64p, C.c_int64, abi.c_f64p, C.c_int64, abi.c_f64p,
+                                              abi.c_f64p, C.c_int32, abi.c_f64p]
         _lib = L
     return _lib
 
@@ -293,3 +303,66 @@ def acquire_volumes_complex(sim_dims, acq_dims, n_volumes, images, t2, fmap, acq
     res = {"re": re, "im": im}
     res.update(cap)
     return res
+
+
+# ---- stack-of-spirals path -----------------------------------------------------------------------
+def _i64(v):
+    a = np.ascontiguousarray(v, dtype=np.int64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def nufft2(type_: int, n, m_lo, m_out, tol: float, u: np.ndarray, data: np.ndarray, sign: int) -> np.ndarray:
+    """`Nufft2::type1` / `type2` (nufft.rs:225-292) in FP64 (gridding with a direct fine-grid DFT)."""
+    (na, npp), (la, lp), (ma, mp) = _i64(n), _i64(m_lo), _i64(m_out)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 2)
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128).ravel())
+    out = np.zeros(int(ma[0] * ma[1]) if type_ == 1 else len(u), np.complex128)
+    _check(lib().oracle_nufft2(type_, npp, lp, mp, tol, u.ctypes.data_as(abi.c_f64p), len(u),
+                               d.view(np.float64).ctypes.data_as(abi.c_f64p), sign,
+                               out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+    return out
+
+
+def nufft2_direct(type_: int, n, m_lo, m_out, u: np.ndarray, data: np.ndarray, sign: int) -> np.ndarray:
+    """The literal sums of the 2D NUFFT pair (FP64)."""
+    (na, npp), (la, lp), (ma, mp) = _i64(n), _i64(m_lo), _i64(m_out)
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 2)
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128).ravel())
+    out = np.zeros(int(ma[0] * ma[1]) if type_ == 1 else len(u), np.complex128)
+    _check(lib().oracle_nufft2_direct(type_, npp, lp, mp, u.ctypes.data_as(abi.c_f64p), len(u),
+                                      d.view(np.float64).ctypes.data_as(abi.c_f64p), sign,
+                                      out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+    return out
+
+
+def spiral_kspace_exact(inp: SliceInput, acq: Acquisition, coil: int, ncoils: int, k, tau, log_amp=None) -> np.ndarray:
+    """`spiral_kspace_exact` (spiral.rs:107-137), FP64."""
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 2)
+    tau = np.ascontiguousarray(tau, dtype=np.float64)
+    la = keep.f64(np.ravel(log_amp)) if log_amp is not None else None
+    out = np.zeros(len(k), np.complex128)
+    _check(lib().oracle_spiral_kspace_exact(C.byref(s), C.byref(acq.to_c()), coil, ncoils,
+                                            k.ctypes.data_as(abi.c_f64p), tau.ctypes.data_as(abi.c_f64p), len(k), la,
+                                            out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+    return out
+
+
+def spiral_segmented(inp: SliceInput, acq: Acquisition, coil: int, ncoils: int, k, tau_idx, tau_l, b,
+                     log_amp=None, decay_inside=True) -> np.ndarray:
+    """`SegmentedForward::apply` (spiral.rs:174-201) for the plan (tau_l, b), type-2 transforms as
+    exact sums, FP64."""
+    keep = _Keep()
+    s = slice_input_c(inp, keep)
+    k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 2)
+    ti, tip = _i64(tau_idx)
+    tl = np.ascontiguousarray(tau_l, dtype=np.float64)
+    bb = np.ascontiguousarray(np.asarray(b, dtype=np.complex128))
+    la = keep.f64(np.ravel(log_amp)) if log_amp is not None else None
+    out = np.zeros(len(k), np.complex128)
+    _check(lib().oracle_spiral_segmented(C.byref(s), C.byref(acq.to_c()), coil, ncoils, k.ctypes.data_as(abi.c_f64p),
+                                         tip, len(k), tl.ctypes.data_as(abi.c_f64p), len(tl),
+                                         bb.view(np.float64).ctypes.data_as(abi.c_f64p), la, int(bool(decay_inside)),
+                                         out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+    return out
