@@ -383,6 +383,39 @@ int mrsim_spiral_segmented_forward(mrsim_context* ctx, const mrsim_slice_input* 
                                    const double d[2], const double f[2], const double* log_amp,
                                    int32_t decay_inside, float* out, mrsim_tseg_info* info);
 
+/* ---- the stack-of-spirals path: the reconstruction ------------------------------------------ */
+/*
+ * `SpiralRecon` (grid_recon.rs:54-325) of one trajectory k [npts][2] (cycles/FOV) on an n x n
+ * image, FP64 on the device: Pipe-Menon weights (10 iterations), the centre normalization, the
+ * window (window_kind / window_a / window_b as in mrsim_acquisition), the image band, the power
+ * iteration for lambda_hi, then per image `iterations` Chebyshev steps over
+ * [lambda_hi / kappa, lambda_hi] and the residual check.  `SpiralRecon::new` is iterations = 80,
+ * kappa = 100, band_limited = 1.  Sample and image buffers are host (re, im) f64 pairs.
+ */
+typedef struct mrsim_spiral_recon mrsim_spiral_recon;
+
+int mrsim_spiral_recon_create(mrsim_context* ctx, const double* k, int64_t npts, int64_t n,
+                              int32_t window_kind, double window_a, double window_b,
+                              int64_t iterations, double kappa, int32_t band_limited,
+                              mrsim_spiral_recon** out);
+int mrsim_spiral_recon_destroy(mrsim_spiral_recon* rec);
+/* lambda_hi, the power iterations run, and the normalized weights [npts] (any may be NULL). */
+int mrsim_spiral_recon_info(const mrsim_spiral_recon* rec, double* lambda_hi,
+                            int64_t* power_iterations, double* weights);
+/* `gridding` (grid_recon.rs:231): n^2 A^H W d for samples [batch][npts] -> [batch][n*n]. */
+int mrsim_spiral_recon_gridding(mrsim_spiral_recon* rec, const double* samples, int64_t batch,
+                                double* out);
+/* `image` (grid_recon.rs:238-275) of each of `batch` sample sets -> [batch][n*n].  Fails with
+ * the reference's message when a residual grows. */
+int mrsim_spiral_recon_image(mrsim_spiral_recon* rec, const double* samples, int64_t batch,
+                             double* out);
+/* `reconstruct_rings` (grid_recon.rs:285-320) of n_partitions partitions at once: coil_samples
+ * [partition][coil][npts], zsens [partition][coil], coils in rings of `ring` (coil q is element
+ * q % ring); out [partition][n*n].  `reconstruct` is ring = ncoils with zsens all 1. */
+int mrsim_spiral_recon_rings(mrsim_spiral_recon* rec, const double* coil_samples,
+                             int64_t n_partitions, int64_t ncoils, int64_t ring,
+                             const double* zsens, double* out);
+
 #ifdef __cplusplus
 }
 #endif

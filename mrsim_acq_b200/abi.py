@@ -180,6 +180,13 @@ def _declare(lib):
                                                      C.c_int64, c_f64p, C.POINTER(C.c_int64), C.c_int64, c_f64p,
                                                      C.c_int64, C.c_double, c_f64p, c_f64p, c_f64p, C.c_int32,
                                                      c_f32p, C.POINTER(TsegInfo_)]),
+        "mrsim_spiral_recon_create": (C.c_int, [P, c_f64p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double,
+                                                C.c_int64, C.c_double, C.c_int32, C.POINTER(P)]),
+        "mrsim_spiral_recon_destroy": (C.c_int, [P]),
+        "mrsim_spiral_recon_info": (C.c_int, [P, c_f64p, C.POINTER(C.c_int64), c_f64p]),
+        "mrsim_spiral_recon_gridding": (C.c_int, [P, c_f64p, C.c_int64, c_f64p]),
+        "mrsim_spiral_recon_image": (C.c_int, [P, c_f64p, C.c_int64, c_f64p]),
+        "mrsim_spiral_recon_rings": (C.c_int, [P, c_f64p, C.c_int64, C.c_int64, C.c_int64, c_f64p, c_f64p]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -13,6 +13,7 @@
 #include "series.h"
 #include "spiral.h"
 #include "spiral_host.h"
+#include "spiral_recon.h"
 
 namespace {
 thread_local std::string g_last_error;
@@ -65,6 +66,30 @@ int on_ctx(mrsim_context* ctx, F&& f) {
 struct mrsim_epi_operator {
   mrsim::EpiOperator* impl;
 };
+
+struct mrsim_spiral_recon {
+  mrsim::SpiralRecon* impl;
+};
+
+namespace {
+// host (re, im) f64 buffers through the device
+template <class F>
+int recon_call(mrsim_spiral_recon* rec, const double* in, size_t in_elems, double* out, size_t out_elems, F&& f) {
+  if (!rec) return guarded([] { need(nullptr, "reconstruction"); });
+  return on_ctx(rec->impl->ctx, [&] {
+    need(in, "samples");
+    need(out, "out");
+    cudaStream_t st = rec->impl->ctx->stream;
+    mrsim::DevArena T;
+    double2* din = (double2*)T.upload(in, in_elems * 16, st);
+    double2* dout = (double2*)T.alloc(out_elems * 16);
+    f(din, dout);
+    MRSIM_CUDA(cudaMemcpyAsync(out, dout, out_elems * 16, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+}  // namespace
 
 #pragma GCC visibility push(default)
 extern "C" {
@@ -643,6 +668,74 @@ int mrsim_spiral_segmented_forward(mrsim_context* ctx, const mrsim_slice_input* 
       info->grid_err = r.grid_err;
     }
   });
+}
+
+int mrsim_spiral_recon_create(mrsim_context* ctx, const double* k, int64_t npts, int64_t n, int32_t window_kind,
+                              double window_a, double window_b, int64_t iterations, double kappa,
+                              int32_t band_limited, mrsim_spiral_recon** out) {
+  return on_ctx(ctx, [&] {
+    need(out, "out");
+    need(k, "k");
+    if (npts <= 0 || npts > ((int64_t)1 << 28)) mrsim::fail("sample count out of range");
+    if (iterations > 100000) mrsim::fail("Chebyshev iterations out of range");
+    mrsim_acquisition w = mrsim::acquisition_default();
+    w.window_kind = window_kind;
+    w.window_a = window_a;
+    w.window_b = window_b;
+    auto* r = new mrsim::SpiralRecon(ctx, k, (int)npts, (int)n, w, (int)iterations, kappa, band_limited != 0);
+    *out = new mrsim_spiral_recon{r};
+  });
+}
+
+int mrsim_spiral_recon_destroy(mrsim_spiral_recon* rec) {
+  return guarded([&] {
+    if (!rec) return;
+    mrsim_context* ctx = rec->impl->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    MRSIM_CUDA(cudaSetDevice(ctx->device));
+    delete rec->impl;
+    delete rec;
+  });
+}
+
+int mrsim_spiral_recon_info(const mrsim_spiral_recon* rec, double* lambda_hi, int64_t* power_iterations,
+                            double* weights) {
+  return guarded([&] {
+    need(rec, "reconstruction");
+    const mrsim::SpiralRecon* r = rec->impl;
+    if (lambda_hi) *lambda_hi = r->lambda_hi;
+    if (power_iterations) *power_iterations = r->power_iterations;
+    if (weights) std::memcpy(weights, r->w_host.data(), r->w_host.size() * 8);
+  });
+}
+
+int mrsim_spiral_recon_gridding(mrsim_spiral_recon* rec, const double* samples, int64_t batch, double* out) {
+  if (batch <= 0) return guarded([] { mrsim::fail("batch must be positive"); });
+  const size_t np = rec ? (size_t)rec->impl->npts : 0, nn = rec ? (size_t)rec->impl->n * rec->impl->n : 0;
+  return recon_call(rec, samples, np * batch, out, nn * batch,
+                    [&](double2* i, double2* o) { rec->impl->gridding(i, (int)batch, o); });
+}
+
+int mrsim_spiral_recon_image(mrsim_spiral_recon* rec, const double* samples, int64_t batch, double* out) {
+  if (batch <= 0) return guarded([] { mrsim::fail("batch must be positive"); });
+  const size_t np = rec ? (size_t)rec->impl->npts : 0, nn = rec ? (size_t)rec->impl->n * rec->impl->n : 0;
+  return recon_call(rec, samples, np * batch, out, nn * batch, [&](double2* i, double2* o) {
+    for (int64_t b0 = 0; b0 < batch; b0 += mrsim::kMaxBatch) {
+      const int nb = (int)std::min<int64_t>(mrsim::kMaxBatch, batch - b0);
+      rec->impl->images(i + b0 * np, nb, o + b0 * nn);
+    }
+  });
+}
+
+int mrsim_spiral_recon_rings(mrsim_spiral_recon* rec, const double* coil_samples, int64_t n_partitions,
+                             int64_t ncoils, int64_t ring, const double* zsens, double* out) {
+  if (n_partitions <= 0 || ncoils <= 0) return guarded([] { mrsim::fail("partitions and coils must be positive"); });
+  const size_t np = rec ? (size_t)rec->impl->npts : 0, nn = rec ? (size_t)rec->impl->n * rec->impl->n : 0;
+  return recon_call(rec, coil_samples, np * ncoils * n_partitions, out, nn * n_partitions,
+                    [&](double2* i, double2* o) {
+                      need(zsens, "zsens");
+                      rec->impl->rings(i, (int)n_partitions, (int)ncoils, (int)ring, zsens, o);
+                    });
 }
 
 }  // extern "C"

@@ -1,4 +1,5 @@
-// nufft.h — the device NUFFT pair and the spiral forwards (see nufft_kernels.cu, spiral.cpp).
+// nufft.h — the device NUFFT pair, FFTs and the spiral forwards (see nufft_kernels.cu, spiral.cpp,
+// spiral_recon.cpp).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -7,26 +8,54 @@
 
 namespace mrsim {
 
-// One NUFFT geometry (`Nufft2::new`, nufft.rs:162-182): periods n, fine grid nf = 2n, modes
-// m_lo .. m_lo + m_out per axis; device tables corr (1/psi-hat per mode) and tw (e^{-i2pi k/nf}).
-struct NufftGrid {
-  int n0, n1, nf0, nf1, w;
-  float beta;
-  int m_lo0, m_lo1, m_out0, m_out1;
-  const float* corr0;
-  const float* corr1;
-  const float2* tw0;
-  const float2* tw1;
+template <class R>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+template <>
+struct Vec2<double> {
+  using type = double2;
 };
 
-void nufft_fft2(const NufftGrid& g, float2* grid, int batch, int sign, cudaStream_t st);
+// One NUFFT geometry (`Nufft2::new`, nufft.rs:162-182): periods n, fine grid nf = 2n, modes
+// m_lo .. m_lo + m_out per axis; device tables corr (1/psi-hat per mode) and tw (e^{-i2pi k/nf}).
+// R = float for the forwards, double for the reconstruction.
+template <class R>
+struct NufftGridT {
+  using V = typename Vec2<R>::type;
+  int n0, n1, nf0, nf1, w;
+  R beta;
+  int m_lo0, m_lo1, m_out0, m_out1;
+  const R* corr0;
+  const R* corr1;
+  const V* tw0;
+  const V* tw1;
+};
+using NufftGrid = NufftGridT<float>;
+
+// In-place 2D FFT of `batch` grids of n0 x n1 (layout c0 + n0 c1, batch stride n0 n1), sign -1 or
+// +1, unnormalized; tw0 / tw1 hold e^{-i2pi k/n} for each axis.
+template <class V>
+void fft2(V* grid, int n0, int n1, const V* tw0, const V* tw1, int batch, int sign, cudaStream_t st);
+
+template <class R>
+void nufft_fft2(const NufftGridT<R>& g, typename Vec2<R>::type* grid, int batch, int sign, cudaStream_t st) {
+  fft2(grid, g.nf0, g.nf1, g.tw0, g.tw1, batch, sign, st);
+}
+
 // Type 2 (nufft.rs:259-292): out[b][j] = sum_m modes[b][m] e^{sign i2pi (u_j0 m0/n0 + u_j1 m1/n1)},
 // optional per-batch scale; `work` holds batch fine grids.
-void nufft_type2(const NufftGrid& g, const float2* modes, int batch, size_t mode_stride, const double* u, int npts,
-                 float2* out, size_t out_stride, float2* work, int sign, const float* scale, cudaStream_t st);
+template <class R>
+void nufft_type2(const NufftGridT<R>& g, const typename Vec2<R>::type* modes, int batch, size_t mode_stride,
+                 const double* u, int npts, typename Vec2<R>::type* out, size_t out_stride,
+                 typename Vec2<R>::type* work, int sign, const R* scale, cudaStream_t st);
 // Type 1 (nufft.rs:225-256): modes[b][m] = sum_j w[b][j] e^{sign i2pi (...)}.
-void nufft_type1(const NufftGrid& g, const double* u, int npts, const float2* wts, int batch, size_t w_stride,
-                 float2* modes, size_t mode_stride, float2* work, int sign, cudaStream_t st);
+template <class R>
+void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const typename Vec2<R>::type* wts, int batch,
+                 size_t w_stride, typename Vec2<R>::type* modes, size_t mode_stride, typename Vec2<R>::type* work,
+                 int sign, cudaStream_t st);
 
 // The exact spiral sum (`spiral_kspace_exact`, spiral.rs:107-137) of one slice and coil.
 struct SpiralExactArgs {

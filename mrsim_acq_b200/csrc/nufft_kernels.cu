@@ -24,56 +24,77 @@ __device__ __forceinline__ int wrap(int m, int n) {
   return m < 0 ? m + n : m;
 }
 
+template <class R>
+__device__ __forceinline__ typename Vec2<R>::type mk2(R a, R b);
+template <>
+__device__ __forceinline__ float2 mk2<float>(float a, float b) {
+  return make_float2(a, b);
+}
+template <>
+__device__ __forceinline__ double2 mk2<double>(double a, double b) {
+  return make_double2(a, b);
+}
+__device__ __forceinline__ float es_exp(float x) { return __expf(x); }
+__device__ __forceinline__ double es_exp(double x) { return exp(x); }
+
 // First fine cell and the w taps of coordinate u (period n) on a fine grid of nf = 2n cells.
-__device__ __forceinline__ int es_taps(double u, int nf, int w, float beta, float* k) {
+template <class R>
+__device__ __forceinline__ int es_taps(double u, int nf, int w, R beta, R* k) {
   const double half = 0.5 * w;
   double p = fmod(2.0 * u, (double)nf);
   if (p < 0.0) p += nf;
   const int m0 = (int)floor(p - half) + 1;
-  const float ih = (float)(1.0 / half);
+  const R ih = (R)(1.0 / half);
 #pragma unroll 4
   for (int i = 0; i < w; ++i) {
-    const float z = (float)((double)(m0 + i) - p) * ih;
-    k[i] = fabsf(z) < 1.0f ? __expf(beta * (sqrtf(1.0f - z * z) - 1.0f)) : 0.0f;
+    const R z = (R)((double)(m0 + i) - p) * ih;
+    k[i] = fabs(z) < (R)1 ? es_exp(beta * (sqrt((R)1 - z * z) - (R)1)) : (R)0;
   }
   return m0;
 }
 
 constexpr int kWMax = 16;
 
-__global__ void place_kernel(const NufftGrid g, const float2* __restrict__ modes, float2* __restrict__ grid, int batch,
-                             size_t mode_stride, size_t grid_stride, const float* __restrict__ scale) {
+template <class R>
+__global__ void place_kernel(const NufftGridT<R> g, const typename Vec2<R>::type* __restrict__ modes,
+                             typename Vec2<R>::type* __restrict__ grid, int batch, size_t mode_stride,
+                             size_t grid_stride, const R* __restrict__ scale) {
+  using V = typename Vec2<R>::type;
   const int b = blockIdx.y;
   const int nmodes = g.m_out0 * g.m_out1;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nmodes; e += gridDim.x * blockDim.x) {
     const int j0 = e % g.m_out0, j1 = e / g.m_out0;
     const int b0 = wrap(g.m_lo0 + j0, g.nf0), b1 = wrap(g.m_lo1 + j1, g.nf1);
-    float2 v = modes[b * mode_stride + e];
-    float s = g.corr0[j0] * g.corr1[j1];
+    V v = modes[b * mode_stride + e];
+    R s = g.corr0[j0] * g.corr1[j1];
     if (scale) s *= scale[b];
-    grid[b * grid_stride + (size_t)b0 + (size_t)g.nf0 * b1] = make_float2(v.x * s, v.y * s);
+    grid[b * grid_stride + (size_t)b0 + (size_t)g.nf0 * b1] = mk2<R>(v.x * s, v.y * s);
   }
 }
 
-__global__ void extract_kernel(const NufftGrid g, const float2* __restrict__ grid, float2* __restrict__ modes,
-                               size_t grid_stride, size_t mode_stride) {
+template <class R>
+__global__ void extract_kernel(const NufftGridT<R> g, const typename Vec2<R>::type* __restrict__ grid,
+                               typename Vec2<R>::type* __restrict__ modes, size_t grid_stride, size_t mode_stride) {
+  using V = typename Vec2<R>::type;
   const int b = blockIdx.y;
   const int nmodes = g.m_out0 * g.m_out1;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nmodes; e += gridDim.x * blockDim.x) {
     const int j0 = e % g.m_out0, j1 = e / g.m_out0;
     const int b0 = wrap(g.m_lo0 + j0, g.nf0), b1 = wrap(g.m_lo1 + j1, g.nf1);
-    const float2 v = grid[b * grid_stride + (size_t)b0 + (size_t)g.nf0 * b1];
-    const float s = g.corr0[j0] * g.corr1[j1];
-    modes[b * mode_stride + e] = make_float2(v.x * s, v.y * s);
+    const V v = grid[b * grid_stride + (size_t)b0 + (size_t)g.nf0 * b1];
+    const R s = g.corr0[j0] * g.corr1[j1];
+    modes[b * mode_stride + e] = mk2<R>(v.x * s, v.y * s);
   }
 }
 
 // One CTA per line of length n (power of two): stride between elements `es`, between lines
 // `ls`; lines = blockIdx.x within batch item blockIdx.y (batch stride `bs`).
-__global__ void fft_pow2_kernel(float2* __restrict__ data, int n, int logn, size_t es, size_t ls, size_t bs,
-                                const float2* __restrict__ tw, int sign) {
-  extern __shared__ float2 buf[];
-  float2* base = data + blockIdx.y * bs + blockIdx.x * ls;
+template <class V>
+__global__ void fft_pow2_kernel(V* __restrict__ data, int n, int logn, size_t es, size_t ls, size_t bs,
+                                const V* __restrict__ tw, int sign) {
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V* buf = reinterpret_cast<V*>(fft_smem);
+  V* base = data + blockIdx.y * bs + blockIdx.x * ls;
   // bit-reversed load
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const int r = __brev(i) >> (32 - logn);
@@ -85,12 +106,19 @@ __global__ void fft_pow2_kernel(float2* __restrict__ data, int n, int logn, size
     for (int t = threadIdx.x; t < n / 2; t += blockDim.x) {
       const int grp = t / h, pos = t % h;
       const int i0 = grp * m + pos, i1 = i0 + h;
-      float2 w = tw[(size_t)pos * (n / m)];  // e^{-i 2 pi pos / m}
+      V w = tw[(size_t)pos * (n / m)];  // e^{-i 2 pi pos / m}
       if (sign > 0) w.y = -w.y;
-      const float2 a = buf[i0], b = buf[i1];
-      const float2 bw = make_float2(b.x * w.x - b.y * w.y, b.x * w.y + b.y * w.x);
-      buf[i0] = make_float2(a.x + bw.x, a.y + bw.y);
-      buf[i1] = make_float2(a.x - bw.x, a.y - bw.y);
+      const V a = buf[i0], b = buf[i1];
+      V bw;
+      bw.x = b.x * w.x - b.y * w.y;
+      bw.y = b.x * w.y + b.y * w.x;
+      V s0, s1;
+      s0.x = a.x + bw.x;
+      s0.y = a.y + bw.y;
+      s1.x = a.x - bw.x;
+      s1.y = a.y - bw.y;
+      buf[i0] = s0;
+      buf[i1] = s1;
     }
     __syncthreads();
   }
@@ -98,65 +126,76 @@ __global__ void fft_pow2_kernel(float2* __restrict__ data, int n, int logn, size
 }
 
 // Direct DFT of one line (any n), e^{sign i 2 pi j k / n}.
-__global__ void dft_line_kernel(float2* __restrict__ data, int n, size_t es, size_t ls, size_t bs,
-                                const float2* __restrict__ tw, int sign) {
-  extern __shared__ float2 buf[];
-  float2* base = data + blockIdx.y * bs + blockIdx.x * ls;
+template <class V>
+__global__ void dft_line_kernel(V* __restrict__ data, int n, size_t es, size_t ls, size_t bs, const V* __restrict__ tw,
+                                int sign) {
+  extern __shared__ __align__(16) unsigned char fft_smem[];
+  V* buf = reinterpret_cast<V*>(fft_smem);
+  V* base = data + blockIdx.y * bs + blockIdx.x * ls;
   for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = base[(size_t)i * es];
   __syncthreads();
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    float ar = 0.f, ai = 0.f;
+    decltype(V().x) ar = 0, ai = 0;
     for (int j = 0; j < n; ++j) {
-      float2 w = tw[((long long)j * k) % n];
+      V w = tw[((long long)j * k) % n];
       if (sign > 0) w.y = -w.y;
-      const float2 a = buf[j];
-      ar = fmaf(a.x, w.x, fmaf(-a.y, w.y, ar));
-      ai = fmaf(a.x, w.y, fmaf(a.y, w.x, ai));
+      const V a = buf[j];
+      ar = fma(a.x, w.x, fma(-a.y, w.y, ar));
+      ai = fma(a.x, w.y, fma(a.y, w.x, ai));
     }
-    base[(size_t)k * es] = make_float2(ar, ai);  // inputs are in shared memory: no hazard
+    V o;
+    o.x = ar;
+    o.y = ai;
+    base[(size_t)k * es] = o;  // inputs are in shared memory: no hazard
   }
 }
 
 // Type 2: out[j] = sum over the w x w taps of grid, for each point of each batch item.
-__global__ void interp_kernel(const NufftGrid g, const float2* __restrict__ grid, const double* __restrict__ u, int npts,
-                              float2* __restrict__ out, size_t grid_stride, size_t out_stride) {
+template <class R>
+__global__ void interp_kernel(const NufftGridT<R> g, const typename Vec2<R>::type* __restrict__ grid,
+                              const double* __restrict__ u, int npts, typename Vec2<R>::type* __restrict__ out,
+                              size_t grid_stride, size_t out_stride) {
+  using V = typename Vec2<R>::type;
   const int b = blockIdx.y;
-  const float2* G = grid + b * grid_stride;
+  const V* G = grid + b * grid_stride;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npts; j += gridDim.x * blockDim.x) {
-    float k0[kWMax], k1[kWMax];
-    const int a0 = es_taps(u[2 * j], g.nf0, g.w, g.beta, k0);
-    const int a1 = es_taps(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
-    float re = 0.f, im = 0.f;
+    R k0[kWMax], k1[kWMax];
+    const int a0 = es_taps<R>(u[2 * j], g.nf0, g.w, g.beta, k0);
+    const int a1 = es_taps<R>(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
+    R re = 0, im = 0;
     for (int i1 = 0; i1 < g.w; ++i1) {
       const int c1 = wrap(a1 + i1, g.nf1);
-      const float2* row = G + (size_t)g.nf0 * c1;
-      float rr = 0.f, ri = 0.f;
+      const V* row = G + (size_t)g.nf0 * c1;
+      R rr = 0, ri = 0;
       for (int i0 = 0; i0 < g.w; ++i0) {
-        const float2 v = __ldg(row + wrap(a0 + i0, g.nf0));
-        rr = fmaf(v.x, k0[i0], rr);
-        ri = fmaf(v.y, k0[i0], ri);
+        const V v = __ldg(row + wrap(a0 + i0, g.nf0));
+        rr = fma(v.x, k0[i0], rr);
+        ri = fma(v.y, k0[i0], ri);
       }
-      re = fmaf(rr, k1[i1], re);
-      im = fmaf(ri, k1[i1], im);
+      re = fma(rr, k1[i1], re);
+      im = fma(ri, k1[i1], im);
     }
-    out[b * out_stride + j] = make_float2(re, im);
+    out[b * out_stride + j] = mk2<R>(re, im);
   }
 }
 
-// Type 1 spreading: grid += w_j * taps (FP32 atomics).
-__global__ void spread_kernel(const NufftGrid g, float2* __restrict__ grid, const double* __restrict__ u, int npts,
-                              const float2* __restrict__ wts, size_t grid_stride, size_t w_stride) {
+// Type 1 spreading: grid += w_j * taps (atomics).
+template <class R>
+__global__ void spread_kernel(const NufftGridT<R> g, typename Vec2<R>::type* __restrict__ grid,
+                              const double* __restrict__ u, int npts, const typename Vec2<R>::type* __restrict__ wts,
+                              size_t grid_stride, size_t w_stride) {
+  using V = typename Vec2<R>::type;
   const int b = blockIdx.y;
-  float2* G = grid + b * grid_stride;
+  V* G = grid + b * grid_stride;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npts; j += gridDim.x * blockDim.x) {
-    float k0[kWMax], k1[kWMax];
-    const int a0 = es_taps(u[2 * j], g.nf0, g.w, g.beta, k0);
-    const int a1 = es_taps(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
-    const float2 wv = wts[b * w_stride + j];
+    R k0[kWMax], k1[kWMax];
+    const int a0 = es_taps<R>(u[2 * j], g.nf0, g.w, g.beta, k0);
+    const int a1 = es_taps<R>(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
+    const V wv = wts[b * w_stride + j];
     for (int i1 = 0; i1 < g.w; ++i1) {
       const int c1 = wrap(a1 + i1, g.nf1);
-      float* row = reinterpret_cast<float*>(G + (size_t)g.nf0 * c1);
-      const float wr = wv.x * k1[i1], wi = wv.y * k1[i1];
+      R* row = reinterpret_cast<R*>(G + (size_t)g.nf0 * c1);
+      const R wr = wv.x * k1[i1], wi = wv.y * k1[i1];
       for (int i0 = 0; i0 < g.w; ++i0) {
         const int c0 = wrap(a0 + i0, g.nf0);
         atomicAdd(row + 2 * c0, wr * k0[i0]);
@@ -280,53 +319,71 @@ __global__ void segment_combine_kernel(const float2* __restrict__ seg, int npts,
 }  // namespace
 
 // ---- launchers ------------------------------------------------------------------------------------
-void nufft_fft2(const NufftGrid& g, float2* grid, int batch, int sign, cudaStream_t st) {
-  const size_t gs = (size_t)g.nf0 * g.nf1;
-  // rows (axis 0, contiguous), then columns (axis 1, stride nf0)
+template <class V>
+void fft2(V* grid, int n0, int n1, const V* tw0, const V* tw1, int batch, int sign, cudaStream_t st) {
+  const size_t gs = (size_t)n0 * n1;
+  // rows (axis 0, contiguous), then columns (axis 1, stride n0)
   for (int axis = 0; axis < 2; ++axis) {
-    const int n = axis == 0 ? g.nf0 : g.nf1;
-    const int lines = axis == 0 ? g.nf1 : g.nf0;
-    const size_t es = axis == 0 ? 1 : (size_t)g.nf0;
-    const size_t ls = axis == 0 ? (size_t)g.nf0 : 1;
-    const float2* tw = axis == 0 ? g.tw0 : g.tw1;
+    const int n = axis == 0 ? n0 : n1;
+    const int lines = axis == 0 ? n1 : n0;
+    const size_t es = axis == 0 ? 1 : (size_t)n0;
+    const size_t ls = axis == 0 ? (size_t)n0 : 1;
+    const V* tw = axis == 0 ? tw0 : tw1;
     const int threads = std::min(256, std::max(32, n / 2));
     dim3 grid_dim(lines, batch);
-    const size_t smem = sizeof(float2) * n;  // n <= 16384: at most 128 KiB
+    const size_t smem = sizeof(V) * n;  // n <= 16384: at most 256 KiB in FP64, refused above 227 KiB
     if ((n & (n - 1)) == 0) {
       int logn = 0;
       while ((1 << logn) < n) ++logn;
       if (smem > 48 * 1024)
-        cudaFuncSetAttribute(fft_pow2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      fft_pow2_kernel<<<grid_dim, threads, smem, st>>>(grid, n, logn, es, ls, gs, tw, sign);
+        cudaFuncSetAttribute(fft_pow2_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      fft_pow2_kernel<V><<<grid_dim, threads, smem, st>>>(grid, n, logn, es, ls, gs, tw, sign);
     } else {
       if (smem > 48 * 1024)
-        cudaFuncSetAttribute(dft_line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      dft_line_kernel<<<grid_dim, std::min(256, n), smem, st>>>(grid, n, es, ls, gs, tw, sign);
+        cudaFuncSetAttribute(dft_line_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      dft_line_kernel<V><<<grid_dim, std::min(256, n), smem, st>>>(grid, n, es, ls, gs, tw, sign);
     }
   }
 }
+template void fft2<float2>(float2*, int, int, const float2*, const float2*, int, int, cudaStream_t);
+template void fft2<double2>(double2*, int, int, const double2*, const double2*, int, int, cudaStream_t);
 
-void nufft_type2(const NufftGrid& g, const float2* modes, int batch, size_t mode_stride, const double* u, int npts,
-                 float2* out, size_t out_stride, float2* work, int sign, const float* scale, cudaStream_t st) {
+template <class R>
+void nufft_type2(const NufftGridT<R>& g, const typename Vec2<R>::type* modes, int batch, size_t mode_stride,
+                 const double* u, int npts, typename Vec2<R>::type* out, size_t out_stride,
+                 typename Vec2<R>::type* work, int sign, const R* scale, cudaStream_t st) {
+  using V = typename Vec2<R>::type;
   const size_t gs = (size_t)g.nf0 * g.nf1;
-  cudaMemsetAsync(work, 0, gs * batch * sizeof(float2), st);
+  cudaMemsetAsync(work, 0, gs * batch * sizeof(V), st);
   dim3 pg((g.m_out0 * g.m_out1 + 255) / 256, batch);
-  place_kernel<<<pg, 256, 0, st>>>(g, modes, work, batch, mode_stride, gs, scale);
+  place_kernel<R><<<pg, 256, 0, st>>>(g, modes, work, batch, mode_stride, gs, scale);
   nufft_fft2(g, work, batch, sign, st);
   dim3 ig(std::max(1, std::min((npts + 127) / 128, 4096)), batch);
-  interp_kernel<<<ig, 128, 0, st>>>(g, work, u, npts, out, gs, out_stride);
+  interp_kernel<R><<<ig, 128, 0, st>>>(g, work, u, npts, out, gs, out_stride);
 }
 
-void nufft_type1(const NufftGrid& g, const double* u, int npts, const float2* wts, int batch, size_t w_stride,
-                 float2* modes, size_t mode_stride, float2* work, int sign, cudaStream_t st) {
+template <class R>
+void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const typename Vec2<R>::type* wts, int batch,
+                 size_t w_stride, typename Vec2<R>::type* modes, size_t mode_stride, typename Vec2<R>::type* work,
+                 int sign, cudaStream_t st) {
+  using V = typename Vec2<R>::type;
   const size_t gs = (size_t)g.nf0 * g.nf1;
-  cudaMemsetAsync(work, 0, gs * batch * sizeof(float2), st);
+  cudaMemsetAsync(work, 0, gs * batch * sizeof(V), st);
   dim3 sg(std::max(1, std::min((npts + 127) / 128, 4096)), batch);
-  spread_kernel<<<sg, 128, 0, st>>>(g, work, u, npts, wts, gs, w_stride);
+  spread_kernel<R><<<sg, 128, 0, st>>>(g, work, u, npts, wts, gs, w_stride);
   nufft_fft2(g, work, batch, sign, st);
   dim3 eg((g.m_out0 * g.m_out1 + 255) / 256, batch);
-  extract_kernel<<<eg, 256, 0, st>>>(g, work, modes, gs, mode_stride);
+  extract_kernel<R><<<eg, 256, 0, st>>>(g, work, modes, gs, mode_stride);
 }
+
+template void nufft_type2<float>(const NufftGridT<float>&, const float2*, int, size_t, const double*, int, float2*,
+                                 size_t, float2*, int, const float*, cudaStream_t);
+template void nufft_type2<double>(const NufftGridT<double>&, const double2*, int, size_t, const double*, int, double2*,
+                                  size_t, double2*, int, const double*, cudaStream_t);
+template void nufft_type1<float>(const NufftGridT<float>&, const double*, int, const float2*, int, size_t, float2*,
+                                 size_t, float2*, int, cudaStream_t);
+template void nufft_type1<double>(const NufftGridT<double>&, const double*, int, const double2*, int, size_t,
+                                  double2*, size_t, double2*, int, cudaStream_t);
 
 void spiral_exact(const SpiralExactArgs& a, cudaStream_t st) {
   spiral_exact_kernel<<<(a.npts + 255) / 256, 256, 0, st>>>(a);

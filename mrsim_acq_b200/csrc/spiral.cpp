@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 
 #include "driver.h"
 #include "host_tables.h"
@@ -21,58 +22,74 @@ int nufft_width(double tol) {  // nufft.rs:48, 165
 }
 
 // 1/psi-hat(k) of the modes m_lo .. m_lo + m_out on nf fine cells (`deapodization`, nufft.rs:113-123)
-static std::vector<float> deapodization(int nf, int w, double beta, int m_lo, int m_out) {
+static std::vector<double> deapodization(int nf, int w, double beta, int m_lo, int m_out) {
   const double half = w / 2.0;
   auto psi = [&](double z) { return std::fabs(z) < 1.0 ? std::exp(beta * (std::sqrt(1.0 - z * z) - 1.0)) : 0.0; };
-  std::vector<float> c(m_out);
+  std::vector<double> c(m_out);
   for (int j = 0; j < m_out; ++j) {
     const double k = (double)(m_lo + j);
     double s = psi(0.0);
     for (double m = 1.0; m < half; m += 1.0) s += 2.0 * psi(m / half) * std::cos(kTau * k * m / nf);
-    c[j] = (float)(1.0 / s);
+    c[j] = 1.0 / s;
   }
   return c;
 }
 
-NufftGrid make_nufft(DevArena& A, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
-                     cudaStream_t st) {
+// e^{-i2pi k/n}, k = 0..n-1, on the device in precision R.
+template <class R>
+const void* upload_twiddles(DevArena& A, int n, cudaStream_t st) {
+  using V = typename Vec2<R>::type;
+  std::vector<V> t(n);
+  for (int k = 0; k < n; ++k) {
+    t[k].x = (R)std::cos(-kTau * k / n);
+    t[k].y = (R)std::sin(-kTau * k / n);
+  }
+  return A.upload(t.data(), t.size() * sizeof(V), st);
+}
+template const void* upload_twiddles<float>(DevArena&, int, cudaStream_t);
+template const void* upload_twiddles<double>(DevArena&, int, cudaStream_t);
+
+template <class R>
+NufftGridT<R> make_nufft(DevArena& A, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
+                         cudaStream_t st) {
+  using V = typename Vec2<R>::type;
   if (m_out0 <= 0 || m_out1 <= 0 || m_lo0 < -(n0 / 2) || m_lo0 + m_out0 - 1 > n0 / 2 || m_lo1 < -(n1 / 2) ||
       m_lo1 + m_out1 - 1 > n1 / 2)
     fail("mode band must sit inside the coarse Nyquist band");
-  if (n0 <= 0 || n1 <= 0 || n0 > 8192 || n1 > 8192) fail("NUFFT period must be in 1..8192");
-  NufftGrid g;
+  const int n_max = sizeof(R) == 8 ? 4096 : 8192;  // the fine-grid line must fit in shared memory
+  if (n0 <= 0 || n1 <= 0 || n0 > n_max || n1 > n_max)
+    fail("NUFFT period must be in 1.." + std::to_string(n_max));
+  NufftGridT<R> g;
   std::memset(&g, 0, sizeof g);
   g.n0 = n0;
   g.n1 = n1;
   g.nf0 = 2 * n0;
   g.nf1 = 2 * n1;
   g.w = nufft_width(tol);
-  g.beta = (float)(2.30 * g.w);
+  g.beta = (R)(2.30 * g.w);
   g.m_lo0 = m_lo0;
   g.m_lo1 = m_lo1;
   g.m_out0 = m_out0;
   g.m_out1 = m_out1;
   const double beta = 2.30 * g.w;
-  auto c0 = deapodization(g.nf0, g.w, beta, m_lo0, m_out0);
-  auto c1 = deapodization(g.nf1, g.w, beta, m_lo1, m_out1);
-  g.corr0 = (const float*)A.upload(c0.data(), c0.size() * 4, st);
-  g.corr1 = (const float*)A.upload(c1.data(), c1.size() * 4, st);
-  auto tw = [&](int n) {
-    std::vector<float2> t(n);
-    for (int k = 0; k < n; ++k) t[k] = make_float2((float)std::cos(-kTau * k / n), (float)std::sin(-kTau * k / n));
-    return (const float2*)A.upload(t.data(), t.size() * sizeof(float2), st);
-  };
-  g.tw0 = tw(g.nf0);
-  g.tw1 = g.nf1 == g.nf0 ? g.tw0 : tw(g.nf1);
+  auto cast = [](const std::vector<double>& v) { return std::vector<R>(v.begin(), v.end()); };
+  auto c0 = cast(deapodization(g.nf0, g.w, beta, m_lo0, m_out0));
+  auto c1 = cast(deapodization(g.nf1, g.w, beta, m_lo1, m_out1));
+  g.corr0 = (const R*)A.upload(c0.data(), c0.size() * sizeof(R), st);
+  g.corr1 = (const R*)A.upload(c1.data(), c1.size() * sizeof(R), st);
+  g.tw0 = (const V*)upload_twiddles<R>(A, g.nf0, st);
+  g.tw1 = g.nf1 == g.nf0 ? g.tw0 : (const V*)upload_twiddles<R>(A, g.nf1, st);
   return g;
 }
+template NufftGridT<float> make_nufft<float>(DevArena&, int, int, int, int, int, int, double, cudaStream_t);
+template NufftGridT<double> make_nufft<double>(DevArena&, int, int, int, int, int, int, double, cudaStream_t);
 
 // ---- host-buffer NUFFT pair -----------------------------------------------------------------------
 void nufft2_host(mrsim_context* ctx, int type, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
                  const double* u, int npts, const float* in, int sign, float* out) {
   cudaStream_t st = ctx->stream;
   DevArena A;
-  NufftGrid g = make_nufft(A, n0, n1, m_lo0, m_lo1, m_out0, m_out1, tol, st);
+  NufftGrid g = make_nufft<float>(A, n0, n1, m_lo0, m_lo1, m_out0, m_out1, tol, st);
   const size_t nm = (size_t)m_out0 * m_out1;
   if (npts == 0) {  // no points: type 2 has no values, type 1 all-zero modes
     if (type == 1) std::memset(out, 0, nm * sizeof(float2));
@@ -84,13 +101,13 @@ void nufft2_host(mrsim_context* ctx, int type, int n0, int n1, int m_lo0, int m_
   if (type == 2) {
     const float2* dm = (const float2*)A.upload(in, nm * sizeof(float2), st);
     float2* dout = (float2*)A.alloc((size_t)npts * sizeof(float2));
-    nufft_type2(g, dm, 1, nm, du, npts, dout, npts, work, sign, nullptr, st);
+    nufft_type2<float>(g, dm, 1, nm, du, npts, dout, npts, work, sign, nullptr, st);
     MRSIM_CUDA(cudaGetLastError());
     MRSIM_CUDA(cudaMemcpyAsync(out, dout, (size_t)npts * sizeof(float2), cudaMemcpyDeviceToHost, st));
   } else {
     const float2* dw = (const float2*)A.upload(in, (size_t)npts * sizeof(float2), st);
     float2* dm = (float2*)A.alloc(nm * sizeof(float2));
-    nufft_type1(g, du, npts, dw, 1, npts, dm, nm, work, sign, st);
+    nufft_type1<float>(g, du, npts, dw, 1, npts, dm, nm, work, sign, st);
     MRSIM_CUDA(cudaGetLastError());
     MRSIM_CUDA(cudaMemcpyAsync(out, dm, nm * sizeof(float2), cudaMemcpyDeviceToHost, st));
   }
@@ -236,7 +253,7 @@ SegmentedInfo spiral_segmented_host(mrsim_context* ctx, const mrsim_slice_input&
     tidx[j] = (int)tau_idx[j];
   }
   DevArena A;
-  NufftGrid g = make_nufft(A, snx, sny, -sxs, -sys, snx, sny, 1e-12, st);
+  NufftGrid g = make_nufft<float>(A, snx, sny, -sxs, -sys, snx, sny, 1e-12, st);
   const float2* dx = (const float2*)A.upload(x.data(), n * sizeof(float2), st);
   const float2* drate = (const float2*)A.upload(rate.data(), n * sizeof(float2), st);
   const double* dtl = (const double*)A.upload(plan.tau_l.data(), plan.tau_l.size() * 8, st);
@@ -245,7 +262,7 @@ SegmentedInfo spiral_segmented_host(mrsim_context* ctx, const mrsim_slice_input&
   const double* du = (const double*)A.upload(k, (size_t)npts * 2 * 8, st);
   float2* seg = (float2*)A.alloc((size_t)L * npts * sizeof(float2));
   float2* work = (float2*)A.alloc((size_t)L * g.nf0 * g.nf1 * sizeof(float2));
-  nufft_type2(g, imgs, L, n, du, npts, seg, npts, work, 1, nullptr, st);
+  nufft_type2<float>(g, imgs, L, n, du, npts, seg, npts, work, 1, nullptr, st);
   const double* db = (const double*)A.upload(plan.b.data(), plan.b.size() * 8, st);
   const float2* dstat = (const float2*)A.upload(stat.data(), stat.size() * sizeof(float2), st);
   const int* dti = (const int*)A.upload(tidx.data(), tidx.size() * 4, st);

@@ -10,8 +10,11 @@
 namespace mrsim {
 
 int nufft_width(double tol);
-NufftGrid make_nufft(DevArena& A, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
-                     cudaStream_t st);
+template <class R>
+NufftGridT<R> make_nufft(DevArena& A, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
+                         cudaStream_t st);
+template <class R>
+const void* upload_twiddles(DevArena& A, int n, cudaStream_t st);
 void nufft2_host(mrsim_context* ctx, int type, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
                  const double* u, int npts, const float* in, int sign, float* out);
 void spiral_exact_host(mrsim_context* ctx, const mrsim_slice_input& inp, const mrsim_acquisition& acq, int coil,

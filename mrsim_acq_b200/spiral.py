@@ -1,8 +1,9 @@
 """Python mirror of the reference's stack-of-spirals pieces, over the C ABI.
 
 `spiral_tau_c` / `spiral_trajectory` (readout.rs:564-620), `tseg.plan` (tseg.rs:230-289),
-`epg_cpmg` (epg.rs:101-125), the 2D NUFFT pair `Nufft2` (nufft.rs:125-299) and the spiral
-forwards `spiral_kspace_exact` / `SegmentedForward` (spiral.rs:83-201).  Host plans run in the
+`epg_cpmg` (epg.rs:101-125), the 2D NUFFT pair `Nufft2` (nufft.rs:125-299), the spiral
+forwards `spiral_kspace_exact` / `SegmentedForward` (spiral.rs:83-201) and the reconstruction
+`SpiralRecon` (grid_recon.rs:54-325).  Host plans run in the
 library's C++; the NUFFT pair and the forwards run on the device (no CPU path).
 """
 from __future__ import annotations
@@ -15,7 +16,7 @@ import numpy as np
 
 from . import abi
 from .abi import check, lib
-from .api import Acquisition, Context, SliceInput, _Keep, default_context, slice_input_c
+from .api import Acquisition, Context, KspaceWindow, SliceInput, _Keep, default_context, slice_input_c
 
 
 def spiral_tau_c(nx: int, interleaves: int, readout_ms: float, dwell_ms: float, radial_oversampling: float) -> float:
@@ -186,3 +187,105 @@ def spiral_segmented_forward(inp: SliceInput, acq: Acquisition, coil: int, ncoil
                                                out.view(np.float32).ctypes.data_as(abi.c_f32p), C.byref(info)))
     return out, {"l": int(info.l), "m": int(info.m), "bound": info.bound, "b_sum": info.b_sum,
                  "grid_err": info.grid_err}
+
+
+# ---- the reconstruction ----------------------------------------------------------------------------
+LS_ITERATIONS = 80
+LS_KAPPA = 100.0
+
+
+def _c128(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128))
+
+
+class SpiralRecon:
+    """`SpiralRecon` (grid_recon.rs:54-325) on the device, FP64.  Images are complex128 [n, n]
+    (layout x + n y)."""
+
+    def __init__(self, k: np.ndarray, n: int, window: Optional[KspaceWindow] = None,
+                 iterations: int = LS_ITERATIONS, kappa: float = LS_KAPPA, band_limited: bool = True,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 2)
+        self.n = int(n)
+        window = window or KspaceWindow.none()
+        h = C.c_void_p()
+        check(lib().mrsim_spiral_recon_create(self.ctx.handle, self.k.ctypes.data_as(abi.c_f64p), len(self.k), self.n,
+                                              int(window.kind), float(window.a), float(window.b), int(iterations),
+                                              float(kappa), int(bool(band_limited)), C.byref(h)))
+        self.handle = h
+
+    @classmethod
+    def new(cls, k, n, window=None, ctx=None) -> "SpiralRecon":
+        return cls(k, n, window, ctx=ctx)
+
+    @property
+    def npts(self) -> int:
+        return len(self.k)
+
+    def _info(self):
+        lam, its = C.c_double(), C.c_int64()
+        w = np.zeros(self.npts)
+        check(lib().mrsim_spiral_recon_info(self.handle, C.byref(lam), C.byref(its), w.ctypes.data_as(abi.c_f64p)))
+        return lam.value, its.value, w
+
+    @property
+    def lambda_hi(self) -> float:
+        return self._info()[0]
+
+    @property
+    def power_iterations(self) -> int:
+        return self._info()[1]
+
+    def weights(self) -> np.ndarray:
+        return self._info()[2]
+
+    def _run(self, fn, d, batch_shape):
+        d = _c128(d)
+        batch = d.size // self.npts
+        if d.size != batch * self.npts or batch == 0:
+            raise ValueError("one value per sample")
+        out = np.zeros(batch * self.n * self.n, np.complex128)
+        check(fn(self.handle, d.view(np.float64).ctypes.data_as(abi.c_f64p), batch,
+                 out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+        return out.reshape(batch_shape + (self.n, self.n))
+
+    def gridding(self, d) -> np.ndarray:
+        d = _c128(d)
+        return self._run(lib().mrsim_spiral_recon_gridding, d, d.shape[:-1])
+
+    def image(self, d) -> np.ndarray:
+        d = _c128(d)
+        return self._run(lib().mrsim_spiral_recon_image, d, d.shape[:-1])
+
+    def reconstruct_rings(self, coil_samples, ring: int, zsens) -> np.ndarray:
+        """coil_samples [(partition,) coil, npts]; zsens [(partition,) coil] -> [(partition,) n, n]."""
+        cs = _c128(coil_samples)
+        single = cs.ndim == 2
+        if single:
+            cs = cs[None]
+        zs = np.ascontiguousarray(np.asarray(zsens, dtype=np.float64).reshape(cs.shape[0], cs.shape[1]))
+        out = np.zeros(cs.shape[0] * self.n * self.n, np.complex128)
+        check(lib().mrsim_spiral_recon_rings(self.handle, cs.view(np.float64).ctypes.data_as(abi.c_f64p), cs.shape[0],
+                                             cs.shape[1], int(ring), zs.ctypes.data_as(abi.c_f64p),
+                                             out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+        out = out.reshape(cs.shape[0], self.n, self.n)
+        return out[0] if single else out
+
+    def reconstruct(self, coil_samples, acq: Acquisition) -> np.ndarray:
+        nc = max(int(acq.n_coils), 1)
+        cs = _c128(coil_samples)
+        if cs.shape[-2] != nc:
+            raise ValueError("one sample set per coil")
+        return self.reconstruct_rings(cs, nc, np.ones(cs.shape[:-1]))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().mrsim_spiral_recon_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1803,6 +1803,54 @@ std::vector<GoldenCase> golden_outputs() {
 }
 
 
+
+// ---- FFT (the reference calls rustfft): radix-2 for powers of two, else the direct DFT; the
+// same unnormalized transform e^{sign i2pi jk/n}, within rounding ----
+void fft1d(std::vector<Cx>& a, int sign) {
+  const size_t n = a.size();
+  if (n <= 1) return;
+  if ((n & (n - 1)) != 0) {
+    std::vector<Cx> out(n);
+    for (size_t k = 0; k < n; ++k) {
+      Cx acc{0.0, 0.0};
+      for (size_t j = 0; j < n; ++j) acc = cadd(acc, cmul(a[j], ccis((double)sign * TAU * (double)((j * k) % n) / (double)n)));
+      out[k] = acc;
+    }
+    a = out;
+    return;
+  }
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (size_t len = 2; len <= n; len <<= 1) {
+    for (size_t i = 0; i < n; i += len)
+      for (size_t k = 0; k < len / 2; ++k) {
+        Cx w = ccis((double)sign * TAU * (double)k / (double)len);
+        Cx u = a[i + k], v = cmul(a[i + k + len / 2], w);
+        a[i + k] = cadd(u, v);
+        a[i + k + len / 2] = {u.re - v.re, u.im - v.im};
+      }
+  }
+}
+
+void fft2d(std::vector<Cx>& g, size_t n0, size_t n1, int sign) {
+  std::vector<Cx> line(n0);
+  for (size_t l = 0; l < n1; ++l) {
+    for (size_t i = 0; i < n0; ++i) line[i] = g[i + n0 * l];
+    fft1d(line, sign);
+    for (size_t i = 0; i < n0; ++i) g[i + n0 * l] = line[i];
+  }
+  line.resize(n1);
+  for (size_t l = 0; l < n0; ++l) {
+    for (size_t i = 0; i < n1; ++i) line[i] = g[l + n0 * i];
+    fft1d(line, sign);
+    for (size_t i = 0; i < n1; ++i) g[l + n0 * i] = line[i];
+  }
+}
+
 // ============================ stack-of-spirals path =========================================
 // `Nufft2` nufft.rs:125-299, FP64.  The fine-grid transform is a separable direct DFT (the
 // reference calls rustfft; a DFT is the same linear map, within rounding).
@@ -1847,22 +1895,7 @@ struct Nufft2O {
     int64_t r = m % (int64_t)n;
     return (size_t)(r < 0 ? r + (int64_t)n : r);
   }
-  void dft2(std::vector<Cx>& g, int sign) const {  // nufft.rs:209-229
-    for (int a = 0; a < 2; ++a) {
-      size_t len = nf[a], lines = nf[1 - a];
-      std::vector<Cx> tw(len), line(len), out(len);
-      for (size_t k = 0; k < len; ++k) tw[k] = ccis((double)sign * TAU * (double)k / (double)len);
-      for (size_t l = 0; l < lines; ++l) {
-        for (size_t i = 0; i < len; ++i) line[i] = a == 0 ? g[i + nf[0] * l] : g[l + nf[0] * i];
-        for (size_t k = 0; k < len; ++k) {
-          Cx acc{0.0, 0.0};
-          for (size_t j = 0; j < len; ++j) acc = cadd(acc, cmul(line[j], tw[(j * k) % len]));
-          out[k] = acc;
-        }
-        for (size_t i = 0; i < len; ++i) (a == 0 ? g[i + nf[0] * l] : g[l + nf[0] * i]) = out[i];
-      }
-    }
-  }
+  void dft2(std::vector<Cx>& g, int sign) const { fft2d(g, nf[0], nf[1], sign); }  // nufft.rs:209-229
   std::vector<Cx> type1(const double* u, size_t npts, const Cx* wts, int sign) const {  // nufft.rs:236-262
     std::vector<Cx> g(nf[0] * nf[1], Cx{0.0, 0.0});
     std::vector<double> k0(w), k1(w);
@@ -2028,6 +2061,170 @@ std::vector<Cx> spiral_segmented(const mrsim_slice_input& inp, const mrsim_acqui
   }
   return out;
 }
+
+
+// `SpiralRecon` grid_recon.rs:54-325, FP64 with the NUFFT pair as the reference applies it.
+struct SpiralReconO {
+  size_t n;
+  std::vector<double> k, w, win;
+  Nufft2O nufft;
+  std::vector<bool> keep;
+  bool band;
+  double lambda_hi = 0.0, kappa;
+  size_t iterations;
+  int64_t power_its = 0;
+  static Nufft2O make(size_t n) {
+    int64_t nn[2] = {(int64_t)n, (int64_t)n}, lo[2] = {-(int64_t)(n / 2), -(int64_t)(n / 2)}, mo[2] = {(int64_t)n, (int64_t)n};
+    return Nufft2O(nn, lo, mo, 1e-12);
+  }
+  static double norm(const std::vector<Cx>& v) {
+    double s = 0.0;
+    for (const Cx& c : v) s += c.re * c.re + c.im * c.im;
+    return std::sqrt(s);
+  }
+  SpiralReconO(const double* k_, size_t npts, size_t n_, const mrsim_acquisition& wa, size_t its, double kap, bool band_)
+      : n(n_), k(k_, k_ + 2 * npts), nufft(make(n_)), band(band_), kappa(kap), iterations(its) {
+    w.assign(npts, 1.0);
+    for (int it = 0; it < 10; ++it) {  // `pipe_menon` grid_recon.rs:54-66
+      std::vector<Cx> wts(npts);
+      for (size_t j = 0; j < npts; ++j) wts[j] = {w[j], 0.0};
+      std::vector<Cx> img = nufft.type1(k.data(), npts, wts.data(), -1);
+      std::vector<Cx> back = nufft.type2(img.data(), k.data(), npts, 1);
+      for (size_t j = 0; j < npts; ++j) w[j] /= std::hypot(back[j].re, back[j].im);
+    }
+    auto dirichlet = [&](double kk) {
+      Cx acc{0.0, 0.0};
+      for (size_t x = 0; x < n; ++x) acc = cadd(acc, ccis(TAU * kk * ((double)x - (double)(n / 2)) / (double)n));
+      return cscale(acc, 1.0 / (double)n);
+    };
+    Cx centre{0.0, 0.0};
+    for (size_t j = 0; j < npts; ++j) centre = cadd(centre, cscale(cmul(dirichlet(k[2 * j]), dirichlet(k[2 * j + 1])), w[j]));
+    double s = 1.0 / centre.re;
+    for (double& x : w) x *= s;
+    double radius = 0.0;
+    for (size_t j = 0; j < npts; ++j) {
+      win.push_back(window_at(wa, k[2 * j] / (double)n, k[2 * j + 1] / (double)n));
+      radius = std::max(radius, std::hypot(k[2 * j], k[2 * j + 1]));
+    }
+    size_t hu = (n + 1) / 2;
+    auto sg = [&](size_t i) { return i < hu ? (double)i : (double)i - (double)n; };
+    for (size_t i = 0; i < n * n; ++i) keep.push_back(std::hypot(sg(i % n), sg(i / n)) <= radius);
+    uint64_t st = 0x9E3779B97F4A7C15ull;
+    auto rnd = [&]() {
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      return (double)(st >> 11) / (double)(1ull << 53) - 0.5;
+    };
+    std::vector<Cx> v(n * n);
+    for (Cx& c : v) {
+      c.re = rnd();
+      c.im = rnd();
+    }
+    double lam = 0.0;
+    for (int it = 0; it < 1000; ++it) {
+      double nv = norm(v);
+      std::vector<Cx> u = normal(v);
+      double nu = norm(u);
+      double next = nu / nv;
+      for (size_t i = 0; i < v.size(); ++i) v[i] = cscale(u[i], 1.0 / nu);
+      bool done = std::fabs(next - lam) <= 1e-10 * next;
+      lam = next;
+      ++power_its;
+      if (done) break;
+    }
+    lambda_hi = 1.1 * lam;
+  }
+  std::vector<Cx> forward(const std::vector<Cx>& x) const {
+    double sc = 1.0 / (double)(n * n);
+    std::vector<Cx> o = nufft.type2(x.data(), k.data(), k.size() / 2, 1);
+    for (Cx& c : o) c = {c.re * sc, c.im * sc};
+    return o;
+  }
+  std::vector<Cx> adjoint(const std::vector<Cx>& r) const {
+    double sc = 1.0 / (double)(n * n);
+    std::vector<Cx> wts(r.size());
+    for (size_t j = 0; j < r.size(); ++j) wts[j] = {r[j].re * w[j] * sc, r[j].im * w[j] * sc};
+    return nufft.type1(k.data(), r.size(), wts.data(), -1);
+  }
+  void project(std::vector<Cx>& x) const {
+    if (!band) return;
+    fft2d(x, n, n, -1);
+    for (size_t i = 0; i < x.size(); ++i)
+      if (!keep[i]) x[i] = {0.0, 0.0};
+    fft2d(x, n, n, 1);
+    double s = 1.0 / (double)(n * n);
+    for (Cx& c : x) c = {c.re * s, c.im * s};
+  }
+  std::vector<Cx> normal(const std::vector<Cx>& x) const {
+    std::vector<Cx> xq = x;
+    project(xq);
+    std::vector<Cx> y = adjoint(forward(xq));
+    project(y);
+    return y;
+  }
+  std::vector<Cx> gridding(const std::vector<Cx>& d) const {
+    std::vector<Cx> o = adjoint(d);
+    for (Cx& c : o) c = cscale(c, (double)(n * n));
+    return o;
+  }
+  std::vector<Cx> image(const std::vector<Cx>& d) const {
+    std::vector<Cx> dw(d.size());
+    for (size_t j = 0; j < d.size(); ++j) dw[j] = cscale(d[j], win[j]);
+    double hi = lambda_hi, lo = lambda_hi / kappa;
+    double theta = (hi + lo) / 2.0, delta = (hi - lo) / 2.0;
+    double sigma1 = theta / delta;
+    double rho = 1.0 / sigma1;
+    std::vector<Cx> x(n * n, Cx{0.0, 0.0});
+    std::vector<Cx> r = adjoint(dw);
+    project(r);
+    double r0 = norm(r);
+    std::vector<Cx> dir(r.size());
+    for (size_t i = 0; i < r.size(); ++i) dir[i] = cscale(r[i], 1.0 / theta);
+    for (size_t it = 0; it < iterations; ++it) {
+      for (size_t i = 0; i < x.size(); ++i) x[i] = cadd(x[i], dir[i]);
+      std::vector<Cx> nd = normal(dir);
+      for (size_t i = 0; i < r.size(); ++i) r[i] = {r[i].re - nd[i].re, r[i].im - nd[i].im};
+      double rho1 = 1.0 / (2.0 * sigma1 - rho);
+      for (size_t i = 0; i < dir.size(); ++i) dir[i] = cadd(cscale(dir[i], rho1 * rho), cscale(r[i], 2.0 * rho1 / delta));
+      rho = rho1;
+    }
+    double rn = norm(r);
+    if (!(rn <= (1.0 + 1e-6) * r0 + 1e-300)) throw Fail("spiral reconstruction: the residual grew");
+    return x;
+  }
+  std::vector<Cx> rings(const Cx* coil, size_t ncoils, size_t ring, const double* zsens) const {
+    size_t npts = k.size() / 2, rows = ncoils / ring;
+    std::vector<Cx> wsum(n * n, Cx{0.0, 0.0});
+    std::vector<double> ssum(n * n, 0.0);
+    for (size_t a = 0; a < ring; ++a) {
+      std::vector<Cx> img;
+      if (rows == 1 && zsens[a] == 1.0) {
+        img = image(std::vector<Cx>(coil + a * npts, coil + (a + 1) * npts));
+      } else {
+        std::vector<Cx> d(npts, Cx{0.0, 0.0});
+        for (size_t r = 0; r < rows; ++r) {
+          size_t q = r * ring + a;
+          for (size_t j = 0; j < npts; ++j) d[j] = cadd(d[j], cscale(coil[q * npts + j], zsens[q]));
+        }
+        img = image(d);
+      }
+      double z2 = 0.0;
+      for (size_t r = 0; r < rows; ++r) z2 += zsens[r * ring + a] * zsens[r * ring + a];
+      for (size_t y = 0; y < n; ++y)
+        for (size_t x = 0; x < n; ++x) {
+          double s = coil_sensitivity(a, ring, (double)x, (double)y, n, n);
+          size_t i = x + n * y;
+          wsum[i] = cadd(wsum[i], cscale(img[i], s));
+          ssum[i] += s * s * z2;
+        }
+    }
+    std::vector<Cx> out(n * n);
+    for (size_t i = 0; i < n * n; ++i) {
+      double s = std::max(ssum[i], 1e-12);
+      out[i] = {wsum[i].re / s, wsum[i].im / s};
+    }
+    return out;
+  }
+};
 
 thread_local std::string g_err;
 std::vector<GoldenCase>* g_golden = nullptr;
@@ -2280,6 +2477,35 @@ int oracle_spiral_segmented(const mrsim_slice_input* inp, const mrsim_acquisitio
     put_cx(spiral_segmented(*inp, *acq, (size_t)coil, (size_t)ncoils, k, tau_idx, (size_t)npts, tau_l, (size_t)L, b,
                             log_amp, decay_inside != 0),
            out);
+  });
+}
+
+// mode 0: reconstruct_rings of batch partitions; 1: image of each of batch sample sets; 2: gridding
+int oracle_spiral_recon(const double* k, int64_t npts, int64_t n, int32_t window_kind, double window_a, double window_b,
+                        int64_t iterations, double kappa, int32_t band, int32_t mode, const double* data, int64_t batch,
+                        int64_t ncoils, int64_t ring, const double* zsens, double* out, double* lambda_hi,
+                        int64_t* power_its, double* weights) {
+  return guard([&] {
+    mrsim_acquisition wa = acq_default();
+    wa.window_kind = window_kind;
+    wa.window_a = window_a;
+    wa.window_b = window_b;
+    SpiralReconO r(k, (size_t)npts, (size_t)n, wa, (size_t)iterations, kappa, band != 0);
+    if (lambda_hi) *lambda_hi = r.lambda_hi;
+    if (power_its) *power_its = r.power_its;
+    if (weights) std::memcpy(weights, r.w.data(), r.w.size() * 8);
+    const Cx* d = reinterpret_cast<const Cx*>(data);
+    size_t nn = (size_t)(n * n);
+    for (int64_t b = 0; b < batch; ++b) {
+      std::vector<Cx> o;
+      if (mode == 0)
+        o = r.rings(d + (size_t)b * ncoils * npts, (size_t)ncoils, (size_t)ring, zsens + (size_t)b * ncoils);
+      else if (mode == 1)
+        o = r.image(std::vector<Cx>(d + (size_t)b * npts, d + (size_t)(b + 1) * npts));
+      else
+        o = r.gridding(std::vector<Cx>(d + (size_t)b * npts, d + (size_t)(b + 1) * npts));
+      put_cx(o, out + 2 * nn * (size_t)b);
+    }
   });
 }
 

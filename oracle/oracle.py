@@ -76,6 +76,10 @@ def lib():
         L.oracle_spiral_segmented.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), C.c_int64, C.c_int64,
                                               abi.c_f64p, i64p, C.c_int64, abi.c_f64p, C.c_int64, abi.c_f64p,
                                               abi.c_f64p, C.c_int32, abi.c_f64p]
+        L.oracle_spiral_recon.argtypes = [abi.c_f64p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double,
+                                          C.c_int64, C.c_double, C.c_int32, C.c_int32, abi.c_f64p, C.c_int64,
+                                          C.c_int64, C.c_int64, abi.c_f64p, abi.c_f64p, abi.c_f64p, i64p,
+                                          abi.c_f64p]
         _lib = L
     return _lib
 
@@ -366,3 +370,32 @@ def spiral_segmented(inp: SliceInput, acq: Acquisition, coil: int, ncoils: int, 
                                          bb.view(np.float64).ctypes.data_as(abi.c_f64p), la, int(bool(decay_inside)),
                                          out.view(np.float64).ctypes.data_as(abi.c_f64p)))
     return out
+
+
+def spiral_recon(k, n: int, data, mode: str = "image", window=(0, 0.0, 0.0), iterations: int = 80,
+                 kappa: float = 100.0, band: bool = True, ring: int = 1, zsens=None):
+    """`SpiralRecon` (grid_recon.rs:54-325) in FP64 with the reference's NUFFT-pair normal operator.
+    mode "image" / "gridding": data [batch, npts]; "rings": data [partition, coil, npts], zsens
+    [partition, coil].  Returns (images [batch, n, n], lambda_hi, power iterations, weights)."""
+    k = np.ascontiguousarray(k, dtype=np.float64).reshape(-1, 2)
+    npts = len(k)
+    d = np.ascontiguousarray(np.asarray(data, dtype=np.complex128))
+    m = {"rings": 0, "image": 1, "gridding": 2}[mode]
+    if m == 0:
+        d = d.reshape(-1, d.shape[-2], npts)
+        batch, ncoils = d.shape[0], d.shape[1]
+        zs = np.ascontiguousarray(np.asarray(zsens, dtype=np.float64).reshape(batch, ncoils))
+        zp = zs.ctypes.data_as(abi.c_f64p)
+    else:
+        d = d.reshape(-1, npts)
+        batch, ncoils, zp = d.shape[0], 1, None
+    out = np.zeros(batch * n * n, np.complex128)
+    lam = C.c_double()
+    its = C.c_int64()
+    w = np.zeros(npts)
+    _check(lib().oracle_spiral_recon(k.ctypes.data_as(abi.c_f64p), npts, n, int(window[0]), float(window[1]),
+                                     float(window[2]), iterations, kappa, int(band), m,
+                                     d.view(np.float64).ctypes.data_as(abi.c_f64p), batch, ncoils, ring, zp,
+                                     out.view(np.float64).ctypes.data_as(abi.c_f64p), C.byref(lam), C.byref(its),
+                                     w.ctypes.data_as(abi.c_f64p)))
+    return out.reshape(batch, n, n), lam.value, its.value, w
