@@ -314,6 +314,75 @@ int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* im
                                   float* kspace, float* comp_grad, float* fmap_grad,
                                   float* r2_grad);
 
+/* ---- the 3D echo trains (kspace3d.rs, readout.rs:75-322) ----------------------------------- */
+enum { MRSIM_KZ_CENTRIC = 0, MRSIM_KZ_LINEAR = 1 };                            /* readout.rs:75 */
+
+/* `EchoTrain` (readout.rs:82-95). */
+typedef struct mrsim_echo_train {
+  int64_t etl;
+  double esp_ms;
+  double refocusing_deg;
+  int32_t kz_order;        /* MRSIM_KZ_* */
+  int32_t reserved;
+  int64_t kz_segments;
+  double refocusing_time_ms;
+} mrsim_echo_train;
+
+/* `Readout3d::Grase` (readout.rs:103-106). */
+typedef struct mrsim_grase_readout {
+  int64_t ky_segments;
+  double t_line_ms;
+  int32_t reverse_phase;
+  int32_t reserved;
+} mrsim_grase_readout;
+
+/* The inputs of `simulate_acquisition_3d` (kspace3d.rs:549-565): images as the 2D series takes
+ * them (ncomp arrays of snx*sny*nz*n_volumes, vox*nv+g); t2 / t1 / t_inhom per compartment over
+ * the simulation volume (t1 NULL = infinite; required below 180 degrees of refocusing; t_inhom
+ * NULL = Acquisition::t_inhom); `line_weights` = `LineWeights::w` [g][shot][c] or NULL; the
+ * in-plane GRAPPA reference scan (`GrappaCalibration`, kspace.rs:1646) when
+ * has_grappa_calibration, else the first volume's images and `seed`.  Per-shot images
+ * (`ShotSet`) are not taken. */
+typedef struct mrsim_acquisition_3d_input {
+  int64_t sim_dims[3];
+  int64_t acq_dims[3];
+  int64_t n_volumes;
+  int64_t ncomp;
+  const float* const* images;
+  const mrsim_t2* t2;
+  const mrsim_t2* t1;
+  const float* fmap;
+  const mrsim_t2* t_inhom;
+  const mrsim_phase_model* phase;
+  const double* line_weights;
+  int32_t has_grappa_calibration;
+  int32_t reserved;
+  const float* const* grappa_calibration_images;   /* ncomp sim volumes */
+  uint64_t grappa_calibration_seed;
+} mrsim_acquisition_3d_input;
+
+/* `kz_order` (readout.rs:167-189). */
+int mrsim_kz_order(int64_t nz, int32_t order, int64_t* out);
+/* `grase_lines` (readout.rs:283-322): per line p*ny + ky its shot, echo (1-based), t and trf
+ * (ms) and polarity (any output may be NULL); e_c and n_shots. */
+int mrsim_grase_lines(const mrsim_echo_train* train, const mrsim_grase_readout* ro, int64_t ny,
+                      int64_t nz, int64_t* shot, int64_t* echo, double* t_ms, double* trf_ms,
+                      int8_t* polarity, int64_t* e_c, int64_t* n_shots);
+/* `simulate_acquisition_3d` (kspace3d.rs:549-565) with a GRASE readout, on the device: per
+ * volume every compartment's 2D forward (within-echo timing, class or voxel decay), the centred
+ * z-DFT, the line weights and sampling, spikes and noise per (volume, partition, coil), the
+ * inverse z-DFT, GRAPPA (one kernel per slice from the reference scan) and the 2D reconstruction.
+ * mag / phase: f32, vox*nv + g. */
+int mrsim_simulate_acquisition_3d(mrsim_context* ctx, const mrsim_acquisition_3d_input* in,
+                                  const mrsim_acquisition* acq, const mrsim_echo_train* train,
+                                  const mrsim_grase_readout* ro, uint64_t seed, float* mag,
+                                  float* phase);
+/* `kspace_3d_observed` (kspace3d.rs:439-456): volume g's acquired 3D k-space per coil before
+ * spikes and noise, out [coil][(p*ny + ky)*nx + kx] (re, im) f32. */
+int mrsim_kspace_3d_observed(mrsim_context* ctx, const mrsim_acquisition_3d_input* in,
+                             const mrsim_acquisition* acq, const mrsim_echo_train* train,
+                             const mrsim_grase_readout* ro, int64_t g, float* out);
+
 /* ---- the stack-of-spirals path: host plans ------------------------------------------------ */
 /* `spiral_tau_c` (readout.rs:564-596): the constant-angular-velocity centre region (ms). */
 int mrsim_spiral_tau_c(int64_t nx, int64_t interleaves, double readout_ms, double dwell_ms,

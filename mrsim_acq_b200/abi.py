@@ -108,6 +108,32 @@ class TsegInfo_(C.Structure):
                 ("bound", C.c_double)]
 
 
+class EchoTrain_(C.Structure):
+    """`mrsim_echo_train` — `EchoTrain` (readout.rs:82-95)."""
+
+    _fields_ = [("etl", C.c_int64), ("esp_ms", C.c_double), ("refocusing_deg", C.c_double), ("kz_order", C.c_int32),
+                ("reserved", C.c_int32), ("kz_segments", C.c_int64), ("refocusing_time_ms", C.c_double)]
+
+
+class GraseReadout_(C.Structure):
+    """`mrsim_grase_readout` — `Readout3d::Grase` (readout.rs:103-106)."""
+
+    _fields_ = [("ky_segments", C.c_int64), ("t_line_ms", C.c_double), ("reverse_phase", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class Acquisition3dInput_(C.Structure):
+    """`mrsim_acquisition_3d_input` — the inputs of `simulate_acquisition_3d` (kspace3d.rs:549)."""
+
+    _fields_ = [
+        ("sim_dims", C.c_int64 * 3), ("acq_dims", C.c_int64 * 3), ("n_volumes", C.c_int64), ("ncomp", C.c_int64),
+        ("images", C.POINTER(c_f32p)), ("t2", C.POINTER(T2_)), ("t1", C.POINTER(T2_)), ("fmap", c_f32p),
+        ("t_inhom", C.POINTER(T2_)), ("phase", C.POINTER(PhaseModel_)), ("line_weights", c_f64p),
+        ("has_grappa_calibration", C.c_int32), ("reserved", C.c_int32),
+        ("grappa_calibration_images", C.POINTER(c_f32p)), ("grappa_calibration_seed", C.c_uint64),
+    ]
+
+
 class LibraryMissing(RuntimeError):
     pass
 
@@ -180,6 +206,15 @@ def _declare(lib):
                                                      C.c_int64, c_f64p, C.POINTER(C.c_int64), C.c_int64, c_f64p,
                                                      C.c_int64, C.c_double, c_f64p, c_f64p, c_f64p, C.c_int32,
                                                      c_f32p, C.POINTER(TsegInfo_)]),
+        "mrsim_kz_order": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_int64)]),
+        "mrsim_grase_lines": (C.c_int, [C.POINTER(EchoTrain_), C.POINTER(GraseReadout_), C.c_int64, C.c_int64,
+                                        C.POINTER(C.c_int64), C.POINTER(C.c_int64), c_f64p, c_f64p,
+                                        C.POINTER(C.c_int8), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "mrsim_simulate_acquisition_3d": (C.c_int, [P, C.POINTER(Acquisition3dInput_), C.POINTER(Acquisition_),
+                                                    C.POINTER(EchoTrain_), C.POINTER(GraseReadout_), C.c_uint64,
+                                                    c_f32p, c_f32p]),
+        "mrsim_kspace_3d_observed": (C.c_int, [P, C.POINTER(Acquisition3dInput_), C.POINTER(Acquisition_),
+                                               C.POINTER(EchoTrain_), C.POINTER(GraseReadout_), C.c_int64, c_f32p]),
         "mrsim_spiral_recon_create": (C.c_int, [P, c_f64p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double,
                                                 C.c_int64, C.c_double, C.c_int32, C.POINTER(P)]),
         "mrsim_spiral_recon_destroy": (C.c_int, [P]),

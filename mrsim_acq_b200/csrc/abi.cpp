@@ -11,6 +11,8 @@
 #include "host_tables.h"
 #include "mrsim_internal.h"
 #include "series.h"
+#include "grase3d.h"
+#include "host3d.h"
 #include "spiral.h"
 #include "spiral_host.h"
 #include "spiral_recon.h"
@@ -736,6 +738,68 @@ int mrsim_spiral_recon_rings(mrsim_spiral_recon* rec, const double* coil_samples
                       need(zsens, "zsens");
                       rec->impl->rings(i, (int)n_partitions, (int)ncoils, (int)ring, zsens, o);
                     });
+}
+
+// ---- 3D echo trains -------------------------------------------------------------------------------
+int mrsim_kz_order(int64_t nz, int32_t order, int64_t* out) {
+  return guarded([&] {
+    if (nz <= 0) mrsim::fail("nz must be positive");
+    need(out, "out");
+    auto v = mrsim::kz_order((int)nz, order);
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i];
+  });
+}
+
+int mrsim_grase_lines(const mrsim_echo_train* train, const mrsim_grase_readout* ro, int64_t ny, int64_t nz,
+                      int64_t* shot, int64_t* echo, double* t_ms, double* trf_ms, int8_t* polarity, int64_t* e_c,
+                      int64_t* n_shots) {
+  return guarded([&] {
+    need(train, "train");
+    need(ro, "readout");
+    if (ny <= 0 || nz <= 0) mrsim::fail("ny and nz must be positive");
+    mrsim::Grase3dTable T = mrsim::grase_lines(*train, *ro, (int)ny, (int)nz);
+    for (size_t i = 0; i < T.lines.size(); ++i) {
+      if (shot) shot[i] = T.lines[i].shot;
+      if (echo) echo[i] = T.lines[i].echo;
+      if (t_ms) t_ms[i] = T.lines[i].t_ms;
+      if (trf_ms) trf_ms[i] = T.lines[i].trf_ms;
+      if (polarity) polarity[i] = T.lines[i].polarity;
+    }
+    if (e_c) *e_c = T.e_c;
+    if (n_shots) *n_shots = T.n_shots;
+  });
+}
+
+static void check_3d_input(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                           const mrsim_echo_train* train, const mrsim_grase_readout* ro) {
+  need(in, "input");
+  need(acq, "acq");
+  need(train, "train");
+  need(ro, "readout");
+  if (in->n_volumes < 0) mrsim::fail("negative volume count");
+  if (in->ncomp > 0 && !in->images) mrsim::fail("compartment image is not on the simulation grid");
+  for (int64_t c = 0; c < in->ncomp; ++c)
+    if (!in->images[c]) mrsim::fail("compartment image is not on the simulation grid");
+}
+
+int mrsim_simulate_acquisition_3d(mrsim_context* ctx, const mrsim_acquisition_3d_input* in,
+                                  const mrsim_acquisition* acq, const mrsim_echo_train* train,
+                                  const mrsim_grase_readout* ro, uint64_t seed, float* mag, float* phase) {
+  return on_ctx(ctx, [&] {
+    check_3d_input(in, acq, train, ro);
+    need(mag, "mag");
+    need(phase, "phase");
+    mrsim::grase_acquire(ctx, *in, *acq, *train, *ro, seed, mag, phase);
+  });
+}
+
+int mrsim_kspace_3d_observed(mrsim_context* ctx, const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                             const mrsim_echo_train* train, const mrsim_grase_readout* ro, int64_t g, float* out) {
+  return on_ctx(ctx, [&] {
+    check_3d_input(in, acq, train, ro);
+    need(out, "out");
+    mrsim::grase_observed(ctx, *in, *acq, *train, *ro, (int)g, out);
+  });
 }
 
 }  // extern "C"

@@ -1,0 +1,492 @@
+// grase3d.cu — the 3D GRASE echo-train acquisition on the device (reference
+// `simulate_acquisition_3d_complex_cal`, kspace3d.rs:483-547, with `Plan::compartments` /
+// `Plan::kspace` :125-232, `partitions_to_slices` :235-281, `reconstruct_slices` :283-297 and
+// `grappa_kernels_3d` :310-325).
+//
+// Per chunk of volumes, one batched forward launch computes every needed 2D k-space: one unit per
+// (volume, compartment, slice) for class compartments (relaxation off, the decay a line weight)
+// and per (volume, compartment, echo, slice) for voxel compartments (ln A_e and the T2/T2' maps
+// inside the forward).  Then one kernel forms the centred z-DFT, the class and line weights, the
+// compartment sum and the sampling per (volume, coil, partition, line, column); the spikes and
+// noise run on the (volume, partition, coil) streams; one kernel applies the inverse z-DFT
+// (1/nz) into per-slice coil k-spaces, and the 2D reconstruction (GRAPPA apply, window, inverse
+// DFT, Roemer) runs on all slices of the chunk at once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "driver.h"
+#include "grase3d.h"
+#include "host3d.h"
+#include "host_tables.h"
+#include "mrsim_internal.h"
+#include "recon_kernels.h"
+#include "series_parts.h"
+
+namespace mrsim {
+
+namespace {
+
+struct ZdftArgs {
+  const float2* K;        // [gl][src][z][q][ky][kx]
+  float2* out;            // [gl][q][p][ky][kx]
+  const float2* zk;       // [p][z]
+  const int* src;         // [c][p]: source index of compartment c at partition p
+  const float* wc;        // [c][p][ky]: class line weight (1 for voxel compartments)
+  const float* lw;        // [g][shot][c] or NULL
+  const int* shot;        // [p][ky]
+  const unsigned char* row_acquired;  // [ky]
+  int nx, ny, nz, nc, ncomp, nsrc, n_shots, g0;
+};
+
+// out = sampling * sum_c lw(g, shot, c) * (w_c(p, ky) * sum_z K[src(c, p)][z] zk[p][z])
+__global__ void grase_zdft_kernel(const ZdftArgs a) {
+  const int per = a.nx * a.ny;
+  const int p = blockIdx.y;
+  const int gq = blockIdx.z;  // gl * nc + q
+  const int gl = gq / a.nc, q = gq % a.nc;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < per; i += gridDim.x * blockDim.x) {
+    const int ky = i / a.nx;
+    float2 v = make_float2(0.f, 0.f);
+    if (a.row_acquired[ky]) {
+      for (int c = 0; c < a.ncomp; ++c) {
+        const int s = a.src[c * a.nz + p];
+        const float2* Kc = a.K + ((size_t)(gl * a.nsrc + s) * a.nz) * a.nc * per + (size_t)q * per + i;
+        float ar = 0.f, ai = 0.f;
+        for (int z = 0; z < a.nz; ++z) {
+          const float2 k = Kc[(size_t)z * a.nc * per];
+          const float2 e = a.zk[p * a.nz + z];
+          ar += k.x * e.x - k.y * e.y;
+          ai += k.x * e.y + k.y * e.x;
+        }
+        const float w = a.wc[((size_t)c * a.nz + p) * a.ny + ky];
+        ar *= w;
+        ai *= w;
+        const float l = a.lw ? a.lw[((size_t)(a.g0 + gl) * a.n_shots + a.shot[p * a.ny + ky]) * a.ncomp + c] : 1.f;
+        v.x += ar * l;
+        v.y += ai * l;
+      }
+    }
+    a.out[(((size_t)gl * a.nc + q) * a.nz + p) * per + i] = v;
+  }
+}
+
+// slices[gl][z][q] = (1/nz) sum_p k3[gl][q][p] conj(zk[p][z])
+__global__ void grase_izdft_kernel(const float2* __restrict__ k3, const float2* __restrict__ zk, int nx, int ny,
+                                   int nz, int nc, float2* __restrict__ slices) {
+  const int per = nx * ny;
+  const int z = blockIdx.y;
+  const int gq = blockIdx.z, gl = gq / nc, q = gq % nc;
+  const float inv = 1.0f / (float)nz;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < per; i += gridDim.x * blockDim.x) {
+    float ar = 0.f, ai = 0.f;
+    for (int p = 0; p < nz; ++p) {
+      const float2 k = k3[(((size_t)gl * nc + q) * nz + p) * per + i];
+      const float2 e = zk[p * nz + z];
+      ar += k.x * e.x + k.y * e.y;
+      ai += k.y * e.x - k.x * e.y;
+    }
+    slices[(((size_t)gl * nz + z) * nc + q) * per + i] = make_float2(ar * inv, ai * inv);
+  }
+}
+
+// combined [gl][z][ny][nx] -> magnitude / phase at vox * nv + g
+__global__ void volume_output_kernel(const float2* __restrict__ comb, int g0, int ngl, int nv, size_t nvox,
+                                     float* __restrict__ mag, float* __restrict__ ph) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)ngl * nvox;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int gl = (int)(i / nvox);
+    const size_t vox = i % nvox;
+    const float2 c = comb[i];
+    const size_t o = vox * nv + (g0 + gl);
+    mag[o] = sqrtf(c.x * c.x + c.y * c.y);
+    ph[o] = atan2f(c.y, c.x);
+  }
+}
+
+dim3 grid3(size_t per, int y, int z) {
+  return dim3((unsigned)std::max<size_t>(1, std::min<size_t>((per + 255) / 256, 1024)), (unsigned)y, (unsigned)z);
+}
+
+}  // namespace
+
+// ---- the plan --------------------------------------------------------------------------------------
+struct GrasePlan {
+  int snx, sny, nz, nx, ny, o, ncomp, nc, etl;
+  size_t plane, nvox;
+  Grase3dTable table;
+  LineTimingTab within;
+  std::vector<CompMode> modes;
+  std::vector<uint8_t> mask;
+  std::vector<float2> zk;
+  // sources: class compartment c -> one; voxel compartment c -> one per echo that reads a partition
+  struct Src {
+    int c, e;  // e = 0 for class
+  };
+  std::vector<Src> srcs;
+  std::vector<int> src_of;  // [c][p]
+  std::vector<float> wc;    // [c][p][ky]
+};
+
+static GrasePlan make_plan(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
+                           const mrsim_echo_train& train, const mrsim_grase_readout& ro) {
+  GrasePlan P;
+  P.snx = (int)in.sim_dims[0];
+  P.sny = (int)in.sim_dims[1];
+  P.nz = (int)in.sim_dims[2];
+  P.nx = (int)in.acq_dims[0];
+  P.ny = (int)in.acq_dims[1];
+  if (P.nz != (int)in.acq_dims[2]) fail("partition count must match; z is never oversampled");
+  if (P.snx <= 0 || P.sny <= 0 || P.nx <= 0 || P.ny <= 0 || P.nz <= 0) fail("empty simulation grid or acquired matrix");
+  if (!(P.snx % P.nx == 0 && P.sny % P.ny == 0)) fail("sim grid must be an integer multiple of the acquired matrix");
+  P.o = P.snx / P.nx;
+  if (P.o != P.sny / P.ny) fail("oversampling must match on both axes");
+  P.ncomp = (int)in.ncomp;
+  if (P.ncomp > kMaxComp) fail("more than 8 compartments");
+  P.nc = (int)std::max<int64_t>(acq.n_coils, 1);
+  if (P.nc > kMaxCoils) fail("more than 64 coils");
+  if (P.nx > 1024) fail("acquired matrix too wide for the reconstruction");
+  P.plane = (size_t)P.snx * P.sny;
+  P.nvox = P.plane * P.nz;
+  if (!in.fmap) fail("fieldmap is not on the simulation grid");
+  if (P.ncomp > 0 && (!in.images || !in.t2)) fail("compartment image is not on the simulation grid");
+  if (acq.echo != MRSIM_ECHO_SPIN) fail("the 3D echo trains are spin-echo trains");
+  if (acq.eddy_strength != 0.0 || acq.eddy_quad != 0.0 || acq.eddy_phase != 0.0)
+    fail("the eddy model is not available in 3D (an echo-dependent eddy evolution breaks the z factorization)");
+  if (!(acq.partial_fourier >= 1.0 || acq.pf_mode != MRSIM_PF_SCANNER))
+    fail("Scanner partial Fourier is defined by the 2D EPI train; the 3D readouts take FiberfoxCompatible or "
+         "Contiguous");
+  if ((ro.reverse_phase != 0) != (acq.reverse_phase != 0))
+    fail("the readout's phase-encode sign must be the acquisition's");
+  P.table = grase_lines(train, ro, P.ny, P.nz);
+  P.within.t_ms = P.table.block.t_ms;
+  P.within.trf_ms = P.table.block.t_ms;
+  P.within.tread_ms = P.table.block.t_ms;
+  P.within.polarity = P.table.block.polarity;
+  P.etl = (int)train.etl;
+  P.modes = resolve_modes(in.t2, in.t1, in.t_inhom, P.ncomp, acq, train, P.nvox);
+  P.mask = sampling_mask(P.nx, P.ny, acq);
+  const double zs = (double)(P.nz / 2);
+  P.zk.resize((size_t)P.nz * P.nz);
+  for (int p = 0; p < P.nz; ++p)
+    for (int z = 0; z < P.nz; ++z) {
+      const double th = kTau * ((double)p - zs) * ((double)z - zs) / (double)P.nz;  // `zkernel` kspace3d.rs:90-101
+      P.zk[(size_t)p * P.nz + z] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+  P.src_of.assign((size_t)P.ncomp * P.nz, 0);
+  P.wc.assign((size_t)P.ncomp * P.nz * P.ny, 1.f);
+  for (int c = 0; c < P.ncomp; ++c) {
+    const CompMode& m = P.modes[c];
+    if (!m.voxel) {
+      const int s = (int)P.srcs.size();
+      P.srcs.push_back({c, 0});
+      for (int p = 0; p < P.nz; ++p) {
+        P.src_of[(size_t)c * P.nz + p] = s;
+        for (int ky = 0; ky < P.ny; ++ky) {
+          const GraseLine& L = P.table.line(p, ky);
+          P.wc[((size_t)c * P.nz + p) * P.ny + ky] =
+              acq.do_relaxation ? (float)line_weight(m.ln_a[L.echo - 1], L.t_ms, m.t2_ms, m.t2p_ms) : 1.f;
+        }
+      }
+    } else {
+      int emax = 0;
+      for (auto& L : P.table.lines) emax = std::max(emax, L.echo);
+      for (int e = 1; e <= emax; ++e) {
+        bool used = false;
+        for (int p = 0; p < P.nz; ++p) used = used || P.table.line(p, 0).echo == e;
+        if (!used) continue;
+        const int s = (int)P.srcs.size();
+        P.srcs.push_back({c, e});
+        for (int p = 0; p < P.nz; ++p)
+          if (P.table.line(p, 0).echo == e) P.src_of[(size_t)c * P.nz + p] = s;
+      }
+    }
+  }
+  return P;
+}
+
+// The device-resident inputs of one acquisition (images of every volume on the device, unit-major).
+struct GraseInputs {
+  float* img = nullptr;    // [g][z][c][plane]
+  float* fmap = nullptr;   // [z][plane]
+  float* t2 = nullptr;     // [c][nvox] (voxel compartments' values), or NULL
+  float* ti = nullptr;
+  float* lna = nullptr;    // [c][e][nvox] for voxel compartments
+  int nv = 0;
+};
+
+static GraseInputs upload_inputs(DevArena& A, const GrasePlan& P, const mrsim_acquisition_3d_input& in,
+                                 const float* const* images, int nv, const mrsim_acquisition& acq, cudaStream_t st) {
+  GraseInputs I;
+  I.nv = nv;
+  const size_t per_comp = P.nvox * nv;
+  float* staging = (float*)A.alloc(std::max<size_t>(1, per_comp * P.ncomp) * 4);
+  for (int c = 0; c < P.ncomp; ++c)
+    MRSIM_CUDA(cudaMemcpyAsync(staging + (size_t)c * per_comp, images[c], per_comp * 4, cudaMemcpyHostToDevice, st));
+  I.img = (float*)A.alloc(std::max<size_t>(1, per_comp * P.ncomp) * 4);
+  if (P.ncomp) launch_series_transpose(staging, I.img, P.ncomp, nv, P.nz, (int)P.plane, st);
+  I.fmap = (float*)A.upload(in.fmap, P.nvox * 4, st);
+  bool any_voxel = false;
+  for (auto& m : P.modes) any_voxel = any_voxel || m.voxel;
+  if (any_voxel) {
+    std::vector<float> t2((size_t)P.ncomp * P.nvox, 1.f), ti((size_t)P.ncomp * P.nvox, 1.f);
+    std::vector<float> la((size_t)P.ncomp * P.etl * P.nvox, 0.f);
+    for (int c = 0; c < P.ncomp; ++c) {
+      if (!P.modes[c].voxel) continue;
+      for (size_t i = 0; i < P.nvox; ++i) {
+        t2[(size_t)c * P.nvox + i] = in.t2[c].is_map ? in.t2[c].map[i] : in.t2[c].value;
+        ti[(size_t)c * P.nvox + i] =
+            in.t_inhom ? (in.t_inhom[c].is_map ? in.t_inhom[c].map[i] : in.t_inhom[c].value) : (float)acq.t_inhom;
+      }
+      for (int e = 0; e < P.etl; ++e)
+        for (size_t i = 0; i < P.nvox; ++i)
+          la[((size_t)c * P.etl + e) * P.nvox + i] = (float)P.modes[c].maps[e][i];
+    }
+    I.t2 = (float*)A.upload(t2.data(), t2.size() * 4, st);
+    I.ti = (float*)A.upload(ti.data(), ti.size() * 4, st);
+    I.lna = (float*)A.upload(la.data(), la.size() * 4, st);
+  }
+  return I;
+}
+
+// The acquired 3D k-space (before spikes and noise) of volumes g0..g1 into k3 [gl][q][p][ky][kx].
+static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_acquisition& acq,
+                         const mrsim_phase_model* phase, const float* d_lw, int n_shots, int g0, int g1,
+                         const std::vector<uint8_t>& mask, float2* k3, cudaStream_t st) {
+  const int ngl = g1 - g0, nsrc = (int)P.srcs.size(), nz = P.nz, nc = P.nc;
+  const size_t per = (size_t)P.nx * P.ny;
+  DevArena C;
+  mrsim_acquisition norel = acq;
+  norel.do_relaxation = 0;
+  norel.noise_variance = 0.0;
+  norel.n_spikes = 0;
+  mrsim_acquisition rel = norel;
+  rel.do_relaxation = 1;
+  float one[kMaxComp];
+  for (int c = 0; c < kMaxComp; ++c) one[c] = 1.f;
+  std::vector<LineRec> Lc, Lv;
+  lines_for(Lc, norel, P.nx, P.ny, false, true, 1, one, one, false, &P.within);
+  lines_for(Lv, rel, P.nx, P.ny, false, false, 1, one, one, false, &P.within);
+  const int n_lines = (int)Lc.size();
+  const LineRec* dLc = (const LineRec*)C.upload(Lc.data(), std::max<size_t>(1, Lc.size()) * sizeof(LineRec), st);
+  const LineRec* dLv = (const LineRec*)C.upload(Lv.data(), std::max<size_t>(1, Lv.size()) * sizeof(LineRec), st);
+  const size_t nunit = (size_t)ngl * nsrc * nz;
+  float2* K = (float2*)C.alloc(std::max<size_t>(1, nunit * nc * per) * sizeof(float2));
+  MRSIM_CUDA(cudaMemsetAsync(K, 0, nunit * nc * per * sizeof(float2), st));
+  float2* gs = (float2*)C.alloc(std::max<size_t>(1, nunit * nc * std::max(n_lines, 1) * P.snx) * sizeof(float2));
+  float* ph = (float*)C.alloc(std::max<size_t>(1, nunit * P.plane) * 4);
+  GeoTab geo = build_geo(C, P.snx, P.sny, P.nx, P.ny, nc, acq.ghost_offset, st);
+  mrsim_phase_model zero;
+  std::memset(&zero, 0, sizeof zero);
+  Batch Bc, Bv;
+  for (int gl = 0; gl < ngl; ++gl)
+    for (int s = 0; s < nsrc; ++s)
+      for (int z = 0; z < nz; ++z) {
+        const GrasePlan::Src& S = P.srcs[s];
+        const size_t u = ((size_t)gl * nsrc + s) * nz + z;
+        UnitInputs ui;
+        std::memset(&ui, 0, sizeof ui);
+        ui.comp = I.img + (((size_t)(g0 + gl) * nz + z) * P.ncomp + S.c) * P.plane;
+        ui.comp_stride = (long long)P.plane;
+        ui.fmap = I.fmap + (size_t)z * P.plane;
+        ui.map_stride = (long long)P.nvox;
+        ui.kspace = K + u * nc * per;
+        ui.g = gs + u * nc * std::max(n_lines, 1) * P.snx;
+        ui.phase_out = ph + u * P.plane;
+        ui.phase = phase ? phase : &zero;
+        ui.z = z;
+        ui.nz_full = nz;
+        const CompMode& m = P.modes[S.c];
+        if (!m.voxel) {
+          ui.lines = dLc;
+          ui.n_lines = n_lines;
+          add_unit(Bc, ui, P.snx, P.sny, P.nx, P.ny, 1, nc, false, one, one, geo, norel);
+        } else {
+          ui.t2map = I.t2 + (size_t)S.c * P.nvox + (size_t)z * P.plane;
+          ui.timap = I.ti + (size_t)S.c * P.nvox + (size_t)z * P.plane;
+          ui.log_amp = I.lna + ((size_t)S.c * P.etl + (S.e - 1)) * P.nvox + (size_t)z * P.plane;
+          ui.lines = dLv;
+          ui.n_lines = n_lines;
+          add_unit(Bv, ui, P.snx, P.sny, P.nx, P.ny, 1, nc, true, one, one, geo, rel);
+        }
+      }
+  if (n_lines > 0) {
+    run_forward(Bc, st);
+    run_forward(Bv, st);
+  }
+  // the z-DFT, weights, compartment sum and sampling
+  std::vector<unsigned char> rows(P.ny);
+  for (int ky = 0; ky < P.ny; ++ky) rows[ky] = mask[(size_t)ky * P.nx] ? 1 : 0;
+  std::vector<int> shot((size_t)nz * P.ny);
+  for (int p = 0; p < nz; ++p)
+    for (int ky = 0; ky < P.ny; ++ky) shot[(size_t)p * P.ny + ky] = P.table.line(p, ky).shot;
+  ZdftArgs a;
+  a.K = K;
+  a.out = k3;
+  a.zk = (const float2*)C.upload(P.zk.data(), P.zk.size() * sizeof(float2), st);
+  a.src = (const int*)C.upload(P.src_of.data(), std::max<size_t>(1, P.src_of.size()) * 4, st);
+  a.wc = (const float*)C.upload(P.wc.data(), std::max<size_t>(1, P.wc.size()) * 4, st);
+  a.lw = d_lw;
+  a.shot = (const int*)C.upload(shot.data(), shot.size() * 4, st);
+  a.row_acquired = (const unsigned char*)C.upload(rows.data(), rows.size(), st);
+  a.nx = P.nx;
+  a.ny = P.ny;
+  a.nz = nz;
+  a.nc = nc;
+  a.ncomp = P.ncomp;
+  a.nsrc = nsrc;
+  a.n_shots = n_shots;
+  a.g0 = g0;
+  grase_zdft_kernel<<<grid3(per, nz, ngl * nc), 256, 0, st>>>(a);
+  MRSIM_CUDA(cudaGetLastError());
+  MRSIM_CUDA(cudaStreamSynchronize(st));  // C's buffers are freed on return
+}
+
+// spikes and noise per (volume, partition, coil) (`partitions_to_slices` kspace3d.rs:235-262)
+static void grase_noise(DevArena& A, const GrasePlan& P, float2* k3, int g0, int g1, uint64_t seed,
+                        const std::vector<uint8_t>& mask, const mrsim_acquisition& acq, cudaStream_t st) {
+  if (acq.n_spikes <= 0 && !(acq.noise_variance > 0.0)) return;
+  const size_t per = (size_t)P.nx * P.ny;
+  std::vector<int> acquired, rows;
+  for (size_t i = 0; i < per; ++i)
+    if (mask[i]) acquired.push_back((int)i);
+  for (int ky = 0; ky < P.ny; ++ky)
+    if (mask[(size_t)ky * P.nx]) rows.push_back(ky);
+  std::vector<NoiseSpec> specs;
+  std::vector<int> picks;
+  for (int g = g0; g < g1; ++g)
+    for (int p = 0; p < P.nz; ++p) {
+      const uint64_t pseed = (((uint64_t)g * 0x1000001ull) + (uint64_t)p) * 0x9E37ull ^ seed ^ kSeedSalt3d;
+      for (int q = 0; q < P.nc; ++q) {
+        const int off = (int)picks.size();
+        if (acq.n_spikes > 0) {  // `spike_picks` kspace3d.rs:327-332: a stream per coil
+          Rng rng(pseed ^ 0xA5A5123456789ABCull ^ ((uint64_t)q * 0xC2B2AE3D27D4EB4Full));
+          for (int64_t s = 0; s < acq.n_spikes; ++s)
+            picks.push_back(acquired.empty() ? 0 : acquired[(size_t)(rng.next_u64() % (uint64_t)acquired.size())]);
+        }
+        specs.push_back({k3 + (((size_t)(g - g0) * P.nc + q) * P.nz + p) * per, pseed, q, off});
+      }
+    }
+  run_noise(A, specs, rows, picks, P.nx, P.ny, acq, st);
+  MRSIM_CUDA(cudaGetLastError());
+}
+
+void grase_observed(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
+                    const mrsim_echo_train& train, const mrsim_grase_readout& ro, int g, float* out) {
+  cudaStream_t st = ctx->stream;
+  GrasePlan P = make_plan(in, acq, train, ro);
+  if (g < 0 || g >= (int)in.n_volumes) fail("volume index out of range");
+  DevArena A;
+  GraseInputs I = upload_inputs(A, P, in, in.images, (int)in.n_volumes, acq, st);
+  const float* d_lw = nullptr;
+  if (in.line_weights) {
+    std::vector<float> lw((size_t)in.n_volumes * P.table.n_shots * P.ncomp);
+    for (size_t i = 0; i < lw.size(); ++i) lw[i] = (float)in.line_weights[i];
+    d_lw = (const float*)A.upload(lw.data(), lw.size() * 4, st);
+  }
+  const size_t per = (size_t)P.nx * P.ny;
+  float2* k3 = (float2*)A.alloc((size_t)P.nc * P.nz * per * sizeof(float2));
+  grase_kspace(P, I, acq, in.phase, d_lw, P.table.n_shots, g, g + 1, P.mask, k3, st);
+  MRSIM_CUDA(cudaMemcpyAsync(out, k3, (size_t)P.nc * P.nz * per * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+}
+
+void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
+                   const mrsim_echo_train& train, const mrsim_grase_readout& ro, uint64_t seed, float* mag,
+                   float* ph) {
+  cudaStream_t st = ctx->stream;
+  GrasePlan P = make_plan(in, acq, train, ro);
+  const int nv = (int)in.n_volumes, nz = P.nz, nc = P.nc, nx = P.nx, ny = P.ny;
+  const size_t per = (size_t)nx * ny;
+  const int accel = (int)std::max<int64_t>(acq.accel, 1);
+  DevArena A;
+  GraseInputs I = upload_inputs(A, P, in, in.images, nv, acq, st);
+  const float* d_lw = nullptr;
+  if (in.line_weights) {
+    std::vector<float> lw((size_t)nv * P.table.n_shots * P.ncomp);
+    for (size_t i = 0; i < lw.size(); ++i) lw[i] = (float)in.line_weights[i];
+    d_lw = (const float*)A.upload(lw.data(), std::max<size_t>(1, lw.size()) * 4, st);
+  }
+  const float2* d_zk = (const float2*)A.upload(P.zk.data(), P.zk.size() * sizeof(float2), st);
+  // GRAPPA: one kernel per slice, fitted on the reference scan (`grappa_kernels_3d`)
+  float2* W = nullptr;
+  const size_t w_per_slice = (size_t)(accel - 1) * nc * 6 * nc;
+  if (accel > 1 && nv > 0) {
+    mrsim_acquisition acq_cal = acq;
+    acq_cal.accel = 1;
+    acq_cal.n_spikes = 0;
+    GrasePlan Pc = make_plan(in, acq_cal, train, ro);
+    DevArena C;
+    const float* const* cal_images = in.images;
+    int cal_nv = nv;
+    uint64_t cal_seed = seed;
+    if (in.has_grappa_calibration) {
+      if (!in.grappa_calibration_images) fail("the GRAPPA calibration images are NULL");
+      cal_images = in.grappa_calibration_images;
+      cal_nv = 1;
+      cal_seed = in.grappa_calibration_seed;
+    }
+    GraseInputs Ic = upload_inputs(C, Pc, in, cal_images, cal_nv, acq_cal, st);
+    float2* k3 = (float2*)C.alloc((size_t)nc * nz * per * sizeof(float2));
+    grase_kspace(Pc, Ic, acq_cal, in.phase, nullptr, Pc.table.n_shots, 0, 1, Pc.mask, k3, st);
+    grase_noise(C, Pc, k3, 0, 1, cal_seed ^ kSeedSaltGrappaCal, Pc.mask, acq_cal, st);
+    float2* sl = (float2*)C.alloc((size_t)nz * nc * per * sizeof(float2));
+    grase_izdft_kernel<<<grid3(per, nz, nc), 256, 0, st>>>(k3, d_zk, nx, ny, nz, nc, sl);
+    std::vector<float2*> refs;
+    for (int z = 0; z < nz; ++z) refs.push_back(sl + (size_t)z * nc * per);
+    W = fit_grappa(A, refs, nx, ny, nc, acq_cal, accel, (int)acq.acs_lines, st);
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  }
+  ReconTables T = build_recon_tables(A, nx, ny, nc, acq, st);
+  float* d_mag = (float*)A.alloc(std::max<size_t>(1, per * nz * nv) * 4);
+  float* d_ph = (float*)A.alloc(std::max<size_t>(1, per * nz * nv) * 4);
+  // chunks of volumes within a scratch budget
+  const size_t nsrc = P.srcs.size();
+  const size_t bytes_per_vol = (nsrc * nz * nc * per * 8) * 2 + nsrc * nz * (size_t)nc * ny * P.snx * 8 +
+                               (size_t)nc * nz * per * 8 * 2 + (size_t)nz * per * 8;
+  const size_t budget = (size_t)4 << 30;
+  const int vchunk = (int)std::max<size_t>(1, std::min<size_t>(std::max(nv, 1), budget / std::max<size_t>(1, bytes_per_vol)));
+  for (int g0 = 0; g0 < nv; g0 += vchunk) {
+    const int g1 = std::min(nv, g0 + vchunk), ngl = g1 - g0;
+    DevArena C;
+    float2* k3 = (float2*)C.alloc((size_t)ngl * nc * nz * per * sizeof(float2));
+    grase_kspace(P, I, acq, in.phase, d_lw, P.table.n_shots, g0, g1, P.mask, k3, st);
+    grase_noise(C, P, k3, g0, g1, seed, P.mask, acq, st);
+    float2* sl = (float2*)C.alloc((size_t)ngl * nz * nc * per * sizeof(float2));
+    grase_izdft_kernel<<<grid3(per, nz, ngl * nc), 256, 0, st>>>(k3, d_zk, nx, ny, nz, nc, sl);
+    float2* comb = (float2*)C.alloc((size_t)ngl * nz * per * sizeof(float2));
+    std::vector<ReconJob> jobs;
+    for (int gl = 0; gl < ngl; ++gl)
+      for (int z = 0; z < nz; ++z) {
+        ReconJob J;
+        std::memset(&J, 0, sizeof J);
+        J.k = sl + ((size_t)gl * nz + z) * nc * per;
+        J.grappa_w = W ? W + (size_t)z * w_per_slice : nullptr;
+        J.window = T.window;
+        J.ex_tab = T.ex_tab;
+        J.ey_tab = T.ey_tab;
+        J.sens = T.sens;
+        J.inv_ssum = T.inv_ssum;
+        J.combined = comb + ((size_t)gl * nz + z) * per;
+        J.nx = nx;
+        J.ny = ny;
+        J.nc = nc;
+        jobs.push_back(J);
+      }
+    const ReconJob* d_jobs = (const ReconJob*)C.upload(jobs.data(), jobs.size() * sizeof(ReconJob), st);
+    if (accel > 1) launch_grappa_apply(d_jobs, (int)jobs.size(), T.fills, T.n_fills, nx, nc, st);
+    launch_recon_combine(d_jobs, (int)jobs.size(), nx, ny, false, st);
+    volume_output_kernel<<<1024, 256, 0, st>>>(comb, g0, ngl, nv, per * nz, d_mag, d_ph);
+    MRSIM_CUDA(cudaGetLastError());
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  }
+  MRSIM_CUDA(cudaMemcpyAsync(mag, d_mag, per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+  MRSIM_CUDA(cudaMemcpyAsync(ph, d_ph, per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace mrsim

@@ -15,23 +15,12 @@
 #include "noise_kernels.h"
 #include "recon_kernels.h"
 #include "series.h"
+#include "series_parts.h"
 
 namespace mrsim {
 
-namespace {
 
 // Tables of one acquired geometry for the reconstruction.
-struct ReconTables {
-  float2* ex_tab = nullptr;
-  float2* ey_tab = nullptr;
-  float* sens = nullptr;
-  float* inv_ssum = nullptr;
-  float* window = nullptr;
-  int4* fills = nullptr;
-  int n_fills = 0;
-  std::vector<float> sens_host;
-};
-
 ReconTables build_recon_tables(DevArena& A, int nx, int ny, int nc, const mrsim_acquisition& acq, cudaStream_t st) {
   ReconTables T;
   const int xs = nx / 2, ys = ny / 2;
@@ -81,32 +70,6 @@ ReconTables build_recon_tables(DevArena& A, int nx, int ny, int nc, const mrsim_
 }
 
 // One batch of forward units: descriptors, statics, plan.
-struct Batch {
-  std::vector<UnitDesc> units;
-  std::vector<StaticDesc> statics;
-};
-
-struct UnitInputs {
-  const float* comp;
-  long long comp_stride;
-  const float* fmap;
-  const float* t2map;
-  const float* timap;
-  long long map_stride;
-  const float* log_amp;
-  const LineRec* lines;
-  int n_lines;
-  float2* kspace;
-  float2* g;
-  float* phase_out;
-  const double* phase0;  // explicit phase (device) or NULL: the phase model
-  const mrsim_phase_model* phase;
-  ShotParams shot;
-  int z, nz_full;
-  bool has_eddy;
-  double grad[3];
-};
-
 void add_unit(Batch& B, const UnitInputs& in, int snx, int sny, int nx, int ny, int ncomp, int ncoils, bool maps,
               const float* t2u, const float* tiu, const GeoTab& geo, const mrsim_acquisition& acq) {
   const bool eddy = acq.eddy_strength != 0.0 && in.has_eddy;
@@ -220,14 +183,6 @@ void lines_for(std::vector<LineRec>& out, const mrsim_acquisition& acq, int nx, 
   }
 }
 
-// spikes + noise for a list of (k-space of one coil) jobs
-struct NoiseSpec {
-  float2* k;
-  uint64_t slice_seed;
-  int coil;
-  int pick_offset;  // into the picks array, n_spikes per unit
-};
-
 void run_noise(DevArena& A, const std::vector<NoiseSpec>& specs, const std::vector<int>& rows,
                const std::vector<int>& picks, int nx, int ny, const mrsim_acquisition& acq, cudaStream_t st) {
   const bool do_spikes = acq.n_spikes > 0 && !picks.empty();
@@ -317,7 +272,6 @@ bool uniform_relaxation(const mrsim_t2* t2, const mrsim_t2* ti, int ncomp) {
   return u;
 }
 
-}  // namespace
 
 // =============================================================================================
 // Per slice (`simulate_slice_with`, kspace.rs:1271-1284)

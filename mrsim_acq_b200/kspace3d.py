@@ -1,0 +1,152 @@
+"""Python mirror of the reference's 3D echo-train acquisition (`kspace3d.rs`, `readout.rs:75-322`)
+over the C ABI: `EchoTrain`, `KzOrder`, `Readout3d::Grase`, `LineWeights`, `kz_order`,
+`grase_lines`, `simulate_acquisition_3d` and `kspace_3d_observed`.  The acquisition runs on the
+device (no CPU path)."""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import enum
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .abi import check, lib
+from .api import Acquisition, Context, PhaseModel, T2, _Keep, default_context
+
+
+class KzOrder(enum.IntEnum):  # readout.rs:75-80
+    Centric = 0
+    Linear = 1
+
+
+@dataclasses.dataclass
+class EchoTrain:
+    """`EchoTrain` (readout.rs:82-95)."""
+
+    etl: int
+    esp_ms: float
+    refocusing_deg: float
+    kz_order: KzOrder = KzOrder.Centric
+    kz_segments: int = 1
+    refocusing_time_ms: float = 2.0
+
+    def to_c(self) -> abi.EchoTrain_:
+        return abi.EchoTrain_(int(self.etl), float(self.esp_ms), float(self.refocusing_deg), int(self.kz_order), 0,
+                              int(self.kz_segments), float(self.refocusing_time_ms))
+
+
+@dataclasses.dataclass
+class GraseReadout:
+    """`Readout3d::Grase` (readout.rs:103-106)."""
+
+    ky_segments: int
+    t_line_ms: float
+    reverse_phase: bool = False
+
+    def to_c(self) -> abi.GraseReadout_:
+        return abi.GraseReadout_(int(self.ky_segments), float(self.t_line_ms), int(bool(self.reverse_phase)), 0)
+
+
+@dataclasses.dataclass
+class LineWeights:
+    """`LineWeights` (kspace3d.rs:46-60): w[(g * n_shots + s) * n_compartments + c]."""
+
+    n_shots: int
+    n_compartments: int
+    w: np.ndarray
+
+
+@dataclasses.dataclass
+class GraseTable:
+    """`Grase3dTable` (readout.rs:236-280): per line p * ny + ky."""
+
+    shot: np.ndarray
+    echo: np.ndarray
+    t_ms: np.ndarray
+    trf_ms: np.ndarray
+    polarity: np.ndarray
+    e_c: int
+    n_shots: int
+
+
+def kz_order(nz: int, order: KzOrder) -> np.ndarray:
+    out = np.zeros(nz, np.int64)
+    check(lib().mrsim_kz_order(nz, int(order), out.ctypes.data_as(C.POINTER(C.c_int64))))
+    return out
+
+
+def grase_lines(train: EchoTrain, ro: GraseReadout, ny: int, nz: int) -> GraseTable:
+    n = ny * nz
+    shot, echo = np.zeros(n, np.int64), np.zeros(n, np.int64)
+    t, trf, pol = np.zeros(n), np.zeros(n), np.zeros(n, np.int8)
+    e_c, n_shots = C.c_int64(), C.c_int64()
+    P = C.POINTER(C.c_int64)
+    check(lib().mrsim_grase_lines(C.byref(train.to_c()), C.byref(ro.to_c()), ny, nz, shot.ctypes.data_as(P),
+                                  echo.ctypes.data_as(P), t.ctypes.data_as(abi.c_f64p), trf.ctypes.data_as(abi.c_f64p),
+                                  pol.ctypes.data_as(C.POINTER(C.c_int8)), C.byref(e_c), C.byref(n_shots)))
+    return GraseTable(shot, echo, t, trf, pol, e_c.value, n_shots.value)
+
+
+def acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,
+                           t_inhom: Optional[Sequence[T2]], phase: Optional[PhaseModel],
+                           line_weights: Optional[LineWeights], grappa_calibration, keep: _Keep):
+    s = abi.Acquisition3dInput_()
+    for i in range(3):
+        s.sim_dims[i] = int(sim_dims[i])
+        s.acq_dims[i] = int(acq_dims[i])
+    s.n_volumes = int(n_volumes)
+    s.ncomp = len(images)
+    s.images = keep.ptrs([np.ravel(a) for a in images])
+    s.t2 = keep.t2s(t2)
+    s.t1 = keep.t2s(t1) if t1 is not None else None
+    s.fmap = keep.f32(np.ravel(fmap))
+    s.t_inhom = keep.t2s(t_inhom) if t_inhom is not None else None
+    if phase is not None:
+        pm = phase.to_c()
+        keep.append(pm)
+        s.phase = C.pointer(pm)
+    if line_weights is not None:
+        s.line_weights = keep.f64(np.ravel(line_weights.w))
+    if grappa_calibration is not None:
+        cal_images, cal_seed = grappa_calibration
+        s.has_grappa_calibration = 1
+        s.grappa_calibration_images = keep.ptrs([np.ravel(a) for a in cal_images])
+        s.grappa_calibration_seed = int(cal_seed) & 0xFFFFFFFFFFFFFFFF
+    return s
+
+
+def simulate_acquisition_3d(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T2], t1: Optional[Sequence[T2]],
+                            fmap, t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain,
+                            readout: GraseReadout, line_weights: Optional[LineWeights] = None,
+                            phase: Optional[PhaseModel] = None, seed: int = 0, grappa_calibration=None,
+                            ctx: Optional[Context] = None):
+    """`simulate_acquisition_3d` (kspace3d.rs:549-565), GRASE: (magnitude, phase) f32 at vox * nv + g."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
+                               grappa_calibration, keep)
+    n = int(np.prod(acq_dims)) * n_volumes
+    mag, ph = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    check(lib().mrsim_simulate_acquisition_3d(ctx.handle, C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
+                                              C.byref(readout.to_c()), int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                              mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
+    return mag, ph
+
+
+def kspace_3d_observed(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,
+                       t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain, readout: GraseReadout,
+                       line_weights: Optional[LineWeights] = None, phase: Optional[PhaseModel] = None, g: int = 0,
+                       ctx: Optional[Context] = None) -> np.ndarray:
+    """`kspace_3d_observed` (kspace3d.rs:439-456): complex64 [coil, p, ky, kx] of volume g."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
+                               None, keep)
+    nx, ny, nz = acq_dims
+    nc = max(int(acq.n_coils), 1)
+    out = np.zeros(nc * nz * ny * nx, np.complex64)
+    check(lib().mrsim_kspace_3d_observed(ctx.handle, C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
+                                         C.byref(readout.to_c()), g, out.view(np.float32).ctypes.data_as(abi.c_f32p)))
+    return out.reshape(nc, nz, ny, nx)

@@ -2226,6 +2226,419 @@ struct SpiralReconO {
   }
 };
 
+
+// ============================ the 3D GRASE echo train =====================================
+// readout.rs:167-322 (kz order, GRASE block and lines), epg.rs:47-125 (CPMG amplitudes),
+// kspace3d.rs:42-547 (modes, z-DFT, compartments, line weights, partitions, reconstruction).
+std::vector<size_t> kz_order_o(size_t nz, int order) {
+  std::vector<size_t> out;
+  if (order == MRSIM_KZ_LINEAR) {
+    for (size_t p = 0; p < nz; ++p) out.push_back(p);
+    return out;
+  }
+  size_t c = nz / 2;
+  out.push_back(c);
+  size_t d = 1;
+  while (out.size() < nz) {
+    if (c + d < nz) out.push_back(c + d);
+    if (d <= c && out.size() < nz) out.push_back(c - d);
+    ++d;
+  }
+  return out;
+}
+
+struct GLine {
+  size_t shot, echo;
+  double t_ms, trf_ms;
+  int8_t pol;
+};
+struct GTable {
+  size_t ny, nz, e_c, n_shots;
+  std::vector<GLine> lines;
+  std::vector<double> t_ms;
+  std::vector<int8_t> pol;
+  const GLine& line(size_t p, size_t ky) const { return lines[p * ny + ky]; }
+};
+
+GTable grase_lines_o(const mrsim_echo_train& tr, const mrsim_grase_readout& ro, size_t ny, size_t nz) {
+  size_t kys = (size_t)ro.ky_segments, kzs = (size_t)tr.kz_segments;
+  if (kys == 0 || ny % kys != 0) throw Fail("phase-encode lines do not divide into ky segments");
+  size_t epi = ny / kys;
+  GTable T;
+  T.ny = ny;
+  T.nz = nz;
+  T.t_ms.resize(ny);
+  T.pol.resize(ny);
+  for (size_t ky = 0; ky < ny; ++ky) {
+    size_t j = ky / kys;
+    size_t a = ro.reverse_phase ? j : epi - 1 - j;
+    T.t_ms[ky] = ((double)a - ((double)epi - 1.0) / 2.0) * ro.t_line_ms;
+    T.pol[ky] = a % 2 == 1 ? -1 : 1;
+  }
+  if (kzs == 0 || nz % kzs != 0) throw Fail("partitions do not divide into kz segments");
+  if ((size_t)tr.etl != nz / kzs) throw Fail("echo train length mismatch");
+  std::vector<size_t> order = kz_order_o(nz, tr.kz_order);
+  T.lines.assign(ny * nz, GLine{0, 0, 0.0, 0.0, 0});
+  for (size_t sy = 0; sy < kys; ++sy)
+    for (size_t sz = 0; sz < kzs; ++sz) {
+      size_t shot = sy * kzs + sz;
+      for (size_t e = 1; e <= (size_t)tr.etl; ++e) {
+        size_t pp = order[sz + kzs * (e - 1)];
+        for (size_t j = 0; j < epi; ++j) {
+          size_t ky = sy + kys * j;
+          double t = T.t_ms[ky];
+          T.lines[pp * ny + ky] = GLine{shot, e, t, (double)e * tr.esp_ms + t, T.pol[ky]};
+        }
+      }
+    }
+  size_t n = 0;
+  while (order[n] != nz / 2) ++n;
+  T.e_c = n / kzs + 1;
+  T.n_shots = kys * kzs;
+  return T;
+}
+
+// `epg_cpmg` epg.rs:101-125 (Weigel's extended phase graphs; ln of the echo amplitudes)
+std::vector<double> epg_cpmg_o(size_t n_echoes, double esp, double b_deg, double t1, double t2) {
+  size_t n = 2 * n_echoes + 2;
+  std::vector<Cx> fp(n, Cx{0, 0}), fm(n, Cx{0, 0}), z(n, Cx{0, 0});
+  z[0] = {1.0, 0.0};
+  auto rot = [&](double alpha, double phi) {
+    double ch = std::cos(alpha / 2.0), sh = std::sin(alpha / 2.0);
+    double c2 = ch * ch, s2 = sh * sh, sa = std::sin(alpha), ca = std::cos(alpha);
+    Cx e2p = ccis(2.0 * phi), e2m = ccis(-2.0 * phi), e1p = ccis(phi), e1m = ccis(-phi);
+    Cx I{0.0, 1.0}, mI{0.0, -1.0};
+    for (size_t k = 0; k < n; ++k) {
+      Cx a = fp[k], b = fm[k], c = z[k];
+      fp[k] = cadd(cadd(cscale(a, c2), cscale(cmul(e2p, b), s2)), cscale(cmul(cmul(mI, e1p), c), sa));
+      fm[k] = cadd(cadd(cscale(cmul(e2m, a), s2), cscale(b, c2)), cscale(cmul(cmul(I, e1m), c), sa));
+      z[k] = cadd(cadd(cscale(cmul(cmul(mI, e1m), a), sa / 2.0), cscale(cmul(cmul(I, e1p), b), sa / 2.0)), cscale(c, ca));
+    }
+  };
+  auto relax = [&](double e1, double e2) {
+    for (size_t k = 0; k < n; ++k) {
+      fp[k] = cscale(fp[k], e2);
+      fm[k] = cscale(fm[k], e2);
+      z[k] = cscale(z[k], e1);
+    }
+    z[0] = cadd(z[0], Cx{1.0 - e1, 0.0});
+  };
+  auto shift = [&]() {
+    for (size_t k = n - 1; k >= 1; --k) fp[k] = fp[k - 1];
+    for (size_t k = 0; k + 1 < n; ++k) fm[k] = fm[k + 1];
+    fm[n - 1] = {0.0, 0.0};
+    fp[0] = {fm[0].re, -fm[0].im};
+  };
+  auto decay = [](double dt, double t) { return std::isinf(t) ? 1.0 : std::exp(-dt / t); };
+  rot(PI / 2.0, 0.0);
+  double norm = std::hypot(fp[0].re, fp[0].im);
+  double e1 = decay(esp / 2.0, t1), e2 = decay(esp / 2.0, t2);
+  std::vector<double> out(n_echoes);
+  for (size_t e = 0; e < n_echoes; ++e) {
+    relax(e1, e2);
+    shift();
+    rot(b_deg * PI / 180.0, PI / 2.0);
+    shift();
+    relax(e1, e2);
+    double a = std::hypot(fp[0].re, fp[0].im) / norm;
+    out[e] = a == 0.0 ? -INFINITY : std::log(a);
+  }
+  return out;
+}
+
+struct Mode3 {
+  bool voxel = false;
+  std::vector<double> ln_a;
+  double t2 = 0, t2p = 0;
+  std::vector<std::vector<double>> maps;
+};
+
+std::vector<Mode3> resolve_modes_o(const mrsim_t2* t2, const mrsim_t2* t1, const mrsim_t2* ti, size_t ncomp,
+                                   const mrsim_acquisition& acq, const mrsim_echo_train& tr, size_t nvox) {
+  if (acq.do_relaxation && tr.refocusing_deg != 180.0 && !t1) throw Fail("refocusing below 180 degrees needs T1");
+  size_t etl = (size_t)tr.etl;
+  std::vector<Mode3> modes(ncomp);
+  for (size_t c = 0; c < ncomp; ++c) {
+    mrsim_t2 t1c = t1 ? t1[c] : mrsim_t2{nullptr, INFINITY, 0};
+    mrsim_t2 tic = ti ? ti[c] : mrsim_t2{nullptr, (float)acq.t_inhom, 0};
+    if (!t2[c].is_map && !t1c.is_map && !tic.is_map) {
+      modes[c].ln_a = epg_cpmg_o(etl, tr.esp_ms, tr.refocusing_deg, (double)t1c.value, (double)t2[c].value);
+      modes[c].t2 = t2[c].value;
+      modes[c].t2p = tic.value;
+    } else if (!acq.do_relaxation) {
+      modes[c].ln_a.assign(etl, 0.0);
+      modes[c].t2 = INFINITY;
+      modes[c].t2p = INFINITY;
+    } else {
+      modes[c].voxel = true;
+      modes[c].maps.assign(etl, std::vector<double>(nvox));
+      for (size_t i = 0; i < nvox; ++i) {
+        float a = t1c.is_map ? t1c.map[i] : t1c.value, b = t2[c].is_map ? t2[c].map[i] : t2[c].value;
+        std::vector<double> la = epg_cpmg_o(etl, tr.esp_ms, tr.refocusing_deg, (double)a, (double)b);
+        for (size_t e = 0; e < etl; ++e) modes[c].maps[e][i] = la[e];
+      }
+    }
+  }
+  return modes;
+}
+
+double line_weight_o(double ln_a, double t, double t2, double t2p) {
+  double d2 = std::isinf(t2) ? 0.0 : t / t2;
+  double dp = std::isinf(t2p) ? 0.0 : std::fabs(t) / t2p;
+  return std::exp(ln_a - d2 - dp);
+}
+
+struct Plan3 {
+  size_t snx, sny, nz, nx, ny, o, ncomp;
+  mrsim_acquisition acq;
+  GTable table;
+  LineTiming within;
+  std::vector<Mode3> modes;
+  const mrsim_t2* t2;
+  const mrsim_t2* ti;
+  const float* fmap;
+  mrsim_phase_model phase;
+  std::vector<Cx> zk;
+  std::vector<uint8_t> mask;
+
+  // `Plan::compartments` kspace3d.rs:125-204: img(c, vox) of one volume, coil q
+  std::vector<std::vector<Cx>> compartments(const std::function<float(size_t, size_t)>& img, size_t q,
+                                            size_t ncoils) const {
+    size_t nplane = snx * sny;
+    mrsim_acquisition norel = acq, rel = acq;
+    norel.do_relaxation = 0;
+    norel.noise_variance = 0.0;
+    norel.n_spikes = 0;
+    rel.do_relaxation = 1;
+    rel.noise_variance = 0.0;
+    rel.n_spikes = 0;
+    Shot zero;
+    std::vector<std::vector<double>> phis(nz);
+    for (size_t z = 0; z < nz; ++z) phis[z] = phase_slice(phase, zero, snx, sny, o, z, nz);
+    std::vector<std::vector<Cx>> out(ncomp, std::vector<Cx>(nz * ny * nx, Cx{0, 0}));
+    for (size_t c = 0; c < ncomp; ++c) {
+      auto plane = [&](size_t z) {
+        std::vector<float> v(nplane);
+        for (size_t i = 0; i < nplane; ++i) v[i] = img(c, z * nplane + i);
+        return v;
+      };
+      auto one = [&](size_t z, const std::vector<float>& pl, const mrsim_acquisition& a, const double* la) {
+        const float* comps[1] = {pl.data()};
+        mrsim_t2 t2s[1] = {t2[c].is_map ? mrsim_t2{t2[c].map + z * nplane, 0.f, 1} : t2[c]};
+        mrsim_t2 tis[1];
+        if (ti) tis[0] = ti[c].is_map ? mrsim_t2{ti[c].map + z * nplane, 0.f, 1} : ti[c];
+        mrsim_slice_input inp;
+        std::memset(&inp, 0, sizeof inp);
+        inp.compartments = comps;
+        inp.ncomp = 1;
+        inp.t2 = t2s;
+        inp.t_inhom = ti ? tis : nullptr;
+        inp.fmap = fmap + z * nplane;
+        inp.phase0 = phis[z].data();
+        inp.sim[0] = (int64_t)snx;
+        inp.sim[1] = (int64_t)sny;
+        inp.acq_matrix[0] = (int64_t)nx;
+        inp.acq_matrix[1] = (int64_t)ny;
+        inp.z = (int64_t)z;
+        inp.nz = (int64_t)nz;
+        return build_coil_kspace_timed(inp, a, q, ncoils, within, la);
+      };
+      const Mode3& m = modes[c];
+      if (!m.voxel) {
+        std::vector<std::vector<Cx>> k2(nz);
+        for (size_t z = 0; z < nz; ++z) k2[z] = one(z, plane(z), norel, nullptr);
+        for (size_t p = 0; p < nz; ++p)
+          for (size_t ky = 0; ky < ny; ++ky) {
+            const GLine& L = table.line(p, ky);
+            double w = acq.do_relaxation ? line_weight_o(m.ln_a[L.echo - 1], L.t_ms, m.t2, m.t2p) : 1.0;
+            for (size_t kx = 0; kx < nx; ++kx) {
+              Cx acc{0, 0};
+              for (size_t z = 0; z < nz; ++z) acc = cadd(acc, cmul(k2[z][ky * nx + kx], zk[p * nz + z]));
+              out[c][(p * ny + ky) * nx + kx] = cscale(acc, w);
+            }
+          }
+      } else {
+        std::vector<std::vector<float>> planes(nz);
+        for (size_t z = 0; z < nz; ++z) planes[z] = plane(z);
+        size_t emax = 0;
+        for (auto& L : table.lines) emax = std::max(emax, L.echo);
+        for (size_t e = 1; e <= emax; ++e) {
+          std::vector<size_t> ps;
+          for (size_t p = 0; p < nz; ++p)
+            if (table.line(p, 0).echo == e) ps.push_back(p);
+          if (ps.empty()) continue;
+          std::vector<std::vector<Cx>> k2(nz);
+          for (size_t z = 0; z < nz; ++z) k2[z] = one(z, planes[z], rel, m.maps[e - 1].data() + z * nplane);
+          for (size_t p : ps)
+            for (size_t ky = 0; ky < ny; ++ky)
+              for (size_t kx = 0; kx < nx; ++kx) {
+                Cx acc{0, 0};
+                for (size_t z = 0; z < nz; ++z) acc = cadd(acc, cmul(k2[z][ky * nx + kx], zk[p * nz + z]));
+                out[c][(p * ny + ky) * nx + kx] = acc;
+              }
+        }
+      }
+    }
+    return out;
+  }
+
+  // `Plan::kspace` kspace3d.rs:206-232 (no shot images)
+  std::vector<Cx> kspace(const float* const* images, size_t n_volumes, size_t g, size_t q, size_t ncoils,
+                         const double* lw) const {
+    auto base = compartments([&](size_t c, size_t v) { return images[c][v * n_volumes + g]; }, q, ncoils);
+    std::vector<Cx> k(nz * ny * nx, Cx{0, 0});
+    for (size_t p = 0; p < nz; ++p)
+      for (size_t ky = 0; ky < ny; ++ky) {
+        const GLine& L = table.line(p, ky);
+        for (size_t c = 0; c < ncomp; ++c) {
+          double w = lw ? lw[(g * table.n_shots + L.shot) * ncomp + c] : 1.0;
+          for (size_t kx = 0; kx < nx; ++kx) {
+            size_t i = (p * ny + ky) * nx + kx;
+            k[i] = cadd(k[i], cscale(base[c][i], w));
+          }
+        }
+        if (!mask[ky * nx])
+          for (size_t kx = 0; kx < nx; ++kx) k[(p * ny + ky) * nx + kx] = Cx{0, 0};
+      }
+    return k;
+  }
+};
+
+Plan3 plan3(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq, const mrsim_echo_train& tr,
+            const mrsim_grase_readout& ro) {
+  Plan3 P;
+  P.snx = in.sim_dims[0];
+  P.sny = in.sim_dims[1];
+  P.nz = in.sim_dims[2];
+  P.nx = in.acq_dims[0];
+  P.ny = in.acq_dims[1];
+  if ((size_t)in.acq_dims[2] != P.nz) throw Fail("partition count must match; z is never oversampled");
+  P.o = P.snx / P.nx;
+  P.ncomp = in.ncomp;
+  P.acq = acq;
+  P.table = grase_lines_o(tr, ro, P.ny, P.nz);
+  P.within.t_ms = P.table.t_ms;
+  P.within.trf_ms = P.table.t_ms;
+  P.within.tread_ms = P.table.t_ms;
+  P.within.polarity = P.table.pol;
+  P.modes = resolve_modes_o(in.t2, in.t1, in.t_inhom, P.ncomp, acq, tr, P.snx * P.sny * P.nz);
+  P.t2 = in.t2;
+  P.ti = in.t_inhom;
+  P.fmap = in.fmap;
+  if (in.phase) P.phase = *in.phase;
+  else std::memset(&P.phase, 0, sizeof P.phase);
+  double zs = (double)(P.nz / 2);
+  P.zk.resize(P.nz * P.nz);
+  for (size_t p = 0; p < P.nz; ++p)
+    for (size_t z = 0; z < P.nz; ++z) {
+      double th = TAU * ((double)p - zs) * ((double)z - zs) / (double)P.nz;
+      P.zk[p * P.nz + z] = Cx{std::cos(th), std::sin(th)};
+    }
+  P.mask = sampling_mask(P.nx, P.ny, acq);
+  return P;
+}
+
+// `partitions_to_slices` kspace3d.rs:235-281
+std::vector<std::vector<Cx>> partitions_to_slices_o(std::vector<Cx>& k, const std::vector<uint8_t>& mask,
+                                                    const std::vector<Cx>& zk, size_t nx, size_t ny, size_t nz,
+                                                    size_t g, size_t q, uint64_t seed, const mrsim_acquisition& acq,
+                                                    double sigma) {
+  const uint64_t salt3d = 0x334452454144ull;
+  for (size_t p = 0; p < nz; ++p) {
+    Cx* part = k.data() + p * ny * nx;
+    uint64_t pseed = (((uint64_t)g * 0x1000001ull) + (uint64_t)p) * 0x9E37ull ^ seed ^ salt3d;
+    if (acq.n_spikes > 0) {
+      Cx peak{0, 0};
+      double pm = 0.0;
+      for (size_t i = 0; i < nx * ny; ++i)
+        if (cabs_(part[i]) > pm) {
+          pm = cabs_(part[i]);
+          peak = part[i];
+        }
+      std::vector<size_t> acquired;
+      for (size_t i = 0; i < nx * ny; ++i)
+        if (mask[i]) acquired.push_back(i);
+      Rng rng(pseed ^ 0xA5A5123456789ABCull ^ ((uint64_t)q * 0xC2B2AE3D27D4EB4Full));
+      for (int64_t s2 = 0; s2 < acq.n_spikes; ++s2) {
+        size_t pick = acquired[(size_t)(rng.next_u64() % (uint64_t)acquired.size())];
+        part[pick] = cscale(peak, acq.spike_amplitude);
+      }
+    }
+    if (acq.noise_variance > 0.0) {
+      Rng rng((pseed ^ ((uint64_t)q * 0x9E3779B9ull)) | 1ull);
+      for (size_t i = 0; i < nx * ny; ++i)
+        if (mask[i]) {
+          part[i].re += rng.gauss() * sigma;
+          part[i].im += rng.gauss() * sigma;
+        }
+    }
+  }
+  std::vector<std::vector<Cx>> slices(nz, std::vector<Cx>(ny * nx, Cx{0, 0}));
+  for (size_t z = 0; z < nz; ++z) {
+    for (size_t p = 0; p < nz; ++p) {
+      Cx kc = zk[p * nz + z];
+      Cx conj{kc.re, -kc.im};
+      for (size_t i = 0; i < ny * nx; ++i) slices[z][i] = cadd(slices[z][i], cmul(k[p * ny * nx + i], conj));
+    }
+    for (Cx& c : slices[z]) c = cscale(c, 1.0 / (double)nz);
+  }
+  return slices;
+}
+
+// `simulate_acquisition_3d_complex_cal` kspace3d.rs:483-547 (GRASE, no shot images)
+std::vector<std::vector<Cx>> acquire_3d_o(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
+                                          const mrsim_echo_train& tr, const mrsim_grase_readout& ro, uint64_t seed,
+                                          int threads) {
+  Plan3 pl = plan3(in, acq, tr, ro);
+  size_t nz = pl.nz, nx = pl.nx, ny = pl.ny, nv = in.n_volumes;
+  size_t ncoils = std::max<int64_t>(acq.n_coils, 1);
+  double sigma = std::sqrt(acq.noise_variance / (double)(nx * ny));
+  std::vector<GrappaKernel> kernels;
+  if (acq.accel > 1 && nv > 0) {
+    mrsim_acquisition acq_cal = acq;
+    acq_cal.accel = 1;
+    acq_cal.n_spikes = 0;
+    const float* const* cal_images = in.images;
+    size_t cal_nv = nv;
+    uint64_t cal_seed = seed;
+    if (in.has_grappa_calibration) {
+      cal_images = in.grappa_calibration_images;
+      cal_nv = 1;
+      cal_seed = in.grappa_calibration_seed;
+    }
+    Plan3 cal = plan3(in, acq_cal, tr, ro);
+    std::vector<std::vector<std::vector<Cx>>> parts(ncoils);
+    parallel_for(ncoils, threads, [&](size_t q) {
+      std::vector<Cx> k = cal.kspace(cal_images, cal_nv, 0, q, ncoils, nullptr);
+      parts[q] = partitions_to_slices_o(k, cal.mask, cal.zk, nx, ny, nz, 0, q, cal_seed ^ SEED_SALT_GRAPPA_CAL, acq_cal,
+                                        sigma);
+    });
+    std::vector<uint8_t> lines = sampling_mask(1, ny, acq_cal);
+    for (size_t z = 0; z < nz; ++z) {
+      std::vector<std::vector<Cx>> coils(ncoils);
+      for (size_t q = 0; q < ncoils; ++q) coils[q] = parts[q][z];
+      kernels.push_back(grappa_fit(coils, nx, ny, acq.accel, acq.acs_lines, lines));
+    }
+  }
+  std::vector<std::vector<Cx>> vols(nv);
+  parallel_for(nv, threads, [&](size_t g) {
+    std::vector<std::vector<std::vector<Cx>>> parts(ncoils);
+    for (size_t q = 0; q < ncoils; ++q) {
+      std::vector<Cx> k = pl.kspace(in.images, nv, g, q, ncoils, in.line_weights);
+      parts[q] = partitions_to_slices_o(k, pl.mask, pl.zk, nx, ny, nz, g, q, seed, acq, sigma);
+    }
+    std::vector<Cx> out(nx * ny * nz);
+    for (size_t z = 0; z < nz; ++z) {
+      std::vector<std::vector<Cx>> coils(ncoils);
+      for (size_t q = 0; q < ncoils; ++q) coils[q] = parts[q][z];
+      SliceRecon R = reconstruct_coils_full(coils, acq, nx, ny, false, false, false, kernels.empty() ? nullptr : &kernels[z]);
+      for (size_t i = 0; i < nx * ny; ++i) out[i + nx * ny * z] = R.combined[i];
+    }
+    vols[g] = out;
+  });
+  return vols;
+}
+
 thread_local std::string g_err;
 std::vector<GoldenCase>* g_golden = nullptr;
 
@@ -2505,6 +2918,67 @@ int oracle_spiral_recon(const double* k, int64_t npts, int64_t n, int32_t window
       else
         o = r.gridding(std::vector<Cx>(d + (size_t)b * npts, d + (size_t)(b + 1) * npts));
       put_cx(o, out + 2 * nn * (size_t)b);
+    }
+  });
+}
+
+int oracle_kz_order(int64_t nz, int32_t order, int64_t* out) {
+  return guard([&] {
+    auto v = kz_order_o((size_t)nz, order);
+    for (size_t i = 0; i < v.size(); ++i) out[i] = (int64_t)v[i];
+  });
+}
+
+int oracle_epg_cpmg(int64_t n, double esp, double b, double t1, double t2, double* out) {
+  return guard([&] {
+    auto v = epg_cpmg_o((size_t)n, esp, b, t1, t2);
+    std::memcpy(out, v.data(), v.size() * 8);
+  });
+}
+
+int oracle_grase_lines(const mrsim_echo_train* tr, const mrsim_grase_readout* ro, int64_t ny, int64_t nz, int64_t* shot,
+                       int64_t* echo, double* t_ms, double* trf_ms, int8_t* pol, int64_t* e_c, int64_t* n_shots) {
+  return guard([&] {
+    GTable T = grase_lines_o(*tr, *ro, (size_t)ny, (size_t)nz);
+    for (size_t i = 0; i < T.lines.size(); ++i) {
+      shot[i] = (int64_t)T.lines[i].shot;
+      echo[i] = (int64_t)T.lines[i].echo;
+      t_ms[i] = T.lines[i].t_ms;
+      trf_ms[i] = T.lines[i].trf_ms;
+      pol[i] = T.lines[i].pol;
+    }
+    *e_c = (int64_t)T.e_c;
+    *n_shots = (int64_t)T.n_shots;
+  });
+}
+
+int oracle_kspace_3d_observed(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                              const mrsim_echo_train* tr, const mrsim_grase_readout* ro, int64_t g, double* out) {
+  return guard([&] {
+    Plan3 pl = plan3(*in, *acq, *tr, *ro);
+    size_t ncoils = std::max<int64_t>(acq->n_coils, 1), per = pl.nz * pl.ny * pl.nx;
+    for (size_t q = 0; q < ncoils; ++q) {
+      std::vector<Cx> k = pl.kspace(in->images, in->n_volumes, (size_t)g, q, ncoils, in->line_weights);
+      put_cx(k, out + 2 * per * q);
+    }
+  });
+}
+
+// `simulate_acquisition_3d` (kspace3d.rs:549-589): complex volumes [g][vox] (FP64) and the f32
+// magnitude / phase at vox * nv + g
+int oracle_simulate_acquisition_3d(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                                   const mrsim_echo_train* tr, const mrsim_grase_readout* ro, uint64_t seed,
+                                   int32_t threads, double* vols_out, float* mag, float* ph) {
+  return guard([&] {
+    auto vols = acquire_3d_o(*in, *acq, *tr, *ro, seed, threads);
+    size_t nv = in->n_volumes;
+    for (size_t g = 0; g < vols.size(); ++g) {
+      if (vols_out) put_cx(vols[g], vols_out + 2 * vols[g].size() * g);
+      for (size_t vox = 0; vox < vols[g].size(); ++vox) {
+        float re = (float)vols[g][vox].re, im = (float)vols[g][vox].im;
+        if (mag) mag[vox * nv + g] = std::sqrt(re * re + im * im);
+        if (ph) ph[vox * nv + g] = std::atan2(im, re);
+      }
     }
   });
 }

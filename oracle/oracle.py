@@ -80,6 +80,15 @@ def lib():
                                           C.c_int64, C.c_double, C.c_int32, C.c_int32, abi.c_f64p, C.c_int64,
                                           C.c_int64, C.c_int64, abi.c_f64p, abi.c_f64p, abi.c_f64p, i64p,
                                           abi.c_f64p]
+        A3 = P(abi.Acquisition3dInput_)
+        L.oracle_kz_order.argtypes = [C.c_int64, C.c_int32, i64p]
+        L.oracle_epg_cpmg.argtypes = [C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, abi.c_f64p]
+        L.oracle_grase_lines.argtypes = [P(abi.EchoTrain_), P(abi.GraseReadout_), C.c_int64, C.c_int64, i64p, i64p,
+                                         abi.c_f64p, abi.c_f64p, P(C.c_int8), i64p, i64p]
+        L.oracle_kspace_3d_observed.argtypes = [A3, P(abi.Acquisition_), P(abi.EchoTrain_), P(abi.GraseReadout_),
+                                                C.c_int64, abi.c_f64p]
+        L.oracle_simulate_acquisition_3d.argtypes = [A3, P(abi.Acquisition_), P(abi.EchoTrain_), P(abi.GraseReadout_),
+                                                     C.c_uint64, C.c_int32, abi.c_f64p, abi.c_f32p, abi.c_f32p]
         _lib = L
     return _lib
 
@@ -399,3 +408,63 @@ def spiral_recon(k, n: int, data, mode: str = "image", window=(0, 0.0, 0.0), ite
                                      out.view(np.float64).ctypes.data_as(abi.c_f64p), C.byref(lam), C.byref(its),
                                      w.ctypes.data_as(abi.c_f64p)))
     return out.reshape(batch, n, n), lam.value, its.value, w
+
+
+# ---- the 3D GRASE echo train -------------------------------------------------------------------------
+def kz_order(nz: int, order: int) -> np.ndarray:
+    out = np.zeros(nz, np.int64)
+    _check(lib().oracle_kz_order(nz, int(order), out.ctypes.data_as(C.POINTER(C.c_int64))))
+    return out
+
+
+def epg_cpmg(n: int, esp: float, b: float, t1: float, t2: float) -> np.ndarray:
+    out = np.zeros(n)
+    _check(lib().oracle_epg_cpmg(n, esp, b, t1, t2, out.ctypes.data_as(abi.c_f64p)))
+    return out
+
+
+def grase_lines(train, ro, ny: int, nz: int) -> dict:
+    n = ny * nz
+    shot, echo = np.zeros(n, np.int64), np.zeros(n, np.int64)
+    t, trf, pol = np.zeros(n), np.zeros(n), np.zeros(n, np.int8)
+    e_c, n_shots = C.c_int64(), C.c_int64()
+    P = C.POINTER(C.c_int64)
+    _check(lib().oracle_grase_lines(C.byref(train.to_c()), C.byref(ro.to_c()), ny, nz, shot.ctypes.data_as(P),
+                                    echo.ctypes.data_as(P), t.ctypes.data_as(abi.c_f64p), trf.ctypes.data_as(abi.c_f64p),
+                                    pol.ctypes.data_as(C.POINTER(C.c_int8)), C.byref(e_c), C.byref(n_shots)))
+    return {"shot": shot, "echo": echo, "t_ms": t, "trf_ms": trf, "polarity": pol, "e_c": e_c.value,
+            "n_shots": n_shots.value}
+
+
+def kspace_3d_observed(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition, train, ro,
+                       line_weights=None, phase=None, g: int = 0) -> np.ndarray:
+    """`kspace_3d_observed` (kspace3d.rs:439-456), FP64: complex128 [coil, p, ky, kx]."""
+    from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
+                               None, keep)
+    nx, ny, nz = acq_dims
+    nc = max(acq.n_coils, 1)
+    out = np.zeros(nc * nz * ny * nx, np.complex128)
+    _check(lib().oracle_kspace_3d_observed(C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()), C.byref(ro.to_c()),
+                                           g, out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+    return out.reshape(nc, nz, ny, nx)
+
+
+def simulate_acquisition_3d(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition, train, ro,
+                            line_weights=None, phase=None, seed: int = 0, grappa_calibration=None, threads: int = 0):
+    """`simulate_acquisition_3d` (kspace3d.rs:549-589), FP64: (complex volumes [g, vox], mag, phase)."""
+    import os
+    from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
+                               grappa_calibration, keep)
+    nvox = int(np.prod(acq_dims))
+    vols = np.zeros(n_volumes * nvox, np.complex128)
+    mag, ph = np.zeros(nvox * n_volumes, np.float32), np.zeros(nvox * n_volumes, np.float32)
+    _check(lib().oracle_simulate_acquisition_3d(C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
+                                                C.byref(ro.to_c()), int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                                threads or (os.cpu_count() or 1),
+                                                vols.view(np.float64).ctypes.data_as(abi.c_f64p),
+                                                mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
+    return vols.reshape(n_volumes, nvox), mag, ph
