@@ -383,6 +383,58 @@ int mrsim_kspace_3d_observed(mrsim_context* ctx, const mrsim_acquisition_3d_inpu
                              const mrsim_acquisition* acq, const mrsim_echo_train* train,
                              const mrsim_grase_readout* ro, int64_t g, float* out);
 
+/* ---- the stack of spirals (kspace3d.rs:858-1569, readout.rs:107-160, 622-700) -------------- */
+/* `KzSampling` (readout.rs:107-160). */
+typedef struct mrsim_kz_sampling {
+  double partial_fourier;  /* (0.5, 1] */
+  int64_t accel;           /* >= 1 */
+} mrsim_kz_sampling;
+
+/* `Readout3d::Spiral` (readout.rs:103-106). */
+typedef struct mrsim_spiral_readout {
+  int64_t interleaves;
+  double readout_ms;
+  double dwell_ms;
+  double radial_oversampling;
+  mrsim_kz_sampling kz;
+} mrsim_spiral_readout;
+
+/* `KzOptions` (kspace3d.rs:1173-1178): coil rings along z, the kz calibration acquisition
+ * (images: ncomp sim volumes, read only when kz.accel > 1) and the partial-Fourier recon
+ * (0 = ZeroFill, 1 = Pocs). */
+typedef struct mrsim_kz_options {
+  int64_t coil_rows;
+  const float* const* calibration_images;
+  uint64_t calibration_seed;
+  int32_t pocs;
+  int32_t reserved;
+} mrsim_kz_options;
+
+/* `spiral_lines` (readout.rs:653-676): per partition acquired (0/1), echo (1-based, 0 = not
+ * read) and kz segment; band start, centre echo, shots, and the samples per interleaf. */
+int mrsim_spiral_lines(const mrsim_echo_train* train, const mrsim_spiral_readout* ro, int64_t nx,
+                       int64_t ny, int64_t nz, uint8_t* acquired, int64_t* echo,
+                       int64_t* kz_segment, int64_t* band_start, int64_t* e_c, int64_t* n_shots,
+                       int64_t* samples_per_interleaf);
+/* `simulate_acquisition_3d_kz` (kspace3d.rs:567-589) with a spiral readout (`spiral_volumes`
+ * :1472-1569): per slice the certified time-segmented forward of every compartment and coil
+ * element, the centred z-DFT with the rings' z profiles, echo amplitudes and line weights, the
+ * noise per (volume, partition, coil), the kz GRAPPA fill from the calibration acquisition, POCS or
+ * zero fill along z, the inverse z-DFT and the spiral reconstruction with the ring Roemer
+ * combine, on the device.  kz_opts may be NULL (one ring, no kz acceleration).  mag / phase f32
+ * at vox*nv + g. */
+int mrsim_simulate_acquisition_3d_spiral(mrsim_context* ctx, const mrsim_acquisition_3d_input* in,
+                                         const mrsim_acquisition* acq, const mrsim_echo_train* train,
+                                         const mrsim_spiral_readout* ro,
+                                         const mrsim_kz_options* kz_opts, uint64_t seed,
+                                         float* mag, float* phase);
+/* `SpiralPlan::samples_all` (kspace3d.rs:1047-1060): volume g's samples per coil before noise,
+ * out [coil][p*nsamp + j] (re, im) f32 (zero on partitions not read). */
+int mrsim_spiral_samples_3d(mrsim_context* ctx, const mrsim_acquisition_3d_input* in,
+                            const mrsim_acquisition* acq, const mrsim_echo_train* train,
+                            const mrsim_spiral_readout* ro, const mrsim_kz_options* kz_opts,
+                            int64_t g, float* out);
+
 /* ---- the stack-of-spirals path: host plans ------------------------------------------------ */
 /* `spiral_tau_c` (readout.rs:564-596): the constant-angular-velocity centre region (ms). */
 int mrsim_spiral_tau_c(int64_t nx, int64_t interleaves, double readout_ms, double dwell_ms,

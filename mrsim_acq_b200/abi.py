@@ -134,6 +134,26 @@ class Acquisition3dInput_(C.Structure):
     ]
 
 
+class KzSampling_(C.Structure):
+    """`mrsim_kz_sampling` — `KzSampling` (readout.rs:107-160)."""
+
+    _fields_ = [("partial_fourier", C.c_double), ("accel", C.c_int64)]
+
+
+class SpiralReadout_(C.Structure):
+    """`mrsim_spiral_readout` — `Readout3d::Spiral` (readout.rs:103-106)."""
+
+    _fields_ = [("interleaves", C.c_int64), ("readout_ms", C.c_double), ("dwell_ms", C.c_double),
+                ("radial_oversampling", C.c_double), ("kz", KzSampling_)]
+
+
+class KzOptions_(C.Structure):
+    """`mrsim_kz_options` — `KzOptions` (kspace3d.rs:1173-1178)."""
+
+    _fields_ = [("coil_rows", C.c_int64), ("calibration_images", C.POINTER(c_f32p)), ("calibration_seed", C.c_uint64),
+                ("pocs", C.c_int32), ("reserved", C.c_int32)]
+
+
 class LibraryMissing(RuntimeError):
     pass
 
@@ -215,6 +235,16 @@ def _declare(lib):
                                                     c_f32p, c_f32p]),
         "mrsim_kspace_3d_observed": (C.c_int, [P, C.POINTER(Acquisition3dInput_), C.POINTER(Acquisition_),
                                                C.POINTER(EchoTrain_), C.POINTER(GraseReadout_), C.c_int64, c_f32p]),
+        "mrsim_spiral_lines": (C.c_int, [C.POINTER(EchoTrain_), C.POINTER(SpiralReadout_), C.c_int64, C.c_int64,
+                                         C.c_int64, C.POINTER(C.c_uint8), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                         C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                         C.POINTER(C.c_int64)]),
+        "mrsim_simulate_acquisition_3d_spiral": (C.c_int, [P, C.POINTER(Acquisition3dInput_), C.POINTER(Acquisition_),
+                                                           C.POINTER(EchoTrain_), C.POINTER(SpiralReadout_),
+                                                           C.POINTER(KzOptions_), C.c_uint64, c_f32p, c_f32p]),
+        "mrsim_spiral_samples_3d": (C.c_int, [P, C.POINTER(Acquisition3dInput_), C.POINTER(Acquisition_),
+                                              C.POINTER(EchoTrain_), C.POINTER(SpiralReadout_), C.POINTER(KzOptions_),
+                                              C.c_int64, c_f32p]),
         "mrsim_spiral_recon_create": (C.c_int, [P, c_f64p, C.c_int64, C.c_int64, C.c_int32, C.c_double, C.c_double,
                                                 C.c_int64, C.c_double, C.c_int32, C.POINTER(P)]),
         "mrsim_spiral_recon_destroy": (C.c_int, [P]),

@@ -12,6 +12,7 @@
 #include "mrsim_internal.h"
 #include "series.h"
 #include "grase3d.h"
+#include "spiral3d.h"
 #include "host3d.h"
 #include "spiral.h"
 #include "spiral_host.h"
@@ -799,6 +800,60 @@ int mrsim_kspace_3d_observed(mrsim_context* ctx, const mrsim_acquisition_3d_inpu
     check_3d_input(in, acq, train, ro);
     need(out, "out");
     mrsim::grase_observed(ctx, *in, *acq, *train, *ro, (int)g, out);
+  });
+}
+
+int mrsim_spiral_lines(const mrsim_echo_train* train, const mrsim_spiral_readout* ro, int64_t nx, int64_t ny,
+                       int64_t nz, uint8_t* acquired, int64_t* echo, int64_t* kz_segment, int64_t* band_start,
+                       int64_t* e_c, int64_t* n_shots, int64_t* samples_per_interleaf) {
+  return guarded([&] {
+    need(train, "train");
+    need(ro, "readout");
+    if (nx <= 0 || ny <= 0 || nz <= 0) mrsim::fail("empty matrix");
+    mrsim::Spiral3dTable T = mrsim::spiral_lines(*train, *ro, (int)nx, (int)ny, (int)nz);
+    for (int p = 0; p < (int)nz; ++p) {
+      if (acquired) acquired[p] = T.acquired[p];
+      if (echo) echo[p] = T.echo[p];
+      if (kz_segment) kz_segment[p] = T.kz_segment[p];
+    }
+    if (band_start) *band_start = T.band_start;
+    if (e_c) *e_c = T.e_c;
+    if (n_shots) *n_shots = T.n_shots;
+    if (samples_per_interleaf) *samples_per_interleaf = (int64_t)T.traj.tau_ms.size();
+  });
+}
+
+static void check_spiral_3d(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                            const mrsim_echo_train* train, const mrsim_spiral_readout* ro) {
+  need(in, "input");
+  need(acq, "acq");
+  need(train, "train");
+  need(ro, "readout");
+  if (in->n_volumes < 0) mrsim::fail("negative volume count");
+  if (in->ncomp > 0 && !in->images) mrsim::fail("compartment image is not on the simulation grid");
+  for (int64_t c = 0; c < in->ncomp; ++c)
+    if (!in->images[c]) mrsim::fail("compartment image is not on the simulation grid");
+}
+
+int mrsim_simulate_acquisition_3d_spiral(mrsim_context* ctx, const mrsim_acquisition_3d_input* in,
+                                         const mrsim_acquisition* acq, const mrsim_echo_train* train,
+                                         const mrsim_spiral_readout* ro, const mrsim_kz_options* kz_opts,
+                                         uint64_t seed, float* mag, float* phase) {
+  return on_ctx(ctx, [&] {
+    check_spiral_3d(in, acq, train, ro);
+    need(mag, "mag");
+    need(phase, "phase");
+    mrsim::spiral3d_acquire(ctx, *in, *acq, *train, *ro, kz_opts, seed, mag, phase);
+  });
+}
+
+int mrsim_spiral_samples_3d(mrsim_context* ctx, const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                            const mrsim_echo_train* train, const mrsim_spiral_readout* ro,
+                            const mrsim_kz_options* kz_opts, int64_t g, float* out) {
+  return on_ctx(ctx, [&] {
+    check_spiral_3d(in, acq, train, ro);
+    need(out, "out");
+    mrsim::spiral3d_samples(ctx, *in, *acq, *train, *ro, kz_opts, (int)g, out);
   });
 }
 

@@ -1,7 +1,8 @@
-"""Python mirror of the reference's 3D echo-train acquisition (`kspace3d.rs`, `readout.rs:75-322`)
-over the C ABI: `EchoTrain`, `KzOrder`, `Readout3d::Grase`, `LineWeights`, `kz_order`,
-`grase_lines`, `simulate_acquisition_3d` and `kspace_3d_observed`.  The acquisition runs on the
-device (no CPU path)."""
+"""Python mirror of the reference's 3D echo-train acquisition (`kspace3d.rs`, `readout.rs:75-700`)
+over the C ABI: `EchoTrain`, `KzOrder`, `Readout3d::Grase` / `Readout3d::Spiral`, `KzSampling`,
+`KzOptions`, `LineWeights`, `kz_order`, `grase_lines`, `spiral_lines`, `simulate_acquisition_3d`
+(GRASE or stack of spirals), `kspace_3d_observed` and `spiral_samples_3d`.  The acquisition runs on
+the device (no CPU path)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -47,6 +48,76 @@ class GraseReadout:
 
     def to_c(self) -> abi.GraseReadout_:
         return abi.GraseReadout_(int(self.ky_segments), float(self.t_line_ms), int(bool(self.reverse_phase)), 0)
+
+
+@dataclasses.dataclass
+class KzSampling:
+    """`KzSampling` (readout.rs:107-160)."""
+
+    partial_fourier: float = 1.0
+    accel: int = 1
+
+    def to_c(self) -> abi.KzSampling_:
+        return abi.KzSampling_(float(self.partial_fourier), int(self.accel))
+
+
+@dataclasses.dataclass
+class SpiralReadout:
+    """`Readout3d::Spiral` (readout.rs:103-106)."""
+
+    interleaves: int
+    readout_ms: float
+    dwell_ms: float
+    radial_oversampling: float = 1.2
+    kz: KzSampling = dataclasses.field(default_factory=KzSampling)
+
+    def to_c(self) -> abi.SpiralReadout_:
+        return abi.SpiralReadout_(int(self.interleaves), float(self.readout_ms), float(self.dwell_ms),
+                                  float(self.radial_oversampling), self.kz.to_c())
+
+
+@dataclasses.dataclass
+class KzOptions:
+    """`KzOptions` (kspace3d.rs:1173-1178): calibration_images one sim volume per compartment."""
+
+    coil_rows: int = 1
+    calibration_images: Optional[Sequence[np.ndarray]] = None
+    calibration_seed: int = 0
+    pocs: bool = False
+
+    def to_c(self, keep: _Keep) -> abi.KzOptions_:
+        o = abi.KzOptions_()
+        o.coil_rows = int(self.coil_rows)
+        if self.calibration_images is not None:
+            o.calibration_images = keep.ptrs([np.ravel(a) for a in self.calibration_images])
+        o.calibration_seed = int(self.calibration_seed) & 0xFFFFFFFFFFFFFFFF
+        o.pocs = int(bool(self.pocs))
+        keep.append(o)
+        return o
+
+
+@dataclasses.dataclass
+class SpiralTable:
+    """`Spiral3dTable` (readout.rs:622-651), per partition."""
+
+    acquired: np.ndarray
+    echo: np.ndarray
+    kz_segment: np.ndarray
+    band_start: int
+    e_c: int
+    n_shots: int
+    samples_per_interleaf: int
+
+
+def spiral_lines(train: EchoTrain, ro: SpiralReadout, nx: int, ny: int, nz: int) -> SpiralTable:
+    acq = np.zeros(nz, np.uint8)
+    echo, seg = np.zeros(nz, np.int64), np.zeros(nz, np.int64)
+    vals = [C.c_int64() for _ in range(4)]
+    P = C.POINTER(C.c_int64)
+    check(lib().mrsim_spiral_lines(C.byref(train.to_c()), C.byref(ro.to_c()), nx, ny, nz,
+                                   acq.ctypes.data_as(C.POINTER(C.c_uint8)), echo.ctypes.data_as(P),
+                                   seg.ctypes.data_as(P), *[C.byref(v) for v in vals]))
+    return SpiralTable(acq.astype(bool), echo, seg, *[v.value for v in vals])
 
 
 @dataclasses.dataclass
@@ -119,20 +190,51 @@ def acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2: Sequence[T
 
 def simulate_acquisition_3d(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T2], t1: Optional[Sequence[T2]],
                             fmap, t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain,
-                            readout: GraseReadout, line_weights: Optional[LineWeights] = None,
+                            readout, line_weights: Optional[LineWeights] = None,
                             phase: Optional[PhaseModel] = None, seed: int = 0, grappa_calibration=None,
-                            ctx: Optional[Context] = None):
-    """`simulate_acquisition_3d` (kspace3d.rs:549-565), GRASE: (magnitude, phase) f32 at vox * nv + g."""
+                            kz_opts: Optional[KzOptions] = None, ctx: Optional[Context] = None):
+    """`simulate_acquisition_3d` / `_kz` (kspace3d.rs:549-589), GRASE or stack of spirals:
+    (magnitude, phase) f32 at vox * nv + g."""
     ctx = ctx or default_context()
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
                                grappa_calibration, keep)
     n = int(np.prod(acq_dims)) * n_volumes
     mag, ph = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    if isinstance(readout, SpiralReadout):
+        ko = C.byref(kz_opts.to_c(keep)) if kz_opts is not None else None
+        check(lib().mrsim_simulate_acquisition_3d_spiral(ctx.handle, C.byref(s), C.byref(acq.to_c()),
+                                                         C.byref(train.to_c()), C.byref(readout.to_c()), ko,
+                                                         int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                                         mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
+        return mag, ph
+    if kz_opts is not None:
+        raise ValueError("coil rings along z and kz undersampling are the stack of spirals', not GRASE's")
     check(lib().mrsim_simulate_acquisition_3d(ctx.handle, C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
                                               C.byref(readout.to_c()), int(seed) & 0xFFFFFFFFFFFFFFFF,
                                               mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
     return mag, ph
+
+
+def spiral_samples_3d(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,
+                      t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain, readout: SpiralReadout,
+                      line_weights: Optional[LineWeights] = None, phase: Optional[PhaseModel] = None, g: int = 0,
+                      kz_opts: Optional[KzOptions] = None, ctx: Optional[Context] = None) -> np.ndarray:
+    """`SpiralPlan::samples_all` (kspace3d.rs:1047-1060): complex64 [coil, partition, sample] before noise."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
+                               None, keep)
+    nz = acq_dims[2]
+    tab = spiral_lines(train, readout, acq_dims[0], acq_dims[1], nz)
+    nsamp = tab.samples_per_interleaf * readout.interleaves
+    nc = max(int(acq.n_coils), 1)
+    out = np.zeros(nc * nz * nsamp, np.complex64)
+    ko = C.byref(kz_opts.to_c(keep)) if kz_opts is not None else None
+    check(lib().mrsim_spiral_samples_3d(ctx.handle, C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
+                                        C.byref(readout.to_c()), ko, g,
+                                        out.view(np.float32).ctypes.data_as(abi.c_f32p)))
+    return out.reshape(nc, nz, nsamp)
 
 
 def kspace_3d_observed(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,

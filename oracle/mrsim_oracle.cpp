@@ -23,6 +23,8 @@
 #include <mutex>
 #include <thread>
 #include <functional>
+#include <map>
+#include <tuple>
 
 #include "../include/mrsim_acq.h"
 
@@ -2639,6 +2641,440 @@ std::vector<std::vector<Cx>> acquire_3d_o(const mrsim_acquisition_3d_input& in, 
   return vols;
 }
 
+
+// ============================ the stack of spirals ========================================
+// readout.rs:107-160 (KzSampling), 564-700 (trajectory, spiral_lines, spiral_kz_order),
+// kspace3d.rs:858-1569 (plan, samples, KzGrappa, POCS, spiral noise, spiral_volumes).  The
+// in-plane forward is the exact spiral sum (`spiral_kspace_exact`), which the reference's
+// time-segmented forward approximates to its certified 1e-7.
+struct SpiralTabO {
+  size_t nz, band_start, kz_segments, e_c, n_shots, ns, nsamp, interleaves;
+  double readout_ms;
+  std::vector<double> k, tau;
+  std::vector<uint8_t> acquired;
+  std::vector<size_t> echo, kz_segment;
+};
+
+SpiralTabO spiral_table_o(const mrsim_echo_train& tr, const mrsim_spiral_readout& ro, size_t n, size_t nz) {
+  SpiralTabO T;
+  size_t il = (size_t)ro.interleaves;
+  double k_max = (double)n / 2.0, n_turns = ro.radial_oversampling * (double)n / (2.0 * (double)il), t = ro.readout_ms;
+  double den = 1.0 / std::pow(k_max * ro.dwell_ms, 2) - 4.0 * PI * PI * n_turns * n_turns / (t * t);
+  double tau_c = 1.0 / (t * den);
+  size_t ns = (size_t)std::floor(t / ro.dwell_ms * (1.0 + 1e-12));
+  for (size_t j = 0; j < ns; ++j) T.tau.push_back(((double)j + 0.5) * ro.dwell_ms);
+  for (size_t s = 0; s < il; ++s)
+    for (size_t j = 0; j < ns; ++j) {
+      double tau = T.tau[j];
+      double u = tau < tau_c ? tau / std::sqrt(tau_c * t) : std::sqrt(tau / t);
+      double th = TAU * (n_turns * u + (double)s / (double)il);
+      T.k.push_back(k_max * u * std::cos(th));
+      T.k.push_back(k_max * u * std::sin(th));
+    }
+  T.ns = ns;
+  T.nsamp = ns * il;
+  T.interleaves = il;
+  T.readout_ms = t;
+  T.nz = nz;
+  size_t kept = std::min(nz, (size_t)std::round((double)nz * ro.kz.partial_fourier));
+  T.band_start = nz - kept;
+  int64_t c = (int64_t)(nz / 2), a = ro.kz.accel;
+  T.acquired.resize(nz);
+  for (size_t p = 0; p < nz; ++p) T.acquired[p] = p >= T.band_start && (((int64_t)p - c) % a + a) % a == 0;
+  std::vector<size_t> order;
+  for (size_t p : kz_order_o(nz, tr.kz_order))
+    if (T.acquired[p]) order.push_back(p);
+  size_t kzs = (size_t)tr.kz_segments;
+  if (kzs == 0 || order.size() % kzs != 0) throw Fail("partitions read do not divide into kz segments");
+  if ((size_t)tr.etl != order.size() / kzs) throw Fail("echo train length mismatch");
+  T.echo.assign(nz, 0);
+  T.kz_segment.assign(nz, 0);
+  for (size_t i = 0; i < order.size(); ++i) {
+    T.echo[order[i]] = i / kzs + 1;
+    T.kz_segment[order[i]] = i % kzs;
+  }
+  T.kz_segments = kzs;
+  T.e_c = T.echo[nz / 2];
+  T.n_shots = il * kzs;
+  return T;
+}
+
+double coil_row_sensitivity_o(size_t row, size_t rows, double z, size_t nz) {
+  if (rows <= 1) return 1.0;
+  double centre = (double)nz * ((double)row + 0.5) / (double)rows - 0.5;
+  double sigma = 0.6 * (double)nz / (double)rows;
+  return std::exp(-std::pow(z - centre, 2) / (2.0 * sigma * sigma)) + 0.15;
+}
+
+struct SpiralPlanO {
+  size_t snx, sny, nz, n, o, ncomp, rows, ring;
+  mrsim_acquisition acq;
+  SpiralTabO table;
+  std::vector<Mode3> modes;
+  const mrsim_t2* t2;
+  const mrsim_t2* ti;
+  const float* fmap;
+  mrsim_phase_model phase;
+  std::vector<Cx> zk;
+
+  // `SpiralPlan::compartments` (kspace3d.rs:942-1012) with the exact in-plane sum, element a of
+  // the rings: out[r][c][p * nsamp + j]
+  std::vector<std::vector<std::vector<Cx>>> compartments(const std::function<float(size_t, size_t)>& img, size_t a)
+      const {
+    size_t nplane = snx * sny, nsamp = table.nsamp;
+    Shot zero;
+    std::vector<std::vector<Cx>> zkq(rows, zk);
+    if (rows > 1)
+      for (size_t r = 0; r < rows; ++r)
+        for (size_t i = 0; i < nz * nz; ++i) zkq[r][i] = cscale(zk[i], coil_row_sensitivity_o(r, rows, (double)(i % nz), nz));
+    std::vector<double> taus(nsamp);
+    for (size_t j = 0; j < nsamp; ++j) taus[j] = table.tau[j % table.ns];
+    std::vector<std::vector<std::vector<Cx>>> out(rows, std::vector<std::vector<Cx>>(ncomp, std::vector<Cx>(nz * nsamp, Cx{0, 0})));
+    for (size_t c = 0; c < ncomp; ++c) {
+      std::vector<std::vector<float>> planes(nz, std::vector<float>(nplane));
+      for (size_t z = 0; z < nz; ++z)
+        for (size_t i = 0; i < nplane; ++i) planes[z][i] = img(c, z * nplane + i);
+      auto one = [&](size_t z, const double* la, bool voxel) {
+        std::vector<double> phi = phase_slice(phase, zero, snx, sny, o, z, nz);
+        const float* comps[1] = {planes[z].data()};
+        mrsim_t2 t2s[1] = {t2[c].is_map ? mrsim_t2{t2[c].map + z * nplane, 0.f, 1} : t2[c]};
+        mrsim_t2 tis[1];
+        if (ti) tis[0] = ti[c].is_map ? mrsim_t2{ti[c].map + z * nplane, 0.f, 1} : ti[c];
+        mrsim_slice_input inp;
+        std::memset(&inp, 0, sizeof inp);
+        inp.compartments = comps;
+        inp.ncomp = 1;
+        inp.t2 = t2s;
+        inp.t_inhom = ti ? tis : nullptr;
+        inp.fmap = fmap + z * nplane;
+        inp.phase0 = phi.data();
+        inp.sim[0] = (int64_t)snx;
+        inp.sim[1] = (int64_t)sny;
+        inp.acq_matrix[0] = inp.acq_matrix[1] = (int64_t)n;
+        inp.z = (int64_t)z;
+        inp.nz = (int64_t)nz;
+        mrsim_acquisition a2 = acq;
+        a2.do_relaxation = voxel ? 1 : 0;
+        return spiral_kspace_exact(inp, a2, a, ring, table.k.data(), taus.data(), nsamp, la);
+      };
+      auto zsum = [&](const std::vector<Cx>& zkr, const std::vector<std::vector<Cx>>& k2, size_t p, size_t j) {
+        Cx acc{0, 0};
+        for (size_t z = 0; z < nz; ++z) acc = cadd(acc, cmul(k2[z][j], zkr[p * nz + z]));
+        return acc;
+      };
+      const Mode3& m = modes[c];
+      if (!m.voxel) {
+        std::vector<std::vector<Cx>> k2(nz);
+        for (size_t z = 0; z < nz; ++z) k2[z] = one(z, nullptr, false);
+        for (size_t p = 0; p < nz; ++p) {
+          if (!table.acquired[p]) continue;
+          size_t e = table.echo[p];
+          for (size_t j = 0; j < nsamp; ++j) {
+            double w = acq.do_relaxation ? line_weight_o(m.ln_a[e - 1], table.tau[j % table.ns], m.t2, m.t2p) : 1.0;
+            for (size_t r = 0; r < rows; ++r) out[r][c][p * nsamp + j] = cscale(zsum(zkq[r], k2, p, j), w);
+          }
+        }
+      } else {
+        size_t emax = 0;
+        for (size_t e : table.echo) emax = std::max(emax, e);
+        for (size_t e = 1; e <= emax; ++e) {
+          std::vector<size_t> ps;
+          for (size_t p = 0; p < nz; ++p)
+            if (table.acquired[p] && table.echo[p] == e) ps.push_back(p);
+          if (ps.empty()) continue;
+          std::vector<std::vector<Cx>> k2(nz);
+          for (size_t z = 0; z < nz; ++z) k2[z] = one(z, m.maps[e - 1].data() + z * nplane, true);
+          for (size_t p : ps)
+            for (size_t j = 0; j < nsamp; ++j)
+              for (size_t r = 0; r < rows; ++r) out[r][c][p * nsamp + j] = zsum(zkq[r], k2, p, j);
+        }
+      }
+    }
+    return out;
+  }
+
+  // `samples_all` (kspace3d.rs:1014-1060): out[q] with q = r ring + a
+  std::vector<std::vector<Cx>> samples_all(const float* const* images, size_t nv, size_t g, const double* lw) const {
+    size_t nsamp = table.nsamp;
+    std::vector<std::vector<Cx>> out(ring * rows);
+    for (size_t a = 0; a < ring; ++a) {
+      auto base = compartments([&](size_t c, size_t v) { return images[c][v * nv + g]; }, a);
+      for (size_t r = 0; r < rows; ++r) {
+        std::vector<Cx> k(nz * nsamp, Cx{0, 0});
+        for (size_t p = 0; p < nz; ++p) {
+          if (!table.acquired[p]) continue;
+          for (size_t j = 0; j < nsamp; ++j) {
+            size_t shot = (j / table.ns) * table.kz_segments + table.kz_segment[p];
+            size_t i = p * nsamp + j;
+            for (size_t c = 0; c < ncomp; ++c) {
+              double w = lw ? lw[(g * table.n_shots + shot) * ncomp + c] : 1.0;
+              k[i] = cadd(k[i], cscale(base[r][c][i], w));
+            }
+          }
+        }
+        out[r * ring + a] = k;
+      }
+    }
+    return out;
+  }
+};
+
+void spiral_noise_o(std::vector<Cx>& k, const std::vector<uint8_t>& acquired, size_t nsamp, size_t g, size_t q,
+                    uint64_t seed, double sigma) {
+  const uint64_t salt3d = 0x334452454144ull;
+  for (size_t p = 0; p < acquired.size(); ++p) {
+    if (!acquired[p]) continue;
+    uint64_t pseed = (((uint64_t)g * 0x1000001ull) + (uint64_t)p) * 0x9E37ull ^ seed ^ salt3d;
+    Rng rng((pseed ^ ((uint64_t)q * 0x9E3779B9ull)) | 1ull);
+    for (size_t j = 0; j < nsamp; ++j) {
+      k[p * nsamp + j].re += rng.gauss() * sigma;
+      k[p * nsamp + j].im += rng.gauss() * sigma;
+    }
+  }
+}
+
+// `KzGrappa` (kspace3d.rs:1261-1389)
+struct KzGrappaO {
+  size_t accel, nc;
+  std::map<std::pair<size_t, unsigned>, std::vector<Cx>> weights;
+  static std::vector<int64_t> offsets(size_t accel, size_t d) {
+    int64_t r = (int64_t)accel, dd = (int64_t)d;
+    return {-dd - r, -dd, r - dd, 2 * r - dd};
+  }
+  static std::vector<std::tuple<size_t, size_t, unsigned>> targets(const SpiralTabO& T, size_t accel) {
+    std::vector<std::tuple<size_t, size_t, unsigned>> out;
+    int64_t c = (int64_t)(T.nz / 2);
+    for (size_t p = T.band_start; p < T.nz; ++p) {
+      if (T.acquired[p]) continue;
+      size_t d = (size_t)((((int64_t)p - c) % (int64_t)accel + (int64_t)accel) % (int64_t)accel);
+      unsigned pat = 0;
+      auto offs = offsets(accel, d);
+      for (size_t s = 0; s < 4; ++s) {
+        int64_t src = (int64_t)p + offs[s];
+        if (src >= 0 && (size_t)src < T.nz && T.acquired[(size_t)src]) pat |= 1u << s;
+      }
+      out.emplace_back(p, d, pat);
+    }
+    return out;
+  }
+  static KzGrappaO fit(const SpiralTabO& T, size_t accel, const std::vector<std::vector<Cx>>& cal, size_t nsamp) {
+    KzGrappaO K;
+    K.accel = accel;
+    K.nc = cal.size();
+    size_t nz = T.nz, nc = cal.size(), lo = T.band_start;
+    for (auto& [p, d, pat] : targets(T, accel)) {
+      if (pat == 0) throw Fail("partition of the partial-Fourier band has no acquired partition within reach");
+      if (K.weights.count({d, pat})) continue;
+      std::vector<int64_t> offs;
+      auto all = offsets(accel, d);
+      for (size_t s = 0; s < 4; ++s)
+        if (pat & (1u << s)) offs.push_back(all[s]);
+      size_t nfeat = offs.size() * nc;
+      std::vector<std::vector<Cx>> aha(nfeat, std::vector<Cx>(nfeat, Cx{0, 0})), ahb(nc, std::vector<Cx>(nfeat, Cx{0, 0}));
+      std::vector<Cx> f(nfeat);
+      size_t rows = 0;
+      for (size_t t = lo; t < nz; ++t) {
+        std::vector<size_t> srcs;
+        for (int64_t o2 : offs) {
+          int64_t pp = (int64_t)t + o2;
+          if (pp >= (int64_t)lo && pp < (int64_t)nz) srcs.push_back((size_t)pp);
+        }
+        if (srcs.size() != offs.size()) continue;
+        for (size_t j = 0; j < nsamp; ++j) {
+          for (size_t s = 0; s < srcs.size(); ++s)
+            for (size_t q = 0; q < nc; ++q) f[s * nc + q] = cal[q][srcs[s] * nsamp + j];
+          for (size_t i = 0; i < nfeat; ++i) {
+            Cx fic{f[i].re, -f[i].im};
+            for (size_t jj = 0; jj < nfeat; ++jj) aha[i][jj] = cadd(aha[i][jj], cmul(fic, f[jj]));
+            for (size_t q = 0; q < nc; ++q) ahb[q][i] = cadd(ahb[q][i], cmul(fic, cal[q][t * nsamp + j]));
+          }
+          ++rows;
+        }
+      }
+      if (rows == 0) throw Fail("the calibration band holds no partition with the kernel's sources");
+      double trace = 0.0;
+      for (size_t i = 0; i < nfeat; ++i) trace += aha[i][i].re;
+      if (!(trace > 0.0)) throw Fail("the kz calibration acquisition is empty");
+      double sc = (double)nfeat / trace;
+      for (auto& row : aha)
+        for (Cx& a : row) a = cscale(a, sc);
+      for (auto& b : ahb)
+        for (Cx& v : b) v = cscale(v, sc);
+      for (size_t i = 0; i < nfeat; ++i) aha[i][i].re += 1e-8;
+      std::vector<Cx> w;
+      for (auto& b : ahb)
+        for (const Cx& x : solve_hermitian(aha, b)) w.push_back(x);
+      K.weights[{d, pat}] = w;
+    }
+    return K;
+  }
+  void fill(const SpiralTabO& T, std::vector<std::vector<Cx>>& k, size_t nsamp) const {
+    for (auto& [p, d, pat] : targets(T, accel)) {
+      auto it = weights.find({d, pat});
+      if (it == weights.end()) continue;
+      const std::vector<Cx>& w = it->second;
+      std::vector<size_t> srcs;
+      auto all = offsets(accel, d);
+      for (size_t s = 0; s < 4; ++s)
+        if (pat & (1u << s)) srcs.push_back((size_t)((int64_t)p + all[s]));
+      size_t nfeat = srcs.size() * nc;
+      for (size_t j = 0; j < nsamp; ++j)
+        for (size_t qt = 0; qt < nc; ++qt) {
+          Cx v{0, 0};
+          for (size_t s = 0; s < srcs.size(); ++s)
+            for (size_t qs = 0; qs < nc; ++qs) v = cadd(v, cmul(w[qt * nfeat + s * nc + qs], k[qs][srcs[s] * nsamp + j]));
+          k[qt][p * nsamp + j] = v;
+        }
+    }
+  }
+};
+
+// `pocs_along_z` (kspace3d.rs:1201-1259)
+std::vector<std::vector<Cx>> pocs_along_z_o(const std::vector<std::vector<Cx>>& h, size_t lo, const std::vector<Cx>& zk,
+                                            size_t nz) {
+  size_t nplane = h[0].size(), c = nz / 2;
+  size_t m = std::min(c - lo, nz - 1 - c);
+  auto hann = [&](size_t p) {
+    double d = std::fabs((double)p - (double)c);
+    return d > (double)m ? 0.0 : 0.5 * (1.0 + std::cos(PI * d / ((double)m + 1.0)));
+  };
+  auto inv = [&](const std::vector<Cx>& k, size_t z) {
+    Cx acc{0, 0};
+    for (size_t p = 0; p < nz; ++p) acc = cadd(acc, cmul(k[p], Cx{zk[p * nz + z].re, -zk[p * nz + z].im}));
+    return cscale(acc, 1.0 / (double)nz);
+  };
+  auto fwd = [&](const std::vector<Cx>& x, size_t p) {
+    Cx acc{0, 0};
+    for (size_t z = 0; z < nz; ++z) acc = cadd(acc, cmul(x[z], zk[p * nz + z]));
+    return acc;
+  };
+  std::vector<std::vector<Cx>> out(nz, std::vector<Cx>(nplane));
+  std::vector<Cx> k(nz), x(nz), low(nz), unit(nz);
+  for (size_t i = 0; i < nplane; ++i) {
+    for (size_t p = 0; p < nz; ++p) {
+      k[p] = p >= lo ? h[p][i] : Cx{0, 0};
+      low[p] = cscale(k[p], hann(p));
+    }
+    for (size_t z = 0; z < nz; ++z) {
+      Cx v = inv(low, z);
+      double a = cabs_(v);
+      unit[z] = a > 0.0 ? cscale(v, 1.0 / a) : Cx{1.0, 0.0};
+    }
+    for (int it = 0; it < 10; ++it) {
+      for (size_t z = 0; z < nz; ++z) x[z] = cscale(unit[z], cabs_(inv(k, z)));
+      for (size_t p = 0; p < lo; ++p) k[p] = fwd(x, p);
+    }
+    for (size_t z = 0; z < nz; ++z) out[z][i] = inv(k, z);
+  }
+  return out;
+}
+
+// `spiral_volumes` (kspace3d.rs:1472-1569)
+std::vector<std::vector<Cx>> spiral_volumes_o(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
+                                              const mrsim_echo_train& tr, const mrsim_spiral_readout& ro,
+                                              const mrsim_kz_options* opts, uint64_t seed, int threads) {
+  SpiralPlanO pl;
+  pl.snx = in.sim_dims[0];
+  pl.sny = in.sim_dims[1];
+  pl.nz = in.sim_dims[2];
+  pl.n = in.acq_dims[0];
+  pl.o = pl.snx / pl.n;
+  pl.ncomp = in.ncomp;
+  size_t ncoils = std::max<int64_t>(acq.n_coils, 1);
+  pl.rows = opts ? (size_t)opts->coil_rows : 1;
+  pl.ring = ncoils / pl.rows;
+  pl.acq = acq;
+  pl.table = spiral_table_o(tr, ro, pl.n, pl.nz);
+  pl.modes = resolve_modes_o(in.t2, in.t1, in.t_inhom, pl.ncomp, acq, tr, pl.snx * pl.sny * pl.nz);
+  pl.t2 = in.t2;
+  pl.ti = in.t_inhom;
+  pl.fmap = in.fmap;
+  if (in.phase) pl.phase = *in.phase;
+  else std::memset(&pl.phase, 0, sizeof pl.phase);
+  double zs = (double)(pl.nz / 2);
+  pl.zk.resize(pl.nz * pl.nz);
+  for (size_t p = 0; p < pl.nz; ++p)
+    for (size_t z = 0; z < pl.nz; ++z) pl.zk[p * pl.nz + z] = ccis(TAU * ((double)p - zs) * ((double)z - zs) / (double)pl.nz);
+  size_t nz = pl.nz, n = pl.n, nsamp = pl.table.nsamp, nv = in.n_volumes;
+  double sigma = std::sqrt(acq.noise_variance / (double)(n * n));
+  KzGrappaO kzk;
+  bool accel = ro.kz.accel > 1;
+  if (accel) {
+    mrsim_spiral_readout cro = ro;
+    cro.kz.accel = 1;
+    mrsim_echo_train ctr = tr;
+    size_t n_cal = pl.nz - pl.table.band_start;  // the band without the acceleration
+    ctr.etl = (int64_t)(n_cal / (size_t)tr.kz_segments);
+    SpiralPlanO cal = pl;
+    cal.table = spiral_table_o(ctr, cro, pl.n, pl.nz);
+    cal.modes = resolve_modes_o(in.t2, in.t1, in.t_inhom, pl.ncomp, acq, ctr, pl.snx * pl.sny * pl.nz);
+    auto samples = cal.samples_all(opts->calibration_images, 1, 0, nullptr);
+    if (sigma > 0.0)
+      for (size_t q = 0; q < samples.size(); ++q)
+        spiral_noise_o(samples[q], cal.table.acquired, nsamp, 0, q, opts->calibration_seed ^ 0x4B5A43414C00ull, sigma);
+    kzk = KzGrappaO::fit(pl.table, (size_t)ro.kz.accel, samples, nsamp);
+  }
+  std::vector<std::vector<double>> zsens(ncoils, std::vector<double>(nz));
+  for (size_t q = 0; q < ncoils; ++q)
+    for (size_t z = 0; z < nz; ++z) zsens[q][z] = coil_row_sensitivity_o(q / pl.ring, pl.rows, (double)z, nz);
+  bool pocs = ro.kz.partial_fourier < 1.0 && pl.table.band_start > 0 && opts && opts->pocs;
+  mrsim_acquisition wa = acq;
+  SpiralReconO rec(pl.table.k.data(), nsamp, n, wa, 80, 100.0, true);
+  std::vector<std::vector<Cx>> vols(nv);
+  parallel_for(nv, threads, [&](size_t g) {
+    auto coil_k = pl.samples_all(in.images, nv, g, in.line_weights);
+    if (acq.noise_variance > 0.0)
+      for (size_t q = 0; q < coil_k.size(); ++q) spiral_noise_o(coil_k[q], pl.table.acquired, nsamp, g, q, seed, sigma);
+    if (accel) kzk.fill(pl.table, coil_k, nsamp);
+    std::vector<Cx> out(n * n * nz);
+    if (pocs) {
+      size_t lo = pl.table.band_start;
+      std::vector<Cx> wsum(n * n * nz, Cx{0, 0});
+      std::vector<double> ssum(n * n * nz, 0.0);
+      for (size_t q = 0; q < coil_k.size(); ++q) {
+        std::vector<std::vector<Cx>> h(nz);
+        for (size_t p = 0; p < nz; ++p)
+          h[p] = p >= lo ? rec.image(std::vector<Cx>(coil_k[q].begin() + p * nsamp, coil_k[q].begin() + (p + 1) * nsamp))
+                         : std::vector<Cx>(n * n, Cx{0, 0});
+        auto img = pocs_along_z_o(h, lo, pl.zk, nz);
+        for (size_t z = 0; z < nz; ++z)
+          for (size_t i = 0; i < n * n; ++i) {
+            double s = coil_sensitivity(q % pl.ring, pl.ring, (double)(i % n), (double)(i / n), n, n) * zsens[q][z];
+            wsum[i + n * n * z] = cadd(wsum[i + n * n * z], cscale(img[z][i], s));
+            ssum[i + n * n * z] += s * s;
+          }
+      }
+      for (size_t i = 0; i < out.size(); ++i) {
+        double s = std::max(ssum[i], 1e-12);
+        out[i] = {wsum[i].re / s, wsum[i].im / s};
+      }
+    } else {
+      std::vector<std::vector<std::vector<Cx>>> parts(coil_k.size(), std::vector<std::vector<Cx>>(nz, std::vector<Cx>(nsamp, Cx{0, 0})));
+      for (size_t q = 0; q < coil_k.size(); ++q)
+        for (size_t z = 0; z < nz; ++z) {
+          for (size_t p = 0; p < nz; ++p) {
+            Cx kc = pl.zk[p * nz + z];
+            Cx conj{kc.re, -kc.im};
+            for (size_t j = 0; j < nsamp; ++j) parts[q][z][j] = cadd(parts[q][z][j], cmul(coil_k[q][p * nsamp + j], conj));
+          }
+          for (Cx& v : parts[q][z]) v = cscale(v, 1.0 / (double)nz);
+        }
+      for (size_t z = 0; z < nz; ++z) {
+        std::vector<Cx> coils;
+        std::vector<double> zz;
+        for (size_t q = 0; q < coil_k.size(); ++q) {
+          coils.insert(coils.end(), parts[q][z].begin(), parts[q][z].end());
+          zz.push_back(zsens[q][z]);
+        }
+        auto img = rec.rings(coils.data(), coil_k.size(), pl.ring, zz.data());
+        for (size_t i = 0; i < n * n; ++i) out[i + n * n * z] = img[i];
+      }
+    }
+    vols[g] = out;
+  });
+  return vols;
+}
+
 thread_local std::string g_err;
 std::vector<GoldenCase>* g_golden = nullptr;
 
@@ -2971,6 +3407,75 @@ int oracle_simulate_acquisition_3d(const mrsim_acquisition_3d_input* in, const m
                                    int32_t threads, double* vols_out, float* mag, float* ph) {
   return guard([&] {
     auto vols = acquire_3d_o(*in, *acq, *tr, *ro, seed, threads);
+    size_t nv = in->n_volumes;
+    for (size_t g = 0; g < vols.size(); ++g) {
+      if (vols_out) put_cx(vols[g], vols_out + 2 * vols[g].size() * g);
+      for (size_t vox = 0; vox < vols[g].size(); ++vox) {
+        float re = (float)vols[g][vox].re, im = (float)vols[g][vox].im;
+        if (mag) mag[vox * nv + g] = std::sqrt(re * re + im * im);
+        if (ph) ph[vox * nv + g] = std::atan2(im, re);
+      }
+    }
+  });
+}
+
+int oracle_spiral_lines(const mrsim_echo_train* tr, const mrsim_spiral_readout* ro, int64_t n, int64_t nz,
+                        uint8_t* acquired, int64_t* echo, int64_t* kz_segment, int64_t* band_start, int64_t* e_c,
+                        int64_t* n_shots, double* k, double* tau) {
+  return guard([&] {
+    SpiralTabO T = spiral_table_o(*tr, *ro, (size_t)n, (size_t)nz);
+    for (size_t p = 0; p < T.nz; ++p) {
+      acquired[p] = T.acquired[p];
+      echo[p] = (int64_t)T.echo[p];
+      kz_segment[p] = (int64_t)T.kz_segment[p];
+    }
+    *band_start = (int64_t)T.band_start;
+    *e_c = (int64_t)T.e_c;
+    *n_shots = (int64_t)T.n_shots;
+    if (k) std::memcpy(k, T.k.data(), T.k.size() * 8);
+    if (tau) std::memcpy(tau, T.tau.data(), T.tau.size() * 8);
+  });
+}
+
+int oracle_spiral_samples_3d(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                             const mrsim_echo_train* tr, const mrsim_spiral_readout* ro, const mrsim_kz_options* opts,
+                             int64_t g, double* out) {
+  return guard([&] {
+    SpiralPlanO pl;
+    pl.snx = in->sim_dims[0];
+    pl.sny = in->sim_dims[1];
+    pl.nz = in->sim_dims[2];
+    pl.n = in->acq_dims[0];
+    pl.o = pl.snx / pl.n;
+    pl.ncomp = in->ncomp;
+    size_t ncoils = std::max<int64_t>(acq->n_coils, 1);
+    pl.rows = opts ? (size_t)opts->coil_rows : 1;
+    pl.ring = ncoils / pl.rows;
+    pl.acq = *acq;
+    pl.table = spiral_table_o(*tr, *ro, pl.n, pl.nz);
+    pl.modes = resolve_modes_o(in->t2, in->t1, in->t_inhom, pl.ncomp, *acq, *tr, pl.snx * pl.sny * pl.nz);
+    pl.t2 = in->t2;
+    pl.ti = in->t_inhom;
+    pl.fmap = in->fmap;
+    if (in->phase) pl.phase = *in->phase;
+    else std::memset(&pl.phase, 0, sizeof pl.phase);
+    double zs = (double)(pl.nz / 2);
+    pl.zk.resize(pl.nz * pl.nz);
+    for (size_t p = 0; p < pl.nz; ++p)
+      for (size_t z = 0; z < pl.nz; ++z)
+        pl.zk[p * pl.nz + z] = ccis(TAU * ((double)p - zs) * ((double)z - zs) / (double)pl.nz);
+    auto s = pl.samples_all(in->images, in->n_volumes, (size_t)g, in->line_weights);
+    size_t per = pl.nz * pl.table.nsamp;
+    for (size_t q = 0; q < s.size(); ++q) put_cx(s[q], out + 2 * per * q);
+  });
+}
+
+int oracle_simulate_acquisition_3d_spiral(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                                          const mrsim_echo_train* tr, const mrsim_spiral_readout* ro,
+                                          const mrsim_kz_options* opts, uint64_t seed, int32_t threads,
+                                          double* vols_out, float* mag, float* ph) {
+  return guard([&] {
+    auto vols = spiral_volumes_o(*in, *acq, *tr, *ro, opts, seed, threads);
     size_t nv = in->n_volumes;
     for (size_t g = 0; g < vols.size(); ++g) {
       if (vols_out) put_cx(vols[g], vols_out + 2 * vols[g].size() * g);

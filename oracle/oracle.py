@@ -89,6 +89,14 @@ def lib():
                                                 C.c_int64, abi.c_f64p]
         L.oracle_simulate_acquisition_3d.argtypes = [A3, P(abi.Acquisition_), P(abi.EchoTrain_), P(abi.GraseReadout_),
                                                      C.c_uint64, C.c_int32, abi.c_f64p, abi.c_f32p, abi.c_f32p]
+        KO = P(abi.KzOptions_)
+        L.oracle_spiral_lines.argtypes = [P(abi.EchoTrain_), P(abi.SpiralReadout_), C.c_int64, C.c_int64,
+                                          P(C.c_uint8), i64p, i64p, i64p, i64p, i64p, abi.c_f64p, abi.c_f64p]
+        L.oracle_spiral_samples_3d.argtypes = [A3, P(abi.Acquisition_), P(abi.EchoTrain_), P(abi.SpiralReadout_), KO,
+                                               C.c_int64, abi.c_f64p]
+        L.oracle_simulate_acquisition_3d_spiral.argtypes = [A3, P(abi.Acquisition_), P(abi.EchoTrain_),
+                                                            P(abi.SpiralReadout_), KO, C.c_uint64, C.c_int32,
+                                                            abi.c_f64p, abi.c_f32p, abi.c_f32p]
         _lib = L
     return _lib
 
@@ -467,4 +475,63 @@ def simulate_acquisition_3d(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap,
                                                 threads or (os.cpu_count() or 1),
                                                 vols.view(np.float64).ctypes.data_as(abi.c_f64p),
                                                 mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
+    return vols.reshape(n_volumes, nvox), mag, ph
+
+
+# ---- the stack of spirals ------------------------------------------------------------------------------
+def spiral_lines(train, ro, n: int, nz: int) -> dict:
+    acq = np.zeros(nz, np.uint8)
+    echo, seg = np.zeros(nz, np.int64), np.zeros(nz, np.int64)
+    vals = [C.c_int64() for _ in range(3)]
+    from mrsim_acq_b200.spiral import spiral_trajectory
+    tr = spiral_trajectory(n, n, ro.interleaves, ro.readout_ms, ro.dwell_ms, ro.radial_oversampling)
+    k = np.zeros(tr.k.size)
+    tau = np.zeros(len(tr.tau_ms))
+    P = C.POINTER(C.c_int64)
+    _check(lib().oracle_spiral_lines(C.byref(train.to_c()), C.byref(ro.to_c()), n, nz,
+                                     acq.ctypes.data_as(C.POINTER(C.c_uint8)), echo.ctypes.data_as(P),
+                                     seg.ctypes.data_as(P), *[C.byref(v) for v in vals], k.ctypes.data_as(abi.c_f64p),
+                                     tau.ctypes.data_as(abi.c_f64p)))
+    return {"acquired": acq.astype(bool), "echo": echo, "kz_segment": seg, "band_start": vals[0].value,
+            "e_c": vals[1].value, "n_shots": vals[2].value, "k": k.reshape(-1, 2), "tau_ms": tau}
+
+
+def _kz_c(kz_opts, keep):
+    return C.byref(kz_opts.to_c(keep)) if kz_opts is not None else None
+
+
+def spiral_samples_3d(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition, train, ro,
+                      line_weights=None, phase=None, g: int = 0, kz_opts=None) -> np.ndarray:
+    """`SpiralPlan::samples_all` with the exact in-plane sum, FP64: complex128 [coil, partition, sample]."""
+    from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
+                               None, keep)
+    nz = acq_dims[2]
+    tab = spiral_lines(train, ro, acq_dims[0], nz)
+    nsamp = len(tab["k"])
+    nc = max(acq.n_coils, 1)
+    out = np.zeros(nc * nz * nsamp, np.complex128)
+    _check(lib().oracle_spiral_samples_3d(C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()), C.byref(ro.to_c()),
+                                          _kz_c(kz_opts, keep), g, out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+    return out.reshape(nc, nz, nsamp)
+
+
+def simulate_acquisition_3d_spiral(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition,
+                                   train, ro, line_weights=None, phase=None, seed: int = 0, kz_opts=None,
+                                   threads: int = 0):
+    """`spiral_volumes` (kspace3d.rs:1472-1569), FP64: (complex volumes [g, vox], mag, phase)."""
+    import os
+    from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
+                               None, keep)
+    nvox = int(np.prod(acq_dims))
+    vols = np.zeros(n_volumes * nvox, np.complex128)
+    mag, ph = np.zeros(nvox * n_volumes, np.float32), np.zeros(nvox * n_volumes, np.float32)
+    _check(lib().oracle_simulate_acquisition_3d_spiral(C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
+                                                       C.byref(ro.to_c()), _kz_c(kz_opts, keep),
+                                                       int(seed) & 0xFFFFFFFFFFFFFFFF, threads or (os.cpu_count() or 1),
+                                                       vols.view(np.float64).ctypes.data_as(abi.c_f64p),
+                                                       mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
     return vols.reshape(n_volumes, nvox), mag, ph
