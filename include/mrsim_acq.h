@@ -383,6 +383,67 @@ int mrsim_kspace_3d_observed(mrsim_context* ctx, const mrsim_acquisition_3d_inpu
                              const mrsim_acquisition* acq, const mrsim_echo_train* train,
                              const mrsim_grase_readout* ro, int64_t g, float* out);
 
+/* ---- the 3D gradient-echo stack-of-EPI train (kspace3d.rs:590-856, readout.rs:356-462) ----- */
+/* `ExcitationTrain` (readout.rs:362-369); echo_times_ms strictly increasing, n_echoes >= 1. */
+typedef struct mrsim_excitation_train {
+  int64_t kz_segments;
+  int32_t kz_order;         /* MRSIM_KZ_* */
+  int32_t reserved;
+  double exc_spacing_ms;
+  const double* echo_times_ms;
+  int64_t n_echoes;
+  double excitation_time_ms;
+} mrsim_excitation_train;
+
+/* `Ge3dReadout` (readout.rs:374-379). */
+typedef struct mrsim_ge3d_readout {
+  int64_t ky_segments;
+  double t_line_ms;
+  int32_t reverse_phase;
+  int32_t reserved;
+} mrsim_ge3d_readout;
+
+/* `GeVolume` (kspace3d.rs:592-603): per compartment one sim volume (NULL = a compartment this
+ * volume does not use; its weights must be 0) and the excitation weights
+ * w[(p * ky_segments + sy) * ncomp + c].  Per-shot images are not taken. */
+typedef struct mrsim_ge_volume {
+  const float* const* images;
+  const double* weights;
+} mrsim_ge_volume;
+
+/* The `volume` callback: fill *out for volume g (pointers valid until the next call or the end
+ * of the acquisition call); return 0, or non-zero to abort with MRSIM_ERR_INVALID.  Called on the
+ * calling thread, once per volume (and once more for volume 0 when a GRAPPA reference is needed
+ * and none is given). */
+typedef int (*mrsim_ge_volume_fn)(int64_t g, void* user, mrsim_ge_volume* out);
+
+typedef struct mrsim_acquisition_ge_input {
+  int64_t sim_dims[3];
+  int64_t acq_dims[3];
+  int64_t n_volumes;
+  int64_t ncomp;
+  const mrsim_t2* t2;
+  const float* fmap;
+  const mrsim_t2* t_inhom;            /* ncomp or NULL */
+  const mrsim_phase_model* phase;
+  mrsim_ge_volume_fn volume;
+  void* user;
+  const mrsim_ge_volume* reference;   /* the GRAPPA reference scan's volume, or NULL */
+} mrsim_acquisition_ge_input;
+
+/* `ge3d_lines` (readout.rs:418-450): per line p*ny + ky its shot, excitation, t (ms) and
+ * polarity (any output may be NULL); n_shots, n_exc and e_c (0-based excitation). */
+int mrsim_ge3d_lines(const mrsim_excitation_train* train, const mrsim_ge3d_readout* ro, int64_t ny,
+                     int64_t nz, int64_t* shot, int64_t* excitation, double* t_ms,
+                     int8_t* polarity, int64_t* n_shots, int64_t* n_exc, int64_t* e_c);
+/* `simulate_acquisition_3d_ge` (kspace3d.rs:837-856) on the device: per echo e, mag[e] and
+ * phase[e] (f32, vox*nv + g). */
+int mrsim_simulate_acquisition_3d_ge(mrsim_context* ctx, const mrsim_acquisition_ge_input* in,
+                                     const mrsim_acquisition* acq,
+                                     const mrsim_excitation_train* train,
+                                     const mrsim_ge3d_readout* ro, uint64_t seed,
+                                     float* const* mag, float* const* phase);
+
 /* ---- the stack of spirals (kspace3d.rs:858-1569, readout.rs:107-160, 622-700) -------------- */
 /* `KzSampling` (readout.rs:107-160). */
 typedef struct mrsim_kz_sampling {

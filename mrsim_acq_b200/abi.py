@@ -134,6 +134,40 @@ class Acquisition3dInput_(C.Structure):
     ]
 
 
+class ExcitationTrain_(C.Structure):
+    """`mrsim_excitation_train` — `ExcitationTrain` (readout.rs:362-369)."""
+
+    _fields_ = [("kz_segments", C.c_int64), ("kz_order", C.c_int32), ("reserved", C.c_int32),
+                ("exc_spacing_ms", C.c_double), ("echo_times_ms", c_f64p), ("n_echoes", C.c_int64),
+                ("excitation_time_ms", C.c_double)]
+
+
+class Ge3dReadout_(C.Structure):
+    """`mrsim_ge3d_readout` — `Ge3dReadout` (readout.rs:374-379)."""
+
+    _fields_ = [("ky_segments", C.c_int64), ("t_line_ms", C.c_double), ("reverse_phase", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class GeVolume_(C.Structure):
+    """`mrsim_ge_volume` — `GeVolume` (kspace3d.rs:592-603) without per-shot images."""
+
+    _fields_ = [("images", C.POINTER(c_f32p)), ("weights", c_f64p)]
+
+
+GE_VOLUME_FN = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_void_p, C.POINTER(GeVolume_))
+
+
+class AcquisitionGeInput_(C.Structure):
+    """`mrsim_acquisition_ge_input` — the inputs of `simulate_acquisition_3d_ge` (kspace3d.rs:837)."""
+
+    _fields_ = [
+        ("sim_dims", C.c_int64 * 3), ("acq_dims", C.c_int64 * 3), ("n_volumes", C.c_int64), ("ncomp", C.c_int64),
+        ("t2", C.POINTER(T2_)), ("fmap", c_f32p), ("t_inhom", C.POINTER(T2_)), ("phase", C.POINTER(PhaseModel_)),
+        ("volume", GE_VOLUME_FN), ("user", C.c_void_p), ("reference", C.POINTER(GeVolume_)),
+    ]
+
+
 class KzSampling_(C.Structure):
     """`mrsim_kz_sampling` — `KzSampling` (readout.rs:107-160)."""
 
@@ -235,6 +269,12 @@ def _declare(lib):
                                                     c_f32p, c_f32p]),
         "mrsim_kspace_3d_observed": (C.c_int, [P, C.POINTER(Acquisition3dInput_), C.POINTER(Acquisition_),
                                                C.POINTER(EchoTrain_), C.POINTER(GraseReadout_), C.c_int64, c_f32p]),
+        "mrsim_ge3d_lines": (C.c_int, [C.POINTER(ExcitationTrain_), C.POINTER(Ge3dReadout_), C.c_int64, C.c_int64,
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64), c_f64p, C.POINTER(C.c_int8),
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "mrsim_simulate_acquisition_3d_ge": (C.c_int, [P, C.POINTER(AcquisitionGeInput_), C.POINTER(Acquisition_),
+                                                       C.POINTER(ExcitationTrain_), C.POINTER(Ge3dReadout_),
+                                                       C.c_uint64, C.POINTER(c_f32p), C.POINTER(c_f32p)]),
         "mrsim_spiral_lines": (C.c_int, [C.POINTER(EchoTrain_), C.POINTER(SpiralReadout_), C.c_int64, C.c_int64,
                                          C.c_int64, C.POINTER(C.c_uint8), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                          C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),

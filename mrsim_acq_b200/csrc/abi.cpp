@@ -857,5 +857,39 @@ int mrsim_spiral_samples_3d(mrsim_context* ctx, const mrsim_acquisition_3d_input
   });
 }
 
+int mrsim_ge3d_lines(const mrsim_excitation_train* train, const mrsim_ge3d_readout* ro, int64_t ny, int64_t nz,
+                     int64_t* shot, int64_t* excitation, double* t_ms, int8_t* polarity, int64_t* n_shots,
+                     int64_t* n_exc, int64_t* e_c) {
+  return guarded([&] {
+    need(train, "train");
+    need(ro, "readout");
+    if (ny <= 0 || nz <= 0) mrsim::fail("ny and nz must be positive");
+    mrsim::Ge3dTable T = mrsim::ge3d_lines(*train, *ro, (int)ny, (int)nz);
+    for (size_t i = 0; i < T.lines.size(); ++i) {
+      if (shot) shot[i] = T.lines[i].shot;
+      if (excitation) excitation[i] = T.lines[i].excitation;
+      if (t_ms) t_ms[i] = T.lines[i].t_ms;
+      if (polarity) polarity[i] = T.lines[i].polarity;
+    }
+    if (n_shots) *n_shots = T.n_shots;
+    if (n_exc) *n_exc = T.n_exc;
+    if (e_c) *e_c = T.e_c;
+  });
+}
+
+int mrsim_simulate_acquisition_3d_ge(mrsim_context* ctx, const mrsim_acquisition_ge_input* in,
+                                     const mrsim_acquisition* acq, const mrsim_excitation_train* train,
+                                     const mrsim_ge3d_readout* ro, uint64_t seed, float* const* mag,
+                                     float* const* phase) {
+  return on_ctx(ctx, [&] {
+    need(in, "input");
+    need(acq, "acq");
+    need(train, "train");
+    need(ro, "readout");
+    if (in->n_volumes < 0) mrsim::fail("negative volume count");
+    mrsim::ge_acquire(ctx, *in, *acq, *train, *ro, seed, mag, phase);
+  });
+}
+
 }  // extern "C"
 #pragma GCC visibility pop

@@ -130,6 +130,9 @@ struct GrasePlan {
   std::vector<Src> srcs;
   std::vector<int> src_of;  // [c][p]
   std::vector<float> wc;    // [c][p][ky]
+  std::vector<int> shot;    // [p][ky]: the index of the line weights (GRASE's shot, GE's excitation)
+  int n_shots = 0;
+  std::vector<char> used;   // per compartment
 };
 
 static GrasePlan make_plan(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
@@ -168,6 +171,11 @@ static GrasePlan make_plan(const mrsim_acquisition_3d_input& in, const mrsim_acq
   P.within.tread_ms = P.table.block.t_ms;
   P.within.polarity = P.table.block.polarity;
   P.etl = (int)train.etl;
+  P.shot.resize((size_t)P.nz * P.ny);
+  for (int p = 0; p < P.nz; ++p)
+    for (int ky = 0; ky < P.ny; ++ky) P.shot[(size_t)p * P.ny + ky] = P.table.line(p, ky).shot;
+  P.n_shots = P.table.n_shots;
+  P.used.assign(P.ncomp, 1);
   P.modes = resolve_modes(in.t2, in.t1, in.t_inhom, P.ncomp, acq, train, P.nvox);
   P.mask = sampling_mask(P.nx, P.ny, acq);
   const double zs = (double)(P.nz / 2);
@@ -255,7 +263,7 @@ static GraseInputs upload_inputs(DevArena& A, const GrasePlan& P, const mrsim_ac
 
 // The acquired 3D k-space (before spikes and noise) of volumes g0..g1 into k3 [gl][q][p][ky][kx].
 static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_acquisition& acq,
-                         const mrsim_phase_model* phase, const float* d_lw, int n_shots, int g0, int g1,
+                         const mrsim_phase_model* phase, const float* d_lw, int g0, int g1,
                          const std::vector<uint8_t>& mask, float2* k3, cudaStream_t st) {
   const int ngl = g1 - g0, nsrc = (int)P.srcs.size(), nz = P.nz, nc = P.nc;
   const size_t per = (size_t)P.nx * P.ny;
@@ -301,6 +309,7 @@ static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_a
         ui.z = z;
         ui.nz_full = nz;
         const CompMode& m = P.modes[S.c];
+        if (!P.used[S.c]) continue;
         if (!m.voxel) {
           ui.lines = dLc;
           ui.n_lines = n_lines;
@@ -308,7 +317,7 @@ static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_a
         } else {
           ui.t2map = I.t2 + (size_t)S.c * P.nvox + (size_t)z * P.plane;
           ui.timap = I.ti + (size_t)S.c * P.nvox + (size_t)z * P.plane;
-          ui.log_amp = I.lna + ((size_t)S.c * P.etl + (S.e - 1)) * P.nvox + (size_t)z * P.plane;
+          ui.log_amp = S.e > 0 ? I.lna + ((size_t)S.c * P.etl + (S.e - 1)) * P.nvox + (size_t)z * P.plane : nullptr;
           ui.lines = dLv;
           ui.n_lines = n_lines;
           add_unit(Bv, ui, P.snx, P.sny, P.nx, P.ny, 1, nc, true, one, one, geo, rel);
@@ -321,9 +330,7 @@ static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_a
   // the z-DFT, weights, compartment sum and sampling
   std::vector<unsigned char> rows(P.ny);
   for (int ky = 0; ky < P.ny; ++ky) rows[ky] = mask[(size_t)ky * P.nx] ? 1 : 0;
-  std::vector<int> shot((size_t)nz * P.ny);
-  for (int p = 0; p < nz; ++p)
-    for (int ky = 0; ky < P.ny; ++ky) shot[(size_t)p * P.ny + ky] = P.table.line(p, ky).shot;
+  const std::vector<int>& shot = P.shot;
   ZdftArgs a;
   a.K = K;
   a.out = k3;
@@ -339,7 +346,7 @@ static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_a
   a.nc = nc;
   a.ncomp = P.ncomp;
   a.nsrc = nsrc;
-  a.n_shots = n_shots;
+  a.n_shots = P.n_shots;
   a.g0 = g0;
   grase_zdft_kernel<<<grid3(per, nz, ngl * nc), 256, 0, st>>>(a);
   MRSIM_CUDA(cudaGetLastError());
@@ -390,7 +397,7 @@ void grase_observed(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, co
   }
   const size_t per = (size_t)P.nx * P.ny;
   float2* k3 = (float2*)A.alloc((size_t)P.nc * P.nz * per * sizeof(float2));
-  grase_kspace(P, I, acq, in.phase, d_lw, P.table.n_shots, g, g + 1, P.mask, k3, st);
+  grase_kspace(P, I, acq, in.phase, d_lw, g, g + 1, P.mask, k3, st);
   MRSIM_CUDA(cudaMemcpyAsync(out, k3, (size_t)P.nc * P.nz * per * sizeof(float2), cudaMemcpyDeviceToHost, st));
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
@@ -432,7 +439,7 @@ void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, con
     }
     GraseInputs Ic = upload_inputs(C, Pc, in, cal_images, cal_nv, acq_cal, st);
     float2* k3 = (float2*)C.alloc((size_t)nc * nz * per * sizeof(float2));
-    grase_kspace(Pc, Ic, acq_cal, in.phase, nullptr, Pc.table.n_shots, 0, 1, Pc.mask, k3, st);
+    grase_kspace(Pc, Ic, acq_cal, in.phase, nullptr, 0, 1, Pc.mask, k3, st);
     grase_noise(C, Pc, k3, 0, 1, cal_seed ^ kSeedSaltGrappaCal, Pc.mask, acq_cal, st);
     float2* sl = (float2*)C.alloc((size_t)nz * nc * per * sizeof(float2));
     grase_izdft_kernel<<<grid3(per, nz, nc), 256, 0, st>>>(k3, d_zk, nx, ny, nz, nc, sl);
@@ -454,7 +461,7 @@ void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, con
     const int g1 = std::min(nv, g0 + vchunk), ngl = g1 - g0;
     DevArena C;
     float2* k3 = (float2*)C.alloc((size_t)ngl * nc * nz * per * sizeof(float2));
-    grase_kspace(P, I, acq, in.phase, d_lw, P.table.n_shots, g0, g1, P.mask, k3, st);
+    grase_kspace(P, I, acq, in.phase, d_lw, g0, g1, P.mask, k3, st);
     grase_noise(C, P, k3, g0, g1, seed, P.mask, acq, st);
     float2* sl = (float2*)C.alloc((size_t)ngl * nz * nc * per * sizeof(float2));
     grase_izdft_kernel<<<grid3(per, nz, ngl * nc), 256, 0, st>>>(k3, d_zk, nx, ny, nz, nc, sl);
@@ -486,6 +493,274 @@ void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, con
   }
   MRSIM_CUDA(cudaMemcpyAsync(mag, d_mag, per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
   MRSIM_CUDA(cudaMemcpyAsync(ph, d_ph, per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+}
+
+// ---- the 3D gradient-echo train (`simulate_acquisition_3d_ge_complex`, kspace3d.rs:732-835) -------
+// Per echo: the 2D forward with gradient-echo formation at t_echo = TE_e, its line timing
+// t = the block's, trf = TE_e + t; class compartments (uniform T2, T2') take the decay
+// exp(-(TE_e + t)(1/T2 + 1/T2')) as a line weight, the others decay inside the forward.  The
+// per-excitation weights w[(p ky_segments + sy) ncomp + c] enter as the z-DFT's line weights.
+namespace {
+
+struct GeVolumeData {
+  std::vector<const float*> images;  // ncomp (NULL = unused)
+  std::vector<double> weights;
+};
+
+GeVolumeData fetch_ge_volume(const mrsim_acquisition_ge_input& in, int g, int n_exc_lines) {
+  mrsim_ge_volume v;
+  std::memset(&v, 0, sizeof v);
+  if (!in.volume) fail("the volume callback is NULL");
+  if (in.volume(g, in.user, &v) != 0) fail("volume " + std::to_string(g) + ": the volume callback failed");
+  GeVolumeData d;
+  d.images.assign((size_t)in.ncomp, nullptr);
+  if (in.ncomp > 0 && !v.images) fail("volume " + std::to_string(g) + ": no compartment images");
+  for (int c = 0; c < (int)in.ncomp; ++c) d.images[c] = v.images[c];
+  if (!v.weights) fail("volume " + std::to_string(g) + ": weights are not (partition, ky segment, compartment)");
+  d.weights.assign(v.weights, v.weights + n_exc_lines);
+  for (int c = 0; c < (int)in.ncomp; ++c)
+    if (!d.images[c])
+      for (int x = 0; x < n_exc_lines / std::max<int>(1, (int)in.ncomp); ++x)
+        if (d.weights[(size_t)x * in.ncomp + c] != 0.0)
+          fail("volume " + std::to_string(g) + ": compartment " + std::to_string(c) +
+               " has no image but a nonzero weight");
+  return d;
+}
+
+}  // namespace
+
+static GrasePlan make_ge_plan(const mrsim_acquisition_ge_input& in, const mrsim_acquisition& acq,
+                              const mrsim_excitation_train& train, const mrsim_ge3d_readout& ro, Ge3dTable& table) {
+  GrasePlan P;
+  P.snx = (int)in.sim_dims[0];
+  P.sny = (int)in.sim_dims[1];
+  P.nz = (int)in.sim_dims[2];
+  P.nx = (int)in.acq_dims[0];
+  P.ny = (int)in.acq_dims[1];
+  if (P.nz != (int)in.acq_dims[2]) fail("partition count must match; z is never oversampled");
+  if (P.snx <= 0 || P.sny <= 0 || P.nx <= 0 || P.ny <= 0 || P.nz <= 0) fail("empty simulation grid or acquired matrix");
+  if (!(P.snx % P.nx == 0 && P.sny % P.ny == 0)) fail("sim grid must be an integer multiple of the acquired matrix");
+  P.o = P.snx / P.nx;
+  if (P.o != P.sny / P.ny) fail("oversampling must match on both axes");
+  P.ncomp = (int)in.ncomp;
+  if (P.ncomp > kMaxComp) fail("more than 8 compartments");
+  P.nc = (int)std::max<int64_t>(acq.n_coils, 1);
+  if (P.nc > kMaxCoils) fail("more than 64 coils");
+  if (P.nx > 1024) fail("acquired matrix too wide for the reconstruction");
+  P.plane = (size_t)P.snx * P.sny;
+  P.nvox = P.plane * P.nz;
+  if (!in.fmap) fail("fieldmap is not on the simulation grid");
+  if (P.ncomp > 0 && !in.t2) fail("t2 has 0 entries for " + std::to_string(P.ncomp) + " compartments");
+  if (acq.echo != MRSIM_ECHO_GRADIENT) fail("the 3D gradient-echo train is a gradient-echo acquisition");
+  if (acq.eddy_strength != 0.0 || acq.eddy_quad != 0.0 || acq.eddy_phase != 0.0)
+    fail("the eddy model is not available in 3D (an excitation-dependent eddy evolution breaks the z factorization)");
+  if (!(acq.partial_fourier >= 1.0)) fail("partial Fourier is not available on the 3D gradient-echo train");
+  if ((ro.reverse_phase != 0) != (acq.reverse_phase != 0))
+    fail("the readout's phase-encode sign must be the acquisition's");
+  if (train.n_echoes < 1 || !train.echo_times_ms) fail("a 3D gradient-echo train needs at least one echo time");
+  table = ge3d_lines(train, ro, P.ny, P.nz);
+  P.etl = 0;
+  P.shot.resize((size_t)P.nz * P.ny);
+  const int kys = (int)ro.ky_segments;
+  for (int p = 0; p < P.nz; ++p)
+    for (int ky = 0; ky < P.ny; ++ky) P.shot[(size_t)p * P.ny + ky] = p * kys + ky % kys;
+  P.n_shots = P.nz * kys;
+  P.used.assign(P.ncomp, 1);
+  P.modes.resize(P.ncomp);
+  for (int c = 0; c < P.ncomp; ++c) {
+    const mrsim_t2 ti = in.t_inhom ? in.t_inhom[c] : mrsim_t2{nullptr, (float)acq.t_inhom, 0};
+    CompMode& m = P.modes[c];
+    if (!in.t2[c].is_map && !ti.is_map) {
+      m.t2_ms = in.t2[c].value;
+      m.t2p_ms = ti.value;
+    } else if (acq.do_relaxation) {
+      m.voxel = true;  // decay inside the forward; no echo amplitudes on a gradient-echo train
+    } else {
+      m.t2_ms = INFINITY;
+      m.t2p_ms = INFINITY;
+    }
+  }
+  P.mask = sampling_mask(P.nx, P.ny, acq);
+  const double zs = (double)(P.nz / 2);
+  P.zk.resize((size_t)P.nz * P.nz);
+  for (int p = 0; p < P.nz; ++p)
+    for (int z = 0; z < P.nz; ++z) {
+      const double th = kTau * ((double)p - zs) * ((double)z - zs) / (double)P.nz;
+      P.zk[(size_t)p * P.nz + z] = make_float2((float)std::cos(th), (float)std::sin(th));
+    }
+  P.src_of.assign((size_t)P.ncomp * P.nz, 0);
+  for (int c = 0; c < P.ncomp; ++c) {
+    P.srcs.push_back({c, 0});
+    for (int p = 0; p < P.nz; ++p) P.src_of[(size_t)c * P.nz + p] = c;
+  }
+  P.within.t_ms = table.block.t_ms;
+  P.within.tread_ms = table.block.t_ms;
+  P.within.polarity = table.block.polarity;
+  return P;
+}
+
+// The plan of echo e: the line timing at TE_e and the class decay weights.
+static void ge_echo(GrasePlan& P, const mrsim_acquisition& acq, double te) {
+  P.within.trf_ms.resize(P.ny);
+  for (int ky = 0; ky < P.ny; ++ky) P.within.trf_ms[ky] = te + P.within.t_ms[ky];
+  P.wc.assign((size_t)P.ncomp * P.nz * P.ny, 1.f);
+  for (int c = 0; c < P.ncomp; ++c) {
+    const CompMode& m = P.modes[c];
+    if (m.voxel || !acq.do_relaxation) continue;
+    for (int ky = 0; ky < P.ny; ++ky) {
+      const double trf = te + P.within.t_ms[ky];  // `ge_line_weight` kspace3d.rs:607-612
+      const double d2 = std::isinf(m.t2_ms) ? 0.0 : trf / m.t2_ms;
+      const double dp = std::isinf(m.t2p_ms) ? 0.0 : trf / m.t2p_ms;
+      const float w = (float)std::exp(-d2 - dp);
+      for (int p = 0; p < P.nz; ++p) P.wc[((size_t)c * P.nz + p) * P.ny + ky] = w;
+    }
+  }
+}
+
+// One volume's inputs (images of the compartments it uses, voxel maps) and its weights.
+static GraseInputs upload_ge_volume(DevArena& A, const GrasePlan& P, const mrsim_acquisition_ge_input& in,
+                                    const GeVolumeData& v, const mrsim_acquisition& acq, const float** d_lw,
+                                    cudaStream_t st) {
+  GraseInputs I;
+  I.nv = 1;
+  I.img = (float*)A.alloc(std::max<size_t>(1, P.nvox * P.ncomp) * 4);
+  MRSIM_CUDA(cudaMemsetAsync(I.img, 0, std::max<size_t>(1, P.nvox * P.ncomp) * 4, st));
+  for (int c = 0; c < P.ncomp; ++c) {
+    if (!v.images[c]) continue;
+    for (int z = 0; z < P.nz; ++z)  // [z][c][plane]
+      MRSIM_CUDA(cudaMemcpyAsync(I.img + ((size_t)z * P.ncomp + c) * P.plane, v.images[c] + (size_t)z * P.plane,
+                                 P.plane * 4, cudaMemcpyHostToDevice, st));
+  }
+  I.fmap = (float*)A.upload(in.fmap, P.nvox * 4, st);
+  bool any_voxel = false;
+  for (auto& m : P.modes) any_voxel = any_voxel || m.voxel;
+  if (any_voxel) {
+    std::vector<float> t2((size_t)P.ncomp * P.nvox, 1.f), ti((size_t)P.ncomp * P.nvox, 1.f);
+    for (int c = 0; c < P.ncomp; ++c) {
+      if (!P.modes[c].voxel) continue;
+      for (size_t i = 0; i < P.nvox; ++i) {
+        t2[(size_t)c * P.nvox + i] = in.t2[c].is_map ? in.t2[c].map[i] : in.t2[c].value;
+        ti[(size_t)c * P.nvox + i] =
+            in.t_inhom ? (in.t_inhom[c].is_map ? in.t_inhom[c].map[i] : in.t_inhom[c].value) : (float)acq.t_inhom;
+      }
+    }
+    I.t2 = (float*)A.upload(t2.data(), t2.size() * 4, st);
+    I.ti = (float*)A.upload(ti.data(), ti.size() * 4, st);
+  }
+  std::vector<float> lw(v.weights.begin(), v.weights.end());
+  *d_lw = (const float*)A.upload(lw.data(), std::max<size_t>(1, lw.size()) * 4, st);
+  return I;
+}
+
+void ge_acquire(mrsim_context* ctx, const mrsim_acquisition_ge_input& in, const mrsim_acquisition& acq,
+                const mrsim_excitation_train& train, const mrsim_ge3d_readout& ro, uint64_t seed, float* const* mag,
+                float* const* ph) {
+  cudaStream_t st = ctx->stream;
+  Ge3dTable table;
+  GrasePlan P = make_ge_plan(in, acq, train, ro, table);
+  const int nv = (int)in.n_volumes, nz = P.nz, nc = P.nc, nx = P.nx, ny = P.ny;
+  const int n_echoes = (int)train.n_echoes, n_exc_lines = nz * (int)ro.ky_segments * P.ncomp;
+  const size_t per = (size_t)nx * ny;
+  const int accel = (int)std::max<int64_t>(acq.accel, 1);
+  for (int e = 0; e < n_echoes; ++e) {
+    if (!mag || !ph || !mag[e] || !ph[e]) fail("an output buffer of echo " + std::to_string(e) + " is NULL");
+    if (e > 0 && !(train.echo_times_ms[e] > train.echo_times_ms[e - 1]))
+      fail("the echo times must increase strictly");
+  }
+  DevArena A;
+  const float2* d_zk = (const float2*)A.upload(P.zk.data(), P.zk.size() * sizeof(float2), st);
+  ReconTables T = build_recon_tables(A, nx, ny, nc, acq, st);
+  const size_t w_per_slice = (size_t)(accel - 1) * nc * 6 * nc;
+  // GRAPPA: per echo, one kernel per slice from the reference scan (`reference`, else volume 0)
+  std::vector<float2*> W(n_echoes, nullptr);
+  if (accel > 1 && nv > 0) {
+    GeVolumeData ref;
+    if (in.reference) {
+      ref.images.assign(in.reference->images, in.reference->images + in.ncomp);
+      ref.weights.assign(in.reference->weights, in.reference->weights + n_exc_lines);
+    } else {
+      ref = fetch_ge_volume(in, 0, n_exc_lines);
+    }
+    mrsim_acquisition acq_cal = acq;
+    acq_cal.accel = 1;
+    acq_cal.n_spikes = 0;
+    GrasePlan Pc = P;
+    Pc.mask = sampling_mask(nx, ny, acq_cal);
+    for (int c = 0; c < P.ncomp; ++c) Pc.used[c] = ref.images[c] != nullptr;
+    DevArena C;
+    const float* d_lw = nullptr;
+    GraseInputs Ic = upload_ge_volume(C, Pc, in, ref, acq, &d_lw, st);
+    for (int e = 0; e < n_echoes; ++e) {
+      const double te = train.echo_times_ms[e];
+      ge_echo(Pc, acq_cal, te);
+      mrsim_acquisition ae = acq_cal;
+      ae.t_echo = te;
+      float2* k3 = (float2*)C.alloc((size_t)nc * nz * per * sizeof(float2));
+      grase_kspace(Pc, Ic, ae, in.phase, d_lw, 0, 1, Pc.mask, k3, st);
+      grase_noise(C, Pc, k3, 0, 1, (seed ^ echo_salt((uint64_t)e)) ^ kSeedSaltGrappaCal, Pc.mask, acq_cal, st);
+      float2* sl = (float2*)C.alloc((size_t)nz * nc * per * sizeof(float2));
+      grase_izdft_kernel<<<grid3(per, nz, nc), 256, 0, st>>>(k3, d_zk, nx, ny, nz, nc, sl);
+      std::vector<float2*> refs;
+      for (int z = 0; z < nz; ++z) refs.push_back(sl + (size_t)z * nc * per);
+      W[e] = fit_grappa(A, refs, nx, ny, nc, acq_cal, accel, (int)acq.acs_lines, st);
+      MRSIM_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+  std::vector<float*> d_mag(n_echoes), d_ph(n_echoes);
+  for (int e = 0; e < n_echoes; ++e) {
+    d_mag[e] = (float*)A.alloc(std::max<size_t>(1, per * nz * nv) * 4);
+    d_ph[e] = (float*)A.alloc(std::max<size_t>(1, per * nz * nv) * 4);
+  }
+  for (int g = 0; g < nv; ++g) {
+    GeVolumeData v = fetch_ge_volume(in, g, n_exc_lines);
+    GrasePlan Pg = P;
+    for (int c = 0; c < P.ncomp; ++c) Pg.used[c] = v.images[c] != nullptr;
+    DevArena C;
+    const float* d_lw = nullptr;
+    GraseInputs I = upload_ge_volume(C, Pg, in, v, acq, &d_lw, st);
+    for (int e = 0; e < n_echoes; ++e) {
+      const double te = train.echo_times_ms[e];
+      ge_echo(Pg, acq, te);
+      mrsim_acquisition ae = acq;
+      ae.t_echo = te;
+      DevArena E;
+      float2* k3 = (float2*)E.alloc((size_t)nc * nz * per * sizeof(float2));
+      grase_kspace(Pg, I, ae, in.phase, d_lw, 0, 1, Pg.mask, k3, st);
+      // the noise and spikes of echo e on its own streams (echo 0 unsalted)
+      grase_noise(E, Pg, k3, g, g + 1, seed ^ echo_salt((uint64_t)e), Pg.mask, acq, st);
+      float2* sl = (float2*)E.alloc((size_t)nz * nc * per * sizeof(float2));
+      grase_izdft_kernel<<<grid3(per, nz, nc), 256, 0, st>>>(k3, d_zk, nx, ny, nz, nc, sl);
+      float2* comb = (float2*)E.alloc((size_t)nz * per * sizeof(float2));
+      std::vector<ReconJob> jobs;
+      for (int z = 0; z < nz; ++z) {
+        ReconJob J;
+        std::memset(&J, 0, sizeof J);
+        J.k = sl + (size_t)z * nc * per;
+        J.grappa_w = W[e] ? W[e] + (size_t)z * w_per_slice : nullptr;
+        J.window = T.window;
+        J.ex_tab = T.ex_tab;
+        J.ey_tab = T.ey_tab;
+        J.sens = T.sens;
+        J.inv_ssum = T.inv_ssum;
+        J.combined = comb + (size_t)z * per;
+        J.nx = nx;
+        J.ny = ny;
+        J.nc = nc;
+        jobs.push_back(J);
+      }
+      const ReconJob* d_jobs = (const ReconJob*)E.upload(jobs.data(), jobs.size() * sizeof(ReconJob), st);
+      if (accel > 1) launch_grappa_apply(d_jobs, (int)jobs.size(), T.fills, T.n_fills, nx, nc, st);
+      launch_recon_combine(d_jobs, (int)jobs.size(), nx, ny, false, st);
+      volume_output_kernel<<<1024, 256, 0, st>>>(comb, g, 1, nv, per * nz, d_mag[e], d_ph[e]);
+      MRSIM_CUDA(cudaGetLastError());
+      MRSIM_CUDA(cudaStreamSynchronize(st));
+    }
+  }
+  for (int e = 0; e < n_echoes; ++e) {
+    MRSIM_CUDA(cudaMemcpyAsync(mag[e], d_mag[e], per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaMemcpyAsync(ph[e], d_ph[e], per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+  }
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
 

@@ -14,4 +14,9 @@ void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, con
 void grase_observed(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
                     const mrsim_echo_train& train, const mrsim_grase_readout& ro, int g, float* out);
 
+// `simulate_acquisition_3d_ge` (kspace3d.rs:732-856): per echo e, mag[e] / ph[e] at vox * nv + g.
+void ge_acquire(mrsim_context* ctx, const mrsim_acquisition_ge_input& in, const mrsim_acquisition& acq,
+                const mrsim_excitation_train& train, const mrsim_ge3d_readout& ro, uint64_t seed, float* const* mag,
+                float* const* ph);
+
 }  // namespace mrsim

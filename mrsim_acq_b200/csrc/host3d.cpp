@@ -95,6 +95,42 @@ Grase3dTable grase_lines(const mrsim_echo_train& train, const mrsim_grase_readou
   return T;
 }
 
+Ge3dTable ge3d_lines(const mrsim_excitation_train& train, const mrsim_ge3d_readout& ro, int ny, int nz) {
+  if (nz < 2) fail("a 3D gradient-echo train on " + std::to_string(nz) + " partition is a 2D readout");
+  Ge3dTable T;
+  T.block = grase_block(ny, (int)ro.ky_segments, ro.t_line_ms, ro.reverse_phase != 0);
+  const int kzs = (int)train.kz_segments;
+  if (kzs <= 0 || nz % kzs != 0)
+    fail(std::to_string(nz) + " partitions do not divide into " + std::to_string(train.kz_segments) + " kz segments");
+  T.n_exc = nz / kzs;
+  auto order = kz_order(nz, train.kz_order);
+  T.ny = ny;
+  T.nz = nz;
+  T.lines.assign((size_t)ny * nz, Ge3dLine{0, 0, 0.0, 0});
+  std::vector<char> seen((size_t)ny * nz, 0);
+  for (int sy = 0; sy < (int)ro.ky_segments; ++sy)
+    for (int sz = 0; sz < kzs; ++sz) {
+      const int shot = sy * kzs + sz;
+      for (int j = 0; j < T.n_exc; ++j) {
+        const int p = order[sz + kzs * j];
+        for (int i = 0; i < T.block.epi; ++i) {
+          const int ky = sy + (int)ro.ky_segments * i;
+          const size_t at = (size_t)p * ny + ky;
+          if (seen[at]) fail("line (" + std::to_string(p) + ", " + std::to_string(ky) + ") read twice");
+          seen[at] = 1;
+          T.lines[at] = Ge3dLine{shot, j, T.block.t_ms[ky], T.block.polarity[ky]};
+        }
+      }
+    }
+  for (char s : seen)
+    if (!s) fail("a line was never read");
+  int n_c = 0;
+  while (order[n_c] != nz / 2) ++n_c;
+  T.n_shots = (int)ro.ky_segments * kzs;
+  T.e_c = n_c / kzs;
+  return T;
+}
+
 double line_weight(double ln_a, double t_ms, double t2_ms, double t2p_ms) {
   const double d2 = std::isinf(t2_ms) ? 0.0 : t_ms / t2_ms;
   const double dp = std::isinf(t2p_ms) ? 0.0 : std::fabs(t_ms) / t2p_ms;

@@ -36,6 +36,20 @@ struct Grase3dTable {
 int centre_echo(const mrsim_echo_train& train, int nz);
 Grase3dTable grase_lines(const mrsim_echo_train& train, const mrsim_grase_readout& ro, int ny, int nz);
 
+// `Ge3dLine` / `Ge3dTable` / `ge3d_lines` (readout.rs:381-450), lines indexed p * ny + ky.
+struct Ge3dLine {
+  int shot, excitation;
+  double t_ms;
+  int8_t polarity;
+};
+struct Ge3dTable {
+  int ny = 0, nz = 0, n_shots = 0, n_exc = 0, e_c = 0;
+  std::vector<Ge3dLine> lines;
+  GraseBlock block;
+  const Ge3dLine& line(int p, int ky) const { return lines[(size_t)p * ny + ky]; }
+};
+Ge3dTable ge3d_lines(const mrsim_excitation_train& train, const mrsim_ge3d_readout& ro, int ny, int nz);
+
 // `resolve_modes` (kspace3d.rs:388-432): per compartment, class (ln A per echo, uniform T2/T2')
 // or voxel (ln A_e maps per echo over the simulation volume).
 struct CompMode {

@@ -1,7 +1,9 @@
 """Python mirror of the reference's 3D echo-train acquisition (`kspace3d.rs`, `readout.rs:75-700`)
 over the C ABI: `EchoTrain`, `KzOrder`, `Readout3d::Grase` / `Readout3d::Spiral`, `KzSampling`,
 `KzOptions`, `LineWeights`, `kz_order`, `grase_lines`, `spiral_lines`, `simulate_acquisition_3d`
-(GRASE or stack of spirals), `kspace_3d_observed` and `spiral_samples_3d`.  The acquisition runs on
+(GRASE or stack of spirals), `kspace_3d_observed` and `spiral_samples_3d`; and the 3D
+gradient-echo train: `ExcitationTrain`, `Ge3dReadout`, `GeVolume`, `ge3d_lines`,
+`simulate_acquisition_3d_ge`.  The acquisition runs on
 the device (no CPU path)."""
 from __future__ import annotations
 
@@ -252,3 +254,151 @@ def kspace_3d_observed(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[
     check(lib().mrsim_kspace_3d_observed(ctx.handle, C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
                                          C.byref(readout.to_c()), g, out.view(np.float32).ctypes.data_as(abi.c_f32p)))
     return out.reshape(nc, nz, ny, nx)
+
+
+# ---- the 3D gradient-echo train ------------------------------------------------------------------------
+@dataclasses.dataclass
+class ExcitationTrain:
+    """`ExcitationTrain` (readout.rs:362-369)."""
+
+    kz_segments: int
+    kz_order: KzOrder
+    exc_spacing_ms: float
+    echo_times_ms: Sequence[float]
+    excitation_time_ms: float = 2.0
+
+    def to_c(self, keep: _Keep) -> abi.ExcitationTrain_:
+        t = abi.ExcitationTrain_()
+        t.kz_segments = int(self.kz_segments)
+        t.kz_order = int(self.kz_order)
+        t.exc_spacing_ms = float(self.exc_spacing_ms)
+        t.echo_times_ms = keep.f64(np.asarray(self.echo_times_ms, dtype=np.float64))
+        t.n_echoes = len(self.echo_times_ms)
+        t.excitation_time_ms = float(self.excitation_time_ms)
+        keep.append(t)
+        return t
+
+
+@dataclasses.dataclass
+class Ge3dReadout:
+    """`Ge3dReadout` (readout.rs:374-379)."""
+
+    ky_segments: int
+    t_line_ms: float
+    reverse_phase: bool = False
+
+    def to_c(self) -> abi.Ge3dReadout_:
+        return abi.Ge3dReadout_(int(self.ky_segments), float(self.t_line_ms), int(bool(self.reverse_phase)), 0)
+
+
+@dataclasses.dataclass
+class GeVolume:
+    """`GeVolume` (kspace3d.rs:592-603): per compartment one sim volume (None = unused) and the
+    excitation weights w[(p * ky_segments + sy) * ncomp + c]."""
+
+    images: Sequence[Optional[np.ndarray]]
+    weights: np.ndarray
+
+
+@dataclasses.dataclass
+class GeTable:
+    """`Ge3dTable` (readout.rs:393-407)."""
+
+    shot: np.ndarray
+    excitation: np.ndarray
+    t_ms: np.ndarray
+    polarity: np.ndarray
+    n_shots: int
+    n_exc: int
+    e_c: int
+
+
+def ge3d_lines(train: ExcitationTrain, ro: Ge3dReadout, ny: int, nz: int) -> GeTable:
+    keep = _Keep()
+    n = ny * nz
+    shot, exc = np.zeros(n, np.int64), np.zeros(n, np.int64)
+    t, pol = np.zeros(n), np.zeros(n, np.int8)
+    vals = [C.c_int64() for _ in range(3)]
+    P = C.POINTER(C.c_int64)
+    check(lib().mrsim_ge3d_lines(C.byref(train.to_c(keep)), C.byref(ro.to_c()), ny, nz, shot.ctypes.data_as(P),
+                                 exc.ctypes.data_as(P), t.ctypes.data_as(abi.c_f64p),
+                                 pol.ctypes.data_as(C.POINTER(C.c_int8)), *[C.byref(v) for v in vals]))
+    return GeTable(shot, exc, t, pol, *[v.value for v in vals])
+
+
+class _GeVolumes:
+    """The `volume` callback over a Python callable, keeping each volume's buffers alive."""
+
+    def __init__(self, volume, ncomp):
+        self.volume, self.ncomp, self.keep = volume, ncomp, None
+        self.error = None
+        self.fn = abi.GE_VOLUME_FN(self._call)
+
+    @staticmethod
+    def fill(v: GeVolume, ncomp: int, keep: _Keep) -> abi.GeVolume_:
+        out = abi.GeVolume_()
+        ps = (abi.c_f32p * max(1, ncomp))()
+        for c in range(ncomp):
+            im = v.images[c]
+            ps[c] = keep.f32(np.ravel(im)) if im is not None and np.size(im) > 0 else None
+        keep.append(ps)
+        out.images = ps
+        out.weights = keep.f64(np.ravel(v.weights))
+        return out
+
+    def _call(self, g, user, out):
+        try:
+            self.keep = _Keep()
+            out[0] = self.fill(self.volume(int(g)), self.ncomp, self.keep)
+            return 0
+        except Exception as e:  # the library turns a non-zero return into an error
+            self.error = e
+            return 1
+
+
+def ge_input_c(sim_dims, acq_dims, n_volumes, t2: Sequence[T2], fmap, t_inhom: Optional[Sequence[T2]],
+               phase: Optional[PhaseModel], vols: _GeVolumes, reference: Optional[GeVolume], keep: _Keep):
+    s = abi.AcquisitionGeInput_()
+    for i in range(3):
+        s.sim_dims[i] = int(sim_dims[i])
+        s.acq_dims[i] = int(acq_dims[i])
+    s.n_volumes = int(n_volumes)
+    s.ncomp = len(t2)
+    s.t2 = keep.t2s(t2)
+    s.fmap = keep.f32(np.ravel(fmap))
+    s.t_inhom = keep.t2s(t_inhom) if t_inhom is not None else None
+    if phase is not None:
+        pm = phase.to_c()
+        keep.append(pm)
+        s.phase = C.pointer(pm)
+    s.volume = vols.fn
+    if reference is not None:
+        r = _GeVolumes.fill(reference, len(t2), keep)
+        keep.append(r)
+        s.reference = C.pointer(r)
+    return s
+
+
+def simulate_acquisition_3d_ge(sim_dims, acq_dims, n_volumes: int, t2: Sequence[T2], fmap,
+                               t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: ExcitationTrain,
+                               readout: Ge3dReadout, volume, phase: Optional[PhaseModel] = None, seed: int = 0,
+                               reference: Optional[GeVolume] = None, ctx: Optional[Context] = None):
+    """`simulate_acquisition_3d_ge` (kspace3d.rs:837-856): per echo (magnitude, phase) f32 at vox * nv + g.
+    `volume(g)` returns the GeVolume of volume g, called once per volume on this thread."""
+    ctx = ctx or default_context()
+    keep = _Keep()
+    vols = _GeVolumes(volume, len(t2))
+    s = ge_input_c(sim_dims, acq_dims, n_volumes, t2, fmap, t_inhom, phase, vols, reference, keep)
+    n = int(np.prod(acq_dims)) * n_volumes
+    ne = len(train.echo_times_ms)
+    mags = [np.zeros(n, np.float32) for _ in range(ne)]
+    phs = [np.zeros(n, np.float32) for _ in range(ne)]
+    mp = (abi.c_f32p * ne)(*[m.ctypes.data_as(abi.c_f32p) for m in mags])
+    pp = (abi.c_f32p * ne)(*[p.ctypes.data_as(abi.c_f32p) for p in phs])
+    status = lib().mrsim_simulate_acquisition_3d_ge(ctx.handle, C.byref(s), C.byref(acq.to_c()),
+                                                    C.byref(train.to_c(keep)), C.byref(readout.to_c()),
+                                                    int(seed) & 0xFFFFFFFFFFFFFFFF, mp, pp)
+    if vols.error is not None:
+        raise vols.error
+    check(status)
+    return list(zip(mags, phs))

@@ -3075,6 +3075,221 @@ std::vector<std::vector<Cx>> spiral_volumes_o(const mrsim_acquisition_3d_input& 
   return vols;
 }
 
+
+// ============================ the 3D gradient-echo train ==================================
+// readout.rs:356-450 (`ExcitationTrain`, `ge3d_lines`), kspace3d.rs:590-856 (`GePlan`,
+// `simulate_acquisition_3d_ge_complex`).
+struct GeVolO {
+  std::vector<std::vector<float>> images;  // empty = unused
+  std::vector<double> weights;
+};
+
+GeVolO ge_copy(const mrsim_ge_volume& v, size_t ncomp, size_t nvox, size_t n_exc_lines) {
+  GeVolO o;
+  o.images.resize(ncomp);
+  for (size_t c = 0; c < ncomp; ++c)
+    if (v.images[c]) o.images[c].assign(v.images[c], v.images[c] + nvox);
+  o.weights.assign(v.weights, v.weights + n_exc_lines);
+  return o;
+}
+
+struct GePlanO {
+  size_t snx, sny, nz, nx, ny, o, ncomp, kys;
+  mrsim_acquisition acq;
+  std::vector<double> t_ms;
+  std::vector<int8_t> pol;
+  std::vector<std::pair<bool, std::pair<double, double>>> cls;  // (class?, (T2, T2'))
+  const mrsim_t2* t2;
+  const mrsim_t2* ti;
+  const float* fmap;
+  mrsim_phase_model phase;
+  std::vector<Cx> zk;
+  std::vector<uint8_t> mask;
+
+  std::vector<std::vector<Cx>> compartments(const GeVolO& vol, size_t q, size_t ncoils, double te) const {
+    size_t nplane = snx * sny;
+    mrsim_acquisition base = acq;
+    base.echo = MRSIM_ECHO_GRADIENT;
+    base.t_echo = te;
+    base.noise_variance = 0.0;
+    base.n_spikes = 0;
+    mrsim_acquisition norel = base, rel = base;
+    norel.do_relaxation = 0;
+    rel.do_relaxation = 1;
+    LineTiming within;
+    within.t_ms = t_ms;
+    for (double t : t_ms) within.trf_ms.push_back(te + t);
+    within.tread_ms = t_ms;
+    within.polarity = pol;
+    Shot zero;
+    std::vector<std::vector<Cx>> out(ncomp);
+    for (size_t c = 0; c < ncomp; ++c) {
+      if (vol.images[c].empty()) continue;
+      bool voxel = !cls[c].first && acq.do_relaxation;
+      const mrsim_acquisition& ac = voxel ? rel : norel;
+      std::vector<std::vector<Cx>> k2(nz);
+      for (size_t z = 0; z < nz; ++z) {
+        std::vector<double> phi = phase_slice(phase, zero, snx, sny, o, z, nz);
+        const float* comps[1] = {vol.images[c].data() + z * nplane};
+        mrsim_t2 t2s[1] = {t2[c].is_map ? mrsim_t2{t2[c].map + z * nplane, 0.f, 1} : t2[c]};
+        mrsim_t2 tis[1];
+        if (ti) tis[0] = ti[c].is_map ? mrsim_t2{ti[c].map + z * nplane, 0.f, 1} : ti[c];
+        mrsim_slice_input inp;
+        std::memset(&inp, 0, sizeof inp);
+        inp.compartments = comps;
+        inp.ncomp = 1;
+        inp.t2 = t2s;
+        inp.t_inhom = ti ? tis : nullptr;
+        inp.fmap = fmap + z * nplane;
+        inp.phase0 = phi.data();
+        inp.sim[0] = (int64_t)snx;
+        inp.sim[1] = (int64_t)sny;
+        inp.acq_matrix[0] = (int64_t)nx;
+        inp.acq_matrix[1] = (int64_t)ny;
+        inp.z = (int64_t)z;
+        inp.nz = (int64_t)nz;
+        k2[z] = build_coil_kspace_timed(inp, ac, q, ncoils, within, nullptr);
+      }
+      std::vector<Cx> kc(nz * ny * nx);
+      for (size_t p = 0; p < nz; ++p)
+        for (size_t ky = 0; ky < ny; ++ky) {
+          double w = 1.0;
+          if (cls[c].first && acq.do_relaxation) {
+            double trf = te + t_ms[ky], t2v = cls[c].second.first, tpv = cls[c].second.second;
+            double d2 = std::isinf(t2v) ? 0.0 : trf / t2v, dp = std::isinf(tpv) ? 0.0 : trf / tpv;
+            w = std::exp(-d2 - dp);
+          }
+          for (size_t kx = 0; kx < nx; ++kx) {
+            Cx acc{0, 0};
+            for (size_t z = 0; z < nz; ++z) acc = cadd(acc, cmul(k2[z][ky * nx + kx], zk[p * nz + z]));
+            kc[(p * ny + ky) * nx + kx] = cscale(acc, w);
+          }
+        }
+      out[c] = kc;
+    }
+    return out;
+  }
+
+  std::vector<Cx> kspace(const GeVolO& vol, size_t q, size_t ncoils, double te) const {
+    auto base = compartments(vol, q, ncoils, te);
+    std::vector<Cx> k(nz * ny * nx, Cx{0, 0});
+    for (size_t p = 0; p < nz; ++p)
+      for (size_t ky = 0; ky < ny; ++ky) {
+        if (!mask[ky * nx]) continue;
+        size_t sy = ky % kys;
+        for (size_t c = 0; c < ncomp; ++c) {
+          if (vol.images[c].empty()) continue;
+          double w = vol.weights[(p * kys + sy) * ncomp + c];
+          for (size_t kx = 0; kx < nx; ++kx) {
+            size_t i = (p * ny + ky) * nx + kx;
+            k[i] = cadd(k[i], cscale(base[c][i], w));
+          }
+        }
+      }
+    return k;
+  }
+};
+
+std::vector<std::vector<std::vector<Cx>>> ge_volumes_o(const mrsim_acquisition_ge_input& in, const mrsim_acquisition& acq,
+                                                       const mrsim_excitation_train& tr, const mrsim_ge3d_readout& ro,
+                                                       uint64_t seed, int threads) {
+  GePlanO pl;
+  pl.snx = in.sim_dims[0];
+  pl.sny = in.sim_dims[1];
+  pl.nz = in.sim_dims[2];
+  pl.nx = in.acq_dims[0];
+  pl.ny = in.acq_dims[1];
+  pl.o = pl.snx / pl.nx;
+  pl.ncomp = in.ncomp;
+  pl.kys = (size_t)ro.ky_segments;
+  pl.acq = acq;
+  size_t epi = pl.ny / pl.kys;
+  for (size_t ky = 0; ky < pl.ny; ++ky) {  // `grase_block`
+    size_t j = ky / pl.kys, a = ro.reverse_phase ? j : epi - 1 - j;
+    pl.t_ms.push_back(((double)a - ((double)epi - 1.0) / 2.0) * ro.t_line_ms);
+    pl.pol.push_back(a % 2 == 1 ? -1 : 1);
+  }
+  for (size_t c = 0; c < pl.ncomp; ++c) {
+    mrsim_t2 tic = in.t_inhom ? in.t_inhom[c] : mrsim_t2{nullptr, (float)acq.t_inhom, 0};
+    bool u = !in.t2[c].is_map && !tic.is_map;
+    pl.cls.push_back({u, {(double)in.t2[c].value, (double)tic.value}});
+  }
+  pl.t2 = in.t2;
+  pl.ti = in.t_inhom;
+  pl.fmap = in.fmap;
+  if (in.phase) pl.phase = *in.phase;
+  else std::memset(&pl.phase, 0, sizeof pl.phase);
+  double zs = (double)(pl.nz / 2);
+  pl.zk.resize(pl.nz * pl.nz);
+  for (size_t p = 0; p < pl.nz; ++p)
+    for (size_t z = 0; z < pl.nz; ++z) pl.zk[p * pl.nz + z] = ccis(TAU * ((double)p - zs) * ((double)z - zs) / (double)pl.nz);
+  pl.mask = sampling_mask(pl.nx, pl.ny, acq);
+  size_t nz = pl.nz, nx = pl.nx, ny = pl.ny, nv = in.n_volumes, nvox = pl.snx * pl.sny * nz;
+  size_t ncoils = std::max<int64_t>(acq.n_coils, 1), n_echoes = tr.n_echoes;
+  size_t n_exc_lines = nz * pl.kys * pl.ncomp;
+  double sigma = std::sqrt(acq.noise_variance / (double)(nx * ny));
+  std::vector<GeVolO> vols(nv);
+  for (size_t g = 0; g < nv; ++g) {
+    mrsim_ge_volume v;
+    std::memset(&v, 0, sizeof v);
+    if (in.volume((int64_t)g, in.user, &v) != 0) throw Fail("the volume callback failed");
+    vols[g] = ge_copy(v, pl.ncomp, nvox, n_exc_lines);
+  }
+  std::vector<std::vector<GrappaKernel>> kernels(n_echoes);
+  if (acq.accel > 1 && nv > 0) {
+    GeVolO cal;
+    if (in.reference) {
+      cal = ge_copy(*in.reference, pl.ncomp, nvox, n_exc_lines);
+    } else {
+      mrsim_ge_volume v;
+      std::memset(&v, 0, sizeof v);
+      if (in.volume(0, in.user, &v) != 0) throw Fail("the volume callback failed");
+      cal = ge_copy(v, pl.ncomp, nvox, n_exc_lines);
+    }
+    mrsim_acquisition acq_cal = acq;
+    acq_cal.accel = 1;
+    acq_cal.n_spikes = 0;
+    GePlanO cpl = pl;
+    cpl.acq = acq_cal;
+    cpl.mask = sampling_mask(nx, ny, acq_cal);
+    std::vector<uint8_t> lines = sampling_mask(1, ny, acq_cal);
+    for (size_t e = 0; e < n_echoes; ++e) {
+      uint64_t se = seed ^ ((uint64_t)e * 0xD1B54A32D192ED03ull);
+      std::vector<std::vector<std::vector<Cx>>> parts(ncoils);
+      parallel_for(ncoils, threads, [&](size_t q) {
+        std::vector<Cx> k = cpl.kspace(cal, q, ncoils, tr.echo_times_ms[e]);
+        parts[q] = partitions_to_slices_o(k, cpl.mask, cpl.zk, nx, ny, nz, 0, q, se ^ SEED_SALT_GRAPPA_CAL, acq_cal, sigma);
+      });
+      for (size_t z = 0; z < nz; ++z) {
+        std::vector<std::vector<Cx>> coils(ncoils);
+        for (size_t q = 0; q < ncoils; ++q) coils[q] = parts[q][z];
+        kernels[e].push_back(grappa_fit(coils, nx, ny, acq.accel, acq.acs_lines, lines));
+      }
+    }
+  }
+  std::vector<std::vector<std::vector<Cx>>> out(nv, std::vector<std::vector<Cx>>(n_echoes));
+  parallel_for(nv, threads, [&](size_t g) {
+    for (size_t e = 0; e < n_echoes; ++e) {
+      uint64_t se = seed ^ ((uint64_t)e * 0xD1B54A32D192ED03ull);
+      std::vector<std::vector<std::vector<Cx>>> parts(ncoils);
+      for (size_t q = 0; q < ncoils; ++q) {
+        std::vector<Cx> k = pl.kspace(vols[g], q, ncoils, tr.echo_times_ms[e]);
+        parts[q] = partitions_to_slices_o(k, pl.mask, pl.zk, nx, ny, nz, g, q, se, acq, sigma);
+      }
+      std::vector<Cx> v(nx * ny * nz);
+      for (size_t z = 0; z < nz; ++z) {
+        std::vector<std::vector<Cx>> coils(ncoils);
+        for (size_t q = 0; q < ncoils; ++q) coils[q] = parts[q][z];
+        SliceRecon R = reconstruct_coils_full(coils, acq, nx, ny, false, false, false,
+                                              kernels[e].empty() ? nullptr : &kernels[e][z]);
+        for (size_t i = 0; i < nx * ny; ++i) v[i + nx * ny * z] = R.combined[i];
+      }
+      out[g][e] = v;
+    }
+  });
+  return out;
+}
+
 thread_local std::string g_err;
 std::vector<GoldenCase>* g_golden = nullptr;
 
@@ -3485,6 +3700,39 @@ int oracle_simulate_acquisition_3d_spiral(const mrsim_acquisition_3d_input* in, 
         if (ph) ph[vox * nv + g] = std::atan2(im, re);
       }
     }
+  });
+}
+
+// `simulate_acquisition_3d_ge` (kspace3d.rs:732-856): complex volumes [e][g][vox] (FP64) and per
+// echo the f32 magnitude / phase at vox * nv + g
+int oracle_simulate_acquisition_3d_ge(const mrsim_acquisition_ge_input* in, const mrsim_acquisition* acq,
+                                      const mrsim_excitation_train* tr, const mrsim_ge3d_readout* ro, uint64_t seed,
+                                      int32_t threads, double* vols_out, float* const* mag, float* const* ph) {
+  return guard([&] {
+    auto vols = ge_volumes_o(*in, *acq, *tr, *ro, seed, threads);
+    size_t nv = in->n_volumes, ne = tr->n_echoes;
+    size_t nvox = (size_t)(in->acq_dims[0] * in->acq_dims[1] * in->acq_dims[2]);
+    for (size_t e = 0; e < ne; ++e)
+      for (size_t g = 0; g < nv; ++g) {
+        if (vols_out) put_cx(vols[g][e], vols_out + 2 * nvox * (e * nv + g));
+        for (size_t vox = 0; vox < nvox; ++vox) {
+          float re = (float)vols[g][e][vox].re, im = (float)vols[g][e][vox].im;
+          if (mag) mag[e][vox * nv + g] = std::sqrt(re * re + im * im);
+          if (ph) ph[e][vox * nv + g] = std::atan2(im, re);
+        }
+      }
+  });
+}
+
+// `reconstruct_coils` (kspace.rs:1291-1298) without a GRAPPA kernel: coils [nc][ny*nx] -> combined
+int oracle_reconstruct_coils(const double* coils, int64_t nc, int64_t nx, int64_t ny, const mrsim_acquisition* acq,
+                             double* out) {
+  return guard([&] {
+    std::vector<std::vector<Cx>> k(nc, std::vector<Cx>(nx * ny));
+    for (int64_t q = 0; q < nc; ++q)
+      for (int64_t i = 0; i < nx * ny; ++i) k[q][i] = {coils[2 * (q * nx * ny + i)], coils[2 * (q * nx * ny + i) + 1]};
+    SliceRecon R = reconstruct_coils_full(k, *acq, nx, ny, false, false, false, nullptr);
+    put_cx(R.combined, out);
   });
 }
 

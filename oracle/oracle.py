@@ -89,6 +89,11 @@ def lib():
                                                 C.c_int64, abi.c_f64p]
         L.oracle_simulate_acquisition_3d.argtypes = [A3, P(abi.Acquisition_), P(abi.EchoTrain_), P(abi.GraseReadout_),
                                                      C.c_uint64, C.c_int32, abi.c_f64p, abi.c_f32p, abi.c_f32p]
+        L.oracle_simulate_acquisition_3d_ge.argtypes = [P(abi.AcquisitionGeInput_), P(abi.Acquisition_),
+                                                        P(abi.ExcitationTrain_), P(abi.Ge3dReadout_), C.c_uint64,
+                                                        C.c_int32, abi.c_f64p, P(abi.c_f32p), P(abi.c_f32p)]
+        L.oracle_reconstruct_coils.argtypes = [abi.c_f64p, C.c_int64, C.c_int64, C.c_int64, P(abi.Acquisition_),
+                                               abi.c_f64p]
         KO = P(abi.KzOptions_)
         L.oracle_spiral_lines.argtypes = [P(abi.EchoTrain_), P(abi.SpiralReadout_), C.c_int64, C.c_int64,
                                           P(C.c_uint8), i64p, i64p, i64p, i64p, i64p, abi.c_f64p, abi.c_f64p]
@@ -535,3 +540,37 @@ def simulate_acquisition_3d_spiral(sim_dims, acq_dims, n_volumes, images, t2, t1
                                                        vols.view(np.float64).ctypes.data_as(abi.c_f64p),
                                                        mag.ctypes.data_as(abi.c_f32p), ph.ctypes.data_as(abi.c_f32p)))
     return vols.reshape(n_volumes, nvox), mag, ph
+
+
+# ---- the 3D gradient-echo train ----------------------------------------------------------------------
+def simulate_acquisition_3d_ge(sim_dims, acq_dims, n_volumes, t2, fmap, t_inhom, acq: Acquisition, train, ro, volume,
+                               phase=None, seed: int = 0, reference=None, threads: int = 0):
+    """`simulate_acquisition_3d_ge` (kspace3d.rs:732-856), FP64: complex volumes [e, g, vox] and per
+    echo (mag, phase) f32."""
+    import os
+    from mrsim_acq_b200.kspace3d import _GeVolumes, ge_input_c
+    keep = _Keep()
+    vols = _GeVolumes(volume, len(t2))
+    s = ge_input_c(sim_dims, acq_dims, n_volumes, t2, fmap, t_inhom, phase, vols, reference, keep)
+    nvox = int(np.prod(acq_dims))
+    ne = len(train.echo_times_ms)
+    out = np.zeros(ne * n_volumes * nvox, np.complex128)
+    mags = [np.zeros(nvox * n_volumes, np.float32) for _ in range(ne)]
+    phs = [np.zeros(nvox * n_volumes, np.float32) for _ in range(ne)]
+    mp = (abi.c_f32p * ne)(*[m.ctypes.data_as(abi.c_f32p) for m in mags])
+    pp = (abi.c_f32p * ne)(*[p.ctypes.data_as(abi.c_f32p) for p in phs])
+    _check(lib().oracle_simulate_acquisition_3d_ge(C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c(keep)),
+                                                   C.byref(ro.to_c()), int(seed) & 0xFFFFFFFFFFFFFFFF,
+                                                   threads or (os.cpu_count() or 1),
+                                                   out.view(np.float64).ctypes.data_as(abi.c_f64p), mp, pp))
+    return out.reshape(ne, n_volumes, nvox), list(zip(mags, phs))
+
+
+def reconstruct_coils(coils: np.ndarray, acq: Acquisition) -> np.ndarray:
+    """`reconstruct_coils` (kspace.rs:1291-1298) without GRAPPA, FP64: coils [nc, ny, nx] -> [ny, nx]."""
+    k = np.ascontiguousarray(coils, dtype=np.complex128)
+    nc, ny, nx = k.shape
+    out = np.zeros(ny * nx, np.complex128)
+    _check(lib().oracle_reconstruct_coils(k.view(np.float64).ctypes.data_as(abi.c_f64p), nc, nx, ny,
+                                          C.byref(acq.to_c()), out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+    return out.reshape(ny, nx)
