@@ -489,12 +489,39 @@ int mrsim_simulate_acquisition_3d_spiral(mrsim_context* ctx, const mrsim_acquisi
                                          const mrsim_spiral_readout* ro,
                                          const mrsim_kz_options* kz_opts, uint64_t seed,
                                          float* mag, float* phase);
+/* `SpiralSegmentation` / `spiral_segmentation` (kspace3d.rs:860-870, 1441-1470): the certified
+ * time segmentations a spiral series will use, per slice and mode (class first), or the error
+ * naming the slice whose rate rectangle cannot be certified.  Images are not read.  With rows
+ * NULL only *count is written. */
+typedef struct mrsim_spiral_segmentation_row {
+  int32_t z, voxel, l, m;
+  double b_sum, bound;
+} mrsim_spiral_segmentation_row;
+int mrsim_spiral_segmentation(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                              const mrsim_echo_train* train, const mrsim_spiral_readout* ro,
+                              int64_t capacity, mrsim_spiral_segmentation_row* rows,
+                              int64_t* count);
+
 /* `SpiralPlan::samples_all` (kspace3d.rs:1047-1060): volume g's samples per coil before noise,
  * out [coil][p*nsamp + j] (re, im) f32 (zero on partitions not read). */
 int mrsim_spiral_samples_3d(mrsim_context* ctx, const mrsim_acquisition_3d_input* in,
                             const mrsim_acquisition* acq, const mrsim_echo_train* train,
                             const mrsim_spiral_readout* ro, const mrsim_kz_options* kz_opts,
                             int64_t g, float* out);
+
+/* ---- timing checks of the 3D trains (readout.rs:326-354, 460-500, 706-730) ---------------- */
+/* 0 when the train fits its RF and sampling intervals, else MRSIM_ERR_INVALID with the
+ * reference's message.  `check_spiral_timing` writes the train's end (ms) to end_ms (may be NULL). */
+int mrsim_check_grase_timing(const mrsim_echo_train* train, const mrsim_grase_readout* ro,
+                             int64_t ny, int64_t nz, double t_exc_ms, double tr_ms);
+int mrsim_check_ge3d_timing(const mrsim_excitation_train* train, const mrsim_ge3d_readout* ro,
+                            int64_t ny, int64_t nz, double t_exc_ms, double tr_ms);
+int mrsim_check_spiral_timing(const mrsim_echo_train* train, const mrsim_spiral_readout* ro,
+                              int64_t nx, int64_t ny, int64_t nz, double t_exc_ms, double tr_ms,
+                              double* end_ms);
+/* `esp_from_echo_time` (readout.rs:286-288) and `spiral_esp_from_echo_time` (:702-704). */
+double mrsim_esp_from_echo_time(double te_ms, int64_t e_c, const mrsim_grase_readout* ro, int64_t ny);
+double mrsim_spiral_esp_from_echo_time(double te_ms, int64_t e_c);
 
 /* ---- the stack-of-spirals path: host plans ------------------------------------------------ */
 /* `spiral_tau_c` (readout.rs:564-596): the constant-angular-velocity centre region (ms). */
@@ -534,6 +561,13 @@ int mrsim_epg_cpmg(int64_t n_echoes, double esp_ms, double refocusing_deg, doubl
 /* ---- the stack-of-spirals path: device NUFFT pair and spiral forwards ---------------------- */
 /* Kernel width of the exponential-of-semicircle NUFFT at tolerance tol (nufft.rs:165). */
 int mrsim_nufft_kernel_width(double tol);
+
+/* `Nufft1::new` + `run` (nufft.rs:41-107) on the device in FP64: nw weight vectors (weights
+ * [nw][npos] (re, im) f64) at sources `pos` (cells, any real, period n) to the integer frequencies
+ * k_lo .. k_lo + n_out (inside [-n/2, n/2]): out [nw][n_out] (re, im) f64,
+ * F[k] = sum_j w_j e^{+i2pi k pos_j / n}. */
+int mrsim_nufft1(mrsim_context* ctx, int64_t n, int64_t k_lo, int64_t n_out, double tol,
+                 const double* pos, int64_t npos, const double* weights, int64_t nw, double* out);
 
 /* `Nufft2::type1` (nufft.rs:225-256) on the device, host buffers: periods n, modes m_lo ..
  * m_lo + m_out per axis (inside [-n/2, n/2]), points u [npts][2] (period-n coordinates),

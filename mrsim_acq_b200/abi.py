@@ -188,6 +188,13 @@ class KzOptions_(C.Structure):
                 ("pocs", C.c_int32), ("reserved", C.c_int32)]
 
 
+class SpiralSegmentationRow_(C.Structure):
+    """`mrsim_spiral_segmentation_row` — `SpiralSegmentation` (kspace3d.rs:860-870)."""
+
+    _fields_ = [("z", C.c_int32), ("voxel", C.c_int32), ("l", C.c_int32), ("m", C.c_int32), ("b_sum", C.c_double),
+                ("bound", C.c_double)]
+
+
 class LibraryMissing(RuntimeError):
     pass
 
@@ -250,6 +257,8 @@ def _declare(lib):
                                       C.POINTER(TsegInfo_)]),
         "mrsim_epg_cpmg": (C.c_int, [C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, c_f64p]),
         "mrsim_nufft_kernel_width": (C.c_int, [C.c_double]),
+        "mrsim_nufft1": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int64, C.c_double, c_f64p, C.c_int64, c_f64p,
+                                   C.c_int64, c_f64p]),
         "mrsim_nufft2_type1": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                          C.c_double, c_f64p, C.c_int64, c_f32p, C.c_int32, c_f32p]),
         "mrsim_nufft2_type2": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
@@ -275,6 +284,17 @@ def _declare(lib):
         "mrsim_simulate_acquisition_3d_ge": (C.c_int, [P, C.POINTER(AcquisitionGeInput_), C.POINTER(Acquisition_),
                                                        C.POINTER(ExcitationTrain_), C.POINTER(Ge3dReadout_),
                                                        C.c_uint64, C.POINTER(c_f32p), C.POINTER(c_f32p)]),
+        "mrsim_check_grase_timing": (C.c_int, [C.POINTER(EchoTrain_), C.POINTER(GraseReadout_), C.c_int64, C.c_int64,
+                                               C.c_double, C.c_double]),
+        "mrsim_check_ge3d_timing": (C.c_int, [C.POINTER(ExcitationTrain_), C.POINTER(Ge3dReadout_), C.c_int64,
+                                              C.c_int64, C.c_double, C.c_double]),
+        "mrsim_check_spiral_timing": (C.c_int, [C.POINTER(EchoTrain_), C.POINTER(SpiralReadout_), C.c_int64, C.c_int64,
+                                                C.c_int64, C.c_double, C.c_double, c_f64p]),
+        "mrsim_esp_from_echo_time": (C.c_double, [C.c_double, C.c_int64, C.POINTER(GraseReadout_), C.c_int64]),
+        "mrsim_spiral_esp_from_echo_time": (C.c_double, [C.c_double, C.c_int64]),
+        "mrsim_spiral_segmentation": (C.c_int, [C.POINTER(Acquisition3dInput_), C.POINTER(Acquisition_),
+                                                C.POINTER(EchoTrain_), C.POINTER(SpiralReadout_), C.c_int64,
+                                                C.POINTER(SpiralSegmentationRow_), C.POINTER(C.c_int64)]),
         "mrsim_spiral_lines": (C.c_int, [C.POINTER(EchoTrain_), C.POINTER(SpiralReadout_), C.c_int64, C.c_int64,
                                          C.c_int64, C.POINTER(C.c_uint8), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                          C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),

@@ -891,5 +891,75 @@ int mrsim_simulate_acquisition_3d_ge(mrsim_context* ctx, const mrsim_acquisition
   });
 }
 
+int mrsim_nufft1(mrsim_context* ctx, int64_t n, int64_t k_lo, int64_t n_out, double tol, const double* pos,
+                 int64_t npos, const double* weights, int64_t nw, double* out) {
+  return on_ctx(ctx, [&] {
+    if (npos < 0 || npos > ((int64_t)1 << 30) || nw <= 0 || nw > 4096) mrsim::fail("NUFFT point or vector count out of range");
+    need(out, "out");
+    if (npos > 0) {
+      need(pos, "pos");
+      need(weights, "weights");
+    }
+    mrsim::nufft1_host(ctx, (int)n, (int)k_lo, (int)n_out, tol, pos, (int)npos, weights, (int)nw, out);
+  });
+}
+
+int mrsim_check_grase_timing(const mrsim_echo_train* train, const mrsim_grase_readout* ro, int64_t ny, int64_t nz,
+                             double t_exc_ms, double tr_ms) {
+  return guarded([&] {
+    need(train, "train");
+    need(ro, "readout");
+    std::string e = mrsim::check_grase_timing(*train, mrsim::grase_lines(*train, *ro, (int)ny, (int)nz), t_exc_ms, tr_ms);
+    if (!e.empty()) mrsim::fail(e);
+  });
+}
+
+int mrsim_check_ge3d_timing(const mrsim_excitation_train* train, const mrsim_ge3d_readout* ro, int64_t ny, int64_t nz,
+                            double t_exc_ms, double tr_ms) {
+  return guarded([&] {
+    need(train, "train");
+    need(ro, "readout");
+    std::string e = mrsim::check_ge3d_timing(*train, mrsim::ge3d_lines(*train, *ro, (int)ny, (int)nz), t_exc_ms, tr_ms);
+    if (!e.empty()) mrsim::fail(e);
+  });
+}
+
+int mrsim_check_spiral_timing(const mrsim_echo_train* train, const mrsim_spiral_readout* ro, int64_t nx, int64_t ny,
+                              int64_t nz, double t_exc_ms, double tr_ms, double* end_ms) {
+  return guarded([&] {
+    need(train, "train");
+    need(ro, "readout");
+    mrsim::spiral_lines(*train, *ro, (int)nx, (int)ny, (int)nz);  // the table's own checks first
+    std::string e = mrsim::check_spiral_timing(*train, ro->readout_ms, t_exc_ms, tr_ms, end_ms);
+    if (!e.empty()) mrsim::fail(e);
+  });
+}
+
+double mrsim_esp_from_echo_time(double te_ms, int64_t e_c, const mrsim_grase_readout* ro, int64_t ny) {
+  // `esp_from_echo_time` (readout.rs:286-288): (TE - t(ky = ny/2)) / e_c
+  mrsim::GraseBlock b = mrsim::grase_block((int)ny, (int)ro->ky_segments, ro->t_line_ms, ro->reverse_phase != 0);
+  return (te_ms - b.t_ms[b.t_ms.size() / 2]) / (double)e_c;
+}
+
+double mrsim_spiral_esp_from_echo_time(double te_ms, int64_t e_c) { return te_ms / (double)e_c; }  // readout.rs:702
+
+int mrsim_spiral_segmentation(const mrsim_acquisition_3d_input* in, const mrsim_acquisition* acq,
+                              const mrsim_echo_train* train, const mrsim_spiral_readout* ro, int64_t capacity,
+                              mrsim_spiral_segmentation_row* rows, int64_t* count) {
+  return guarded([&] {
+    need(in, "input");
+    need(acq, "acq");
+    need(train, "train");
+    need(ro, "readout");
+    need(count, "count");
+    auto v = mrsim::spiral_segmentation(*in, *acq, *train, *ro);
+    *count = (int64_t)v.size();
+    if (!rows) return;
+    if (capacity < (int64_t)v.size()) mrsim::fail("row capacity below the segmentations");
+    for (size_t i = 0; i < v.size(); ++i)
+      rows[i] = mrsim_spiral_segmentation_row{v[i].z, v[i].voxel, v[i].l, v[i].m, v[i].b_sum, v[i].bound};
+  });
+}
+
 }  // extern "C"
 #pragma GCC visibility pop

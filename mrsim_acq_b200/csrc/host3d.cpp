@@ -4,10 +4,12 @@
 #include "host3d.h"
 
 #include <cmath>
+#include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
+#include <algorithm>
 #include <utility>
 
 #include "mrsim_internal.h"
@@ -129,6 +131,90 @@ Ge3dTable ge3d_lines(const mrsim_excitation_train& train, const mrsim_ge3d_reado
   T.n_shots = (int)ro.ky_segments * kzs;
   T.e_c = n_c / kzs;
   return T;
+}
+
+namespace {
+std::string fmt(const char* f, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, f);
+  std::vsnprintf(buf, sizeof buf, f, ap);
+  va_end(ap);
+  return buf;
+}
+double block_extent(const GraseBlock& b) {
+  double m = 0.0;
+  for (double t : b.t_ms) m = std::max(m, std::fabs(t));
+  return m;
+}
+}  // namespace
+
+std::string check_grase_timing(const mrsim_echo_train& train, const Grase3dTable& t, double t_exc_ms, double tr_ms) {
+  const double t_line = t.block.t_line_ms, extent = block_extent(t.block), half = train.esp_ms / 2.0;
+  const double need = extent + t_line / 2.0 + train.refocusing_time_ms / 2.0;
+  if (need > half + 1e-9)
+    return fmt("the %d-line EPI block reaches %.4f ms from its echo (lines of %.4f ms), and with half the %.3f ms "
+               "refocusing time needs %.4f ms, more than half the echo spacing (%.4f ms of %.4f ms). Fewer lines per "
+               "block (more ky segments, a smaller matrix), shorter lines, or a longer echo spacing would fit: the echo "
+               "spacing must be at least %.4f ms",
+               t.block.epi, extent + t_line / 2.0, t_line, train.refocusing_time_ms, need, half, train.esp_ms,
+               2.0 * need);
+  if (half - train.refocusing_time_ms / 2.0 <= 0.0)
+    return fmt("the first refocusing pulse (%.3f ms long, centred %.4f ms after the excitation) overlaps the excitation",
+               train.refocusing_time_ms, half);
+  const double last = t_exc_ms + (double)train.etl * train.esp_ms + extent + t_line / 2.0;
+  if (last > tr_ms + 1e-9)
+    return fmt("the echo train ends at %.4f ms (excitation at %.4f ms, %lld echoes of %.4f ms), after the %.4f ms "
+               "repetition",
+               last, t_exc_ms, (long long)train.etl, train.esp_ms, tr_ms);
+  return "";
+}
+
+std::string check_ge3d_timing(const mrsim_excitation_train& train, const Ge3dTable& t, double t_exc_ms, double tr_ms) {
+  const double* tes = train.echo_times_ms;
+  const int n = (int)train.n_echoes;
+  if (n < 1 || !tes) return "a 3D gradient-echo train needs at least one echo time";
+  const double half = block_extent(t.block) + t.block.t_line_ms / 2.0, pulse = train.excitation_time_ms / 2.0;
+  auto lo = [&](int e) { return tes[e] - half; };
+  auto hi = [&](int e) { return tes[e] + half; };
+  if (lo(0) < pulse - 1e-9)
+    return fmt("echo 1 at %.4f ms: its %d-line block starts %.4f ms after the excitation, inside the excitation pulse "
+               "(half of %.3f ms); a later echo time or a shorter block would fit",
+               tes[0], t.block.epi, lo(0), train.excitation_time_ms);
+  for (int e = 1; e < n; ++e)
+    if (lo(e) < hi(e - 1) - 1e-9)
+      return fmt("echo %d at %.4f ms and echo %d at %.4f ms: their blocks of %.4f ms each side overlap", e, tes[e - 1],
+                 e + 1, tes[e], half);
+  const double end = hi(n - 1);
+  if (t.n_exc > 1 && end > train.exc_spacing_ms - pulse + 1e-9)
+    return fmt("the last echo's block ends %.4f ms after its excitation, after the next excitation pulse starts at "
+               "%.4f ms (excitation spacing %.4f ms, pulse %.3f ms): the spacing must be at least %.4f ms",
+               end, train.exc_spacing_ms - pulse, train.exc_spacing_ms, train.excitation_time_ms, end + pulse);
+  const double last = t_exc_ms + ((double)t.n_exc - 1.0) * train.exc_spacing_ms + end;
+  if (last > tr_ms + 1e-9)
+    return fmt("the train ends at %.4f ms (%d excitations %.4f ms apart from %.4f ms), after the %.4f ms repetition",
+               last, t.n_exc, train.exc_spacing_ms, t_exc_ms, tr_ms);
+  return "";
+}
+
+std::string check_spiral_timing(const mrsim_echo_train& train, double readout_ms, double t_exc_ms, double tr_ms,
+                                double* end_ms) {
+  const double t = readout_ms, half = train.esp_ms / 2.0, need = t + train.refocusing_time_ms / 2.0;
+  if (need > half + 1e-9)
+    return fmt("the %g ms spiral with half the %.3f ms refocusing time needs %.4f ms after its echo, more than half the "
+               "echo spacing (%.4f ms of %.4f ms): it would run into the next refocusing pulse. A shorter spiral (more "
+               "interleaves) or a longer echo spacing would fit: the echo spacing must be at least %.4f ms",
+               t, train.refocusing_time_ms, need, half, train.esp_ms, 2.0 * need);
+  if (half - train.refocusing_time_ms / 2.0 <= 0.0)
+    return fmt("the first refocusing pulse (%.3f ms long, centred %.4f ms after the excitation) overlaps the excitation",
+               train.refocusing_time_ms, half);
+  const double last = t_exc_ms + (double)train.etl * train.esp_ms + t;
+  if (last > tr_ms + 1e-9)
+    return fmt("the echo train ends at %.4f ms (excitation at %.4f ms, %lld echoes of %.4f ms, a %g ms spiral), after "
+               "the %.4f ms repetition",
+               last, t_exc_ms, (long long)train.etl, train.esp_ms, t, tr_ms);
+  if (end_ms) *end_ms = last;
+  return "";
 }
 
 double line_weight(double ln_a, double t_ms, double t2_ms, double t2p_ms) {

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "mrsim_acq.h"
@@ -63,6 +64,13 @@ std::vector<CompMode> resolve_modes(const mrsim_t2* t2, const mrsim_t2* t1, cons
 
 // `line_weight` (kspace3d.rs:83-88): exp(ln_a - t/T2 - |t|/T2'), infinite times meaning no decay.
 double line_weight(double ln_a, double t_ms, double t2_ms, double t2p_ms);
+
+// The timing checks of the trains (readout.rs:326-354, 460-500, 706-730): an empty string when
+// the train fits, else the reference's message.  check_spiral_timing writes the train's end.
+std::string check_grase_timing(const mrsim_echo_train& train, const Grase3dTable& t, double t_exc_ms, double tr_ms);
+std::string check_ge3d_timing(const mrsim_excitation_train& train, const Ge3dTable& t, double t_exc_ms, double tr_ms);
+std::string check_spiral_timing(const mrsim_echo_train& train, double readout_ms, double t_exc_ms, double tr_ms,
+                                double* end_ms);
 
 constexpr uint64_t kSeedSalt3d = 0x334452454144ull;  // "3DREAD" (kspace3d.rs:42)
 

@@ -57,6 +57,18 @@ void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const typena
                  size_t w_stride, typename Vec2<R>::type* modes, size_t mode_stride, typename Vec2<R>::type* work,
                  int sign, cudaStream_t st);
 
+// The 1D type-1 NUFFT (`Nufft1`, nufft.rs:25-112) in FP64: sources at `pos` (cells, period n),
+// outputs at integer frequencies k_lo .. k_lo + n_out, F[k] = sum_j w_j e^{+i2pi k pos_j / n}, for
+// nw weight vectors sharing the positions.  corr and tw on the device; work holds nw fine grids.
+struct Nufft1Grid {
+  int n, nf, w, k_lo, n_out;
+  double beta;
+  const double* corr;
+  const double2* tw;
+};
+void nufft1_run(const Nufft1Grid& g, const double* pos, int npos, const double2* wts, int nw, double2* out,
+                double2* work, cudaStream_t st);
+
 // The exact spiral sum (`spiral_kspace_exact`, spiral.rs:107-137) of one slice and coil.
 struct SpiralExactArgs {
   const double* k;        // npts x 2, cycles/FOV

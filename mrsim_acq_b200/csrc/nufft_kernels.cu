@@ -205,6 +205,35 @@ __global__ void spread_kernel(const NufftGridT<R> g, typename Vec2<R>::type* __r
   }
 }
 
+// ---- the 1D type-1 NUFFT (`Nufft1`, nufft.rs:25-112), FP64 --------------------------------------
+// Spreading: one thread per source, every weight vector in turn (the kernel is evaluated once per
+// source, as the reference does); FP64 atomics on the fine grid of each weight vector.
+__global__ void spread1_kernel(const double* __restrict__ pos, int npos, const double2* __restrict__ wts, int nw,
+                               int nf, int w, double beta, double2* __restrict__ grid) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npos; j += gridDim.x * blockDim.x) {
+    double k[kWMax];
+    const int m0 = es_taps<double>(pos[j], nf, w, beta, k);  // fine position 2 pos on nf = 2n cells
+    for (int q = 0; q < nw; ++q) {
+      const double2 wv = wts[(size_t)q * npos + j];
+      double* g = reinterpret_cast<double*>(grid + (size_t)q * nf);
+      for (int i = 0; i < w; ++i) {
+        const int c = wrap(m0 + i, nf);
+        atomicAdd(g + 2 * c, wv.x * k[i]);
+        atomicAdd(g + 2 * c + 1, wv.y * k[i]);
+      }
+    }
+  }
+}
+
+__global__ void extract1_kernel(const double2* __restrict__ grid, int nf, int k_lo, int n_out,
+                                const double* __restrict__ corr, int nw, double2* __restrict__ out) {
+  const int q = blockIdx.y;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n_out; j += gridDim.x * blockDim.x) {
+    const double2 v = grid[(size_t)q * nf + wrap(k_lo + j, nf)];
+    out[(size_t)q * n_out + j] = make_double2(v.x * corr[j], v.y * corr[j]);
+  }
+}
+
 // ---- spiral forwards ---------------------------------------------------------------------------
 // The exact sum (`spiral_kspace_exact`, spiral.rs:107-137): one thread per sample, voxels staged
 // in shared memory in tiles; the k.r + f tau phase in FP64 (nonuniform k), reduced to turns.
@@ -325,6 +354,7 @@ void fft2(V* grid, int n0, int n1, const V* tw0, const V* tw1, int batch, int si
   // rows (axis 0, contiguous), then columns (axis 1, stride n0)
   for (int axis = 0; axis < 2; ++axis) {
     const int n = axis == 0 ? n0 : n1;
+    if (n == 1) continue;  // a length-1 transform is the identity
     const int lines = axis == 0 ? n1 : n0;
     const size_t es = axis == 0 ? 1 : (size_t)n0;
     const size_t ls = axis == 0 ? (size_t)n0 : 1;
@@ -384,6 +414,18 @@ template void nufft_type1<float>(const NufftGridT<float>&, const double*, int, c
                                  size_t, float2*, int, cudaStream_t);
 template void nufft_type1<double>(const NufftGridT<double>&, const double*, int, const double2*, int, size_t,
                                   double2*, size_t, double2*, int, cudaStream_t);
+
+
+void nufft1_run(const Nufft1Grid& g, const double* pos, int npos, const double2* wts, int nw, double2* out,
+                double2* work, cudaStream_t st) {
+  cudaMemsetAsync(work, 0, (size_t)nw * g.nf * sizeof(double2), st);
+  if (npos > 0)
+    spread1_kernel<<<std::max(1, std::min((npos + 127) / 128, 4096)), 128, 0, st>>>(pos, npos, wts, nw, g.nf, g.w,
+                                                                                   g.beta, work);
+  fft2<double2>(work, g.nf, 1, g.tw, g.tw, nw, 1, st);  // the inverse transform (e^{+i}) of each fine grid
+  dim3 eg((g.n_out + 255) / 256, nw);
+  extract1_kernel<<<eg, 256, 0, st>>>(work, g.nf, g.k_lo, g.n_out, g.corr, nw, out);
+}
 
 void spiral_exact(const SpiralExactArgs& a, cudaStream_t st) {
   spiral_exact_kernel<<<(a.npts + 255) / 256, 256, 0, st>>>(a);

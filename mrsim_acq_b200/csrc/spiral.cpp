@@ -84,6 +84,34 @@ NufftGridT<R> make_nufft(DevArena& A, int n0, int n1, int m_lo0, int m_lo1, int 
 template NufftGridT<float> make_nufft<float>(DevArena&, int, int, int, int, int, int, double, cudaStream_t);
 template NufftGridT<double> make_nufft<double>(DevArena&, int, int, int, int, int, int, double, cudaStream_t);
 
+// ---- the 1D type-1 NUFFT (`Nufft1::new` / `run`, nufft.rs:41-107) on host buffers, FP64 ---------
+void nufft1_host(mrsim_context* ctx, int n, int k_lo, int n_out, double tol, const double* pos, int npos,
+                 const double* weights, int nw, double* out) {
+  if (!(n_out > 0 && k_lo >= -(n / 2) && k_lo + n_out - 1 <= n / 2))
+    fail("output band must sit inside the coarse Nyquist band");
+  if (n <= 0 || n > 4096) fail("NUFFT period must be in 1..4096");
+  cudaStream_t st = ctx->stream;
+  DevArena A;
+  Nufft1Grid g;
+  g.n = n;
+  g.nf = 2 * n;
+  g.w = nufft_width(tol);
+  g.beta = 2.30 * g.w;
+  g.k_lo = k_lo;
+  g.n_out = n_out;
+  auto corr = deapodization(g.nf, g.w, g.beta, k_lo, n_out);
+  g.corr = (const double*)A.upload(corr.data(), corr.size() * 8, st);
+  g.tw = (const double2*)upload_twiddles<double>(A, g.nf, st);
+  const double* dp = npos > 0 ? (const double*)A.upload(pos, (size_t)npos * 8, st) : nullptr;
+  const double2* dw = npos > 0 ? (const double2*)A.upload(weights, (size_t)nw * npos * 16, st) : nullptr;
+  double2* dout = (double2*)A.alloc((size_t)nw * n_out * 16);
+  double2* work = (double2*)A.alloc((size_t)nw * g.nf * 16);
+  nufft1_run(g, dp, npos, dw, nw, dout, work, st);
+  MRSIM_CUDA(cudaGetLastError());
+  MRSIM_CUDA(cudaMemcpyAsync(out, dout, (size_t)nw * n_out * 16, cudaMemcpyDeviceToHost, st));
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+}
+
 // ---- host-buffer NUFFT pair -----------------------------------------------------------------------
 void nufft2_host(mrsim_context* ctx, int type, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
                  const double* u, int npts, const float* in, int sign, float* out) {

@@ -15,6 +15,8 @@ NufftGridT<R> make_nufft(DevArena& A, int n0, int n1, int m_lo0, int m_lo1, int 
                          cudaStream_t st);
 template <class R>
 const void* upload_twiddles(DevArena& A, int n, cudaStream_t st);
+void nufft1_host(mrsim_context* ctx, int n, int k_lo, int n_out, double tol, const double* pos, int npos,
+                 const double* weights, int nw, double* out);
 void nufft2_host(mrsim_context* ctx, int type, int n0, int n1, int m_lo0, int m_lo1, int m_out0, int m_out1, double tol,
                  const double* u, int npts, const float* in, int sign, float* out);
 void spiral_exact_host(mrsim_context* ctx, const mrsim_slice_input& inp, const mrsim_acquisition& acq, int coil,

@@ -471,6 +471,84 @@ std::vector<double2> solve_hermitian_host(std::vector<std::vector<double2>> h, s
 }  // namespace
 
 // ---- the plan ----------------------------------------------------------------------------------------
+// Per slice, the off-resonance interval (Hz) and the decay interval (1/ms) of its voxel-mode
+// compartments (`spiral_rects` kspace3d.rs:876-905).
+struct SliceRect {
+  int z;
+  double f[2], d[2];
+  bool has_d;
+};
+
+static std::vector<SliceRect> spiral_rects(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
+                                           const std::vector<CompMode>& modes, size_t plane, int nz) {
+  std::vector<SliceRect> out;
+  for (int z = 0; z < nz; ++z) {
+    SliceRect r;
+    r.z = z;
+    r.f[0] = r.f[1] = 0.0;
+    r.d[0] = r.d[1] = 0.0;
+    r.has_d = false;
+    if (acq.do_distortions) {
+      float lo = INFINITY, hi = -INFINITY;
+      for (size_t i = 0; i < plane; ++i) {
+        lo = std::min(lo, in.fmap[(size_t)z * plane + i]);
+        hi = std::max(hi, in.fmap[(size_t)z * plane + i]);
+      }
+      r.f[0] = lo;
+      r.f[1] = hi;
+    }
+    for (size_t c = 0; c < modes.size(); ++c) {
+      if (!modes[c].voxel) continue;
+      for (size_t i = (size_t)z * plane; i < (size_t)(z + 1) * plane; ++i) {
+        const double t2 = in.t2[c].is_map ? (double)in.t2[c].map[i] : (double)in.t2[c].value;
+        const double tp = in.t_inhom ? (in.t_inhom[c].is_map ? (double)in.t_inhom[c].map[i]
+                                                              : (double)in.t_inhom[c].value)
+                                     : acq.t_inhom;
+        const double v = 1.0 / t2 + 1.0 / tp;
+        if (!r.has_d) {
+          r.d[0] = r.d[1] = v;
+          r.has_d = true;
+        } else {
+          r.d[0] = std::min(r.d[0], v);
+          r.d[1] = std::max(r.d[1], v);
+        }
+      }
+    }
+    out.push_back(r);
+  }
+  return out;
+}
+
+// `spiral_segmentation` (kspace3d.rs:1441-1470): per slice and mode the certified plan's figures.
+std::vector<SpiralSegmentationRow> spiral_segmentation(const mrsim_acquisition_3d_input& in,
+                                                       const mrsim_acquisition& acq, const mrsim_echo_train& train,
+                                                       const mrsim_spiral_readout& ro) {
+  const int nz = (int)in.sim_dims[2];
+  const size_t plane = (size_t)in.sim_dims[0] * in.sim_dims[1];
+  if (!in.fmap) fail("fieldmap is not on the simulation grid");
+  if (in.ncomp > 0 && !in.t2) fail("t2 is NULL");
+  Spiral3dTable T = spiral_lines(train, ro, (int)in.acq_dims[0], (int)in.acq_dims[1], nz);
+  auto modes = resolve_modes(in.t2, in.t1, in.t_inhom, (int)in.ncomp, acq, train, plane * nz);
+  bool any_class = false;
+  for (auto& m : modes) any_class = any_class || !m.voxel;
+  std::vector<SpiralSegmentationRow> out;
+  for (const SliceRect& r : spiral_rects(in, acq, modes, plane, nz)) {
+    auto add = [&](bool voxel, const double* d) {
+      TsegPlan p;
+      try {
+        p = tseg_plan(T.traj.tau_ms, T.traj.readout_ms, d, r.f);
+      } catch (const Error& e) {
+        fail("slice " + std::to_string(r.z) + ": " + e.what());
+      }
+      out.push_back({r.z, voxel ? 1 : 0, p.l, p.m, p.b_sum, p.bound});
+    };
+    const double zero[2] = {0.0, 0.0};
+    if (any_class) add(false, zero);
+    if (r.has_d) add(true, r.d);
+  }
+  return out;
+}
+
 struct SpiralPlan3 {
   int snx, sny, nz, n, o, ncomp, nc, rows, ring, ns, nsamp;
   size_t plane, nvox;
@@ -564,43 +642,14 @@ static SpiralPlan3 make_spiral_plan(const mrsim_acquisition_3d_input& in, const 
   P.modes = resolve_modes(in.t2, in.t1, in.t_inhom, P.ncomp, acq, train, P.nvox);
   for (auto& m : P.modes) (m.voxel ? P.any_voxel : P.any_class) = true;
   build_sources(P, acq);
-  // per-slice rate rectangles and certified segmentations (`spiral_rects` kspace3d.rs:876-905)
+  // per-slice certified segmentations
   P.class_plan.resize(P.nz);
   P.voxel_plan.resize(P.nz);
   std::vector<double> tau(P.table.traj.tau_ms);
-  for (int z = 0; z < P.nz; ++z) {
-    double f[2] = {0.0, 0.0};
-    if (acq.do_distortions) {
-      float lo = INFINITY, hi = -INFINITY;
-      for (size_t i = 0; i < P.plane; ++i) {
-        lo = std::min(lo, in.fmap[(size_t)z * P.plane + i]);
-        hi = std::max(hi, in.fmap[(size_t)z * P.plane + i]);
-      }
-      f[0] = lo;
-      f[1] = hi;
-    }
-    bool has_d = false;
-    double d[2] = {0.0, 0.0};
-    for (int c = 0; c < P.ncomp; ++c) {
-      if (!P.modes[c].voxel) continue;
-      for (size_t i = (size_t)z * P.plane; i < (size_t)(z + 1) * P.plane; ++i) {
-        const double t2 = in.t2[c].is_map ? (double)in.t2[c].map[i] : (double)in.t2[c].value;
-        const double tp = in.t_inhom ? (in.t_inhom[c].is_map ? (double)in.t_inhom[c].map[i]
-                                                              : (double)in.t_inhom[c].value)
-                                     : acq.t_inhom;
-        const double r = 1.0 / t2 + 1.0 / tp;
-        if (!has_d) {
-          d[0] = d[1] = r;
-          has_d = true;
-        } else {
-          d[0] = std::min(d[0], r);
-          d[1] = std::max(d[1], r);
-        }
-      }
-    }
+  for (const SliceRect& r : spiral_rects(in, acq, P.modes, P.plane, P.nz)) {
     const double zero[2] = {0.0, 0.0};
-    if (P.any_class) P.class_plan[z] = tseg_plan(tau, P.table.traj.readout_ms, zero, f);
-    if (has_d) P.voxel_plan[z] = tseg_plan(tau, P.table.traj.readout_ms, d, f);
+    if (P.any_class) P.class_plan[r.z] = tseg_plan(tau, P.table.traj.readout_ms, zero, r.f);
+    if (r.has_d) P.voxel_plan[r.z] = tseg_plan(tau, P.table.traj.readout_ms, r.d, r.f);
   }
   // the centred z-DFT kernel, the ring z profiles, the object phase, the half-cell phase
   const double zs = (double)(P.nz / 2);

@@ -21,6 +21,14 @@ std::vector<uint8_t> kz_acquired(const mrsim_kz_sampling& kz, int nz);
 Spiral3dTable spiral_lines(const mrsim_echo_train& train, const mrsim_spiral_readout& ro, int nx, int ny, int nz);
 double coil_row_sensitivity(int row, int rows, double z, int nz);
 
+struct SpiralSegmentationRow {
+  int z, voxel, l, m;
+  double b_sum, bound;
+};
+std::vector<SpiralSegmentationRow> spiral_segmentation(const mrsim_acquisition_3d_input& in,
+                                                       const mrsim_acquisition& acq, const mrsim_echo_train& train,
+                                                       const mrsim_spiral_readout& ro);
+
 // `spiral_volumes` (kspace3d.rs:1472-1569) through the f32 magnitude / phase of
 // `simulate_acquisition_3d_kz`; host buffers.
 void spiral3d_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,

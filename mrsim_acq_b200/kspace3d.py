@@ -402,3 +402,44 @@ def simulate_acquisition_3d_ge(sim_dims, acq_dims, n_volumes: int, t2: Sequence[
         raise vols.error
     check(status)
     return list(zip(mags, phs))
+
+
+# ---- timing checks of the trains (readout.rs:286-288, 326-354, 460-500, 702-730) -------------------
+def esp_from_echo_time(te_ms: float, e_c: int, ro: GraseReadout, ny: int) -> float:
+    return float(lib().mrsim_esp_from_echo_time(te_ms, e_c, C.byref(ro.to_c()), ny))
+
+
+def spiral_esp_from_echo_time(te_ms: float, e_c: int) -> float:
+    return float(lib().mrsim_spiral_esp_from_echo_time(te_ms, e_c))
+
+
+def check_grase_timing(train: EchoTrain, ro: GraseReadout, ny: int, nz: int, t_exc_ms: float, tr_ms: float) -> None:
+    check(lib().mrsim_check_grase_timing(C.byref(train.to_c()), C.byref(ro.to_c()), ny, nz, t_exc_ms, tr_ms))
+
+
+def check_ge3d_timing(train: ExcitationTrain, ro: Ge3dReadout, ny: int, nz: int, t_exc_ms: float, tr_ms: float) -> None:
+    keep = _Keep()
+    check(lib().mrsim_check_ge3d_timing(C.byref(train.to_c(keep)), C.byref(ro.to_c()), ny, nz, t_exc_ms, tr_ms))
+
+
+def check_spiral_timing(train: EchoTrain, ro: SpiralReadout, nx: int, ny: int, nz: int, t_exc_ms: float,
+                        tr_ms: float) -> float:
+    end = C.c_double()
+    check(lib().mrsim_check_spiral_timing(C.byref(train.to_c()), C.byref(ro.to_c()), nx, ny, nz, t_exc_ms, tr_ms,
+                                          C.byref(end)))
+    return end.value
+
+
+def spiral_segmentation(sim_dims, acq_dims, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,
+                        t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain, readout: SpiralReadout):
+    """`spiral_segmentation` (kspace3d.rs:1441-1470): a list of dicts (z, voxel, l, m, b_sum, bound)."""
+    keep = _Keep()
+    s = acquisition_3d_input_c(sim_dims, acq_dims, 0, [np.zeros(1, np.float32)] * len(t2), t2, t1, fmap, t_inhom,
+                               None, None, None, keep)
+    n = C.c_int64()
+    check(lib().mrsim_spiral_segmentation(C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
+                                          C.byref(readout.to_c()), 0, None, C.byref(n)))
+    rows = (abi.SpiralSegmentationRow_ * max(1, n.value))()
+    check(lib().mrsim_spiral_segmentation(C.byref(s), C.byref(acq.to_c()), C.byref(train.to_c()),
+                                          C.byref(readout.to_c()), n.value, rows, C.byref(n)))
+    return [dict(z=r.z, voxel=bool(r.voxel), l=r.l, m=r.m, b_sum=r.b_sum, bound=r.bound) for r in rows[:n.value]]

@@ -105,6 +105,27 @@ def nufft_kernel_width(tol: float) -> int:
     return int(lib().mrsim_nufft_kernel_width(tol))
 
 
+class Nufft1:
+    """`Nufft1` (nufft.rs:25-112) on the device, FP64: period n, outputs at k_lo .. k_lo + n_out."""
+
+    def __init__(self, n: int, k_lo: int, n_out: int, tol: float, ctx: Optional[Context] = None):
+        self.n, self.k_lo, self.n_out, self.tol = int(n), int(k_lo), int(n_out), float(tol)
+        self.ctx = ctx or default_context()
+
+    def kernel_width(self) -> int:
+        return nufft_kernel_width(self.tol)
+
+    def run(self, pos: np.ndarray, weights: Sequence[np.ndarray]) -> np.ndarray:
+        """`run`: weights = complex vectors sharing `pos`; returns complex128 [len(weights), n_out]."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.complex128).reshape(-1, len(pos)))
+        out = np.zeros((len(w), self.n_out), np.complex128)
+        check(lib().mrsim_nufft1(self.ctx.handle, self.n, self.k_lo, self.n_out, self.tol,
+                                 pos.ctypes.data_as(abi.c_f64p), len(pos), w.view(np.float64).ctypes.data_as(abi.c_f64p),
+                                 len(w), out.view(np.float64).ctypes.data_as(abi.c_f64p)))
+        return out
+
+
 class Nufft2:
     """`Nufft2` (nufft.rs:125-299): periods n, modes m_lo .. m_lo + m_out per axis.  Modes are
     complex arrays [m_out1, m_out0] (layout (m0 - m_lo0) + m_out0 (m1 - m_lo1)); points u [npts, 2]."""

@@ -263,3 +263,40 @@ def test_segmented_refuses_several_compartments(gpu_ctx):
     with pytest.raises(MrsimError, match="one compartment"):
         S.spiral_segmented_forward(inp, Acquisition(), 0, 1, np.zeros((1, 2)), np.zeros(1, np.int64), np.zeros(1), 1.0,
                                    S.RateRect((0.0, 0.0), (0.0, 0.0)), ctx=gpu_ctx)
+
+
+# ---- the 1D type-1 NUFFT (`Nufft1`, the `kspace` y-stage's transform) -------------------------------
+def _direct1(n, k_lo, n_out, pos, w):
+    k = (k_lo + np.arange(n_out))[:, None]
+    return (np.exp(1j * TAU * k * pos[None, :] / n) * w[None, :]).sum(1)
+
+
+def test_nufft1_matches_the_direct_sum(gpu_ctx):
+    # nufft.rs `matches_the_direct_sum`: the reference's Rng(42) draws, two weight vectors, the
+    # FP64 bar 10 tol x total
+    rng = Rng(42)
+    for n, k_lo, n_out, tol in [(48, -12, 24, 1e-12), (140, -35, 70, 1e-12), (16, -8, 16, 1e-12), (64, -16, 32, 1e-8)]:
+        nsrc = 3 * n
+        pos = np.array([(rng.unit() - 0.5) * 3.0 * n for _ in range(nsrc)])
+        re = np.array([rng.unit() - 0.5 for _ in range(nsrc)])
+        im = np.array([rng.unit() - 0.5 for _ in range(nsrc)])
+        re2 = np.array([rng.unit() for _ in range(nsrc)])
+        w = [re + 1j * im, re2 + 0j]
+        got = S.Nufft1(n, k_lo, n_out, tol, ctx=gpu_ctx).run(pos, w)
+        for q in range(2):
+            want = _direct1(n, k_lo, n_out, pos, w[q])
+            total = np.abs(w[q]).sum()
+            assert np.abs(got[q] - want).max() <= 10.0 * tol * total, (n, q)
+
+
+def test_nufft1_integer_positions_reduce_to_the_dft(gpu_ctx):
+    n = 32
+    pos = np.arange(n, dtype=np.float64)
+    w = np.sin(pos * 0.3) + 0j
+    got = S.Nufft1(n, -16, 32, 1e-12, ctx=gpu_ctx).run(pos, [w])[0]
+    assert np.abs(got - _direct1(n, -16, 32, pos, w)).max() < 1e-10
+
+
+def test_nufft1_refuses_a_band_outside_nyquist(gpu_ctx):
+    with pytest.raises(MrsimError, match="coarse Nyquist band"):
+        S.Nufft1(16, -9, 16, 1e-12, ctx=gpu_ctx).run(np.zeros(3), [np.zeros(3, complex)])
