@@ -1,9 +1,11 @@
 /*
  * mrsim_acq.h — C ABI of the B200 k-space acquisition library (libmrsim_acq_cuda.so).
  *
- * The library is a drop-in for the 2D EPI k-space path of the Rust crate `mrsim-acq`
- * (per-slice exact-DFT forward, GRAPPA calibration and apply, window, inverse DFT, Roemer
- * combine, series driver).  Every entry point cites the reference item it replaces as
+ * The library is a drop-in for the k-space path of the Rust crate `mrsim-acq`: the 2D EPI
+ * per-slice exact-DFT forward and its adjoint, GRAPPA calibration and apply, window, inverse DFT,
+ * Roemer combine and series drivers; the 3D GRASE, gradient-echo and stack-of-spirals trains; and
+ * the spiral pieces (NUFFT pair, certified time segmentation, spiral forwards and
+ * reconstruction, trajectory and EPG).  Every entry point cites the reference item it replaces as
  * `file:line` within the reference crate.  A Rust shim behind a `gpu` cargo feature binds these
  * symbols one for one (see INTEGRATION.md for the `extern "C"` block).
  *
