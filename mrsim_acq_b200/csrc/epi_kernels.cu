@@ -51,6 +51,24 @@ __device__ __forceinline__ float ft_turns(float f, float t_hi, float t_lo) {
   return r + fmaf(f, t_lo, e);
 }
 
+// cp.async helpers (16-byte copies zero-fill the bytes past src_bytes)
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_n() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(gmem_src), "r"(src_bytes));
+}
+
 // ---------------------------------------------------------------------------------------------
 // statics: a(x,y) = frac( (phi0 + eddy object phase) / 2pi ) in FP64, stored as f32 turns.
 // phi0 = phase0[i] (explicit) or the phase model `PhaseModel::at` (phase.rs:141) sampled by
@@ -278,6 +296,238 @@ __global__ void __launch_bounds__(128, 4) ystage_kernel(const UnitDesc* __restri
 }
 
 // ---------------------------------------------------------------------------------------------
+// y-stage of the forward with the per-row inputs staged in shared memory (every unit of the plan
+// has snx % 4 == 0 and 16-byte aligned input planes).  Same sums as ystage_kernel:
+//   * a CTA of 256 threads covers 128 columns x 8 lines (two groups of 4 lines, one column each)
+//     x QG coils, so each row's inputs serve 8 lines;
+//   * the inputs of RC rows (static phase, fieldmap, compartments, and with voxel maps T2, T2',
+//     log amplitude) arrive through a 3-stage ring filled by cooperative 16-byte cp.async, one
+//     barrier per RC rows, in place of per-thread global loads one row ahead.
+constexpr int kFwdStages = 3;
+__host__ __device__ __forceinline__ constexpr int fwdq_planes(int nc, bool maps) { return maps ? 3 + 3 * nc : 2 + nc; }
+__host__ __device__ __forceinline__ constexpr int fwdq_rows(int nc, bool maps) {
+  return fwdq_planes(nc, maps) <= 5 ? 8 : fwdq_planes(nc, maps) <= 12 ? 4 : 2;
+}
+
+template <int QG, int NC, bool MAPS>
+__global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __restrict__ units,
+                                                          const Tile* __restrict__ tiles) {
+  constexpr int T = 4, TL = 8;
+  constexpr int NPL = fwdq_planes(NC, MAPS);
+  constexpr int RC = fwdq_rows(NC, MAPS);
+  constexpr int STAGE = NPL * RC * 128;        // floats per stage
+  constexpr int PIECES = NPL * RC * 32;        // 16-byte pieces per stage
+  constexpr int PPT = (PIECES + 255) / 256;
+  constexpr int QGP = (QG + 3) / 4 * 4;
+  // plane order: 0 static phase, 1 fieldmap, 2.. compartments, then T2, T2' maps and log amplitude
+  constexpr int P_COMP = 2, P_T2 = 2 + NC, P_TI = 2 + 2 * NC, P_LA = 2 + 3 * NC;
+  extern __shared__ __align__(16) float smem[];
+  float* ring = smem;                           // [stage][plane][RC][128]
+  float* Bt = ring + kFwdStages * STAGE;        // [sny][TL]
+  const Tile tl = tiles[blockIdx.x];
+  const UnitDesc& u = units[tl.unit];
+  const int snx = u.snx, sny = u.sny, ncomp = u.ncomp;
+  float* Ey = Bt + sny * TL;                    // [sny][QGP]
+  __shared__ const float* plane_s[NPL];
+  __shared__ float rel_s[TL][kMaxComp];
+  __shared__ float tinh_s[TL], trf_s[TL], thi_s[TL], tlo_s[TL];
+  const int tid = threadIdx.x;
+  const bool distort = (u.flags & UF_DISTORT) != 0;
+  if (tid < NPL) {
+    const float* pp = nullptr;
+    const int k = tid;
+    if (k == 0) pp = u.phase;
+    else if (k == 1) pp = distort ? u.fmap : nullptr;
+    else if (k < P_T2) pp = (k - P_COMP) < ncomp ? u.comp + (size_t)(k - P_COMP) * u.comp_stride : nullptr;
+    else if (k < P_TI) pp = ((k - P_T2) < ncomp && u.t2map) ? u.t2map + (size_t)(k - P_T2) * u.map_stride : nullptr;
+    else if (k < P_LA) pp = ((k - P_TI) < ncomp && u.timap) ? u.timap + (size_t)(k - P_TI) * u.map_stride : nullptr;
+    else pp = u.log_amp;
+    plane_s[k] = pp;
+  }
+  __syncthreads();
+  const int x0 = tl.x0;
+  const int nch = (sny + RC - 1) / RC;
+  auto issue_rows = [&](int c) {
+    if (c < nch) {
+      float* dst = ring + (c % kFwdStages) * STAGE;
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) {
+        const int k = tid + 256 * i;
+        if (PIECES % 256 == 0 || k < PIECES) {
+          const int pl = k / (RC * 32), rem = k % (RC * 32);
+          const int r = rem >> 5, c4 = (rem & 31) * 4;
+          const float* base = plane_s[pl];
+          const int y = c * RC + r, xx = x0 + c4;
+          if (base != nullptr) {
+            const bool ok = y < sny && xx < snx;
+            cp_async16(dst + (pl * RC + r) * 128 + c4, ok ? base + (size_t)y * snx + xx : base, ok ? 16 : 0);
+          }
+        }
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int c = 0; c < kFwdStages - 1; ++c) issue_rows(c);
+
+  const int nl = min(TL, u.n_lines - tl.line0);
+  const int ys = u.ny / 2;
+  const int oy = sny / u.ny;
+  const int sys = oy * ys;
+  for (int idx = tid; idx < sny * TL; idx += 256) {
+    const int y = idx / TL, j = idx % TL;
+    float v = 0.f;
+    if (j < nl) {
+      const LineRec& L = u.lines[tl.line0 + j];
+      const long long K = L.ky - ys;
+      const long long Y = 2LL * (y - sys) - (oy - 1);
+      const long long m2 = 2LL * sny;
+      double tv = (double)((K * Y) % m2) / (double)m2;
+      if (u.flags & UF_EDDY) {
+        const double yc = ((double)y - sys - (oy - 1) / 2.0) / oy;
+        tv += ((double)u.eddy_cy * yc + (double)u.eddy_qy * yc * yc) * (double)L.decay;
+      }
+      tv -= rint(tv);
+      v = (float)tv;
+    }
+    Bt[idx] = v;
+  }
+  for (int idx = tid; idx < QGP * sny; idx += 256) {
+    const int y = idx / QGP, qq = idx % QGP;
+    const int q = tl.q0 + qq;
+    Ey[idx] = (qq < QG && q < u.ncoils) ? u.geo.ey[(size_t)q * sny + y] : 0.f;
+  }
+  if (tid < TL) {
+    const int j = tid;
+    if (j < nl) {
+      const LineRec& L = u.lines[tl.line0 + j];
+      thi_s[j] = L.t_hi;
+      tlo_s[j] = L.t_lo;
+      tinh_s[j] = L.inhom_ms;
+      trf_s[j] = L.trf_ms;
+      for (int c = 0; c < kMaxComp; ++c) rel_s[j][c] = L.rel[c];
+    } else {
+      thi_s[j] = tlo_s[j] = tinh_s[j] = trf_s[j] = 0.f;
+      for (int c = 0; c < kMaxComp; ++c) rel_s[j][c] = 0.f;
+    }
+  }
+  __syncthreads();
+
+  const int col = tid & 127, lg = tid >> 7;
+  const int jb = lg * T;
+  const int x = x0 + col;
+  const bool xok = x < snx;
+  const float off = u.geo.coil_off;
+  float exq[QG];
+#pragma unroll
+  for (int qq = 0; qq < QG; ++qq) {
+    const int q = tl.q0 + qq;
+    exq[qq] = (xok && q < u.ncoils) ? u.geo.ex[(size_t)q * snx + x] : 0.f;
+  }
+  float thi[T], tlo[T], relr[T][MAPS ? 1 : NC], trf[MAPS ? T : 1], tinh[MAPS ? T : 1];
+#pragma unroll
+  for (int j = 0; j < T; ++j) {
+    thi[j] = thi_s[jb + j];
+    tlo[j] = tlo_s[jb + j];
+    if (MAPS) {
+      trf[MAPS ? j : 0] = trf_s[jb + j];
+      tinh[MAPS ? j : 0] = tinh_s[jb + j];
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) relr[j][MAPS ? 0 : c] = rel_s[jb + j][c];
+    }
+  }
+  const bool has_phase = plane_s[0] != nullptr, has_f = plane_s[1] != nullptr;
+  const bool has_t2 = MAPS && plane_s[P_T2] != nullptr, has_ti = MAPS && plane_s[P_TI] != nullptr;
+  const bool has_la = MAPS && plane_s[P_LA] != nullptr;
+  float2 acc[T][QG];
+#pragma unroll
+  for (int j = 0; j < T; ++j)
+#pragma unroll
+    for (int qq = 0; qq < QG; ++qq) acc[j][qq] = make_float2(0.f, 0.f);
+
+  for (int c = 0; c < nch; ++c) {
+    cp_async_wait_n<kFwdStages - 2>();
+    __syncthreads();  // rows of chunk c landed; every thread is done with chunk c - 1
+    issue_rows(c + kFwdStages - 1);
+    const float* S = ring + (c % kFwdStages) * STAGE + col;
+    const int rn = min(RC, sny - c * RC);
+    for (int r = 0; r < rn; ++r) {
+      const int y = c * RC + r;
+      const float a = has_phase ? S[(0 * RC + r) * 128] : 0.f;
+      const float f = has_f ? S[(1 * RC + r) * 128] : 0.f;
+      float m[NC];
+#pragma unroll
+      for (int cc = 0; cc < NC; ++cc) m[cc] = cc < ncomp ? S[((P_COMP + cc) * RC + r) * 128] : 0.f;
+      float r2[MAPS ? NC : 1], r2i[MAPS ? NC : 1];
+      float la = 0.f;
+      if (MAPS) {
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          r2[MAPS ? cc : 0] = r2i[MAPS ? cc : 0] = 0.f;
+          if (cc < ncomp) {
+            const float t2 = has_t2 ? S[((P_T2 + cc) * RC + r) * 128] : u.t2u[cc];
+            const float ti = has_ti ? S[((P_TI + cc) * RC + r) * 128] : u.tiu[cc];
+            r2[MAPS ? cc : 0] = 1.0f / t2;
+            r2i[MAPS ? cc : 0] = 1.0f / ti;
+          }
+        }
+        if (has_la) la = S[(P_LA * RC + r) * 128];
+      }
+      float amp[QG];
+#pragma unroll
+      for (int q4 = 0; q4 < QGP; q4 += 4) {
+        const float4 e4 = *reinterpret_cast<const float4*>(Ey + y * QGP + q4);
+        const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (q4 + k < QG) amp[q4 + k] = fmaf(exq[q4 + k], ev[k], off);
+      }
+      const float4 b4 = *reinterpret_cast<const float4*>(Bt + y * TL + jb);
+      const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+      for (int j = 0; j < T; ++j) {
+        float th = a + bt[j] + ft_turns(f, thi[j], tlo[j]);
+        th = frac_turn(th);
+        float sn, cs;
+        __sincosf(kTwoPiF * th, &sn, &cs);
+        float W = 0.f;
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          if (cc < ncomp) {
+            float rr;
+            if (MAPS)
+              rr = __expf(la - trf[MAPS ? j : 0] * r2[MAPS ? cc : 0] - tinh[MAPS ? j : 0] * r2i[MAPS ? cc : 0]);
+            else
+              rr = relr[j][MAPS ? 0 : cc];
+            W = fmaf(rr, m[cc], W);
+          }
+        }
+        const float wr = W * cs, wi = W * sn;
+#pragma unroll
+        for (int qq = 0; qq < QG; ++qq) {
+          acc[j][qq].x = fmaf(amp[qq], wr, acc[j][qq].x);
+          acc[j][qq].y = fmaf(amp[qq], wi, acc[j][qq].y);
+        }
+      }
+    }
+  }
+  cp_async_wait0();
+  if (!xok) return;
+  const float s = u.signal_scale;
+#pragma unroll
+  for (int qq = 0; qq < QG; ++qq) {
+    const int q = tl.q0 + qq;
+    if (q >= u.ncoils) break;
+#pragma unroll
+    for (int j = 0; j < T; ++j) {
+      if (jb + j < nl)
+        u.g[((size_t)q * u.n_lines + tl.line0 + jb + j) * snx + x] = make_float2(acc[j][qq].x * s, acc[j][qq].y * s);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
 // y-adjoint: per voxel, over every line j and coil q:
 //   H_j = s * sum_q (ex_q ey_q + off) h_q[j][x];   Z_j = conj(e^{i2pi theta_j}) H_j
 //   comp_grad_c = sum_j rel_cj Z_j                          (A^H r, complex)
@@ -285,14 +535,6 @@ __global__ void __launch_bounds__(128, 4) ystage_kernel(const UnitDesc* __restri
 //   r2_grad_c   = -2 m_c Re(sum_j trf_j rel_cj Z_j)         (dL/dR2_c)
 // A CTA of 128 threads covers 128 columns x TY rows (one column each).  The line table sits in
 // shared memory; h arrives by cp.async in double-buffered chunks of JC lines x every coil.
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
 // The number of lines per h chunk for `ncoils` coils (16 coil-lines per chunk, at least one line).
 __host__ __device__ __forceinline__ int adjoint_chunk_lines(int ncoils) { return ncoils >= 16 ? 1 : 16 / ncoils; }
 
@@ -479,6 +721,252 @@ __global__ void __launch_bounds__(128) yadjoint_kernel(const UnitDesc* __restric
 #pragma unroll
   for (int ty = 0; ty < TY; ++ty) {
     const int y = y0 + ty;
+    if (y >= sny) break;
+    const size_t i = (size_t)x + (size_t)snx * y;
+    float fg = 0.f;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (c >= ncomp) break;
+      u.comp_grad[c * plane + i] = cg[ty][c];
+      if (GRADS) {
+        const float m = __ldg(u.comp + (size_t)c * u.comp_stride + i);
+        fg = fmaf(m, Uy[ty][GRADS ? c : 0], fg);
+        if (u.r2_grad) u.r2_grad[c * plane + i] = -2.0f * m * Vx[ty][GRADS ? c : 0];
+      }
+    }
+    if (GRADS && u.fmap_grad) u.fmap_grad[i] = distort ? 4.0f * 3.14159265358979f * fg : 0.f;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// y-adjoint for a compile-time coil count NQ (every unit of the plan has NQ coils, an even snx and
+// 16-byte aligned h rows).  Same sums as yadjoint_kernel, reorganised so the per-(line, voxel)
+// work is the coil combination and the phase:
+//   * a CTA of 256 threads covers 128 columns x 2*TY rows (two groups of TY rows, one column each;
+//     TY = 4 with class decay, 2 with voxel maps, whose rates take the registers);
+//   * amp_q(x, y) = s * (ex_q(x) ey_q(y) + off) of the thread's TY rows sits in registers, so the
+//     coil combination is 2 FMAs per (coil, row) from one shared load of h per coil;
+//   * h arrives through a 3-stage ring of JC-line chunks (every coil, 128 columns) filled by
+//     cooperative 16-byte cp.async, one barrier per chunk;
+//   * the line table carries rel_cj, rel_cj * t_j and rel_cj * trf_j (class decay), so every
+//     accumulator update is one FMA.
+constexpr int kAdjStages = 3;
+__host__ __device__ __forceinline__ constexpr int adjq_chunk_lines(int nq) { return nq >= 16 ? 1 : 16 / nq; }
+__host__ __device__ __forceinline__ constexpr int adjq_line_floats(int nc, bool maps) {
+  return ((maps ? 5 : 4 + 3 * nc) + 3) / 4 * 4;
+}
+// rows per thread: 4 with class decay and up to 3 compartments, else 2 (registers)
+__host__ __device__ __forceinline__ constexpr int adjq_rows(int nc, bool maps) { return !maps && nc <= 3 ? 4 : 2; }
+
+
+template <int NQ, int TY, int NC, bool MAPS, bool GRADS>
+__global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __restrict__ units,
+                                                            const int4* __restrict__ tiles) {
+  extern __shared__ __align__(16) float smem[];
+  static_assert(TY == 2 || TY == 4, "the row phases are read as one float2 / float4");
+  constexpr int ROWS = 2 * TY;
+  constexpr int JC = adjq_chunk_lines(NQ);
+  constexpr int LF = adjq_line_floats(NC, MAPS);
+  constexpr int STAGE = JC * NQ * 128;        // float2 per stage
+  constexpr int PIECES = JC * NQ * 64;        // 16-byte pieces per stage
+  constexpr int PPT = (PIECES + 255) / 256;   // pieces per thread
+  const int4 tl = tiles[blockIdx.x];          // unit, y0, x0
+  const UnitDesc& u = units[tl.x];
+  const int snx = u.snx, sny = u.sny, ncomp = u.ncomp, nlines = u.n_lines;
+  const int y0 = tl.y, x0 = tl.z;
+  float2* hbuf = reinterpret_cast<float2*>(smem);
+  float* Bt = reinterpret_cast<float*>(hbuf + kAdjStages * STAGE);  // [nlines][ROWS]
+  float* Lt = Bt + nlines * ROWS;                                    // [nlines][LF]
+  const int tid = threadIdx.x;
+  const int col = tid & 127, rg = tid >> 7;
+  const int x = x0 + col;
+  const bool xok = x < snx;
+  const int nchunks = (nlines + JC - 1) / JC;
+
+  // this thread's 16-byte pieces of a chunk: (line jj, coil q, column pair p)
+  const float2* __restrict__ gsrc = u.g;
+  const size_t qstride = (size_t)nlines * snx;
+  auto issue_chunk = [&](int c) {
+    if (c < nchunks) {
+      const int j0 = c * JC;
+      float2* dst = hbuf + (c % kAdjStages) * STAGE;
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) {
+        const int k = tid + 256 * i;
+        if (PIECES % 256 == 0 || k < PIECES) {
+          const int r = k >> 6, pcol = (k & 63) * 2;
+          const int jj = r / NQ, q = r % NQ;
+          const int j = j0 + jj, xx = x0 + pcol;
+          const bool ok = j < nlines && xx < snx;
+          const float2* src = ok ? gsrc + q * qstride + (size_t)j * snx + xx : gsrc;
+          cp_async16(dst + r * 128 + pcol, src, ok ? 16 : 0);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int c = 0; c < kAdjStages - 1; ++c) issue_chunk(c);
+
+  const int ys = u.ny / 2;
+  const int oy = sny / u.ny;
+  const int sys = oy * ys;
+  for (int idx = tid; idx < nlines * ROWS; idx += 256) {
+    const int j = idx / ROWS, r = idx % ROWS;
+    const int y = y0 + r;
+    float v = 0.f;
+    if (y < sny) {
+      const LineRec& L = u.lines[j];
+      const long long K = L.ky - ys;
+      const long long Y = 2LL * (y - sys) - (oy - 1);
+      const long long m2 = 2LL * sny;
+      double tv = (double)((K * Y) % m2) / (double)m2;
+      if (u.flags & UF_EDDY) {
+        const double yc = ((double)y - sys - (oy - 1) / 2.0) / oy;
+        tv += ((double)u.eddy_cy * yc + (double)u.eddy_qy * yc * yc) * (double)L.decay;
+      }
+      tv -= rint(tv);
+      v = (float)tv;
+    }
+    Bt[idx] = v;
+  }
+  for (int j = tid; j < nlines; j += 256) {
+    const LineRec& L = u.lines[j];
+    float* e = Lt + j * LF;
+    const float tph = L.t_hi + L.t_lo;
+    e[0] = L.t_hi;
+    e[1] = L.t_lo;
+    e[2] = L.trf_ms;
+    e[3] = L.inhom_ms;
+    if (MAPS) {
+      e[4] = tph;
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        e[4 + c] = L.rel[c];
+        e[4 + NC + c] = L.rel[c] * tph;
+        e[4 + 2 * NC + c] = L.rel[c] * L.trf_ms;
+      }
+    }
+  }
+
+  // per-thread constants of its 4 rows
+  const bool distort = (u.flags & UF_DISTORT) != 0;
+  const int xs_ = xok ? x : 0;
+  const float s = u.signal_scale, off = u.geo.coil_off;
+  float amp[TY][NQ];
+  float a[TY], f[TY];
+  float r2[TY][MAPS ? NC : 1], r2i[TY][MAPS ? NC : 1], la[TY];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const float ex = u.geo.ex[(size_t)q * snx + xs_];
+#pragma unroll
+    for (int ty = 0; ty < TY; ++ty) {
+      const int y = min(y0 + rg * TY + ty, sny - 1);
+      amp[ty][q] = s * fmaf(ex, u.geo.ey[(size_t)q * sny + y], off);
+    }
+  }
+#pragma unroll
+  for (int ty = 0; ty < TY; ++ty) {
+    const int y = min(y0 + rg * TY + ty, sny - 1);
+    const int i = xs_ + snx * y;
+    a[ty] = u.phase ? __ldg(u.phase + i) : 0.f;
+    f[ty] = distort ? __ldg(u.fmap + i) : 0.f;
+    la[ty] = (MAPS && u.log_amp) ? __ldg(u.log_amp + i) : 0.f;
+    if (MAPS) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        r2[ty][MAPS ? c : 0] = r2i[ty][MAPS ? c : 0] = 0.f;
+        if (c < ncomp) {
+          const float t2 = u.t2map ? __ldg(u.t2map + (size_t)c * u.map_stride + i) : u.t2u[c];
+          const float ti = u.timap ? __ldg(u.timap + (size_t)c * u.map_stride + i) : u.tiu[c];
+          r2[ty][MAPS ? c : 0] = 1.0f / t2;
+          r2i[ty][MAPS ? c : 0] = 1.0f / ti;
+        }
+      }
+    }
+  }
+  float2 cg[TY][NC];
+  float Uy[TY][GRADS ? NC : 1], Vx[TY][GRADS ? NC : 1];
+#pragma unroll
+  for (int ty = 0; ty < TY; ++ty)
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      cg[ty][c] = make_float2(0.f, 0.f);
+      if (GRADS) Uy[ty][GRADS ? c : 0] = Vx[ty][GRADS ? c : 0] = 0.f;
+    }
+
+  for (int c = 0; c < nchunks; ++c) {
+    cp_async_wait_n<kAdjStages - 2>();
+    __syncthreads();  // chunk c landed for every thread; every thread is done with chunk c - 1
+    issue_chunk(c + kAdjStages - 1);
+    const float2* hs = hbuf + (c % kAdjStages) * STAGE + col;
+    const int j0 = c * JC;
+    const int jn = min(JC, nlines - j0);
+    for (int jj = 0; jj < jn; ++jj) {
+      const int j = j0 + jj;
+      const float* e = Lt + j * LF;
+      const float4 e0 = *reinterpret_cast<const float4*>(e);
+      const float thi = e0.x, tlo = e0.y, trf = e0.z, tinh = e0.w;
+      float2 H[TY];
+#pragma unroll
+      for (int ty = 0; ty < TY; ++ty) H[ty] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const float2 h = hs[(jj * NQ + q) * 128];
+#pragma unroll
+        for (int ty = 0; ty < TY; ++ty) {
+          H[ty].x = fmaf(amp[ty][q], h.x, H[ty].x);
+          H[ty].y = fmaf(amp[ty][q], h.y, H[ty].y);
+        }
+      }
+      float bt[TY];
+      if (TY == 4) {
+        const float4 b4 = *reinterpret_cast<const float4*>(Bt + j * ROWS + rg * TY);
+        bt[0] = b4.x, bt[1] = b4.y, bt[TY > 2 ? 2 : 0] = b4.z, bt[TY > 3 ? 3 : 0] = b4.w;
+      } else {
+        const float2 b2 = *reinterpret_cast<const float2*>(Bt + j * ROWS + rg * TY);
+        bt[0] = b2.x, bt[1] = b2.y;
+      }
+      const float tph = MAPS ? e[4] : 0.f;
+#pragma unroll
+      for (int ty = 0; ty < TY; ++ty) {
+        float th = a[ty] + bt[ty] + ft_turns(f[ty], thi, tlo);
+        th = frac_turn(th);
+        float sn, cs;
+        __sincosf(kTwoPiF * th, &sn, &cs);
+        const float zr = fmaf(cs, H[ty].x, sn * H[ty].y);  // Z = conj(P) * H
+        const float zi = fmaf(cs, H[ty].y, -sn * H[ty].x);
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          if (cc < ncomp) {
+            float r, rt, rf;
+            if (MAPS) {
+              r = __expf(la[ty] - trf * r2[ty][MAPS ? cc : 0] - tinh * r2i[ty][MAPS ? cc : 0]);
+              rt = r * tph;
+              rf = r * trf;
+            } else {
+              r = e[4 + cc];
+              rt = e[4 + NC + cc];
+              rf = e[4 + 2 * NC + cc];
+            }
+            cg[ty][cc].x = fmaf(r, zr, cg[ty][cc].x);
+            cg[ty][cc].y = fmaf(r, zi, cg[ty][cc].y);
+            if (GRADS) {
+              Uy[ty][GRADS ? cc : 0] = fmaf(rt, zi, Uy[ty][GRADS ? cc : 0]);
+              Vx[ty][GRADS ? cc : 0] = fmaf(rf, zr, Vx[ty][GRADS ? cc : 0]);
+            }
+          }
+        }
+      }
+    }
+  }
+  cp_async_wait0();
+  if (!xok) return;
+  const size_t plane = (size_t)snx * sny;
+#pragma unroll
+  for (int ty = 0; ty < TY; ++ty) {
+    const int y = y0 + rg * TY + ty;
     if (y >= sny) break;
     const size_t i = (size_t)x + (size_t)snx * y;
     float fg = 0.f;
@@ -695,11 +1183,29 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
     for (int i = 0; i < n; ++i) max_comp = std::max(max_comp, hu[i].ncomp);
     p->nc = max_comp <= 1 ? 1 : max_comp <= 2 ? 2 : max_comp <= 3 ? 3 : max_comp <= 4 ? 4 : 8;
     p->qg = max_coils <= 1 ? 1 : max_coils <= 2 ? 2 : max_coils <= 4 ? 4 : 8;
+    // the staged-input forward serves a pass when every unit has snx % 4 == 0 and 16-byte aligned
+    // input planes (cooperative 16-byte copies)
+    auto al16 = [](const void* q) { return ((uintptr_t)q & 15) == 0; };
+    for (int pass = 0; pass < 2; ++pass) {
+      bool ok = true;
+      for (int i = 0; i < n; ++i) {
+        const UnitDesc& u = hu[i];
+        if (((u.flags & UF_MAPS) != 0) != (pass == 1)) continue;
+        ok = ok && (u.snx % 4) == 0 && al16(u.phase) && al16(u.fmap) && al16(u.comp) && al16(u.t2map) &&
+             al16(u.timap) && al16(u.log_amp) && (u.ncomp <= 1 || u.comp_stride % 4 == 0) &&
+             (u.ncomp <= 1 || (u.map_stride % 4) == 0);
+      }
+      // eight coils with voxel maps (two or more compartments) or eight compartments take more
+      // registers than the 256-thread CTA leaves: those shapes keep the per-thread-load kernel
+      if (p->qg == 8 && (p->nc == 8 || (pass == 1 && p->nc >= 2))) ok = false;
+      p->fwdq[pass] = ok;
+    }
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<int4> tiles;
+      const int step = p->fwdq[pass] ? 8 : kT;
       for (int i = 0; i < n; ++i) {
         if (((hu[i].flags & UF_MAPS) != 0) != (pass == 1)) continue;
-        for (int l = 0; l < hu[i].n_lines; l += kT)
+        for (int l = 0; l < hu[i].n_lines; l += step)
           for (int x0 = 0; x0 < hu[i].snx; x0 += 128)
             for (int q0 = 0; q0 < hu[i].ncoils; q0 += p->qg) tiles.push_back(make_int4(i, l, x0, q0));
       }
@@ -724,14 +1230,22 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->n_gtiles[dir] = (int)xt.size();
       p->d_gtiles[dir] = dev_upload(p, xt.data(), sizeof(XTile) * xt.size());
     }
+    // the fixed-coil-count y-adjoint serves a pass when every unit has the same coil count (1, 2,
+    // 4 or 8), an even snx and 16-byte aligned h rows (cooperative 16-byte copies)
+    int nq_all = n > 0 ? hu[0].ncoils : 0;
+    for (int i = 0; i < n; ++i)
+      if (hu[i].ncoils != nq_all || (hu[i].snx & 1) || ((uintptr_t)hu[i].g & 15)) nq_all = 0;
+    if (nq_all != 1 && nq_all != 2 && nq_all != 4 && nq_all != 8) nq_all = 0;
     for (int pass = 0; pass < 4; ++pass) {
       bool maps = pass & 1, grads = pass & 2;
+      p->adjq[pass] = (maps && p->nc == 8) ? 0 : nq_all;
+      const int step = p->adjq[pass] ? 2 * adjq_rows(p->nc, maps) : kTY;
       std::vector<int4> yt;
       for (int i = 0; i < n; ++i) {
         bool um = (hu[i].flags & UF_MAPS) != 0;
         bool ug = (hu[i].flags & (UF_WANT_FMAP_GRAD | UF_WANT_R2_GRAD)) != 0;
         if (um != maps || ug != grads) continue;
-        for (int y0 = 0; y0 < hu[i].sny; y0 += kTY)
+        for (int y0 = 0; y0 < hu[i].sny; y0 += step)
           for (int x0 = 0; x0 < hu[i].snx; x0 += 128) yt.push_back(make_int4(i, y0, x0, 0));
       }
       p->n_atiles[pass] = (int)yt.size();
@@ -766,6 +1280,27 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
     if (p->n_ytiles[pass] == 0) continue;
     const bool maps = pass == 1;
     const int QG = p->qg, NCv = p->nc;
+    if (p->fwdq[pass]) {
+      const size_t smq = sizeof(float) * ((size_t)kFwdStages * fwdq_planes(NCv, maps) * fwdq_rows(NCv, maps) * 128 +
+                                          (size_t)p->max_sny * (8 + (QG + 3) / 4 * 4));
+      bool launched = false;
+#define MRSIM_YF(QGV, NCV, M)                                                           \
+  if (QG == QGV && NCv == NCV && maps == M) {                                           \
+    auto k = ystage_q_kernel<QGV, NCV, M>;                                              \
+    set_smem(k, smq);                                                                   \
+    k<<<(unsigned)p->n_ytiles[pass], 256, smq, st>>>(p->d_units, (const Tile*)p->d_ytiles[pass]); \
+    launched = true;                                                                    \
+  }
+#define MRSIM_YFQ(NCV, M) MRSIM_YF(1, NCV, M) MRSIM_YF(2, NCV, M) MRSIM_YF(4, NCV, M) MRSIM_YF(8, NCV, M)
+#define MRSIM_YFN(M) MRSIM_YFQ(1, M) MRSIM_YFQ(2, M) MRSIM_YFQ(3, M) MRSIM_YFQ(4, M) MRSIM_YFQ(8, M)
+      MRSIM_YFN(false) MRSIM_YFN(true)
+#undef MRSIM_YFN
+#undef MRSIM_YFQ
+#undef MRSIM_YF
+      if (!launched) fail("no forward kernel instance for this unit shape");
+      MRSIM_CUDA(cudaGetLastError());
+      continue;
+    }
     const size_t sm = sizeof(float) * (size_t)p->max_sny * (kT + (QG + 3) / 4 * 4);
     bool launched = false;
 #define MRSIM_Y(QGV, NCV, M)                                                            \
@@ -805,6 +1340,29 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st) {
     if (p->n_atiles[pass] == 0) continue;
     const bool maps = pass & 1, grads = (pass & 2) != 0;
     const int NCv = p->nc;
+    if (p->adjq[pass]) {
+      const int NQv = p->adjq[pass];
+      const size_t smq = sizeof(float2) * (size_t)kAdjStages * adjq_chunk_lines(NQv) * NQv * 128 +
+                         sizeof(float) * (size_t)p->max_lines * (2 * adjq_rows(NCv, maps) + adjq_line_floats(NCv, maps));
+      bool launched = false;
+#define MRSIM_AQ(NQV, NCV, M, G)                                                        \
+  if (NQv == NQV && NCv == NCV && maps == M && grads == G) {                            \
+    auto k = yadjoint_q_kernel<NQV, adjq_rows(NCV, M), NCV, M, G>;                      \
+    set_smem(k, smq);                                                                   \
+    k<<<(unsigned)p->n_atiles[pass], 256, smq, st>>>(p->d_units, p->d_atiles[pass]);    \
+    launched = true;                                                                    \
+  }
+#define MRSIM_AQC(NCV, M, G) MRSIM_AQ(1, NCV, M, G) MRSIM_AQ(2, NCV, M, G) MRSIM_AQ(4, NCV, M, G) MRSIM_AQ(8, NCV, M, G)
+#define MRSIM_AQN(M, G) MRSIM_AQC(1, M, G) MRSIM_AQC(2, M, G) MRSIM_AQC(3, M, G) MRSIM_AQC(4, M, G)
+      MRSIM_AQN(false, false) MRSIM_AQN(true, false) MRSIM_AQN(false, true) MRSIM_AQN(true, true)
+      MRSIM_AQC(8, false, false) MRSIM_AQC(8, false, true)
+#undef MRSIM_AQN
+#undef MRSIM_AQC
+#undef MRSIM_AQ
+      if (!launched) fail("no adjoint kernel instance for this unit shape");
+      MRSIM_CUDA(cudaGetLastError());
+      continue;
+    }
     size_t sm = sizeof(float2) * (size_t)2 * p->max_hchunk * 128 +
                 sizeof(float) * ((size_t)kTY * (p->max_lines + p->max_coils) + 128 * (size_t)p->max_coils +
                                  (size_t)p->max_lines * (5 + NCv));

@@ -146,6 +146,11 @@ struct EpiPlan {
   int n_gtiles[2] = {0, 0};
   int4* d_atiles[4] = {nullptr, nullptr, nullptr, nullptr};
   int n_atiles[4] = {0, 0, 0, 0};
+  // forward y-stage pass (maps) served by the staged-input kernel (8 lines per tile)
+  bool fwdq[2] = {false, false};
+  // y-adjoint pass (maps | grads << 1) served by the fixed-coil-count kernel: its coil count, or 0
+  // for the general kernel
+  int adjq[4] = {0, 0, 0, 0};
   std::vector<void*> allocs;
   ~EpiPlan();
 };
