@@ -104,6 +104,32 @@ GeoTab build_geo(DevArena& arena, int snx, int sny, int nx, int ny, int ncoils, 
     }
   }
   GeoTab g;
+  g.xf = nullptr;
+  if (snx >= 8 && snx <= kXfftMaxN && (snx & (snx - 1)) == 0) {
+    // the factored x-stage: tw[x][kx] = premod_pol(x) * e^{i2pi (kx-xs) x/snx} * post(kx)
+    std::vector<float2> xf((size_t)snx / 2 + 2 * (size_t)snx + nx);
+    for (int k = 0; k < snx / 2; ++k) {
+      const double ph = -kTau * (double)k / (double)snx;
+      xf[k] = make_float2((float)std::cos(ph), (float)std::sin(ph));
+    }
+    for (int pol = 0; pol < 2; ++pol) {
+      const double gh = pol == 0 ? ghost : -ghost;
+      for (int x = 0; x < snx; ++x) {
+        double turns = gh * ((double)x - c) / (double)snx;
+        turns -= std::rint(turns);
+        xf[(size_t)snx / 2 + (size_t)pol * snx + x] =
+            make_float2((float)std::cos(kTau * turns), (float)std::sin(kTau * turns));
+      }
+    }
+    const long long c2 = 2LL * sxs + (ox - 1);  // 2c, an integer
+    for (int kx = 0; kx < nx; ++kx) {
+      const long long K = kx - xs;
+      double turns = -(double)((K * c2) % m2) / (double)m2;
+      turns -= std::rint(turns);
+      xf[(size_t)snx / 2 + 2 * (size_t)snx + kx] = make_float2((float)std::cos(kTau * turns), (float)std::sin(kTau * turns));
+    }
+    g.xf = (const float2*)arena.upload(xf.data(), xf.size() * sizeof(float2), st);
+  }
   g.ex = (const float*)arena.upload(ex.data(), ex.size() * 4, st);
   g.ey = (const float*)arena.upload(ey.data(), ey.size() * 4, st);
   g.tw = (const float2*)arena.upload(tw.data(), tw.size() * sizeof(float2), st);

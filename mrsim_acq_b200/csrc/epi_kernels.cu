@@ -51,6 +51,10 @@ __device__ __forceinline__ float ft_turns(float f, float t_hi, float t_lo) {
   return r + fmaf(f, t_lo, e);
 }
 
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
 // cp.async helpers (16-byte copies zero-fill the bytes past src_bytes)
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -405,7 +409,7 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
       tlo_s[j] = L.t_lo;
       tinh_s[j] = L.inhom_ms;
       trf_s[j] = L.trf_ms;
-      for (int c = 0; c < kMaxComp; ++c) rel_s[j][c] = L.rel[c];
+      for (int c = 0; c < kMaxComp; ++c) rel_s[j][c] = c < ncomp ? L.rel[c] : 0.f;
     } else {
       thi_s[j] = tlo_s[j] = tinh_s[j] = trf_s[j] = 0.f;
       for (int c = 0; c < kMaxComp; ++c) rel_s[j][c] = 0.f;
@@ -494,7 +498,7 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
         float W = 0.f;
 #pragma unroll
         for (int cc = 0; cc < NC; ++cc) {
-          if (cc < ncomp) {
+          if (!MAPS || cc < ncomp) {  // class decay: rel and m are 0 past ncomp
             float rr;
             if (MAPS)
               rr = __expf(la - trf[MAPS ? j : 0] * r2[MAPS ? cc : 0] - tinh[MAPS ? j : 0] * r2i[MAPS ? cc : 0]);
@@ -842,10 +846,11 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
       e[4] = tph;
     } else {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        e[4 + c] = L.rel[c];
-        e[4 + NC + c] = L.rel[c] * tph;
-        e[4 + 2 * NC + c] = L.rel[c] * L.trf_ms;
+      for (int c = 0; c < NC; ++c) {  // zero weights past ncomp: those accumulators stay 0
+        const float r = c < ncomp ? L.rel[c] : 0.f;
+        e[4 + c] = r;
+        e[4 + NC + c] = r * tph;
+        e[4 + 2 * NC + c] = r * L.trf_ms;
       }
     }
   }
@@ -939,7 +944,7 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
         const float zi = fmaf(cs, H[ty].y, -sn * H[ty].x);
 #pragma unroll
         for (int cc = 0; cc < NC; ++cc) {
-          if (cc < ncomp) {
+          if (!MAPS || cc < ncomp) {
             float r, rt, rf;
             if (MAPS) {
               r = __expf(la[ty] - trf * r2[ty][MAPS ? cc : 0] - tinh * r2i[ty][MAPS ? cc : 0]);
@@ -1105,6 +1110,109 @@ __global__ void __launch_bounds__(256) xgemm_kernel(const UnitDesc* __restrict__
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// x-stage as per-row FFTs when snx = N is a power of two.  The twiddle of the line's polarity
+// factors as tw[x][kx] = premod(x) e^{i2pi K x/N} post(kx), K = kx - xs, since
+// (K + gh)(x - c) = K x + gh (x - c) - K c, so
+//   forward : out[q][row_j][kx] = (1/nvox) post(kx) FFT+[ g[q][j][x] E_j(x) premod(x) ](K mod N)
+//   adjoint : h[q][j][x]        = (1/nvox) conj(E_j(x) premod(x)) FFT-[ r[q][row_j][kx] conj(post(kx)) at K mod N ](x)
+// (FFT+- : sum e^{+-i2pi k x/N}).  A CTA of 256 threads transforms up to 2048/N rows of one unit
+// ([coil][line] order) in shared memory: radix-2 decimation in time from bit-reversed loads.
+// Tile = (unit, first row, rows).
+template <bool ADJ>
+__global__ void __launch_bounds__(256) xfft_kernel(const UnitDesc* __restrict__ units, const int4* __restrict__ tiles) {
+  __shared__ __align__(16) float2 buf[kXfftMaxN];
+  __shared__ __align__(16) float2 tws[kXfftMaxN / 2];
+  __shared__ int rq[256], rline[256], rrow[256], rpol[256];
+  __shared__ float rdec[256];
+  const int4 t = tiles[blockIdx.x];
+  const UnitDesc& u = units[t.x];
+  const int r0 = t.y, nr = t.z;
+  const int N = u.snx, nx = u.nx, nl = u.n_lines;
+  const int logn = 31 - __clz(N), half = N >> 1;
+  const int tid = threadIdx.x;
+  const float2* __restrict__ xf = u.geo.xf;
+  const float2* __restrict__ premod = xf + half;
+  const float2* __restrict__ post = xf + half + 2 * N;
+  for (int k = tid; k < half; k += 256) tws[k] = xf[k];
+  for (int r = tid; r < nr; r += 256) {
+    const int R = r0 + r, q = R / nl, j = R % nl;
+    const LineRec& L = u.lines[j];
+    rq[r] = q;
+    rline[r] = j;
+    rrow[r] = L.row;
+    rpol[r] = L.pol < 0 ? 1 : 0;
+    rdec[r] = L.decay;
+  }
+  __syncthreads();
+  const int ox = N / nx, xs = nx / 2, sxs = ox * xs;
+  const double xoff = (ox - 1.0) / 2.0;
+  const bool eddy = (u.flags & UF_EDDY) != 0;
+  // E_j(x) = e^{i2pi (cx xc + qx xc^2 + z) decay_j}: the x and z parts of the eddy polynomial
+  auto eddy_factor = [&](int x, float dec) {
+    const double xc = ((double)x - sxs - xoff) / ox;
+    double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)dec;
+    tv -= rint(tv);
+    float sn, cs;
+    __sincosf(kTwoPiF * (float)tv, &sn, &cs);
+    return make_float2(cs, sn);
+  };
+  const float inv_n = 1.0f / (float)(N * u.sny);
+  const int kpos = nx - xs;  // K in [-xs, kpos)
+  if (!ADJ) {
+    for (int e = tid; e < nr * N; e += 256) {
+      const int r = e >> logn, x = e & (N - 1);
+      const float2 v = u.g[(size_t)(r0 + r) * N + x];
+      float2 m = premod[rpol[r] * N + x];
+      if (eddy) m = cmul(m, eddy_factor(x, rdec[r]));
+      buf[(r << logn) + (__brev(x) >> (32 - logn))] = cmul(v, m);
+    }
+  } else {
+    for (int e = tid; e < nr * N; e += 256) {
+      const int r = e >> logn, k = e & (N - 1);
+      const int K = k < kpos ? k : k - N;
+      const int kx = K + xs;
+      float2 v = make_float2(0.f, 0.f);
+      if (kx >= 0 && kx < nx) {
+        const float2 p = post[kx];
+        v = cmul(u.kspace[((size_t)rq[r] * u.n_rows + rrow[r]) * nx + kx], make_float2(p.x, -p.y));
+      }
+      buf[(r << logn) + (__brev(k) >> (32 - logn))] = v;
+    }
+  }
+  __syncthreads();
+  for (int s = 1; s <= logn; ++s) {
+    const int h = 1 << (s - 1);
+    for (int b = tid; b < nr * half; b += 256) {
+      const int r = b >> (logn - 1), bb = b & (half - 1);
+      const int pos = bb & (h - 1), grp = bb >> (s - 1);
+      const int i0 = (r << logn) + (grp << s) + pos, i1 = i0 + h;
+      float2 w = tws[pos << (logn - s)];  // e^{-i2pi pos / 2h}
+      if (!ADJ) w.y = -w.y;
+      const float2 a = buf[i0], bw = cmul(buf[i1], w);
+      buf[i0] = make_float2(a.x + bw.x, a.y + bw.y);
+      buf[i1] = make_float2(a.x - bw.x, a.y - bw.y);
+    }
+    __syncthreads();
+  }
+  if (!ADJ) {
+    for (int e = tid; e < nr * nx; e += 256) {
+      const int r = e / nx, kx = e % nx;
+      const int k = (kx - xs) & (N - 1);
+      const float2 v = cmul(buf[(r << logn) + k], post[kx]);
+      u.kspace[((size_t)rq[r] * u.n_rows + rrow[r]) * nx + kx] = make_float2(v.x * inv_n, v.y * inv_n);
+    }
+  } else {
+    for (int e = tid; e < nr * N; e += 256) {
+      const int r = e >> logn, x = e & (N - 1);
+      float2 m = premod[rpol[r] * N + x];
+      if (eddy) m = cmul(m, eddy_factor(x, rdec[r]));
+      const float2 v = cmul(buf[e], make_float2(m.x, -m.y));
+      u.g[(size_t)(r0 + r) * N + x] = make_float2(v.x * inv_n, v.y * inv_n);
+    }
+  }
+}
+
 template <class K>
 void set_smem(K kernel, size_t bytes) {
   if (bytes > 48 * 1024) MRSIM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -1212,9 +1320,25 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->n_ytiles[pass] = (int)tiles.size();
       p->d_ytiles[pass] = (int4*)dev_upload(p, tiles.data(), sizeof(int4) * tiles.size());
     }
+    // x-stage as per-row FFTs when every unit has a power-of-two snx with FFT tables
+    p->xfft = n > 0;
+    for (int i = 0; i < n; ++i) {
+      const int N = hu[i].snx;
+      if (hu[i].geo.xf == nullptr || N < 8 || N > kXfftMaxN || (N & (N - 1)) != 0 || hu[i].nx > N) p->xfft = false;
+    }
+    if (p->xfft) {
+      std::vector<int4> ft;
+      for (int i = 0; i < n; ++i) {
+        const int rows = hu[i].ncoils * hu[i].n_lines;
+        const int per = std::min(256, kXfftMaxN / hu[i].snx);
+        for (int r0 = 0; r0 < rows; r0 += per) ft.push_back(make_int4(i, r0, std::min(per, rows - r0), 0));
+      }
+      p->n_ftiles = (int)ft.size();
+      p->d_ftiles = (int4*)dev_upload(p, ft.data(), sizeof(int4) * ft.size());
+    }
     // x-stage GEMM tiles, from host copies of the line tables (one copy per distinct table)
     std::map<const LineRec*, std::vector<LineRec>> host_lines;
-    for (int dir = 0; dir < 2; ++dir) {
+    for (int dir = 0; dir < 2 && !p->xfft; ++dir) {
       std::vector<XTile> xt;
       for (int i = 0; i < n; ++i) {
         const int nl = hu[i].n_lines;
@@ -1322,6 +1446,13 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
 }
 
 void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st) {
+  if (p->xfft) {
+    if (p->n_ftiles) {
+      xfft_kernel<false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
+      MRSIM_CUDA(cudaGetLastError());
+    }
+    return;
+  }
   if (p->n_gtiles[0]) {
     xgemm_kernel<false><<<(unsigned)p->n_gtiles[0], 256, 0, st>>>(p->d_units, (const XTile*)p->d_gtiles[0]);
     MRSIM_CUDA(cudaGetLastError());
@@ -1329,6 +1460,13 @@ void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st) {
 }
 
 void epi_plan_adjoint_xstage(const EpiPlan* p, cudaStream_t st) {
+  if (p->xfft) {
+    if (p->n_ftiles) {
+      xfft_kernel<true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
+      MRSIM_CUDA(cudaGetLastError());
+    }
+    return;
+  }
   if (p->n_gtiles[1]) {
     xgemm_kernel<true><<<(unsigned)p->n_gtiles[1], 256, 0, st>>>(p->d_units, (const XTile*)p->d_gtiles[1]);
     MRSIM_CUDA(cudaGetLastError());

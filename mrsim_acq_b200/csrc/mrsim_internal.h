@@ -15,6 +15,7 @@ namespace mrsim {
 
 constexpr int kMaxComp = 8;   // compartments per unit handled by the kernels
 constexpr int kMaxCoils = 64; // coils per series
+constexpr int kXfftMaxN = 2048; // largest power-of-two snx of the FFT x-stage (one CTA holds 2048 points)
 
 // An error carrying the library status code; the ABI layer turns it into (status, message).
 struct Error : std::runtime_error {
@@ -48,6 +49,9 @@ struct GeoTab {
   const float* ey;      // [coil][sny]
   const float2* tw;     // [pol 0/1][x][kx]  e^{i2pi (kx-xs+gh)(x-c)/snx}
   float coil_off;       // 0.15 (ring of coils) or 0 (single coil)
+  // x-stage FFT tables when snx is a power of two (else NULL): [snx/2] e^{-i2pi k/snx}, then
+  // [pol 0/1][x] e^{i2pi gh (x-c)/snx}, then [kx] e^{-i2pi (kx-xs) c/snx}
+  const float2* xf;
 };
 
 // One unit of work: one slice of one volume, all echoes.  Device pointers throughout.
@@ -146,6 +150,10 @@ struct EpiPlan {
   int n_gtiles[2] = {0, 0};
   int4* d_atiles[4] = {nullptr, nullptr, nullptr, nullptr};
   int n_atiles[4] = {0, 0, 0, 0};
+  // x-stage as per-row FFTs (every unit has a power-of-two snx and FFT tables): tiles of rows
+  bool xfft = false;
+  int4* d_ftiles = nullptr;
+  int n_ftiles = 0;
   // forward y-stage pass (maps) served by the staged-input kernel (8 lines per tile)
   bool fwdq[2] = {false, false};
   // y-adjoint pass (maps | grads << 1) served by the fixed-coil-count kernel: its coil count, or 0
