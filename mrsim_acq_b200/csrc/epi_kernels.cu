@@ -1213,6 +1213,154 @@ __global__ void __launch_bounds__(256) xfft_kernel(const UnitDesc* __restrict__ 
   }
 }
 
+// The same x-stage with one warp per row for N = 32 E (E = 1..16), no block barriers: lane t
+// holds x[t + 32 m] (m < E).  With n = t + 32 m and k = k1 + E k2, W = e^{+-i2pi/N}:
+//   X[k1 + E k2] = sum_t W^{t k1} [ sum_m x[t + 32 m] W^{32 m k1} ] W^{E t k2}
+// so each lane does an E-point DFT of its registers (radix-2, unrolled), the twiddles W^{t k1},
+// and the 32-point DFTs over t run as five radix-2 decimation-in-frequency stages of lane
+// shuffles, which leave X[k1 + E k2] in lane bitrev5(k2).  A per-warp shared row (padded one
+// slot in 32) puts the results back in natural order for coalesced stores.
+__host__ __device__ constexpr int bitrev_c(int v, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((v >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+__host__ __device__ constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
+
+template <int E, bool ADJ>
+__global__ void __launch_bounds__(256) xfft_warp_kernel(const UnitDesc* __restrict__ units,
+                                                        const int4* __restrict__ tiles) {
+  constexpr int N = 32 * E, LE = log2_c(E);
+  constexpr int NP = N + N / 32;  // padded row
+  __shared__ __align__(16) float2 tw[N];  // e^{-i2pi j/N}
+  __shared__ __align__(16) float2 rb[8][NP];
+  const int4 t = tiles[blockIdx.x];
+  const UnitDesc& u = units[t.x];
+  const int r0 = t.y, nr = t.z;
+  const int nx = u.nx, nl = u.n_lines;
+  const float2* __restrict__ xf = u.geo.xf;
+  const float2* __restrict__ premod = xf + N / 2;
+  const float2* __restrict__ post = xf + N / 2 + 2 * N;
+  for (int k = threadIdx.x; k < N / 2; k += 256) {
+    const float2 w = xf[k];
+    tw[k] = w;
+    tw[k + N / 2] = make_float2(-w.x, -w.y);
+  }
+  __syncthreads();
+  // W(j) = e^{sigma i2pi j/N}: sigma = +1 forward, -1 adjoint
+  auto W = [&](int j) {
+    const float2 w = tw[j];
+    return ADJ ? w : make_float2(w.x, -w.y);
+  };
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ox = N / nx, xs = nx / 2, sxs = ox * xs;
+  const double xoff = (ox - 1.0) / 2.0;
+  const bool eddy = (u.flags & UF_EDDY) != 0;
+  const float inv_n = 1.0f / (float)(N * u.sny);
+  const int kpos = nx - xs;
+  float2* row = rb[warp];
+  for (int r = warp; r < nr; r += 8) {
+    const int R = r0 + r, q = R / nl, j = R % nl;
+    const LineRec& L = u.lines[j];
+    const int pol = L.pol < 0 ? 1 : 0;
+    const float dec = L.decay;
+    float2 b[E];
+    if (!ADJ) {
+      const float2* gr = u.g + (size_t)R * N;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const int x = lane + 32 * m;
+        float2 md = premod[pol * N + x];
+        if (eddy) {
+          const double xc = ((double)x - sxs - xoff) / ox;
+          double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)dec;
+          tv -= rint(tv);
+          float sn, cs;
+          __sincosf(kTwoPiF * (float)tv, &sn, &cs);
+          md = cmul(md, make_float2(cs, sn));
+        }
+        b[bitrev_c(m, LE)] = cmul(gr[x], md);
+      }
+    } else {
+      const float2* kr = u.kspace + ((size_t)q * u.n_rows + L.row) * nx;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const int n = lane + 32 * m;
+        const int kx = (n < kpos ? n : n - N) + xs;
+        float2 v = make_float2(0.f, 0.f);
+        if (kx >= 0 && kx < nx) {
+          const float2 p = post[kx];
+          v = cmul(kr[kx], make_float2(p.x, -p.y));
+        }
+        b[bitrev_c(m, LE)] = v;
+      }
+    }
+    // E-point DFT of the registers (decimation in time from bit-reversed order)
+#pragma unroll
+    for (int len = 2; len <= E; len <<= 1) {
+#pragma unroll
+      for (int i = 0; i < E; i += len) {
+#pragma unroll
+        for (int p = 0; p < len / 2; ++p) {
+          float2 v = b[i + p + len / 2];
+          if (p != 0) v = cmul(v, W(p * (E / len) * 32));
+          const float2 a = b[i + p];
+          b[i + p] = make_float2(a.x + v.x, a.y + v.y);
+          b[i + p + len / 2] = make_float2(a.x - v.x, a.y - v.y);
+        }
+      }
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) b[k1] = cmul(b[k1], W(lane * k1));
+    // 32-point DFTs across the lanes: radix-2 decimation in frequency
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+      const bool up = (lane & h) != 0;
+      const float sg = up ? -1.f : 1.f;
+      const float2 w = up ? W((lane & (h - 1)) * (N / (2 * h))) : make_float2(1.f, 0.f);
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) {
+        const float ox_ = __shfl_xor_sync(0xffffffffu, b[k1].x, h);
+        const float oy_ = __shfl_xor_sync(0xffffffffu, b[k1].y, h);
+        b[k1] = cmul(make_float2(fmaf(sg, b[k1].x, ox_), fmaf(sg, b[k1].y, oy_)), w);
+      }
+    }
+    const int k2 = __brev(lane) >> 27;
+#pragma unroll
+    for (int k1 = 0; k1 < E; ++k1) {
+      const int k = k1 + E * k2;
+      row[k + (k >> 5)] = b[k1];
+    }
+    __syncwarp();
+    if (!ADJ) {
+      float2* out = u.kspace + ((size_t)q * u.n_rows + L.row) * nx;
+      for (int kx = lane; kx < nx; kx += 32) {
+        const int k = (kx - xs) & (N - 1);
+        const float2 v = cmul(row[k + (k >> 5)], post[kx]);
+        out[kx] = make_float2(v.x * inv_n, v.y * inv_n);
+      }
+    } else {
+      float2* gr = u.g + (size_t)R * N;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const int x = lane + 32 * m;
+        float2 md = premod[pol * N + x];
+        if (eddy) {
+          const double xc = ((double)x - sxs - xoff) / ox;
+          double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)dec;
+          tv -= rint(tv);
+          float sn, cs;
+          __sincosf(kTwoPiF * (float)tv, &sn, &cs);
+          md = cmul(md, make_float2(cs, sn));
+        }
+        const float2 v = cmul(row[x + (x >> 5)], make_float2(md.x, -md.y));
+        gr[x] = make_float2(v.x * inv_n, v.y * inv_n);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 template <class K>
 void set_smem(K kernel, size_t bytes) {
   if (bytes > 48 * 1024) MRSIM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -1327,10 +1475,14 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       if (hu[i].geo.xf == nullptr || N < 8 || N > kXfftMaxN || (N & (N - 1)) != 0 || hu[i].nx > N) p->xfft = false;
     }
     if (p->xfft) {
+      const int N0 = hu[0].snx;
+      p->xfft_e = (N0 >= 32 && N0 <= 512) ? N0 / 32 : 0;
+      for (int i = 0; i < n; ++i)
+        if (hu[i].snx != N0) p->xfft_e = 0;
       std::vector<int4> ft;
       for (int i = 0; i < n; ++i) {
         const int rows = hu[i].ncoils * hu[i].n_lines;
-        const int per = std::min(256, kXfftMaxN / hu[i].snx);
+        const int per = p->xfft_e ? 32 : std::min(256, kXfftMaxN / hu[i].snx);
         for (int r0 = 0; r0 < rows; r0 += per) ft.push_back(make_int4(i, r0, std::min(per, rows - r0), 0));
       }
       p->n_ftiles = (int)ft.size();
@@ -1448,7 +1600,14 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
 void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st) {
   if (p->xfft) {
     if (p->n_ftiles) {
-      xfft_kernel<false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
+      switch (p->xfft_e) {
+        case 1: xfft_warp_kernel<1, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 2: xfft_warp_kernel<2, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 4: xfft_warp_kernel<4, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 8: xfft_warp_kernel<8, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 16: xfft_warp_kernel<16, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        default: xfft_kernel<false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
+      }
       MRSIM_CUDA(cudaGetLastError());
     }
     return;
@@ -1462,7 +1621,14 @@ void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st) {
 void epi_plan_adjoint_xstage(const EpiPlan* p, cudaStream_t st) {
   if (p->xfft) {
     if (p->n_ftiles) {
-      xfft_kernel<true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
+      switch (p->xfft_e) {
+        case 1: xfft_warp_kernel<1, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 2: xfft_warp_kernel<2, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 4: xfft_warp_kernel<4, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 8: xfft_warp_kernel<8, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        case 16: xfft_warp_kernel<16, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
+        default: xfft_kernel<true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
+      }
       MRSIM_CUDA(cudaGetLastError());
     }
     return;

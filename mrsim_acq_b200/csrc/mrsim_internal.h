@@ -152,6 +152,7 @@ struct EpiPlan {
   int n_atiles[4] = {0, 0, 0, 0};
   // x-stage as per-row FFTs (every unit has a power-of-two snx and FFT tables): tiles of rows
   bool xfft = false;
+  int xfft_e = 0;  // > 0: every unit has snx = 32 * xfft_e and the warp-per-row FFT runs
   int4* d_ftiles = nullptr;
   int n_ftiles = 0;
   // forward y-stage pass (maps) served by the staged-input kernel (8 lines per tile)
