@@ -311,7 +311,9 @@ int mrsim_probe_fp32_tflops(mrsim_context* ctx, double* tflops);
 int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace, float* comp_grad,
                                     float* fmap_grad, float* r2_grad);
 /* Synchronous, host buffers: upload images, forward, copy k-space to the host, adjoint of that
- * k-space (the residual of zero data), copy the gradients to the host.  Any output may be NULL. */
+ * k-space (the residual of zero data), copy the gradients to the host.  Any output may be NULL.
+ * Computed in groups of volumes whose results copy back on a second stream while the next group
+ * computes (page-locked host buffers let those copies overlap). */
 int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images,
                                   float* kspace, float* comp_grad, float* fmap_grad,
                                   float* r2_grad);

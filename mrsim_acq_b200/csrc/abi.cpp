@@ -505,22 +505,7 @@ int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* im
                                   float* fmap_grad, float* r2_grad) {
   if (!op) return guarded([] { need(nullptr, "operator"); });
   return on_ctx(op->impl->ctx, [&] {
-    auto* o = op->impl;
-    cudaStream_t st = o->ctx->stream;
-    const size_t plane = (size_t)o->snx * o->sny, nunits = (size_t)o->nv * o->nz;
-    if (images) mrsim::upload_series_images(o, images);
-    mrsim::epi_operator_forward(o);
-    if (kspace)
-      MRSIM_CUDA(cudaMemcpyAsync(kspace, o->d_kspace, o->kspace_elems * sizeof(float2), cudaMemcpyDeviceToHost, st));
-    mrsim::epi_operator_adjoint(o);
-    if (comp_grad)
-      MRSIM_CUDA(cudaMemcpyAsync(comp_grad, o->d_comp_grad, nunits * o->ncomp * plane * sizeof(float2),
-                                 cudaMemcpyDeviceToHost, st));
-    if (fmap_grad && o->d_fmap_grad)
-      MRSIM_CUDA(cudaMemcpyAsync(fmap_grad, o->d_fmap_grad, nunits * plane * 4, cudaMemcpyDeviceToHost, st));
-    if (r2_grad && o->d_r2_grad)
-      MRSIM_CUDA(cudaMemcpyAsync(r2_grad, o->d_r2_grad, nunits * o->ncomp * plane * 4, cudaMemcpyDeviceToHost, st));
-    MRSIM_CUDA(cudaStreamSynchronize(st));
+    mrsim::epi_operator_apply_host(op->impl, images, kspace, comp_grad, fmap_grad, r2_grad);
   });
 }
 

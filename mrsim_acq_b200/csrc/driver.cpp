@@ -172,7 +172,10 @@ void append_lines(std::vector<LineRec>& out, const mrsim_acquisition& acq, const
 
 // =============================================================================================
 // The batched forward/adjoint operator of a 2D EPI series.
-EpiOperator::~EpiOperator() {}
+EpiOperator::~EpiOperator() {
+  for (cudaEvent_t e : events) cudaEventDestroy(e);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
+}
 
 static void validate_series(const mrsim_acquisition_input& in, const mrsim_acquisition& acq) {
   const int64_t snx = in.sim_dims[0], sny = in.sim_dims[1], nz = in.sim_dims[2];
@@ -388,5 +391,54 @@ void epi_operator_forward(EpiOperator* op) {
 }
 
 void epi_operator_adjoint(EpiOperator* op) { epi_plan_adjoint(op->plan.get(), op->ctx->stream); }
+
+void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* kspace, float* comp_grad,
+                             float* fmap_grad, float* r2_grad) {
+  cudaStream_t st = o->ctx->stream;
+  const int nv = o->nv, nz = o->nz;
+  // groups of volumes: about eight, so the first group's compute is all the copies wait for
+  const int per = std::max(1, (nv + 7) / 8);
+  const int ngroups = (nv + per - 1) / per;
+  if (!o->copy_stream) MRSIM_CUDA(cudaStreamCreateWithFlags(&o->copy_stream, cudaStreamNonBlocking));
+  while ((int)o->events.size() < 2 * ngroups) {
+    cudaEvent_t e;
+    MRSIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    o->events.push_back(e);
+  }
+  cudaStream_t cs = o->copy_stream;
+  const size_t plane = (size_t)o->snx * o->sny;
+  const size_t kunit = o->kspace_elems / ((size_t)nv * nz);  // k-space elements per unit
+  if (images) upload_series_images(o, images);
+  const EpiPlan* p = o->plan.get();
+  epi_plan_statics(p, st);
+  for (int gi = 0; gi < ngroups; ++gi) {
+    const int u0 = gi * per * nz, u1 = std::min(nv, (gi + 1) * per) * nz;
+    epi_plan_forward(p, st, u0, u1);
+    MRSIM_CUDA(cudaEventRecord(o->events[2 * gi], st));
+    epi_plan_adjoint(p, st, u0, u1);
+    MRSIM_CUDA(cudaEventRecord(o->events[2 * gi + 1], st));
+  }
+  for (int gi = 0; gi < ngroups; ++gi) {
+    const size_t u0 = (size_t)gi * per * nz, nu = (size_t)std::min(nv, (gi + 1) * per) * nz - u0;
+    MRSIM_CUDA(cudaStreamWaitEvent(cs, o->events[2 * gi], 0));
+    if (kspace)
+      MRSIM_CUDA(cudaMemcpyAsync(kspace + 2 * u0 * kunit, o->d_kspace + u0 * kunit, nu * kunit * sizeof(float2),
+                                 cudaMemcpyDeviceToHost, cs));
+    MRSIM_CUDA(cudaStreamWaitEvent(cs, o->events[2 * gi + 1], 0));
+    if (comp_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(comp_grad + 2 * u0 * o->ncomp * plane, o->d_comp_grad + u0 * o->ncomp * plane,
+                                 nu * o->ncomp * plane * sizeof(float2), cudaMemcpyDeviceToHost, cs));
+    if (fmap_grad && o->d_fmap_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(fmap_grad + u0 * plane, o->d_fmap_grad + u0 * plane, nu * plane * 4,
+                                 cudaMemcpyDeviceToHost, cs));
+    if (r2_grad && o->d_r2_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(r2_grad + u0 * o->ncomp * plane, o->d_r2_grad + u0 * o->ncomp * plane,
+                                 nu * o->ncomp * plane * 4, cudaMemcpyDeviceToHost, cs));
+  }
+  // the compute stream ends after the copies, so work queued on it later sees the outputs copied
+  MRSIM_CUDA(cudaEventRecord(o->events[0], cs));
+  MRSIM_CUDA(cudaStreamWaitEvent(st, o->events[0], 0));
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+}
 
 }  // namespace mrsim

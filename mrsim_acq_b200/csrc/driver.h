@@ -49,6 +49,9 @@ struct EpiOperator {
   float* d_fmap_grad = nullptr;
   float* d_r2_grad = nullptr;
   std::unique_ptr<EpiPlan> plan;
+  // host-buffer apply: a copy stream and per-chunk events, made on first use
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> events;
   ~EpiOperator();
 };
 
@@ -58,6 +61,11 @@ EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_inp
 void upload_series_images(EpiOperator* op, const float* const* host_images);
 void epi_operator_forward(EpiOperator* op);
 void epi_operator_adjoint(EpiOperator* op);
+// Forward + adjoint from host images to host k-space and gradients (any output may be NULL),
+// pipelined by groups of volumes: the results of one group copy back on a second stream while the
+// next group computes.
+void epi_operator_apply_host(EpiOperator* op, const float* const* images, float* kspace, float* comp_grad,
+                             float* fmap_grad, float* r2_grad);
 
 // noalloc.cu: the forward of one slice with every intermediate in static device arrays.
 void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquisition& acq, float2* out,

@@ -1459,12 +1459,15 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<int4> tiles;
       const int step = p->fwdq[pass] ? 8 : kT;
+      p->y_start[pass].assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
+        p->y_start[pass][i] = (int)tiles.size();
         if (((hu[i].flags & UF_MAPS) != 0) != (pass == 1)) continue;
         for (int l = 0; l < hu[i].n_lines; l += step)
           for (int x0 = 0; x0 < hu[i].snx; x0 += 128)
             for (int q0 = 0; q0 < hu[i].ncoils; q0 += p->qg) tiles.push_back(make_int4(i, l, x0, q0));
       }
+      p->y_start[pass][n] = (int)tiles.size();
       p->n_ytiles[pass] = (int)tiles.size();
       p->d_ytiles[pass] = (int4*)dev_upload(p, tiles.data(), sizeof(int4) * tiles.size());
     }
@@ -1480,11 +1483,14 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       for (int i = 0; i < n; ++i)
         if (hu[i].snx != N0) p->xfft_e = 0;
       std::vector<int4> ft;
+      p->f_start.assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
+        p->f_start[i] = (int)ft.size();
         const int rows = hu[i].ncoils * hu[i].n_lines;
         const int per = p->xfft_e ? 32 : std::min(256, kXfftMaxN / hu[i].snx);
         for (int r0 = 0; r0 < rows; r0 += per) ft.push_back(make_int4(i, r0, std::min(per, rows - r0), 0));
       }
+      p->f_start[n] = (int)ft.size();
       p->n_ftiles = (int)ft.size();
       p->d_ftiles = (int4*)dev_upload(p, ft.data(), sizeof(int4) * ft.size());
     }
@@ -1492,7 +1498,9 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
     std::map<const LineRec*, std::vector<LineRec>> host_lines;
     for (int dir = 0; dir < 2 && !p->xfft; ++dir) {
       std::vector<XTile> xt;
+      p->g_start[dir].assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
+        p->g_start[dir][i] = (int)xt.size();
         const int nl = hu[i].n_lines;
         if (nl == 0) continue;
         auto it = host_lines.find(hu[i].lines);
@@ -1503,6 +1511,7 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
         }
         append_xtiles(xt, hu[i], i, it->second.data(), dir);
       }
+      p->g_start[dir][n] = (int)xt.size();
       p->n_gtiles[dir] = (int)xt.size();
       p->d_gtiles[dir] = dev_upload(p, xt.data(), sizeof(XTile) * xt.size());
     }
@@ -1517,13 +1526,16 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->adjq[pass] = (maps && p->nc == 8) ? 0 : nq_all;
       const int step = p->adjq[pass] ? 2 * adjq_rows(p->nc, maps) : kTY;
       std::vector<int4> yt;
+      p->a_start[pass].assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
+        p->a_start[pass][i] = (int)yt.size();
         bool um = (hu[i].flags & UF_MAPS) != 0;
         bool ug = (hu[i].flags & (UF_WANT_FMAP_GRAD | UF_WANT_R2_GRAD)) != 0;
         if (um != maps || ug != grads) continue;
         for (int y0 = 0; y0 < hu[i].sny; y0 += step)
           for (int x0 = 0; x0 < hu[i].snx; x0 += 128) yt.push_back(make_int4(i, y0, x0, 0));
       }
+      p->a_start[pass][n] = (int)yt.size();
       p->n_atiles[pass] = (int)yt.size();
       p->d_atiles[pass] = (int4*)dev_upload(p, yt.data(), sizeof(int4) * yt.size());
     }
@@ -1534,26 +1546,43 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
   return p;
 }
 
-void epi_plan_statics(const EpiPlan* p, cudaStream_t st) {
-  if (p->n_statics == 0) return;
-  dim3 grid((p->max_static_n + 255) / 256, p->n_statics);
-  statics_kernel<<<grid, 256, 0, st>>>(p->d_statics);
+namespace {
+// The tiles of units [u0, u1) in a list with per-unit starts `start` (empty: the whole list).
+struct TileRange {
+  int t0, n;
+};
+TileRange tile_range(const std::vector<int>& start, int n_tiles, int u0, int u1) {
+  if (start.empty() || (u0 == 0 && (u1 < 0 || u1 == (int)start.size() - 1))) return {0, n_tiles};
+  if (u1 < 0) u1 = (int)start.size() - 1;
+  if (u0 < 0 || u0 > u1 || u1 >= (int)start.size()) fail("unit range outside the plan");
+  return {start[u0], start[u1] - start[u0]};
+}
+}  // namespace
+
+void epi_plan_statics(const EpiPlan* p, cudaStream_t st, int u0, int u1) {
+  if (u1 < 0) u1 = p->n_statics;
+  if (u0 < 0 || u0 > u1 || u1 > p->n_statics) fail("unit range outside the plan");
+  if (u1 == u0) return;
+  dim3 grid((p->max_static_n + 255) / 256, u1 - u0);
+  statics_kernel<<<grid, 256, 0, st>>>(p->d_statics + u0);
   MRSIM_CUDA(cudaGetLastError());
 }
 
-void epi_plan_forward(const EpiPlan* p, cudaStream_t st) {
-  epi_plan_forward_ystage(p, st);
-  epi_plan_forward_xstage(p, st);
+void epi_plan_forward(const EpiPlan* p, cudaStream_t st, int u0, int u1) {
+  epi_plan_forward_ystage(p, st, u0, u1);
+  epi_plan_forward_xstage(p, st, u0, u1);
 }
 
-void epi_plan_adjoint(const EpiPlan* p, cudaStream_t st) {
-  epi_plan_adjoint_xstage(p, st);
-  epi_plan_adjoint_ystage(p, st);
+void epi_plan_adjoint(const EpiPlan* p, cudaStream_t st, int u0, int u1) {
+  epi_plan_adjoint_xstage(p, st, u0, u1);
+  epi_plan_adjoint_ystage(p, st, u0, u1);
 }
 
-void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
+void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) {
   for (int pass = 0; pass < 2; ++pass) {
-    if (p->n_ytiles[pass] == 0) continue;
+    const TileRange R = tile_range(p->y_start[pass], p->n_ytiles[pass], u0, u1);
+    if (R.n == 0) continue;
+    const Tile* tiles = (const Tile*)p->d_ytiles[pass] + R.t0;
     const bool maps = pass == 1;
     const int QG = p->qg, NCv = p->nc;
     if (p->fwdq[pass]) {
@@ -1564,7 +1593,7 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
   if (QG == QGV && NCv == NCV && maps == M) {                                           \
     auto k = ystage_q_kernel<QGV, NCV, M>;                                              \
     set_smem(k, smq);                                                                   \
-    k<<<(unsigned)p->n_ytiles[pass], 256, smq, st>>>(p->d_units, (const Tile*)p->d_ytiles[pass]); \
+    k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                              \
     launched = true;                                                                    \
   }
 #define MRSIM_YFQ(NCV, M) MRSIM_YF(1, NCV, M) MRSIM_YF(2, NCV, M) MRSIM_YF(4, NCV, M) MRSIM_YF(8, NCV, M)
@@ -1583,7 +1612,7 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
   if (QG == QGV && NCv == NCV && maps == M) {                                           \
     auto k = ystage_kernel<kT, QGV, NCV, M>;                                            \
     set_smem(k, sm);                                                                    \
-    k<<<(unsigned)p->n_ytiles[pass], 128, sm, st>>>(p->d_units, (const Tile*)p->d_ytiles[pass]); \
+    k<<<(unsigned)R.n, 128, sm, st>>>(p->d_units, tiles);                               \
     launched = true;                                                                    \
   }
 #define MRSIM_YQ(NCV, M) MRSIM_Y(1, NCV, M) MRSIM_Y(2, NCV, M) MRSIM_Y(4, NCV, M) MRSIM_Y(8, NCV, M)
@@ -1597,51 +1626,52 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st) {
   }
 }
 
-void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st) {
+namespace {
+void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) {
   if (p->xfft) {
-    if (p->n_ftiles) {
-      switch (p->xfft_e) {
-        case 1: xfft_warp_kernel<1, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 2: xfft_warp_kernel<2, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 4: xfft_warp_kernel<4, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 8: xfft_warp_kernel<8, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 16: xfft_warp_kernel<16, false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        default: xfft_kernel<false><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
-      }
-      MRSIM_CUDA(cudaGetLastError());
+    const TileRange R = tile_range(p->f_start, p->n_ftiles, u0, u1);
+    if (R.n == 0) return;
+    const int4* tiles = p->d_ftiles + R.t0;
+    const unsigned g = (unsigned)R.n;
+#define MRSIM_XF(ADJ)                                                                             \
+  switch (p->xfft_e) {                                                                            \
+    case 1: xfft_warp_kernel<1, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
+    case 2: xfft_warp_kernel<2, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
+    case 4: xfft_warp_kernel<4, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
+    case 8: xfft_warp_kernel<8, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
+    case 16: xfft_warp_kernel<16, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;              \
+    default: xfft_kernel<ADJ><<<g, 256, 0, st>>>(p->d_units, tiles);                              \
+  }
+    if (adj) {
+      MRSIM_XF(true)
+    } else {
+      MRSIM_XF(false)
     }
+#undef MRSIM_XF
+    MRSIM_CUDA(cudaGetLastError());
     return;
   }
-  if (p->n_gtiles[0]) {
-    xgemm_kernel<false><<<(unsigned)p->n_gtiles[0], 256, 0, st>>>(p->d_units, (const XTile*)p->d_gtiles[0]);
-    MRSIM_CUDA(cudaGetLastError());
-  }
+  const int dir = adj ? 1 : 0;
+  const TileRange R = tile_range(p->g_start[dir], p->n_gtiles[dir], u0, u1);
+  if (R.n == 0) return;
+  const XTile* tiles = (const XTile*)p->d_gtiles[dir] + R.t0;
+  if (adj)
+    xgemm_kernel<true><<<(unsigned)R.n, 256, 0, st>>>(p->d_units, tiles);
+  else
+    xgemm_kernel<false><<<(unsigned)R.n, 256, 0, st>>>(p->d_units, tiles);
+  MRSIM_CUDA(cudaGetLastError());
 }
+}  // namespace
 
-void epi_plan_adjoint_xstage(const EpiPlan* p, cudaStream_t st) {
-  if (p->xfft) {
-    if (p->n_ftiles) {
-      switch (p->xfft_e) {
-        case 1: xfft_warp_kernel<1, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 2: xfft_warp_kernel<2, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 4: xfft_warp_kernel<4, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 8: xfft_warp_kernel<8, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        case 16: xfft_warp_kernel<16, true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles); break;
-        default: xfft_kernel<true><<<(unsigned)p->n_ftiles, 256, 0, st>>>(p->d_units, p->d_ftiles);
-      }
-      MRSIM_CUDA(cudaGetLastError());
-    }
-    return;
-  }
-  if (p->n_gtiles[1]) {
-    xgemm_kernel<true><<<(unsigned)p->n_gtiles[1], 256, 0, st>>>(p->d_units, (const XTile*)p->d_gtiles[1]);
-    MRSIM_CUDA(cudaGetLastError());
-  }
-}
+void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1) { launch_xstage(p, st, u0, u1, false); }
 
-void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st) {
+void epi_plan_adjoint_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1) { launch_xstage(p, st, u0, u1, true); }
+
+void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) {
   for (int pass = 0; pass < 4; ++pass) {
-    if (p->n_atiles[pass] == 0) continue;
+    const TileRange R = tile_range(p->a_start[pass], p->n_atiles[pass], u0, u1);
+    if (R.n == 0) continue;
+    const int4* tiles = p->d_atiles[pass] + R.t0;
     const bool maps = pass & 1, grads = (pass & 2) != 0;
     const int NCv = p->nc;
     if (p->adjq[pass]) {
@@ -1653,7 +1683,7 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st) {
   if (NQv == NQV && NCv == NCV && maps == M && grads == G) {                            \
     auto k = yadjoint_q_kernel<NQV, adjq_rows(NCV, M), NCV, M, G>;                      \
     set_smem(k, smq);                                                                   \
-    k<<<(unsigned)p->n_atiles[pass], 256, smq, st>>>(p->d_units, p->d_atiles[pass]);    \
+    k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                              \
     launched = true;                                                                    \
   }
 #define MRSIM_AQC(NCV, M, G) MRSIM_AQ(1, NCV, M, G) MRSIM_AQ(2, NCV, M, G) MRSIM_AQ(4, NCV, M, G) MRSIM_AQ(8, NCV, M, G)
@@ -1675,7 +1705,7 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st) {
   if (NCv == NCV && maps == M && grads == G) {                                          \
     auto k = yadjoint_kernel<kTY, NCV, M, G>;                                           \
     set_smem(k, sm);                                                                    \
-    k<<<(unsigned)p->n_atiles[pass], 128, sm, st>>>(p->d_units, p->d_atiles[pass]);     \
+    k<<<(unsigned)R.n, 128, sm, st>>>(p->d_units, tiles);                               \
     launched = true;                                                                    \
   }
 #define MRSIM_AN(M, G) MRSIM_A(1, M, G) MRSIM_A(2, M, G) MRSIM_A(3, M, G) MRSIM_A(4, M, G) MRSIM_A(8, M, G)

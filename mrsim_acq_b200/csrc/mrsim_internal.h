@@ -160,19 +160,22 @@ struct EpiPlan {
   // y-adjoint pass (maps | grads << 1) served by the fixed-coil-count kernel: its coil count, or 0
   // for the general kernel
   int adjq[4] = {0, 0, 0, 0};
+  // first tile of each unit in each list (n_units + 1 entries; empty: launch whole lists only)
+  std::vector<int> y_start[2], a_start[4], f_start, g_start[2];
   std::vector<void*> allocs;
   ~EpiPlan();
 };
 EpiPlan* epi_plan_create(const UnitDesc* units, int n, const StaticDesc* statics, int ns);
 // The x-stage tiles of one unit (dir 0 forward, 1 adjoint); `lines` is a host copy of its table.
 void append_xtiles(std::vector<XTile>& out, const UnitDesc& u, int unit_index, const LineRec* lines, int dir);
-void epi_plan_statics(const EpiPlan* p, cudaStream_t st);
-void epi_plan_forward(const EpiPlan* p, cudaStream_t st);
-void epi_plan_adjoint(const EpiPlan* p, cudaStream_t st);
-void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st);
-void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st);
-void epi_plan_adjoint_xstage(const EpiPlan* p, cudaStream_t st);
-void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st);
+// Each launcher covers units [u0, u1) of the plan (u1 < 0: every unit).
+void epi_plan_statics(const EpiPlan* p, cudaStream_t st, int u0 = 0, int u1 = -1);
+void epi_plan_forward(const EpiPlan* p, cudaStream_t st, int u0 = 0, int u1 = -1);
+void epi_plan_adjoint(const EpiPlan* p, cudaStream_t st, int u0 = 0, int u1 = -1);
+void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st, int u0 = 0, int u1 = -1);
+void epi_plan_forward_xstage(const EpiPlan* p, cudaStream_t st, int u0 = 0, int u1 = -1);
+void epi_plan_adjoint_xstage(const EpiPlan* p, cudaStream_t st, int u0 = 0, int u1 = -1);
+void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st, int u0 = 0, int u1 = -1);
 // FP32 FMA throughput probe (misc_kernels.cu): TFLOP/s of a register-resident FMA loop.
 double probe_fp32_tflops(cudaStream_t st);
 
