@@ -312,8 +312,8 @@ int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace,
                                     float* fmap_grad, float* r2_grad);
 /* Synchronous, host buffers: upload images, forward, copy k-space to the host, adjoint of that
  * k-space (the residual of zero data), copy the gradients to the host.  Any output may be NULL.
- * Computed in groups of volumes whose results copy back on a second stream while the next group
- * computes (page-locked host buffers let those copies overlap). */
+ * Computed in groups of slices (of volumes for a single slice) whose images upload, and whose
+ * results copy back, while other groups compute (page-locked host buffers let the copies overlap). */
 int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images,
                                   float* kspace, float* comp_grad, float* fmap_grad,
                                   float* r2_grad);

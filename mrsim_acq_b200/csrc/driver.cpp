@@ -175,6 +175,7 @@ void append_lines(std::vector<LineRec>& out, const mrsim_acquisition& acq, const
 EpiOperator::~EpiOperator() {
   for (cudaEvent_t e : events) cudaEventDestroy(e);
   if (copy_stream) cudaStreamDestroy(copy_stream);
+  if (upload_stream) cudaStreamDestroy(upload_stream);
 }
 
 static void validate_series(const mrsim_acquisition_input& in, const mrsim_acquisition& acq) {
@@ -294,8 +295,10 @@ EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_inp
       for (int i = 0; i < 3; ++i) grad[i] = in.eddy_drive[3 * g + i];
     for (int zl = 0; zl < nz; ++zl) {
       const int z = slice_z ? (int)slice_z[zl] : zl;
-      const size_t ui = (size_t)g * nz + zl;
-      UnitDesc& u = units[ui];
+      // memory is volume-major (ui); the plan orders units slice-major (pi) so that a range of
+      // slices is a range of plan units
+      const size_t ui = (size_t)g * nz + zl, pi = (size_t)zl * nv + g;
+      UnitDesc& u = units[pi];
       std::memset(&u, 0, sizeof u);
       u.snx = snx;
       u.sny = sny;
@@ -338,7 +341,7 @@ EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_inp
       u.fmap_grad = op->d_fmap_grad ? op->d_fmap_grad + ui * plane : nullptr;
       u.r2_grad = op->d_r2_grad ? op->d_r2_grad + ui * ncomp * plane : nullptr;
 
-      StaticDesc& sd = statics[ui];
+      StaticDesc& sd = statics[pi];
       std::memset(&sd, 0, sizeof sd);
       sd.snx = snx;
       sd.sny = sny;
@@ -396,48 +399,84 @@ void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* 
                              float* fmap_grad, float* r2_grad) {
   cudaStream_t st = o->ctx->stream;
   const int nv = o->nv, nz = o->nz;
-  // groups of volumes: about eight, so the first group's compute is all the copies wait for
-  const int per = std::max(1, (nv + 7) / 8);
-  const int ngroups = (nv + per - 1) / per;
-  if (!o->copy_stream) MRSIM_CUDA(cudaStreamCreateWithFlags(&o->copy_stream, cudaStreamNonBlocking));
-  while ((int)o->events.size() < 2 * ngroups) {
+  // Groups are boxes of volumes [g0, g1) x slices [z0, z1), each a range of the slice-major plan
+  // units: about eight groups of whole slices, or with one slice, about eight groups of volumes.
+  struct Box {
+    int g0, g1, z0, z1;
+  };
+  std::vector<Box> boxes;
+  if (nz >= 2) {
+    const int per = std::max(1, (nz + 7) / 8);
+    for (int z0 = 0; z0 < nz; z0 += per) boxes.push_back({0, nv, z0, std::min(nz, z0 + per)});
+  } else {
+    const int per = std::max(1, (nv + 7) / 8);
+    for (int g0 = 0; g0 < nv; g0 += per) boxes.push_back({g0, std::min(nv, g0 + per), 0, nz});
+  }
+  const int ng = (int)boxes.size();
+  for (cudaStream_t* s : {&o->copy_stream, &o->upload_stream})
+    if (!*s) MRSIM_CUDA(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+  while ((int)o->events.size() < 3 * ng + 1) {
     cudaEvent_t e;
     MRSIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     o->events.push_back(e);
   }
-  cudaStream_t cs = o->copy_stream;
+  cudaEvent_t* ev = o->events.data();
+  cudaStream_t cs = o->copy_stream, us = o->upload_stream;
   const size_t plane = (size_t)o->snx * o->sny;
-  const size_t kunit = o->kspace_elems / ((size_t)nv * nz);  // k-space elements per unit
-  if (images) upload_series_images(o, images);
+  const size_t per_comp = (size_t)nz * plane * nv;  // host floats per compartment
+  float* staging = images ? (float*)workspace(o->ctx, 20, per_comp * o->ncomp * 4) : nullptr;
+  // uploads: by slice groups on their own stream (the reference layout keeps a slice range of
+  // every volume contiguous), else all at once
+  if (images) {
+    MRSIM_CUDA(cudaEventRecord(ev[3 * ng], st));  // earlier work on the compute stream is done first
+    MRSIM_CUDA(cudaStreamWaitEvent(us, ev[3 * ng], 0));
+    for (int b = 0; b < ng; ++b) {
+      const Box& B = boxes[b];
+      if (nz >= 2 || b == 0) {
+        const size_t f0 = nz >= 2 ? (size_t)B.z0 * plane * nv : 0;
+        const size_t nf = nz >= 2 ? (size_t)(B.z1 - B.z0) * plane * nv : per_comp;
+        for (int c = 0; c < o->ncomp; ++c)
+          MRSIM_CUDA(cudaMemcpyAsync(staging + (size_t)c * per_comp + f0, images[c] + f0, nf * 4,
+                                     cudaMemcpyHostToDevice, us));
+      }
+      MRSIM_CUDA(cudaEventRecord(ev[3 * b], us));
+    }
+  }
   const EpiPlan* p = o->plan.get();
   epi_plan_statics(p, st);
-  for (int gi = 0; gi < ngroups; ++gi) {
-    const int u0 = gi * per * nz, u1 = std::min(nv, (gi + 1) * per) * nz;
+  for (int b = 0; b < ng; ++b) {
+    const Box& B = boxes[b];
+    if (images) {
+      MRSIM_CUDA(cudaStreamWaitEvent(st, ev[3 * b], 0));
+      if (nz >= 2 || b == 0)
+        launch_series_transpose(staging, o->d_images, o->ncomp, nv, nz, (int)plane, st, nz >= 2 ? B.z0 : 0,
+                                nz >= 2 ? B.z1 : nz);
+    }
+    const int u0 = B.z0 * nv + B.g0, u1 = (B.z1 - 1) * nv + B.g1;  // slice-major plan units
     epi_plan_forward(p, st, u0, u1);
-    MRSIM_CUDA(cudaEventRecord(o->events[2 * gi], st));
+    MRSIM_CUDA(cudaEventRecord(ev[3 * b + 1], st));
     epi_plan_adjoint(p, st, u0, u1);
-    MRSIM_CUDA(cudaEventRecord(o->events[2 * gi + 1], st));
+    MRSIM_CUDA(cudaEventRecord(ev[3 * b + 2], st));
   }
-  for (int gi = 0; gi < ngroups; ++gi) {
-    const size_t u0 = (size_t)gi * per * nz, nu = (size_t)std::min(nv, (gi + 1) * per) * nz - u0;
-    MRSIM_CUDA(cudaStreamWaitEvent(cs, o->events[2 * gi], 0));
-    if (kspace)
-      MRSIM_CUDA(cudaMemcpyAsync(kspace + 2 * u0 * kunit, o->d_kspace + u0 * kunit, nu * kunit * sizeof(float2),
-                                 cudaMemcpyDeviceToHost, cs));
-    MRSIM_CUDA(cudaStreamWaitEvent(cs, o->events[2 * gi + 1], 0));
-    if (comp_grad)
-      MRSIM_CUDA(cudaMemcpyAsync(comp_grad + 2 * u0 * o->ncomp * plane, o->d_comp_grad + u0 * o->ncomp * plane,
-                                 nu * o->ncomp * plane * sizeof(float2), cudaMemcpyDeviceToHost, cs));
-    if (fmap_grad && o->d_fmap_grad)
-      MRSIM_CUDA(cudaMemcpyAsync(fmap_grad + u0 * plane, o->d_fmap_grad + u0 * plane, nu * plane * 4,
-                                 cudaMemcpyDeviceToHost, cs));
-    if (r2_grad && o->d_r2_grad)
-      MRSIM_CUDA(cudaMemcpyAsync(r2_grad + u0 * o->ncomp * plane, o->d_r2_grad + u0 * o->ncomp * plane,
-                                 nu * o->ncomp * plane * 4, cudaMemcpyDeviceToHost, cs));
+  // downloads: the box is nv' rows (volumes) of (z1 - z0) units, pitch nz units
+  const size_t kunit = o->kspace_elems / ((size_t)nv * nz);
+  auto down = [&](const Box& B, void* host, const void* dev, size_t unit_bytes) {
+    const size_t off = ((size_t)B.g0 * nz + B.z0) * unit_bytes, pitch = (size_t)nz * unit_bytes;
+    MRSIM_CUDA(cudaMemcpy2DAsync((char*)host + off, pitch, (const char*)dev + off, pitch, (B.z1 - B.z0) * unit_bytes,
+                                 B.g1 - B.g0, cudaMemcpyDeviceToHost, cs));
+  };
+  for (int b = 0; b < ng; ++b) {
+    const Box& B = boxes[b];
+    MRSIM_CUDA(cudaStreamWaitEvent(cs, ev[3 * b + 1], 0));
+    if (kspace) down(B, kspace, o->d_kspace, kunit * sizeof(float2));
+    MRSIM_CUDA(cudaStreamWaitEvent(cs, ev[3 * b + 2], 0));
+    if (comp_grad) down(B, comp_grad, o->d_comp_grad, o->ncomp * plane * sizeof(float2));
+    if (fmap_grad && o->d_fmap_grad) down(B, fmap_grad, o->d_fmap_grad, plane * 4);
+    if (r2_grad && o->d_r2_grad) down(B, r2_grad, o->d_r2_grad, o->ncomp * plane * 4);
   }
-  // the compute stream ends after the copies, so work queued on it later sees the outputs copied
-  MRSIM_CUDA(cudaEventRecord(o->events[0], cs));
-  MRSIM_CUDA(cudaStreamWaitEvent(st, o->events[0], 0));
+  // the compute stream ends after the copies, so work queued on it later sees them done
+  MRSIM_CUDA(cudaEventRecord(ev[3 * ng], cs));
+  MRSIM_CUDA(cudaStreamWaitEvent(st, ev[3 * ng], 0));
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
 

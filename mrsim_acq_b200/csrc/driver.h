@@ -49,8 +49,8 @@ struct EpiOperator {
   float* d_fmap_grad = nullptr;
   float* d_r2_grad = nullptr;
   std::unique_ptr<EpiPlan> plan;
-  // host-buffer apply: a copy stream and per-chunk events, made on first use
-  cudaStream_t copy_stream = nullptr;
+  // host-buffer apply: download and upload streams and per-group events, made on first use
+  cudaStream_t copy_stream = nullptr, upload_stream = nullptr;
   std::vector<cudaEvent_t> events;
   ~EpiOperator();
 };
@@ -62,8 +62,8 @@ void upload_series_images(EpiOperator* op, const float* const* host_images);
 void epi_operator_forward(EpiOperator* op);
 void epi_operator_adjoint(EpiOperator* op);
 // Forward + adjoint from host images to host k-space and gradients (any output may be NULL),
-// pipelined by groups of volumes: the results of one group copy back on a second stream while the
-// next group computes.
+// pipelined by groups of slices (or of volumes for one slice): a group's images upload, and its
+// results copy back, on two more streams while other groups compute.
 void epi_operator_apply_host(EpiOperator* op, const float* const* images, float* kspace, float* comp_grad,
                              float* fmap_grad, float* r2_grad);
 
@@ -72,6 +72,9 @@ void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquis
                                 cudaStream_t st);
 
 // misc_kernels.cu
-void launch_series_transpose(const float* staging, float* out, int ncomp, int nv, int nz, int plane, cudaStream_t st);
+// Slices [z0, z1) (z1 < 0: all) of the reference image layout (per compartment [z][y][x][g]) into
+// the unit-major layout [g][z][c][y][x].
+void launch_series_transpose(const float* staging, float* out, int ncomp, int nv, int nz, int plane, cudaStream_t st,
+                             int z0 = 0, int z1 = -1);
 
 }  // namespace mrsim

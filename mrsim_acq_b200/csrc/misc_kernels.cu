@@ -10,13 +10,14 @@ namespace {
 // staging: per compartment c, the reference series layout in[c][vox * nv + g] with
 // vox = p + plane * z; out: [g][z][c][p].  One thread per (c, vox) reads nv consecutive values.
 __global__ void series_transpose_kernel(const float* __restrict__ in, float* __restrict__ out, int ncomp, int nv,
-                                        int nz, int plane) {
+                                        int nz, int plane, int z0, int z1) {
   const long long nvox = (long long)nz * plane;
-  const long long total = nvox * ncomp;
+  const long long span = (long long)(z1 - z0) * plane;
+  const long long total = span * ncomp;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(t / nvox);
-    const long long vox = t % nvox;
+    const int c = (int)(t / span);
+    const long long vox = (long long)z0 * plane + t % span;
     const int z = (int)(vox / plane), p = (int)(vox % plane);
     const float* src = in + (size_t)c * nvox * nv + (size_t)vox * nv;
     for (int g = 0; g < nv; ++g) out[(((size_t)g * nz + z) * ncomp + c) * plane + p] = src[g];
@@ -111,10 +112,13 @@ void launch_series_output(const float2* combined, const float* sigma, float* re,
   MRSIM_CUDA(cudaGetLastError());
 }
 
-void launch_series_transpose(const float* staging, float* out, int ncomp, int nv, int nz, int plane, cudaStream_t st) {
-  const long long total = (long long)nz * plane * ncomp;
+void launch_series_transpose(const float* staging, float* out, int ncomp, int nv, int nz, int plane, cudaStream_t st,
+                             int z0, int z1) {
+  if (z1 < 0) z1 = nz;
+  const long long total = (long long)(z1 - z0) * plane * ncomp;
+  if (total <= 0) return;
   int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-  series_transpose_kernel<<<blocks, 256, 0, st>>>(staging, out, ncomp, nv, nz, plane);
+  series_transpose_kernel<<<blocks, 256, 0, st>>>(staging, out, ncomp, nv, nz, plane, z0, z1);
   MRSIM_CUDA(cudaGetLastError());
 }
 
