@@ -132,6 +132,14 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+# DRAM bytes per unit (one slice of one volume) of the two y-stage kernels, from one ncu capture of
+# this workload at 24 volumes (720 units): dram__bytes.sum.per_second x gpu__time_duration.sum of
+# yadjoint_q_kernel<8,4,3,0,1> (1055.8 MB) and ystage_q_kernel<8,3,0> (564.5 MB); the summaries are
+# profiles/yadjoint_q_kernel_epi-series-sim128-v24.md and profiles/ystage_q_kernel_epi-series-sim128-v24.md.
+# Traffic grows with the units processed (each unit reads and writes its own planes).
+NCU_DRAM_BYTES_PER_UNIT = {"adjoint_ystage": 1055.8e6 / 720, "forward_ystage": 564.5e6 / 720}
+
+
 def algorithmic_flops(op_units, n_lines, snx, sny, nx, ncoils, ncomp):
     """Per launch over all units: the canonical per-(slice, volume, echo) work of the exact DFT,
     y-stage 4*Q*C*snx*sny*ny_acq and x-stage 8*Q*snx*nx*ny_acq, summed over echoes (n_lines is
@@ -230,7 +238,9 @@ def run_ours(args, rank, world, local_rank):
     pk, pk_kind = peaks()
     # dominant kernel: the larger of the forward / adjoint y-stages
     dom = 1 if stage_avg[1] >= stage_avg[4] else 4
+    dom_name = ["statics", "forward_ystage", "forward_xstage", "adjoint_xstage", "adjoint_ystage"][dom]
     achieved = fy / (stage_avg[dom] * 1e-3) / 1e12
+    traffic = NCU_DRAM_BYTES_PER_UNIT[dom_name] * units
     res = {
         "metric": METRIC, "value": samples * world / (ms_step * 1e-3), "unit": "samples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -243,11 +253,11 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": samples * world / (float(e2e_ms.item()) * 1e-3), "unit": "samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "call": "mrsim_epi_operator_apply_host (host images in, k-space and gradients out)"},
-        "roofline": {"bound": "fp32", "kernel": ["statics", "forward_ystage", "forward_xstage", "adjoint_xstage",
-                                                 "adjoint_ystage"][dom],
+        "roofline": {"bound": "fp32", "kernel": dom_name,
                      "achieved": achieved, "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
                      "peak_source": "measured live: register FMA loop on this GPU (no FP32 entry in MEASURED_PEAKS.json)",
-                     "algorithmic_flops_per_launch": fy, "traffic": None,
+                     "algorithmic_flops_per_launch": fy, "traffic": traffic,
+                     "traffic_source": "ncu DRAM bytes per unit (24-volume capture) x units of this launch",
                      "stage_ms": dict(zip(["statics", "forward_ystage", "forward_xstage", "adjoint_xstage",
                                            "adjoint_ystage"], [round(float(v), 4) for v in stage_avg]))},
         "gpu_launches": 5 * args.steps,
