@@ -1213,7 +1213,7 @@ __global__ void __launch_bounds__(256) xfft_kernel(const UnitDesc* __restrict__ 
   }
 }
 
-// The same x-stage with one warp per row for N = 32 E (E = 1..16), no block barriers: lane t
+// The same x-stage with one warp per row for N = 32 E (E = 1..8), no block barriers: lane t
 // holds x[t + 32 m] (m < E).  With n = t + 32 m and k = k1 + E k2, W = e^{+-i2pi/N}:
 //   X[k1 + E k2] = sum_t W^{t k1} [ sum_m x[t + 32 m] W^{32 m k1} ] W^{E t k2}
 // so each lane does an E-point DFT of its registers (radix-2, unrolled), the twiddles W^{t k1},
@@ -1228,23 +1228,36 @@ __host__ __device__ constexpr int bitrev_c(int v, int bits) {
 __host__ __device__ constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
 
 template <int E, bool ADJ>
-__global__ void __launch_bounds__(256) xfft_warp_kernel(const UnitDesc* __restrict__ units,
-                                                        const int4* __restrict__ tiles) {
+__global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const UnitDesc* __restrict__ units,
+                                                           const int4* __restrict__ tiles) {
   constexpr int N = 32 * E, LE = log2_c(E);
   constexpr int NP = N + N / 32;  // padded row
-  __shared__ __align__(16) float2 tw[N];  // e^{-i2pi j/N}
+  constexpr int RT = 32;          // rows per tile
+  __shared__ __align__(16) float2 tw[N];        // e^{-i2pi j/N}
+  __shared__ __align__(16) float2 pm[2 * N];    // premodulation per polarity
+  __shared__ __align__(16) float2 pt[N];        // post-twiddle per kx (nx <= N)
   __shared__ __align__(16) float2 rb[8][NP];
+  __shared__ int rq[RT], rrow[RT], rpol[RT];
+  __shared__ float rdec[RT];
   const int4 t = tiles[blockIdx.x];
   const UnitDesc& u = units[t.x];
   const int r0 = t.y, nr = t.z;
   const int nx = u.nx, nl = u.n_lines;
   const float2* __restrict__ xf = u.geo.xf;
-  const float2* __restrict__ premod = xf + N / 2;
-  const float2* __restrict__ post = xf + N / 2 + 2 * N;
   for (int k = threadIdx.x; k < N / 2; k += 256) {
     const float2 w = xf[k];
     tw[k] = w;
     tw[k + N / 2] = make_float2(-w.x, -w.y);
+  }
+  for (int k = threadIdx.x; k < 2 * N; k += 256) pm[k] = xf[N / 2 + k];
+  for (int k = threadIdx.x; k < nx; k += 256) pt[k] = xf[N / 2 + 2 * N + k];
+  for (int r = threadIdx.x; r < nr; r += 256) {
+    const int R = r0 + r;
+    const LineRec& L = u.lines[R % nl];
+    rq[r] = R / nl;
+    rrow[r] = L.row;
+    rpol[r] = L.pol < 0 ? 1 : 0;
+    rdec[r] = L.decay;
   }
   __syncthreads();
   // W(j) = e^{sigma i2pi j/N}: sigma = +1 forward, -1 adjoint
@@ -1259,37 +1272,39 @@ __global__ void __launch_bounds__(256) xfft_warp_kernel(const UnitDesc* __restri
   const float inv_n = 1.0f / (float)(N * u.sny);
   const int kpos = nx - xs;
   float2* row = rb[warp];
+  // premodulation of the line's polarity times E_j(x) = e^{i2pi (cx xc + qx xc^2 + z) decay_j}
+  auto modulation = [&](int pol, float dec, int x) {
+    float2 md = pm[pol * N + x];
+    if (eddy) {
+      const double xc = ((double)x - sxs - xoff) / ox;
+      double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)dec;
+      tv -= rint(tv);
+      float sn, cs;
+      __sincosf(kTwoPiF * (float)tv, &sn, &cs);
+      md = cmul(md, make_float2(cs, sn));
+    }
+    return md;
+  };
   for (int r = warp; r < nr; r += 8) {
-    const int R = r0 + r, q = R / nl, j = R % nl;
-    const LineRec& L = u.lines[j];
-    const int pol = L.pol < 0 ? 1 : 0;
-    const float dec = L.decay;
+    const int R = r0 + r, q = rq[r], orow = rrow[r], pol = rpol[r];
+    const float dec = rdec[r];
     float2 b[E];
     if (!ADJ) {
       const float2* gr = u.g + (size_t)R * N;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
-        float2 md = premod[pol * N + x];
-        if (eddy) {
-          const double xc = ((double)x - sxs - xoff) / ox;
-          double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)dec;
-          tv -= rint(tv);
-          float sn, cs;
-          __sincosf(kTwoPiF * (float)tv, &sn, &cs);
-          md = cmul(md, make_float2(cs, sn));
-        }
-        b[bitrev_c(m, LE)] = cmul(gr[x], md);
+        b[bitrev_c(m, LE)] = cmul(gr[x], modulation(pol, dec, x));
       }
     } else {
-      const float2* kr = u.kspace + ((size_t)q * u.n_rows + L.row) * nx;
+      const float2* kr = u.kspace + ((size_t)q * u.n_rows + orow) * nx;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int n = lane + 32 * m;
         const int kx = (n < kpos ? n : n - N) + xs;
         float2 v = make_float2(0.f, 0.f);
         if (kx >= 0 && kx < nx) {
-          const float2 p = post[kx];
+          const float2 p = pt[kx];
           v = cmul(kr[kx], make_float2(p.x, -p.y));
         }
         b[bitrev_c(m, LE)] = v;
@@ -1333,10 +1348,10 @@ __global__ void __launch_bounds__(256) xfft_warp_kernel(const UnitDesc* __restri
     }
     __syncwarp();
     if (!ADJ) {
-      float2* out = u.kspace + ((size_t)q * u.n_rows + L.row) * nx;
+      float2* out = u.kspace + ((size_t)q * u.n_rows + orow) * nx;
       for (int kx = lane; kx < nx; kx += 32) {
         const int k = (kx - xs) & (N - 1);
-        const float2 v = cmul(row[k + (k >> 5)], post[kx]);
+        const float2 v = cmul(row[k + (k >> 5)], pt[kx]);
         out[kx] = make_float2(v.x * inv_n, v.y * inv_n);
       }
     } else {
@@ -1344,15 +1359,7 @@ __global__ void __launch_bounds__(256) xfft_warp_kernel(const UnitDesc* __restri
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
-        float2 md = premod[pol * N + x];
-        if (eddy) {
-          const double xc = ((double)x - sxs - xoff) / ox;
-          double tv = ((double)u.eddy_cx * xc + (double)u.eddy_qx * xc * xc + (double)u.eddy_z) * (double)dec;
-          tv -= rint(tv);
-          float sn, cs;
-          __sincosf(kTwoPiF * (float)tv, &sn, &cs);
-          md = cmul(md, make_float2(cs, sn));
-        }
+        const float2 md = modulation(pol, dec, x);
         const float2 v = cmul(row[x + (x >> 5)], make_float2(md.x, -md.y));
         gr[x] = make_float2(v.x * inv_n, v.y * inv_n);
       }
@@ -1479,7 +1486,7 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
     }
     if (p->xfft) {
       const int N0 = hu[0].snx;
-      p->xfft_e = (N0 >= 32 && N0 <= 512) ? N0 / 32 : 0;
+      p->xfft_e = (N0 >= 32 && N0 <= 256) ? N0 / 32 : 0;
       for (int i = 0; i < n; ++i)
         if (hu[i].snx != N0) p->xfft_e = 0;
       std::vector<int4> ft;
@@ -1639,7 +1646,6 @@ void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) 
     case 2: xfft_warp_kernel<2, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
     case 4: xfft_warp_kernel<4, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
     case 8: xfft_warp_kernel<8, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
-    case 16: xfft_warp_kernel<16, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;              \
     default: xfft_kernel<ADJ><<<g, 256, 0, st>>>(p->d_units, tiles);                              \
   }
     if (adj) {
