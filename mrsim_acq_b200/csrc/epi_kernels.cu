@@ -787,30 +787,39 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
   const bool xok = x < snx;
   const int nchunks = (nlines + JC - 1) / JC;
 
-  // this thread's 16-byte pieces of a chunk: (line jj, coil q, column pair p)
+  // This thread's 16-byte pieces k = tid + 256 i of a chunk: row r = k / 64 = (line jj, coil q),
+  // column pair 2 (k % 64); the destination is float2 2k of the stage.  The source offset of
+  // each piece for the chunk's first line (or -1 past snx) sits in a per-thread shared table, so
+  // a chunk costs one shared load, a compare and a select per piece.  (The plan keeps
+  // NQ * lines * snx below 2^31.)
+  __shared__ int ptab[PPT * 256];
   const float2* __restrict__ gsrc = u.g;
-  const size_t qstride = (size_t)nlines * snx;
-  auto issue_chunk = [&](int c) {
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) {
+    const int k = tid + 256 * i;
+    if (PIECES % 256 == 0 || k < PIECES) {
+      const int r = k >> 6, xx = x0 + (k & 63) * 2;
+      ptab[i * 256 + tid] = xx < snx ? ((r % NQ) * nlines + r / NQ) * snx + xx : -1;
+    }
+  }
+  auto issue_chunk = [&](int c, int stage) {
     if (c < nchunks) {
-      const int j0 = c * JC;
-      float2* dst = hbuf + (c % kAdjStages) * STAGE;
+      const int rem = nlines - c * JC, jo = c * JC * snx;
+      float2* dst = hbuf + stage * STAGE;
 #pragma unroll
       for (int i = 0; i < PPT; ++i) {
         const int k = tid + 256 * i;
         if (PIECES % 256 == 0 || k < PIECES) {
-          const int r = k >> 6, pcol = (k & 63) * 2;
-          const int jj = r / NQ, q = r % NQ;
-          const int j = j0 + jj, xx = x0 + pcol;
-          const bool ok = j < nlines && xx < snx;
-          const float2* src = ok ? gsrc + q * qstride + (size_t)j * snx + xx : gsrc;
-          cp_async16(dst + r * 128 + pcol, src, ok ? 16 : 0);
+          const int o = ptab[i * 256 + tid];
+          const bool ok = o >= 0 && ((tid >> 6) + 4 * i) / NQ < rem;
+          cp_async16(dst + 2 * k, gsrc + (ok ? o + jo : 0), ok ? 16 : 0);
         }
       }
     }
     cp_async_commit();
   };
 #pragma unroll
-  for (int c = 0; c < kAdjStages - 1; ++c) issue_chunk(c);
+  for (int c = 0; c < kAdjStages - 1; ++c) issue_chunk(c, c);
 
   const int ys = u.ny / 2;
   const int oy = sny / u.ny;
@@ -901,23 +910,30 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
       if (GRADS) Uy[ty][GRADS ? c : 0] = Vx[ty][GRADS ? c : 0] = 0.f;
     }
 
+  int s_use = 0, s_issue = kAdjStages - 1;  // stages of chunk c and of chunk c + stages - 1
   for (int c = 0; c < nchunks; ++c) {
     cp_async_wait_n<kAdjStages - 2>();
     __syncthreads();  // chunk c landed for every thread; every thread is done with chunk c - 1
-    issue_chunk(c + kAdjStages - 1);
-    const float2* hs = hbuf + (c % kAdjStages) * STAGE + col;
+    issue_chunk(c + kAdjStages - 1, s_issue);
+    s_issue = s_issue + 1 == kAdjStages ? 0 : s_issue + 1;
+    const float2* hs = hbuf + s_use * STAGE + col;
+    s_use = s_use + 1 == kAdjStages ? 0 : s_use + 1;
     const int j0 = c * JC;
-    const int jn = min(JC, nlines - j0);
-    for (int jj = 0; jj < jn; ++jj) {
+#pragma unroll
+    for (int jj = 0; jj < JC; ++jj) {
       const int j = j0 + jj;
+      if (j >= nlines) break;
       const float* e = Lt + j * LF;
       const float4 e0 = *reinterpret_cast<const float4*>(e);
       const float thi = e0.x, tlo = e0.y, trf = e0.z, tinh = e0.w;
       float2 H[TY];
+      {
+        const float2 h = hs[jj * NQ * 128];
 #pragma unroll
-      for (int ty = 0; ty < TY; ++ty) H[ty] = make_float2(0.f, 0.f);
+        for (int ty = 0; ty < TY; ++ty) H[ty] = make_float2(amp[ty][0] * h.x, amp[ty][0] * h.y);
+      }
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
+      for (int q = 1; q < NQ; ++q) {
         const float2 h = hs[(jj * NQ + q) * 128];
 #pragma unroll
         for (int ty = 0; ty < TY; ++ty) {
@@ -1526,7 +1542,9 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
     // 4 or 8), an even snx and 16-byte aligned h rows (cooperative 16-byte copies)
     int nq_all = n > 0 ? hu[0].ncoils : 0;
     for (int i = 0; i < n; ++i)
-      if (hu[i].ncoils != nq_all || (hu[i].snx & 1) || ((uintptr_t)hu[i].g & 15)) nq_all = 0;
+      if (hu[i].ncoils != nq_all || (hu[i].snx & 1) || ((uintptr_t)hu[i].g & 15) ||
+          (long long)hu[i].ncoils * hu[i].n_lines * hu[i].snx >= (1LL << 31))
+        nq_all = 0;
     if (nq_all != 1 && nq_all != 2 && nq_all != 4 && nq_all != 8) nq_all = 0;
     for (int pass = 0; pass < 4; ++pass) {
       bool maps = pass & 1, grads = pass & 2;
