@@ -231,8 +231,9 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms = torch.tensor([e0.elapsed_time(e1) / max(e2e_steps, 1)], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
-    h2d = sum(a.nbytes for a in host_imgs)
-    d2h = sum(v.nbytes for v in out.values() if v is not None)
+    # bytes that cross the host link per call (the library skips k-space rows the sampling never
+    # acquires and zero-fills them on the host)
+    h2d, d2h = op.host_bytes()
 
     fp32 = ctx.probe_fp32_tflops()
     pk, pk_kind = peaks()

@@ -317,6 +317,11 @@ int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace,
 int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images,
                                   float* kspace, float* comp_grad, float* fmap_grad,
                                   float* r2_grad);
+/* Bytes one mrsim_epi_operator_apply_host call moves between host and device with every input
+ * and output given: the images up; the acquired k-space rows (the other rows are zero-filled on
+ * the host when the acquired rows form a uniform stride, else every row) and the gradients down. */
+int mrsim_epi_operator_host_bytes(const mrsim_epi_operator* op, int64_t* upload_bytes,
+                                  int64_t* download_bytes);
 
 /* ---- the 3D echo trains (kspace3d.rs, readout.rs:75-322) ----------------------------------- */
 enum { MRSIM_KZ_CENTRIC = 0, MRSIM_KZ_LINEAR = 1 };                            /* readout.rs:75 */

@@ -250,6 +250,7 @@ def _declare(lib):
         "mrsim_probe_fp32_tflops": (C.c_int, [P, C.POINTER(C.c_double)]),
         "mrsim_epi_operator_adjoint_host": (C.c_int, [P, c_f32p, c_f32p, c_f32p, c_f32p]),
         "mrsim_epi_operator_apply_host": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
+        "mrsim_epi_operator_host_bytes": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "mrsim_spiral_tau_c": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, c_f64p]),
         "mrsim_spiral_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
                                               C.c_int64, c_f64p, c_f64p, C.POINTER(SpiralInfo_)]),

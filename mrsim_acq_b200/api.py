@@ -653,6 +653,13 @@ class EpiOperator:
                                                   p(out.get("fmap_grad")), p(out.get("r2_grad"))))
         return out
 
+    def host_bytes(self) -> tuple:
+        """(upload, download) bytes one `apply_host` call moves over the host link with every
+        output requested (acquired k-space rows only when they form a uniform stride)."""
+        up, down = C.c_int64(), C.c_int64()
+        check(lib().mrsim_epi_operator_host_bytes(self.handle, C.byref(up), C.byref(down)))
+        return int(up.value), int(down.value)
+
     def adjoint_host(self, kspace: np.ndarray) -> dict:
         """Synchronous adjoint / VJP of a host k-space (complex64, the k-space buffer's shape)."""
         shp = self.shapes()

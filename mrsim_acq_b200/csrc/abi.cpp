@@ -501,6 +501,20 @@ int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace,
   });
 }
 
+int mrsim_epi_operator_host_bytes(const mrsim_epi_operator* op, int64_t* upload_bytes, int64_t* download_bytes) {
+  return guarded([&] {
+    need(op, "operator");
+    need(upload_bytes, "upload_bytes");
+    need(download_bytes, "download_bytes");
+    const auto* o = op->impl;
+    const int64_t plane = (int64_t)o->snx * o->sny, units = (int64_t)o->nv * o->nz;
+    const int64_t rows = o->krow_n > 0 ? (int64_t)o->krow_n * o->n_echoes : (int64_t)o->n_echoes * o->ny;
+    *upload_bytes = units * o->ncomp * plane * 4;
+    *download_bytes = units * o->ncoils * rows * o->nx * 8 + units * o->ncomp * plane * 8 +
+                      (o->d_fmap_grad ? units * plane * 4 : 0) + (o->d_r2_grad ? units * o->ncomp * plane * 4 : 0);
+  });
+}
+
 int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images, float* kspace, float* comp_grad,
                                   float* fmap_grad, float* r2_grad) {
   if (!op) return guarded([] { need(nullptr, "operator"); });

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <thread>
 #include <tuple>
 
 #include "driver.h"
@@ -250,6 +251,21 @@ EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_inp
       }
   }
   op->n_lines = (int)lines.size();
+  {
+    // the acquired rows: the same arithmetic progression of ky in every echo?
+    std::vector<std::vector<int>> ky(ne);
+    for (const LineRec& L : lines) ky[L.row / ny].push_back(L.ky);
+    bool ok = !ky.empty() && !ky[0].empty();
+    for (int e = 1; e < ne && ok; ++e) ok = ky[e] == ky[0];
+    int step = 1;
+    if (ok && ky[0].size() > 1) step = ky[0][1] - ky[0][0];
+    for (size_t i = 1; ok && i < ky[0].size(); ++i) ok = ky[0][i] - ky[0][i - 1] == step;
+    if (ok && step >= 1 && ny % step == 0) {
+      op->krow0 = ky[0][0];
+      op->krow_step = step;
+      op->krow_n = (int)ky[0].size();
+    }
+  }
   op->samples_per_step = (int64_t)nv * nz * ncoils * (int64_t)lines.size() * nx;
 
   DevArena& A = op->arena;
@@ -465,10 +481,59 @@ void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* 
     MRSIM_CUDA(cudaMemcpy2DAsync((char*)host + off, pitch, (const char*)dev + off, pitch, (B.z1 - B.z0) * unit_bytes,
                                  B.g1 - B.g0, cudaMemcpyDeviceToHost, cs));
   };
+  // k-space: with a strided row pattern only the acquired rows cross PCIe (one pitched 3D copy per
+  // volume of a box: rows k0 + s i of every [unit][coil][echo] block of ny rows), and host threads
+  // zero the other rows of the output meanwhile
+  const int nx = o->nx, ny = o->ny;
+  const bool sparse_k = kspace && o->krow_n > 0;
+  const size_t row_bytes = (size_t)nx * sizeof(float2), blocks_per_unit = (size_t)o->ncoils * o->n_echoes;
+  auto down_k = [&](const Box& B) {
+    for (int g = B.g0; g < B.g1; ++g) {
+      const size_t off = ((size_t)g * nz + B.z0) * kunit * sizeof(float2) + (size_t)o->krow0 * row_bytes;
+      cudaMemcpy3DParms m;
+      std::memset(&m, 0, sizeof m);
+      m.srcPtr = make_cudaPitchedPtr((char*)o->d_kspace + off, o->krow_step * row_bytes, row_bytes, ny / o->krow_step);
+      m.dstPtr = make_cudaPitchedPtr((char*)kspace + off, o->krow_step * row_bytes, row_bytes, ny / o->krow_step);
+      m.extent = make_cudaExtent(row_bytes, o->krow_n, (size_t)(B.z1 - B.z0) * blocks_per_unit);
+      m.kind = cudaMemcpyDeviceToHost;
+      MRSIM_CUDA(cudaMemcpy3DAsync(&m, cs));
+    }
+  };
+  struct Joiner {
+    std::vector<std::thread> t;
+    ~Joiner() {
+      for (auto& th : t) th.join();
+    }
+  } zeroers;
+  if (sparse_k) {
+    const size_t nblocks = (size_t)nv * nz * blocks_per_unit;
+    std::vector<char> acquired(ny, 0);
+    for (int i = 0; i < o->krow_n; ++i) acquired[o->krow0 + i * o->krow_step] = 1;
+    const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    for (int t = 0; t < nt; ++t)
+      zeroers.t.emplace_back([=]() {
+        for (size_t b = nblocks * t / nt; b < nblocks * (t + 1) / nt; ++b) {
+          char* blk = (char*)kspace + b * ny * row_bytes;
+          for (int y = 0; y < ny;) {  // runs of rows that are not acquired
+            if (acquired[y]) {
+              ++y;
+              continue;
+            }
+            int y1 = y;
+            while (y1 < ny && !acquired[y1]) ++y1;
+            std::memset(blk + (size_t)y * row_bytes, 0, (size_t)(y1 - y) * row_bytes);
+            y = y1;
+          }
+        }
+      });
+  }
   for (int b = 0; b < ng; ++b) {
     const Box& B = boxes[b];
     MRSIM_CUDA(cudaStreamWaitEvent(cs, ev[3 * b + 1], 0));
-    if (kspace) down(B, kspace, o->d_kspace, kunit * sizeof(float2));
+    if (sparse_k)
+      down_k(B);
+    else if (kspace)
+      down(B, kspace, o->d_kspace, kunit * sizeof(float2));
     MRSIM_CUDA(cudaStreamWaitEvent(cs, ev[3 * b + 2], 0));
     if (comp_grad) down(B, comp_grad, o->d_comp_grad, o->ncomp * plane * sizeof(float2));
     if (fmap_grad && o->d_fmap_grad) down(B, fmap_grad, o->d_fmap_grad, plane * 4);

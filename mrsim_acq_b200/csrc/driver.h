@@ -49,6 +49,9 @@ struct EpiOperator {
   float* d_fmap_grad = nullptr;
   float* d_r2_grad = nullptr;
   std::unique_ptr<EpiPlan> plan;
+  // acquired k-space rows of every echo as k0 + s i (i < n) with ny % s == 0, or n = 0: the host
+  // call then downloads only those rows and zero-fills the others on the host
+  int krow0 = 0, krow_step = 0, krow_n = 0;
   // host-buffer apply: download and upload streams and per-group events, made on first use
   cudaStream_t copy_stream = nullptr, upload_stream = nullptr;
   std::vector<cudaEvent_t> events;

@@ -114,3 +114,28 @@ def test_apply_host_volume_groups_match_the_oracle(nv, nz, gpu_ctx):
         for g in range(nv):
             e = rel_l2(out[key][g], adj[key][g])
             assert e <= TOL, f"{key} volume {g}: rel-L2 {e:.2e}"
+
+
+def test_apply_host_fills_the_rows_it_does_not_download(gpu_ctx):
+    """The host call downloads only the acquired k-space rows when they form a uniform stride
+    and zero-fills the others on the host: outputs preset to garbage come back identical to
+    outputs preset to zero, with exact zeros outside the acquired rows."""
+    s, acq, tes, kw = _setup(eddy=False, nv=3, nz=2, coils=4)
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], 3, s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
+    clean = op.apply_host(s["images"])
+    shp = op.shapes()
+    dirty = {"kspace": np.full(shp["kspace"], np.nan + 1j * np.nan, np.complex64),
+             "comp_grad": np.full(shp["comp_grad"], 7.0, np.complex64),
+             "fmap_grad": np.full(shp["fmap_grad"], -3.0, np.float32),
+             "r2_grad": np.full(shp["r2_grad"], 5.0, np.float32)}
+    out = op.apply_host(s["images"], dirty)
+    for key in ("kspace", "comp_grad", "fmap_grad", "r2_grad"):
+        assert np.array_equal(out[key], clean[key]), key
+    mask = api.sampling_mask(s["acq_dims"][0], s["acq_dims"][1], acq).reshape(s["acq_dims"][1], -1)[:, 0]
+    assert np.all(out["kspace"][..., ~mask.astype(bool), :] == 0)
+    up, down = op.host_bytes()
+    assert up == sum(a.nbytes for a in s["images"])
+    rows = int(mask.sum()) * len(tes)
+    kbytes = 3 * 2 * 4 * rows * s["acq_dims"][0] * 8
+    assert down == kbytes + sum(clean[k].nbytes for k in ("comp_grad", "fmap_grad", "r2_grad"))
