@@ -360,12 +360,12 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
         if (PIECES % 256 == 0 || k < PIECES) {
           const int pl = k / (RC * 32), rem = k % (RC * 32);
           const int r = rem >> 5, c4 = (rem & 31) * 4;
+          // absent planes (no static phase, no distortion, compartments past ncomp) and rows
+          // or columns past the plane zero-fill: the row loop reads every plane unconditionally
           const float* base = plane_s[pl];
           const int y = c * RC + r, xx = x0 + c4;
-          if (base != nullptr) {
-            const bool ok = y < sny && xx < snx;
-            cp_async16(dst + (pl * RC + r) * 128 + c4, ok ? base + (size_t)y * snx + xx : base, ok ? 16 : 0);
-          }
+          const bool ok = base != nullptr && y < sny && xx < snx;
+          cp_async16(dst + (pl * RC + r) * 128 + c4, ok ? base + (size_t)y * snx + xx : (const float*)u.g, ok ? 16 : 0);
         }
       }
     }
@@ -441,7 +441,6 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
       for (int c = 0; c < NC; ++c) relr[j][MAPS ? 0 : c] = rel_s[jb + j][c];
     }
   }
-  const bool has_phase = plane_s[0] != nullptr, has_f = plane_s[1] != nullptr;
   const bool has_t2 = MAPS && plane_s[P_T2] != nullptr, has_ti = MAPS && plane_s[P_TI] != nullptr;
   const bool has_la = MAPS && plane_s[P_LA] != nullptr;
   float2 acc[T][QG];
@@ -458,11 +457,11 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
     const int rn = min(RC, sny - c * RC);
     for (int r = 0; r < rn; ++r) {
       const int y = c * RC + r;
-      const float a = has_phase ? S[(0 * RC + r) * 128] : 0.f;
-      const float f = has_f ? S[(1 * RC + r) * 128] : 0.f;
+      const float a = S[(0 * RC + r) * 128];
+      const float f = S[(1 * RC + r) * 128];
       float m[NC];
 #pragma unroll
-      for (int cc = 0; cc < NC; ++cc) m[cc] = cc < ncomp ? S[((P_COMP + cc) * RC + r) * 128] : 0.f;
+      for (int cc = 0; cc < NC; ++cc) m[cc] = S[((P_COMP + cc) * RC + r) * 128];
       float r2[MAPS ? NC : 1], r2i[MAPS ? NC : 1];
       float la = 0.f;
       if (MAPS) {
@@ -1474,9 +1473,9 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
              al16(u.timap) && al16(u.log_amp) && (u.ncomp <= 1 || u.comp_stride % 4 == 0) &&
              (u.ncomp <= 1 || (u.map_stride % 4) == 0);
       }
-      // eight coils with voxel maps (two or more compartments) or eight compartments take more
+      // eight coils with voxel maps (four or more compartments) or eight compartments take more
       // registers than the 256-thread CTA leaves: those shapes keep the per-thread-load kernel
-      if (p->qg == 8 && (p->nc == 8 || (pass == 1 && p->nc >= 2))) ok = false;
+      if (p->qg == 8 && (p->nc == 8 || (pass == 1 && p->nc >= 4))) ok = false;
       p->fwdq[pass] = ok;
     }
     for (int pass = 0; pass < 2; ++pass) {

@@ -31,10 +31,11 @@ def _setup(maps=False, eddy=True, gradient=False, nv=2, nz=2, ncomp=3, coils=4):
     return s, acq, tes, kw
 
 
-@pytest.mark.parametrize("maps,eddy,gradient", [(False, False, False), (False, True, False), (True, True, False),
-                                                (False, True, True)])
-def test_series_forward_and_adjoint_match_the_oracle(maps, eddy, gradient, gpu_ctx):
-    s, acq, tes, kw = _setup(maps, eddy, gradient)
+@pytest.mark.parametrize("maps,eddy,gradient,coils", [(False, False, False, 4), (False, True, False, 4),
+                                                      (True, True, False, 4), (False, True, True, 4),
+                                                      (True, False, False, 8), (False, False, False, 8)])
+def test_series_forward_and_adjoint_match_the_oracle(maps, eddy, gradient, coils, gpu_ctx):
+    s, acq, tes, kw = _setup(maps, eddy, gradient, coils=coils)
     op = api.EpiOperator(s["sim_dims"], s["acq_dims"], s["n_volumes"], s["t2"], s["fmap"], acq, images=s["images"],
                          echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
     out = op.apply_host(None)
