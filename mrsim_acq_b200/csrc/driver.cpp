@@ -134,6 +134,23 @@ GeoTab build_geo(DevArena& arena, int snx, int sny, int nx, int ny, int ncoils, 
     }
     g.xf = (const float2*)arena.upload(xf.data(), xf.size() * sizeof(float2), st);
   }
+  {
+    // coil classes of bitwise-equal ey rows
+    std::vector<int> cls(ncoils, -1);
+    std::vector<float> eyc;
+    int ncls = 0;
+    for (int q = 0; q < ncoils; ++q) {
+      for (int q2 = 0; q2 < q && cls[q] < 0; ++q2)
+        if (std::memcmp(&ey[(size_t)q * sny], &ey[(size_t)q2 * sny], sizeof(float) * sny) == 0) cls[q] = cls[q2];
+      if (cls[q] < 0) {
+        cls[q] = ncls++;
+        eyc.insert(eyc.end(), ey.begin() + (size_t)q * sny, ey.begin() + (size_t)(q + 1) * sny);
+      }
+    }
+    g.ncls = ncls;
+    g.cls = (const int*)arena.upload(cls.data(), cls.size() * sizeof(int), st);
+    g.eyc = (const float*)arena.upload(eyc.data(), eyc.size() * 4, st);
+  }
   g.ex = (const float*)arena.upload(ex.data(), ex.size() * 4, st);
   g.ey = (const float*)arena.upload(ey.data(), ey.size() * 4, st);
   g.tw = (const float2*)arena.upload(tw.data(), tw.size() * sizeof(float2), st);

@@ -313,16 +313,20 @@ __host__ __device__ __forceinline__ constexpr int fwdq_rows(int nc, bool maps) {
   return fwdq_planes(nc, maps) <= 5 ? 8 : fwdq_planes(nc, maps) <= 12 ? 4 : 2;
 }
 
-template <int QG, int NC, bool MAPS>
+// NV > 0: the tile holds every coil of the unit and accumulates coil classes instead of coils
+// (NV = classes + 1 for the coil offset): acc_v += ey_v(y) W P, acc_off += W P, and the epilogue
+// expands g_q = s (ex_q acc_cls(q) + off acc_off).
+template <int QG, int NV, int NC, bool MAPS>
 __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __restrict__ units,
                                                           const Tile* __restrict__ tiles) {
   constexpr int T = 4, TL = 8;
+  constexpr int NA = NV ? NV : QG;             // accumulators per line
   constexpr int NPL = fwdq_planes(NC, MAPS);
   constexpr int RC = fwdq_rows(NC, MAPS);
   constexpr int STAGE = NPL * RC * 128;        // floats per stage
   constexpr int PIECES = NPL * RC * 32;        // 16-byte pieces per stage
   constexpr int PPT = (PIECES + 255) / 256;
-  constexpr int QGP = (QG + 3) / 4 * 4;
+  constexpr int QGP = (NA + 3) / 4 * 4;
   // plane order: 0 static phase, 1 fieldmap, 2.. compartments, then T2, T2' maps and log amplitude
   constexpr int P_COMP = 2, P_T2 = 2 + NC, P_TI = 2 + 2 * NC, P_LA = 2 + 3 * NC;
   extern __shared__ __align__(16) float smem[];
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
   const Tile tl = tiles[blockIdx.x];
   const UnitDesc& u = units[tl.unit];
   const int snx = u.snx, sny = u.sny, ncomp = u.ncomp;
-  float* Ey = Bt + sny * TL;                    // [sny][QGP]
+  float* Ey = Bt + sny * TL;                    // [sny][QGP]: ey per coil, or per class and 1
   __shared__ const float* plane_s[NPL];
   __shared__ float rel_s[TL][kMaxComp];
   __shared__ float tinh_s[TL], trf_s[TL], thi_s[TL], tlo_s[TL];
@@ -398,8 +402,13 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
   }
   for (int idx = tid; idx < QGP * sny; idx += 256) {
     const int y = idx / QGP, qq = idx % QGP;
-    const int q = tl.q0 + qq;
-    Ey[idx] = (qq < QG && q < u.ncoils) ? u.geo.ey[(size_t)q * sny + y] : 0.f;
+    if (NV) {
+      const int nc = u.geo.ncls;
+      Ey[idx] = qq < nc ? u.geo.eyc[(size_t)qq * sny + y] : (qq == nc ? 1.f : 0.f);
+    } else {
+      const int q = tl.q0 + qq;
+      Ey[idx] = (qq < QG && q < u.ncoils) ? u.geo.ey[(size_t)q * sny + y] : 0.f;
+    }
   }
   if (tid < TL) {
     const int j = tid;
@@ -422,11 +431,13 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
   const int x = x0 + col;
   const bool xok = x < snx;
   const float off = u.geo.coil_off;
-  float exq[QG];
+  float exq[NV ? 1 : QG];
+  if (!NV) {
 #pragma unroll
-  for (int qq = 0; qq < QG; ++qq) {
-    const int q = tl.q0 + qq;
-    exq[qq] = (xok && q < u.ncoils) ? u.geo.ex[(size_t)q * snx + x] : 0.f;
+    for (int qq = 0; qq < QG; ++qq) {
+      const int q = tl.q0 + qq;
+      exq[NV ? 0 : qq] = (xok && q < u.ncoils) ? u.geo.ex[(size_t)q * snx + x] : 0.f;
+    }
   }
   float thi[T], tlo[T], relr[T][MAPS ? 1 : NC], trf[MAPS ? T : 1], tinh[MAPS ? T : 1];
 #pragma unroll
@@ -443,11 +454,11 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
   }
   const bool has_t2 = MAPS && plane_s[P_T2] != nullptr, has_ti = MAPS && plane_s[P_TI] != nullptr;
   const bool has_la = MAPS && plane_s[P_LA] != nullptr;
-  float2 acc[T][QG];
+  float2 acc[T][NA];
 #pragma unroll
   for (int j = 0; j < T; ++j)
 #pragma unroll
-    for (int qq = 0; qq < QG; ++qq) acc[j][qq] = make_float2(0.f, 0.f);
+    for (int qq = 0; qq < NA; ++qq) acc[j][qq] = make_float2(0.f, 0.f);
 
   for (int c = 0; c < nch; ++c) {
     cp_async_wait_n<kFwdStages - 2>();
@@ -477,14 +488,14 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
         }
         if (has_la) la = S[(P_LA * RC + r) * 128];
       }
-      float amp[QG];
+      float amp[NA];
 #pragma unroll
       for (int q4 = 0; q4 < QGP; q4 += 4) {
         const float4 e4 = *reinterpret_cast<const float4*>(Ey + y * QGP + q4);
         const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-          if (q4 + k < QG) amp[q4 + k] = fmaf(exq[q4 + k], ev[k], off);
+          if (q4 + k < NA) amp[q4 + k] = NV ? ev[k] : fmaf(exq[NV ? 0 : q4 + k], ev[k], off);
       }
       const float4 b4 = *reinterpret_cast<const float4*>(Bt + y * TL + jb);
       const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
@@ -508,9 +519,14 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
         }
         const float wr = W * cs, wi = W * sn;
 #pragma unroll
-        for (int qq = 0; qq < QG; ++qq) {
-          acc[j][qq].x = fmaf(amp[qq], wr, acc[j][qq].x);
-          acc[j][qq].y = fmaf(amp[qq], wi, acc[j][qq].y);
+        for (int qq = 0; qq < NA; ++qq) {
+          if (NV && qq == NA - 1) {  // the coil-offset row is all ones
+            acc[j][qq].x += wr;
+            acc[j][qq].y += wi;
+          } else {
+            acc[j][qq].x = fmaf(amp[qq], wr, acc[j][qq].x);
+            acc[j][qq].y = fmaf(amp[qq], wi, acc[j][qq].y);
+          }
         }
       }
     }
@@ -518,6 +534,24 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
   cp_async_wait0();
   if (!xok) return;
   const float s = u.signal_scale;
+  if (NV) {
+    // expand the classes to the unit's coils (all in this tile)
+    for (int q = 0; q < u.ncoils; ++q) {
+      const int cl = u.geo.cls[q];
+      const float e = s * u.geo.ex[(size_t)q * snx + x], o = s * off;
+#pragma unroll
+      for (int j = 0; j < T; ++j) {
+        float2 v = acc[j][0];
+#pragma unroll
+        for (int k = 1; k < NA - 1; ++k)
+          if (cl == k) v = acc[j][k];
+        if (jb + j < nl)
+          u.g[((size_t)q * u.n_lines + tl.line0 + jb + j) * snx + x] =
+              make_float2(fmaf(e, v.x, o * acc[j][NA - 1].x), fmaf(e, v.y, o * acc[j][NA - 1].y));
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int qq = 0; qq < QG; ++qq) {
     const int q = tl.q0 + qq;
@@ -1477,6 +1511,14 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       // registers than the 256-thread CTA leaves: those shapes keep the per-thread-load kernel
       if (p->qg == 8 && (p->nc == 8 || (pass == 1 && p->nc >= 4))) ok = false;
       p->fwdq[pass] = ok;
+      // coil classes: every unit with the same 8 coils in 5 classes (the ring) -> 6 accumulators
+      bool cl = ok && n > 0 && p->qg == 8 && (pass == 0 || p->nc <= 3);
+      for (int i = 0; i < n && cl; ++i) {
+        const UnitDesc& u = hu[i];
+        if (((u.flags & UF_MAPS) != 0) != (pass == 1)) continue;
+        cl = u.ncoils == 8 && u.geo.ncls == 5 && u.geo.coil_off != 0.f && u.geo.cls && u.geo.eyc;
+      }
+      p->fwd_nv[pass] = cl ? 6 : 0;
     }
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<int4> tiles;
@@ -1613,16 +1655,19 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
       const size_t smq = sizeof(float) * ((size_t)kFwdStages * fwdq_planes(NCv, maps) * fwdq_rows(NCv, maps) * 128 +
                                           (size_t)p->max_sny * (8 + (QG + 3) / 4 * 4));
       bool launched = false;
-#define MRSIM_YF(QGV, NCV, M)                                                           \
-  if (QG == QGV && NCv == NCV && maps == M) {                                           \
-    auto k = ystage_q_kernel<QGV, NCV, M>;                                              \
+      const int NVv = p->fwd_nv[pass];
+#define MRSIM_YF(QGV, NVV, NCV, M)                                                      \
+  if (QG == QGV && NVv == NVV && NCv == NCV && maps == M) {                             \
+    auto k = ystage_q_kernel<QGV, NVV, NCV, M>;                                         \
     set_smem(k, smq);                                                                   \
     k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                              \
     launched = true;                                                                    \
   }
-#define MRSIM_YFQ(NCV, M) MRSIM_YF(1, NCV, M) MRSIM_YF(2, NCV, M) MRSIM_YF(4, NCV, M) MRSIM_YF(8, NCV, M)
+#define MRSIM_YFQ(NCV, M) MRSIM_YF(1, 0, NCV, M) MRSIM_YF(2, 0, NCV, M) MRSIM_YF(4, 0, NCV, M) MRSIM_YF(8, 0, NCV, M)
 #define MRSIM_YFN(M) MRSIM_YFQ(1, M) MRSIM_YFQ(2, M) MRSIM_YFQ(3, M) MRSIM_YFQ(4, M) MRSIM_YFQ(8, M)
       MRSIM_YFN(false) MRSIM_YFN(true)
+      MRSIM_YF(8, 6, 1, false) MRSIM_YF(8, 6, 2, false) MRSIM_YF(8, 6, 3, false) MRSIM_YF(8, 6, 4, false)
+      MRSIM_YF(8, 6, 1, true) MRSIM_YF(8, 6, 2, true) MRSIM_YF(8, 6, 3, true)
 #undef MRSIM_YFN
 #undef MRSIM_YFQ
 #undef MRSIM_YF

@@ -52,6 +52,11 @@ struct GeoTab {
   // x-stage FFT tables when snx is a power of two (else NULL): [snx/2] e^{-i2pi k/snx}, then
   // [pol 0/1][x] e^{i2pi gh (x-c)/snx}, then [kx] e^{-i2pi (kx-xs) c/snx}
   const float2* xf;
+  // coil classes: coils whose ey rows are bitwise equal share a class (a ring of 8 coils has 5),
+  // so sum_q amp_q(x,y) v = sum_d ey_d(y) (sum_{q in d} ex_q v) + off sum v.  ncls = 0: none.
+  int ncls;
+  const int* cls;     // [coil] class index
+  const float* eyc;   // [class][sny] the class rows
 };
 
 // One unit of work: one slice of one volume, all echoes.  Device pointers throughout.
@@ -157,6 +162,8 @@ struct EpiPlan {
   int n_ftiles = 0;
   // forward y-stage pass (maps) served by the staged-input kernel (8 lines per tile)
   bool fwdq[2] = {false, false};
+  // ... and accumulating coil classes: their count plus the coil offset row, or 0
+  int fwd_nv[2] = {0, 0};
   // y-adjoint pass (maps | grads << 1) served by the fixed-coil-count kernel: its coil count, or 0
   // for the general kernel
   int adjq[4] = {0, 0, 0, 0};
