@@ -796,7 +796,9 @@ __host__ __device__ __forceinline__ constexpr int adjq_line_floats(int nc, bool 
 __host__ __device__ __forceinline__ constexpr int adjq_rows(int nc, bool maps) { return !maps && nc <= 3 ? 4 : 2; }
 
 
-template <int NQ, int TY, int NC, bool MAPS, bool GRADS>
+// VIRT: the h rows are the NQ = classes + 1 class rows of the class-mode x-adjoint (scale, ex and
+// the coil offset already applied), so amp_v(y) = ey_v(y) for the classes and 1 for the offset row.
+template <int NQ, int TY, int NC, bool MAPS, bool GRADS, bool VIRT>
 __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __restrict__ units,
                                                             const int4* __restrict__ tiles) {
   extern __shared__ __align__(16) float smem[];
@@ -906,11 +908,14 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
   float r2[TY][MAPS ? NC : 1], r2i[TY][MAPS ? NC : 1], la[TY];
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
-    const float ex = u.geo.ex[(size_t)q * snx + xs_];
+    const float ex = VIRT ? 0.f : u.geo.ex[(size_t)q * snx + xs_];
 #pragma unroll
     for (int ty = 0; ty < TY; ++ty) {
       const int y = min(y0 + rg * TY + ty, sny - 1);
-      amp[ty][q] = s * fmaf(ex, u.geo.ey[(size_t)q * sny + y], off);
+      if (VIRT)
+        amp[ty][q] = q < NQ - 1 ? u.geo.eyc[(size_t)q * sny + y] : 1.f;
+      else
+        amp[ty][q] = s * fmaf(ex, u.geo.ey[(size_t)q * sny + y], off);
     }
   }
 #pragma unroll
@@ -1276,12 +1281,19 @@ __host__ __device__ constexpr int bitrev_c(int v, int bits) {
 }
 __host__ __device__ constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
 
-template <int E, bool ADJ>
+// CLS (adjoint, 8 coils in 5 classes + offset): a tile is (unit, first line, up to 4 lines) x all
+// 8 coils, warp w transforms coil w of each line into shared memory, and the CTA then writes the
+// 6 class rows G_v = s sum_{q in v} ex_q h_q, G_off = s off sum_q h_q ([v][line][x] in g) that
+// the class-mode y-adjoint combines as sum_v ey_v(y) G_v + G_off.
+template <int E, bool ADJ, bool CLS>
 __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const UnitDesc* __restrict__ units,
                                                            const int4* __restrict__ tiles) {
   constexpr int N = 32 * E, LE = log2_c(E);
   constexpr int NP = N + N / 32;  // padded row
   constexpr int RT = 32;          // rows per tile
+  static_assert(!CLS || (ADJ && E <= 4), "coil classes: adjoint rows of at most 128 points");
+  __shared__ __align__(16) float2 hsm[CLS ? 4 * 8 * N : 1];  // [line][coil][x]
+  __shared__ int cls_s[8];
   __shared__ __align__(16) float2 tw[N];        // e^{-i2pi j/N}
   __shared__ __align__(16) float2 pm[2 * N];    // premodulation per polarity
   __shared__ __align__(16) float2 pt[N];        // post-twiddle per kx (nx <= N)
@@ -1290,7 +1302,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   __shared__ float rdec[RT];
   const int4 t = tiles[blockIdx.x];
   const UnitDesc& u = units[t.x];
-  const int r0 = t.y, nr = t.z;
+  const int r0 = t.y, nr = CLS ? 8 * t.z : t.z;  // CLS: first line, lines
   const int nx = u.nx, nl = u.n_lines;
   const float2* __restrict__ xf = u.geo.xf;
   for (int k = threadIdx.x; k < N / 2; k += 256) {
@@ -1300,8 +1312,9 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   }
   for (int k = threadIdx.x; k < 2 * N; k += 256) pm[k] = xf[N / 2 + k];
   for (int k = threadIdx.x; k < nx; k += 256) pt[k] = xf[N / 2 + 2 * N + k];
+  if (CLS && threadIdx.x < 8) cls_s[threadIdx.x] = u.geo.cls[threadIdx.x];
   for (int r = threadIdx.x; r < nr; r += 256) {
-    const int R = r0 + r;
+    const int R = CLS ? (r & 7) * nl + r0 + (r >> 3) : r0 + r;  // CLS: row r = (line r / 8, coil r % 8)
     const LineRec& L = u.lines[R % nl];
     rq[r] = R / nl;
     rrow[r] = L.row;
@@ -1335,7 +1348,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     return md;
   };
   for (int r = warp; r < nr; r += 8) {
-    const int R = r0 + r, q = rq[r], orow = rrow[r], pol = rpol[r];
+    const int R = CLS ? (r & 7) * nl + r0 + (r >> 3) : r0 + r, q = rq[r], orow = rrow[r], pol = rpol[r];
     const float dec = rdec[r];
     float2 b[E];
     if (!ADJ) {
@@ -1404,7 +1417,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
         out[kx] = make_float2(v.x * inv_n, v.y * inv_n);
       }
     } else {
-      float2* gr = u.g + (size_t)R * N;
+      float2* gr = CLS ? hsm + ((r >> 3) * 8 + (r & 7)) * N : u.g + (size_t)R * N;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
@@ -1414,6 +1427,34 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
       }
     }
     __syncwarp();
+  }
+  if (CLS) {
+    __syncthreads();
+    const float s = u.signal_scale, so = s * u.geo.coil_off;
+    const int nj = nr >> 3;
+    for (int e = threadIdx.x; e < nj * N; e += 256) {
+      const int jl = e >> LE >> 5, x = e & (N - 1);
+      float2 G[6];
+#pragma unroll
+      for (int v = 0; v < 6; ++v) G[v] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float2 h = hsm[(jl * 8 + q) * N + x];
+        const float ex = s * u.geo.ex[(size_t)q * N + x];
+        const int c = cls_s[q];
+#pragma unroll
+        for (int v = 0; v < 5; ++v)
+          if (c == v) {
+            G[v].x = fmaf(ex, h.x, G[v].x);
+            G[v].y = fmaf(ex, h.y, G[v].y);
+          }
+        G[5].x += h.x;
+        G[5].y += h.y;
+      }
+      G[5] = make_float2(so * G[5].x, so * G[5].y);
+#pragma unroll
+      for (int v = 0; v < 6; ++v) u.g[((size_t)v * nl + r0 + jl) * N + x] = G[v];
+    }
   }
 }
 
@@ -1605,6 +1646,29 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->n_atiles[pass] = (int)yt.size();
       p->d_atiles[pass] = (int4*)dev_upload(p, yt.data(), sizeof(int4) * yt.size());
     }
+    // coil classes in the adjoint: every unit has the 8-coil ring (5 classes + offset), rows of
+    // at most 128 points in the warp FFT, and the fixed-count y-adjoint for its shape
+    {
+      bool cl = n > 0 && p->xfft && p->xfft_e >= 1 && p->xfft_e <= 4 && p->nc <= 4 && nq_all == 8;
+      for (int i = 0; i < n && cl; ++i) {
+        const UnitDesc& u = hu[i];
+        cl = u.ncoils == 8 && u.geo.ncls == 5 && u.geo.coil_off != 0.f && u.geo.cls && u.geo.eyc;
+      }
+      for (int pass = 0; pass < 4 && cl; ++pass) cl = p->adjq[pass] == 8;
+      if (cl) {
+        std::vector<int4> ct;
+        p->c_start.assign(n + 1, 0);
+        for (int i = 0; i < n; ++i) {
+          p->c_start[i] = (int)ct.size();
+          for (int j0 = 0; j0 < hu[i].n_lines; j0 += 4) ct.push_back(make_int4(i, j0, std::min(4, hu[i].n_lines - j0), 0));
+        }
+        p->c_start[n] = (int)ct.size();
+        p->n_ctiles = (int)ct.size();
+        p->d_ctiles = (int4*)dev_upload(p, ct.data(), sizeof(int4) * ct.size());
+        p->adj_cls = true;
+        for (int pass = 0; pass < 4; ++pass) p->adjq[pass] = 6;
+      }
+    }
   } catch (...) {
     delete p;
     throw;
@@ -1697,6 +1761,19 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
 
 namespace {
 void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) {
+  if (adj && p->adj_cls) {
+    const TileRange R = tile_range(p->c_start, p->n_ctiles, u0, u1);
+    if (R.n == 0) return;
+    const int4* tiles = p->d_ctiles + R.t0;
+    const unsigned g = (unsigned)R.n;
+    switch (p->xfft_e) {
+      case 1: xfft_warp_kernel<1, true, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;
+      case 2: xfft_warp_kernel<2, true, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;
+      default: xfft_warp_kernel<4, true, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;
+    }
+    MRSIM_CUDA(cudaGetLastError());
+    return;
+  }
   if (p->xfft) {
     const TileRange R = tile_range(p->f_start, p->n_ftiles, u0, u1);
     if (R.n == 0) return;
@@ -1704,10 +1781,10 @@ void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) 
     const unsigned g = (unsigned)R.n;
 #define MRSIM_XF(ADJ)                                                                             \
   switch (p->xfft_e) {                                                                            \
-    case 1: xfft_warp_kernel<1, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
-    case 2: xfft_warp_kernel<2, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
-    case 4: xfft_warp_kernel<4, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
-    case 8: xfft_warp_kernel<8, ADJ><<<g, 256, 0, st>>>(p->d_units, tiles); break;                \
+    case 1: xfft_warp_kernel<1, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+    case 2: xfft_warp_kernel<2, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+    case 4: xfft_warp_kernel<4, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+    case 8: xfft_warp_kernel<8, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
     default: xfft_kernel<ADJ><<<g, 256, 0, st>>>(p->d_units, tiles);                              \
   }
     if (adj) {
@@ -1747,20 +1824,27 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
       const size_t smq = sizeof(float2) * (size_t)kAdjStages * adjq_chunk_lines(NQv) * NQv * 128 +
                          sizeof(float) * (size_t)p->max_lines * (2 * adjq_rows(NCv, maps) + adjq_line_floats(NCv, maps));
       bool launched = false;
-#define MRSIM_AQ(NQV, NCV, M, G)                                                        \
-  if (NQv == NQV && NCv == NCV && maps == M && grads == G) {                            \
-    auto k = yadjoint_q_kernel<NQV, adjq_rows(NCV, M), NCV, M, G>;                      \
+      const bool virt = p->adj_cls;
+#define MRSIM_AQV(NQV, NCV, M, G, V)                                                    \
+  if (NQv == NQV && NCv == NCV && maps == M && grads == G && virt == V) {               \
+    auto k = yadjoint_q_kernel<NQV, adjq_rows(NCV, M), NCV, M, G, V>;                   \
     set_smem(k, smq);                                                                   \
     k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                              \
     launched = true;                                                                    \
   }
+#define MRSIM_AQ(NQV, NCV, M, G) MRSIM_AQV(NQV, NCV, M, G, false)
 #define MRSIM_AQC(NCV, M, G) MRSIM_AQ(1, NCV, M, G) MRSIM_AQ(2, NCV, M, G) MRSIM_AQ(4, NCV, M, G) MRSIM_AQ(8, NCV, M, G)
 #define MRSIM_AQN(M, G) MRSIM_AQC(1, M, G) MRSIM_AQC(2, M, G) MRSIM_AQC(3, M, G) MRSIM_AQC(4, M, G)
+#define MRSIM_AQK(M, G) MRSIM_AQV(6, 1, M, G, true) MRSIM_AQV(6, 2, M, G, true) MRSIM_AQV(6, 3, M, G, true) \
+  MRSIM_AQV(6, 4, M, G, true)
       MRSIM_AQN(false, false) MRSIM_AQN(true, false) MRSIM_AQN(false, true) MRSIM_AQN(true, true)
       MRSIM_AQC(8, false, false) MRSIM_AQC(8, false, true)
+      MRSIM_AQK(false, false) MRSIM_AQK(true, false) MRSIM_AQK(false, true) MRSIM_AQK(true, true)
+#undef MRSIM_AQK
 #undef MRSIM_AQN
 #undef MRSIM_AQC
 #undef MRSIM_AQ
+#undef MRSIM_AQV
       if (!launched) fail("no adjoint kernel instance for this unit shape");
       MRSIM_CUDA(cudaGetLastError());
       continue;

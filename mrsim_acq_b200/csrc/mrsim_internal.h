@@ -158,6 +158,12 @@ struct EpiPlan {
   // x-stage as per-row FFTs (every unit has a power-of-two snx and FFT tables): tiles of rows
   bool xfft = false;
   int xfft_e = 0;  // > 0: every unit has snx = 32 * xfft_e and the warp-per-row FFT runs
+  // coil classes in the adjoint: the x-adjoint writes class rows (tiles of 4 lines x 8 coils) and
+  // the y-adjoint combines 6 rows instead of 8 coils
+  bool adj_cls = false;
+  int4* d_ctiles = nullptr;
+  int n_ctiles = 0;
+  std::vector<int> c_start;
   int4* d_ftiles = nullptr;
   int n_ftiles = 0;
   // forward y-stage pass (maps) served by the staged-input kernel (8 lines per tile)
