@@ -30,6 +30,10 @@
 
 #include "mrsim_internal.h"
 
+// Template flags select whole code paths (packed or scalar, class or coil accumulators); the paths
+// an instance does not take leave loops the front end reports as unreachable.
+#pragma nv_diag_suppress 128
+
 namespace mrsim {
 
 namespace {
@@ -49,6 +53,55 @@ __device__ __forceinline__ float ft_turns(float f, float t_hi, float t_lo) {
   float e = fmaf(f, t_hi, -p);      // exact error of the product
   float r = __fadd_rn(p, -round_fadd(p));  // exact
   return r + fmaf(f, t_lo, e);
+}
+
+// Packed FP32 pairs (sm_100 add/sub/mul/fma.rn.f32x2): one instruction for two lanes, each lane
+// rounding exactly like the scalar operation, so a packed computation is bitwise the scalar one.
+__device__ __forceinline__ unsigned long long pk2(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+  float2 d;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(r));
+  return d;
+}
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(c)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+// frac_turn and ft_turns on a pair of lanes.  ft_turns2 takes -f (nf) so that no lane needs a
+// negation: fma(-f, t_hi, p) = -e and fma(-f, t_lo, -e) = -(f t_lo + e) exactly (round to nearest
+// is symmetric), and r - (-(f t_lo + e)) = r + (f t_lo + e).
+__device__ __forceinline__ float2 frac_turn2(float2 v) {
+  const float2 M = dup2(12582912.0f);
+  return fsub2(v, fsub2(fadd2(v, M), M));
+}
+__device__ __forceinline__ float2 ft_turns2(float2 f, float2 nf, float2 t_hi, float2 t_lo) {
+  const float2 M = dup2(12582912.0f);
+  const float2 p = fmul2(f, t_hi);
+  const float2 en = ffma2(nf, t_hi, p);                // -(exact error of the product)
+  const float2 r = fsub2(p, fsub2(fadd2(p, M), M));    // exact
+  return fsub2(r, ffma2(nf, t_lo, en));
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -499,6 +552,32 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
       }
       const float4 b4 = *reinterpret_cast<const float4*>(Bt + y * TL + jb);
       const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
+      if (NV && !MAPS) {
+        // lines (0, 1) and (2, 3) as packed pairs: the same arithmetic, two lanes per instruction
+        const float2 a2 = dup2(a), f2 = dup2(f), nf2 = dup2(-f);
+#pragma unroll
+        for (int jp = 0; jp < T; jp += 2) {
+          float2 th = fadd2(fadd2(a2, make_float2(bt[jp], bt[jp + 1])),
+                            ft_turns2(f2, nf2, make_float2(thi[jp], thi[jp + 1]), make_float2(tlo[jp], tlo[jp + 1])));
+          th = fmul2(dup2(kTwoPiF), frac_turn2(th));
+          float s0, c0, s1, c1;
+          __sincosf(th.x, &s0, &c0);
+          __sincosf(th.y, &s1, &c1);
+          float2 W = fmul2(make_float2(relr[jp][MAPS ? 0 : 0], relr[jp + 1][MAPS ? 0 : 0]), dup2(m[0]));
+#pragma unroll
+          for (int cc = 1; cc < NC; ++cc)
+            W = ffma2(make_float2(relr[jp][MAPS ? 0 : cc], relr[jp + 1][MAPS ? 0 : cc]), dup2(m[cc]), W);
+          const float2 w0 = fmul2(dup2(W.x), make_float2(c0, s0)), w1 = fmul2(dup2(W.y), make_float2(c1, s1));
+#pragma unroll
+          for (int qq = 0; qq < NA - 1; ++qq) {
+            acc[jp][qq] = ffma2(dup2(amp[qq]), w0, acc[jp][qq]);
+            acc[jp + 1][qq] = ffma2(dup2(amp[qq]), w1, acc[jp + 1][qq]);
+          }
+          acc[jp][NA - 1] = fadd2(acc[jp][NA - 1], w0);
+          acc[jp + 1][NA - 1] = fadd2(acc[jp + 1][NA - 1], w1);
+        }
+        continue;
+      }
 #pragma unroll
       for (int j = 0; j < T; ++j) {
         float th = a + bt[j] + ft_turns(f, thi[j], tlo[j]);
@@ -523,6 +602,8 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
           if (NV && qq == NA - 1) {  // the coil-offset row is all ones
             acc[j][qq].x += wr;
             acc[j][qq].y += wi;
+          } else if (NV) {
+            acc[j][qq] = ffma2(make_float2(amp[qq], amp[qq]), make_float2(wr, wi), acc[j][qq]);
           } else {
             acc[j][qq].x = fmaf(amp[qq], wr, acc[j][qq].x);
             acc[j][qq].y = fmaf(amp[qq], wi, acc[j][qq].y);
@@ -938,6 +1019,16 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
       }
     }
   }
+  // PK (class rows, class decay, 4 rows): rows (0, 1) and (2, 3) run as packed f32x2 pairs, with
+  // accumulators pcx/pcy/puy/pvx[pair][c] holding the two rows' Re/Im comp sums, t- and trf-sums
+  constexpr bool PK = VIRT && !MAPS && TY == 4;
+  float2 pcx[PK ? 2 : 1][NC], pcy[PK ? 2 : 1][NC], puy[PK ? 2 : 1][NC], pvx[PK ? 2 : 1][NC];
+  if (PK) {
+#pragma unroll
+    for (int pp = 0; pp < (PK ? 2 : 1); ++pp)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) pcx[pp][c] = pcy[pp][c] = puy[pp][c] = pvx[pp][c] = make_float2(0.f, 0.f);
+  }
   float2 cg[TY][NC];
   float Uy[TY][GRADS ? NC : 1], Vx[TY][GRADS ? NC : 1];
 #pragma unroll
@@ -964,6 +1055,56 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
       const float* e = Lt + j * LF;
       const float4 e0 = *reinterpret_cast<const float4*>(e);
       const float thi = e0.x, tlo = e0.y, trf = e0.z, tinh = e0.w;
+      if (PK) {
+        float2 Hx[2], Hy[2];  // [pair] = rows (2p, 2p + 1)
+        {
+          const float2 h = hs[jj * NQ * 128];
+#pragma unroll
+          for (int pp = 0; pp < 2; ++pp) {
+            const float2 am = make_float2(amp[2 * pp][0], amp[(2 * pp + 1) % TY][0]);
+            Hx[pp] = fmul2(am, dup2(h.x));
+            Hy[pp] = fmul2(am, dup2(h.y));
+          }
+        }
+#pragma unroll
+        for (int q = 1; q < NQ; ++q) {
+          const float2 h = hs[(jj * NQ + q) * 128];
+          const float2 hx = dup2(h.x), hy = dup2(h.y);
+#pragma unroll
+          for (int pp = 0; pp < 2; ++pp) {
+            const float2 am = make_float2(amp[2 * pp][q], amp[(2 * pp + 1) % TY][q]);
+            Hx[pp] = ffma2(am, hx, Hx[pp]);
+            Hy[pp] = ffma2(am, hy, Hy[pp]);
+          }
+        }
+        const float4 b4 = *reinterpret_cast<const float4*>(Bt + j * ROWS + rg * TY);
+        const float2 thi2 = dup2(thi), tlo2 = dup2(tlo);
+#pragma unroll
+        for (int pp = 0; pp < 2; ++pp) {
+          const int t0 = 2 * pp, t1 = (2 * pp + 1) % TY;
+          const float2 bt2 = pp == 0 ? make_float2(b4.x, b4.y) : make_float2(b4.z, b4.w);
+          float2 th = fadd2(fadd2(make_float2(a[t0], a[t1]), bt2),
+                            ft_turns2(make_float2(f[t0], f[t1]), make_float2(-f[t0], -f[t1]), thi2, tlo2));
+          th = fmul2(dup2(kTwoPiF), frac_turn2(th));
+          float s0, c0, s1, c1;
+          __sincosf(th.x, &s0, &c0);
+          __sincosf(th.y, &s1, &c1);
+          const float2 cs2 = make_float2(c0, c1), sn2 = make_float2(s0, s1);
+          const float2 zr = ffma2(cs2, Hx[pp], fmul2(sn2, Hy[pp]));  // Z = conj(P) H per row
+          const float2 zi = ffma2(cs2, Hy[pp], fsub2(dup2(0.f), fmul2(sn2, Hx[pp])));
+#pragma unroll
+          for (int cc = 0; cc < NC; ++cc) {
+            const float2 r = dup2(e[4 + cc]);
+            pcx[PK ? pp : 0][cc] = ffma2(r, zr, pcx[PK ? pp : 0][cc]);
+            pcy[PK ? pp : 0][cc] = ffma2(r, zi, pcy[PK ? pp : 0][cc]);
+            if (GRADS) {
+              puy[PK ? pp : 0][cc] = ffma2(dup2(e[4 + NC + cc]), zi, puy[PK ? pp : 0][cc]);
+              pvx[PK ? pp : 0][cc] = ffma2(dup2(e[4 + 2 * NC + cc]), zr, pvx[PK ? pp : 0][cc]);
+            }
+          }
+        }
+        continue;
+      }
       float2 H[TY];
       {
         const float2 h = hs[jj * NQ * 128];
@@ -1022,6 +1163,20 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
   }
   cp_async_wait0();
   if (!xok) return;
+  if (PK) {
+#pragma unroll
+    for (int ty = 0; ty < TY; ++ty)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const int pp = PK ? ty >> 1 : 0;
+        const bool hi = ty & 1;
+        cg[ty][c] = make_float2(hi ? pcx[pp][c].y : pcx[pp][c].x, hi ? pcy[pp][c].y : pcy[pp][c].x);
+        if (GRADS) {
+          Uy[ty][GRADS ? c : 0] = hi ? puy[pp][c].y : puy[pp][c].x;
+          Vx[ty][GRADS ? c : 0] = hi ? pvx[pp][c].y : pvx[pp][c].x;
+        }
+      }
+  }
   const size_t plane = (size_t)snx * sny;
 #pragma unroll
   for (int ty = 0; ty < TY; ++ty) {
