@@ -96,6 +96,18 @@ __device__ __forceinline__ float2 frac_turn2(float2 v) {
   const float2 M = dup2(12582912.0f);
   return fsub2(v, fsub2(fadd2(v, M), M));
 }
+// The reduced phase s + f t (s = static phase + k.r term, |s| <= 1 turn) on a pair of lanes with
+// one rounding to an integer: with p = f t_hi (product error e exact by FMA) and n = round(p + s),
+//   theta = ((p - n) + s) - (-(f t_lo + e)),   |theta| <= 1/2 + an ulp of p.
+// p - n is exact for |p| >= 1 (a multiple of ulp(p) below 2) and otherwise rounds at ulp(1), so
+// theta carries the rounding of the two-reduction form (ft_turns, then frac_turn) in fewer adds.
+__device__ __forceinline__ float2 phase_turns2(float2 s, float2 f, float2 nf, float2 t_hi, float2 t_lo) {
+  const float2 M = dup2(12582912.0f);
+  const float2 p = fmul2(f, t_hi);
+  const float2 en = ffma2(nf, t_hi, p);                     // -(exact error of the product)
+  const float2 n = fsub2(fadd2(fadd2(p, s), M), M);         // round(p + s)
+  return fsub2(fadd2(fsub2(p, n), s), ffma2(nf, t_lo, en));
+}
 __device__ __forceinline__ float2 ft_turns2(float2 f, float2 nf, float2 t_hi, float2 t_lo) {
   const float2 M = dup2(12582912.0f);
   const float2 p = fmul2(f, t_hi);
@@ -557,9 +569,9 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
         const float2 a2 = dup2(a), f2 = dup2(f), nf2 = dup2(-f);
 #pragma unroll
         for (int jp = 0; jp < T; jp += 2) {
-          float2 th = fadd2(fadd2(a2, make_float2(bt[jp], bt[jp + 1])),
-                            ft_turns2(f2, nf2, make_float2(thi[jp], thi[jp + 1]), make_float2(tlo[jp], tlo[jp + 1])));
-          th = fmul2(dup2(kTwoPiF), frac_turn2(th));
+          float2 th = phase_turns2(fadd2(a2, make_float2(bt[jp], bt[jp + 1])), f2, nf2,
+                                   make_float2(thi[jp], thi[jp + 1]), make_float2(tlo[jp], tlo[jp + 1]));
+          th = fmul2(dup2(kTwoPiF), th);
           float s0, c0, s1, c1;
           __sincosf(th.x, &s0, &c0);
           __sincosf(th.y, &s1, &c1);
@@ -1056,18 +1068,14 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
       const float4 e0 = *reinterpret_cast<const float4*>(e);
       const float thi = e0.x, tlo = e0.y, trf = e0.z, tinh = e0.w;
       if (PK) {
-        float2 Hx[2], Hy[2];  // [pair] = rows (2p, 2p + 1)
+        float2 Hx[2], Hy[2];  // [pair] = rows (2p, 2p + 1); starts from the offset row (amplitude 1)
         {
-          const float2 h = hs[jj * NQ * 128];
-#pragma unroll
-          for (int pp = 0; pp < 2; ++pp) {
-            const float2 am = make_float2(amp[2 * pp][0], amp[(2 * pp + 1) % TY][0]);
-            Hx[pp] = fmul2(am, dup2(h.x));
-            Hy[pp] = fmul2(am, dup2(h.y));
-          }
+          const float2 h = hs[(jj * NQ + NQ - 1) * 128];
+          Hx[0] = Hx[1] = dup2(h.x);
+          Hy[0] = Hy[1] = dup2(h.y);
         }
 #pragma unroll
-        for (int q = 1; q < NQ; ++q) {
+        for (int q = 0; q < NQ - 1; ++q) {
           const float2 h = hs[(jj * NQ + q) * 128];
           const float2 hx = dup2(h.x), hy = dup2(h.y);
 #pragma unroll
@@ -1083,9 +1091,9 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
         for (int pp = 0; pp < 2; ++pp) {
           const int t0 = 2 * pp, t1 = (2 * pp + 1) % TY;
           const float2 bt2 = pp == 0 ? make_float2(b4.x, b4.y) : make_float2(b4.z, b4.w);
-          float2 th = fadd2(fadd2(make_float2(a[t0], a[t1]), bt2),
-                            ft_turns2(make_float2(f[t0], f[t1]), make_float2(-f[t0], -f[t1]), thi2, tlo2));
-          th = fmul2(dup2(kTwoPiF), frac_turn2(th));
+          float2 th = phase_turns2(fadd2(make_float2(a[t0], a[t1]), bt2), make_float2(f[t0], f[t1]),
+                                   make_float2(-f[t0], -f[t1]), thi2, tlo2);
+          th = fmul2(dup2(kTwoPiF), th);
           float s0, c0, s1, c1;
           __sincosf(th.x, &s0, &c0);
           __sincosf(th.y, &s1, &c1);
