@@ -908,7 +908,10 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
   const int y0 = tl.y, x0 = tl.z;
   float2* hbuf = reinterpret_cast<float2*>(smem);
   float* Bt = reinterpret_cast<float*>(hbuf + kAdjStages * STAGE);  // [nlines][ROWS]
-  float* Lt = Bt + nlines * ROWS;                                    // [nlines][LF]
+  // the line tables cover whole chunks (zero entries past nlines), so the packed path runs every
+  // line of a chunk without a branch
+  const int nlp = (nlines + JC - 1) / JC * JC;
+  float* Lt = Bt + nlp * ROWS;                                       // [nlp][LF]
   const int tid = threadIdx.x;
   const int col = tid & 127, rg = tid >> 7;
   const int x = x0 + col;
@@ -952,11 +955,11 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
   const int ys = u.ny / 2;
   const int oy = sny / u.ny;
   const int sys = oy * ys;
-  for (int idx = tid; idx < nlines * ROWS; idx += 256) {
+  for (int idx = tid; idx < nlp * ROWS; idx += 256) {
     const int j = idx / ROWS, r = idx % ROWS;
     const int y = y0 + r;
     float v = 0.f;
-    if (y < sny) {
+    if (y < sny && j < nlines) {
       const LineRec& L = u.lines[j];
       const long long K = L.ky - ys;
       const long long Y = 2LL * (y - sys) - (oy - 1);
@@ -971,9 +974,14 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
     }
     Bt[idx] = v;
   }
-  for (int j = tid; j < nlines; j += 256) {
-    const LineRec& L = u.lines[j];
+  for (int j = tid; j < nlp; j += 256) {
     float* e = Lt + j * LF;
+    if (j >= nlines) {
+#pragma unroll
+      for (int k = 0; k < LF; ++k) e[k] = 0.f;
+      continue;
+    }
+    const LineRec& L = u.lines[j];
     const float tph = L.t_hi + L.t_lo;
     e[0] = L.t_hi;
     e[1] = L.t_lo;
@@ -1063,7 +1071,7 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
 #pragma unroll
     for (int jj = 0; jj < JC; ++jj) {
       const int j = j0 + jj;
-      if (j >= nlines) break;
+      if (!PK && j >= nlines) break;  // (the packed path reads the zero entries instead)
       const float* e = Lt + j * LF;
       const float4 e0 = *reinterpret_cast<const float4*>(e);
       const float thi = e0.x, tlo = e0.y, trf = e0.z, tinh = e0.w;
@@ -1985,7 +1993,8 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
     if (p->adjq[pass]) {
       const int NQv = p->adjq[pass];
       const size_t smq = sizeof(float2) * (size_t)kAdjStages * adjq_chunk_lines(NQv) * NQv * 128 +
-                         sizeof(float) * (size_t)p->max_lines * (2 * adjq_rows(NCv, maps) + adjq_line_floats(NCv, maps));
+                         sizeof(float) * (size_t)(p->max_lines + adjq_chunk_lines(NQv)) *
+                             (2 * adjq_rows(NCv, maps) + adjq_line_floats(NCv, maps));
       bool launched = false;
       const bool virt = p->adj_cls;
 #define MRSIM_AQV(NQV, NCV, M, G, V)                                                    \
