@@ -89,13 +89,6 @@ __device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 
-// frac_turn and ft_turns on a pair of lanes.  ft_turns2 takes -f (nf) so that no lane needs a
-// negation: fma(-f, t_hi, p) = -e and fma(-f, t_lo, -e) = -(f t_lo + e) exactly (round to nearest
-// is symmetric), and r - (-(f t_lo + e)) = r + (f t_lo + e).
-__device__ __forceinline__ float2 frac_turn2(float2 v) {
-  const float2 M = dup2(12582912.0f);
-  return fsub2(v, fsub2(fadd2(v, M), M));
-}
 // The reduced phase s + f t (s = static phase + k.r term, |s| <= 1 turn) on a pair of lanes with
 // one rounding to an integer: with p = f t_hi (product error e exact by FMA) and n = round(p + s),
 //   theta = ((p - n) + s) - (-(f t_lo + e)),   |theta| <= 1/2 + an ulp of p.
@@ -107,13 +100,6 @@ __device__ __forceinline__ float2 phase_turns2(float2 s, float2 f, float2 nf, fl
   const float2 en = ffma2(nf, t_hi, p);                     // -(exact error of the product)
   const float2 n = fsub2(fadd2(fadd2(p, s), M), M);         // round(p + s)
   return fsub2(fadd2(fsub2(p, n), s), ffma2(nf, t_lo, en));
-}
-__device__ __forceinline__ float2 ft_turns2(float2 f, float2 nf, float2 t_hi, float2 t_lo) {
-  const float2 M = dup2(12582912.0f);
-  const float2 p = fmul2(f, t_hi);
-  const float2 en = ffma2(nf, t_hi, p);                // -(exact error of the product)
-  const float2 r = fsub2(p, fsub2(fadd2(p, M), M));    // exact
-  return fsub2(r, ffma2(nf, t_lo, en));
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -144,36 +130,59 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src,
 // `phase_slice` (kspace.rs:1156-1180).
 __global__ void statics_kernel(const StaticDesc* descs) {
   const StaticDesc& d = descs[blockIdx.y];
-  int n = d.snx * d.sny;
+  const int n = d.snx * d.sny;
   const double inv_tau = 0.15915494309189533577;
-  int ox = d.snx / d.nx, oy = d.sny / d.ny;
-  int sxs = ox * (d.nx / 2), sys = oy * (d.ny / 2);
-  double xoff = (ox - 1.0) / 2.0, yoff = (oy - 1.0) / 2.0;
+  const int ox = d.snx / d.nx, oy = d.sny / d.ny;
+  const int sxs = ox * (d.nx / 2), sys = oy * (d.ny / 2);
+  const double xoff = (ox - 1.0) / 2.0, yoff = (oy - 1.0) / 2.0;
+  const bool explicit_phase = (d.flags & 1) != 0;
+  // Within a slice the phase model is a quadratic in (x, y): with r0 = (x - sx - off)/o,
+  // r1 = (y - sy - off)/o and r2 the slice coordinate, background + shot term are
+  //   A + B r0 + C r1 + D r0^2 + E r1^2 + F r0 r1
+  // and the eddy object-phase ramp is affine in x and y.  Each thread forms the six FP64
+  // coefficients once and evaluates its voxels by Horner's rule.
+  double c00 = 0, cx = 0, cy = 0, cxx = 0, cyy = 0, cxy = 0;
+  {
+    const double o = d.o, sx = d.snx / 2.0, sy = d.sny / 2.0, off = (o - 1.0) / 2.0;
+    const double r2 = d.z - d.nz_full / 2.0;
+    const double* c = d.bg;
+    double A = 0, B = 0, C = 0, D = 0, E = 0, F = 0;
+    if (!explicit_phase) {
+      const double* q = d.shot_q;
+      const double* dx = d.shot_dx;
+      const double* rot = d.shot_rot;
+      A = d.global + c[0] + c[3] * r2 + c[6] * r2 * r2 + q[0] * (dx[0] + rot[1] * r2) +
+          q[1] * (dx[1] - rot[0] * r2) + q[2] * dx[2];
+      B = c[1] + c[8] * r2 + q[1] * rot[2] - q[2] * rot[1];
+      C = c[2] + c[9] * r2 - q[0] * rot[2] + q[2] * rot[0];
+      D = c[4];
+      E = c[5];
+      F = c[7];
+    }
+    // r0 = a0 + x / o, r1 = b0 + y / o
+    const double a0 = -(sx + off) / o, b0 = -(sy + off) / o, io = 1.0 / o;
+    c00 = A + B * a0 + C * b0 + D * a0 * a0 + E * b0 * b0 + F * a0 * b0;
+    cx = (B + 2.0 * D * a0 + F * b0) * io;
+    cy = (C + 2.0 * E * b0 + F * a0) * io;
+    cxx = D * io * io;
+    cyy = E * io * io;
+    cxy = F * io * io;
+    if (d.flags & 2) {  // + e0 (x - sxs - xoff)/ox + e1 (y - sys - yoff)/oy + e2 zc
+      const double* e = d.eddy_phase_coef;
+      c00 += -e[0] * (sxs + xoff) / ox - e[1] * (sys + yoff) / oy + e[2] * d.zc_c;
+      cx += e[0] / ox;
+      cy += e[1] / oy;
+    }
+  }
+  const double* __restrict__ phase0 = d.phase0;
+  float* __restrict__ out = d.out;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int x = i % d.snx, y = i / d.snx;
-    double p0;
-    if (d.flags & 1) {
-      p0 = d.phase0[i];
-    } else {
-      double sx = d.snx / 2.0, sy = d.sny / 2.0, off = (d.o - 1.0) / 2.0;
-      double r0 = (x - sx - off) / d.o, r1 = (y - sy - off) / d.o, r2 = d.z - d.nz_full / 2.0;
-      const double* c = d.bg;
-      double bg = c[0] + c[1] * r0 + c[2] * r1 + c[3] * r2 + c[4] * r0 * r0 + c[5] * r1 * r1 + c[6] * r2 * r2 +
-                  c[7] * r0 * r1 + c[8] * r0 * r2 + c[9] * r1 * r2;
-      double cr0 = d.shot_rot[1] * r2 - d.shot_rot[2] * r1;
-      double cr1 = d.shot_rot[2] * r0 - d.shot_rot[0] * r2;
-      double cr2 = d.shot_rot[0] * r1 - d.shot_rot[1] * r0;
-      double shot = d.shot_q[0] * (d.shot_dx[0] + cr0) + d.shot_q[1] * (d.shot_dx[1] + cr1) +
-                    d.shot_q[2] * (d.shot_dx[2] + cr2);
-      p0 = d.global + bg + shot;
-    }
-    if (d.flags & 2) {
-      double xc = (x - sxs - xoff) / ox, yc = (y - sys - yoff) / oy;
-      p0 += d.eddy_phase_coef[0] * xc + d.eddy_phase_coef[1] * yc + d.eddy_phase_coef[2] * d.zc_c;
-    }
+    const double x = i % d.snx, y = i / d.snx;
+    double p0 = explicit_phase ? phase0[i] : fma(x, fma(cxx, x, fma(cxy, y, cx)), fma(y, fma(cyy, y, cy), c00));
+    if (explicit_phase && (d.flags & 2)) p0 += fma(cx, x, fma(cy, y, c00));
     double tt = p0 * inv_tau;
     tt -= rint(tt);
-    d.out[i] = (float)tt;
+    out[i] = (float)tt;
   }
 }
 
@@ -1864,7 +1873,7 @@ void epi_plan_statics(const EpiPlan* p, cudaStream_t st, int u0, int u1) {
   if (u1 < 0) u1 = p->n_statics;
   if (u0 < 0 || u0 > u1 || u1 > p->n_statics) fail("unit range outside the plan");
   if (u1 == u0) return;
-  dim3 grid((p->max_static_n + 255) / 256, u1 - u0);
+  dim3 grid(std::min(8, (p->max_static_n + 255) / 256), u1 - u0);  // a few voxels per thread
   statics_kernel<<<grid, 256, 0, st>>>(p->d_statics + u0);
   MRSIM_CUDA(cudaGetLastError());
 }
