@@ -140,3 +140,25 @@ def test_apply_host_fills_the_rows_it_does_not_download(gpu_ctx):
     rows = int(mask.sum()) * len(tes)
     kbytes = 3 * 2 * 4 * rows * s["acq_dims"][0] * 8
     assert down == kbytes + sum(clean[k].nbytes for k in ("comp_grad", "fmap_grad", "r2_grad"))
+
+
+@pytest.mark.parametrize("nx,ny,pf,tes", [(16, 16, 0.625, (15.0, 35.0, 55.0)), (12, 12, 0.75, (20.0, 40.0))])
+def test_coil_classes_odd_lines_and_dft_widths_match_the_oracle(nx, ny, pf, tes, gpu_ctx):
+    """Eight ring coils run the coil-class kernels: an odd number of acquired lines per unit (the
+    adjoint's last line chunk is half empty) and a 24-point sim width (no power of two: the
+    x-stage is the DFT GEMM while the forward still accumulates coil classes)."""
+    s = cases.series_case(nx=nx, ny=ny, nv=2, nz=2, ncomp=3)
+    acq = Acquisition(n_coils=8, accel=2, partial_fourier=pf, pf_mode=PartialFourierMode.Scanner, t_line=0.5,
+                      t_echo=30.0, ghost_offset=0.02)
+    kw = dict(t_inhom=s["t_inhom"], phase=PhaseModel.hbcd_like(), seed=42)
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], 2, s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=list(tes), grads=3, ctx=gpu_ctx, **kw)
+    out = op.apply_host(None)
+    want = oracle.series_forward(s["sim_dims"], s["acq_dims"], 2, s["images"], s["t2"], s["fmap"], acq,
+                                 echo_times_ms=list(tes), **kw)
+    assert rel_l2(out["kspace"], want) <= TOL
+    adj = oracle.series_adjoint(s["sim_dims"], s["acq_dims"], 2, s["images"], s["t2"], s["fmap"], acq,
+                                out["kspace"].astype(np.complex128), echo_times_ms=list(tes), **kw)
+    for key in ("comp_grad", "fmap_grad", "r2_grad"):
+        e = rel_l2(out[key], adj[key])
+        assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
