@@ -149,6 +149,17 @@ def algorithmic_flops(op_units, n_lines, snx, sny, nx, ncoils, ncomp):
     return y, x
 
 
+def max_over_ranks(v, world, device="cuda"):
+    """The maximum of a per-rank scalar over every rank of the job (the value itself on one rank):
+    step times are reported as the slowest rank's."""
+    if world <= 1:
+        return float(v)
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from mrsim_acq_b200 import api
@@ -200,10 +211,7 @@ def run_ours(args, rank, world, local_rank):
     total_ms = t_begin.elapsed_time(t_end)
     stage_ms = np.array([[evs[k][i].elapsed_time(evs[k][i + 1]) for i in range(5)] for k in range(args.steps)])
     stage_avg = stage_ms.mean(axis=0)
-    ms = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(ms, op=torch.distributed.ReduceOp.MAX)
-    ms_step = float(ms.item()) / args.steps
+    ms_step = max_over_ranks(total_ms, world) / args.steps
 
     # end to end through the host-buffer C ABI call (pinned host memory)
     shp = op.shapes()
@@ -228,9 +236,7 @@ def run_ours(args, rank, world, local_rank):
         op.apply_host(host_imgs, out)
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1) / max(e2e_steps, 1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(e2e_ms, op=torch.distributed.ReduceOp.MAX)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / max(e2e_steps, 1), world)
     # bytes that cross the host link per call (the library skips k-space rows the sampling never
     # acquires and zero-fills them on the host)
     h2d, d2h = op.host_bytes()
@@ -251,7 +257,7 @@ def run_ours(args, rank, world, local_rank):
                    "coils": acq.n_coils, "accel": acq.accel, "partial_fourier": acq.partial_fourier,
                    "samples_per_step_per_gpu": samples, "parallelism": f"weak x{world} (independent series)",
                    "l2": "inputs (236 MB images) larger than L2; no flush"},
-        "e2e": {"value": samples * world / (float(e2e_ms.item()) * 1e-3), "unit": "samples/s",
+        "e2e": {"value": samples * world / (e2e_ms * 1e-3), "unit": "samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "call": "mrsim_epi_operator_apply_host (host images in, k-space and gradients out)"},
         "roofline": {"bound": "fp32", "kernel": dom_name,
