@@ -896,12 +896,17 @@ __host__ __device__ __forceinline__ constexpr int adjq_line_floats(int nc, bool 
 }
 // rows per thread: 4 with class decay and up to 3 compartments, else 2 (registers)
 __host__ __device__ __forceinline__ constexpr int adjq_rows(int nc, bool maps) { return !maps && nc <= 3 ? 4 : 2; }
+// ... the same with coil-class rows (two rows per thread in 80 registers and three CTAs per SM
+// measured 30 % slower than four rows: the per-line loads then serve half the rows)
+__host__ __device__ __forceinline__ constexpr int adjq_rows_v(int nc, bool maps, bool virt) {
+  return adjq_rows(nc, maps);
+}
 
 
 // VIRT: the h rows are the NQ = classes + 1 class rows of the class-mode x-adjoint (scale, ex and
 // the coil offset already applied), so amp_v(y) = ey_v(y) for the classes and 1 for the offset row.
 template <int NQ, int TY, int NC, bool MAPS, bool GRADS, bool VIRT>
-__global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __restrict__ units,
+__global__ void __launch_bounds__(256, (VIRT && !MAPS && TY == 2) ? 3 : 2) yadjoint_q_kernel(const UnitDesc* __restrict__ units,
                                                             const int4* __restrict__ tiles) {
   extern __shared__ __align__(16) float smem[];
   static_assert(TY == 2 || TY == 4, "the row phases are read as one float2 / float4");
@@ -1050,11 +1055,12 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
   }
   // PK (class rows, class decay, 4 rows): rows (0, 1) and (2, 3) run as packed f32x2 pairs, with
   // accumulators pcx/pcy/puy/pvx[pair][c] holding the two rows' Re/Im comp sums, t- and trf-sums
-  constexpr bool PK = VIRT && !MAPS && TY == 4;
-  float2 pcx[PK ? 2 : 1][NC], pcy[PK ? 2 : 1][NC], puy[PK ? 2 : 1][NC], pvx[PK ? 2 : 1][NC];
+  constexpr bool PK = VIRT && !MAPS;
+  constexpr int NPR = PK ? TY / 2 : 1;  // row pairs
+  float2 pcx[NPR][NC], pcy[NPR][NC], puy[NPR][NC], pvx[NPR][NC];
   if (PK) {
 #pragma unroll
-    for (int pp = 0; pp < (PK ? 2 : 1); ++pp)
+    for (int pp = 0; pp < NPR; ++pp)
 #pragma unroll
       for (int c = 0; c < NC; ++c) pcx[pp][c] = pcy[pp][c] = puy[pp][c] = pvx[pp][c] = make_float2(0.f, 0.f);
   }
@@ -1085,29 +1091,39 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
       const float4 e0 = *reinterpret_cast<const float4*>(e);
       const float thi = e0.x, tlo = e0.y, trf = e0.z, tinh = e0.w;
       if (PK) {
-        float2 Hx[2], Hy[2];  // [pair] = rows (2p, 2p + 1); starts from the offset row (amplitude 1)
+        float2 Hx[NPR], Hy[NPR];  // [pair] = rows (2p, 2p + 1); starts from the offset row (amplitude 1)
         {
           const float2 h = hs[(jj * NQ + NQ - 1) * 128];
-          Hx[0] = Hx[1] = dup2(h.x);
-          Hy[0] = Hy[1] = dup2(h.y);
+#pragma unroll
+          for (int pp = 0; pp < NPR; ++pp) {
+            Hx[pp] = dup2(h.x);
+            Hy[pp] = dup2(h.y);
+          }
         }
 #pragma unroll
         for (int q = 0; q < NQ - 1; ++q) {
           const float2 h = hs[(jj * NQ + q) * 128];
           const float2 hx = dup2(h.x), hy = dup2(h.y);
 #pragma unroll
-          for (int pp = 0; pp < 2; ++pp) {
+          for (int pp = 0; pp < NPR; ++pp) {
             const float2 am = make_float2(amp[2 * pp][q], amp[(2 * pp + 1) % TY][q]);
             Hx[pp] = ffma2(am, hx, Hx[pp]);
             Hy[pp] = ffma2(am, hy, Hy[pp]);
           }
         }
-        const float4 b4 = *reinterpret_cast<const float4*>(Bt + j * ROWS + rg * TY);
+        float2 btp[NPR];
+        if (TY == 4) {
+          const float4 b4 = *reinterpret_cast<const float4*>(Bt + j * ROWS + rg * TY);
+          btp[0] = make_float2(b4.x, b4.y);
+          btp[NPR - 1] = make_float2(b4.z, b4.w);
+        } else {
+          btp[0] = *reinterpret_cast<const float2*>(Bt + j * ROWS + rg * TY);
+        }
         const float2 thi2 = dup2(thi), tlo2 = dup2(tlo);
 #pragma unroll
-        for (int pp = 0; pp < 2; ++pp) {
+        for (int pp = 0; pp < NPR; ++pp) {
           const int t0 = 2 * pp, t1 = (2 * pp + 1) % TY;
-          const float2 bt2 = pp == 0 ? make_float2(b4.x, b4.y) : make_float2(b4.z, b4.w);
+          const float2 bt2 = btp[pp];
           float2 th = phase_turns2(fadd2(make_float2(a[t0], a[t1]), bt2), make_float2(f[t0], f[t1]),
                                    make_float2(-f[t0], -f[t1]), thi2, tlo2);
           th = fmul2(dup2(kTwoPiF), th);
@@ -1193,7 +1209,7 @@ __global__ void __launch_bounds__(256, 2) yadjoint_q_kernel(const UnitDesc* __re
     for (int ty = 0; ty < TY; ++ty)
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        const int pp = PK ? ty >> 1 : 0;
+        const int pp = PK ? (ty >> 1) % NPR : 0;
         const bool hi = ty & 1;
         cg[ty][c] = make_float2(hi ? pcx[pp][c].y : pcx[pp][c].x, hi ? pcy[pp][c].y : pcy[pp][c].x);
         if (GRADS) {
@@ -1808,10 +1824,20 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
           (long long)hu[i].ncoils * hu[i].n_lines * hu[i].snx >= (1LL << 31))
         nq_all = 0;
     if (nq_all != 1 && nq_all != 2 && nq_all != 4 && nq_all != 8) nq_all = 0;
+    // coil classes in the adjoint: every unit has the 8-coil ring (5 classes + offset), rows of
+    // at most 128 points in the warp FFT, and the fixed-count y-adjoint for its shape
+    {
+      bool cl = n > 0 && p->xfft && p->xfft_e >= 1 && p->xfft_e <= 4 && p->nc <= 4 && nq_all == 8;
+      for (int i = 0; i < n && cl; ++i) {
+        const UnitDesc& u = hu[i];
+        cl = u.ncoils == 8 && u.geo.ncls == 5 && u.geo.coil_off != 0.f && u.geo.cls && u.geo.eyc;
+      }
+      p->adj_cls = cl;
+    }
     for (int pass = 0; pass < 4; ++pass) {
       bool maps = pass & 1, grads = pass & 2;
-      p->adjq[pass] = (maps && p->nc == 8) ? 0 : nq_all;
-      const int step = p->adjq[pass] ? 2 * adjq_rows(p->nc, maps) : kTY;
+      p->adjq[pass] = p->adj_cls ? 6 : (maps && p->nc == 8) ? 0 : nq_all;
+      const int step = p->adjq[pass] ? 2 * adjq_rows_v(p->nc, maps, p->adj_cls) : kTY;
       std::vector<int4> yt;
       p->a_start[pass].assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
@@ -1826,28 +1852,16 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->n_atiles[pass] = (int)yt.size();
       p->d_atiles[pass] = (int4*)dev_upload(p, yt.data(), sizeof(int4) * yt.size());
     }
-    // coil classes in the adjoint: every unit has the 8-coil ring (5 classes + offset), rows of
-    // at most 128 points in the warp FFT, and the fixed-count y-adjoint for its shape
-    {
-      bool cl = n > 0 && p->xfft && p->xfft_e >= 1 && p->xfft_e <= 4 && p->nc <= 4 && nq_all == 8;
-      for (int i = 0; i < n && cl; ++i) {
-        const UnitDesc& u = hu[i];
-        cl = u.ncoils == 8 && u.geo.ncls == 5 && u.geo.coil_off != 0.f && u.geo.cls && u.geo.eyc;
+    if (p->adj_cls) {  // the x-adjoint's tiles: 4 lines x the 8 coils
+      std::vector<int4> ct;
+      p->c_start.assign(n + 1, 0);
+      for (int i = 0; i < n; ++i) {
+        p->c_start[i] = (int)ct.size();
+        for (int j0 = 0; j0 < hu[i].n_lines; j0 += 4) ct.push_back(make_int4(i, j0, std::min(4, hu[i].n_lines - j0), 0));
       }
-      for (int pass = 0; pass < 4 && cl; ++pass) cl = p->adjq[pass] == 8;
-      if (cl) {
-        std::vector<int4> ct;
-        p->c_start.assign(n + 1, 0);
-        for (int i = 0; i < n; ++i) {
-          p->c_start[i] = (int)ct.size();
-          for (int j0 = 0; j0 < hu[i].n_lines; j0 += 4) ct.push_back(make_int4(i, j0, std::min(4, hu[i].n_lines - j0), 0));
-        }
-        p->c_start[n] = (int)ct.size();
-        p->n_ctiles = (int)ct.size();
-        p->d_ctiles = (int4*)dev_upload(p, ct.data(), sizeof(int4) * ct.size());
-        p->adj_cls = true;
-        for (int pass = 0; pass < 4; ++pass) p->adjq[pass] = 6;
-      }
+      p->c_start[n] = (int)ct.size();
+      p->n_ctiles = (int)ct.size();
+      p->d_ctiles = (int4*)dev_upload(p, ct.data(), sizeof(int4) * ct.size());
     }
   } catch (...) {
     delete p;
@@ -2003,12 +2017,12 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
       const int NQv = p->adjq[pass];
       const size_t smq = sizeof(float2) * (size_t)kAdjStages * adjq_chunk_lines(NQv) * NQv * 128 +
                          sizeof(float) * (size_t)(p->max_lines + adjq_chunk_lines(NQv)) *
-                             (2 * adjq_rows(NCv, maps) + adjq_line_floats(NCv, maps));
+                             (2 * adjq_rows_v(NCv, maps, p->adj_cls) + adjq_line_floats(NCv, maps));
       bool launched = false;
       const bool virt = p->adj_cls;
 #define MRSIM_AQV(NQV, NCV, M, G, V)                                                    \
   if (NQv == NQV && NCv == NCV && maps == M && grads == G && virt == V) {               \
-    auto k = yadjoint_q_kernel<NQV, adjq_rows(NCV, M), NCV, M, G, V>;                   \
+    auto k = yadjoint_q_kernel<NQV, adjq_rows_v(NCV, M, V), NCV, M, G, V>;              \
     set_smem(k, smq);                                                                   \
     k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                              \
     launched = true;                                                                    \
