@@ -162,3 +162,26 @@ def test_coil_classes_odd_lines_and_dft_widths_match_the_oracle(nx, ny, pf, tes,
     for key in ("comp_grad", "fmap_grad", "r2_grad"):
         e = rel_l2(out[key], adj[key])
         assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
+
+
+@pytest.mark.parametrize("coils,eddy", [(8, False), (4, True)])
+def test_128_point_rows_match_the_oracle(coils, eddy, gpu_ctx):
+    """The bench's width (64 acquired columns on 128 sim columns): the x-stage runs as 16 x 8 FFTs
+    (into coil-class rows for the 8-coil adjoint), with and without the eddy x/z factor."""
+    s = cases.series_case(nx=64, ny=64, nv=1, nz=1, ncomp=3)
+    acq = Acquisition(n_coils=coils, accel=2, partial_fourier=0.75, pf_mode=PartialFourierMode.Scanner, t_line=0.5,
+                      t_echo=30.0, ghost_offset=0.05, eddy_strength=2.0 if eddy else 0.0, eddy_quad=0.3)
+    tes = [15.0, 35.0, 55.0]
+    kw = dict(t_inhom=s["t_inhom"], phase=PhaseModel.hbcd_like(), seed=42,
+              eddy_drive=[(0.5, -0.4, 0.7)] if eddy else None)
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], 1, s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
+    out = op.apply_host(None)
+    want = oracle.series_forward(s["sim_dims"], s["acq_dims"], 1, s["images"], s["t2"], s["fmap"], acq,
+                                 echo_times_ms=tes, **kw)
+    assert rel_l2(out["kspace"], want) <= TOL
+    adj = oracle.series_adjoint(s["sim_dims"], s["acq_dims"], 1, s["images"], s["t2"], s["fmap"], acq,
+                                out["kspace"].astype(np.complex128), echo_times_ms=tes, **kw)
+    for key in ("comp_grad", "fmap_grad", "r2_grad"):
+        e = rel_l2(out[key], adj[key])
+        assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
