@@ -390,9 +390,11 @@ __host__ __device__ __forceinline__ constexpr int fwdq_rows(int nc, bool maps) {
 // NV > 0: the tile holds every coil of the unit and accumulates coil classes instead of coils
 // (NV = classes + 1 for the coil offset): acc_v += ey_v(y) W P, acc_off += W P, and the epilogue
 // expands g_q = s (ex_q acc_cls(q) + off acc_off).
+// cls_rows (with NV): write the class rows G_v = s T_v and G_off = s off T_off ([v][line][x], the
+// layout the class-mode x-stage expands) instead of the coil rows.
 template <int QG, int NV, int NC, bool MAPS>
 __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __restrict__ units,
-                                                          const Tile* __restrict__ tiles) {
+                                                          const Tile* __restrict__ tiles, int cls_rows) {
   constexpr int T = 4, TL = 8;
   constexpr int NA = NV ? NV : QG;             // accumulators per line
   constexpr int NPL = fwdq_planes(NC, MAPS);
@@ -636,6 +638,18 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
   cp_async_wait0();
   if (!xok) return;
   const float s = u.signal_scale;
+  if (NV && cls_rows) {
+#pragma unroll
+    for (int j = 0; j < T; ++j) {
+      if (jb + j >= nl) break;
+#pragma unroll
+      for (int v = 0; v < NA; ++v) {
+        const float sv = v == NA - 1 ? s * off : s;
+        u.g[((size_t)v * u.n_lines + tl.line0 + jb + j) * snx + x] = make_float2(sv * acc[j][v].x, sv * acc[j][v].y);
+      }
+    }
+    return;
+  }
   if (NV) {
     // expand the classes to the unit's coils (all in this tile)
     for (int q = 0; q < u.ncoils; ++q) {
@@ -1477,17 +1491,18 @@ __host__ __device__ constexpr int bitrev_c(int v, int bits) {
 }
 __host__ __device__ constexpr int log2_c(int v) { return v <= 1 ? 0 : 1 + log2_c(v / 2); }
 
-// CLS (adjoint, 8 coils in 5 classes + offset): a tile is (unit, first line, up to 4 lines) x all
-// 8 coils, warp w transforms coil w of each line into shared memory, and the CTA then writes the
+// CLS (8 coils in 5 classes + offset): a tile is (unit, first line, up to 4 lines) x all 8 coils.
+// Adjoint: warp w transforms coil w of each line into shared memory, and the CTA then writes the
 // 6 class rows G_v = s sum_{q in v} ex_q h_q, G_off = s off sum_q h_q ([v][line][x] in g) that
-// the class-mode y-adjoint combines as sum_v ey_v(y) G_v + G_off.
+// the class-mode y-adjoint combines as sum_v ey_v(y) G_v + G_off.  Forward: the CTA stages the
+// tile's class rows from the class-mode y-stage and each row loads g_q = ex_q G_cls(q) + G_off.
 template <int E, bool ADJ, bool CLS>
 __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const UnitDesc* __restrict__ units,
                                                            const int4* __restrict__ tiles) {
   constexpr int N = 32 * E, LE = log2_c(E);
   constexpr int NP = N + N / 32;  // padded row
   constexpr int RT = 32;          // rows per tile
-  static_assert(!CLS || (ADJ && E <= 4), "coil classes: adjoint rows of at most 128 points");
+  static_assert(!CLS || E <= 4, "coil classes: rows of at most 128 points");
   __shared__ __align__(16) float2 hsm[CLS ? 4 * 8 * N : 1];  // [line][coil][x]
   __shared__ int cls_s[8];
   __shared__ __align__(16) float2 tw[N];        // e^{-i2pi j/N}
@@ -1530,6 +1545,13 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   const float inv_n = 1.0f / (float)(N * u.sny);
   const int kpos = nx - xs;
   float2* row = rb[warp];
+  if (CLS && !ADJ) {  // the tile's class rows: [line][v][x]
+    for (int e = threadIdx.x; e < (nr >> 3) * 6 * N; e += 256) {
+      const int jl = e / (6 * N), v = (e / N) % 6, x = e % N;
+      hsm[e] = u.g[((size_t)v * nl + r0 + jl) * N + x];
+    }
+    __syncthreads();
+  }
   // premodulation of the line's polarity times E_j(x) = e^{i2pi (cx xc + qx xc^2 + z) decay_j}
   auto modulation = [&](int pol, float dec, int x) {
     float2 md = pm[pol * N + x];
@@ -1547,7 +1569,17 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     const int R = CLS ? (r & 7) * nl + r0 + (r >> 3) : r0 + r, q = rq[r], orow = rrow[r], pol = rpol[r];
     const float dec = rdec[r];
     float2 b[E];
-    if (!ADJ) {
+    if (!ADJ && CLS) {
+      const int jl = r >> 3, c = cls_s[q];
+      const float2* cr = hsm + (jl * 6) * N;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const int x = lane + 32 * m;
+        const float ex = u.geo.ex[(size_t)q * N + x];
+        const float2 gv = cr[c * N + x], go = cr[5 * N + x];
+        b[bitrev_c(m, LE)] = cmul(make_float2(fmaf(ex, gv.x, go.x), fmaf(ex, gv.y, go.y)), modulation(pol, dec, x));
+      }
+    } else if (!ADJ) {
       const float2* gr = u.g + (size_t)R * N;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
@@ -1624,7 +1656,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     }
     __syncwarp();
   }
-  if (CLS) {
+  if (CLS && ADJ) {
     __syncthreads();
     const float s = u.signal_scale, so = s * u.geo.coil_off;
     const int nj = nr >> 3;
@@ -1795,6 +1827,17 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->n_ftiles = (int)ft.size();
       p->d_ftiles = (int4*)dev_upload(p, ft.data(), sizeof(int4) * ft.size());
     }
+    // coil classes through the forward x-stage: every unit's y-stage runs in class mode and the
+    // rows have at most 128 points
+    {
+      bool fc = p->xfft && p->xfft_e >= 1 && p->xfft_e <= 4 && n > 0;
+      for (int pass = 0; pass < 2 && fc; ++pass) {
+        bool any = false;
+        for (int i = 0; i < n && !any; ++i) any = ((hu[i].flags & UF_MAPS) != 0) == (pass == 1);
+        if (any && p->fwd_nv[pass] != 6) fc = false;
+      }
+      p->fwd_cls = fc;
+    }
     // x-stage GEMM tiles, from host copies of the line tables (one copy per distinct table)
     std::map<const LineRec*, std::vector<LineRec>> host_lines;
     for (int dir = 0; dir < 2 && !p->xfft; ++dir) {
@@ -1852,7 +1895,7 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->n_atiles[pass] = (int)yt.size();
       p->d_atiles[pass] = (int4*)dev_upload(p, yt.data(), sizeof(int4) * yt.size());
     }
-    if (p->adj_cls) {  // the x-adjoint's tiles: 4 lines x the 8 coils
+    if (p->adj_cls || p->fwd_cls) {  // the class x-stage tiles: 4 lines x the 8 coils
       std::vector<int4> ct;
       p->c_start.assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
@@ -1918,7 +1961,7 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
   if (QG == QGV && NVv == NVV && NCv == NCV && maps == M) {                             \
     auto k = ystage_q_kernel<QGV, NVV, NCV, M>;                                         \
     set_smem(k, smq);                                                                   \
-    k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                              \
+    k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles, p->fwd_cls ? 1 : 0);          \
     launched = true;                                                                    \
   }
 #define MRSIM_YFQ(NCV, M) MRSIM_YF(1, 0, NCV, M) MRSIM_YF(2, 0, NCV, M) MRSIM_YF(4, 0, NCV, M) MRSIM_YF(8, 0, NCV, M)
@@ -1955,16 +1998,23 @@ void epi_plan_forward_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
 
 namespace {
 void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) {
-  if (adj && p->adj_cls) {
+  if ((adj && p->adj_cls) || (!adj && p->fwd_cls)) {
     const TileRange R = tile_range(p->c_start, p->n_ctiles, u0, u1);
     if (R.n == 0) return;
     const int4* tiles = p->d_ctiles + R.t0;
     const unsigned g = (unsigned)R.n;
-    switch (p->xfft_e) {
-      case 1: xfft_warp_kernel<1, true, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;
-      case 2: xfft_warp_kernel<2, true, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;
-      default: xfft_warp_kernel<4, true, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;
+#define MRSIM_XC(ADJ)                                                                             \
+  switch (p->xfft_e) {                                                                            \
+    case 1: xfft_warp_kernel<1, ADJ, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;          \
+    case 2: xfft_warp_kernel<2, ADJ, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;          \
+    default: xfft_warp_kernel<4, ADJ, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+  }
+    if (adj) {
+      MRSIM_XC(true)
+    } else {
+      MRSIM_XC(false)
     }
+#undef MRSIM_XC
     MRSIM_CUDA(cudaGetLastError());
     return;
   }

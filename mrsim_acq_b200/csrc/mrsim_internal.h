@@ -161,6 +161,9 @@ struct EpiPlan {
   // coil classes in the adjoint: the x-adjoint writes class rows (tiles of 4 lines x 8 coils) and
   // the y-adjoint combines 6 rows instead of 8 coils
   bool adj_cls = false;
+  // coil classes in the forward: the y-stage writes the 6 class rows and the x-stage expands them
+  // (the same tiles of 4 lines x 8 coils)
+  bool fwd_cls = false;
   int4* d_ctiles = nullptr;
   int n_ctiles = 0;
   std::vector<int> c_start;
