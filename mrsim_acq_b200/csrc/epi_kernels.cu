@@ -21,6 +21,16 @@
 // The adjoint is the Hermitian transpose with respect to complex compartment images, plus the
 // vector-Jacobian products of L = sum |k - d|^2 with respect to the fieldmap and each
 // compartment's R2 = 1/T2 (the reference has no adjoint; the oracle is the FP64 transpose).
+//
+// Kernels, in the order a step runs them:
+//   statics_kernel                     static phase a(x,y) in turns (FP64 per-slice quadratic)
+//   ystage_q_kernel / ystage_kernel    y-stage (staged-input form; per-thread-load fallback);
+//                                      with the 8-coil ring it accumulates 5 ey classes + offset
+//   xfft_warp_kernel / xfft_kernel /   x-stage: warp-per-row FFT (N = 32..256), shared-memory
+//   xgemm_kernel                       radix-2 FFT (other powers of two), DFT GEMM (other widths)
+//   yadjoint_q_kernel / yadjoint_kernel  y-adjoint (fixed coil or class count; any coil count)
+// The class-mode and packed (f32x2) paths are exact rearrangements: equal ey rows, and lanes that
+// round like the scalar operations.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
