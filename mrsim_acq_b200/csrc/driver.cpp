@@ -109,7 +109,7 @@ GeoTab build_geo(DevArena& arena, int snx, int sny, int nx, int ny, int ncoils, 
   }
   GeoTab g;
   g.xf = nullptr;
-  if (snx >= 8 && snx <= kXfftMaxN && (snx & (snx - 1)) == 0) {
+  if ((snx >= 8 && snx <= kXfftMaxN && (snx & (snx - 1)) == 0) || (snx % 32 == 0 && snx <= 256)) {
     // the factored x-stage: tw[x][kx] = premod_pol(x) * e^{i2pi (kx-xs) x/snx} * post(kx)
     std::vector<float2> xf((size_t)snx / 2 + 2 * (size_t)snx + nx);
     for (int k = 0; k < snx / 2; ++k) {

@@ -1487,7 +1487,7 @@ __global__ void __launch_bounds__(256) xfft_kernel(const UnitDesc* __restrict__ 
   }
 }
 
-// The same x-stage with one warp per row for N = 32 E (E = 1..8), no block barriers: lane t
+// The same x-stage with one warp per row for N = 32 E (E = 1..8, any E), no block barriers: lane t
 // holds x[t + 32 m] (m < E).  With n = t + 32 m and k = k1 + E k2, W = e^{+-i2pi/N}:
 //   X[k1 + E k2] = sum_t W^{t k1} [ sum_m x[t + 32 m] W^{32 m k1} ] W^{E t k2}
 // so each lane does an E-point DFT of its registers (radix-2, unrolled), the twiddles W^{t k1},
@@ -1510,6 +1510,7 @@ template <int E, bool ADJ, bool CLS>
 __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const UnitDesc* __restrict__ units,
                                                            const int4* __restrict__ tiles) {
   constexpr int N = 32 * E, LE = log2_c(E);
+  constexpr bool P2 = (E & (E - 1)) == 0;  // E a power of two: radix-2 register DFT, else direct
   constexpr int NP = N + N / 32;  // padded row
   constexpr int RT = 32;          // rows per tile
   static_assert(!CLS || E <= 4, "coil classes: rows of at most 128 points");
@@ -1587,14 +1588,14 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
         const int x = lane + 32 * m;
         const float ex = u.geo.ex[(size_t)q * N + x];
         const float2 gv = cr[c * N + x], go = cr[5 * N + x];
-        b[bitrev_c(m, LE)] = cmul(make_float2(fmaf(ex, gv.x, go.x), fmaf(ex, gv.y, go.y)), modulation(pol, dec, x));
+        b[P2 ? bitrev_c(m, LE) : m] = cmul(make_float2(fmaf(ex, gv.x, go.x), fmaf(ex, gv.y, go.y)), modulation(pol, dec, x));
       }
     } else if (!ADJ) {
       const float2* gr = u.g + (size_t)R * N;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
-        b[bitrev_c(m, LE)] = cmul(gr[x], modulation(pol, dec, x));
+        b[P2 ? bitrev_c(m, LE) : m] = cmul(gr[x], modulation(pol, dec, x));
       }
     } else {
       const float2* kr = u.kspace + ((size_t)q * u.n_rows + orow) * nx;
@@ -1607,12 +1608,27 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
           const float2 p = pt[kx];
           v = cmul(kr[kx], make_float2(p.x, -p.y));
         }
-        b[bitrev_c(m, LE)] = v;
+        b[P2 ? bitrev_c(m, LE) : m] = v;
       }
     }
-    // E-point DFT of the registers (decimation in time from bit-reversed order)
+    // E-point DFT of the registers: decimation in time from bit-reversed order, or for E not a
+    // power of two the direct sum Y[k1] = sum_m b[m] W^{32 (m k1 mod E)}
+    if (!P2) {
+      float2 y[E];
 #pragma unroll
-    for (int len = 2; len <= E; len <<= 1) {
+      for (int k1 = 0; k1 < E; ++k1) {
+        y[k1] = b[0];
+#pragma unroll
+        for (int m = 1; m < E; ++m) {
+          const float2 v = (m * k1) % E == 0 ? b[m] : cmul(b[m], W(32 * ((m * k1) % E)));
+          y[k1] = make_float2(y[k1].x + v.x, y[k1].y + v.y);
+        }
+      }
+#pragma unroll
+      for (int k1 = 0; k1 < E; ++k1) b[k1] = y[k1];
+    }
+#pragma unroll
+    for (int len = 2; len <= (P2 ? E : 1); len <<= 1) {
 #pragma unroll
       for (int i = 0; i < E; i += len) {
 #pragma unroll
@@ -1650,7 +1666,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     if (!ADJ) {
       float2* out = u.kspace + ((size_t)q * u.n_rows + orow) * nx;
       for (int kx = lane; kx < nx; kx += 32) {
-        const int k = (kx - xs) & (N - 1);
+        const int k = ((kx - xs) % N + N) % N;
         const float2 v = cmul(row[k + (k >> 5)], pt[kx]);
         out[kx] = make_float2(v.x * inv_n, v.y * inv_n);
       }
@@ -1671,7 +1687,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     const float s = u.signal_scale, so = s * u.geo.coil_off;
     const int nj = nr >> 3;
     for (int e = threadIdx.x; e < nj * N; e += 256) {
-      const int jl = e >> LE >> 5, x = e & (N - 1);
+      const int jl = e / N, x = e % N;
       float2 G[6];
 #pragma unroll
       for (int v = 0; v < 6; ++v) G[v] = make_float2(0.f, 0.f);
@@ -1818,11 +1834,12 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
     p->xfft = n > 0;
     for (int i = 0; i < n; ++i) {
       const int N = hu[i].snx;
-      if (hu[i].geo.xf == nullptr || N < 8 || N > kXfftMaxN || (N & (N - 1)) != 0 || hu[i].nx > N) p->xfft = false;
+      const bool pow2 = N >= 8 && N <= kXfftMaxN && (N & (N - 1)) == 0, warp = N % 32 == 0 && N <= 256;
+      if (hu[i].geo.xf == nullptr || !(pow2 || warp) || hu[i].nx > N) p->xfft = false;
     }
     if (p->xfft) {
       const int N0 = hu[0].snx;
-      p->xfft_e = (N0 >= 32 && N0 <= 256) ? N0 / 32 : 0;
+      p->xfft_e = (N0 % 32 == 0 && N0 <= 256) ? N0 / 32 : 0;
       for (int i = 0; i < n; ++i)
         if (hu[i].snx != N0) p->xfft_e = 0;
       std::vector<int4> ft;
@@ -2017,6 +2034,7 @@ void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) 
   switch (p->xfft_e) {                                                                            \
     case 1: xfft_warp_kernel<1, ADJ, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;          \
     case 2: xfft_warp_kernel<2, ADJ, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;          \
+    case 3: xfft_warp_kernel<3, ADJ, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;          \
     default: xfft_warp_kernel<4, ADJ, true><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
   }
     if (adj) {
@@ -2037,7 +2055,11 @@ void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) 
   switch (p->xfft_e) {                                                                            \
     case 1: xfft_warp_kernel<1, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
     case 2: xfft_warp_kernel<2, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+    case 3: xfft_warp_kernel<3, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
     case 4: xfft_warp_kernel<4, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+    case 5: xfft_warp_kernel<5, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+    case 6: xfft_warp_kernel<6, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
+    case 7: xfft_warp_kernel<7, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
     case 8: xfft_warp_kernel<8, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;         \
     default: xfft_kernel<ADJ><<<g, 256, 0, st>>>(p->d_units, tiles);                              \
   }

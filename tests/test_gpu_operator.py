@@ -185,3 +185,26 @@ def test_128_point_rows_match_the_oracle(coils, eddy, gpu_ctx):
     for key in ("comp_grad", "fmap_grad", "r2_grad"):
         e = rel_l2(out[key], adj[key])
         assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
+
+
+@pytest.mark.parametrize("nx,coils", [(48, 8), (80, 4), (96, 8)])
+def test_rows_of_32e_points_match_the_oracle(nx, coils, gpu_ctx):
+    """Sim widths 96, 160 and 192 (32 E with E = 3, 5, 6 -- 192 is the differentiation config's
+    grid): the warp FFT's E-point register DFT is a direct sum, the 96-point rows also go through
+    the coil-class x-stages."""
+    s = cases.series_case(nx=nx, ny=nx, nv=1, nz=1, ncomp=3)
+    acq = Acquisition(n_coils=coils, accel=2, partial_fourier=0.75, pf_mode=PartialFourierMode.Scanner, t_line=0.5,
+                      t_echo=30.0, ghost_offset=0.05, eddy_strength=2.0, eddy_quad=0.3)
+    tes = [15.0, 35.0]
+    kw = dict(t_inhom=s["t_inhom"], phase=PhaseModel.hbcd_like(), seed=42, eddy_drive=[(0.5, -0.4, 0.7)])
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], 1, s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
+    out = op.apply_host(None)
+    want = oracle.series_forward(s["sim_dims"], s["acq_dims"], 1, s["images"], s["t2"], s["fmap"], acq,
+                                 echo_times_ms=tes, **kw)
+    assert rel_l2(out["kspace"], want) <= TOL
+    adj = oracle.series_adjoint(s["sim_dims"], s["acq_dims"], 1, s["images"], s["t2"], s["fmap"], acq,
+                                out["kspace"].astype(np.complex128), echo_times_ms=tes, **kw)
+    for key in ("comp_grad", "fmap_grad", "r2_grad"):
+        e = rel_l2(out[key], adj[key])
+        assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
