@@ -69,3 +69,15 @@ def test_empty_slice_gives_zero_kspace(gpu_ctx):
     inp.compartments = [np.zeros_like(c) for c in inp.compartments]
     got = api.build_coil_kspaces(inp, acq, ctx=gpu_ctx)
     assert np.all(got == 0)
+
+
+@pytest.mark.parametrize("idx", [0, 11, 20, 33])
+def test_eight_ring_coils_match_the_oracle(idx, gpu_ctx):
+    """Eight ring coils put the per-slice forward on the coil-class kernels (5 classes of equal
+    ey rows + the coil offset, class rows through the x-stage); every coil against the oracle."""
+    name, inp, acq = cases.golden_cases()[idx]
+    acq = acq.replace(n_coils=8, accel=1, acs_lines=0)
+    got = api.build_coil_kspaces(inp, acq, ctx=gpu_ctx)
+    for q in range(8):
+        want = oracle.build_coil_kspace(inp, acq, q, 8)
+        assert rel_l2(got[q], want) <= TOL, f"{name} coil {q}: rel-L2 {rel_l2(got[q], want):.2e}"
