@@ -156,3 +156,20 @@ def test_invalid_inputs_fail_with_the_reference_messages(gpu_ctx):
         api.simulate_acquisition_echoes(inp, [inp.images, inp.images], acq, [40.0, 30.0], ctx=gpu_ctx)
     with pytest.raises(MrsimError, match="slice_z entries must be below nz_full 1"):
         api.simulate_acquisition_complex(inp, acq, AcquisitionOptions(slice_z=[3], nz_full=1), ctx=gpu_ctx)
+
+
+@pytest.mark.parametrize("maps", [False, True])
+def test_series_with_eight_ring_coils_matches_the_oracle(maps, gpu_ctx):
+    """Eight ring coils put the series on the coil-class forward (class rows through the x-stage);
+    GRAPPA, noise, spikes, recon and the coil combine downstream of it against the oracle."""
+    inp, acq = _series(nv=2, nz=2, maps=maps)
+    acq = acq.replace(n_coils=8)
+    opts = AcquisitionOptions(kspace_slices=[1], acquired=True, reconstructed=True, coil_images=True)
+    got = api.simulate_acquisition_complex(inp, acq, opts, ctx=gpu_ctx)
+    want = _oracle_series(inp, acq, opts)
+    z = got["re"] + 1j * got["im"]
+    w = want["re"] + 1j * want["im"]
+    assert rel_l2(z, w) <= TOL, rel_l2(z, w)
+    for key in ("acquired", "reconstructed", "coil_images", "combined"):
+        gw = want[key].view(np.complex64).reshape(got[key].shape)
+        assert rel_l2(got[key], gw) <= TOL, (key, rel_l2(got[key], gw))
