@@ -257,9 +257,10 @@ def run_ours(args, rank, world, local_rank):
                    "coils": acq.n_coils, "accel": acq.accel, "partial_fourier": acq.partial_fourier,
                    "samples_per_step_per_gpu": samples, "parallelism": f"weak x{world} (independent series)",
                    "l2": "inputs (236 MB images) larger than L2; no flush"},
-        "e2e": {"value": samples * world / (e2e_ms * 1e-3), "unit": "samples/s",
+        "e2e": {"value": samples * world / (e2e_ms * 1e-3) if e2e_steps else None, "unit": "samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "call": "mrsim_epi_operator_apply_host (host images in, k-space and gradients out)"},
+                "call": "mrsim_epi_operator_apply_host (host images in, k-space and gradients out)"
+                        + ("" if e2e_steps else "; not run (--no-e2e)")},
         "roofline": {"bound": "fp32", "kernel": dom_name,
                      "achieved": achieved, "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32,
                      "peak_source": "measured live: register FMA loop on this GPU (no FP32 entry in MEASURED_PEAKS.json)",

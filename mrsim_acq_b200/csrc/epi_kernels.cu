@@ -1556,11 +1556,18 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   const float inv_n = 1.0f / (float)(N * u.sny);
   const int kpos = nx - xs;
   float2* row = rb[warp];
-  if (CLS && !ADJ) {  // the tile's class rows: [line][v][x]
-    for (int e = threadIdx.x; e < (nr >> 3) * 6 * N; e += 256) {
-      const int jl = e / (6 * N), v = (e / N) % 6, x = e % N;
-      hsm[e] = u.g[((size_t)v * nl + r0 + jl) * N + x];
+  // forward: the 8 coils' ex rows ([q][x]) after the class rows of at most 4 lines (24 N float2)
+  float* exs = CLS ? reinterpret_cast<float*>(hsm + 24 * N) : nullptr;
+  if (CLS && !ADJ) {  // the tile's class rows, [line][v][x], as 16-byte pieces (N is even and the
+                      // rows of g start on 16-byte boundaries), and the ex rows
+    constexpr int HN = N / 2;
+    const float4* __restrict__ g4 = reinterpret_cast<const float4*>(u.g);
+    float4* h4 = reinterpret_cast<float4*>(hsm);
+    for (int e = threadIdx.x; e < (nr >> 3) * 6 * HN; e += 256) {
+      const int jl = e / (6 * HN), v = (e / HN) % 6, x2 = e % HN;
+      h4[e] = g4[((size_t)v * nl + r0 + jl) * HN + x2];
     }
+    for (int e = threadIdx.x; e < 8 * N; e += 256) exs[e] = u.geo.ex[e];
     __syncthreads();
   }
   // premodulation of the line's polarity times E_j(x) = e^{i2pi (cx xc + qx xc^2 + z) decay_j}
@@ -1576,6 +1583,19 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     }
     return md;
   };
+  // adjoint: the k-space samples of the warp's next row are loaded while the current row transforms
+  // (zero outside the acquired kx)
+  float2 pre[ADJ ? E : 1];
+  auto fetch = [&](int r) {
+    const float2* kr = u.kspace + ((size_t)rq[r] * u.n_rows + rrow[r]) * nx;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int n = lane + 32 * m;
+      const int kx = (n < kpos ? n : n - N) + xs;
+      pre[ADJ ? m : 0] = kx >= 0 && kx < nx ? kr[kx] : make_float2(0.f, 0.f);
+    }
+  };
+  if (ADJ && warp < nr) fetch(warp);
   for (int r = warp; r < nr; r += 8) {
     const int R = CLS ? (r & 7) * nl + r0 + (r >> 3) : r0 + r, q = rq[r], orow = rrow[r], pol = rpol[r];
     const float dec = rdec[r];
@@ -1586,7 +1606,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
-        const float ex = u.geo.ex[(size_t)q * N + x];
+        const float ex = exs[q * N + x];
         const float2 gv = cr[c * N + x], go = cr[5 * N + x];
         b[P2 ? bitrev_c(m, LE) : m] = cmul(make_float2(fmaf(ex, gv.x, go.x), fmaf(ex, gv.y, go.y)), modulation(pol, dec, x));
       }
@@ -1598,7 +1618,10 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
         b[P2 ? bitrev_c(m, LE) : m] = cmul(gr[x], modulation(pol, dec, x));
       }
     } else {
-      const float2* kr = u.kspace + ((size_t)q * u.n_rows + orow) * nx;
+      float2 cur[E];
+#pragma unroll
+      for (int m = 0; m < E; ++m) cur[m] = pre[ADJ ? m : 0];
+      if (r + 8 < nr) fetch(r + 8);
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int n = lane + 32 * m;
@@ -1606,7 +1629,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
         float2 v = make_float2(0.f, 0.f);
         if (kx >= 0 && kx < nx) {
           const float2 p = pt[kx];
-          v = cmul(kr[kx], make_float2(p.x, -p.y));
+          v = cmul(cur[m], make_float2(p.x, -p.y));
         }
         b[P2 ? bitrev_c(m, LE) : m] = v;
       }
@@ -1685,6 +1708,9 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   if (CLS && ADJ) {
     __syncthreads();
     const float s = u.signal_scale, so = s * u.geo.coil_off;
+    float* sex = reinterpret_cast<float*>(&rb[0][0]);  // s ex_q(x), [q][x], in the free reorder rows
+    for (int e = threadIdx.x; e < 8 * N; e += 256) sex[e] = s * u.geo.ex[e];
+    __syncthreads();
     const int nj = nr >> 3;
     for (int e = threadIdx.x; e < nj * N; e += 256) {
       const int jl = e / N, x = e % N;
@@ -1694,7 +1720,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const float2 h = hsm[(jl * 8 + q) * N + x];
-        const float ex = s * u.geo.ex[(size_t)q * N + x];
+        const float ex = sex[q * N + x];
         const int c = cls_s[q];
 #pragma unroll
         for (int v = 0; v < 5; ++v)
