@@ -193,7 +193,9 @@ void append_lines(std::vector<LineRec>& out, const mrsim_acquisition& acq, const
 
 // Zero `n` bytes at `p` with streaming (non-temporal) stores where the ISA has them: the write
 // does not first read the lines into the cache, so it takes half the memory traffic of a plain
-// memset and leaves the bandwidth to the concurrent device-to-host copies.
+// memset and leaves the bandwidth to the concurrent device-to-host copies.  Streaming stores are
+// weakly ordered: a thread calls stream_fence() once after its last zero_stream, before it ends
+// (a fence per call would drain the write-combining buffers on every 512-byte row).
 static void zero_stream(char* p, size_t n) {
 #if defined(__SSE2__)
   while (n > 0 && ((uintptr_t)p & 15)) {
@@ -208,10 +210,12 @@ static void zero_stream(char* p, size_t n) {
     _mm_stream_si128((__m128i*)(p + 48), z);
   }
   for (; n >= 16; n -= 16, p += 16) _mm_stream_si128((__m128i*)p, z);
+#endif
   std::memset(p, 0, n);
+}
+static void stream_fence() {
+#if defined(__SSE2__)
   _mm_sfence();
-#else
-  std::memset(p, 0, n);
 #endif
 }
 
@@ -569,6 +573,7 @@ void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* 
             y = y1;
           }
         }
+        stream_fence();
       });
   }
   for (int b = 0; b < ng; ++b) {
