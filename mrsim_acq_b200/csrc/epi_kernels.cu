@@ -1525,7 +1525,11 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   const int4 t = tiles[blockIdx.x];
   const UnitDesc& u = units[t.x];
   const int r0 = t.y, nr = CLS ? 8 * t.z : t.z;  // CLS: first line, lines
-  const int nx = u.nx, nl = u.n_lines;
+  const int nx = u.nx, nl = u.n_lines, n_rows = u.n_rows;
+  // the unit's buffers, read once: the row loop's warp barriers order memory, so the fields would
+  // otherwise be loaded again for every row
+  float2* const ksp = u.kspace;
+  float2* const gbuf = u.g;
   const float2* __restrict__ xf = u.geo.xf;
   for (int k = threadIdx.x; k < N / 2; k += 256) {
     const float2 w = xf[k];
@@ -1561,7 +1565,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   if (CLS && !ADJ) {  // the tile's class rows, [line][v][x], as 16-byte pieces (N is even and the
                       // rows of g start on 16-byte boundaries), and the ex rows
     constexpr int HN = N / 2;
-    const float4* __restrict__ g4 = reinterpret_cast<const float4*>(u.g);
+    const float4* __restrict__ g4 = reinterpret_cast<const float4*>(gbuf);
     float4* h4 = reinterpret_cast<float4*>(hsm);
     for (int e = threadIdx.x; e < (nr >> 3) * 6 * HN; e += 256) {
       const int jl = e / (6 * HN), v = (e / HN) % 6, x2 = e % HN;
@@ -1587,7 +1591,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   // (zero outside the acquired kx)
   float2 pre[ADJ ? E : 1];
   auto fetch = [&](int r) {
-    const float2* kr = u.kspace + ((size_t)rq[r] * u.n_rows + rrow[r]) * nx;
+    const float2* kr = ksp + ((size_t)rq[r] * n_rows + rrow[r]) * nx;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       const int n = lane + 32 * m;
@@ -1611,7 +1615,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
         b[P2 ? bitrev_c(m, LE) : m] = cmul(make_float2(fmaf(ex, gv.x, go.x), fmaf(ex, gv.y, go.y)), modulation(pol, dec, x));
       }
     } else if (!ADJ) {
-      const float2* gr = u.g + (size_t)R * N;
+      const float2* gr = gbuf + (size_t)R * N;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
@@ -1687,14 +1691,14 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     }
     __syncwarp();
     if (!ADJ) {
-      float2* out = u.kspace + ((size_t)q * u.n_rows + orow) * nx;
+      float2* out = ksp + ((size_t)q * n_rows + orow) * nx;
       for (int kx = lane; kx < nx; kx += 32) {
         const int k = ((kx - xs) % N + N) % N;
         const float2 v = cmul(row[k + (k >> 5)], pt[kx]);
         out[kx] = make_float2(v.x * inv_n, v.y * inv_n);
       }
     } else {
-      float2* gr = CLS ? hsm + ((r >> 3) * 8 + (r & 7)) * N : u.g + (size_t)R * N;
+      float2* gr = CLS ? hsm + ((r >> 3) * 8 + (r & 7)) * N : gbuf + (size_t)R * N;
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
@@ -1733,7 +1737,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
       }
       G[5] = make_float2(so * G[5].x, so * G[5].y);
 #pragma unroll
-      for (int v = 0; v < 6; ++v) u.g[((size_t)v * nl + r0 + jl) * N + x] = G[v];
+      for (int v = 0; v < 6; ++v) gbuf[((size_t)v * nl + r0 + jl) * N + x] = G[v];
     }
   }
 }
