@@ -1530,6 +1530,21 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   // otherwise be loaded again for every row
   float2* const ksp = u.kspace;
   float2* const gbuf = u.g;
+  // forward: the 8 coils' ex rows ([q][x]) after the class rows of at most 4 lines (24 N float2)
+  float* exs = CLS ? reinterpret_cast<float*>(hsm + 24 * N) : nullptr;
+  if (CLS && !ADJ) {  // the tile's class rows, [line][v][x], as 16-byte asynchronous copies issued
+                      // first, so that their latency overlaps the table setup (N is even and the
+                      // rows of g start on 16-byte boundaries); then the ex rows
+    constexpr int HN = N / 2;
+    const float4* g4 = reinterpret_cast<const float4*>(gbuf);
+    float4* h4 = reinterpret_cast<float4*>(hsm);
+    for (int e = threadIdx.x; e < (nr >> 3) * 6 * HN; e += 256) {
+      const int jl = e / (6 * HN), v = (e / HN) % 6, x2 = e % HN;
+      cp_async16(h4 + e, g4 + ((size_t)v * nl + r0 + jl) * HN + x2, 16);
+    }
+    cp_async_commit();
+    for (int e = threadIdx.x; e < 8 * N; e += 256) exs[e] = u.geo.ex[e];
+  }
   const float2* __restrict__ xf = u.geo.xf;
   for (int k = threadIdx.x; k < N / 2; k += 256) {
     const float2 w = xf[k];
@@ -1547,6 +1562,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     rpol[r] = L.pol < 0 ? 1 : 0;
     rdec[r] = L.decay;
   }
+  if (CLS && !ADJ) cp_async_wait0();
   __syncthreads();
   // W(j) = e^{sigma i2pi j/N}: sigma = +1 forward, -1 adjoint
   auto W = [&](int j) {
@@ -1560,20 +1576,6 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   const float inv_n = 1.0f / (float)(N * u.sny);
   const int kpos = nx - xs;
   float2* row = rb[warp];
-  // forward: the 8 coils' ex rows ([q][x]) after the class rows of at most 4 lines (24 N float2)
-  float* exs = CLS ? reinterpret_cast<float*>(hsm + 24 * N) : nullptr;
-  if (CLS && !ADJ) {  // the tile's class rows, [line][v][x], as 16-byte pieces (N is even and the
-                      // rows of g start on 16-byte boundaries), and the ex rows
-    constexpr int HN = N / 2;
-    const float4* __restrict__ g4 = reinterpret_cast<const float4*>(gbuf);
-    float4* h4 = reinterpret_cast<float4*>(hsm);
-    for (int e = threadIdx.x; e < (nr >> 3) * 6 * HN; e += 256) {
-      const int jl = e / (6 * HN), v = (e / HN) % 6, x2 = e % HN;
-      h4[e] = g4[((size_t)v * nl + r0 + jl) * HN + x2];
-    }
-    for (int e = threadIdx.x; e < 8 * N; e += 256) exs[e] = u.geo.ex[e];
-    __syncthreads();
-  }
   // premodulation of the line's polarity times E_j(x) = e^{i2pi (cx xc + qx xc^2 + z) decay_j}
   auto modulation = [&](int pol, float dec, int x) {
     float2 md = pm[pol * N + x];
