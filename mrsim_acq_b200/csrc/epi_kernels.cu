@@ -99,17 +99,17 @@ __device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
 
-// The reduced phase s + f t (s = static phase + k.r term, |s| <= 1 turn) on a pair of lanes with
-// one rounding to an integer: with p = f t_hi (product error e exact by FMA) and n = round(p + s),
-//   theta = ((p - n) + s) - (-(f t_lo + e)),   |theta| <= 1/2 + an ulp of p.
-// p - n is exact for |p| >= 1 (a multiple of ulp(p) below 2) and otherwise rounds at ulp(1), so
-// theta carries the rounding of the two-reduction form (ft_turns, then frac_turn) in fewer adds.
-__device__ __forceinline__ float2 phase_turns2(float2 s, float2 f, float2 nf, float2 t_hi, float2 t_lo) {
+// The reduced phase s + f t (s = static phase + k.r term, |s| <= 1 turn, t = t_hi + t_lo) on a pair
+// of lanes with one rounding to an integer: n = round(s + f t_hi) (the FMA's rounded value serves
+// only to choose n), r = f t_hi - n from one FMA of the exact product (|r| < 2: one rounding of
+// at most ulp(1)/2), and
+//   theta = (r + s) + f t_lo,   |theta| <= 1/2 + ulps,
+// whose last two roundings are at most ulp(1/2)/2 each: six packed operations.
+__device__ __forceinline__ float2 phase_turns2(float2 s, float2 f, float2 t_hi, float2 t_lo) {
   const float2 M = dup2(12582912.0f);
-  const float2 p = fmul2(f, t_hi);
-  const float2 en = ffma2(nf, t_hi, p);                     // -(exact error of the product)
-  const float2 n = fsub2(fadd2(fadd2(p, s), M), M);         // round(p + s)
-  return fsub2(fadd2(fsub2(p, n), s), ffma2(nf, t_lo, en));
+  const float2 nn = fsub2(M, fadd2(ffma2(f, t_hi, s), M));  // -n
+  const float2 r = ffma2(f, t_hi, nn);
+  return ffma2(f, t_lo, fadd2(r, s));
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
@@ -587,10 +587,10 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
       const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
       if (NV && !MAPS) {
         // lines (0, 1) and (2, 3) as packed pairs: the same arithmetic, two lanes per instruction
-        const float2 a2 = dup2(a), f2 = dup2(f), nf2 = dup2(-f);
+        const float2 a2 = dup2(a), f2 = dup2(f);
 #pragma unroll
         for (int jp = 0; jp < T; jp += 2) {
-          float2 th = phase_turns2(fadd2(a2, make_float2(bt[jp], bt[jp + 1])), f2, nf2,
+          float2 th = phase_turns2(fadd2(a2, make_float2(bt[jp], bt[jp + 1])), f2,
                                    make_float2(thi[jp], thi[jp + 1]), make_float2(tlo[jp], tlo[jp + 1]));
           th = fmul2(dup2(kTwoPiF), th);
           float s0, c0, s1, c1;
@@ -1148,8 +1148,7 @@ __global__ void __launch_bounds__(256, (VIRT && !MAPS && TY == 2) ? 3 : 2) yadjo
         for (int pp = 0; pp < NPR; ++pp) {
           const int t0 = 2 * pp, t1 = (2 * pp + 1) % TY;
           const float2 bt2 = btp[pp];
-          float2 th = phase_turns2(fadd2(make_float2(a[t0], a[t1]), bt2), make_float2(f[t0], f[t1]),
-                                   make_float2(-f[t0], -f[t1]), thi2, tlo2);
+          float2 th = phase_turns2(fadd2(make_float2(a[t0], a[t1]), bt2), make_float2(f[t0], f[t1]), thi2, tlo2);
           th = fmul2(dup2(kTwoPiF), th);
           float s0, c0, s1, c1;
           __sincosf(th.x, &s0, &c0);
