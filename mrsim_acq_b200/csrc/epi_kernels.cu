@@ -1745,7 +1745,11 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
 
 template <class K>
 void set_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024) MRSIM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  // past 48 KB of static + dynamic shared memory the launch needs the dynamic opt-in
+  cudaFuncAttributes fa;
+  MRSIM_CUDA(cudaFuncGetAttributes(&fa, kernel));
+  if (bytes + fa.sharedSizeBytes > 48 * 1024)
+    MRSIM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
 }  // namespace

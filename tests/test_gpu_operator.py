@@ -187,6 +187,28 @@ def test_128_point_rows_match_the_oracle(coils, eddy, gpu_ctx):
         assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
 
 
+def test_96_lines_per_unit_match_the_oracle(gpu_ctx):
+    """Full Fourier with R = 2 and three echoes: 96 lines per unit.  The class-mode y-adjoint then
+    takes ~45 KB of dynamic shared memory next to its 3 KB static piece table, over 48 KB together,
+    which its launch must opt into."""
+    s = cases.series_case(nx=64, ny=64, nv=1, nz=1, ncomp=3)
+    acq = Acquisition(n_coils=8, accel=2, partial_fourier=1.0, t_line=0.5, t_echo=30.0, ghost_offset=0.05)
+    tes = [20.0, 55.0, 90.0]  # a full-Fourier train reads from 15.25 ms before its echo
+    kw = dict(t_inhom=s["t_inhom"], phase=PhaseModel.hbcd_like(), seed=42)
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], 1, s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
+    assert op.samples == 1 * 1 * 3 * 32 * 8 * 64
+    out = op.apply_host(None)
+    want = oracle.series_forward(s["sim_dims"], s["acq_dims"], 1, s["images"], s["t2"], s["fmap"], acq,
+                                 echo_times_ms=tes, **kw)
+    assert rel_l2(out["kspace"], want) <= TOL
+    adj = oracle.series_adjoint(s["sim_dims"], s["acq_dims"], 1, s["images"], s["t2"], s["fmap"], acq,
+                                out["kspace"].astype(np.complex128), echo_times_ms=tes, **kw)
+    for key in ("comp_grad", "fmap_grad", "r2_grad"):
+        e = rel_l2(out[key], adj[key])
+        assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
+
+
 @pytest.mark.parametrize("nx,coils", [(48, 8), (80, 4), (96, 8)])
 def test_rows_of_32e_points_match_the_oracle(nx, coils, gpu_ctx):
     """Sim widths 96, 160 and 192 (32 E with E = 3, 5, 6 -- 192 is the differentiation config's
