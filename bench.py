@@ -134,10 +134,10 @@ def peaks():
 
 # DRAM bytes per unit (one slice of one volume) of the two y-stage kernels, from one ncu capture of
 # this workload at 24 volumes (720 units): dram__bytes.sum.per_second x gpu__time_duration.sum of
-# yadjoint_q_kernel<6,4,3,0,1,1> (945.7 MB) and ystage_q_kernel<8,6,3,0> (463.6 MB); the summaries are
+# yadjoint_q_kernel<6,4,3,0,1,1> (946.1 MB) and ystage_q_kernel<8,6,3,0> (463.5 MB); the summaries are
 # profiles/yadjoint_q_kernel_epi-series-sim128-v24.md and profiles/ystage_q_kernel_epi-series-sim128-v24.md.
 # Traffic grows with the units processed (each unit reads and writes its own planes).
-NCU_DRAM_BYTES_PER_UNIT = {"adjoint_ystage": 945.7e6 / 720, "forward_ystage": 463.6e6 / 720}
+NCU_DRAM_BYTES_PER_UNIT = {"adjoint_ystage": 946.1e6 / 720, "forward_ystage": 463.5e6 / 720}
 
 
 def algorithmic_flops(op_units, n_lines, snx, sny, nx, ncoils, ncomp):
