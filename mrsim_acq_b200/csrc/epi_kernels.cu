@@ -50,19 +50,16 @@ namespace {
 
 constexpr float kTwoPiF = 6.28318530717958647692f;
 
-// Round to the nearest integer on the FP32 pipe (|v| < 2^22): adding and subtracting 1.5*2^23
-// leaves v rounded to an integer; exact for the turn reductions below.
-__device__ __forceinline__ float round_fadd(float v) {
-  return __fadd_rn(__fadd_rn(v, 12582912.0f), -12582912.0f);
-}
-__device__ __forceinline__ float frac_turn(float v) { return __fadd_rn(v, -round_fadd(v)); }
-
-// Phase of voxel value f (Hz) at line time t = t_hi + t_lo (s), in turns, reduced.
-__device__ __forceinline__ float ft_turns(float f, float t_hi, float t_lo) {
-  float p = f * t_hi;
-  float e = fmaf(f, t_hi, -p);      // exact error of the product
-  float r = __fadd_rn(p, -round_fadd(p));  // exact
-  return r + fmaf(f, t_lo, e);
+// The reduced phase s + f t in turns (s = static phase + k.r term, |s| <= 1 turn; f the voxel's
+// off-resonance in Hz; t = t_hi + t_lo the line time in s, |f t| < 2^22) with one rounding to an
+// integer: n = round(s + f t_hi) by adding and subtracting 1.5 * 2^23 (the FMA's rounded value
+// serves only to choose n), r = f t_hi - n from one FMA of the exact product (|r| < 2: one rounding
+// of at most ulp(1)/2), and
+//   theta = (r + s) + f t_lo,   |theta| <= 1/2 + ulps,
+// whose last two roundings are at most ulp(1/2)/2 each.
+__device__ __forceinline__ float phase_turns(float s, float f, float t_hi, float t_lo) {
+  const float nn = __fsub_rn(12582912.0f, __fadd_rn(fmaf(f, t_hi, s), 12582912.0f));  // -n
+  return fmaf(f, t_lo, __fadd_rn(fmaf(f, t_hi, nn), s));
 }
 
 // Packed FP32 pairs (sm_100 add/sub/mul/fma.rn.f32x2): one instruction for two lanes, each lane
@@ -345,8 +342,7 @@ __global__ void __launch_bounds__(128, 4) ystage_kernel(const UnitDesc* __restri
     const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
     for (int j = 0; j < T; ++j) {
-      float th = a + bt[j] + ft_turns(f, thi[j], tlo[j]);
-      th = frac_turn(th);
+      const float th = phase_turns(a + bt[j], f, thi[j], tlo[j]);
       float sn, cs;
       __sincosf(kTwoPiF * th, &sn, &cs);
       float W = 0.f;
@@ -613,8 +609,7 @@ __global__ void __launch_bounds__(256, 2) ystage_q_kernel(const UnitDesc* __rest
       }
 #pragma unroll
       for (int j = 0; j < T; ++j) {
-        float th = a + bt[j] + ft_turns(f, thi[j], tlo[j]);
-        th = frac_turn(th);
+        const float th = phase_turns(a + bt[j], f, thi[j], tlo[j]);
         float sn, cs;
         __sincosf(kTwoPiF * th, &sn, &cs);
         float W = 0.f;
@@ -854,8 +849,7 @@ __global__ void __launch_bounds__(128) yadjoint_kernel(const UnitDesc* __restric
 #pragma unroll
       for (int ty = 0; ty < TY; ++ty) {
         const float hr = fmaf(soff, hsr, H[ty].x), hi = fmaf(soff, hsi, H[ty].y);
-        float th = a[ty] + bt[ty] + ft_turns(f[ty], thi, tlo);
-        th = frac_turn(th);
+        const float th = phase_turns(a[ty] + bt[ty], f[ty], thi, tlo);
         float sn, cs;
         __sincosf(kTwoPiF * th, &sn, &cs);
         const float zr = fmaf(cs, hr, sn * hi);  // Z = conj(P) * H
@@ -1195,8 +1189,7 @@ __global__ void __launch_bounds__(256, (VIRT && !MAPS && TY == 2) ? 3 : 2) yadjo
       const float tph = MAPS ? e[4] : 0.f;
 #pragma unroll
       for (int ty = 0; ty < TY; ++ty) {
-        float th = a[ty] + bt[ty] + ft_turns(f[ty], thi, tlo);
-        th = frac_turn(th);
+        const float th = phase_turns(a[ty] + bt[ty], f[ty], thi, tlo);
         float sn, cs;
         __sincosf(kTwoPiF * th, &sn, &cs);
         const float zr = fmaf(cs, H[ty].x, sn * H[ty].y);  // Z = conj(P) * H
