@@ -1664,17 +1664,25 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     }
 #pragma unroll
     for (int k1 = 1; k1 < E; ++k1) b[k1] = cmul(b[k1], W(lane * k1));
-    // 32-point DFTs across the lanes: radix-2 decimation in frequency
+    // 32-point DFTs across the lanes: radix-2 decimation in frequency.  The last two stages'
+    // twiddles are exact: 1 at h = 1, and 1 or W(N/4) = sigma i (a swap and a sign) at h = 2.
 #pragma unroll
     for (int h = 16; h >= 1; h >>= 1) {
       const bool up = (lane & h) != 0;
       const float sg = up ? -1.f : 1.f;
-      const float2 w = up ? W((lane & (h - 1)) * (N / (2 * h))) : make_float2(1.f, 0.f);
+      const float2 w = h >= 4 && up ? W((lane & (h - 1)) * (N / (2 * h))) : make_float2(1.f, 0.f);
+      const bool quarter = h == 2 && up && (lane & 1);
 #pragma unroll
       for (int k1 = 0; k1 < E; ++k1) {
         const float ox_ = __shfl_xor_sync(0xffffffffu, b[k1].x, h);
         const float oy_ = __shfl_xor_sync(0xffffffffu, b[k1].y, h);
-        b[k1] = cmul(make_float2(fmaf(sg, b[k1].x, ox_), fmaf(sg, b[k1].y, oy_)), w);
+        const float2 v = make_float2(fmaf(sg, b[k1].x, ox_), fmaf(sg, b[k1].y, oy_));
+        if (h >= 4)
+          b[k1] = cmul(v, w);
+        else if (h == 2)  // times sigma i: -i for the adjoint (e^{-i pi/2}), +i for the forward
+          b[k1] = quarter ? (ADJ ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x)) : v;
+        else
+          b[k1] = v;
       }
     }
     const int k2 = __brev(lane) >> 27;
