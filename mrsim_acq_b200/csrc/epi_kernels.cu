@@ -1543,8 +1543,17 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
     tw[k] = w;
     tw[k + N / 2] = make_float2(-w.x, -w.y);
   }
-  for (int k = threadIdx.x; k < 2 * N; k += 256) pm[k] = xf[N / 2 + k];
-  for (int k = threadIdx.x; k < nx; k += 256) pt[k] = xf[N / 2 + 2 * N + k];
+  // the output side's table carries the 1/(N sny) scale: the post-twiddle in the forward, the
+  // premodulation in the adjoint
+  const float inv_n = 1.0f / (float)(N * u.sny);
+  for (int k = threadIdx.x; k < 2 * N; k += 256) {
+    const float2 v = xf[N / 2 + k];
+    pm[k] = ADJ ? make_float2(v.x * inv_n, v.y * inv_n) : v;
+  }
+  for (int k = threadIdx.x; k < nx; k += 256) {
+    const float2 v = xf[N / 2 + 2 * N + k];
+    pt[k] = ADJ ? v : make_float2(v.x * inv_n, v.y * inv_n);
+  }
   if (CLS && threadIdx.x < 8) cls_s[threadIdx.x] = u.geo.cls[threadIdx.x];
   for (int r = threadIdx.x; r < nr; r += 256) {
     const int R = CLS ? (r & 7) * nl + r0 + (r >> 3) : r0 + r;  // CLS: row r = (line r / 8, coil r % 8)
@@ -1565,7 +1574,6 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
   const int ox = N / nx, xs = nx / 2, sxs = ox * xs;
   const double xoff = (ox - 1.0) / 2.0;
   const bool eddy = (u.flags & UF_EDDY) != 0;
-  const float inv_n = 1.0f / (float)(N * u.sny);
   const int kpos = nx - xs;
   float2* row = rb[warp];
   // premodulation of the line's polarity times E_j(x) = e^{i2pi (cx xc + qx xc^2 + z) decay_j}
@@ -1655,7 +1663,11 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
 #pragma unroll
         for (int p = 0; p < len / 2; ++p) {
           float2 v = b[i + p + len / 2];
-          if (p != 0) v = cmul(v, W(p * (E / len) * 32));
+          const int j = p * (E / len) * 32;
+          if (4 * j == N)  // W(N/4) = sigma i exactly
+            v = ADJ ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
+          else if (p != 0)
+            v = cmul(v, W(j));
           const float2 a = b[i + p];
           b[i + p] = make_float2(a.x + v.x, a.y + v.y);
           b[i + p + len / 2] = make_float2(a.x - v.x, a.y - v.y);
@@ -1696,8 +1708,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
       float2* out = ksp + ((size_t)q * n_rows + orow) * nx;
       for (int kx = lane; kx < nx; kx += 32) {
         const int k = ((kx - xs) % N + N) % N;
-        const float2 v = cmul(row[k + (k >> 5)], pt[kx]);
-        out[kx] = make_float2(v.x * inv_n, v.y * inv_n);
+        out[kx] = cmul(row[k + (k >> 5)], pt[kx]);
       }
     } else {
       float2* gr = CLS ? hsm + ((r >> 3) * 8 + (r & 7)) * N : gbuf + (size_t)R * N;
@@ -1705,8 +1716,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) xfft_warp_kernel(const Un
       for (int m = 0; m < E; ++m) {
         const int x = lane + 32 * m;
         const float2 md = modulation(pol, dec, x);
-        const float2 v = cmul(row[x + (x >> 5)], make_float2(md.x, -md.y));
-        gr[x] = make_float2(v.x * inv_n, v.y * inv_n);
+        gr[x] = cmul(row[x + (x >> 5)], make_float2(md.x, -md.y));
       }
     }
     __syncwarp();
