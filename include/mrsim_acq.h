@@ -296,6 +296,11 @@ int mrsim_epi_operator_buffers(mrsim_epi_operator* op, float** images, float** k
                                float** comp_grad, float** fmap_grad, float** r2_grad);
 /* Copy host images (reference layout: ncomp arrays of vox*n_volumes + g) to the device. */
 int mrsim_epi_operator_upload_images(mrsim_epi_operator* op, const float* const* images);
+/* Replace the fieldmap (Hz, [z][sny][snx] f32 host array, the layout of `in->fmap`) for every
+ * forward and adjoint queued after the call, which returns once the copy is done: the update
+ * step of a fieldmap fit by gradient descent on fmap_grad.  No reference counterpart (the
+ * reference takes its fieldmap per simulation call and has no adjoint). */
+int mrsim_epi_operator_set_fieldmap(mrsim_epi_operator* op, const float* fmap);
 /* Asynchronous on the context stream: statics + forward into the k-space buffer. */
 int mrsim_epi_operator_forward(mrsim_epi_operator* op);
 /* Asynchronous: adjoint / VJP of the k-space buffer's current contents. */

@@ -244,6 +244,7 @@ def _declare(lib):
         "mrsim_epi_operator_samples": (C.c_int64, [P]),
         "mrsim_epi_operator_buffers": (C.c_int, [P] + [C.POINTER(c_f32p)] * 5),
         "mrsim_epi_operator_upload_images": (C.c_int, [P, C.POINTER(c_f32p)]),
+        "mrsim_epi_operator_set_fieldmap": (C.c_int, [P, c_f32p]),
         "mrsim_epi_operator_forward": (C.c_int, [P]),
         "mrsim_epi_operator_adjoint": (C.c_int, [P]),
         "mrsim_epi_operator_stage": (C.c_int, [P, C.c_int32]),

@@ -617,6 +617,15 @@ class EpiOperator:
         keep = _Keep()
         check(lib().mrsim_epi_operator_upload_images(self.handle, keep.ptrs([np.ravel(a) for a in images])))
 
+    def set_fieldmap(self, fmap: np.ndarray):
+        """Replace the fieldmap (Hz, [z][sny][snx] or flat, float32) for the forwards and adjoints
+        after this call."""
+        snx, sny, nz = self.sim_dims
+        f = np.ascontiguousarray(fmap, np.float32).ravel()
+        if f.size != snx * sny * nz:
+            raise ValueError(f"fieldmap has {f.size} values, the operator {snx * sny * nz}")
+        check(lib().mrsim_epi_operator_set_fieldmap(self.handle, C.cast(f.ctypes.data, abi.c_f32p)))
+
     def forward(self):
         check(lib().mrsim_epi_operator_forward(self.handle))
 

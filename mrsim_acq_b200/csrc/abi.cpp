@@ -447,6 +447,14 @@ int mrsim_epi_operator_upload_images(mrsim_epi_operator* op, const float* const*
   });
 }
 
+int mrsim_epi_operator_set_fieldmap(mrsim_epi_operator* op, const float* fmap) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    need(fmap, "fmap");
+    mrsim::epi_operator_set_fieldmap(op->impl, fmap);
+  });
+}
+
 int mrsim_epi_operator_forward(mrsim_epi_operator* op) {
   if (!op) return guarded([] { need(nullptr, "operator"); });
   return on_ctx(op->impl->ctx, [&] { mrsim::epi_operator_forward(op->impl); });

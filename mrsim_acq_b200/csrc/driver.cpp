@@ -451,6 +451,14 @@ void upload_series_images(EpiOperator* op, const float* const* host_images) {
   launch_series_transpose(staging, op->d_images, op->ncomp, op->nv, op->nz, (int)plane, st);
 }
 
+// A new fieldmap (Hz, [z][sny][snx], the creation layout) for the forwards and adjoints queued
+// after it: the kernels read the device copy directly, and nothing at creation derives from it.
+void epi_operator_set_fieldmap(EpiOperator* op, const float* fmap) {
+  cudaStream_t st = op->ctx->stream;
+  MRSIM_CUDA(cudaMemcpyAsync(op->d_fmap, fmap, (size_t)op->nz * op->snx * op->sny * 4, cudaMemcpyHostToDevice, st));
+  MRSIM_CUDA(cudaStreamSynchronize(st));
+}
+
 void epi_operator_forward(EpiOperator* op) {
   cudaStream_t st = op->ctx->stream;
   epi_plan_statics(op->plan.get(), st);

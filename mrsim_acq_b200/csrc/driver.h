@@ -62,6 +62,7 @@ EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_inp
                                  const double* echo_times_ms, int64_t n_echoes, const int64_t* slice_z,
                                  int64_t nz_full, int grads);
 void upload_series_images(EpiOperator* op, const float* const* host_images);
+void epi_operator_set_fieldmap(EpiOperator* op, const float* fmap);
 void epi_operator_forward(EpiOperator* op);
 void epi_operator_adjoint(EpiOperator* op);
 // Forward + adjoint from host images to host k-space and gradients (any output may be NULL),
