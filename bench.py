@@ -21,6 +21,7 @@ import json
 import math
 import os
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -97,7 +98,10 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        # the samples go to a temporary file unless MRSIM_CLOCKS_DIR names a folder to keep them in
+        keep = os.environ.get("MRSIM_CLOCKS_DIR")
+        folder = keep if keep else tempfile.mkdtemp(prefix="mrsim_clocks_")
+        self.path = os.path.join(folder, f"clocks_rank{device}.csv")
 
     def start(self):
         try:
@@ -134,8 +138,7 @@ def peaks():
 
 # DRAM bytes per unit (one slice of one volume) of the two y-stage kernels, from one ncu capture of
 # this workload at 24 volumes (720 units): dram__bytes.sum.per_second x gpu__time_duration.sum of
-# yadjoint_q_kernel<6,4,3,0,1,1> (946.1 MB) and ystage_q_kernel<8,6,3,0> (463.5 MB); the summaries are
-# profiles/yadjoint_q_kernel_epi-series-sim128-v24.md and profiles/ystage_q_kernel_epi-series-sim128-v24.md.
+# yadjoint_q_kernel<6,4,3,0,1,1> (946.1 MB) and ystage_q_kernel<8,6,3,0> (463.5 MB).
 # Traffic grows with the units processed (each unit reads and writes its own planes).
 NCU_DRAM_BYTES_PER_UNIT = {"adjoint_ystage": 946.1e6 / 720, "forward_ystage": 463.5e6 / 720}
 

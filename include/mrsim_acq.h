@@ -7,7 +7,7 @@
  * the spiral pieces (NUFFT pair, certified time segmentation, spiral forwards and
  * reconstruction, trajectory and EPG).  Every entry point cites the reference item it replaces as
  * `file:line` within the reference crate.  A Rust shim behind a `gpu` cargo feature binds these
- * symbols one for one (see INTEGRATION.md for the `extern "C"` block).
+ * symbols one for one in an `extern "C"` block.
  *
  * Conventions
  *  - Plain pointers and sizes; no C++ or torch types cross the boundary.
@@ -253,9 +253,12 @@ int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisitio
  * when the output is complete.  Intermediates live in static device arrays of ~7.8 MiB held by
  * every GPU that loads the library until exit; limits: n_coils*acquired_lines*snx <= 524288,
  * snx*sny <= 262144, snx*nx <= 65536, n_coils*max(snx,sny) <= 32768, acquired lines <= 1024 —
- * larger inputs fail with MRSIM_ERR_INVALID.  The first call on a device looks up the arrays'
- * addresses (cudaGetSymbolAddress, that device current); make it before any stream capture.
- * Calls share the arrays: calls that overlap on the GPU race and must be serialised. */
+ * larger inputs fail with MRSIM_ERR_INVALID, and so does a data pointer that is not device (or
+ * managed) memory of the current device.  The first call on a device, and the first after that
+ * device's context changed (e.g. after cudaDeviceReset), looks up the arrays' addresses
+ * (cudaGetSymbolAddress, that device current); make the first call before any stream capture
+ * begins.  Each call waits for `stream` before it returns.  Calls share the arrays: calls that
+ * overlap on the GPU race and must be serialised. */
 int mrsim_build_coil_kspaces_noalloc(const mrsim_slice_input* inp, const mrsim_acquisition* acq,
                                      void* stream, float* kspace);
 

@@ -384,6 +384,7 @@ int mrsim_build_coil_kspaces_noalloc(const mrsim_slice_input* inp, const mrsim_a
     need(inp, "inp");
     need(acq, "acq");
     need(kspace, "kspace");
+    check_slice_input(*inp, *acq);
     mrsim::build_coil_kspaces_noalloc(*inp, *acq, (float2*)kspace, (cudaStream_t)stream);
   });
 }

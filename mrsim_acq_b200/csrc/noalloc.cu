@@ -14,9 +14,16 @@
 //  - every GPU that loads the library holds these arrays (about 7.8 MiB) until the process exits;
 //  - the sizes are capped (see the limits below); larger slices are rejected with an error;
 //  - the first call on a device resolves the arrays' device addresses with cudaGetSymbolAddress
-//    (with that device current) and caches them; make that first call before any stream capture;
+//    (with that device current) and caches them with the identity of the device's current CUDA
+//    context; a later call in another context (after cudaDeviceReset, say) resolves them again.
+//    Make the first call before any stream capture begins;
+//  - every call checks that its data pointers are device (or managed) memory of the current
+//    device, so a host pointer passed by mistake is an error, not a device fault;
+//  - each call waits for its stream before it returns (the host tables it stages must outlive
+//    their copies);
 //  - every call shares the arrays, which keep the last call's contents: calls that overlap on
 //    the GPU (two streams, or two host threads) race on them and must be serialised by the caller.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -62,6 +69,7 @@ struct NaAddrs {
   StaticDesc* statics = nullptr;
   int4* ytiles = nullptr;
   XTile* xtiles = nullptr;
+  unsigned long long ctx_id = 0;
   bool ready = false;
 };
 
@@ -69,11 +77,41 @@ constexpr int kMaxDevices = 64;
 NaAddrs g_addrs[kMaxDevices];
 std::mutex g_addr_mu;
 
-// Set-up, once per device, with that device current: the arrays' device addresses.
+// The identity of the calling thread's current CUDA context (0 when it cannot be told): the
+// driver's cuCtxGetCurrent / cuCtxGetId, reached through the runtime's entry-point query so that
+// the library needs no link against the driver library.
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (GetCurrent)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (GetId)f;
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Set-up, once per device (and again if the device's context changed), with that device
+// current: the arrays' device addresses.
 const NaAddrs& addresses(int device) {
   std::lock_guard<std::mutex> lk(g_addr_mu);
   NaAddrs& a = g_addrs[device];
-  if (!a.ready) {
+  const unsigned long long id = current_context_id();
+  if (!a.ready || a.ctx_id != id) {
+    a.ready = false;
     void* p = nullptr;
     MRSIM_CUDA(cudaGetSymbolAddress(&p, na_scratch));
     a.scratch = (float2*)p;
@@ -95,9 +133,27 @@ const NaAddrs& addresses(int device) {
     a.ytiles = (int4*)p;
     MRSIM_CUDA(cudaGetSymbolAddress(&p, na_xtiles));
     a.xtiles = (XTile*)p;
+    a.ctx_id = id;
     a.ready = true;
   }
   return a;
+}
+
+// A data pointer the kernels will read or write must be device (or managed) memory that the
+// current device can reach; cudaPointerGetAttributes allocates nothing.
+void need_device_pointer(const void* p, const char* what, int device) {
+  if (!p) fail(std::string("mrsim_build_coil_kspaces_noalloc: ") + what + " is NULL");
+  cudaPointerAttributes at;
+  std::memset(&at, 0, sizeof at);
+  cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();  // clear the (non-sticky) error the query left behind
+    fail(std::string("mrsim_build_coil_kspaces_noalloc: ") + what + " is not a device pointer");
+  }
+  const bool ok = (at.type == cudaMemoryTypeDevice && at.device == device) || at.type == cudaMemoryTypeManaged;
+  if (!ok)
+    fail(std::string("mrsim_build_coil_kspaces_noalloc: ") + what +
+         " must be device memory of the current device (host memory was passed)");
 }
 
 void too_big(const char* what, size_t need, size_t cap) {
@@ -128,6 +184,11 @@ void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquis
   int dev = 0;
   MRSIM_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) fail("device ordinal out of range");
+  // every pointer a kernel dereferences: device memory of this device, checked before any copy
+  for (int c = 0; c < ncomp; ++c) need_device_pointer(inp.compartments[c], "a compartment plane", dev);
+  need_device_pointer(inp.fmap, "fmap", dev);
+  if (inp.phase0) need_device_pointer(inp.phase0, "phase0", dev);
+  need_device_pointer(out, "kspace", dev);
   const NaAddrs& A = addresses(dev);
 
   const bool eddy = acq.eddy_strength != 0.0 && inp.has_eddy_drive;

@@ -15,6 +15,7 @@ from tests import cases
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
 GOLD = pathlib.Path(__file__).resolve().parent / "golden" / "p4_baseline" / "default"
+GOLD_KSPACE = GOLD.parent / "kspace"
 
 
 def rel_l2(a, b):
@@ -28,6 +29,24 @@ def test_golden_slices_match_the_reference_record(idx, gpu_ctx):
     got = api.simulate_slice(inp, acq, ctx=gpu_ctx)
     want = np.fromfile(GOLD / f"{name}.bin", dtype="<f4").view(np.complex64).reshape(got.shape)
     assert rel_l2(got, want) <= TOL, f"{name}: rel-L2 {rel_l2(got, want):.2e}"
+
+
+@pytest.mark.parametrize("idx", range(39))
+def test_golden_slices_match_the_kspace_build_record(idx, gpu_ctx):
+    """The reference's `kspace` build record (NUFFT y-stage, FFT x-stage and inverse)."""
+    name, inp, acq = cases.golden_cases()[idx]
+    got = api.simulate_slice(inp, acq, ctx=gpu_ctx)
+    want = np.fromfile(GOLD_KSPACE / f"{name}.bin", dtype="<f4").view(np.complex64).reshape(got.shape)
+    assert rel_l2(got, want) <= TOL, f"{name}: rel-L2 {rel_l2(got, want):.2e}"
+
+
+@pytest.mark.parametrize("idx", range(2))
+def test_golden_series_match_the_kspace_build_record(idx, gpu_ctx):
+    name, inp, acq = cases.golden_series_inputs()[idx]
+    mag, ph = api.simulate_acquisition_oversampled(inp, acq, ctx=gpu_ctx)
+    raw = np.fromfile(GOLD_KSPACE / f"{name}.bin", dtype="<f4")
+    gm, gp = raw[: raw.size // 2], raw[raw.size // 2:]
+    assert rel_l2(mag * np.exp(1j * ph), gm * np.exp(1j * gp)) <= TOL
 
 
 @pytest.mark.parametrize("idx", range(2))
