@@ -325,6 +325,25 @@ int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace,
 int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images,
                                   float* kspace, float* comp_grad, float* fmap_grad,
                                   float* r2_grad);
+/* The time-segmented y-stages of the pair (the north star's tensor-core form of the exact DFT; no
+ * reference counterpart: the reference segments only the spiral forward, `tseg::plan`
+ * tseg.rs:230-289 via spiral.rs:141-201).  precision 0 restores the exact per-line phasors;
+ * 1 selects contractions in split f16 (hi + lo operands, three products, FP32 accumulation),
+ * 2 in split bf16.  The lines of each echo (and side of the spin echo) share a segmentation of
+ * the fieldmap phase and the relaxation certified by the reference's planner to 1e-7, so the
+ * y-stage becomes dense complex contractions on the tensor cores (tcgen05, TMEM accumulators,
+ * TMA-loaded constant tables).  Needs uniform T2 / T2', no eddy-current polynomial, at most 4
+ * compartments, sny a multiple of 8, and grads = 0 (the complex-image adjoint only); otherwise
+ * MRSIM_ERR_INVALID.  A fieldmap set later outside the certified range rebuilds the tables. */
+int mrsim_epi_operator_set_segmented(mrsim_epi_operator* op, int32_t precision);
+/* The segmentation in use: groups, per-group segment counts L (max_groups entries) and
+ * certified bounds, and the tensor-pipe FLOP of one forward and one adjoint pass (three split
+ * products per complex MAC pair).  *n_groups = 0 when the exact path is selected. */
+int mrsim_epi_operator_segmentation(const mrsim_epi_operator* op, int32_t* n_groups, int32_t* seg_l,
+                                    double* bound, int32_t max_groups, double* flops_forward,
+                                    double* flops_adjoint);
+/* 0, or the code of a wait inside the segmented kernels that gave up (synchronises the stream). */
+int mrsim_epi_operator_segmented_status(mrsim_epi_operator* op, int32_t* code);
 /* Bytes one mrsim_epi_operator_apply_host call moves between host and device with every input
  * and output given: the images up; the acquired k-space rows (the other rows are zero-filled on
  * the host when the acquired rows form a uniform stride, else every row) and the gradients down. */

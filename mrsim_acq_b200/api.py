@@ -686,6 +686,30 @@ class EpiOperator:
                                                     p(out["r2_grad"])))
         return out
 
+    SEGMENTED = {"exact": 0, "f16": 1, "bf16": 2}
+
+    def set_segmented(self, precision: str = "f16"):
+        """Select the y-stages: "exact" (per-line phasors, FP32), or the time-segmented tensor-core
+        contractions in split "f16" or split "bf16" (`mrsim_epi_operator_set_segmented`)."""
+        check(lib().mrsim_epi_operator_set_segmented(self.handle, self.SEGMENTED[precision]))
+
+    def segmentation(self) -> dict:
+        """The segmentation in use: per-group segment counts and certified bounds, and the tensor
+        FLOP of one forward and one adjoint pass (empty lists on the exact path)."""
+        n = C.c_int32()
+        ls = (C.c_int32 * 64)()
+        bs = (C.c_double * 64)()
+        ff, fa = C.c_double(), C.c_double()
+        check(lib().mrsim_epi_operator_segmentation(self.handle, C.byref(n), ls, bs, 64, C.byref(ff), C.byref(fa)))
+        k = min(int(n.value), 64)
+        return {"L": [int(ls[i]) for i in range(k)], "bound": [float(bs[i]) for i in range(k)],
+                "flops_forward": float(ff.value), "flops_adjoint": float(fa.value)}
+
+    def segmented_status(self) -> int:
+        code = C.c_int32()
+        check(lib().mrsim_epi_operator_segmented_status(self.handle, C.byref(code)))
+        return int(code.value)
+
     def close(self):
         if getattr(self, "handle", None):
             lib().mrsim_epi_operator_destroy(self.handle)

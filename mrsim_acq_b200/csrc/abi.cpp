@@ -8,6 +8,7 @@
 #include <string>
 
 #include "driver.h"
+#include "ts_epi.h"
 #include "host_tables.h"
 #include "mrsim_internal.h"
 #include "series.h"
@@ -473,12 +474,56 @@ int mrsim_epi_operator_stage(mrsim_epi_operator* op, int32_t stage) {
     cudaStream_t st = op->impl->ctx->stream;
     switch (stage) {
       case 0: mrsim::epi_plan_statics(p, st); break;
-      case 1: mrsim::epi_plan_forward_ystage(p, st); break;
+      case 1:
+        if (op->impl->ts)
+          mrsim::ts_forward_ystage(*op->impl->ts, *p, st);
+        else
+          mrsim::epi_plan_forward_ystage(p, st);
+        break;
       case 2: mrsim::epi_plan_forward_xstage(p, st); break;
       case 3: mrsim::epi_plan_adjoint_xstage(p, st); break;
-      case 4: mrsim::epi_plan_adjoint_ystage(p, st); break;
+      case 4:
+        if (op->impl->ts)
+          mrsim::ts_adjoint_ystage(*op->impl->ts, *p, st);
+        else
+          mrsim::epi_plan_adjoint_ystage(p, st);
+        break;
       default: mrsim::fail("stage must be 0..4");
     }
+  });
+}
+
+int mrsim_epi_operator_set_segmented(mrsim_epi_operator* op, int32_t precision) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    MRSIM_CUDA(cudaStreamSynchronize(op->impl->ctx->stream));
+    mrsim::epi_operator_set_segmented(op->impl, precision);
+  });
+}
+
+int mrsim_epi_operator_segmentation(const mrsim_epi_operator* op, int32_t* n_groups, int32_t* seg_l, double* bound,
+                                    int32_t max_groups, double* flops_forward, double* flops_adjoint) {
+  return guarded([&] {
+    need(op, "operator");
+    need(n_groups, "n_groups");
+    const mrsim::TsPlan* t = op->impl->ts;
+    *n_groups = t ? t->n_groups : 0;
+    if (t) {
+      for (int g = 0; g < t->n_groups && g < max_groups; ++g) {
+        if (seg_l) seg_l[g] = t->L[g];
+        if (bound) bound[g] = t->bound[g];
+      }
+    }
+    if (flops_forward) *flops_forward = t ? t->flops_fwd : 0.0;
+    if (flops_adjoint) *flops_adjoint = t ? t->flops_adj : 0.0;
+  });
+}
+
+int mrsim_epi_operator_segmented_status(mrsim_epi_operator* op, int32_t* code) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    need(code, "code");
+    *code = mrsim::epi_operator_segmented_error(op->impl);
   });
 }
 

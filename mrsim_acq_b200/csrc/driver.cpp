@@ -18,6 +18,7 @@
 #include "host_tables.h"
 #include "mrsim_internal.h"
 #include "noise_kernels.h"
+#include "ts_epi.h"
 
 namespace mrsim {
 
@@ -222,6 +223,7 @@ static void stream_fence() {
 // =============================================================================================
 // The batched forward/adjoint operator of a 2D EPI series.
 EpiOperator::~EpiOperator() {
+  ts_plan_destroy(ts);
   for (cudaEvent_t e : events) cudaEventDestroy(e);
   if (copy_stream) cudaStreamDestroy(copy_stream);
   if (upload_stream) cudaStreamDestroy(upload_stream);
@@ -299,6 +301,16 @@ EpiOperator* epi_operator_create(mrsim_context* ctx, const mrsim_acquisition_inp
       }
   }
   op->n_lines = (int)lines.size();
+  op->acq = acq;
+  op->tes = tes;
+  op->h_lines = lines;
+  op->h_fmap.assign(in.fmap, in.fmap + (size_t)nz * snx * sny);
+  for (int c = 0; c < kMaxComp; ++c) {
+    op->t2u[c] = t2u[c];
+    op->tiu[c] = tiu[c];
+  }
+  op->maps = maps;
+  op->any_eddy = any_eddy;
   {
     // the acquired rows: the same arithmetic progression of ky in every echo?
     std::vector<std::vector<int>> ky(ne);
@@ -453,19 +465,56 @@ void upload_series_images(EpiOperator* op, const float* const* host_images) {
 
 // A new fieldmap (Hz, [z][sny][snx], the creation layout) for the forwards and adjoints queued
 // after it: the kernels read the device copy directly, and nothing at creation derives from it.
+// With the time-segmented path selected, a fieldmap outside the range its segmentation certified
+// rebuilds the segmentation and its tables.
 void epi_operator_set_fieldmap(EpiOperator* op, const float* fmap) {
   cudaStream_t st = op->ctx->stream;
-  MRSIM_CUDA(cudaMemcpyAsync(op->d_fmap, fmap, (size_t)op->nz * op->snx * op->sny * 4, cudaMemcpyHostToDevice, st));
+  const size_t n = (size_t)op->nz * op->snx * op->sny;
+  MRSIM_CUDA(cudaMemcpyAsync(op->d_fmap, fmap, n * 4, cudaMemcpyHostToDevice, st));
+  op->h_fmap.assign(fmap, fmap + n);
   MRSIM_CUDA(cudaStreamSynchronize(st));
+  if (op->ts && op->acq.do_distortions) {
+    const auto mm = std::minmax_element(op->h_fmap.begin(), op->h_fmap.end());
+    if (*mm.first < op->ts->fmin || *mm.second > op->ts->fmax) epi_operator_set_segmented(op, op->ts_precision);
+  }
+}
+
+// Selects the y-stages: 0 the exact per-line phasors, 1 / 2 the time-segmented tensor-core
+// contractions in split f16 / split bf16 (built here: segmentation, tables, tensor maps).
+void epi_operator_set_segmented(EpiOperator* op, int precision) {
+  TsPlan* fresh = precision ? ts_plan_build(*op, precision) : nullptr;
+  ts_plan_destroy(op->ts);
+  op->ts = fresh;
+  op->ts_precision = precision;
+}
+
+void epi_operator_forward_units(EpiOperator* op, cudaStream_t st, int u0, int u1) {
+  if (op->ts) {
+    ts_forward_ystage(*op->ts, *op->plan, st, u0, u1);
+    epi_plan_forward_xstage(op->plan.get(), st, u0, u1);
+  } else {
+    epi_plan_forward(op->plan.get(), st, u0, u1);
+  }
+}
+
+void epi_operator_adjoint_units(EpiOperator* op, cudaStream_t st, int u0, int u1) {
+  if (op->ts) {
+    epi_plan_adjoint_xstage(op->plan.get(), st, u0, u1);
+    ts_adjoint_ystage(*op->ts, *op->plan, st, u0, u1);
+  } else {
+    epi_plan_adjoint(op->plan.get(), st, u0, u1);
+  }
 }
 
 void epi_operator_forward(EpiOperator* op) {
   cudaStream_t st = op->ctx->stream;
   epi_plan_statics(op->plan.get(), st);
-  epi_plan_forward(op->plan.get(), st);
+  epi_operator_forward_units(op, st, 0, -1);
 }
 
-void epi_operator_adjoint(EpiOperator* op) { epi_plan_adjoint(op->plan.get(), op->ctx->stream); }
+void epi_operator_adjoint(EpiOperator* op) { epi_operator_adjoint_units(op, op->ctx->stream, 0, -1); }
+
+int epi_operator_segmented_error(EpiOperator* op) { return op->ts ? ts_error(*op->ts, op->ctx->stream) : 0; }
 
 void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* kspace, float* comp_grad,
                              float* fmap_grad, float* r2_grad) {
@@ -525,9 +574,9 @@ void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* 
                                 nz >= 2 ? B.z1 : nz);
     }
     const int u0 = B.z0 * nv + B.g0, u1 = (B.z1 - 1) * nv + B.g1;  // slice-major plan units
-    epi_plan_forward(p, st, u0, u1);
+    epi_operator_forward_units(o, st, u0, u1);
     MRSIM_CUDA(cudaEventRecord(ev[3 * b + 1], st));
-    epi_plan_adjoint(p, st, u0, u1);
+    epi_operator_adjoint_units(o, st, u0, u1);
     MRSIM_CUDA(cudaEventRecord(ev[3 * b + 2], st));
   }
   // downloads: the box is nv' rows (volumes) of (z1 - z0) units, pitch nz units

@@ -10,6 +10,9 @@
 
 namespace mrsim {
 
+struct TsPlan;
+void ts_plan_destroy(TsPlan* p);
+
 // Device allocations owned by one object, freed together.
 struct DevArena {
   std::vector<void*> ptrs;
@@ -55,6 +58,16 @@ struct EpiOperator {
   // host-buffer apply: download and upload streams and per-group events, made on first use
   cudaStream_t copy_stream = nullptr, upload_stream = nullptr;
   std::vector<cudaEvent_t> events;
+  // what the time-segmented path rebuilds its tables from
+  mrsim_acquisition acq{};
+  std::vector<double> tes;
+  std::vector<LineRec> h_lines;
+  std::vector<float> h_fmap;
+  float t2u[kMaxComp] = {0}, tiu[kMaxComp] = {0};
+  bool maps = false, any_eddy = false;
+  // the time-segmented tensor-core y-stages, when selected (mrsim_epi_operator_set_segmented)
+  TsPlan* ts = nullptr;
+  int ts_precision = 0;
   ~EpiOperator();
 };
 
@@ -65,6 +78,11 @@ void upload_series_images(EpiOperator* op, const float* const* host_images);
 void epi_operator_set_fieldmap(EpiOperator* op, const float* fmap);
 void epi_operator_forward(EpiOperator* op);
 void epi_operator_adjoint(EpiOperator* op);
+// plan units [u0, u1) (u1 < 0: all) of the y- and x-stages of either path
+void epi_operator_forward_units(EpiOperator* op, cudaStream_t st, int u0, int u1);
+void epi_operator_adjoint_units(EpiOperator* op, cudaStream_t st, int u0, int u1);
+void epi_operator_set_segmented(EpiOperator* op, int precision);
+int epi_operator_segmented_error(EpiOperator* op);
 // Forward + adjoint from host images to host k-space and gradients (any output may be NULL),
 // pipelined by groups of slices (or of volumes for one slice): a group's images upload, and its
 // results copy back, on two more streams while other groups compute.

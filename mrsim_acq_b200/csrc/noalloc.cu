@@ -172,10 +172,6 @@ void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquis
   if (ncomp > kMaxComp) fail("more than 8 compartments");
   const int ncoils = (int)std::max<int64_t>(acq.n_coils, 1);
   if (ncoils > kMaxCoils) fail("more than 64 coils");
-  if (ncomp > 1)
-    for (int c = 1; c < ncomp; ++c)
-      if (inp.compartments[c] != inp.compartments[0] + (size_t)c * snx * sny)
-        fail("mrsim_build_coil_kspaces_noalloc: compartment planes must be contiguous on the device");
   bool uniform = true;
   for (int c = 0; c < ncomp; ++c) uniform = uniform && !inp.t2[c].is_map;
   if (inp.t_inhom)
@@ -189,6 +185,10 @@ void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquis
   need_device_pointer(inp.fmap, "fmap", dev);
   if (inp.phase0) need_device_pointer(inp.phase0, "phase0", dev);
   need_device_pointer(out, "kspace", dev);
+  if (ncomp > 1)
+    for (int c = 1; c < ncomp; ++c)
+      if (inp.compartments[c] != inp.compartments[0] + (size_t)c * snx * sny)
+        fail("mrsim_build_coil_kspaces_noalloc: compartment planes must be contiguous on the device");
   const NaAddrs& A = addresses(dev);
 
   const bool eddy = acq.eddy_strength != 0.0 && inp.has_eddy_drive;

@@ -54,11 +54,11 @@ def _pair(s, acq, tes, kw, ctx, grads=3):
 
 
 def test_precision_at_scale_geometry_32_coils(gpu_ctx):
-    """128x128 on 256x256, 32 ring coils, 3 compartments, all 128 lines, TE 30 ms."""
+    """128x128 on 256x256, 32 ring coils, 3 compartments, all 128 lines (a 64 ms train), TE 40 ms."""
     s = cases.series_case(nx=128, ny=128, nz=2, o=2, nv=1, ncomp=3)
-    acq = Acquisition(n_coils=32, t_line=0.5, t_echo=30.0, ghost_offset=0.02)
+    acq = Acquisition(n_coils=32, t_line=0.5, t_echo=40.0, ghost_offset=0.02)
     kw = dict(t_inhom=s["t_inhom"], phase=PhaseModel.hbcd_like(), seed=42)
-    print("32 coils, 256 grid:", _pair(s, acq, [30.0], kw, gpu_ctx))
+    print("32 coils, 256 grid:", _pair(s, acq, [40.0], kw, gpu_ctx))
 
 
 def test_sixteen_coil_ring_on_the_series_grid(gpu_ctx):
