@@ -163,6 +163,82 @@ def max_over_ranks(v, world, device="cuda"):
     return float(t.item())
 
 
+STAGES = ["statics", "forward_ystage", "forward_xstage", "adjoint_xstage", "adjoint_ystage"]
+
+
+def time_stages(op, stream, ctx, steps, warmup):
+    """Device time of `steps` forward + adjoint passes (the five stages in order, CUDA events on the
+    context stream): (total ms, per-stage mean ms)."""
+    import torch
+
+    def step(evs=None):
+        for i in range(5):
+            if evs is not None:
+                evs[i].record(stream)
+            op.stage(i)
+        if evs is not None:
+            evs[5].record(stream)
+
+    for _ in range(warmup):
+        step()
+    ctx.synchronize()
+    t_begin = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(steps)]
+    t_begin.record(stream)
+    for k in range(steps):
+        step(evs[k])
+    t_end.record(stream)
+    t_end.synchronize()
+    ctx.synchronize()
+    stage_ms = np.array([[evs[k][i].elapsed_time(evs[k][i + 1]) for i in range(5)] for k in range(steps)])
+    return t_begin.elapsed_time(t_end), stage_ms.mean(axis=0)
+
+
+def segmented_comparison(args, inp, acq, ctx, stream, samples):
+    """The time-segmented tensor-core pair against the exact pair with the same outputs (k-space
+    and the complex-image adjoint, grads = 0), on the same workload: samples/s, the ratio, the
+    segmentation, and the forward contraction's tensor-pipe roofline."""
+    from mrsim_acq_b200.api import EpiOperator, PhaseModel
+    pk, pk_kind = peaks()
+    tensor_peak = pk.get("bf16_tflops_sustained", pk.get("bf16_tflops"))
+
+    def make():
+        return EpiOperator(inp["sim_dims"], inp["acq_dims"], inp["n_volumes"], inp["t2"], inp["fmap"], acq,
+                           images=inp["images"], echo_times_ms=WORKLOAD["echoes"], t_inhom=inp["t_inhom"],
+                           phase=PhaseModel.hbcd_like(), seed=42, grads=0, ctx=ctx)
+
+    out = {}
+    op = make()
+    tot, st = time_stages(op, stream, ctx, args.steps, args.warmup)
+    op.close()
+    exact_ms = tot / args.steps
+    out["exact_same_outputs"] = {"value": samples / (exact_ms * 1e-3), "ms_per_step": exact_ms,
+                                 "stage_ms": dict(zip(STAGES, [round(float(v), 4) for v in st]))}
+    for prec in ("f16", "bf16"):
+        op = make()
+        op.set_segmented(prec)
+        info = op.segmentation()
+        tot, st = time_stages(op, stream, ctx, args.steps, args.warmup)
+        status = op.segmented_status()
+        op.close()
+        ms = tot / args.steps
+        ach_f = info["flops_forward"] / (st[1] * 1e-3) / 1e12
+        ach_a = info["flops_adjoint"] / (st[4] * 1e-3) / 1e12
+        out[prec] = {"value": samples / (ms * 1e-3), "ms_per_step": ms, "ratio_to_exact": exact_ms / ms,
+                     "status": status, "L": info["L"], "max_bound": max(info["bound"]) if info["bound"] else None,
+                     "tensor_flop_per_pass": {"forward": info["flops_forward"], "adjoint": info["flops_adjoint"]},
+                     "stage_ms": dict(zip(STAGES, [round(float(v), 4) for v in st])),
+                     "roofline": {"bound": "tensor", "kernel": "ts_forward_kernel", "achieved": ach_f,
+                                  "peak": tensor_peak, "unit": "TFLOP/s", "frac": ach_f / tensor_peak,
+                                  "adjoint_achieved": ach_a, "adjoint_frac": ach_a / tensor_peak,
+                                  "peak_source": f"bf16_tflops_sustained ({pk_kind})",
+                                  "flop_count": "2 M N K per MMA, the three split products (hi*hi, lo*hi, hi*lo)"}}
+    out["note"] = ("the same k-space and complex-image adjoint from both paths; ratio_to_exact > 1 means the "
+                   "segmented pair is faster")
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from mrsim_acq_b200 import api
@@ -274,6 +350,9 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": 5 * args.steps,
         "clocks": clk,
     }
+    if not args.no_segmented:
+        res["segmented"] = segmented_comparison(args, inp, acq, ctx, stream, samples)
+        res["gpu_launches"] += 3 * 6 * args.steps  # three more operators, up to 6 launches a step
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res["cpu_baseline"] = cpu_baseline(acq, inp, sample_volumes=args.cpu_volumes, sample_slices=args.cpu_slices)
     return res, op, ctx
@@ -342,6 +421,7 @@ def main():
     ap.add_argument("--ref-slices", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--no-segmented", action="store_true", help="skip the time-segmented comparison")
     ap.add_argument("--volumes", type=int, default=0, help="override the volume count (smaller profiling case)")
     args = ap.parse_args()
     if args.volumes > 0:
