@@ -344,6 +344,23 @@ int mrsim_epi_operator_segmentation(const mrsim_epi_operator* op, int32_t* n_gro
                                     double* flops_adjoint);
 /* 0, or the code of a wait inside the segmented kernels that gave up (synchronises the stream). */
 int mrsim_epi_operator_segmented_status(mrsim_epi_operator* op, int32_t* code);
+/* As mrsim_epi_operator_apply_host, with the k-space in the compact layout
+ * [g][z][coil][echo][acquired row][kx]: only the acquired rows, k-space row first + step * i of
+ * mrsim_epi_operator_acquired_rows, no zero-filled rows (the host writes only what crosses the
+ * link).  New API, no reference counterpart: the reference-compatible series entries keep the
+ * zero-filled layout of `KspaceCapture` (kspace.rs:1767-1797).  MRSIM_ERR_INVALID when the
+ * acquired rows of the echoes are not one uniform stride. */
+int mrsim_epi_operator_apply_host_compact(mrsim_epi_operator* op, const float* const* images,
+                                          float* kspace_rows, float* comp_grad, float* fmap_grad,
+                                          float* r2_grad);
+/* The acquired k-space rows of every echo as first + step * i, i < count (count 0: irregular). */
+int mrsim_epi_operator_acquired_rows(const mrsim_epi_operator* op, int32_t* first, int32_t* step,
+                                     int32_t* count);
+/* Bytes a host-buffer call moves with the outputs of `outputs` (bit 0 k-space, 1 comp_grad,
+ * 2 fmap_grad, 3 r2_grad): the images up, the acquired k-space rows and the requested gradients
+ * down. */
+int mrsim_epi_operator_host_bytes_for(const mrsim_epi_operator* op, int32_t outputs,
+                                      int64_t* upload_bytes, int64_t* download_bytes);
 /* Bytes one mrsim_epi_operator_apply_host call moves between host and device with every input
  * and output given: the images up; the acquired k-space rows (the other rows are zero-filled on
  * the host when the acquired rows form a uniform stride, else every row) and the gradients down. */

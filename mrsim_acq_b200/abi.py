@@ -253,6 +253,9 @@ def _declare(lib):
         "mrsim_epi_operator_apply_host": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
         "mrsim_epi_operator_host_bytes": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "mrsim_epi_operator_set_segmented": (C.c_int, [P, C.c_int32]),
+        "mrsim_epi_operator_apply_host_compact": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
+        "mrsim_epi_operator_acquired_rows": (C.c_int, [P] + [C.POINTER(C.c_int32)] * 3),
+        "mrsim_epi_operator_host_bytes_for": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "mrsim_epi_operator_segmentation": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), c_f64p,
                                                       C.c_int32, c_f64p, c_f64p]),
         "mrsim_epi_operator_segmented_status": (C.c_int, [P, C.POINTER(C.c_int32)]),

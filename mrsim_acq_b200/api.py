@@ -662,6 +662,40 @@ class EpiOperator:
                                                   p(out.get("fmap_grad")), p(out.get("r2_grad"))))
         return out
 
+    def acquired_rows(self) -> tuple:
+        """(first, step, count): the acquired k-space rows of every echo (count 0: irregular)."""
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().mrsim_epi_operator_acquired_rows(self.handle, C.byref(a), C.byref(b), C.byref(c)))
+        return int(a.value), int(b.value), int(c.value)
+
+    def apply_host_compact(self, images: Optional[Sequence[np.ndarray]], out: Optional[dict] = None) -> dict:
+        """`apply_host` with the k-space as [g][z][coil][echo][acquired row][kx] (the acquired rows
+        only); gradients set to None in `out` are not computed into the host."""
+        shp = self.shapes()
+        nv, nz, q, ne, ny, nx = shp["kspace"]
+        _, _, rows = self.acquired_rows()
+        if out is None:
+            out = {"kspace": np.zeros((nv, nz, q, ne, rows, nx), np.complex64),
+                   "comp_grad": np.zeros(shp["comp_grad"], np.complex64),
+                   "fmap_grad": np.zeros(shp["fmap_grad"], np.float32) if self.grads & 1 else None,
+                   "r2_grad": np.zeros(shp["r2_grad"], np.float32) if self.grads & 2 else None}
+        keep = _Keep()
+        imgs = keep.ptrs([np.ravel(a) for a in images]) if images is not None else None
+
+        def p(a):
+            return None if a is None else C.cast(a.ctypes.data, abi.c_f32p)
+
+        check(lib().mrsim_epi_operator_apply_host_compact(self.handle, imgs, p(out["kspace"]), p(out.get("comp_grad")),
+                                                          p(out.get("fmap_grad")), p(out.get("r2_grad"))))
+        return out
+
+    def host_bytes_for(self, kspace=True, comp_grad=True, fmap_grad=True, r2_grad=True) -> tuple:
+        """(upload, download) bytes of a host-buffer call with the given outputs."""
+        up, down = C.c_int64(), C.c_int64()
+        m = (1 if kspace else 0) | (2 if comp_grad else 0) | (4 if fmap_grad else 0) | (8 if r2_grad else 0)
+        check(lib().mrsim_epi_operator_host_bytes_for(self.handle, m, C.byref(up), C.byref(down)))
+        return int(up.value), int(down.value)
+
     def host_bytes(self) -> tuple:
         """(upload, download) bytes one `apply_host` call moves over the host link with every
         output requested (acquired k-space rows only when they form a uniform stride)."""

@@ -577,6 +577,45 @@ int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* im
   });
 }
 
+int mrsim_epi_operator_apply_host_compact(mrsim_epi_operator* op, const float* const* images, float* kspace_rows,
+                                          float* comp_grad, float* fmap_grad, float* r2_grad) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    mrsim::epi_operator_apply_host(op->impl, images, kspace_rows, comp_grad, fmap_grad, r2_grad, true);
+  });
+}
+
+int mrsim_epi_operator_acquired_rows(const mrsim_epi_operator* op, int32_t* first, int32_t* step, int32_t* count) {
+  return guarded([&] {
+    need(op, "operator");
+    need(first, "first");
+    need(step, "step");
+    need(count, "count");
+    *first = op->impl->krow0;
+    *step = op->impl->krow_step;
+    *count = op->impl->krow_n;
+  });
+}
+
+int mrsim_epi_operator_host_bytes_for(const mrsim_epi_operator* op, int32_t outputs, int64_t* upload_bytes,
+                                      int64_t* download_bytes) {
+  return guarded([&] {
+    need(op, "operator");
+    need(upload_bytes, "upload_bytes");
+    need(download_bytes, "download_bytes");
+    const auto* o = op->impl;
+    const int64_t plane = (int64_t)o->snx * o->sny, units = (int64_t)o->nv * o->nz;
+    const int64_t rows = o->krow_n > 0 ? (int64_t)o->krow_n * o->n_echoes : (int64_t)o->n_echoes * o->ny;
+    *upload_bytes = units * o->ncomp * plane * 4;
+    int64_t d = 0;
+    if (outputs & 1) d += units * o->ncoils * rows * o->nx * 8;
+    if (outputs & 2) d += units * o->ncomp * plane * 8;
+    if ((outputs & 4) && o->d_fmap_grad) d += units * plane * 4;
+    if ((outputs & 8) && o->d_r2_grad) d += units * o->ncomp * plane * 4;
+    *download_bytes = d;
+  });
+}
+
 
 // ---- stack-of-spirals path ------------------------------------------------------------------------
 int mrsim_spiral_tau_c(int64_t nx, int64_t interleaves, double readout_ms, double dwell_ms, double radial_oversampling,

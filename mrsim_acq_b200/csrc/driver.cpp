@@ -517,7 +517,9 @@ void epi_operator_adjoint(EpiOperator* op) { epi_operator_adjoint_units(op, op->
 int epi_operator_segmented_error(EpiOperator* op) { return op->ts ? ts_error(*op->ts, op->ctx->stream) : 0; }
 
 void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* kspace, float* comp_grad,
-                             float* fmap_grad, float* r2_grad) {
+                             float* fmap_grad, float* r2_grad, bool compact) {
+  if (compact && kspace && o->krow_n <= 0)
+    fail("the compact k-space layout needs the acquired rows at a uniform stride in every echo");
   cudaStream_t st = o->ctx->stream;
   const int nv = o->nv, nz = o->nz;
   // Groups are boxes of volumes [g0, g1) x slices [z0, z1), each a range of the slice-major plan
@@ -598,7 +600,12 @@ void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* 
       cudaMemcpy3DParms m;
       std::memset(&m, 0, sizeof m);
       m.srcPtr = make_cudaPitchedPtr((char*)o->d_kspace + off, o->krow_step * row_bytes, row_bytes, ny / o->krow_step);
-      m.dstPtr = make_cudaPitchedPtr((char*)kspace + off, o->krow_step * row_bytes, row_bytes, ny / o->krow_step);
+      if (compact) {  // [g][z][coil][echo][acquired row][kx], no rows in between
+        const size_t coff = ((size_t)g * nz + B.z0) * blocks_per_unit * o->krow_n * row_bytes;
+        m.dstPtr = make_cudaPitchedPtr((char*)kspace + coff, row_bytes, row_bytes, o->krow_n);
+      } else {
+        m.dstPtr = make_cudaPitchedPtr((char*)kspace + off, o->krow_step * row_bytes, row_bytes, ny / o->krow_step);
+      }
       m.extent = make_cudaExtent(row_bytes, o->krow_n, (size_t)(B.z1 - B.z0) * blocks_per_unit);
       m.kind = cudaMemcpyDeviceToHost;
       MRSIM_CUDA(cudaMemcpy3DAsync(&m, cs));
@@ -610,7 +617,7 @@ void epi_operator_apply_host(EpiOperator* o, const float* const* images, float* 
       for (auto& th : t) th.join();
     }
   } zeroers;
-  if (sparse_k) {
+  if (sparse_k && !compact) {
     const size_t nblocks = (size_t)nv * nz * blocks_per_unit;
     std::vector<char> acquired(ny, 0);
     for (int i = 0; i < o->krow_n; ++i) acquired[o->krow0 + i * o->krow_step] = 1;

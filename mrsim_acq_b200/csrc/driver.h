@@ -86,8 +86,10 @@ int epi_operator_segmented_error(EpiOperator* op);
 // Forward + adjoint from host images to host k-space and gradients (any output may be NULL),
 // pipelined by groups of slices (or of volumes for one slice): a group's images upload, and its
 // results copy back, on two more streams while other groups compute.
+// compact: k-space as [g][z][coil][echo][acquired row][kx] (the acquired rows only), else the
+// reference's zero-filled [g][z][coil][echo][ny][nx]
 void epi_operator_apply_host(EpiOperator* op, const float* const* images, float* kspace, float* comp_grad,
-                             float* fmap_grad, float* r2_grad);
+                             float* fmap_grad, float* r2_grad, bool compact = false);
 
 // noalloc.cu: the forward of one slice with every intermediate in static device arrays.
 void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquisition& acq, float2* out,

@@ -52,6 +52,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort_flag) return false;
+    __nanosleep(32);  // a waiting warp leaves its scheduler's issue slots to the working warps
     if (globaltimer() - t0 > kWaitLimitNs) {
       *abort_flag = 1;
       if (err) atomicCAS(err, 0, code);

@@ -58,8 +58,10 @@ using namespace sm100;
 namespace {
 
 constexpr float kTwoPiF = 6.28318530717958647692f;
-constexpr int kStages = 2;
-constexpr int kStageA = 32768;  // A hi + lo: 128 rows x 128 bytes each
+constexpr int kStages = 2;       // operand stages of A (and of everything in the adjoint)
+constexpr int kMaxBStages = 3;   // stages of the forward's constant B tiles, when they fit
+constexpr int kStageA = 32768;   // A hi + lo: 128 rows x 128 bytes each
+constexpr int kNodeFloats = 6;   // per node in shared memory: t_hi, t_lo, alpha[4]
 
 // error codes written to the plan's device flag
 enum : int { TS_ERR_FULL_A = 1, TS_ERR_FULL_B = 2, TS_ERR_EMPTY = 3, TS_ERR_ACC_FULL = 4, TS_ERR_ACC_EMPTY = 5,
@@ -104,8 +106,10 @@ __device__ __forceinline__ void split2(float re, float im, uint32_t& hi, uint32_
   lo = Split<DT>::pack(re - h.x, im - h.y);
 }
 
+// No memory clobber: the compiler may keep computing the next values across these stores; the
+// async-proxy fence that publishes the tile (a volatile asm with a memory clobber) stays after them.
 __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d));
 }
 
 struct TsSmem {
@@ -120,24 +124,31 @@ __global__ void __launch_bounds__(448, 1) ts_forward_kernel(const __grid_constan
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t b_stage = 2u * (uint32_t)P.np_max * 128u;
+  const int SB = P.b_stages;  // B stages (A has kStages): the constant tiles prefetched further ahead
   unsigned char* sA = smem;
   unsigned char* sB = sA + kStages * kStageA;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + kStages * b_stage);
-  uint64_t* full_a = bars;
-  uint64_t* full_b = bars + kStages;
-  uint64_t* empty = bars + 2 * kStages;
-  uint64_t* acc_full = bars + 3 * kStages;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + SB * b_stage);
+  uint64_t* full_a = bars;                   // [kStages]
+  uint64_t* empty_a = full_a + kStages;      // [kStages]
+  uint64_t* full_b = empty_a + kStages;      // [kMaxBStages]
+  uint64_t* empty_b = full_b + kMaxBStages;  // [kMaxBStages]
+  uint64_t* acc_full = empty_b + kMaxBStages;
   uint64_t* acc_empty = acc_full + 2;
   uint64_t* drain = acc_empty + 2;
   uint32_t* tmem_base_s = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_base_s + 1);
+  // every group's node times and compartment weights: [group][l][t_hi, t_lo, alpha 0..3]
+  float* nodes = reinterpret_cast<float*>(tmem_base_s + 4);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full_a[s], 8);
+      mbar_init(&empty_a[s], 1);
+    }
+    for (int s = 0; s < SB; ++s) {
       mbar_init(&full_b[s], 1);
-      mbar_init(&empty[s], 1);
+      mbar_init(&empty_b[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
@@ -146,6 +157,14 @@ __global__ void __launch_bounds__(448, 1) ts_forward_kernel(const __grid_constan
     mbar_init(drain, 1);
     *abort_s = 0;
     fence_mbar_init();
+  }
+  for (int e = threadIdx.x; e < P.n_groups * kTsMaxL; e += blockDim.x) {
+    const int g = e / kTsMaxL, l = e % kTsMaxL;
+    const TsGroupDev& G = P.groups[g];
+    float* d = nodes + (size_t)e * kNodeFloats;
+    d[0] = G.t_hi[l];
+    d[1] = G.t_lo[l];
+    for (int cc = 0; cc < 4; ++cc) d[2 + cc] = G.alpha[l][cc];
   }
   if (warp == 13) {
     tmem_alloc(tmem_base_s, 512);
@@ -203,19 +222,28 @@ __global__ void __launch_bounds__(448, 1) ts_forward_kernel(const __grid_constan
             load_rows(y8 + 1 < ny8 ? y8 + 1 : 0, na, nf, nm);  // the next chunk in sequence
           }
           const int s = c % kStages;
-          if (!__all_sync(0xffffffffu, mbar_wait(&empty[s], ((c / kStages) & 1) ^ 1, abort_s, P.err, TS_ERR_EMPTY)))
+          if (!__all_sync(0xffffffffu, mbar_wait(&empty_a[s], ((c / kStages) & 1) ^ 1, abort_s, P.err, TS_ERR_EMPTY)))
             goto done;
           {
             // K within the block: (l % 4) 16 + yy 2 + re/im, so node l's rows 4 kh .. 4 kh + 3 are
             // 16-byte chunk 2 (l % 4) + kh
             const uint32_t hi0 = a0 + s * kStageA, lo0 = hi0 + kStageA / 2;
+            // the block's four nodes, read together
+            float th4[4], tl4[4], al4[4][NC];
 #pragma unroll
             for (int dl = 0; dl < 4; ++dl) {
-              const int l = 4 * lq + dl;
-              const float th = G.t_hi[l], tl = G.t_lo[l];
+              const float* nd = nodes + ((size_t)g * kTsMaxL + 4 * lq + dl) * kNodeFloats;
+              th4[dl] = nd[0];
+              tl4[dl] = nd[1];
+#pragma unroll
+              for (int cc = 0; cc < NC; ++cc) al4[dl][cc] = nd[2 + cc];
+            }
+#pragma unroll
+            for (int dl = 0; dl < 4; ++dl) {
+              const float th = th4[dl], tl = tl4[dl];
               float al[NC];
 #pragma unroll
-              for (int cc = 0; cc < NC; ++cc) al[cc] = G.alpha[l][cc];
+              for (int cc = 0; cc < NC; ++cc) al[cc] = al4[dl][cc];
               uint32_t hv[4], lv[4];
 #pragma unroll
               for (int k = 0; k < 4; ++k) {
@@ -281,8 +309,8 @@ __global__ void __launch_bounds__(448, 1) ts_forward_kernel(const __grid_constan
         for (int g = 0; g < P.n_groups; ++g) {
           const TsGroupDev& G = P.groups[g];
           for (int kb = 0; kb < G.kb_f; ++kb, ++c) {
-            const int s = c % kStages;
-            if (!mbar_wait(&empty[s], ((c / kStages) & 1) ^ 1, abort_s, P.err, TS_ERR_EMPTY)) goto tma_done;
+            const int s = c % SB;
+            if (!mbar_wait(&empty_b[s], ((c / SB) & 1) ^ 1, abort_s, P.err, TS_ERR_EMPTY)) goto tma_done;
             mbar_arrive_expect_tx(&full_b[s], 2u * (uint32_t)G.np_f * 128u);
             unsigned char* bh = sB + s * b_stage;
             tma_load_2d(bh, &P.bmap[g], kb * 64, 0, &full_b[s]);
@@ -292,8 +320,8 @@ __global__ void __launch_bounds__(448, 1) ts_forward_kernel(const __grid_constan
       }
     tma_done:
       // loads still in flight (after an abort) land before the CTA leaves
-      for (uint32_t k = c > kStages ? c - kStages : 0; k < c; ++k)
-        mbar_wait(&full_b[k % kStages], (k / kStages) & 1, abort_s, nullptr, 0);
+      for (uint32_t k = c > (uint32_t)SB ? c - SB : 0; k < c; ++k)
+        mbar_wait(&full_b[k % SB], (k / SB) & 1, abort_s, nullptr, 0);
     }
     __syncwarp();
   } else {
@@ -310,20 +338,20 @@ __global__ void __launch_bounds__(448, 1) ts_forward_kernel(const __grid_constan
           const uint32_t d = tmem + (uint32_t)(b * 256);
           const uint32_t idesc = idesc_f16(128, G.np_f, DT);
           for (int kb = 0; kb < G.kb_f; ++kb, ++c) {
-            const int s = c % kStages;
-            const uint32_t par = (c / kStages) & 1;
-            if (!mbar_wait(&full_a[s], par, abort_s, P.err, TS_ERR_FULL_A)) goto mma_done;
-            if (!mbar_wait(&full_b[s], par, abort_s, P.err, TS_ERR_FULL_B)) goto mma_done;
+            const int s = c % kStages, sb = c % SB;
+            if (!mbar_wait(&full_a[s], (c / kStages) & 1, abort_s, P.err, TS_ERR_FULL_A)) goto mma_done;
+            if (!mbar_wait(&full_b[sb], (c / SB) & 1, abort_s, P.err, TS_ERR_FULL_B)) goto mma_done;
             tc_fence_after();
             const uint64_t ah = sw128_desc(a0 + s * kStageA), al = sw128_desc(a0 + s * kStageA + kStageA / 2);
-            const uint64_t bh = sw128_desc(b0 + s * b_stage), bl = sw128_desc(b0 + s * b_stage + P.np_max * 128);
+            const uint64_t bh = sw128_desc(b0 + sb * b_stage), bl = sw128_desc(b0 + sb * b_stage + P.np_max * 128);
 #pragma unroll
             for (int k = 0; k < 4; ++k) umma_f16(d, ah + 2 * k, bh + 2 * k, idesc, (kb | k) != 0);
 #pragma unroll
             for (int k = 0; k < 4; ++k) umma_f16(d, al + 2 * k, bh + 2 * k, idesc, 1);
 #pragma unroll
             for (int k = 0; k < 4; ++k) umma_f16(d, ah + 2 * k, bl + 2 * k, idesc, 1);
-            umma_commit(&empty[s]);
+            umma_commit(&empty_a[s]);
+            umma_commit(&empty_b[sb]);
           }
           umma_commit(&acc_full[b]);
         }
@@ -437,8 +465,18 @@ __global__ void __launch_bounds__(320, 1) ts_adjoint_kernel(const __grid_constan
   uint64_t* drain = acc_empty + 2;
   uint32_t* tmem_base_s = reinterpret_cast<uint32_t*>(drain + 1);
   volatile int* abort_s = reinterpret_cast<volatile int*>(tmem_base_s + 1);
+  // every group's node times and adjoint weights: [group][l][t_hi, t_lo, alpha_adj 0..3]
+  float* nodes = reinterpret_cast<float*>(tmem_base_s + 4);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e = threadIdx.x; e < P.n_groups * kTsMaxL; e += blockDim.x) {
+    const int g = e / kTsMaxL, l = e % kTsMaxL;
+    const TsGroupDev& G = P.groups[g];
+    float* d = nodes + (size_t)e * kNodeFloats;
+    d[0] = G.t_hi[l];
+    d[1] = G.t_lo[l];
+    for (int cc = 0; cc < 4; ++cc) d[2 + cc] = G.alpha_adj[l][cc];
+  }
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
@@ -511,14 +549,15 @@ __global__ void __launch_bounds__(320, 1) ts_adjoint_kernel(const __grid_constan
               for (int p = 0; p < 4; ++p) {
                 const int l = l0 + p;
                 if (l >= G.L) break;
-                const float t = phase_turns(a[k], f[k], G.t_hi[l], G.t_lo[l]);
+                const float* nd = nodes + ((size_t)g * kTsMaxL + l) * kNodeFloats;
+                const float t = phase_turns(a[k], f[k], nd[0], nd[1]);
                 float sn, cs;
                 __sincosf(kTwoPiF * t, &sn, &cs);
                 const float hr = v[2 * p], hi = v[2 * p + 1];
                 const float zr = fmaf(cs, hr, sn * hi), zi = fmaf(cs, hi, -sn * hr);
 #pragma unroll
                 for (int cc = 0; cc < NC; ++cc) {
-                  const float w = G.alpha_adj[l][cc];
+                  const float w = nd[2 + cc];
                   acc[k][cc].x = fmaf(w, zr, acc[k][cc].x);
                   acc[k][cc].y = fmaf(w, zi, acc[k][cc].y);
                 }
@@ -1022,9 +1061,12 @@ template <class K>
 void opt_in(K kernel, size_t bytes) {
   MRSIM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
-size_t ts_smem(int np_max) {
-  return 1024 + (size_t)kStages * kStageA + (size_t)kStages * 2 * np_max * 128 + 16 * 8 + 16;
+// bytes of dynamic shared memory: alignment slack, A and B stages, barriers, the node table
+size_t ts_smem(int np_max, int b_stages, int n_groups) {
+  return 1024 + (size_t)kStages * kStageA + (size_t)b_stages * 2 * np_max * 128 + 16 * 8 + 16 +
+         (size_t)n_groups * kTsMaxL * kNodeFloats * 4;
 }
+constexpr size_t kSmemLimit = 232448;  // 227 KB per CTA
 }  // namespace
 
 void ts_forward_ystage(const TsPlan& T, const EpiPlan& ep, cudaStream_t st, int u0, int u1) {
@@ -1047,7 +1089,8 @@ void ts_forward_ystage(const TsPlan& T, const EpiPlan& ep, cudaStream_t st, int 
   P.snx_tiles = T.snx_tiles;
   P.np_max = T.np_max_f;
   P.u0 = u0;
-  const size_t sm = ts_smem(T.np_max_f);
+  P.b_stages = ts_smem(T.np_max_f, 3, T.n_groups) <= kSmemLimit ? 3 : 2;
+  const size_t sm = ts_smem(T.np_max_f, P.b_stages, T.n_groups);
   const unsigned grid = (unsigned)std::min(P.n_items, T.n_sms);
   const int nc = ep.nc;
 #define MRSIM_TSF(DT, NC)                           \
@@ -1109,7 +1152,7 @@ void ts_adjoint_ystage(const TsPlan& T, const EpiPlan& ep, cudaStream_t st, int 
   P.nyc = T.nyc;
   P.yc = T.yc;
   P.u0 = u0;
-  const size_t sm = ts_smem(T.np_max_a);
+  const size_t sm = ts_smem(T.np_max_a, kStages, T.n_groups);
   const unsigned grid = (unsigned)std::min(P.n_items, T.n_sms);
   const int nc = ep.nc;
 #define MRSIM_TSA(DT, NC)                           \

@@ -47,7 +47,7 @@ struct TsFwdParams {
   float2* cls_out;           // class-row scratch when the x-stage runs per coil, else NULL (u.g)
   long long cls_unit_stride;
   int* err;
-  int n_items, n_groups, na, snx_tiles, np_max, u0;
+  int n_items, n_groups, na, snx_tiles, np_max, u0, b_stages;
 };
 
 struct TsAdjParams {

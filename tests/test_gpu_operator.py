@@ -230,3 +230,24 @@ def test_rows_of_32e_points_match_the_oracle(nx, coils, gpu_ctx):
     for key in ("comp_grad", "fmap_grad", "r2_grad"):
         e = rel_l2(out[key], adj[key])
         assert e <= TOL, f"{key}: rel-L2 {e:.2e}"
+
+
+def test_compact_host_layout_is_the_acquired_rows(gpu_ctx):
+    """The compact host call returns exactly the acquired rows of the zero-filled layout, and the
+    byte query counts what each call moves."""
+    s, acq, tes, kw = _setup(eddy=False, nv=3, nz=2, coils=4)
+    op = api.EpiOperator(s["sim_dims"], s["acq_dims"], s["n_volumes"], s["t2"], s["fmap"], acq, images=s["images"],
+                         echo_times_ms=tes, grads=3, ctx=gpu_ctx, **kw)
+    full = op.apply_host(s["images"])
+    first, step, count = op.acquired_rows()
+    assert count > 0
+    kshape = full["kspace"].shape[:4] + (count, full["kspace"].shape[5])
+    comp = op.apply_host_compact(s["images"], {"kspace": np.zeros(kshape, np.complex64), "comp_grad": None,
+                                               "fmap_grad": None, "r2_grad": None})
+    rows = first + step * np.arange(count)
+    assert np.array_equal(comp["kspace"], full["kspace"][:, :, :, :, rows, :])
+    up, down_all = op.host_bytes_for()
+    _, down_k = op.host_bytes_for(comp_grad=False, fmap_grad=False, r2_grad=False)
+    assert down_k == comp["kspace"].nbytes and up == sum(a.nbytes for a in s["images"])
+    assert down_all == down_k + full["comp_grad"].nbytes + full["fmap_grad"].nbytes + full["r2_grad"].nbytes
+    op.close()
