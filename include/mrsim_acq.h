@@ -367,6 +367,60 @@ int mrsim_epi_operator_host_bytes_for(const mrsim_epi_operator* op, int32_t outp
 int mrsim_epi_operator_host_bytes(const mrsim_epi_operator* op, int64_t* upload_bytes,
                                   int64_t* download_bytes);
 
+/* ---- image motion before the forward (motion.rs) -------------------------------------------- */
+/* A pose is 6 doubles: rotation (degrees about x, y, z; R = Rz Ry Rx) then translation (mm),
+ * `Pose` (motion.rs:43-47).  v2w is the grid's voxel-to-world affine, row-major 4x4.  The
+ * resampling backward-maps every output voxel in FP64 in the reference's operation order and
+ * samples the source trilinearly (edge voxels extend half a voxel, zero beyond): the results are
+ * the reference's bit for bit. */
+/* `resample_by_pose` motion.rs:430-460: one volume (x + nx*(y + ny*z)) into `out`. */
+int mrsim_resample_by_pose(mrsim_context* ctx, const float* src, const int64_t* dims, const double* v2w,
+                           const double* pose, float* out);
+/* `apply_motion` motion.rs:466-482: images[c][vox*n_volumes + g] moved in place by poses[g]
+ * (n_volumes x 6 doubles). */
+int mrsim_apply_motion(mrsim_context* ctx, float* const* images, int64_t ncomp, const int64_t* dims,
+                       int64_t n_volumes, const double* v2w, const double* poses);
+
+enum { MRSIM_DROPOUT_UNIFORM = 0, MRSIM_DROPOUT_SCALED = 1, MRSIM_DROPOUT_SCALED_TO = 2 };
+/* `DropoutLaw` (motion.rs:625-662): Uniform 1 - severity; Scaled 1 - severity (drive/drive_max),
+ * drive < floor exempt; ScaledTo the same with the given max. */
+typedef struct mrsim_dropout_law {
+  int32_t kind;
+  const double* drive;
+  int64_t n_drive;
+  double floor;
+  double max;
+} mrsim_dropout_law;
+/* `MotionEvent` (motion.rs:608-615). */
+typedef struct mrsim_motion_event {
+  int64_t volume;
+  int64_t shot;
+  float severity;
+  double jump_mm[3];
+  double jump_deg[3];
+} mrsim_motion_event;
+/* `DroppedShot` (motion.rs:618-624): slices in full-FOV indices (at most 64). */
+typedef struct mrsim_dropped_shot {
+  int64_t volume;
+  int64_t shot;
+  float attenuation;
+  int64_t n_slices;
+  int64_t slices[64];
+} mrsim_dropped_shot;
+/* `apply_multiband_motion_slab` motion.rs:686-772 (slice_z NULL and nz_full 0: the whole volume,
+ * `apply_multiband_motion` motion.rs:666-680): within-volume shot motion and dropout of
+ * images[c][vox*n_volumes + g] in place; the dropped shots go to `dropped` (capacity entries),
+ * their count to *n_dropped. */
+int mrsim_apply_multiband_motion(mrsim_context* ctx, float* const* images, int64_t ncomp, const int64_t* dims,
+                                 int64_t n_volumes, const double* v2w, int64_t mb, int32_t interleaved,
+                                 const mrsim_dropout_law* law, const mrsim_motion_event* events,
+                                 int64_t n_events, const int64_t* slice_z, int64_t nz_full,
+                                 mrsim_dropped_shot* dropped, int64_t capacity, int64_t* n_dropped);
+/* No reference counterpart: `apply_motion` on an EPI operator's device images (its slab of
+ * slices, grid v2w of the sim grid, poses n_volumes x 6), in place; returns when done.  A moved
+ * series reaches the forward without crossing the host link. */
+int mrsim_epi_operator_apply_motion(mrsim_epi_operator* op, const double* v2w, const double* poses);
+
 /* ---- the 3D echo trains (kspace3d.rs, readout.rs:75-322) ----------------------------------- */
 enum { MRSIM_KZ_CENTRIC = 0, MRSIM_KZ_LINEAR = 1 };                            /* readout.rs:75 */
 

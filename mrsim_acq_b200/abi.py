@@ -58,6 +58,21 @@ class PhaseModel_(C.Structure):
     ]
 
 
+class DropoutLaw_(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("drive", c_f64p), ("n_drive", C.c_int64), ("floor", C.c_double),
+                ("max", C.c_double)]
+
+
+class MotionEvent_(C.Structure):
+    _fields_ = [("volume", C.c_int64), ("shot", C.c_int64), ("severity", C.c_float), ("jump_mm", C.c_double * 3),
+                ("jump_deg", C.c_double * 3)]
+
+
+class DroppedShot_(C.Structure):
+    _fields_ = [("volume", C.c_int64), ("shot", C.c_int64), ("attenuation", C.c_float), ("n_slices", C.c_int64),
+                ("slices", C.c_int64 * 64)]
+
+
 class AcquisitionInput_(C.Structure):
     """`mrsim_acquisition_input` — `AcquisitionInput` (kspace.rs:1720-1740)."""
 
@@ -253,6 +268,14 @@ def _declare(lib):
         "mrsim_epi_operator_apply_host": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
         "mrsim_epi_operator_host_bytes": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "mrsim_epi_operator_set_segmented": (C.c_int, [P, C.c_int32]),
+        "mrsim_resample_by_pose": (C.c_int, [P, c_f32p, C.POINTER(C.c_int64), c_f64p, c_f64p, c_f32p]),
+        "mrsim_apply_motion": (C.c_int, [P, C.POINTER(c_f32p), C.c_int64, C.POINTER(C.c_int64), C.c_int64, c_f64p,
+                                         c_f64p]),
+        "mrsim_apply_multiband_motion": (C.c_int, [P, C.POINTER(c_f32p), C.c_int64, C.POINTER(C.c_int64), C.c_int64,
+                                                   c_f64p, C.c_int64, C.c_int32, C.POINTER(DropoutLaw_),
+                                                   C.POINTER(MotionEvent_), C.c_int64, C.POINTER(C.c_int64), C.c_int64,
+                                                   C.POINTER(DroppedShot_), C.c_int64, C.POINTER(C.c_int64)]),
+        "mrsim_epi_operator_apply_motion": (C.c_int, [P, c_f64p, c_f64p]),
         "mrsim_epi_operator_apply_host_compact": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
         "mrsim_epi_operator_acquired_rows": (C.c_int, [P] + [C.POINTER(C.c_int32)] * 3),
         "mrsim_epi_operator_host_bytes_for": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),

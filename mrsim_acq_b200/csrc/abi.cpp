@@ -8,6 +8,7 @@
 #include <string>
 
 #include "driver.h"
+#include "motion.h"
 #include "ts_epi.h"
 #include "host_tables.h"
 #include "mrsim_internal.h"
@@ -616,6 +617,115 @@ int mrsim_epi_operator_host_bytes_for(const mrsim_epi_operator* op, int32_t outp
   });
 }
 
+
+// ---- image motion -----------------------------------------------------------------------------------
+namespace {
+// the reference layout of n_volumes volumes: element (x, y, z) of volume g at (x + nx (y + ny z)) nv + g
+struct HostSeries {
+  long long sx, sy, sz, sg, sc;
+};
+HostSeries host_strides(const int64_t* dims, int64_t nv) {
+  const long long nvox = dims[0] * dims[1] * dims[2];
+  return {nv, dims[0] * nv, dims[0] * dims[1] * nv, 1, nvox * nv};
+}
+void check_dims(const int64_t* dims, int64_t nv) {
+  need(dims, "dims");
+  if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0 || nv <= 0) mrsim::fail("empty volume or no volumes");
+  if (dims[0] * dims[1] * dims[2] >= (1LL << 31)) mrsim::fail("a volume of 2^31 voxels or more");
+}
+}  // namespace
+
+int mrsim_resample_by_pose(mrsim_context* ctx, const float* src, const int64_t* dims, const double* v2w,
+                           const double* pose, float* out) {
+  return on_ctx(ctx, [&] {
+    need(src, "src");
+    need(v2w, "v2w");
+    need(pose, "pose");
+    need(out, "out");
+    check_dims(dims, 1);
+    cudaStream_t st = ctx->stream;
+    const size_t n = (size_t)(dims[0] * dims[1] * dims[2]);
+    mrsim::DevArena A;
+    float* in = (float*)A.upload(src, n * 4, st);
+    float* o = (float*)A.alloc(n * 4);
+    mrsim::resample_poses_device(in, o, dims, 1, 1, 1, dims[0], dims[0] * dims[1], 0, 0, v2w, pose, st, A);
+    MRSIM_CUDA(cudaMemcpyAsync(out, o, n * 4, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int mrsim_apply_motion(mrsim_context* ctx, float* const* images, int64_t ncomp, const int64_t* dims, int64_t n_volumes,
+                       const double* v2w, const double* poses) {
+  return on_ctx(ctx, [&] {
+    need(images, "images");
+    need(v2w, "v2w");
+    need(poses, "poses");
+    check_dims(dims, n_volumes);
+    if (ncomp <= 0) return;
+    cudaStream_t st = ctx->stream;
+    const HostSeries H = host_strides(dims, n_volumes);
+    const size_t per = (size_t)H.sc;
+    mrsim::DevArena A;
+    float* in = (float*)A.alloc(per * ncomp * 4);
+    float* o = (float*)A.alloc(per * ncomp * 4);
+    for (int64_t c = 0; c < ncomp; ++c)
+      MRSIM_CUDA(cudaMemcpyAsync(in + per * c, images[c], per * 4, cudaMemcpyHostToDevice, st));
+    mrsim::resample_poses_device(in, o, dims, (int)n_volumes, (int)ncomp, H.sx, H.sy, H.sz, H.sg, H.sc, v2w, poses,
+                                 st, A);
+    for (int64_t c = 0; c < ncomp; ++c)
+      MRSIM_CUDA(cudaMemcpyAsync(images[c], o + per * c, per * 4, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int mrsim_apply_multiband_motion(mrsim_context* ctx, float* const* images, int64_t ncomp, const int64_t* dims,
+                                 int64_t n_volumes, const double* v2w, int64_t mb, int32_t interleaved,
+                                 const mrsim_dropout_law* law, const mrsim_motion_event* events, int64_t n_events,
+                                 const int64_t* slice_z, int64_t nz_full, mrsim_dropped_shot* dropped,
+                                 int64_t capacity, int64_t* n_dropped) {
+  return on_ctx(ctx, [&] {
+    need(images, "images");
+    need(v2w, "v2w");
+    need(law, "law");
+    need(n_dropped, "n_dropped");
+    check_dims(dims, n_volumes);
+    if (n_events > 0) need(events, "events");
+    cudaStream_t st = ctx->stream;
+    const HostSeries H = host_strides(dims, n_volumes);
+    const size_t per = (size_t)H.sc;
+    mrsim::DevArena A;
+    float* in = (float*)A.alloc(per * std::max<int64_t>(ncomp, 1) * 4);
+    float* o = (float*)A.alloc(per * std::max<int64_t>(ncomp, 1) * 4);
+    for (int64_t c = 0; c < ncomp; ++c)
+      MRSIM_CUDA(cudaMemcpyAsync(in + per * c, images[c], per * 4, cudaMemcpyHostToDevice, st));
+    *n_dropped = mrsim::multiband_device(in, o, dims, (int)n_volumes, (int)ncomp, H.sx, H.sy, H.sz, H.sg, H.sc, v2w,
+                                         mb, interleaved != 0, *law, events, n_events, slice_z, nz_full, dropped,
+                                         capacity, st, A);
+    for (int64_t c = 0; c < ncomp; ++c)
+      MRSIM_CUDA(cudaMemcpyAsync(images[c], o + per * c, per * 4, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int mrsim_epi_operator_apply_motion(mrsim_epi_operator* op, const double* v2w, const double* poses) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    need(v2w, "v2w");
+    need(poses, "poses");
+    auto* o = op->impl;
+    cudaStream_t st = o->ctx->stream;
+    const long long plane = (long long)o->snx * o->sny;
+    const size_t n = (size_t)o->nv * o->nz * o->ncomp * plane;
+    const int64_t dims[3] = {o->snx, o->sny, o->nz};
+    // the pre-motion images, then the moved ones back into the operator's buffer
+    float* scratch = (float*)mrsim::workspace(o->ctx, 21, n * 4);
+    MRSIM_CUDA(cudaMemcpyAsync(scratch, o->d_images, n * 4, cudaMemcpyDeviceToDevice, st));
+    mrsim::DevArena A;
+    mrsim::resample_poses_device(scratch, o->d_images, dims, o->nv, o->ncomp, 1, o->snx, o->ncomp * plane,
+                                 (long long)o->nz * o->ncomp * plane, plane, v2w, poses, st, A);
+    MRSIM_CUDA(cudaStreamSynchronize(st));  // the pose tables (in A) are read by the kernel
+  });
+}
 
 // ---- stack-of-spirals path ------------------------------------------------------------------------
 int mrsim_spiral_tau_c(int64_t nx, int64_t interleaves, double readout_ms, double dwell_ms, double radial_oversampling,

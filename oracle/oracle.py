@@ -574,3 +574,83 @@ def reconstruct_coils(coils: np.ndarray, acq: Acquisition) -> np.ndarray:
     _check(lib().oracle_reconstruct_coils(k.view(np.float64).ctypes.data_as(abi.c_f64p), nc, nx, ny,
                                           C.byref(acq.to_c()), out.view(np.float64).ctypes.data_as(abi.c_f64p)))
     return out.reshape(ny, nx)
+
+
+# ---- image motion (motion.rs) -----------------------------------------------------------------------
+def _motion_lib():
+    L = lib()
+    if not getattr(L, "_motion_typed", False):
+        P = C.POINTER
+        i64p = P(C.c_int64)
+        L.oracle_motion_trilinear.argtypes = [abi.c_f32p, i64p, abi.c_f64p, abi.c_f32p]
+        L.oracle_resample_by_pose.argtypes = [abi.c_f32p, i64p, abi.c_f64p, abi.c_f64p, abi.c_f32p]
+        L.oracle_apply_motion.argtypes = [P(abi.c_f32p), C.c_int64, i64p, C.c_int64, abi.c_f64p, abi.c_f64p]
+        L.oracle_apply_multiband_motion.argtypes = [P(abi.c_f32p), C.c_int64, i64p, C.c_int64, abi.c_f64p, C.c_int64,
+                                                    C.c_int32, C.c_int32, abi.c_f64p, C.c_int64, C.c_double, C.c_double,
+                                                    i64p, i64p, abi.c_f32p, abi.c_f64p, abi.c_f64p, C.c_int64, i64p,
+                                                    C.c_int64, i64p, i64p, abi.c_f32p, i64p]
+        L._motion_typed = True
+    return L
+
+
+def _i64(a):
+    a = np.ascontiguousarray(a, np.int64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def motion_trilinear(vol, dims, p) -> float:
+    v = np.ascontiguousarray(vol, np.float32)
+    d, dp = _i64(dims)
+    pp = np.ascontiguousarray(p, np.float64)
+    out = np.zeros(1, np.float32)
+    _motion_lib().oracle_motion_trilinear(v.ctypes.data_as(abi.c_f32p), dp, pp.ctypes.data_as(abi.c_f64p),
+                                          out.ctypes.data_as(abi.c_f32p))
+    return float(out[0])
+
+
+def resample_by_pose(src, dims, v2w, pose) -> np.ndarray:
+    s = np.ascontiguousarray(src, np.float32).ravel()
+    out = np.zeros_like(s)
+    d, dp = _i64(dims)
+    m = np.ascontiguousarray(v2w, np.float64).reshape(16)
+    p = np.ascontiguousarray(pose, np.float64).reshape(6)
+    _motion_lib().oracle_resample_by_pose(s.ctypes.data_as(abi.c_f32p), dp, m.ctypes.data_as(abi.c_f64p),
+                                          p.ctypes.data_as(abi.c_f64p), out.ctypes.data_as(abi.c_f32p))
+    return out
+
+
+def apply_motion(images, dims, n_volumes, v2w, poses) -> None:
+    """In place; poses is n_volumes x 6 (rot_deg, trans_mm)."""
+    ptrs = (abi.c_f32p * len(images))(*[a.ctypes.data_as(abi.c_f32p) for a in images])
+    d, dp = _i64(dims)
+    m = np.ascontiguousarray(v2w, np.float64).reshape(16)
+    p = np.ascontiguousarray(poses, np.float64).reshape(-1)
+    _motion_lib().oracle_apply_motion(ptrs, len(images), dp, n_volumes, m.ctypes.data_as(abi.c_f64p),
+                                      p.ctypes.data_as(abi.c_f64p))
+
+
+def apply_multiband_motion(images, dims, n_volumes, v2w, mb, interleaved, law_kind, drive, floor, max_, events,
+                           slice_z=None, nz_full=0):
+    """In place; events are (volume, shot, severity, jump_mm[3], jump_deg[3]); returns the dropped
+    shots as (volume, shot, attenuation)."""
+    ptrs = (abi.c_f32p * len(images))(*[a.ctypes.data_as(abi.c_f32p) for a in images])
+    d, dp = _i64(dims)
+    m = np.ascontiguousarray(v2w, np.float64).reshape(16)
+    dr = np.ascontiguousarray(drive, np.float64)
+    n = len(events)
+    vol, vp = _i64([e[0] for e in events] or [0])
+    shot, sp = _i64([e[1] for e in events] or [0])
+    sev = np.ascontiguousarray([e[2] for e in events] or [0], np.float32)
+    jm = np.ascontiguousarray([e[3] for e in events] or [(0, 0, 0)], np.float64)
+    jd = np.ascontiguousarray([e[4] for e in events] or [(0, 0, 0)], np.float64)
+    sz, szp = _i64(slice_z) if slice_z is not None else (None, None)
+    ov, ovp = _i64(np.zeros(max(n, 1)))
+    osh, oshp = _i64(np.zeros(max(n, 1)))
+    oa = np.zeros(max(n, 1), np.float32)
+    nd, ndp = _i64([0])
+    _motion_lib().oracle_apply_multiband_motion(ptrs, len(images), dp, n_volumes, m.ctypes.data_as(abi.c_f64p), mb,
+                                                int(interleaved), law_kind, dr.ctypes.data_as(abi.c_f64p), dr.size,
+                                                floor, max_, vp, sp, sev.ctypes.data_as(abi.c_f32p),
+                                                jm.ctypes.data_as(abi.c_f64p), jd.ctypes.data_as(abi.c_f64p), n, szp,
+                                                nz_full, ovp, oshp, oa.ctypes.data_as(abi.c_f32p), ndp)
+    return [(int(ov[i]), int(osh[i]), float(oa[i])) for i in range(int(nd[0]))]
