@@ -421,6 +421,36 @@ int mrsim_apply_multiband_motion(mrsim_context* ctx, float* const* images, int64
  * series reaches the forward without crossing the host link. */
 int mrsim_epi_operator_apply_motion(mrsim_epi_operator* op, const double* v2w, const double* poses);
 
+/* ---- writing the series (io.rs) ------------------------------------------------------------- */
+/* NIfTI-1 with the grid's voxel-to-world affine v2w (row-major 4x4); gzip when the path ends in
+ * ".gz".  `write_4d_timed` io.rs:135-146: data (x + nx*(y + ny*z))*nt + t, a 4D header; tr_s > 0
+ * puts the repetition time in pixdim[4] and seconds in xyzt_units (`write_4d` io.rs:131: 0). */
+int mrsim_write_nifti_4d(const char* path, const int64_t* dims, int64_t nt, const float* data, const double* v2w,
+                         double tr_s);
+/* `write_3d` io.rs:149-156: one volume x + nx*(y + ny*z), a 3D header. */
+int mrsim_write_nifti_3d(const char* path, const int64_t* dims, const float* data, const double* v2w);
+/* `hires_grid` io.rs:104-124: the simulation grid of an acquired grid refined in-plane by o. */
+int mrsim_hires_grid(const double* v2w, const int64_t* dims, int64_t o, double* out_v2w, int64_t* out_dims);
+/* `SidecarInfo` io.rs:162-184. */
+typedef struct mrsim_sidecar_info {
+  const char* manufacturer;
+  const char* phase_encoding_direction; /* "i", "j-", ... for the written voxel frame */
+  double total_readout_time;            /* s */
+  double echo_time;                     /* s */
+  double partial_fourier;
+  int64_t accel;
+  int64_t mb;
+  int32_t has_repetition_time;
+  double repetition_time_s;
+  const char* b0_field_source;          /* NULL: none */
+} mrsim_sidecar_info;
+/* `write_complex_4d` io.rs:186-228: <prefix>_part-mag_<suffix>.nii.gz, _part-phase_ (radians) and
+ * their .json sidecars; mag / phase as from mrsim_simulate_acquisition_oversampled, whose device
+ * output pass splits magnitude and phase. */
+int mrsim_write_complex_4d(const char* out_prefix, const char* suffix, const int64_t* dims, int64_t n_volumes,
+                           const float* mag, const float* phase, const double* v2w,
+                           const mrsim_sidecar_info* info);
+
 /* ---- the 3D echo trains (kspace3d.rs, readout.rs:75-322) ----------------------------------- */
 enum { MRSIM_KZ_CENTRIC = 0, MRSIM_KZ_LINEAR = 1 };                            /* readout.rs:75 */
 

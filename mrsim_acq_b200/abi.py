@@ -73,6 +73,13 @@ class DroppedShot_(C.Structure):
                 ("slices", C.c_int64 * 64)]
 
 
+class SidecarInfo_(C.Structure):
+    _fields_ = [("manufacturer", C.c_char_p), ("phase_encoding_direction", C.c_char_p),
+                ("total_readout_time", C.c_double), ("echo_time", C.c_double), ("partial_fourier", C.c_double),
+                ("accel", C.c_int64), ("mb", C.c_int64), ("has_repetition_time", C.c_int32),
+                ("repetition_time_s", C.c_double), ("b0_field_source", C.c_char_p)]
+
+
 class AcquisitionInput_(C.Structure):
     """`mrsim_acquisition_input` — `AcquisitionInput` (kspace.rs:1720-1740)."""
 
@@ -276,6 +283,11 @@ def _declare(lib):
                                                    C.POINTER(MotionEvent_), C.c_int64, C.POINTER(C.c_int64), C.c_int64,
                                                    C.POINTER(DroppedShot_), C.c_int64, C.POINTER(C.c_int64)]),
         "mrsim_epi_operator_apply_motion": (C.c_int, [P, c_f64p, c_f64p]),
+        "mrsim_write_nifti_4d": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.c_int64, c_f32p, c_f64p, C.c_double]),
+        "mrsim_write_nifti_3d": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), c_f32p, c_f64p]),
+        "mrsim_hires_grid": (C.c_int, [c_f64p, C.POINTER(C.c_int64), C.c_int64, c_f64p, C.POINTER(C.c_int64)]),
+        "mrsim_write_complex_4d": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int64), C.c_int64, c_f32p, c_f32p,
+                                             c_f64p, C.POINTER(SidecarInfo_)]),
         "mrsim_epi_operator_apply_host_compact": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),
         "mrsim_epi_operator_acquired_rows": (C.c_int, [P] + [C.POINTER(C.c_int32)] * 3),
         "mrsim_epi_operator_host_bytes_for": (C.c_int, [P, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),

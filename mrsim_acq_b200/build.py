@@ -60,7 +60,7 @@ def build(verbose: bool = False, force: bool = False) -> pathlib.Path:
         objs = list(ex.map(compile_one, srcs))
     if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         cmd = [exe, "-shared", "-o", str(LIB)] + [str(o) for o in objs] + ARCH + [
-            "-cudart", "static", "-Xcompiler", "-fvisibility=hidden", "-lpthread"]
+            "-cudart", "static", "-Xcompiler", "-fvisibility=hidden", "-lpthread", "-lz"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

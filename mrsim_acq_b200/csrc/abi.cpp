@@ -9,6 +9,7 @@
 
 #include "driver.h"
 #include "motion.h"
+#include "nifti.h"
 #include "ts_epi.h"
 #include "host_tables.h"
 #include "mrsim_internal.h"
@@ -310,29 +311,17 @@ int mrsim_simulate_acquisition_complex(mrsim_context* ctx, const mrsim_acquisiti
   });
 }
 
-// magnitude and phase in f32 (`acquire_volumes`, kspace.rs:1827-1846)
-static void mag_phase(const std::vector<float>& re, const std::vector<float>& im, float* mag, float* ph) {
-  for (size_t i = 0; i < re.size(); ++i) {
-    const float r = re[i], m = im[i];
-    mag[i] = std::sqrt(r * r + m * m);
-    ph[i] = std::atan2(m, r);
-  }
-}
-
 int mrsim_simulate_acquisition_oversampled(mrsim_context* ctx, const mrsim_acquisition_input* in,
                                            const mrsim_acquisition* acq, float* mag, float* phase) {
   return on_ctx(ctx, [&] {
     check_series_input(in, acq);
     need(mag, "mag");
     need(phase, "phase");
-    const size_t n = (size_t)in->acq_dims[0] * in->acq_dims[1] * in->acq_dims[2] * in->n_volumes;
-    std::vector<float> re(n), im(n);
     mrsim_acquisition_output out;
     std::memset(&out, 0, sizeof out);
-    out.re = re.data();
-    out.im = im.data();
-    mrsim::acquire_series(ctx, *in, *acq, nullptr, in->seed, in->seed, in->images, out);
-    mag_phase(re, im, mag, phase);
+    out.re = mag;  // the device writes magnitude and phase (kspace.rs:1839-1846) in its output pass
+    out.im = phase;
+    mrsim::acquire_series(ctx, *in, *acq, nullptr, in->seed, in->seed, in->images, out, true);
   });
 }
 
@@ -357,8 +346,6 @@ int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisitio
         mrsim::fail(buf);
       }
     if (n_echoes <= 0) mrsim::fail("simulate_acquisition_echoes needs at least one echo");
-    const size_t n = (size_t)in->acq_dims[0] * in->acq_dims[1] * in->acq_dims[2] * in->n_volumes;
-    std::vector<float> re(n), im(n);
     for (int64_t e = 0; e < n_echoes; ++e) {
       mrsim_acquisition acq_e = *acq;
       acq_e.t_echo = echo_times_ms[e];
@@ -371,11 +358,10 @@ int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisitio
       }
       mrsim_acquisition_output out;
       std::memset(&out, 0, sizeof out);
-      out.re = re.data();
-      out.im = im.data();
+      out.re = mag[e];
+      out.im = phase[e];
       mrsim::acquire_series(ctx, *in, acq_e, &opts, in->seed, in->seed ^ mrsim::echo_salt((uint64_t)e),
-                            images_per_echo[e], out);
-      mag_phase(re, im, mag[e], phase[e]);
+                            images_per_echo[e], out, true);
     }
   });
 }
@@ -617,6 +603,52 @@ int mrsim_epi_operator_host_bytes_for(const mrsim_epi_operator* op, int32_t outp
   });
 }
 
+
+// ---- writing the series ----------------------------------------------------------------------------
+int mrsim_write_nifti_4d(const char* path, const int64_t* dims, int64_t nt, const float* data, const double* v2w,
+                         double tr_s) {
+  return guarded([&] {
+    need(path, "path");
+    need(dims, "dims");
+    need(data, "data");
+    need(v2w, "v2w");
+    mrsim::write_nifti(path, dims, nt, data, v2w, tr_s, true);
+  });
+}
+
+int mrsim_write_nifti_3d(const char* path, const int64_t* dims, const float* data, const double* v2w) {
+  return guarded([&] {
+    need(path, "path");
+    need(dims, "dims");
+    need(data, "data");
+    need(v2w, "v2w");
+    mrsim::write_nifti(path, dims, 1, data, v2w, 0.0, false);
+  });
+}
+
+int mrsim_hires_grid(const double* v2w, const int64_t* dims, int64_t o, double* out_v2w, int64_t* out_dims) {
+  return guarded([&] {
+    need(v2w, "v2w");
+    need(dims, "dims");
+    need(out_v2w, "out_v2w");
+    need(out_dims, "out_dims");
+    mrsim::hires_grid(v2w, dims, o, out_v2w, out_dims);
+  });
+}
+
+int mrsim_write_complex_4d(const char* out_prefix, const char* suffix, const int64_t* dims, int64_t n_volumes,
+                           const float* mag, const float* phase, const double* v2w, const mrsim_sidecar_info* info) {
+  return guarded([&] {
+    need(out_prefix, "out_prefix");
+    need(suffix, "suffix");
+    need(dims, "dims");
+    need(mag, "mag");
+    need(phase, "phase");
+    need(v2w, "v2w");
+    need(info, "info");
+    mrsim::write_complex_4d(out_prefix, suffix, dims, n_volumes, mag, phase, v2w, *info);
+  });
+}
 
 // ---- image motion -----------------------------------------------------------------------------------
 namespace {

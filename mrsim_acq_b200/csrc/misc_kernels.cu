@@ -32,9 +32,11 @@ __device__ __forceinline__ double unit_of(uint64_t seed, uint64_t k) {
 }
 
 // One thread per (volume, slice, y, x) of a chunk of volumes [g0, g1).
+// mag_phase: write the magnitude sqrt(re^2 + im^2) and phase atan2(im, re) in f32 instead of
+// (re, im) (`simulate_acquisition_oversampled`, kspace.rs:1839-1846), in the same pass.
 __global__ void series_output_kernel(const float2* __restrict__ comb, const float* __restrict__ sigma,
                                      float* __restrict__ re, float* __restrict__ im, int g0, int g1, int nv, int nz,
-                                     int nx, int ny, const int* __restrict__ zmap, uint64_t seed) {
+                                     int nx, int ny, const int* __restrict__ zmap, uint64_t seed, int mag_phase) {
   const long long per = (long long)nx * ny;
   const long long total = (long long)(g1 - g0) * nz * per;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
@@ -58,8 +60,13 @@ __global__ void series_output_kernel(const float2* __restrict__ comb, const floa
         i += (float)(n2 * sd);
       }
     }
-    re[vox * nv + g] = r;
-    im[vox * nv + g] = i;
+    if (mag_phase) {
+      re[vox * nv + g] = sqrtf(__fadd_rn(__fmul_rn(r, r), __fmul_rn(i, i)));
+      im[vox * nv + g] = atan2f(i, r);
+    } else {
+      re[vox * nv + g] = r;
+      im[vox * nv + g] = i;
+    }
   }
 }
 
@@ -104,11 +111,13 @@ double probe_fp32_tflops(cudaStream_t st) {
 }
 
 void launch_series_output(const float2* combined, const float* sigma, float* re, float* im, int g0, int g1, int nv,
-                          int nz, int nx, int ny, const int* zmap, uint64_t receiver_seed, cudaStream_t st) {
+                          int nz, int nx, int ny, const int* zmap, uint64_t receiver_seed, cudaStream_t st,
+                          bool mag_phase) {
   const long long total = (long long)(g1 - g0) * nz * nx * ny;
   if (total <= 0) return;
   int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-  series_output_kernel<<<blocks, 256, 0, st>>>(combined, sigma, re, im, g0, g1, nv, nz, nx, ny, zmap, receiver_seed);
+  series_output_kernel<<<blocks, 256, 0, st>>>(combined, sigma, re, im, g0, g1, nv, nz, nx, ny, zmap, receiver_seed,
+                                                mag_phase ? 1 : 0);
   MRSIM_CUDA(cudaGetLastError());
 }
 

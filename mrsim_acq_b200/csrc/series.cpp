@@ -483,7 +483,7 @@ void validate_t2_volumes(const char* what, const mrsim_t2* vols, int ncomp, size
 
 void acquire_series(mrsim_context* ctx, const mrsim_acquisition_input& in, const mrsim_acquisition& acq,
                     const mrsim_acquisition_options* opts_in, uint64_t excitation_seed, uint64_t receiver_seed,
-                    const float* const* images, mrsim_acquisition_output& out) {
+                    const float* const* images, mrsim_acquisition_output& out, bool mag_phase) {
   mrsim_acquisition_options dflt;
   std::memset(&dflt, 0, sizeof dflt);
   const mrsim_acquisition_options& opts = opts_in ? *opts_in : dflt;
@@ -771,7 +771,7 @@ void acquire_series(mrsim_context* ctx, const mrsim_acquisition_input& in, const
       for (int s = 0; s < nsl; ++s)
         MRSIM_CUDA(cudaMemcpyAsync(cap_comb + ((size_t)g * nsl + s) * per, comb + ((size_t)(g - g0) * nz + captured[s]) * per,
                                    per * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-    launch_series_output(comb, d_sigma, d_re, d_im, g0, g1, nv, nz, nx, ny, d_zmap, receiver_seed, st);
+    launch_series_output(comb, d_sigma, d_re, d_im, g0, g1, nv, nz, nx, ny, d_zmap, receiver_seed, st, mag_phase);
     MRSIM_CUDA(cudaStreamSynchronize(st));
   }
   MRSIM_CUDA(cudaMemcpyAsync(out.re, d_re, nvox_acq * nv * 4, cudaMemcpyDeviceToHost, st));

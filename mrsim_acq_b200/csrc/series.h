@@ -27,14 +27,16 @@ std::vector<float2> slice_forward2(mrsim_context* ctx, const mrsim_slice_input& 
 void simulate_slice_full(mrsim_context* ctx, const mrsim_slice_input& inp, const mrsim_acquisition& acq,
                          SliceOutputs& out);
 // `acquire_volumes_complex` (kspace.rs:1851-2125) with explicit excitation and receiver seeds;
-// `images` overrides in.images (the echoes entry passes each echo's images).
+// `images` overrides in.images (the echoes entry passes each echo's images).  mag_phase: out.re /
+// out.im receive the magnitude and phase (kspace.rs:1839-1846), split on the device.
 void acquire_series(mrsim_context* ctx, const mrsim_acquisition_input& in, const mrsim_acquisition& acq,
                     const mrsim_acquisition_options* opts, uint64_t excitation_seed, uint64_t receiver_seed,
-                    const float* const* images, mrsim_acquisition_output& out);
+                    const float* const* images, mrsim_acquisition_output& out, bool mag_phase = false);
 
 // misc_kernels.cu: combined images -> (re, im) in the series layout vox*nv + g, plus the
 // image-space noise of `acquire_volumes_complex` (kspace.rs:2031-2052).
 void launch_series_output(const float2* combined, const float* sigma, float* re, float* im, int g0, int g1, int nv,
-                          int nz, int nx, int ny, const int* zmap, uint64_t receiver_seed, cudaStream_t st);
+                          int nz, int nx, int ny, const int* zmap, uint64_t receiver_seed, cudaStream_t st,
+                          bool mag_phase = false);
 
 }  // namespace mrsim

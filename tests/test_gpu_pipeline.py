@@ -192,3 +192,18 @@ def test_series_with_eight_ring_coils_matches_the_oracle(maps, gpu_ctx):
     for key in ("acquired", "reconstructed", "coil_images", "combined"):
         gw = want[key].view(np.complex64).reshape(got[key].shape)
         assert rel_l2(got[key], gw) <= TOL, (key, rel_l2(got[key], gw))
+
+
+def test_magnitude_and_phase_split_on_the_device(gpu_ctx):
+    """`simulate_acquisition_oversampled` returns magnitude and phase from the device output pass
+    (kspace.rs:1839-1846): the magnitude is sqrt(re^2 + im^2) in f32 bit for bit, the phase
+    atan2(im, re) within 2 f32 ulp of the host's."""
+    name, inp, acq = cases.golden_series_inputs()[0]
+    out = api.simulate_acquisition_complex(inp, acq, ctx=gpu_ctx)
+    mag, ph = api.simulate_acquisition_oversampled(inp, acq, ctx=gpu_ctx)
+    re, im = out["re"].astype(np.float32), out["im"].astype(np.float32)
+    want = np.sqrt(re * re + im * im, dtype=np.float32)
+    assert np.array_equal(mag, want)
+    wph = np.arctan2(im, re).astype(np.float32)
+    ulp = np.abs(ph.view(np.int32).astype(np.int64) - wph.view(np.int32).astype(np.int64))
+    assert ulp.max() <= 2, ulp.max()
