@@ -367,6 +367,27 @@ int mrsim_epi_operator_host_bytes_for(const mrsim_epi_operator* op, int32_t outp
 int mrsim_epi_operator_host_bytes(const mrsim_epi_operator* op, int64_t* upload_bytes,
                                   int64_t* download_bytes);
 
+/* ---- a batch of series of different geometries --------------------------------------------- */
+/* No reference counterpart (the reference runs one series per call): n_series series, each its
+ * own geometry (matrix, grid, slice count; the same acquisition and echoes), as one plan, so each
+ * stage of a forward or adjoint is one launch over every unit (slice of a volume) of every series,
+ * with each unit's own descriptor.  Each series keeps its own buffers in the layouts of
+ * mrsim_epi_operator; `grads` as there. */
+typedef struct mrsim_epi_batch mrsim_epi_batch;
+int mrsim_epi_batch_create(mrsim_context* ctx, int32_t n_series, const mrsim_acquisition_input* const* inputs,
+                           const mrsim_acquisition* acq, const double* echo_times_ms, int64_t n_echoes,
+                           int32_t grads, mrsim_epi_batch** out);
+int mrsim_epi_batch_destroy(mrsim_epi_batch* b);
+/* Acquired k-space samples of one forward over every series. */
+int64_t mrsim_epi_batch_samples(const mrsim_epi_batch* b);
+/* Asynchronous on the context stream: statics + forward of every series; adjoint of every series'
+ * k-space buffer. */
+int mrsim_epi_batch_forward(mrsim_epi_batch* b);
+int mrsim_epi_batch_adjoint(mrsim_epi_batch* b);
+/* Synchronous: series i's k-space and complex-image adjoint to host buffers (layouts of
+ * mrsim_epi_operator; either may be NULL). */
+int mrsim_epi_batch_download(mrsim_epi_batch* b, int32_t series, float* kspace, float* comp_grad);
+
 /* ---- image motion before the forward (motion.rs) -------------------------------------------- */
 /* A pose is 6 doubles: rotation (degrees about x, y, z; R = Rz Ry Rx) then translation (mm),
  * `Pose` (motion.rs:43-47).  v2w is the grid's voxel-to-world affine, row-major 4x4.  The

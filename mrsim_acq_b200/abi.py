@@ -283,6 +283,13 @@ def _declare(lib):
                                                    C.POINTER(MotionEvent_), C.c_int64, C.POINTER(C.c_int64), C.c_int64,
                                                    C.POINTER(DroppedShot_), C.c_int64, C.POINTER(C.c_int64)]),
         "mrsim_epi_operator_apply_motion": (C.c_int, [P, c_f64p, c_f64p]),
+        "mrsim_epi_batch_create": (C.c_int, [P, C.c_int32, C.POINTER(C.POINTER(AcquisitionInput_)),
+                                             C.POINTER(Acquisition_), c_f64p, C.c_int64, C.c_int32, C.POINTER(P)]),
+        "mrsim_epi_batch_destroy": (C.c_int, [P]),
+        "mrsim_epi_batch_samples": (C.c_int64, [P]),
+        "mrsim_epi_batch_forward": (C.c_int, [P]),
+        "mrsim_epi_batch_adjoint": (C.c_int, [P]),
+        "mrsim_epi_batch_download": (C.c_int, [P, C.c_int32, c_f32p, c_f32p]),
         "mrsim_write_nifti_4d": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.c_int64, c_f32p, c_f64p, C.c_double]),
         "mrsim_write_nifti_3d": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), c_f32p, c_f64p]),
         "mrsim_hires_grid": (C.c_int, [c_f64p, C.POINTER(C.c_int64), C.c_int64, c_f64p, C.POINTER(C.c_int64)]),

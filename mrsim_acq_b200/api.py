@@ -550,6 +550,96 @@ def simulate_acquisition_echoes(inp: AcquisitionInput, images_per_echo: Sequence
 
 
 # ---- the series forward/adjoint operator ----------------------------------------------------------
+def _operator_input(keep, sim_dims, acq_dims, n_volumes, t2, fmap, images=None, t_inhom=None, eddy_drive=None,
+                    prep_drive=None, phase=None, seed=0) -> abi.AcquisitionInput_:
+    inp = abi.AcquisitionInput_()
+    for i in range(3):
+        inp.sim_dims[i] = sim_dims[i]
+        inp.acq_dims[i] = acq_dims[i]
+    inp.n_volumes = n_volumes
+    inp.ncomp = len(t2)
+    inp.t2 = keep.t2s(t2)
+    inp.t_inhom = keep.t2s(t_inhom) if t_inhom is not None else None
+    inp.fmap = keep.f32(np.ravel(fmap))
+    if eddy_drive is not None:
+        flags = np.array([d is not None for d in eddy_drive], np.int32)
+        vals = np.array([d if d is not None else (0.0, 0.0, 0.0) for d in eddy_drive], np.float64)
+        keep += [flags, vals]
+        inp.eddy_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        inp.eddy_drive = vals.ctypes.data_as(abi.c_f64p)
+    if prep_drive is not None:
+        flags = np.array([d is not None for d in prep_drive], np.int32)
+        vals = np.array([(d[0], *d[1]) if d is not None else (0, 0, 0, 0) for d in prep_drive], np.float64)
+        keep += [flags, vals]
+        inp.prep_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        inp.prep_drive = vals.ctypes.data_as(abi.c_f64p)
+    ph = (phase or PhaseModel.none()).to_c()
+    keep.append(ph)
+    inp.phase = C.pointer(ph)
+    inp.seed = int(seed)
+    if images is not None:
+        inp.images = keep.ptrs([np.ravel(a) for a in images])
+    keep.append(inp)
+    return inp
+
+
+class EpiBatch:
+    """Several series of different geometries as one plan (`mrsim_epi_batch`): each stage of a
+    forward or adjoint is one launch over every unit of every series.  `series` holds dicts with
+    sim_dims, acq_dims, n_volumes, t2, fmap, images and optionally t_inhom, eddy_drive,
+    prep_drive, phase, seed."""
+
+    def __init__(self, series: Sequence[dict], acq: Acquisition, echo_times_ms: Optional[Sequence[float]] = None,
+                 grads: int = 0, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        keep = _Keep()
+        ins = [_operator_input(keep, s["sim_dims"], s["acq_dims"], s["n_volumes"], s["t2"], s["fmap"],
+                               s.get("images"), s.get("t_inhom"), s.get("eddy_drive"), s.get("prep_drive"),
+                               s.get("phase"), s.get("seed", 0)) for s in series]
+        arr = (C.POINTER(abi.AcquisitionInput_) * len(ins))(*[C.pointer(i) for i in ins])
+        tes = keep.f64(np.asarray(echo_times_ms, np.float64)) if echo_times_ms is not None else None
+        ne = len(echo_times_ms) if echo_times_ms is not None else 0
+        h = C.c_void_p()
+        check(lib().mrsim_epi_batch_create(self.ctx.handle, len(ins), arr, C.byref(acq.to_c()), tes, ne, int(grads),
+                                           C.byref(h)))
+        self.handle = h
+        self.series = [dict(s) for s in series]
+        self.n_coils = max(int(acq.n_coils), 1)
+        self.n_echoes = max(ne, 1)
+
+    @property
+    def samples(self) -> int:
+        return int(lib().mrsim_epi_batch_samples(self.handle))
+
+    def forward(self):
+        check(lib().mrsim_epi_batch_forward(self.handle))
+
+    def adjoint(self):
+        check(lib().mrsim_epi_batch_adjoint(self.handle))
+
+    def download(self, i: int) -> dict:
+        s = self.series[i]
+        snx, sny, nz = s["sim_dims"]
+        nx, ny, _ = s["acq_dims"]
+        nv, nc = s["n_volumes"], len(s["t2"])
+        k = np.zeros((nv, nz, self.n_coils, self.n_echoes, ny, nx), np.complex64)
+        g = np.zeros((nv, nz, nc, sny, snx), np.complex64)
+        check(lib().mrsim_epi_batch_download(self.handle, i, C.cast(k.ctypes.data, abi.c_f32p),
+                                             C.cast(g.ctypes.data, abi.c_f32p)))
+        return {"kspace": k, "comp_grad": g}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().mrsim_epi_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class EpiOperator:
     """The batched forward/adjoint operator of a 2D EPI series (`mrsim_epi_operator`)."""
 
@@ -560,33 +650,8 @@ class EpiOperator:
                  slice_z=None, nz_full: int = 0, ctx: Optional[Context] = None):
         self.ctx = ctx or default_context()
         keep = _Keep()
-        inp = abi.AcquisitionInput_()
-        for i in range(3):
-            inp.sim_dims[i] = sim_dims[i]
-            inp.acq_dims[i] = acq_dims[i]
-        inp.n_volumes = n_volumes
-        inp.ncomp = len(t2)
-        inp.t2 = keep.t2s(t2)
-        inp.t_inhom = keep.t2s(t_inhom) if t_inhom is not None else None
-        inp.fmap = keep.f32(np.ravel(fmap))
-        if eddy_drive is not None:
-            flags = np.array([d is not None for d in eddy_drive], np.int32)
-            vals = np.array([d if d is not None else (0.0, 0.0, 0.0) for d in eddy_drive], np.float64)
-            keep += [flags, vals]
-            inp.eddy_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
-            inp.eddy_drive = vals.ctypes.data_as(abi.c_f64p)
-        if prep_drive is not None:
-            flags = np.array([d is not None for d in prep_drive], np.int32)
-            vals = np.array([(d[0], *d[1]) if d is not None else (0, 0, 0, 0) for d in prep_drive], np.float64)
-            keep += [flags, vals]
-            inp.prep_drive_set = flags.ctypes.data_as(C.POINTER(C.c_int32))
-            inp.prep_drive = vals.ctypes.data_as(abi.c_f64p)
-        ph = (phase or PhaseModel.none()).to_c()
-        keep.append(ph)
-        inp.phase = C.pointer(ph)
-        inp.seed = int(seed)
-        if images is not None:
-            inp.images = keep.ptrs([np.ravel(a) for a in images])
+        inp = _operator_input(keep, sim_dims, acq_dims, n_volumes, t2, fmap, images, t_inhom, eddy_drive, prep_drive,
+                              phase, seed)
         tes = keep.f64(np.asarray(echo_times_ms, np.float64)) if echo_times_ms is not None else None
         ne = len(echo_times_ms) if echo_times_ms is not None else 0
         sz = None

@@ -604,6 +604,76 @@ int mrsim_epi_operator_host_bytes_for(const mrsim_epi_operator* op, int32_t outp
 }
 
 
+// ---- a batch of series of different geometries -----------------------------------------------------
+struct mrsim_epi_batch {
+  mrsim::EpiBatch* impl;
+};
+
+int mrsim_epi_batch_create(mrsim_context* ctx, int32_t n_series, const mrsim_acquisition_input* const* inputs,
+                           const mrsim_acquisition* acq, const double* echo_times_ms, int64_t n_echoes,
+                           int32_t grads, mrsim_epi_batch** out) {
+  return on_ctx(ctx, [&] {
+    need(inputs, "inputs");
+    need(acq, "acq");
+    need(out, "out");
+    for (int32_t i = 0; i < n_series; ++i) {
+      need(inputs[i], "inputs[i]");
+      need(inputs[i]->fmap, "fmap");
+      need(inputs[i]->t2, "t2");
+    }
+    auto* b = new mrsim_epi_batch();
+    try {
+      b->impl = mrsim::epi_batch_create(ctx, n_series, inputs, *acq, echo_times_ms, n_echoes, grads);
+    } catch (...) {
+      delete b;
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int mrsim_epi_batch_destroy(mrsim_epi_batch* b) {
+  return guarded([&] {
+    if (!b) return;
+    if (b->impl) {
+      mrsim_context* ctx = b->impl->ctx;
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      cudaSetDevice(ctx->device);
+      cudaStreamSynchronize(ctx->stream);
+      delete b->impl;
+    }
+    delete b;
+  });
+}
+
+int64_t mrsim_epi_batch_samples(const mrsim_epi_batch* b) { return b && b->impl ? b->impl->samples : 0; }
+
+int mrsim_epi_batch_forward(mrsim_epi_batch* b) {
+  if (!b) return guarded([] { need(nullptr, "batch"); });
+  return on_ctx(b->impl->ctx, [&] { mrsim::epi_batch_forward(b->impl); });
+}
+
+int mrsim_epi_batch_adjoint(mrsim_epi_batch* b) {
+  if (!b) return guarded([] { need(nullptr, "batch"); });
+  return on_ctx(b->impl->ctx, [&] { mrsim::epi_batch_adjoint(b->impl); });
+}
+
+int mrsim_epi_batch_download(mrsim_epi_batch* b, int32_t series, float* kspace, float* comp_grad) {
+  if (!b) return guarded([] { need(nullptr, "batch"); });
+  return on_ctx(b->impl->ctx, [&] {
+    if (series < 0 || series >= (int32_t)b->impl->ops.size()) mrsim::fail("series index out of range");
+    const mrsim::EpiOperator* o = b->impl->ops[series].get();
+    cudaStream_t st = b->impl->ctx->stream;
+    if (kspace)
+      MRSIM_CUDA(cudaMemcpyAsync(kspace, o->d_kspace, o->kspace_elems * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    if (comp_grad)
+      MRSIM_CUDA(cudaMemcpyAsync(comp_grad, o->d_comp_grad,
+                                 (size_t)o->nv * o->nz * o->ncomp * o->snx * o->sny * sizeof(float2),
+                                 cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
 // ---- writing the series ----------------------------------------------------------------------------
 int mrsim_write_nifti_4d(const char* path, const int64_t* dims, int64_t nt, const float* data, const double* v2w,
                          double tr_s) {

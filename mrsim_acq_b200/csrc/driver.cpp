@@ -506,6 +506,36 @@ void epi_operator_adjoint_units(EpiOperator* op, cudaStream_t st, int u0, int u1
   }
 }
 
+EpiBatch* epi_batch_create(mrsim_context* ctx, int n, const mrsim_acquisition_input* const* inputs,
+                           const mrsim_acquisition& acq, const double* echo_times_ms, int64_t n_echoes, int grads) {
+  if (n <= 0) fail("a batch needs at least one series");
+  std::unique_ptr<EpiBatch> b(new EpiBatch());
+  b->ctx = ctx;
+  std::vector<UnitDesc> units;
+  std::vector<StaticDesc> statics;
+  for (int i = 0; i < n; ++i) {
+    if (!inputs[i]) fail("series " + std::to_string(i) + " is NULL");
+    b->ops.emplace_back(epi_operator_create(ctx, *inputs[i], acq, echo_times_ms, n_echoes, nullptr, 0, grads));
+    const EpiPlan& p = *b->ops.back()->plan;
+    b->unit0.push_back((int)units.size());
+    units.insert(units.end(), p.host_units.begin(), p.host_units.end());
+    std::vector<StaticDesc> sd(p.n_statics);
+    MRSIM_CUDA(cudaMemcpy(sd.data(), p.d_statics, sizeof(StaticDesc) * sd.size(), cudaMemcpyDeviceToHost));
+    statics.insert(statics.end(), sd.begin(), sd.end());
+    b->samples += b->ops.back()->samples_per_step;
+  }
+  b->plan.reset(epi_plan_create(units.data(), (int)units.size(), statics.data(), (int)statics.size()));
+  MRSIM_CUDA(cudaStreamSynchronize(ctx->stream));
+  return b.release();
+}
+
+void epi_batch_forward(EpiBatch* b) {
+  epi_plan_statics(b->plan.get(), b->ctx->stream);
+  epi_plan_forward(b->plan.get(), b->ctx->stream);
+}
+
+void epi_batch_adjoint(EpiBatch* b) { epi_plan_adjoint(b->plan.get(), b->ctx->stream); }
+
 void epi_operator_forward(EpiOperator* op) {
   cudaStream_t st = op->ctx->stream;
   epi_plan_statics(op->plan.get(), st);

@@ -91,6 +91,21 @@ int epi_operator_segmented_error(EpiOperator* op);
 void epi_operator_apply_host(EpiOperator* op, const float* const* images, float* kspace, float* comp_grad,
                              float* fmap_grad, float* r2_grad, bool compact = false);
 
+// Several series of different geometries (matrix, grid, slice count, coils) in one plan: each
+// series keeps its own operator (buffers, tables, line list) and the units of all of them form
+// one unit list, so each stage of a forward or adjoint is one launch over every unit.
+struct EpiBatch {
+  mrsim_context* ctx = nullptr;
+  std::vector<std::unique_ptr<EpiOperator>> ops;
+  std::vector<int> unit0;  // first plan unit of each series
+  std::unique_ptr<EpiPlan> plan;
+  int64_t samples = 0;
+};
+EpiBatch* epi_batch_create(mrsim_context* ctx, int n, const mrsim_acquisition_input* const* inputs,
+                           const mrsim_acquisition& acq, const double* echo_times_ms, int64_t n_echoes, int grads);
+void epi_batch_forward(EpiBatch* b);
+void epi_batch_adjoint(EpiBatch* b);
+
 // noalloc.cu: the forward of one slice with every intermediate in static device arrays.
 void build_coil_kspaces_noalloc(const mrsim_slice_input& inp, const mrsim_acquisition& acq, float2* out,
                                 cudaStream_t st);
