@@ -342,6 +342,15 @@ int mrsim_epi_operator_set_segmented(mrsim_epi_operator* op, int32_t precision);
 int mrsim_epi_operator_segmentation(const mrsim_epi_operator* op, int32_t* n_groups, int32_t* seg_l,
                                     double* bound, int32_t max_groups, double* flops_forward,
                                     double* flops_adjoint);
+/* The autotuner (no reference counterpart): times the plan's tunables on the operator's first
+ * units with device events — coil classes on/off, the x-stage as FFTs or as the DFT GEMM, the
+ * fixed-coil y-adjoint's rows per thread (4 or 2) and, with flags bit 0, the segmented path in
+ * split f16 / bf16 — keeps the fastest, and records it in the text file cache_path (one line per
+ * operator shape; NULL: no cache).  A shape found in the cache takes its recorded choice without
+ * timing.  The choice is written to `choice` (NUL-terminated, capacity choice_cap) and the timed
+ * forward + adjoint of the timed units to *ms (0 when taken from the cache). */
+int mrsim_epi_operator_tune(mrsim_epi_operator* op, const char* cache_path, int32_t flags, char* choice,
+                            int64_t choice_cap, double* ms);
 /* 0, or the code of a wait inside the segmented kernels that gave up (synchronises the stream). */
 int mrsim_epi_operator_segmented_status(mrsim_epi_operator* op, int32_t* code);
 /* As mrsim_epi_operator_apply_host, with the k-space in the compact layout

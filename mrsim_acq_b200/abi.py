@@ -301,6 +301,8 @@ def _declare(lib):
         "mrsim_epi_operator_segmentation": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), c_f64p,
                                                       C.c_int32, c_f64p, c_f64p]),
         "mrsim_epi_operator_segmented_status": (C.c_int, [P, C.POINTER(C.c_int32)]),
+        "mrsim_epi_operator_tune": (C.c_int, [P, C.c_char_p, C.c_int32, C.c_char_p, C.c_int64,
+                                              C.POINTER(C.c_double)]),
         "mrsim_spiral_tau_c": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, c_f64p]),
         "mrsim_spiral_trajectory": (C.c_int, [C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
                                               C.c_int64, c_f64p, c_f64p, C.POINTER(SpiralInfo_)]),

@@ -804,6 +804,15 @@ class EpiOperator:
         return {"L": [int(ls[i]) for i in range(k)], "bound": [float(bs[i]) for i in range(k)],
                 "flops_forward": float(ff.value), "flops_adjoint": float(fa.value)}
 
+    def tune(self, cache_path: Optional[str] = None, segmented: bool = False) -> dict:
+        """The autotuner (`mrsim_epi_operator_tune`): keeps the fastest plan for this shape and
+        returns {"choice": ..., "ms": timed forward + adjoint of the timed units, 0 if cached}."""
+        buf = C.create_string_buffer(256)
+        ms = C.c_double()
+        check(lib().mrsim_epi_operator_tune(self.handle, str(cache_path).encode() if cache_path else None,
+                                            1 if segmented else 0, buf, 256, C.byref(ms)))
+        return {"choice": buf.value.decode(), "ms": float(ms.value)}
+
     def segmented_status(self) -> int:
         code = C.c_int32()
         check(lib().mrsim_epi_operator_segmented_status(self.handle, C.byref(code)))

@@ -506,6 +506,20 @@ int mrsim_epi_operator_segmentation(const mrsim_epi_operator* op, int32_t* n_gro
   });
 }
 
+int mrsim_epi_operator_tune(mrsim_epi_operator* op, const char* cache_path, int32_t flags, char* choice,
+                            int64_t choice_cap, double* ms) {
+  if (!op) return guarded([] { need(nullptr, "operator"); });
+  return on_ctx(op->impl->ctx, [&] {
+    MRSIM_CUDA(cudaStreamSynchronize(op->impl->ctx->stream));
+    const std::string c = mrsim::epi_operator_tune(op->impl, cache_path, flags, ms);
+    if (choice && choice_cap > 0) {
+      const size_t n = std::min<size_t>(c.size(), (size_t)choice_cap - 1);
+      std::memcpy(choice, c.data(), n);
+      choice[n] = 0;
+    }
+  });
+}
+
 int mrsim_epi_operator_segmented_status(mrsim_epi_operator* op, int32_t* code) {
   if (!op) return guarded([] { need(nullptr, "operator"); });
   return on_ctx(op->impl->ctx, [&] {

@@ -536,6 +536,138 @@ void epi_batch_forward(EpiBatch* b) {
 
 void epi_batch_adjoint(EpiBatch* b) { epi_plan_adjoint(b->plan.get(), b->ctx->stream); }
 
+// ---- the autotuner ------------------------------------------------------------------------------
+namespace {
+std::string tune_key(const EpiOperator& o) {
+  char buf[256];
+  std::snprintf(buf, sizeof buf, "epi snx%d sny%d nx%d ny%d coils%d comp%d lines%d echoes%d maps%d grads%d%d", o.snx,
+                o.sny, o.nx, o.ny, o.ncoils, o.ncomp, o.n_lines, o.n_echoes, o.maps ? 1 : 0, o.want_fmap ? 1 : 0,
+                o.want_r2 ? 1 : 0);
+  return buf;
+}
+struct TuneChoice {
+  EpiPlanOptions opt;
+  int segmented = 0;  // 0 exact, 1 split f16, 2 split bf16
+};
+std::string describe(const TuneChoice& c) {
+  char buf[160];
+  std::snprintf(buf, sizeof buf, "classes=%d x=%s adjoint_rows=%d path=%s", c.opt.no_classes ? 0 : 1,
+                c.opt.dft_x ? "dft-gemm" : "fft", c.opt.adj_rows, c.segmented == 0 ? "exact" : c.segmented == 1 ? "segmented-f16" : "segmented-bf16");
+  return buf;
+}
+bool parse_choice(const std::string& v, TuneChoice& c) {
+  int cls = 1, rows = 0;
+  char x[32] = {0}, path[32] = {0};
+  if (std::sscanf(v.c_str(), "classes=%d x=%31s adjoint_rows=%d path=%31s", &cls, x, &rows, path) != 4) return false;
+  c.opt.no_classes = cls ? 0 : 1;
+  c.opt.dft_x = std::string(x) == "dft-gemm" ? 1 : 0;
+  c.opt.adj_rows = rows;
+  const std::string ps(path);
+  c.segmented = ps == "segmented-f16" ? 1 : ps == "segmented-bf16" ? 2 : 0;
+  return true;
+}
+void apply_choice(EpiOperator* op, const TuneChoice& c) {
+  op->plan.reset(epi_plan_create(op->plan->host_units.data(), op->plan->n_units, op->plan->host_statics.data(),
+                                 (int)op->plan->host_statics.size(), &c.opt));
+  epi_operator_set_segmented(op, c.segmented);
+}
+}  // namespace
+
+std::string epi_operator_tune(EpiOperator* op, const char* cache_path, int flags, double* ms_out) {
+  const std::string key = tune_key(*op);
+  // the cache: one "key<TAB>choice" line per shape
+  std::vector<std::pair<std::string, std::string>> lines;
+  if (cache_path) {
+    if (FILE* f = std::fopen(cache_path, "r")) {
+      char buf[1024];
+      while (std::fgets(buf, sizeof buf, f)) {
+        std::string l(buf);
+        while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
+        const size_t t = l.find('\t');
+        if (t != std::string::npos) lines.emplace_back(l.substr(0, t), l.substr(t + 1));
+      }
+      std::fclose(f);
+    }
+    for (auto& kv : lines) {
+      TuneChoice c;
+      if (kv.first == key && parse_choice(kv.second, c)) {
+        apply_choice(op, c);
+        if (ms_out) *ms_out = 0.0;
+        return describe(c) + " (cached)";
+      }
+    }
+  }
+  cudaStream_t st = op->ctx->stream;
+  const bool had_cls = op->plan->fwd_cls || op->plan->adj_cls;
+  const bool had_fft = op->plan->xfft;
+  bool has_four = false;
+  for (int pass = 0; pass < 4; ++pass) has_four = has_four || (op->plan->adjq[pass] && op->plan->adj_ty[pass] == 4);
+  std::vector<TuneChoice> cands;
+  for (int nc = 0; nc <= (had_cls ? 1 : 0); ++nc)
+    for (int dx = 0; dx <= (had_fft ? 1 : 0); ++dx)
+      for (int rows : {0, 2}) {
+        if (rows == 2 && !has_four) continue;
+        TuneChoice c;
+        c.opt.no_classes = nc;
+        c.opt.dft_x = dx;
+        c.opt.adj_rows = rows;
+        cands.push_back(c);
+        if (flags & 1)
+          for (int sg : {1, 2}) {
+            TuneChoice t = c;
+            t.segmented = sg;
+            cands.push_back(t);
+          }
+      }
+  const int u1 = std::min(op->plan->n_units, 2 * 148);
+  cudaEvent_t e0, e1;
+  MRSIM_CUDA(cudaEventCreate(&e0));
+  MRSIM_CUDA(cudaEventCreate(&e1));
+  double best_ms = 1e300;
+  TuneChoice best;
+  for (const TuneChoice& c : cands) {
+    try {
+      apply_choice(op, c);
+    } catch (const Error&) {
+      continue;  // not valid for this shape (e.g. the segmented path's preconditions)
+    }
+    auto pass = [&] {
+      epi_plan_statics(op->plan.get(), st, 0, u1);
+      epi_operator_forward_units(op, st, 0, u1);
+      epi_operator_adjoint_units(op, st, 0, u1);
+    };
+    pass();
+    MRSIM_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < 3; ++r) pass();
+    MRSIM_CUDA(cudaEventRecord(e1, st));
+    MRSIM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    MRSIM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms / 3.0 < best_ms) {
+      best_ms = ms / 3.0;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  apply_choice(op, best);
+  if (ms_out) *ms_out = best_ms;
+  if (cache_path) {
+    bool replaced = false;
+    for (auto& kv : lines)
+      if (kv.first == key) {
+        kv.second = describe(best);
+        replaced = true;
+      }
+    if (!replaced) lines.emplace_back(key, describe(best));
+    if (FILE* f = std::fopen(cache_path, "w")) {
+      for (auto& kv : lines) std::fprintf(f, "%s\t%s\n", kv.first.c_str(), kv.second.c_str());
+      std::fclose(f);
+    }
+  }
+  return describe(best);
+}
+
 void epi_operator_forward(EpiOperator* op) {
   cudaStream_t st = op->ctx->stream;
   epi_plan_statics(op->plan.get(), st);

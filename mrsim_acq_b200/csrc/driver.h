@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "mrsim_internal.h"
@@ -82,6 +83,10 @@ void epi_operator_adjoint(EpiOperator* op);
 void epi_operator_forward_units(EpiOperator* op, cudaStream_t st, int u0, int u1);
 void epi_operator_adjoint_units(EpiOperator* op, cudaStream_t st, int u0, int u1);
 void epi_operator_set_segmented(EpiOperator* op, int precision);
+// Times the plan's tunables (and with flags bit 0 the segmented path) on the operator's first
+// units, keeps the fastest, and records it in the cache file (NULL: none) under the operator's
+// shape; a shape already in the cache takes its recorded choice without timing.
+std::string epi_operator_tune(EpiOperator* op, const char* cache_path, int flags, double* ms);
 int epi_operator_segmented_error(EpiOperator* op);
 // Forward + adjoint from host images to host k-space and gradients (any output may be NULL),
 // pipelined by groups of slices (or of volumes for one slice): a group's images upload, and its

@@ -1810,11 +1810,13 @@ static void* dev_upload(EpiPlan* p, const void* src, size_t bytes) {
   return d;
 }
 
-EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns) {
+EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns, const EpiPlanOptions* opt) {
   EpiPlan* p = new EpiPlan();
   try {
+    if (opt) p->opt = *opt;
     p->n_units = n;
     p->host_units.assign(hu, hu + n);
+    p->host_statics.assign(hs, hs + ns);
     p->d_units = (UnitDesc*)dev_upload(p, hu, sizeof(UnitDesc) * n);
     p->n_statics = ns;
     p->d_statics = (StaticDesc*)dev_upload(p, hs, sizeof(StaticDesc) * ns);
@@ -1859,7 +1861,7 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
         if (((u.flags & UF_MAPS) != 0) != (pass == 1)) continue;
         cl = u.ncoils == 8 && u.geo.ncls == 5 && u.geo.coil_off != 0.f && u.geo.cls && u.geo.eyc;
       }
-      p->fwd_nv[pass] = cl ? 6 : 0;
+      p->fwd_nv[pass] = (cl && !p->opt.no_classes) ? 6 : 0;
     }
     for (int pass = 0; pass < 2; ++pass) {
       std::vector<int4> tiles;
@@ -1877,7 +1879,7 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->d_ytiles[pass] = (int4*)dev_upload(p, tiles.data(), sizeof(int4) * tiles.size());
     }
     // x-stage as per-row FFTs when every unit has a power-of-two snx with FFT tables
-    p->xfft = n > 0;
+    p->xfft = n > 0 && !p->opt.dft_x;
     for (int i = 0; i < n; ++i) {
       const int N = hu[i].snx;
       const bool pow2 = N >= 8 && N <= kXfftMaxN && (N & (N - 1)) == 0, warp = N % 32 == 0 && N <= 256;
@@ -1948,12 +1950,16 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
         const UnitDesc& u = hu[i];
         cl = u.ncoils == 8 && u.geo.ncls == 5 && u.geo.coil_off != 0.f && u.geo.cls && u.geo.eyc;
       }
-      p->adj_cls = cl;
+      p->adj_cls = cl && !p->opt.no_classes;
     }
     for (int pass = 0; pass < 4; ++pass) {
       bool maps = pass & 1, grads = pass & 2;
       p->adjq[pass] = p->adj_cls ? 6 : (maps && p->nc == 8) ? 0 : nq_all;
-      const int step = p->adjq[pass] ? 2 * adjq_rows_v(p->nc, maps, p->adj_cls) : kTY;
+      // rows per thread: the built-in choice, or 2 where 4 would be (the tunable)
+      int ty = adjq_rows_v(p->nc, maps, p->adj_cls);
+      if (p->opt.adj_rows == 2 && ty == 4) ty = 2;
+      p->adj_ty[pass] = ty;
+      const int step = p->adjq[pass] ? 2 * ty : kTY;
       std::vector<int4> yt;
       p->a_start[pass].assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
@@ -2143,17 +2149,26 @@ void epi_plan_adjoint_ystage(const EpiPlan* p, cudaStream_t st, int u0, int u1) 
     const int NCv = p->nc;
     if (p->adjq[pass]) {
       const int NQv = p->adjq[pass];
+      const int TYv = p->adj_ty[pass];
       const size_t smq = sizeof(float2) * (size_t)kAdjStages * adjq_chunk_lines(NQv) * NQv * 128 +
                          sizeof(float) * (size_t)(p->max_lines + adjq_chunk_lines(NQv)) *
-                             (2 * adjq_rows_v(NCv, maps, p->adj_cls) + adjq_line_floats(NCv, maps));
+                             (2 * TYv + adjq_line_floats(NCv, maps));
       bool launched = false;
       const bool virt = p->adj_cls;
+      // the built-in rows per thread, and 2 rows where the built-in choice is 4
 #define MRSIM_AQV(NQV, NCV, M, G, V)                                                    \
   if (NQv == NQV && NCv == NCV && maps == M && grads == G && virt == V) {               \
-    auto k = yadjoint_q_kernel<NQV, adjq_rows_v(NCV, M, V), NCV, M, G, V>;              \
-    set_smem(k, smq);                                                                   \
-    k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                              \
-    launched = true;                                                                    \
+    if (TYv == adjq_rows_v(NCV, M, V)) {                                                \
+      auto k = yadjoint_q_kernel<NQV, adjq_rows_v(NCV, M, V), NCV, M, G, V>;            \
+      set_smem(k, smq);                                                                 \
+      k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                            \
+      launched = true;                                                                  \
+    } else if (adjq_rows_v(NCV, M, V) == 4 && TYv == 2) {                               \
+      auto k = yadjoint_q_kernel<NQV, 2, NCV, M, G, V>;                                 \
+      set_smem(k, smq);                                                                 \
+      k<<<(unsigned)R.n, 256, smq, st>>>(p->d_units, tiles);                            \
+      launched = true;                                                                  \
+    }                                                                                   \
   }
 #define MRSIM_AQ(NQV, NCV, M, G) MRSIM_AQV(NQV, NCV, M, G, false)
 #define MRSIM_AQC(NCV, M, G) MRSIM_AQ(1, NCV, M, G) MRSIM_AQ(2, NCV, M, G) MRSIM_AQ(4, NCV, M, G) MRSIM_AQ(8, NCV, M, G)

@@ -139,6 +139,14 @@ namespace mrsim {
 void* workspace(mrsim_context* ctx, int slot, size_t bytes);
 
 // ---- the forward/adjoint plan (epi_kernels.cu) -----------------------------------------------
+// The plan's tunables (0: the built-in choice), the space the autotuner searches: coil classes
+// off (per-coil y- and x-stages), the x-stage as the DFT GEMM instead of the FFTs, and the rows
+// per thread of the fixed-coil y-adjoint (2 or 4).
+struct EpiPlanOptions {
+  int no_classes = 0;
+  int dft_x = 0;
+  int adj_rows = 0;
+};
 // Device-resident unit descriptors and tile lists, built once; executing a plan only launches
 // kernels on a stream (no host copies, no synchronisation), so it can be captured in a graph.
 // The caller zeroes the k-space outputs once: un-acquired rows are never written.
@@ -178,10 +186,15 @@ struct EpiPlan {
   int adjq[4] = {0, 0, 0, 0};
   // first tile of each unit in each list (n_units + 1 entries; empty: launch whole lists only)
   std::vector<int> y_start[2], a_start[4], f_start, g_start[2];
+  // rows per thread of the fixed-coil y-adjoint, per pass
+  int adj_ty[4] = {0, 0, 0, 0};
+  EpiPlanOptions opt;
+  std::vector<StaticDesc> host_statics;
   std::vector<void*> allocs;
   ~EpiPlan();
 };
-EpiPlan* epi_plan_create(const UnitDesc* units, int n, const StaticDesc* statics, int ns);
+EpiPlan* epi_plan_create(const UnitDesc* units, int n, const StaticDesc* statics, int ns,
+                         const EpiPlanOptions* opt = nullptr);
 // The x-stage tiles of one unit (dir 0 forward, 1 adjoint); `lines` is a host copy of its table.
 void append_xtiles(std::vector<XTile>& out, const UnitDesc& u, int unit_index, const LineRec* lines, int dir);
 // Each launcher covers units [u0, u1) of the plan (u1 < 0: every unit).
