@@ -308,6 +308,17 @@ def scale_measurements(args, ctx, stream):
                                "seconds_per_volume": dt, "value": n_samp / dt, "unit": "samples/s",
                                "timing": "host-buffer call (mrsim_spiral_samples_3d) by wall clock, host<->device "
                                          "copies included"}
+    # the plain single-shot case on the device (launch-bound: one unit)
+    c1, acq1 = c1_inputs()
+    op = EpiOperator(c1["sim_dims"], c1["acq_dims"], 1, c1["t2"], c1["fmap"], acq1, images=c1["images"],
+                     t_inhom=c1["t_inhom"], phase=PhaseModel.none(), seed=42, grads=0, ctx=ctx)
+    tot, st = time_stages(op, stream, ctx, 20, 3)
+    smp1 = op.samples
+    op.close()
+    out["plain_single_shot"] = {"config": "scan 64x64 on 128x128, 1 slice, 1 coil, 1 compartment, TE 30 ms",
+                                "samples_per_step": smp1, "ms_per_step": tot / 20,
+                                "value": smp1 / (tot / 20 * 1e-3), "unit": "samples/s",
+                                "note": "one unit: five launches of a few microseconds each"}
     return out
 
 
@@ -460,6 +471,7 @@ def run_ours(args, rank, world, local_rank):
         res["gpu_launches"] += 3 * 6 * args.steps  # three more operators, up to 6 launches a step
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res["cpu_baseline"] = cpu_baseline(acq, inp, sample_volumes=args.cpu_volumes, sample_slices=args.cpu_slices)
+        res["cpu_baseline"].update(cpu_baseline_extra(acq, inp))
     return res, op, ctx
 
 
@@ -490,6 +502,57 @@ def cpu_baseline(acq, inp, sample_volumes=1, sample_slices=8, threads=None):
     return {"value": samples / dt, "unit": "samples/s", "cores": threads, "kind": "port",
             "sample": f"{sample_volumes} volume x {sample_slices} slices x {len(WORKLOAD['echoes'])} echoes x "
                       f"{acq.n_coils} coils ({samples} samples), forward + adjoint, FP64, {dt:.2f} s"}
+
+
+def c1_inputs():
+    """The plain single-shot case: scan 64x64 on 128x128, one slice, one coil, one compartment; a
+    seeded 10-ellipse phantom (magnitudes U(0.2, 1), zero phase), T2 80 / T2' 40 ms, spin echo at
+    TE 30 ms, 0.5 ms lines, ky order; a fieldmap of 3 Gaussian blobs (U(-60, 60) Hz, sigma
+    U(8, 20) px)."""
+    from mrsim_acq_b200.api import T2, Acquisition
+    n, o = 64, 2
+    s = n * o
+    rng = np.random.default_rng(1)
+    ys, xs = np.meshgrid((np.arange(s) + 0.5) / s, (np.arange(s) + 0.5) / s, indexing="ij")
+    img = np.zeros((s, s), np.float32)
+    for _ in range(10):
+        cx, cy, a, b, th, mag = (rng.uniform(0.3, 0.7), rng.uniform(0.3, 0.7), rng.uniform(0.05, 0.25),
+                                 rng.uniform(0.05, 0.25), rng.uniform(0, np.pi), rng.uniform(0.2, 1.0))
+        c, sn = np.cos(th), np.sin(th)
+        u = (c * (xs - cx) + sn * (ys - cy)) / a
+        v = (-sn * (xs - cx) + c * (ys - cy)) / b
+        img += np.float32(mag) * (u * u + v * v <= 1.0)
+    rng2 = np.random.default_rng(2)
+    fmap = np.zeros((s, s), np.float32)
+    for _ in range(3):
+        amp, sig = rng2.uniform(-60, 60), rng2.uniform(8, 20) * o
+        cx, cy = rng2.uniform(0.3, 0.7) * s, rng2.uniform(0.3, 0.7) * s
+        fmap += (amp * np.exp(-((xs * s - cx) ** 2 + (ys * s - cy) ** 2) / (2 * sig * sig))).astype(np.float32)
+    acq = Acquisition(t_line=0.5, t_echo=30.0, t_inhom=40.0)
+    return dict(sim_dims=(s, s, 1), acq_dims=(n, n, 1), n_volumes=1, images=[img.reshape(-1)], t2=[T2.uniform(80.0)],
+                t_inhom=[T2.uniform(40.0)], fmap=fmap.reshape(-1)), acq
+
+
+def cpu_baseline_extra(acq, inp):
+    """The exact FP64 port on one host thread (a small sample of the benchmark series), and the
+    plain single-shot case (forward + adjoint) on one thread."""
+    from oracle import oracle
+    from mrsim_acq_b200.api import PhaseModel
+    one = cpu_baseline(acq, inp, sample_volumes=1, sample_slices=4, threads=1)
+    c1, acq1 = c1_inputs()
+    kw = dict(t_inhom=c1["t_inhom"], phase=PhaseModel.none(), seed=42)
+    t0 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        k = oracle.series_forward(c1["sim_dims"], c1["acq_dims"], 1, c1["images"], c1["t2"], c1["fmap"], acq1,
+                                  threads=1, **kw)
+        oracle.series_adjoint(c1["sim_dims"], c1["acq_dims"], 1, c1["images"], c1["t2"], c1["fmap"], acq1, k,
+                              threads=1, **kw)
+    dt = (time.perf_counter() - t0) / reps
+    return {"single_thread": {"value": one["value"], "unit": "samples/s", "cores": 1, "sample": one["sample"]},
+            "plain_single_shot": {"value": 4096 / dt, "unit": "samples/s", "cores": 1,
+                                  "sample": f"scan 64x64 on 128x128, 1 slice, 1 coil, 1 compartment, forward + "
+                                            f"adjoint, FP64, {dt * 1e3:.1f} ms"}}
 
 
 def run_reference(args):
