@@ -481,6 +481,81 @@ int mrsim_write_complex_4d(const char* out_prefix, const char* suffix, const int
                            const float* mag, const float* phase, const double* v2w,
                            const mrsim_sidecar_info* info);
 
+/* ---- spin history of slice-selective excitations under head motion (spin_history.rs) -------- */
+/* The longitudinal magnetisation of every tracked source voxel (class != MRSIM_SPIN_NO_CLASS), as
+ * at most MRSIM_SPIN_MAX_PIECES pieces of its z extent (mz just after each piece's last
+ * excitation and that time), stepped through the excitations of a series on the device.  Per
+ * excitation and excited slice: num[class][cell] = sum l V w (Mz(t) - mz_ref(T1)) and
+ * den[class][cell] = sum l V w mz_ref(T1) over the pieces inside the slice's slab, at the slab
+ * cell nearest each voxel's moved centre (`SpinHistory`, spin_history.rs:171-452).  Each sum runs
+ * in FP64 in the reference's order (source planes, then voxels, then pieces) and is rounded to
+ * f32 once, as the reference does. */
+#define MRSIM_SPIN_NO_CLASS 255
+#define MRSIM_SPIN_MAX_PIECES 8
+enum { MRSIM_PULSE_INVERSION = 0, MRSIM_PULSE_SATURATION = 1 };
+/* `Pulse` (spin_history.rs:63-69): Inversion scales Mz by 1 - 2 epsilon; Saturation sets 0. */
+typedef struct mrsim_pulse {
+  int32_t kind;
+  double t;       /* s, on the series clock */
+  double epsilon; /* inversion only */
+} mrsim_pulse;
+/* The reference magnetisation of an excitation, `mz_ref(T1)` (the closure `excite` takes,
+ * spin_history.rs:311), as one of:
+ *   NONE      the excitation reads no terms (`prime`, spin_history.rs:303-307);
+ *   RECOVERY  1 - (1 - a) exp(-b / T1)   (a = 0: saturation recovery over b seconds);
+ *   CONSTANT  a where T1 > 0, else b;
+ *   REPLAY    Mz at the excitation's time from a just after time b, through the series' pulses
+ *             (0 where T1 <= 0): the static head's closed form;
+ *   VALUES    values[i] for the i-th tracked voxel in source order (host pointer). */
+enum { MRSIM_MZREF_NONE = 0, MRSIM_MZREF_RECOVERY = 1, MRSIM_MZREF_CONSTANT = 2, MRSIM_MZREF_REPLAY = 3,
+       MRSIM_MZREF_VALUES = 4 };
+typedef struct mrsim_mz_reference {
+  int32_t kind;
+  double a, b;
+  const double* values;
+} mrsim_mz_reference;
+/* One shot: the excitation's time (s), the head's world-space transform (p' = m p, row-major
+ * 4x4), the slab indices it excites, its reference and, optionally, a weight per source voxel
+ * (x + nx*(y + ny*z), host pointer) that replaces the source weight for this shot only. */
+typedef struct mrsim_spin_shot {
+  double t;
+  double transform[16];
+  const int64_t* slices;
+  int64_t n_slices;
+  mrsim_mz_reference ref;
+  const float* weight;
+} mrsim_spin_shot;
+typedef struct mrsim_spin_history mrsim_spin_history;
+/* `SpinHistory::new` spin_history.rs:254-289: the source grid (dims, voxel-to-world v2w,
+ * per-voxel T1 in s, weight and class), the slab grid whose z index is the slice, and the
+ * series' pulses in any order.  Every voxel starts fully relaxed. */
+int mrsim_spin_history_create(mrsim_context* ctx, const int64_t* src_dims, const double* src_v2w, const float* t1,
+                              const float* weight, const uint8_t* cls, int64_t n_classes, const int64_t* slab_dims,
+                              const double* slab_v2w, const mrsim_pulse* pulses, int64_t n_pulses,
+                              mrsim_spin_history** out);
+void mrsim_spin_history_destroy(mrsim_spin_history* h);
+/* The number of tracked voxels (the length of a VALUES reference). */
+int mrsim_spin_history_n_tracked(mrsim_spin_history* h, int64_t* n);
+/* `SpinHistory::prime` spin_history.rs:303-307: shot i excites slices[offsets[i]..offsets[i+1]]
+ * at times[i], every shot at `transform`, reading no terms. */
+int mrsim_spin_history_prime(mrsim_spin_history* h, const double* times, const int64_t* slices,
+                             const int64_t* offsets, int64_t n_shots, const double* transform);
+/* The number of floats the terms of `shots` take: sum over the shots that read terms of
+ * n_slices * 2 * n_classes * slab_nx * slab_ny. */
+int mrsim_spin_history_terms_size(mrsim_spin_history* h, const mrsim_spin_shot* shots, int64_t n_shots,
+                                  int64_t* n_floats);
+/* `SpinHistory::excite` spin_history.rs:311-315, for n_shots shots in order: the terms of each
+ * shot that reads them, packed shot after shot as [slice in shot][num, den][class][x + slab_nx*y]
+ * (f32), into the host buffer `terms`.  Returns when done. */
+int mrsim_spin_history_excite(mrsim_spin_history* h, const mrsim_spin_shot* shots, int64_t n_shots, float* terms);
+/* No reference counterpart: the same with `terms` a device buffer, queued on the context's
+ * stream; the call returns once the launches are queued (the host inputs have been copied). */
+int mrsim_spin_history_excite_device(mrsim_spin_history* h, const mrsim_spin_shot* shots, int64_t n_shots,
+                                     float* terms);
+/* `SpinHistory::merges` spin_history.rs:296-301 (synchronises the stream; reports a kernel's
+ * error status). */
+int mrsim_spin_history_merges(mrsim_spin_history* h, uint64_t* merges);
+
 /* ---- the 3D echo trains (kspace3d.rs, readout.rs:75-322) ----------------------------------- */
 enum { MRSIM_KZ_CENTRIC = 0, MRSIM_KZ_LINEAR = 1 };                            /* readout.rs:75 */
 

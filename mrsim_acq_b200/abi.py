@@ -217,6 +217,19 @@ class SpiralSegmentationRow_(C.Structure):
                 ("bound", C.c_double)]
 
 
+class Pulse_(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("t", C.c_double), ("epsilon", C.c_double)]
+
+
+class MzReference_(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("a", C.c_double), ("b", C.c_double), ("values", c_f64p)]
+
+
+class SpinShot_(C.Structure):
+    _fields_ = [("t", C.c_double), ("transform", C.c_double * 16), ("slices", C.POINTER(C.c_int64)),
+                ("n_slices", C.c_int64), ("ref", MzReference_), ("weight", c_f32p)]
+
+
 class LibraryMissing(RuntimeError):
     pass
 
@@ -293,6 +306,17 @@ def _declare(lib):
         "mrsim_write_nifti_4d": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), C.c_int64, c_f32p, c_f64p, C.c_double]),
         "mrsim_write_nifti_3d": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64), c_f32p, c_f64p]),
         "mrsim_hires_grid": (C.c_int, [c_f64p, C.POINTER(C.c_int64), C.c_int64, c_f64p, C.POINTER(C.c_int64)]),
+        "mrsim_spin_history_create": (C.c_int, [P, C.POINTER(C.c_int64), c_f64p, c_f32p, c_f32p,
+                                                C.POINTER(C.c_uint8), C.c_int64, C.POINTER(C.c_int64), c_f64p,
+                                                C.POINTER(Pulse_), C.c_int64, C.POINTER(P)]),
+        "mrsim_spin_history_destroy": (None, [P]),
+        "mrsim_spin_history_n_tracked": (C.c_int, [P, C.POINTER(C.c_int64)]),
+        "mrsim_spin_history_prime": (C.c_int, [P, c_f64p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int64,
+                                               c_f64p]),
+        "mrsim_spin_history_terms_size": (C.c_int, [P, C.POINTER(SpinShot_), C.c_int64, C.POINTER(C.c_int64)]),
+        "mrsim_spin_history_excite": (C.c_int, [P, C.POINTER(SpinShot_), C.c_int64, c_f32p]),
+        "mrsim_spin_history_excite_device": (C.c_int, [P, C.POINTER(SpinShot_), C.c_int64, P]),
+        "mrsim_spin_history_merges": (C.c_int, [P, C.POINTER(C.c_uint64)]),
         "mrsim_write_complex_4d": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_int64), C.c_int64, c_f32p, c_f32p,
                                              c_f64p, C.POINTER(SidecarInfo_)]),
         "mrsim_epi_operator_apply_host_compact": (C.c_int, [P, C.POINTER(c_f32p), c_f32p, c_f32p, c_f32p, c_f32p]),

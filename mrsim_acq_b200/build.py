@@ -27,8 +27,14 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+# Files whose FP64 arithmetic must round as the reference's does: no multiply-add contraction in
+# device or host code.
+NO_CONTRACT = {"spin_history.cu"}
+
+
 def _flags(src: pathlib.Path) -> list[str]:
-    common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+    extra = ["-fmad=false", "-Xcompiler", "-ffp-contract=off"] if src.name in NO_CONTRACT else []
+    common = extra + ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
               "-I", str(HERE.parent / "include")]
     if src.suffix == ".cu":
         return common + ARCH + ["-lineinfo", "-Xptxas", "-O3"]

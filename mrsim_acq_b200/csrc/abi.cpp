@@ -20,6 +20,7 @@
 #include "spiral.h"
 #include "spiral_host.h"
 #include "spiral_recon.h"
+#include "spin_history.h"
 
 namespace {
 thread_local std::string g_last_error;
@@ -75,6 +76,10 @@ struct mrsim_epi_operator {
 
 struct mrsim_spiral_recon {
   mrsim::SpiralRecon* impl;
+};
+
+struct mrsim_spin_history {
+  mrsim::SpinHistoryDev* impl;
 };
 
 namespace {
@@ -1276,6 +1281,116 @@ int mrsim_spiral_segmentation(const mrsim_acquisition_3d_input* in, const mrsim_
     if (capacity < (int64_t)v.size()) mrsim::fail("row capacity below the segmentations");
     for (size_t i = 0; i < v.size(); ++i)
       rows[i] = mrsim_spiral_segmentation_row{v[i].z, v[i].voxel, v[i].l, v[i].m, v[i].b_sum, v[i].bound};
+  });
+}
+
+// ---- spin history (spin_history.rs) --------------------------------------------------------------
+int mrsim_spin_history_create(mrsim_context* ctx, const int64_t* src_dims, const double* src_v2w, const float* t1,
+                              const float* weight, const uint8_t* cls, int64_t n_classes, const int64_t* slab_dims,
+                              const double* slab_v2w, const mrsim_pulse* pulses, int64_t n_pulses,
+                              mrsim_spin_history** out) {
+  return on_ctx(ctx, [&] {
+    need(out, "out");
+    *out = nullptr;
+    need(src_dims, "src_dims");
+    need(src_v2w, "src_v2w");
+    need(t1, "t1");
+    need(weight, "weight");
+    need(cls, "cls");
+    need(slab_dims, "slab_dims");
+    need(slab_v2w, "slab_v2w");
+    if (n_pulses > 0) need(pulses, "pulses");
+    std::unique_ptr<mrsim::SpinHistoryDev> h(mrsim::spin_history_create(
+        ctx, src_dims, src_v2w, t1, weight, cls, n_classes, slab_dims, slab_v2w, pulses, n_pulses));
+    *out = new mrsim_spin_history{h.release()};
+  });
+}
+
+void mrsim_spin_history_destroy(mrsim_spin_history* h) {
+  if (!h) return;
+  {
+    std::lock_guard<std::mutex> lk(h->impl->ctx->mu);
+    cudaSetDevice(h->impl->ctx->device);
+    cudaStreamSynchronize(h->impl->ctx->stream);  // the batch buffers may still be read
+    delete h->impl;
+  }
+  delete h;
+}
+
+int mrsim_spin_history_n_tracked(mrsim_spin_history* h, int64_t* n) {
+  return guarded([&] {
+    need(h, "spin history");
+    need(n, "n");
+    *n = h->impl->nt;
+  });
+}
+
+int mrsim_spin_history_prime(mrsim_spin_history* h, const double* times, const int64_t* slices,
+                             const int64_t* offsets, int64_t n_shots, const double* transform) {
+  if (!h) return guarded([] { need(nullptr, "spin history"); });
+  return on_ctx(h->impl->ctx, [&] {
+    if (n_shots <= 0) return;
+    need(times, "times");
+    need(offsets, "offsets");
+    need(transform, "transform");
+    std::vector<mrsim_spin_shot> shots((size_t)n_shots);
+    for (int64_t s = 0; s < n_shots; ++s) {
+      if (offsets[s + 1] < offsets[s]) mrsim::fail("offsets must not decrease");
+      if (offsets[s + 1] > offsets[s]) need(slices, "slices");
+      mrsim_spin_shot& S = shots[(size_t)s];
+      S = mrsim_spin_shot{};
+      S.t = times[s];
+      std::memcpy(S.transform, transform, sizeof S.transform);
+      S.slices = slices ? slices + offsets[s] : nullptr;
+      S.n_slices = offsets[s + 1] - offsets[s];
+      S.ref.kind = MRSIM_MZREF_NONE;
+    }
+    mrsim::spin_history_run(*h->impl, shots.data(), n_shots, nullptr);
+    MRSIM_CUDA(cudaStreamSynchronize(h->impl->ctx->stream));
+  });
+}
+
+int mrsim_spin_history_terms_size(mrsim_spin_history* h, const mrsim_spin_shot* shots, int64_t n_shots,
+                                  int64_t* n_floats) {
+  return guarded([&] {
+    need(h, "spin history");
+    need(n_floats, "n_floats");
+    if (n_shots > 0) need(shots, "shots");
+    *n_floats = mrsim::spin_history_terms_size(*h->impl, shots, n_shots);
+  });
+}
+
+int mrsim_spin_history_excite(mrsim_spin_history* h, const mrsim_spin_shot* shots, int64_t n_shots, float* terms) {
+  if (!h) return guarded([] { need(nullptr, "spin history"); });
+  return on_ctx(h->impl->ctx, [&] {
+    if (n_shots <= 0) return;
+    need(shots, "shots");
+    const int64_t nf = mrsim::spin_history_terms_size(*h->impl, shots, n_shots);
+    if (nf > 0) need(terms, "terms");
+    float* d = (float*)h->impl->out_b.get((size_t)std::max<int64_t>(nf, 1) * 4);
+    mrsim::spin_history_run(*h->impl, shots, n_shots, d);
+    cudaStream_t st = h->impl->ctx->stream;
+    if (nf > 0) MRSIM_CUDA(cudaMemcpyAsync(terms, d, (size_t)nf * 4, cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+    (void)mrsim::spin_history_merges(*h->impl);  // reports a kernel's error status
+  });
+}
+
+int mrsim_spin_history_excite_device(mrsim_spin_history* h, const mrsim_spin_shot* shots, int64_t n_shots,
+                                     float* terms) {
+  if (!h) return guarded([] { need(nullptr, "spin history"); });
+  return on_ctx(h->impl->ctx, [&] {
+    if (n_shots <= 0) return;
+    need(shots, "shots");
+    mrsim::spin_history_run(*h->impl, shots, n_shots, terms);
+  });
+}
+
+int mrsim_spin_history_merges(mrsim_spin_history* h, uint64_t* merges) {
+  if (!h) return guarded([] { need(nullptr, "spin history"); });
+  return on_ctx(h->impl->ctx, [&] {
+    need(merges, "merges");
+    *merges = mrsim::spin_history_merges(*h->impl);
   });
 }
 

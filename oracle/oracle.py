@@ -654,3 +654,144 @@ def apply_multiband_motion(images, dims, n_volumes, v2w, mb, interleaved, law_ki
                                                 jm.ctypes.data_as(abi.c_f64p), jd.ctypes.data_as(abi.c_f64p), n, szp,
                                                 nz_full, ovp, oshp, oa.ctypes.data_as(abi.c_f32p), ndp)
     return [(int(ov[i]), int(osh[i]), float(oa[i])) for i in range(int(nd[0]))]
+
+
+# ---- spin history (spin_history.rs) -----------------------------------------------------------
+class OraclePieces(C.Structure):
+    """One voxel's pieces (`Pieces`, spin_history.rs:87-92), for the reference's piece tests."""
+    _fields_ = [("n", C.c_int32), ("pad", C.c_int32), ("start", C.c_float * 8), ("mz", C.c_float * 8),
+                ("t", C.c_double * 8)]
+
+
+def _spin_lib():
+    L = lib()
+    if not getattr(L, "_spin_typed", False):
+        P = C.POINTER
+        pp = P(OraclePieces)
+        pul = P(abi.Pulse_)
+        L.oracle_pieces_relaxed.argtypes = [pp]
+        L.oracle_pieces_split.argtypes = [pp, C.c_float]
+        L.oracle_pieces_has_edge.argtypes = [pp, C.c_float]
+        L.oracle_pieces_coalesce.argtypes = [pp]
+        L.oracle_pieces_cut.restype = C.c_uint64
+        L.oracle_pieces_cut.argtypes = [pp, C.c_float, C.c_float, C.c_double, pul, C.c_int64]
+        L.oracle_pieces_merge_closest.argtypes = [pp, C.c_double, pul, C.c_int64, abi.c_f32p, C.c_int32]
+        L.oracle_spin_replay.restype = C.c_double
+        L.oracle_spin_replay.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, pul, C.c_int64]
+        L.oracle_spin_new.restype = C.c_void_p
+        L.oracle_spin_new.argtypes = [P(C.c_int64), abi.c_f64p, abi.c_f32p, abi.c_f32p, P(C.c_uint8), C.c_int64,
+                                      P(C.c_int64), abi.c_f64p, pul, C.c_int64, C.c_char_p, C.c_int64]
+        L.oracle_spin_step.argtypes = [C.c_void_p, P(abi.SpinShot_), abi.c_f32p, C.c_char_p, C.c_int64]
+        L.oracle_spin_merges.restype = C.c_uint64
+        L.oracle_spin_merges.argtypes = [C.c_void_p]
+        L.oracle_spin_n_tracked.restype = C.c_int64
+        L.oracle_spin_n_tracked.argtypes = [C.c_void_p]
+        L.oracle_spin_free.argtypes = [C.c_void_p]
+        L._spin_typed = True
+    return L
+
+
+class Pieces:
+    """The reference's `Pieces` operations on one voxel (f32 edges and Mz, f64 times)."""
+
+    def __init__(self):
+        self.c = OraclePieces()
+        _spin_lib().oracle_pieces_relaxed(C.byref(self.c))
+
+    n = property(lambda self: self.c.n)
+
+    def split(self, u: float) -> bool:
+        return bool(_spin_lib().oracle_pieces_split(C.byref(self.c), u))
+
+    def has_edge(self, u: float) -> bool:
+        return bool(_spin_lib().oracle_pieces_has_edge(C.byref(self.c), u))
+
+    def coalesce(self) -> None:
+        _spin_lib().oracle_pieces_coalesce(C.byref(self.c))
+
+    def cut(self, u0: float, u1: float, t1: float, pulses=()) -> int:
+        from mrsim_acq_b200.spin_history import pulses_c
+        arr, n = pulses_c(list(pulses))
+        return int(_spin_lib().oracle_pieces_cut(C.byref(self.c), u0, u1, t1, arr, n))
+
+    def merge_closest(self, t1: float, pulses=(), protect=()) -> None:
+        from mrsim_acq_b200.spin_history import pulses_c
+        arr, n = pulses_c(list(pulses))
+        pr = np.ascontiguousarray(list(protect) or [0.0], np.float32)
+        _spin_lib().oracle_pieces_merge_closest(C.byref(self.c), t1, arr, n, pr.ctypes.data_as(abi.c_f32p),
+                                                len(protect))
+
+
+def spin_replay(mz: float, t_from: float, t_to: float, t1: float, pulses=()) -> float:
+    from mrsim_acq_b200.spin_history import pulses_c
+    arr, n = pulses_c(list(pulses))
+    return float(_spin_lib().oracle_spin_replay(mz, t_from, t_to, t1, arr, n))
+
+
+class SpinHistory:
+    """The FP64 restatement of `SpinHistory` with the library's Python interface (`prime`,
+    `excite`, `excite_many`, `merges`, `n_tracked`)."""
+
+    def __init__(self, source, slabs, pulses=()):
+        from mrsim_acq_b200.spin_history import NO_CLASS, _RefValues, pulses_c
+        L = _spin_lib()
+        dims = np.ascontiguousarray(source.dims, np.int64)
+        t1 = np.ascontiguousarray(source.t1, np.float32).ravel()
+        w = np.ascontiguousarray(source.weight, np.float32).ravel()
+        cls = np.ascontiguousarray(source.cls, np.uint8).ravel()
+        sdims = np.ascontiguousarray(slabs.dims, np.int64)
+        v2w = np.ascontiguousarray(source.v2w, np.float64).reshape(16)
+        sv2w = np.ascontiguousarray(slabs.v2w, np.float64).reshape(16)
+        parr, npul = pulses_c(list(pulses))
+        err = C.create_string_buffer(512)
+        P = C.POINTER(C.c_int64)
+        self._h = None
+        h = L.oracle_spin_new(dims.ctypes.data_as(P), v2w.ctypes.data_as(abi.c_f64p), t1.ctypes.data_as(abi.c_f32p),
+                              w.ctypes.data_as(abi.c_f32p), cls.ctypes.data_as(C.POINTER(C.c_uint8)),
+                              int(source.n_classes), sdims.ctypes.data_as(P), sv2w.ctypes.data_as(abi.c_f64p), parr,
+                              npul, err, 512)
+        if not h:
+            raise RuntimeError(err.value.decode())
+        self._h = h
+        self.n_classes = int(source.n_classes)
+        self.cells = int(sdims[0] * sdims[1])
+        self._ref_values = _RefValues(t1[cls != NO_CLASS].astype(np.float64))
+
+    @property
+    def n_tracked(self) -> int:
+        return int(_spin_lib().oracle_spin_n_tracked(self._h))
+
+    def excite_many(self, shots) -> list:
+        from mrsim_acq_b200.spin_history import shots_c, unpack_terms
+        L = _spin_lib()
+        keep: list = []
+        arr = shots_c(shots, self._ref_values, keep)
+        outs = []
+        err = C.create_string_buffer(512)
+        for i, s in enumerate(shots):
+            n = 0 if s.mz_ref is None else len(s.slices) * 2 * self.n_classes * self.cells
+            buf = np.zeros(max(n, 1), np.float32)
+            if L.oracle_spin_step(self._h, C.byref(arr[i]), buf.ctypes.data_as(abi.c_f32p), err, 512) != 0:
+                raise RuntimeError(err.value.decode())
+            outs.append(buf[:n])
+        flat = np.concatenate(outs) if outs else np.zeros(0, np.float32)
+        return unpack_terms(shots, flat, self.n_classes, self.cells)
+
+    def excite(self, t, transform, slices, mz_ref, weight=None) -> list:
+        from mrsim_acq_b200.spin_history import Shot
+        return self.excite_many([Shot(t, transform, slices, mz_ref, weight)])[0]
+
+    def prime(self, shots, transform) -> None:
+        from mrsim_acq_b200.spin_history import Shot
+        self.excite_many([Shot(t, transform, sl, None) for t, sl in shots])
+
+    def merges(self) -> int:
+        return int(_spin_lib().oracle_spin_merges(self._h))
+
+    def __del__(self):
+        try:
+            if self._h:
+                _spin_lib().oracle_spin_free(self._h)
+                self._h = None
+        except Exception:
+            pass
