@@ -322,6 +322,89 @@ def scale_measurements(args, ctx, stream):
     return out
 
 
+def spin_history_series():
+    """The spin-history workload at the reference's motivating size: a 197x233x100 source of 1 mm
+    voxels (T1 1.33 s, every third voxel tracked), slabs of 128x136 cells x 20 slices of 5 mm, 40
+    volumes of 20 sequential single-slice shots (TR 4.6 s, 40 ms apart) under a slow drift of
+    0.5 mm through-plane with a (0.5, 0, 0.3) degree tilt, referenced to the 4.6 s saturation
+    recovery."""
+    from mrsim_acq_b200.motion import Pose
+    from mrsim_acq_b200.spin_history import Recovery, Shot, Slabs, Source
+    nx, ny, nz = 197, 233, 100
+    nvox = nx * ny * nz
+    cls = np.where(np.arange(nvox) % 3 == 0, 0, 255).astype(np.uint8)
+    src = Source((nx, ny, nz), np.eye(4), np.full(nvox, 1.33, np.float32), np.ones(nvox, np.float32), cls, 1)
+    s = np.eye(4)
+    s[0, 0], s[1, 1], s[2, 2], s[2, 3] = 197.0 / 128.0, 233.0 / 136.0, 5.0, 2.0
+    slabs = Slabs((128, 136, 20), s)
+    center = (98.0, 116.0, 50.0)
+
+    def volume(v):
+        return [Shot(v * 4.6 + 3.6 + 0.04 * k,
+                     Pose((0.5, 0.0, 0.3), (0.0, 0.0, 0.5 * (v + k / 20.0) / 40.0)).to_matrix(center), [k],
+                     Recovery(4.6)) for k in range(20)]
+    return src, slabs, volume
+
+
+def spin_history_measurement(ctx, stream, cpu=True):
+    """The spin history (800 excitations, one batch of 20 shots per volume) on the device, CUDA
+    events on the context stream around the whole series; beside it the FP64 oracle on one host
+    thread over the same series (the CPU baseline) and the device's agreement with it."""
+    import torch
+    from mrsim_acq_b200.spin_history import SpinHistory, unpack_terms
+    src, slabs, volume = spin_history_series()
+    n_vol = 40
+    vols = [volume(v) for v in range(n_vol)]
+    t0 = time.perf_counter()
+    h = SpinHistory(src, slabs, ctx=ctx)
+    build_s = time.perf_counter() - t0
+    per = h.terms_size(vols[0])
+    out = torch.zeros(per * n_vol, dtype=torch.float32, device="cuda")
+    warm = SpinHistory(src, slabs, ctx=ctx)  # kernels loaded, buffers grown
+    warm.excite_device(vols[0], out.data_ptr())
+    ctx.synchronize()
+    warm.close()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(stream)
+    for v in range(n_vol):
+        h.excite_device(vols[v], out.data_ptr() + 4 * per * v)
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - w0
+    dev_ms = e0.elapsed_time(e1)
+    merges = h.merges()
+    res = {"config": "source 197x233x100 (1 in 3 tracked), slabs 128x136x20, 40 volumes x 20 single-slice "
+                     "shots, drift 0.5 mm + tilt, reference 1 - e^{-4.6/T1}",
+           "excitations": 20 * n_vol, "tracked_voxels": h.n_tracked, "device_ms": dev_ms, "wall_ms": wall * 1e3,
+           "value": 20 * n_vol / (dev_ms * 1e-3), "unit": "excitations/s", "merges": merges,
+           "build_s": build_s, "launches": 2 * n_vol,
+           "timing": "CUDA events on the context stream around the 40 batch calls (host table preparation "
+                     "between launches included)"}
+    if cpu:
+        from oracle import oracle
+        n_cpu = n_vol
+        t0 = time.perf_counter()
+        o = oracle.SpinHistory(src, slabs)
+        o_build = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ora = [o.excite_many(vols[v]) for v in range(n_cpu)]
+        cpu_s = time.perf_counter() - t0
+        dev = out[:per * n_cpu].cpu().numpy()
+        flat = np.concatenate([np.stack([t.num, t.den]).ravel() for vol in ora for terms in vol for t in terms])
+        scale = float(np.abs(flat).max())
+        res["cpu_baseline"] = {"value": 20 * n_cpu / cpu_s, "unit": "excitations/s", "cores": 1, "kind": "port",
+                               "sample": f"the same {n_cpu} volumes ({20 * n_cpu} excitations), FP64 oracle, "
+                                         f"{cpu_s:.2f} s (+ {o_build:.2f} s to build)"}
+        res["merges_oracle"] = o.merges()
+        res["parity"] = {"bit_identical": int(np.count_nonzero(dev == flat)), "elements": int(flat.size),
+                                       "max_abs_err_over_max": float(np.abs(dev.astype(np.float64) - flat).max()
+                                                                     / max(scale, 1e-30))}
+    h.close()
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from mrsim_acq_b200 import api
@@ -466,6 +549,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if not args.no_scale and world == 1:
         res["scale"] = scale_measurements(args, ctx, stream)
+        res["spin_history"] = spin_history_measurement(ctx, stream, cpu=not args.no_cpu_baseline)
+        res["gpu_launches_spin_history"] = res["spin_history"]["launches"]
     if not args.no_segmented and world == 1:
         res["segmented"] = segmented_comparison(args, inp, acq, ctx, stream, samples)
         res["gpu_launches"] += 3 * 6 * args.steps  # three more operators, up to 6 launches a step

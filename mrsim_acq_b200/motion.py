@@ -28,6 +28,20 @@ class Pose:
     def as_array(self) -> np.ndarray:
         return np.array(list(self.rot_deg) + list(self.trans_mm), np.float64)
 
+    def to_matrix(self, center) -> np.ndarray:
+        """The world-space 4x4 transform of the pose about `center` (`Pose::to_matrix`
+        motion.rs:55-68): R = Rz Ry Rx, translation c - R c + t, so `center` maps to center + t."""
+        rx, ry, rz = (np.deg2rad(a) for a in self.rot_deg)
+        X = np.array([[1.0, 0.0, 0.0], [0.0, np.cos(rx), -np.sin(rx)], [0.0, np.sin(rx), np.cos(rx)]])
+        Y = np.array([[np.cos(ry), 0.0, np.sin(ry)], [0.0, 1.0, 0.0], [-np.sin(ry), 0.0, np.cos(ry)]])
+        Z = np.array([[np.cos(rz), -np.sin(rz), 0.0], [np.sin(rz), np.cos(rz), 0.0], [0.0, 0.0, 1.0]])
+        R = Z @ (Y @ X)
+        c = np.asarray(center, np.float64)
+        m = np.eye(4)
+        m[:3, :3] = R
+        m[:3, 3] = c - R @ c + np.asarray(self.trans_mm, np.float64)
+        return m
+
 
 IDENTITY = Pose()
 
