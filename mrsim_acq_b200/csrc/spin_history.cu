@@ -7,15 +7,16 @@
 // the piece slots slot-major, so a warp of neighbouring voxels reads and writes each slot
 // coalesced.  The history of one voxel depends on nothing but its own pieces, so one thread owns
 // one voxel for a whole batch of shots: it loads the pieces once, steps them through every shot
-// of the batch in registers and local memory, and stores them once.
+// of the batch in registers and local memory (L1), and stores them once.
 //
 // Terms.  Per shot, every voxel of an active source plane writes one record: its slab cell (the
 // cell nearest its moved centre, or -1) and its contributions (slice in the shot, l V w (Mz -
 // mz_ref), l V w mz_ref), in the reference's order (slabs ascending, pieces ascending).  A
-// second kernel gathers each output (shot, slice, class, cell): it walks the source voxels whose
-// moved centre can round to the cell and whose z extent can reach the slab (the box of the
-// cell's preimage, z then y then x ascending, which is the reference's plane-then-voxel order)
-// and adds their matching contributions in FP64, then rounds once to f32.  The sums are the
+// second kernel gathers each output (shot, slice, class, cell), a tile of cells per block: the
+// block stages the cells' candidate source voxels in shared memory, and each thread walks the
+// voxels whose moved centre can round to its cell and whose z extent can reach the slab (the box
+// of the cell's preimage, z then y then x ascending, which is the reference's plane-then-voxel
+// order) and adds their matching contributions in FP64, then rounds once to f32.  The sums are the
 // reference's, added in the reference's order: no atomics, the same bits on every run.
 //
 // Arithmetic.  The file is compiled without multiply-add contraction (build.py), so every f64
@@ -49,6 +50,11 @@ GrowBuf::~GrowBuf() {
 
 SpinHistoryDev::~SpinHistoryDev() {
   for (void* p : allocs) cudaFree(p);
+  for (int b = 0; b < 2; ++b) {
+    if (pin_ev[b]) cudaEventSynchronize(pin_ev[b]);
+    if (pin[b]) cudaFreeHost(pin[b]);
+    if (pin_ev[b]) cudaEventDestroy(pin_ev[b]);
+  }
 }
 
 namespace {
@@ -196,7 +202,8 @@ struct StepArgs {
   double* ent_den;
   int16_t* ent_kk;
   long long n_rec;
-  int maxc, nk_max;
+  int maxc, nk_max, ncls;
+  const uint8_t* cls;
   long long nt;
   int nx, ny, snx, sny, snz;
   double len, half_len, vol;
@@ -308,7 +315,7 @@ __global__ void __launch_bounds__(128) spin_step_kernel(StepArgs A) {
       pc.coalesce();
     }
     if (reads) {
-      A.rec_cell[rec] = cell;
+      A.rec_cell[rec] = cell >= 0 ? cell * A.ncls + A.cls[i] : -1;
       A.rec_cnt[rec] = (uint8_t)cnt;
     }
   }
@@ -323,10 +330,14 @@ __global__ void __launch_bounds__(128) spin_step_kernel(StepArgs A) {
   if (merges) atomicAdd(A.merges, merges);
 }
 
+constexpr int kTileX = 16, kTileY = 8;  // slab cells of one gather block (one thread each)
+constexpr int kStageCap = 5632;          // source voxels a gather block stages (44 KiB of shared memory)
+constexpr int kStagePlanes = 256;        // source planes of a staged box whose tables the block keeps
+
 struct GatherArgs {
   const SpinShotDev* shots;
   const int* tabs;
-  const long long* ocum;  // n_read + 1 cumulative output counts
+  const long long* bcum;  // n_read + 1 cumulative block counts
   const int* oshot;       // the batch index of each reading shot
   int n_read;
   const int* idx;
@@ -338,73 +349,217 @@ struct GatherArgs {
   const double* ent_den;
   const int16_t* ent_kk;
   long long n_rec;
-  int nx, ny, nz, snx, ncls;
+  int nx, ny, nz, snx, sny, ncls, tiles_x, tiles;
   long long cells;
   double half_len;
   float* terms;
 };
 
-// One thread per output (shot, slice, class, cell): the contributions of the voxels whose moved
-// centre rounds to the cell, in source order, summed in FP64 and rounded once (the reference's
-// plane-ordered accumulation, spin_history.rs:407-419).
-__global__ void __launch_bounds__(256) spin_gather_kernel(GatherArgs A) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= A.ocum[A.n_read]) return;
-  int lo = 0, hi = A.n_read;  // the reading shot holding output g
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (A.ocum[mid] <= g)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  const SpinShotDev& S = A.shots[A.oshot[lo]];
-  const long long local = g - A.ocum[lo];
-  const int cell = (int)(local % A.cells);
-  const int c = (int)((local / A.cells) % A.ncls);
-  const int kk = (int)(local / (A.cells * A.ncls));
-  const int k = A.tabs[S.slices + kk];
-  const int cx = cell % A.snx, cy = cell / A.snx;
-  // the preimage box of the cell's column over the slab's reach, in source voxel coordinates (a
-  // singular transform has a NaN inverse: the box is then the whole grid)
+// The source voxel box (inclusive, clamped to the grid) holding every voxel whose moved centre can
+// round into slab cells [x0, x1] x [y0, y1] and whose z extent can reach slab k: the corners of
+// that slab box mapped by the shot's inverse (a singular transform has a NaN inverse, and the box
+// is then the whole grid).
+__device__ __forceinline__ void preimage_box(const SpinShotDev& S, int x0, int x1, int y0, int y1, int k,
+                                             double half_len, const int (&ext)[3], int (&b0)[3], int (&b1)[3]) {
   constexpr double d = 1e-3;
   double blo[3] = {INFINITY, INFINITY, INFINITY}, bhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
   for (int corner = 0; corner < 8; ++corner) {
-    const double sx = cx + ((corner & 1) ? 0.5 + d : -0.5 - d);
-    const double sy = cy + ((corner & 2) ? 0.5 + d : -0.5 - d);
-    const double sz = k + ((corner & 4) ? 0.5 + A.half_len + d : -0.5 - A.half_len - d);
+    const double sx = (corner & 1) ? x1 + 0.5 + d : x0 - 0.5 - d;
+    const double sy = (corner & 2) ? y1 + 0.5 + d : y0 - 0.5 - d;
+    const double sz = k + ((corner & 4) ? 0.5 + half_len + d : -0.5 - half_len - d);
+#pragma unroll
     for (int r = 0; r < 3; ++r) {
       const double v = S.minv[4 * r] * sx + S.minv[4 * r + 1] * sy + S.minv[4 * r + 2] * sz + S.minv[4 * r + 3];
       blo[r] = isnan(v) ? -INFINITY : fmin(blo[r], v);
       bhi[r] = isnan(v) ? INFINITY : fmax(bhi[r], v);
     }
   }
-  const int ext[3] = {A.nx, A.ny, A.nz};
-  int b0[3], b1[3];
+#pragma unroll
   for (int r = 0; r < 3; ++r) {
     b0[r] = (int)fmax(0.0, floor(blo[r]));
     b1[r] = (int)fmin((double)(ext[r] - 1), ceil(bhi[r]));
   }
-  double num = 0.0, den = 0.0;
-  for (int z = b0[2]; z <= b1[2]; ++z) {
-    const int base = A.tabs[S.plane_tab + z];
-    if (base < 0) continue;
-    const int pf = A.plane_first[z];
-    for (int y = b0[1]; y <= b1[1]; ++y)
-      for (int x = b0[0]; x <= b1[0]; ++x) {
-        const int t = A.idx[x + A.nx * (y + A.ny * z)];
-        if (t < 0) continue;
-        const long long rec = S.rec + base + (t - pf);
-        if (A.rec_cell[rec] != cell || A.cls[t] != c) continue;
-        const int cnt = A.rec_cnt[rec];
-        for (int e = 0; e < cnt; ++e) {
-          const long long q = (long long)e * A.n_rec + rec;
-          if (A.ent_kk[q] == kk) {
-            num += A.ent_num[q];
-            den += A.ent_den[q];
+}
+
+// One block per tile of 16 x 8 slab cells of one (reading shot, slice, class), one thread per
+// cell.  The block stages the tile's source-voxel box in shared memory (each voxel's cell, or -1
+// when it is untracked, of another class or in a plane the shot does not reach, and its record),
+// then every thread walks its own cell's box from there (z, then y, then x: the reference's
+// plane-then-voxel order) and adds the contributions of the voxels that round to its cell in
+// FP64, rounding once to f32 (spin_history.rs:407-419).  A box too large to stage (a strongly
+// rotated head on fine slabs) is walked in global memory instead, in the same order.
+__global__ void __launch_bounds__(kTileX * kTileY) spin_gather_kernel(GatherArgs A) {
+  __shared__ int key[kStageCap];
+  __shared__ int roff[kStageCap];
+  const long long b = blockIdx.x;
+  int lo = 0, hi = A.n_read;  // the reading shot holding block b
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (A.bcum[mid] <= b)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const SpinShotDev& S = A.shots[A.oshot[lo]];
+  const long long local = b - A.bcum[lo];
+  const int tile = (int)(local % A.tiles);
+  const int c = (int)((local / A.tiles) % A.ncls);
+  const int kk = (int)(local / ((long long)A.tiles * A.ncls));
+  const int k = A.tabs[S.slices + kk];
+  const int tx0 = (tile % A.tiles_x) * kTileX, ty0 = (tile / A.tiles_x) * kTileY;
+  const int tx1 = min(tx0 + kTileX, A.snx) - 1, ty1 = min(ty0 + kTileY, A.sny) - 1;
+  const int ext[3] = {A.nx, A.ny, A.nz};
+  int B0[3], B1[3];
+  preimage_box(S, tx0, tx1, ty0, ty1, k, A.half_len, ext, B0, B1);
+  const int bx = max(B1[0] - B0[0] + 1, 0), by = max(B1[1] - B0[1] + 1, 0), bz = max(B1[2] - B0[2] + 1, 0);
+  const long long total = (long long)bx * by * bz;
+  const bool staged = total <= kStageCap;
+  // the box's planes: their first record in the shot (or -1) and first tracked voxel
+  __shared__ int pbase[kStagePlanes], pfirst[kStagePlanes];
+  const bool planes_fit = bz <= kStagePlanes;
+  if (staged && planes_fit) {
+    for (int zz = threadIdx.x; zz < bz; zz += blockDim.x) {
+      pbase[zz] = A.tabs[S.plane_tab + B0[2] + zz];
+      pfirst[zz] = A.plane_first[B0[2] + zz];
+    }
+  }
+  __syncthreads();
+  const int want_key0 = c;  // keys are cell * n_classes + class
+  if (staged) {
+    // one warp per (y, z) row of the box, lanes across x (no division per voxel), four rows in
+    // flight per warp: their tracked indices are loaded together, then their records' keys and
+    // counts together, so the two dependent round trips overlap across the rows
+    constexpr int kRows = 4;
+    const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5, n_warps = (int)blockDim.x >> 5;
+    const int n_rows = by * bz;
+    for (int row0 = warp; row0 < n_rows; row0 += kRows * n_warps)
+      for (int xx = lane; xx < bx; xx += 32) {
+        int t[kRows], base[kRows], pf[kRows];
+#pragma unroll
+        for (int u = 0; u < kRows; ++u) {
+          const int row = row0 + u * n_warps;
+          t[u] = -1;
+          base[u] = -1;
+          pf[u] = 0;
+          if (row < n_rows) {
+            const int zz = row / by, yy = row - zz * by;
+            const int z = B0[2] + zz, y = B0[1] + yy;
+            base[u] = planes_fit ? pbase[zz] : A.tabs[S.plane_tab + z];
+            pf[u] = planes_fit ? pfirst[zz] : A.plane_first[z];
+            if (base[u] >= 0) t[u] = A.idx[(long long)A.nx * (y + (long long)A.ny * z) + B0[0] + xx];
+          }
+        }
+        int kv[kRows], pk[kRows];
+#pragma unroll
+        for (int u = 0; u < kRows; ++u) {
+          kv[u] = -1;
+          pk[u] = 0;
+          if (t[u] >= 0) {
+            const int ro = base[u] + (t[u] - pf[u]);
+            kv[u] = A.rec_cell[S.rec + ro];
+            pk[u] = (ro << 6) | (int)A.rec_cnt[S.rec + ro];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kRows; ++u) {
+          const int row = row0 + u * n_warps;
+          if (row < n_rows) {
+            key[row * bx + xx] = kv[u];
+            roff[row * bx + xx] = pk[u];
           }
         }
       }
+  }
+  __syncthreads();
+  const int cx = tx0 + (int)threadIdx.x % kTileX, cy = ty0 + (int)threadIdx.x / kTileX;
+  if (cx > tx1 || cy > ty1) return;
+  const int cell = cx + A.snx * cy;
+  const int want = cell * A.ncls + want_key0;
+  int b0[3], b1[3];
+  preimage_box(S, cx, cx, cy, cy, k, A.half_len, ext, b0, b1);
+  double num = 0.0, den = 0.0;
+  if (staged) {
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      b0[r] = max(b0[r], B0[r]);
+      b1[r] = min(b1[r], B1[r]);
+    }
+    // the matching records are collected eight at a time and their first entries loaded
+    // together (the additions keep the source order: record after record, entry after entry)
+    constexpr int kBatch = 8;
+    long long mrec[kBatch];
+    int mcnt[kBatch];
+    int nm = 0;
+    auto flush = [&]() {
+      double en[kBatch], ed[kBatch];
+      int ek[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        ek[u] = -1;
+        en[u] = ed[u] = 0.0;
+        if (u < nm && mcnt[u] > 0) {
+          ek[u] = A.ent_kk[mrec[u]];
+          en[u] = A.ent_num[mrec[u]];
+          ed[u] = A.ent_den[mrec[u]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        if (u >= nm) continue;
+        if (ek[u] == kk) {
+          num += en[u];
+          den += ed[u];
+        }
+        for (int q = 1; q < mcnt[u]; ++q) {
+          const long long j = (long long)q * A.n_rec + mrec[u];
+          if (A.ent_kk[j] == kk) {
+            num += A.ent_num[j];
+            den += A.ent_den[j];
+          }
+        }
+      }
+      nm = 0;
+    };
+    for (int z = b0[2]; z <= b1[2]; ++z)
+      for (int y = b0[1]; y <= b1[1]; ++y) {
+        const int er = bx * ((y - B0[1]) + by * (z - B0[2])) - B0[0];
+        for (int x = b0[0]; x <= b1[0]; ++x) {
+          const int e = er + x;
+          if (key[e] != want) continue;
+          const long long rec = S.rec + (roff[e] >> 6);
+          const int cnt = roff[e] & 63;
+#pragma unroll
+          for (int u = 0; u < kBatch; ++u)
+            if (u == nm) {
+              mrec[u] = rec;
+              mcnt[u] = cnt;
+            }
+          if (++nm == kBatch) flush();
+        }
+      }
+    flush();
+  } else {
+    for (int z = b0[2]; z <= b1[2]; ++z) {
+      const int base = A.tabs[S.plane_tab + z];
+      if (base < 0) continue;
+      const int pf = A.plane_first[z];
+      for (int y = b0[1]; y <= b1[1]; ++y)
+        for (int x = b0[0]; x <= b1[0]; ++x) {
+          const int t = A.idx[x + A.nx * (y + A.ny * z)];
+          if (t < 0) continue;
+          const long long rec = S.rec + base + (t - pf);
+          if (A.rec_cell[rec] != want) continue;
+          const int cnt = A.rec_cnt[rec];
+          for (int q = 0; q < cnt; ++q) {
+            const long long j = (long long)q * A.n_rec + rec;
+            if (A.ent_kk[j] == kk) {
+              num += A.ent_num[j];
+              den += A.ent_den[j];
+            }
+          }
+        }
+    }
   }
   float* o = A.terms + S.out + ((long long)kk * 2 * A.ncls + c) * A.cells + cell;
   o[0] = (float)num;
@@ -487,7 +642,8 @@ SpinHistoryDev* spin_history_create(mrsim_context* ctx, const int64_t* src_dims,
   const int64_t nv = src_dims[0] * src_dims[1] * src_dims[2];
   if (nv >= (1LL << 31)) fail("a source grid of 2^31 voxels or more");
   if (n_classes <= 0 || n_classes > 255) fail("n_classes must be in 1..255");
-  if (slab_dims[0] * slab_dims[1] >= (1LL << 31) || slab_dims[2] > 32767) fail("slab grid too large");
+  // record keys are cell * n_classes + class in an int
+  if (slab_dims[0] * slab_dims[1] * n_classes >= (1LL << 31) || slab_dims[2] > 32767) fail("slab grid too large");
   for (int64_t i = 0; i < n_pulses; ++i)
     if (pulses[i].kind != MRSIM_PULSE_INVERSION && pulses[i].kind != MRSIM_PULSE_SATURATION)
       fail("unknown pulse kind");
@@ -579,6 +735,7 @@ SpinHistoryDev* spin_history_create(mrsim_context* ctx, const int64_t* src_dims,
                                cudaMemcpyHostToDevice, st));
   MRSIM_CUDA(cudaMemsetAsync(h.d_merges, 0, 8, st));
   MRSIM_CUDA(cudaMemsetAsync(h.d_err, 0, 4, st));
+  for (int b = 0; b < 2; ++b) MRSIM_CUDA(cudaEventCreateWithFlags(&h.pin_ev[b], cudaEventDisableTiming));
   MRSIM_CUDA(cudaStreamSynchronize(st));  // the host staging vectors go out of scope
   return H.release();
 }
@@ -610,6 +767,8 @@ void spin_history_run(SpinHistoryDev& h, const mrsim_spin_shot* shots, int64_t n
   to_m4(h.w2v_slab, w2v_slab);
   const size_t rec_budget = std::max<size_t>(1, ((size_t)1 << 30) / record_bytes(h.maxc));  // records per batch
   const size_t w_budget = ((size_t)1 << 30) / 4;  // override weights per batch
+  const int tiles_x = (int)((h.snx + kTileX - 1) / kTileX);
+  const long long tiles = (long long)tiles_x * ((h.sny + kTileY - 1) / kTileY);
   long long out_off = 0;
   int64_t s0 = 0;
   while (s0 < n) {
@@ -700,22 +859,47 @@ void spin_history_run(SpinHistoryDev& h, const mrsim_spin_shot* shots, int64_t n
         D.out = out_off;
         out_off += S.n_slices * 2 * (long long)h.ncls * cells;
         if (S.n_slices > 0) {
-          ocum.push_back(ocum.back() + S.n_slices * (long long)h.ncls * cells);
+          ocum.push_back(ocum.back() + S.n_slices * (long long)h.ncls * tiles);
           oshot.push_back((int)sd.size());
         }
       }
       sd.push_back(D);
     }
-    // upload the batch's tables (pageable copies are staged before cudaMemcpyAsync returns)
-    auto up = [&](GrowBuf& b, const void* src, size_t bytes) {
-      void* p = b.get(bytes);
-      if (bytes) MRSIM_CUDA(cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, st));
-      return p;
-    };
-    const SpinShotDev* d_shots = (const SpinShotDev*)up(h.shots_b, sd.data(), sd.size() * sizeof(SpinShotDev));
-    const int* d_tabs = (const int*)up(h.tabs_b, tabs.data(), tabs.size() * 4);
-    const double* d_values = (const double*)up(h.values_b, values.data(), values.size() * 8);
-    const float* d_weights = (const float*)up(h.weights_b, weights.data(), weights.size() * 4);
+    // the batch's tables packed into the next pinned staging blob (waiting only for the copy out
+    // of it two batches ago) and uploaded in one asynchronous copy
+    auto a16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t o_tabs = a16(sd.size() * sizeof(SpinShotDev));
+    const size_t o_vals = a16(o_tabs + tabs.size() * 4);
+    const size_t o_w = a16(o_vals + values.size() * 8);
+    const size_t o_cum = a16(o_w + weights.size() * 4);
+    const size_t o_osh = a16(o_cum + ocum.size() * 8);
+    const size_t blob = a16(o_osh + oshot.size() * 4);
+    const int pb = h.pin_i;
+    h.pin_i ^= 1;
+    MRSIM_CUDA(cudaEventSynchronize(h.pin_ev[pb]));
+    if (h.pin_n[pb] < blob) {
+      if (h.pin[pb]) MRSIM_CUDA(cudaFreeHost(h.pin[pb]));
+      h.pin[pb] = nullptr;
+      h.pin_n[pb] = 0;
+      MRSIM_CUDA(cudaHostAlloc(&h.pin[pb], blob, cudaHostAllocDefault));
+      h.pin_n[pb] = blob;
+    }
+    char* hb = (char*)h.pin[pb];
+    std::memcpy(hb, sd.data(), sd.size() * sizeof(SpinShotDev));
+    if (!tabs.empty()) std::memcpy(hb + o_tabs, tabs.data(), tabs.size() * 4);
+    if (!values.empty()) std::memcpy(hb + o_vals, values.data(), values.size() * 8);
+    if (!weights.empty()) std::memcpy(hb + o_w, weights.data(), weights.size() * 4);
+    std::memcpy(hb + o_cum, ocum.data(), ocum.size() * 8);
+    if (!oshot.empty()) std::memcpy(hb + o_osh, oshot.data(), oshot.size() * 4);
+    char* db = (char*)h.blob_b.get(blob);
+    MRSIM_CUDA(cudaMemcpyAsync(db, hb, blob, cudaMemcpyHostToDevice, st));
+    MRSIM_CUDA(cudaEventRecord(h.pin_ev[pb], st));
+    const SpinShotDev* d_shots = (const SpinShotDev*)db;
+    const int* d_tabs = (const int*)(db + o_tabs);
+    const double* d_values = (const double*)(db + o_vals);
+    const float* d_weights = (const float*)(db + o_w);
+    // a staged record is addressed by 25 bits (its count in the other 6 of an int)
+    if (n_rec >= (1LL << 25)) fail("more than 2^25 voxels in reach of one shot");
     const size_t nr = (size_t)std::max<long long>(n_rec, 1);
     int* d_rec_cell = (int*)h.rec_cell_b.get(nr * 4);
     uint8_t* d_rec_cnt = (uint8_t*)h.rec_cnt_b.get(nr);
@@ -746,6 +930,8 @@ void spin_history_run(SpinHistoryDev& h, const mrsim_spin_shot* shots, int64_t n
       A.ent_kk = d_kk;
       A.n_rec = (long long)nr;
       A.maxc = h.maxc;
+      A.ncls = h.ncls;
+      A.cls = h.d_cls;
       A.nk_max = (int)(std::floor(h.len) + 2.0);
       A.nt = h.nt;
       A.nx = (int)h.nx;
@@ -762,16 +948,12 @@ void spin_history_run(SpinHistoryDev& h, const mrsim_spin_shot* shots, int64_t n
       MRSIM_CUDA(cudaGetLastError());
     }
     if (!oshot.empty()) {
-      const long long n_out = ocum.back();
-      const size_t cum_bytes = ocum.size() * 8;
-      char* ob = (char*)h.ocum_b.get(cum_bytes + oshot.size() * 4);
-      MRSIM_CUDA(cudaMemcpyAsync(ob, ocum.data(), cum_bytes, cudaMemcpyHostToDevice, st));
-      MRSIM_CUDA(cudaMemcpyAsync(ob + cum_bytes, oshot.data(), oshot.size() * 4, cudaMemcpyHostToDevice, st));
+      const long long n_blocks = ocum.back();
       GatherArgs G{};
       G.shots = d_shots;
       G.tabs = d_tabs;
-      G.ocum = (const long long*)ob;
-      G.oshot = (const int*)(ob + cum_bytes);
+      G.bcum = (const long long*)(db + o_cum);
+      G.oshot = (const int*)(db + o_osh);
       G.n_read = (int)oshot.size();
       G.idx = h.d_idx;
       G.plane_first = h.d_plane_first;
@@ -786,16 +968,20 @@ void spin_history_run(SpinHistoryDev& h, const mrsim_spin_shot* shots, int64_t n
       G.ny = (int)h.ny;
       G.nz = (int)h.nz;
       G.snx = (int)h.snx;
+      G.sny = (int)h.sny;
       G.ncls = h.ncls;
+      G.tiles_x = tiles_x;
+      G.tiles = (int)tiles;
       G.cells = cells;
       G.half_len = h.len / 2.0;
       G.terms = terms;
-      spin_gather_kernel<<<(unsigned)((n_out + 255) / 256), 256, 0, st>>>(G);
+      if (n_blocks >= (1LL << 31)) fail("too many terms in one batch");
+      spin_gather_kernel<<<(unsigned)n_blocks, kTileX * kTileY, 0, st>>>(G);
       MRSIM_CUDA(cudaGetLastError());
     }
+    // the next batch's copies and launches follow these on the stream (a buffer that must grow is
+    // freed by cudaFree, which waits for the device)
     s0 = s1;
-    // the next batch overwrites (and may regrow) the batch buffers these launches read
-    if (s0 < n) MRSIM_CUDA(cudaStreamSynchronize(st));
   }
 }
 

@@ -68,8 +68,14 @@ struct SpinHistoryDev {
   int* d_err = nullptr;
   std::vector<void*> allocs;
   // per-batch buffers
-  GrowBuf shots_b, tabs_b, values_b, weights_b, rec_cell_b, rec_cnt_b, ent_num_b, ent_den_b, ent_kk_b, ocum_b,
-      out_b;
+  GrowBuf blob_b, rec_cell_b, rec_cnt_b, ent_num_b, ent_den_b, ent_kk_b, out_b;
+  // two pinned host blobs that stage a batch's tables, used in turn; each is rewritten only once
+  // the copy out of it (its event) has completed, so the host prepares batch n+1 while the device
+  // still runs batch n
+  void* pin[2] = {nullptr, nullptr};
+  size_t pin_n[2] = {0, 0};
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+  int pin_i = 0;
   ~SpinHistoryDev();
 };
 

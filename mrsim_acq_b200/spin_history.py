@@ -180,6 +180,19 @@ def unpack_terms(shots: Sequence[Shot], flat: np.ndarray, n_classes: int, cells:
     return out
 
 
+class PreparedShots:
+    """Shots marshalled once into the C shot array (`SpinHistory.prepare`), for callers that run
+    the same shot list again or want the marshalling out of a timed loop."""
+
+    def __init__(self, shots: Sequence[Shot], ref_values: "_RefValues"):
+        self.shots = list(shots)
+        self.keep: list = []
+        self.arr = shots_c(self.shots, ref_values, self.keep)
+
+    def __len__(self):
+        return len(self.shots)
+
+
 class SpinHistory:
     """`SpinHistory` (spin_history.rs:171-422) with its state resident on the device."""
 
@@ -232,29 +245,39 @@ class SpinHistory:
         check(lib().mrsim_spin_history_prime(self._h, times.ctypes.data_as(abi.c_f64p), sl.ctypes.data_as(P),
                                              offs.ctypes.data_as(P), len(shots), m.ctypes.data_as(abi.c_f64p)))
 
-    def terms_size(self, shots: Sequence[Shot]) -> int:
+    def prepare(self, shots: Sequence[Shot]) -> PreparedShots:
+        """The shots marshalled for `excite_many` / `excite_device` (callable references are
+        evaluated here, once)."""
+        return PreparedShots(shots, self._ref_values)
+
+    def _arr(self, shots):
+        if isinstance(shots, PreparedShots):
+            return shots.arr, shots.shots
         keep: list = []
         arr = shots_c(shots, self._ref_values, keep)
+        self._keep = keep
+        return arr, shots
+
+    def terms_size(self, shots) -> int:
+        arr, _ = self._arr(shots)
         n = C.c_int64()
         check(lib().mrsim_spin_history_terms_size(self._h, arr, len(shots), C.byref(n)))
         return n.value
 
-    def excite_many(self, shots: Sequence[Shot]) -> list:
-        """The shots in order, in one batch on the device; per shot its SliceTerms (None for a
-        shot with no reference)."""
-        keep: list = []
-        arr = shots_c(shots, self._ref_values, keep)
+    def excite_many(self, shots) -> list:
+        """The shots (a list of Shot or PreparedShots) in order, in one batch on the device; per
+        shot its SliceTerms (None for a shot with no reference)."""
+        arr, shots = self._arr(shots)
         n = C.c_int64()
         check(lib().mrsim_spin_history_terms_size(self._h, arr, len(shots), C.byref(n)))
         flat = np.zeros(max(n.value, 1), np.float32)
         check(lib().mrsim_spin_history_excite(self._h, arr, len(shots), flat.ctypes.data_as(abi.c_f32p)))
         return unpack_terms(shots, flat, self.n_classes, self.cells)
 
-    def excite_device(self, shots: Sequence[Shot], out_ptr: int) -> None:
-        """The shots in order with the packed terms written to device memory at `out_ptr` (queued
-        on the context's stream)."""
-        keep: list = []
-        arr = shots_c(shots, self._ref_values, keep)
+    def excite_device(self, shots, out_ptr: int) -> None:
+        """The shots (a list of Shot or PreparedShots) in order with the packed terms written to
+        device memory at `out_ptr` (queued on the context's stream)."""
+        arr, shots = self._arr(shots)
         check(lib().mrsim_spin_history_excite_device(self._h, arr, len(shots), C.c_void_p(out_ptr)))
 
     def excite(self, t: float, transform, slices: Sequence[int], mz_ref: MzRef,
