@@ -578,13 +578,24 @@ typedef struct mrsim_grase_readout {
   int32_t reserved;
 } mrsim_grase_readout;
 
+/* `ShotSet` (kspace3d.rs:59-65): the images one set of shots of one volume saw (per-shot motion),
+ * per compartment one simulation-grid volume x + snx*(y + sny*z).  Every line (spiral: every
+ * interleave) of a shot in `shots` is computed from these images instead of the volume's own; a
+ * shot in several sets takes the first. */
+typedef struct mrsim_shot_set {
+  const int64_t* shots;
+  int64_t n_shots;
+  const float* const* images;
+} mrsim_shot_set;
+
 /* The inputs of `simulate_acquisition_3d` (kspace3d.rs:549-565): images as the 2D series takes
  * them (ncomp arrays of snx*sny*nz*n_volumes, vox*nv+g); t2 / t1 / t_inhom per compartment over
  * the simulation volume (t1 NULL = infinite; required below 180 degrees of refocusing; t_inhom
  * NULL = Acquisition::t_inhom); `line_weights` = `LineWeights::w` [g][shot][c] or NULL; the
  * in-plane GRAPPA reference scan (`GrappaCalibration`, kspace.rs:1646) when
- * has_grappa_calibration, else the first volume's images and `seed`.  Per-shot images
- * (`ShotSet`) are not taken. */
+ * has_grappa_calibration, else the first volume's images and `seed`; `shot_sets` /
+ * `n_shot_sets` = the per-shot images (`shot_images: Option<&[Vec<ShotSet>]>`): volume g's sets at
+ * shot_sets[g][0 .. n_shot_sets[g]], or both NULL (the reference scan never takes them). */
 typedef struct mrsim_acquisition_3d_input {
   int64_t sim_dims[3];
   int64_t acq_dims[3];
@@ -601,6 +612,8 @@ typedef struct mrsim_acquisition_3d_input {
   int32_t reserved;
   const float* const* grappa_calibration_images;   /* ncomp sim volumes */
   uint64_t grappa_calibration_seed;
+  const mrsim_shot_set* const* shot_sets;          /* n_volumes lists, or NULL */
+  const int64_t* n_shot_sets;                      /* n_volumes counts, or NULL */
 } mrsim_acquisition_3d_input;
 
 /* `kz_order` (readout.rs:167-189). */
@@ -646,11 +659,15 @@ typedef struct mrsim_ge3d_readout {
 } mrsim_ge3d_readout;
 
 /* `GeVolume` (kspace3d.rs:592-603): per compartment one sim volume (NULL = a compartment this
- * volume does not use; its weights must be 0) and the excitation weights
- * w[(p * ky_segments + sy) * ncomp + c].  Per-shot images are not taken. */
+ * volume does not use; its weights must be 0), the excitation weights
+ * w[(p * ky_segments + sy) * ncomp + c], and the per-shot images (`shot_images`: n_shot_sets
+ * sets, each with an image for every compartment the volume uses; 0 / NULL = none; the GRAPPA
+ * reference scan never takes them). */
 typedef struct mrsim_ge_volume {
   const float* const* images;
   const double* weights;
+  const mrsim_shot_set* shot_sets;
+  int64_t n_shot_sets;
 } mrsim_ge_volume;
 
 /* The `volume` callback: fill *out for volume g (pointers valid until the next call or the end

@@ -144,6 +144,12 @@ class GraseReadout_(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class ShotSet_(C.Structure):
+    """`mrsim_shot_set` — `ShotSet` (kspace3d.rs:59-65)."""
+
+    _fields_ = [("shots", C.POINTER(C.c_int64)), ("n_shots", C.c_int64), ("images", C.POINTER(c_f32p))]
+
+
 class Acquisition3dInput_(C.Structure):
     """`mrsim_acquisition_3d_input` — the inputs of `simulate_acquisition_3d` (kspace3d.rs:549)."""
 
@@ -153,6 +159,7 @@ class Acquisition3dInput_(C.Structure):
         ("t_inhom", C.POINTER(T2_)), ("phase", C.POINTER(PhaseModel_)), ("line_weights", c_f64p),
         ("has_grappa_calibration", C.c_int32), ("reserved", C.c_int32),
         ("grappa_calibration_images", C.POINTER(c_f32p)), ("grappa_calibration_seed", C.c_uint64),
+        ("shot_sets", C.POINTER(C.POINTER(ShotSet_))), ("n_shot_sets", C.POINTER(C.c_int64)),
     ]
 
 
@@ -172,9 +179,10 @@ class Ge3dReadout_(C.Structure):
 
 
 class GeVolume_(C.Structure):
-    """`mrsim_ge_volume` — `GeVolume` (kspace3d.rs:592-603) without per-shot images."""
+    """`mrsim_ge_volume` — `GeVolume` (kspace3d.rs:592-603)."""
 
-    _fields_ = [("images", C.POINTER(c_f32p)), ("weights", c_f64p)]
+    _fields_ = [("images", C.POINTER(c_f32p)), ("weights", c_f64p), ("shot_sets", C.POINTER(ShotSet_)),
+                ("n_shot_sets", C.c_int64)]
 
 
 GE_VOLUME_FN = C.CFUNCTYPE(C.c_int, C.c_int64, C.c_void_p, C.POINTER(GeVolume_))

@@ -40,10 +40,12 @@ struct ZdftArgs {
   const float* lw;        // [g][shot][c] or NULL
   const int* shot;        // [p][ky]
   const unsigned char* row_acquired;  // [ky]
-  int nx, ny, nz, nc, ncomp, nsrc, n_shots, g0;
+  const int* line_var;    // [gl][p][ky]: the image variant a line reads (0: the volume's own), or NULL
+  int nx, ny, nz, nc, ncomp, nsrc, n_shots, g0, nvar;
 };
 
-// out = sampling * sum_c lw(g, shot, c) * (w_c(p, ky) * sum_z K[src(c, p)][z] zk[p][z])
+// out = sampling * sum_c lw(g, shot, c) * (w_c(p, ky) * sum_z K[var(p, ky)][src(c, p)][z] zk[p][z]), var
+// the images the line's shot saw (`Plan::kspace` kspace3d.rs:206-232)
 __global__ void grase_zdft_kernel(const ZdftArgs a) {
   const int per = a.nx * a.ny;
   const int p = blockIdx.y;
@@ -55,7 +57,9 @@ __global__ void grase_zdft_kernel(const ZdftArgs a) {
     if (a.row_acquired[ky]) {
       for (int c = 0; c < a.ncomp; ++c) {
         const int s = a.src[c * a.nz + p];
-        const float2* Kc = a.K + ((size_t)(gl * a.nsrc + s) * a.nz) * a.nc * per + (size_t)q * per + i;
+        const int var = a.line_var ? a.line_var[((size_t)gl * a.nz + p) * a.ny + ky] : 0;
+        const float2* Kc =
+            a.K + ((size_t)((gl * a.nvar + var) * a.nsrc + s) * a.nz) * a.nc * per + (size_t)q * per + i;
         float ar = 0.f, ai = 0.f;
         for (int z = 0; z < a.nz; ++z) {
           const float2 k = Kc[(size_t)z * a.nc * per];
@@ -132,6 +136,8 @@ struct GrasePlan {
   std::vector<float> wc;    // [c][p][ky]
   std::vector<int> shot;    // [p][ky]: the index of the line weights (GRASE's shot, GE's excitation)
   int n_shots = 0;
+  std::vector<int> set_shot;  // [p][ky]: the shot whose images the line reads (`ShotSet` membership)
+  int n_set_shots = 0;
   std::vector<char> used;   // per compartment
 };
 
@@ -175,6 +181,8 @@ static GrasePlan make_plan(const mrsim_acquisition_3d_input& in, const mrsim_acq
   for (int p = 0; p < P.nz; ++p)
     for (int ky = 0; ky < P.ny; ++ky) P.shot[(size_t)p * P.ny + ky] = P.table.line(p, ky).shot;
   P.n_shots = P.table.n_shots;
+  P.set_shot = P.shot;
+  P.n_set_shots = P.n_shots;
   P.used.assign(P.ncomp, 1);
   P.modes = resolve_modes(in.t2, in.t1, in.t_inhom, P.ncomp, acq, train, P.nvox);
   P.mask = sampling_mask(P.nx, P.ny, acq);
@@ -261,11 +269,89 @@ static GraseInputs upload_inputs(DevArena& A, const GrasePlan& P, const mrsim_ac
   return I;
 }
 
+// Per-shot images of the volumes of a chunk (`ShotSet`, kspace3d.rs:59-65): variant 0 is each
+// volume's own images, variant v > 0 its set v - 1 (one device volume per used compartment);
+// per volume and line the variant the line reads (the first set holding its shot).
+struct ShotVariants {
+  int nvar = 1;
+  std::vector<std::vector<const float*>> img;  // [gl * nvar + v][c] (v > 0; NULL: no such set)
+  const int* d_line_var = nullptr;             // [gl][p][ky], or NULL when no volume has sets
+};
+
+// The sets of volumes g0..g1 (`sets[gl]`, `n_sets[gl]`): checked (shots inside the train, an
+// image for every compartment the volume uses), uploaded, and the line table built.
+static ShotVariants upload_sets(DevArena& A, const GrasePlan& P, const std::vector<const mrsim_shot_set*>& sets,
+                                const std::vector<int64_t>& n_sets, int first_g, cudaStream_t st, bool upload = true) {
+  ShotVariants V;
+  const int ngl = (int)sets.size();
+  int64_t most = 0;
+  for (int gl = 0; gl < ngl; ++gl) most = std::max<int64_t>(most, sets[gl] ? n_sets[gl] : 0);
+  if (most == 0) return V;
+  V.nvar = (int)most + 1;
+  V.img.assign((size_t)ngl * V.nvar, std::vector<const float*>(P.ncomp, nullptr));
+  std::vector<int> line_var((size_t)ngl * P.nz * P.ny, 0);
+  for (int gl = 0; gl < ngl; ++gl) {
+    if (!sets[gl]) continue;
+    for (int64_t i = 0; i < n_sets[gl]; ++i) {
+      const mrsim_shot_set& S = sets[gl][i];
+      if (S.n_shots > 0 && !S.shots) fail("volume " + std::to_string(first_g + gl) + ": a shot set's shots are NULL");
+      for (int64_t j = 0; j < S.n_shots; ++j)
+        if (S.shots[j] < 0 || S.shots[j] >= P.n_set_shots)
+          fail("a shot index beyond the train's " + std::to_string(P.n_set_shots));
+      for (int c = 0; c < P.ncomp; ++c) {
+        if (!P.used[c]) {
+          if (S.images && S.images[c])
+            fail("volume " + std::to_string(first_g + gl) + ": shot images are not the volume's compartments");
+          continue;
+        }
+        if (!S.images || !S.images[c])
+          fail("volume " + std::to_string(first_g + gl) + ": shot images are not the volume's compartments");
+        if (upload) V.img[(size_t)gl * V.nvar + i + 1][c] = (const float*)A.upload(S.images[c], P.nvox * 4, st);
+      }
+    }
+    for (size_t l = 0; l < P.set_shot.size() && upload; ++l) {
+      const int64_t shot = P.set_shot[l];
+      for (int64_t i = 0; i < n_sets[gl]; ++i) {
+        const mrsim_shot_set& S = sets[gl][i];
+        if (std::find(S.shots, S.shots + S.n_shots, shot) != S.shots + S.n_shots) {
+          line_var[(size_t)gl * P.set_shot.size() + l] = (int)i + 1;
+          break;
+        }
+      }
+    }
+  }
+  if (upload) V.d_line_var = (const int*)A.upload(line_var.data(), line_var.size() * 4, st);
+  return V;
+}
+
+// The 3D input's sets of volumes g0..g1.
+static ShotVariants input_sets(DevArena& A, const GrasePlan& P, const mrsim_acquisition_3d_input& in, int g0, int g1,
+                               cudaStream_t st, bool upload = true) {
+  std::vector<const mrsim_shot_set*> sets;
+  std::vector<int64_t> n;
+  for (int g = g0; g < g1; ++g) {
+    const bool has = in.shot_sets && in.n_shot_sets && in.n_shot_sets[g] > 0;
+    if (has && !in.shot_sets[g]) fail("volume " + std::to_string(g) + ": its shot sets are NULL");
+    sets.push_back(has ? in.shot_sets[g] : nullptr);
+    n.push_back(has ? in.n_shot_sets[g] : 0);
+  }
+  return upload_sets(A, P, sets, n, g0, st, upload);
+}
+// The most image variants any volume needs (1 + its sets).
+static int most_variants(const mrsim_acquisition_3d_input& in) {
+  int64_t most = 0;
+  if (in.shot_sets && in.n_shot_sets)
+    for (int64_t g = 0; g < in.n_volumes; ++g) most = std::max<int64_t>(most, in.n_shot_sets[g]);
+  return (int)most + 1;
+}
+
 // The acquired 3D k-space (before spikes and noise) of volumes g0..g1 into k3 [gl][q][p][ky][kx].
 static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_acquisition& acq,
                          const mrsim_phase_model* phase, const float* d_lw, int g0, int g1,
-                         const std::vector<uint8_t>& mask, float2* k3, cudaStream_t st) {
+                         const std::vector<uint8_t>& mask, float2* k3, cudaStream_t st,
+                         const ShotVariants* V = nullptr) {
   const int ngl = g1 - g0, nsrc = (int)P.srcs.size(), nz = P.nz, nc = P.nc;
+  const int nvar = V ? V->nvar : 1;
   const size_t per = (size_t)P.nx * P.ny;
   DevArena C;
   mrsim_acquisition norel = acq;
@@ -282,7 +368,7 @@ static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_a
   const int n_lines = (int)Lc.size();
   const LineRec* dLc = (const LineRec*)C.upload(Lc.data(), std::max<size_t>(1, Lc.size()) * sizeof(LineRec), st);
   const LineRec* dLv = (const LineRec*)C.upload(Lv.data(), std::max<size_t>(1, Lv.size()) * sizeof(LineRec), st);
-  const size_t nunit = (size_t)ngl * nsrc * nz;
+  const size_t nunit = (size_t)ngl * nvar * nsrc * nz;
   float2* K = (float2*)C.alloc(std::max<size_t>(1, nunit * nc * per) * sizeof(float2));
   MRSIM_CUDA(cudaMemsetAsync(K, 0, nunit * nc * per * sizeof(float2), st));
   float2* gs = (float2*)C.alloc(std::max<size_t>(1, nunit * nc * std::max(n_lines, 1) * P.snx) * sizeof(float2));
@@ -292,13 +378,17 @@ static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_a
   std::memset(&zero, 0, sizeof zero);
   Batch Bc, Bv;
   for (int gl = 0; gl < ngl; ++gl)
+    for (int var = 0; var < nvar; ++var)
     for (int s = 0; s < nsrc; ++s)
       for (int z = 0; z < nz; ++z) {
         const GrasePlan::Src& S = P.srcs[s];
-        const size_t u = ((size_t)gl * nsrc + s) * nz + z;
+        const size_t u = (((size_t)gl * nvar + var) * nsrc + s) * nz + z;
+        const float* set_img = var > 0 ? V->img[(size_t)gl * nvar + var][S.c] : nullptr;
+        if (var > 0 && !set_img) continue;  // a volume with fewer sets, or a compartment it does not use
         UnitInputs ui;
         std::memset(&ui, 0, sizeof ui);
-        ui.comp = I.img + (((size_t)(g0 + gl) * nz + z) * P.ncomp + S.c) * P.plane;
+        ui.comp = var > 0 ? set_img + (size_t)z * P.plane
+                          : I.img + (((size_t)(g0 + gl) * nz + z) * P.ncomp + S.c) * P.plane;
         ui.comp_stride = (long long)P.plane;
         ui.fmap = I.fmap + (size_t)z * P.plane;
         ui.map_stride = (long long)P.nvox;
@@ -348,6 +438,8 @@ static void grase_kspace(const GrasePlan& P, const GraseInputs& I, const mrsim_a
   a.nsrc = nsrc;
   a.n_shots = P.n_shots;
   a.g0 = g0;
+  a.line_var = V ? V->d_line_var : nullptr;
+  a.nvar = nvar;
   grase_zdft_kernel<<<grid3(per, nz, ngl * nc), 256, 0, st>>>(a);
   MRSIM_CUDA(cudaGetLastError());
   MRSIM_CUDA(cudaStreamSynchronize(st));  // C's buffers are freed on return
@@ -397,7 +489,8 @@ void grase_observed(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, co
   }
   const size_t per = (size_t)P.nx * P.ny;
   float2* k3 = (float2*)A.alloc((size_t)P.nc * P.nz * per * sizeof(float2));
-  grase_kspace(P, I, acq, in.phase, d_lw, g, g + 1, P.mask, k3, st);
+  ShotVariants V = input_sets(A, P, in, g, g + 1, st);
+  grase_kspace(P, I, acq, in.phase, d_lw, g, g + 1, P.mask, k3, st, &V);
   MRSIM_CUDA(cudaMemcpyAsync(out, k3, (size_t)P.nc * P.nz * per * sizeof(float2), cudaMemcpyDeviceToHost, st));
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
@@ -410,7 +503,9 @@ void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, con
   const int nv = (int)in.n_volumes, nz = P.nz, nc = P.nc, nx = P.nx, ny = P.ny;
   const size_t per = (size_t)nx * ny;
   const int accel = (int)std::max<int64_t>(acq.accel, 1);
+  const int nvar = most_variants(in);
   DevArena A;
+  if (nvar > 1) (void)input_sets(A, P, in, 0, nv, st, false);  // every volume's sets checked before any work
   GraseInputs I = upload_inputs(A, P, in, in.images, nv, acq, st);
   const float* d_lw = nullptr;
   if (in.line_weights) {
@@ -453,15 +548,17 @@ void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, con
   float* d_ph = (float*)A.alloc(std::max<size_t>(1, per * nz * nv) * 4);
   // chunks of volumes within a scratch budget
   const size_t nsrc = P.srcs.size();
-  const size_t bytes_per_vol = (nsrc * nz * nc * per * 8) * 2 + nsrc * nz * (size_t)nc * ny * P.snx * 8 +
-                               (size_t)nc * nz * per * 8 * 2 + (size_t)nz * per * 8;
+  const size_t bytes_per_vol = ((nsrc * nz * nc * per * 8) * 2 + nsrc * nz * (size_t)nc * ny * P.snx * 8) * nvar +
+                               (size_t)(nvar - 1) * P.ncomp * P.nvox * 4 + (size_t)nc * nz * per * 8 * 2 +
+                               (size_t)nz * per * 8;
   const size_t budget = (size_t)4 << 30;
   const int vchunk = (int)std::max<size_t>(1, std::min<size_t>(std::max(nv, 1), budget / std::max<size_t>(1, bytes_per_vol)));
   for (int g0 = 0; g0 < nv; g0 += vchunk) {
     const int g1 = std::min(nv, g0 + vchunk), ngl = g1 - g0;
     DevArena C;
     float2* k3 = (float2*)C.alloc((size_t)ngl * nc * nz * per * sizeof(float2));
-    grase_kspace(P, I, acq, in.phase, d_lw, g0, g1, P.mask, k3, st);
+    ShotVariants V = input_sets(C, P, in, g0, g1, st);
+    grase_kspace(P, I, acq, in.phase, d_lw, g0, g1, P.mask, k3, st, &V);
     grase_noise(C, P, k3, g0, g1, seed, P.mask, acq, st);
     float2* sl = (float2*)C.alloc((size_t)ngl * nz * nc * per * sizeof(float2));
     grase_izdft_kernel<<<grid3(per, nz, ngl * nc), 256, 0, st>>>(k3, d_zk, nx, ny, nz, nc, sl);
@@ -506,6 +603,8 @@ namespace {
 struct GeVolumeData {
   std::vector<const float*> images;  // ncomp (NULL = unused)
   std::vector<double> weights;
+  const mrsim_shot_set* sets = nullptr;  // `shot_images` (the reference scan takes none)
+  int64_t n_sets = 0;
 };
 
 GeVolumeData fetch_ge_volume(const mrsim_acquisition_ge_input& in, int g, int n_exc_lines) {
@@ -519,6 +618,11 @@ GeVolumeData fetch_ge_volume(const mrsim_acquisition_ge_input& in, int g, int n_
   for (int c = 0; c < (int)in.ncomp; ++c) d.images[c] = v.images[c];
   if (!v.weights) fail("volume " + std::to_string(g) + ": weights are not (partition, ky segment, compartment)");
   d.weights.assign(v.weights, v.weights + n_exc_lines);
+  if (v.n_shot_sets > 0) {
+    if (!v.shot_sets) fail("volume " + std::to_string(g) + ": its shot sets are NULL");
+    d.sets = v.shot_sets;
+    d.n_sets = v.n_shot_sets;
+  }
   for (int c = 0; c < (int)in.ncomp; ++c)
     if (!d.images[c])
       for (int x = 0; x < n_exc_lines / std::max<int>(1, (int)in.ncomp); ++x)
@@ -566,6 +670,10 @@ static GrasePlan make_ge_plan(const mrsim_acquisition_ge_input& in, const mrsim_
   for (int p = 0; p < P.nz; ++p)
     for (int ky = 0; ky < P.ny; ++ky) P.shot[(size_t)p * P.ny + ky] = p * kys + ky % kys;
   P.n_shots = P.nz * kys;
+  P.set_shot.resize((size_t)P.nz * P.ny);
+  for (int p = 0; p < P.nz; ++p)
+    for (int ky = 0; ky < P.ny; ++ky) P.set_shot[(size_t)p * P.ny + ky] = table.line(p, ky).shot;
+  P.n_set_shots = table.n_shots;
   P.used.assign(P.ncomp, 1);
   P.modes.resize(P.ncomp);
   for (int c = 0; c < P.ncomp; ++c) {
@@ -681,6 +789,8 @@ void ge_acquire(mrsim_context* ctx, const mrsim_acquisition_ge_input& in, const 
       ref.weights.assign(in.reference->weights, in.reference->weights + n_exc_lines);
     } else {
       ref = fetch_ge_volume(in, 0, n_exc_lines);
+      ref.sets = nullptr;  // `GeVolume { shot_images: None, .. }` (kspace3d.rs:775)
+      ref.n_sets = 0;
     }
     mrsim_acquisition acq_cal = acq;
     acq_cal.accel = 1;
@@ -719,6 +829,7 @@ void ge_acquire(mrsim_context* ctx, const mrsim_acquisition_ge_input& in, const 
     DevArena C;
     const float* d_lw = nullptr;
     GraseInputs I = upload_ge_volume(C, Pg, in, v, acq, &d_lw, st);
+    const ShotVariants V = upload_sets(C, Pg, {v.sets}, {v.n_sets}, g, st);
     for (int e = 0; e < n_echoes; ++e) {
       const double te = train.echo_times_ms[e];
       ge_echo(Pg, acq, te);
@@ -726,7 +837,7 @@ void ge_acquire(mrsim_context* ctx, const mrsim_acquisition_ge_input& in, const 
       ae.t_echo = te;
       DevArena E;
       float2* k3 = (float2*)E.alloc((size_t)nc * nz * per * sizeof(float2));
-      grase_kspace(Pg, I, ae, in.phase, d_lw, 0, 1, Pg.mask, k3, st);
+      grase_kspace(Pg, I, ae, in.phase, d_lw, 0, 1, Pg.mask, k3, st, &V);
       // the noise and spikes of echo e on its own streams (echo 0 unsalted)
       grase_noise(E, Pg, k3, g, g + 1, seed ^ echo_salt((uint64_t)e), Pg.mask, acq, st);
       float2* sl = (float2*)E.alloc((size_t)nz * nc * per * sizeof(float2));

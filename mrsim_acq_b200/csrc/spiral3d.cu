@@ -187,10 +187,12 @@ struct ZArgs {
   const float* lw;        // [g][shot][c] or NULL
   const int* kzseg;       // [p]
   const unsigned char* acquired;  // [p]
+  const int* shot_var;    // [shot]: the image variant the shot saw (0: the volume's own), or NULL
   int nz, nsamp, ns, ncomp, nsrc, ring, kz_segments, n_shots, g;
 };
 
-// coil q = r ring + a: out[q][p][j] = sum_c lw (w_c sum_z k2[a][src][z][j] zkq[r][p][z])
+// coil q = r ring + a: out[q][p][j] = sum_c lw (w_c sum_z k2[var(shot)][a][src][z][j] zkq[r][p][z]), var
+// the images the sample's shot saw (`samples_rings` kspace3d.rs:1028-1051)
 __global__ void spiral_zdft_kernel(const ZArgs a) {
   const int p = blockIdx.y, q = blockIdx.z;
   const int r = q / a.ring, e = q % a.ring;
@@ -200,7 +202,8 @@ __global__ void spiral_zdft_kernel(const ZArgs a) {
       const int shot = (j / a.ns) * a.kz_segments + a.kzseg[p];
       for (int c = 0; c < a.ncomp; ++c) {
         const int s = a.src[c * a.nz + p];
-        const float2* K = a.k2 + ((size_t)(e * a.nsrc + s) * a.nz) * a.nsamp + j;
+        const int var = a.shot_var ? a.shot_var[shot] : 0;
+        const float2* K = a.k2 + ((size_t)((var * a.ring + e) * a.nsrc + s) * a.nz) * a.nsamp + j;
         float ar = 0.f, ai = 0.f;
         for (int z = 0; z < a.nz; ++z) {
           const float2 k = K[(size_t)z * a.nsamp];
@@ -750,20 +753,56 @@ static SpiralInputs upload_spiral_inputs(DevArena& A, const SpiralPlan3& P, cons
   return I;
 }
 
+// One volume's per-shot images (`ShotSet`, kspace3d.rs:59-65): variant 0 the volume's own
+// images, variant v > 0 its set v - 1; per shot the variant it saw (the first set holding it).
+struct SpiralVariants {
+  int nvar = 1;
+  std::vector<std::vector<const float*>> img;  // [v][c] device sim volumes (v > 0)
+  const int* d_shot_var = nullptr;             // [n_shots], or NULL without sets
+};
+
+static SpiralVariants spiral_sets(DevArena& A, const SpiralPlan3& P, const mrsim_acquisition_3d_input& in, int g,
+                                  cudaStream_t st, bool upload = true) {
+  SpiralVariants V;
+  if (!in.shot_sets || !in.n_shot_sets || in.n_shot_sets[g] <= 0) return V;
+  const mrsim_shot_set* sets = in.shot_sets[g];
+  const int64_t n = in.n_shot_sets[g];
+  if (!sets) fail("volume " + std::to_string(g) + ": its shot sets are NULL");
+  V.nvar = (int)n + 1;
+  V.img.assign((size_t)V.nvar, std::vector<const float*>(P.ncomp, nullptr));
+  std::vector<int> var((size_t)P.table.n_shots, 0);
+  for (int64_t i = n - 1; i >= 0; --i) {  // descending, so the first set holding a shot wins
+    const mrsim_shot_set& S = sets[i];
+    if (S.n_shots > 0 && !S.shots) fail("volume " + std::to_string(g) + ": a shot set's shots are NULL");
+    for (int64_t j = 0; j < S.n_shots; ++j) {
+      if (S.shots[j] < 0 || S.shots[j] >= P.table.n_shots)
+        fail("a shot index beyond the train's " + std::to_string(P.table.n_shots));
+      var[(size_t)S.shots[j]] = (int)i + 1;
+    }
+    for (int c = 0; c < P.ncomp; ++c) {
+      if (!S.images || !S.images[c]) fail("shot images are not per compartment");
+      if (upload) V.img[(size_t)i + 1][c] = (const float*)A.upload(S.images[c], P.nvox * 4, st);
+    }
+  }
+  if (upload) V.d_shot_var = (const int*)A.upload(var.data(), var.size() * 4, st);
+  return V;
+}
+
 // Every coil's samples of volume g before noise: out [q][p][nsamp].
 static void spiral_samples(const SpiralPlan3& P, const SpiralInputs& I, int g, const float* d_lw, float2* out,
-                           cudaStream_t st) {
+                           cudaStream_t st, const SpiralVariants* V = nullptr) {
   const int nsrc = (int)P.srcs.size(), nz = P.nz, nsamp = P.nsamp, ring = P.ring;
+  const int nvar = V ? V->nvar : 1;
   DevArena C;
   NufftGrid grid = make_nufft<float>(C, P.snx, P.sny, -P.o * (P.n / 2), -P.o * (P.n / 2), P.snx, P.sny, 1e-12, st);
   const double* d_k = (const double*)C.upload(P.table.traj.k.data(), P.table.traj.k.size() * 8, st);
   const float2* d_stat = (const float2*)C.upload(P.stat.data(), P.stat.size() * sizeof(float2), st);
-  float2* k2 = (float2*)C.alloc((size_t)ring * nsrc * nz * nsamp * sizeof(float2));
-  MRSIM_CUDA(cudaMemsetAsync(k2, 0, (size_t)ring * nsrc * nz * nsamp * sizeof(float2), st));
+  float2* k2 = (float2*)C.alloc((size_t)nvar * ring * nsrc * nz * nsamp * sizeof(float2));
+  MRSIM_CUDA(cudaMemsetAsync(k2, 0, (size_t)nvar * ring * nsrc * nz * nsamp * sizeof(float2), st));
   // per slice: slots (a, s) with their plans
   int Lmax = 1;
   for (int z = 0; z < nz; ++z) Lmax = std::max({Lmax, P.class_plan[z].l, P.voxel_plan[z].l});
-  const int nslot = ring * nsrc;
+  const int nslot = nvar * ring * nsrc;
   float2* seg = (float2*)C.alloc((size_t)nslot * Lmax * P.plane * sizeof(float2));
   float2* segout = (float2*)C.alloc((size_t)nslot * Lmax * nsamp * sizeof(float2));
   float2* work = (float2*)C.alloc((size_t)nslot * Lmax * grid.nf0 * grid.nf1 * sizeof(float2));
@@ -778,14 +817,16 @@ static void spiral_samples(const SpiralPlan3& P, const SpiralInputs& I, int g, c
     std::vector<int> base(nslot), plan(nslot);
     std::vector<size_t> off(nslot);
     int tot = 0;
+    for (int v = 0; v < nvar; ++v)
     for (int a = 0; a < ring; ++a)
       for (int s = 0; s < nsrc; ++s) {
-        const int i = a * nsrc + s;
+        const int i = (v * ring + a) * nsrc + s;
         const SpiralPlan3::Src& S = P.srcs[s];
         const bool voxel = P.modes[S.c].voxel;
         SegSlot& sl = slots[i];
         std::memset(&sl, 0, sizeof sl);
-        sl.comp = I.img + (((size_t)g * nz + z) * P.ncomp + S.c) * P.plane;
+        sl.comp = v > 0 ? V->img[(size_t)v][S.c] + (size_t)z * P.plane
+                        : I.img + (((size_t)g * nz + z) * P.ncomp + S.c) * P.plane;
         sl.amp = I.amp + (size_t)a * P.plane;
         sl.plan = voxel ? 1 : 0;
         if (voxel) {
@@ -796,7 +837,7 @@ static void spiral_samples(const SpiralPlan3& P, const SpiralInputs& I, int g, c
         base[i] = tot;
         plan[i] = sl.plan;
         tot += voxel ? pv.l : pc.l;
-        off[i] = (((size_t)a * nsrc + s) * nz + z) * nsamp;
+        off[i] = ((((size_t)v * ring + a) * nsrc + s) * nz + z) * nsamp;
       }
     if (tot == 0) continue;
     MRSIM_CUDA(cudaMemcpyAsync(d_slots, slots.data(), slots.size() * sizeof(SegSlot), cudaMemcpyHostToDevice, st));
@@ -850,6 +891,7 @@ static void spiral_samples(const SpiralPlan3& P, const SpiralInputs& I, int g, c
   za.kz_segments = P.table.kz_segments;
   za.n_shots = P.table.n_shots;
   za.g = g;
+  za.shot_var = V ? V->d_shot_var : nullptr;
   spiral_zdft_kernel<<<g3(nsamp, nz, P.nc), 256, 0, st>>>(za);
   MRSIM_CUDA(cudaGetLastError());
   MRSIM_CUDA(cudaStreamSynchronize(st));
@@ -1037,7 +1079,9 @@ void spiral3d_samples(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, 
     d_lw = (const float*)A.upload(lw.data(), std::max<size_t>(1, lw.size()) * 4, st);
   }
   float2* k = (float2*)A.alloc((size_t)P.nc * P.nz * P.nsamp * sizeof(float2));
-  spiral_samples(P, I, g, d_lw, k, st);
+  for (int h = 0; h < (int)in.n_volumes; ++h) (void)spiral_sets(A, P, in, h, st, false);  // every volume's sets checked
+  const SpiralVariants V = spiral_sets(A, P, in, g, st);
+  spiral_samples(P, I, g, d_lw, k, st, &V);
   MRSIM_CUDA(cudaMemcpyAsync(out, k, (size_t)P.nc * P.nz * P.nsamp * sizeof(float2), cudaMemcpyDeviceToHost, st));
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
@@ -1051,6 +1095,7 @@ void spiral3d_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, 
   const int nv = (int)in.n_volumes, nz = P.nz, nc = P.nc, n = P.n, nsamp = P.nsamp;
   const double sigma = std::sqrt(acq.noise_variance / (double)((size_t)n * n));
   DevArena A;
+  for (int g = 0; g < nv; ++g) (void)spiral_sets(A, P, in, g, st, false);  // every volume's sets checked first
   SpiralInputs I = upload_spiral_inputs(A, P, in, in.images, nv, acq, st);
   const float* d_lw = nullptr;
   if (in.line_weights) {
@@ -1102,7 +1147,8 @@ void spiral3d_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, 
   for (int g = 0; g < nv; ++g) {
     DevArena C;
     float2* k = (float2*)C.alloc((size_t)nc * nz * nsamp * sizeof(float2));
-    spiral_samples(P, I, g, d_lw, k, st);
+    const SpiralVariants V = spiral_sets(C, P, in, g, st);
+    spiral_samples(P, I, g, d_lw, k, st, &V);
     spiral_noise(C, P, P.table.acquired, k, g, seed, sigma, st);
     if (accel > 1) kz_fill(ctx, kzk, accel, k, nc, nz, nsamp);
     double2* vol = (double2*)C.alloc(nn * nz * sizeof(double2));

@@ -162,9 +162,36 @@ def grase_lines(train: EchoTrain, ro: GraseReadout, ny: int, nz: int) -> GraseTa
     return GraseTable(shot, echo, t, trf, pol, e_c.value, n_shots.value)
 
 
+@dataclasses.dataclass
+class ShotSet:
+    """`ShotSet` (kspace3d.rs:59-65): the images one set of shots of one volume saw (per-shot
+    motion), one simulation-grid volume (x + snx*(y + sny*z)) per compartment.  Every line (spiral:
+    interleave) of a shot in `shots` is computed from these images; a shot in several sets takes
+    the first."""
+
+    shots: Sequence[int]
+    images: Sequence[Optional[np.ndarray]]
+
+
+def shot_sets_c(sets: Sequence[ShotSet], keep: _Keep):
+    """A C array of `mrsim_shot_set` (None images stay NULL)."""
+    arr = (abi.ShotSet_ * max(1, len(sets)))()
+    for i, st in enumerate(sets):
+        sh = np.ascontiguousarray(st.shots, np.int64)
+        keep.append(sh)
+        ps = (abi.c_f32p * max(1, len(st.images)))()
+        for c, im in enumerate(st.images):
+            ps[c] = keep.f32(np.ravel(im)) if im is not None and np.size(im) > 0 else None
+        keep.append(ps)
+        arr[i] = abi.ShotSet_(sh.ctypes.data_as(C.POINTER(C.c_int64)), sh.size, ps)
+    keep.append(arr)
+    return arr
+
+
 def acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,
                            t_inhom: Optional[Sequence[T2]], phase: Optional[PhaseModel],
-                           line_weights: Optional[LineWeights], grappa_calibration, keep: _Keep):
+                           line_weights: Optional[LineWeights], grappa_calibration, keep: _Keep,
+                           shot_images: Optional[Sequence[Sequence[ShotSet]]] = None):
     s = abi.Acquisition3dInput_()
     for i in range(3):
         s.sim_dims[i] = int(sim_dims[i])
@@ -187,6 +214,19 @@ def acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2: Sequence[T
         s.has_grappa_calibration = 1
         s.grappa_calibration_images = keep.ptrs([np.ravel(a) for a in cal_images])
         s.grappa_calibration_seed = int(cal_seed) & 0xFFFFFFFFFFFFFFFF
+    if shot_images is not None:
+        if len(shot_images) != n_volumes:
+            raise ValueError("shot images per volume")
+        lists = (C.POINTER(abi.ShotSet_) * max(1, n_volumes))()
+        counts = np.zeros(max(1, n_volumes), np.int64)
+        for g, sets in enumerate(shot_images):
+            if sets:
+                lists[g] = C.cast(shot_sets_c(sets, keep), C.POINTER(abi.ShotSet_))
+                counts[g] = len(sets)
+        keep.append(lists)
+        keep.append(counts)
+        s.shot_sets = lists
+        s.n_shot_sets = counts.ctypes.data_as(C.POINTER(C.c_int64))
     return s
 
 
@@ -194,13 +234,14 @@ def simulate_acquisition_3d(sim_dims, acq_dims, n_volumes: int, images, t2: Sequ
                             fmap, t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain,
                             readout, line_weights: Optional[LineWeights] = None,
                             phase: Optional[PhaseModel] = None, seed: int = 0, grappa_calibration=None,
-                            kz_opts: Optional[KzOptions] = None, ctx: Optional[Context] = None):
+                            kz_opts: Optional[KzOptions] = None, ctx: Optional[Context] = None,
+                            shot_images: Optional[Sequence[Sequence[ShotSet]]] = None):
     """`simulate_acquisition_3d` / `_kz` (kspace3d.rs:549-589), GRASE or stack of spirals:
-    (magnitude, phase) f32 at vox * nv + g."""
+    (magnitude, phase) f32 at vox * nv + g.  `shot_images`: per volume its ShotSets, or None."""
     ctx = ctx or default_context()
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
-                               grappa_calibration, keep)
+                               grappa_calibration, keep, shot_images)
     n = int(np.prod(acq_dims)) * n_volumes
     mag, ph = np.zeros(n, np.float32), np.zeros(n, np.float32)
     if isinstance(readout, SpiralReadout):
@@ -221,12 +262,13 @@ def simulate_acquisition_3d(sim_dims, acq_dims, n_volumes: int, images, t2: Sequ
 def spiral_samples_3d(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,
                       t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain, readout: SpiralReadout,
                       line_weights: Optional[LineWeights] = None, phase: Optional[PhaseModel] = None, g: int = 0,
-                      kz_opts: Optional[KzOptions] = None, ctx: Optional[Context] = None) -> np.ndarray:
+                      kz_opts: Optional[KzOptions] = None, ctx: Optional[Context] = None,
+                      shot_images: Optional[Sequence[Sequence[ShotSet]]] = None) -> np.ndarray:
     """`SpiralPlan::samples_all` (kspace3d.rs:1047-1060): complex64 [coil, partition, sample] before noise."""
     ctx = ctx or default_context()
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
-                               None, keep)
+                               None, keep, shot_images)
     nz = acq_dims[2]
     tab = spiral_lines(train, readout, acq_dims[0], acq_dims[1], nz)
     nsamp = tab.samples_per_interleaf * readout.interleaves
@@ -242,12 +284,13 @@ def spiral_samples_3d(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T
 def kspace_3d_observed(sim_dims, acq_dims, n_volumes: int, images, t2: Sequence[T2], t1: Optional[Sequence[T2]], fmap,
                        t_inhom: Optional[Sequence[T2]], acq: Acquisition, train: EchoTrain, readout: GraseReadout,
                        line_weights: Optional[LineWeights] = None, phase: Optional[PhaseModel] = None, g: int = 0,
-                       ctx: Optional[Context] = None) -> np.ndarray:
+                       ctx: Optional[Context] = None,
+                       shot_images: Optional[Sequence[Sequence[ShotSet]]] = None) -> np.ndarray:
     """`kspace_3d_observed` (kspace3d.rs:439-456): complex64 [coil, p, ky, kx] of volume g."""
     ctx = ctx or default_context()
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
-                               None, keep)
+                               None, keep, shot_images)
     nx, ny, nz = acq_dims
     nc = max(int(acq.n_coils), 1)
     out = np.zeros(nc * nz * ny * nx, np.complex64)
@@ -293,11 +336,12 @@ class Ge3dReadout:
 
 @dataclasses.dataclass
 class GeVolume:
-    """`GeVolume` (kspace3d.rs:592-603): per compartment one sim volume (None = unused) and the
-    excitation weights w[(p * ky_segments + sy) * ncomp + c]."""
+    """`GeVolume` (kspace3d.rs:592-603): per compartment one sim volume (None = unused), the
+    excitation weights w[(p * ky_segments + sy) * ncomp + c] and the per-shot images."""
 
     images: Sequence[Optional[np.ndarray]]
     weights: np.ndarray
+    shot_images: Optional[Sequence[ShotSet]] = None
 
 
 @dataclasses.dataclass
@@ -344,6 +388,9 @@ class _GeVolumes:
         keep.append(ps)
         out.images = ps
         out.weights = keep.f64(np.ravel(v.weights))
+        if v.shot_images:
+            out.shot_sets = C.cast(shot_sets_c(v.shot_images, keep), C.POINTER(abi.ShotSet_))
+            out.n_shot_sets = len(v.shot_images)
         return out
 
     def _call(self, g, user, out):

@@ -2390,6 +2390,31 @@ double line_weight_o(double ln_a, double t, double t2, double t2p) {
   return std::exp(ln_a - d2 - dp);
 }
 
+// The first shot set holding `shot` (`sets.iter().position(|s| s.shots.contains(&shot))`,
+// kspace3d.rs:216), or -1.
+int set_of(const mrsim_shot_set* sets, size_t n_sets, int64_t shot) {
+  for (size_t i = 0; i < n_sets; ++i)
+    for (int64_t j = 0; j < sets[i].n_shots; ++j)
+      if (sets[i].shots[j] == shot) return (int)i;
+  return -1;
+}
+// The shot-image checks (kspace3d.rs:369-377): every set's shots inside the train.
+void check_sets(const mrsim_shot_set* sets, size_t n_sets, int64_t n_shots) {
+  for (size_t i = 0; i < n_sets; ++i)
+    for (int64_t j = 0; j < sets[i].n_shots; ++j)
+      if (sets[i].shots[j] < 0 || sets[i].shots[j] >= n_shots)
+        throw std::runtime_error("a shot index beyond the train's " + std::to_string(n_shots));
+}
+const mrsim_shot_set* sets_of(const mrsim_acquisition_3d_input& in, size_t g) {
+  return in.shot_sets && in.n_shot_sets ? in.shot_sets[g] : nullptr;
+}
+size_t n_sets_of(const mrsim_acquisition_3d_input& in, size_t g) {
+  return in.shot_sets && in.n_shot_sets ? (size_t)in.n_shot_sets[g] : 0;
+}
+void check_all_sets(const mrsim_acquisition_3d_input& in, int64_t n_shots) {
+  for (int64_t g = 0; g < in.n_volumes; ++g) check_sets(sets_of(in, (size_t)g), n_sets_of(in, (size_t)g), n_shots);
+}
+
 struct Plan3 {
   size_t snx, sny, nz, nx, ny, o, ncomp;
   mrsim_acquisition acq;
@@ -2484,19 +2509,26 @@ struct Plan3 {
     return out;
   }
 
-  // `Plan::kspace` kspace3d.rs:206-232 (no shot images)
+  // `Plan::kspace` kspace3d.rs:206-232: each line from the images its shot saw (the first set
+  // holding the shot, else the volume's own)
   std::vector<Cx> kspace(const float* const* images, size_t n_volumes, size_t g, size_t q, size_t ncoils,
-                         const double* lw) const {
+                         const double* lw, const mrsim_shot_set* sets = nullptr, size_t n_sets = 0) const {
     auto base = compartments([&](size_t c, size_t v) { return images[c][v * n_volumes + g]; }, q, ncoils);
+    std::vector<std::vector<std::vector<Cx>>> moved(n_sets);
+    for (size_t i = 0; i < n_sets; ++i)
+      moved[i] = compartments([&](size_t c, size_t v) { return sets[i].images[c][v]; }, q, ncoils);
     std::vector<Cx> k(nz * ny * nx, Cx{0, 0});
     for (size_t p = 0; p < nz; ++p)
       for (size_t ky = 0; ky < ny; ++ky) {
         const GLine& L = table.line(p, ky);
+        const std::vector<std::vector<Cx>>* src = &base;
+        const int si = set_of(sets, n_sets, (int64_t)L.shot);
+        if (si >= 0) src = &moved[(size_t)si];
         for (size_t c = 0; c < ncomp; ++c) {
           double w = lw ? lw[(g * table.n_shots + L.shot) * ncomp + c] : 1.0;
           for (size_t kx = 0; kx < nx; ++kx) {
             size_t i = (p * ny + ky) * nx + kx;
-            k[i] = cadd(k[i], cscale(base[c][i], w));
+            k[i] = cadd(k[i], cscale((*src)[c][i], w));
           }
         }
         if (!mask[ky * nx])
@@ -2537,6 +2569,7 @@ Plan3 plan3(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq, 
       P.zk[p * P.nz + z] = Cx{std::cos(th), std::sin(th)};
     }
   P.mask = sampling_mask(P.nx, P.ny, acq);
+  check_all_sets(in, (int64_t)P.table.n_shots);
   return P;
 }
 
@@ -2626,7 +2659,7 @@ std::vector<std::vector<Cx>> acquire_3d_o(const mrsim_acquisition_3d_input& in, 
   parallel_for(nv, threads, [&](size_t g) {
     std::vector<std::vector<std::vector<Cx>>> parts(ncoils);
     for (size_t q = 0; q < ncoils; ++q) {
-      std::vector<Cx> k = pl.kspace(in.images, nv, g, q, ncoils, in.line_weights);
+      std::vector<Cx> k = pl.kspace(in.images, nv, g, q, ncoils, in.line_weights, sets_of(in, g), n_sets_of(in, g));
       parts[q] = partitions_to_slices_o(k, pl.mask, pl.zk, nx, ny, nz, g, q, seed, acq, sigma);
     }
     std::vector<Cx> out(nx * ny * nz);
@@ -2794,11 +2827,16 @@ struct SpiralPlanO {
   }
 
   // `samples_all` (kspace3d.rs:1014-1060): out[q] with q = r ring + a
-  std::vector<std::vector<Cx>> samples_all(const float* const* images, size_t nv, size_t g, const double* lw) const {
+  // `samples_rings` kspace3d.rs:1028-1051: each sample from the images its shot saw
+  std::vector<std::vector<Cx>> samples_all(const float* const* images, size_t nv, size_t g, const double* lw,
+                                           const mrsim_shot_set* sets = nullptr, size_t n_sets = 0) const {
     size_t nsamp = table.nsamp;
     std::vector<std::vector<Cx>> out(ring * rows);
     for (size_t a = 0; a < ring; ++a) {
       auto base = compartments([&](size_t c, size_t v) { return images[c][v * nv + g]; }, a);
+      std::vector<decltype(base)> moved;
+      for (size_t si = 0; si < n_sets; ++si)
+        moved.push_back(compartments([&](size_t c, size_t v) { return sets[si].images[c][v]; }, a));
       for (size_t r = 0; r < rows; ++r) {
         std::vector<Cx> k(nz * nsamp, Cx{0, 0});
         for (size_t p = 0; p < nz; ++p) {
@@ -2806,9 +2844,11 @@ struct SpiralPlanO {
           for (size_t j = 0; j < nsamp; ++j) {
             size_t shot = (j / table.ns) * table.kz_segments + table.kz_segment[p];
             size_t i = p * nsamp + j;
+            const int si = set_of(sets, n_sets, (int64_t)shot);
+            const auto& src = si >= 0 ? moved[(size_t)si] : base;
             for (size_t c = 0; c < ncomp; ++c) {
               double w = lw ? lw[(g * table.n_shots + shot) * ncomp + c] : 1.0;
-              k[i] = cadd(k[i], cscale(base[r][c][i], w));
+              k[i] = cadd(k[i], cscale(src[r][c][i], w));
             }
           }
         }
@@ -2985,6 +3025,7 @@ std::vector<std::vector<Cx>> spiral_volumes_o(const mrsim_acquisition_3d_input& 
   pl.ring = ncoils / pl.rows;
   pl.acq = acq;
   pl.table = spiral_table_o(tr, ro, pl.n, pl.nz);
+  check_all_sets(in, (int64_t)pl.table.n_shots);
   pl.modes = resolve_modes_o(in.t2, in.t1, in.t_inhom, pl.ncomp, acq, tr, pl.snx * pl.sny * pl.nz);
   pl.t2 = in.t2;
   pl.ti = in.t_inhom;
@@ -3022,7 +3063,7 @@ std::vector<std::vector<Cx>> spiral_volumes_o(const mrsim_acquisition_3d_input& 
   SpiralReconO rec(pl.table.k.data(), nsamp, n, wa, 80, 100.0, true);
   std::vector<std::vector<Cx>> vols(nv);
   parallel_for(nv, threads, [&](size_t g) {
-    auto coil_k = pl.samples_all(in.images, nv, g, in.line_weights);
+    auto coil_k = pl.samples_all(in.images, nv, g, in.line_weights, sets_of(in, g), n_sets_of(in, g));
     if (acq.noise_variance > 0.0)
       for (size_t q = 0; q < coil_k.size(); ++q) spiral_noise_o(coil_k[q], pl.table.acquired, nsamp, g, q, seed, sigma);
     if (accel) kzk.fill(pl.table, coil_k, nsamp);
@@ -3079,22 +3120,48 @@ std::vector<std::vector<Cx>> spiral_volumes_o(const mrsim_acquisition_3d_input& 
 // ============================ the 3D gradient-echo train ==================================
 // readout.rs:356-450 (`ExcitationTrain`, `ge3d_lines`), kspace3d.rs:590-856 (`GePlan`,
 // `simulate_acquisition_3d_ge_complex`).
+struct GeSetO {
+  std::vector<int64_t> shots;
+  std::vector<std::vector<float>> images;
+};
 struct GeVolO {
   std::vector<std::vector<float>> images;  // empty = unused
   std::vector<double> weights;
+  std::vector<GeSetO> sets;                // `shot_images`
 };
 
-GeVolO ge_copy(const mrsim_ge_volume& v, size_t ncomp, size_t nvox, size_t n_exc_lines) {
+// `GeVolume` with its shot images (kspace3d.rs:592-603; checks kspace3d.rs:801-807); the
+// reference scan takes none (`shot_images: None`, kspace3d.rs:775).
+GeVolO ge_copy(const mrsim_ge_volume& v, size_t ncomp, size_t nvox, size_t n_exc_lines, size_t g = 0,
+               int64_t n_shots = 0, bool with_sets = false) {
   GeVolO o;
   o.images.resize(ncomp);
   for (size_t c = 0; c < ncomp; ++c)
     if (v.images[c]) o.images[c].assign(v.images[c], v.images[c] + nvox);
   o.weights.assign(v.weights, v.weights + n_exc_lines);
+  if (with_sets && v.shot_sets)
+    for (int64_t i = 0; i < v.n_shot_sets; ++i) {
+      const mrsim_shot_set& ss = v.shot_sets[i];
+      GeSetO so;
+      so.shots.assign(ss.shots, ss.shots + ss.n_shots);
+      so.images.resize(ncomp);
+      for (size_t c = 0; c < ncomp; ++c) {
+        const bool has = ss.images && ss.images[c];
+        if (has != (v.images[c] != nullptr))
+          throw std::runtime_error("volume " + std::to_string(g) + ": shot images are not the volume's compartments");
+        if (has) so.images[c].assign(ss.images[c], ss.images[c] + nvox);
+      }
+      for (int64_t x : so.shots)
+        if (x < 0 || x >= n_shots) throw std::runtime_error("a shot index beyond the train's " + std::to_string(n_shots));
+      o.sets.push_back(std::move(so));
+    }
   return o;
 }
 
 struct GePlanO {
   size_t snx, sny, nz, nx, ny, o, ncomp, kys;
+  std::vector<int64_t> line_shot;  // [p][ky]: `ge3d_lines` shot sy * kz_segments + sz (readout.rs:440-450)
+  int64_t n_shots = 0;
   mrsim_acquisition acq;
   std::vector<double> t_ms;
   std::vector<int8_t> pol;
@@ -3170,19 +3237,33 @@ struct GePlanO {
     return out;
   }
 
+  // `GePlan::kspace` kspace3d.rs:697-728: each line from the images its shot saw
   std::vector<Cx> kspace(const GeVolO& vol, size_t q, size_t ncoils, double te) const {
     auto base = compartments(vol, q, ncoils, te);
+    std::vector<std::vector<std::vector<Cx>>> moved;
+    for (const GeSetO& st : vol.sets) {
+      GeVolO sv;
+      sv.images = st.images;
+      moved.push_back(compartments(sv, q, ncoils, te));
+    }
     std::vector<Cx> k(nz * ny * nx, Cx{0, 0});
     for (size_t p = 0; p < nz; ++p)
       for (size_t ky = 0; ky < ny; ++ky) {
         if (!mask[ky * nx]) continue;
         size_t sy = ky % kys;
+        const std::vector<std::vector<Cx>>* src = &base;
+        const int64_t shot = line_shot[p * ny + ky];
+        for (size_t i = 0; i < vol.sets.size(); ++i)
+          if (std::find(vol.sets[i].shots.begin(), vol.sets[i].shots.end(), shot) != vol.sets[i].shots.end()) {
+            src = &moved[i];
+            break;
+          }
         for (size_t c = 0; c < ncomp; ++c) {
           if (vol.images[c].empty()) continue;
           double w = vol.weights[(p * kys + sy) * ncomp + c];
           for (size_t kx = 0; kx < nx; ++kx) {
             size_t i = (p * ny + ky) * nx + kx;
-            k[i] = cadd(k[i], cscale(base[c][i], w));
+            k[i] = cadd(k[i], cscale((*src)[c][i], w));
           }
         }
       }
@@ -3203,6 +3284,16 @@ std::vector<std::vector<std::vector<Cx>>> ge_volumes_o(const mrsim_acquisition_g
   pl.ncomp = in.ncomp;
   pl.kys = (size_t)ro.ky_segments;
   pl.acq = acq;
+  {
+    const size_t kzs = (size_t)tr.kz_segments;
+    std::vector<size_t> order = kz_order_o(pl.nz, tr.kz_order), pos(pl.nz, 0);
+    for (size_t i = 0; i < order.size(); ++i) pos[order[i]] = i;
+    pl.line_shot.resize(pl.nz * pl.ny);
+    for (size_t p = 0; p < pl.nz; ++p)
+      for (size_t ky = 0; ky < pl.ny; ++ky)
+        pl.line_shot[p * pl.ny + ky] = (int64_t)((ky % pl.kys) * kzs + pos[p] % kzs);
+    pl.n_shots = (int64_t)(pl.kys * kzs);
+  }
   size_t epi = pl.ny / pl.kys;
   for (size_t ky = 0; ky < pl.ny; ++ky) {  // `grase_block`
     size_t j = ky / pl.kys, a = ro.reverse_phase ? j : epi - 1 - j;
@@ -3233,7 +3324,7 @@ std::vector<std::vector<std::vector<Cx>>> ge_volumes_o(const mrsim_acquisition_g
     mrsim_ge_volume v;
     std::memset(&v, 0, sizeof v);
     if (in.volume((int64_t)g, in.user, &v) != 0) throw Fail("the volume callback failed");
-    vols[g] = ge_copy(v, pl.ncomp, nvox, n_exc_lines);
+    vols[g] = ge_copy(v, pl.ncomp, nvox, n_exc_lines, g, pl.n_shots, true);
   }
   std::vector<std::vector<GrappaKernel>> kernels(n_echoes);
   if (acq.accel > 1 && nv > 0) {
@@ -3609,7 +3700,8 @@ int oracle_kspace_3d_observed(const mrsim_acquisition_3d_input* in, const mrsim_
     Plan3 pl = plan3(*in, *acq, *tr, *ro);
     size_t ncoils = std::max<int64_t>(acq->n_coils, 1), per = pl.nz * pl.ny * pl.nx;
     for (size_t q = 0; q < ncoils; ++q) {
-      std::vector<Cx> k = pl.kspace(in->images, in->n_volumes, (size_t)g, q, ncoils, in->line_weights);
+      std::vector<Cx> k = pl.kspace(in->images, in->n_volumes, (size_t)g, q, ncoils, in->line_weights,
+                                    sets_of(*in, (size_t)g), n_sets_of(*in, (size_t)g));
       put_cx(k, out + 2 * per * q);
     }
   });
@@ -3668,6 +3760,7 @@ int oracle_spiral_samples_3d(const mrsim_acquisition_3d_input* in, const mrsim_a
     pl.ring = ncoils / pl.rows;
     pl.acq = *acq;
     pl.table = spiral_table_o(*tr, *ro, pl.n, pl.nz);
+    check_all_sets(*in, (int64_t)pl.table.n_shots);
     pl.modes = resolve_modes_o(in->t2, in->t1, in->t_inhom, pl.ncomp, *acq, *tr, pl.snx * pl.sny * pl.nz);
     pl.t2 = in->t2;
     pl.ti = in->t_inhom;
@@ -3679,7 +3772,8 @@ int oracle_spiral_samples_3d(const mrsim_acquisition_3d_input* in, const mrsim_a
     for (size_t p = 0; p < pl.nz; ++p)
       for (size_t z = 0; z < pl.nz; ++z)
         pl.zk[p * pl.nz + z] = ccis(TAU * ((double)p - zs) * ((double)z - zs) / (double)pl.nz);
-    auto s = pl.samples_all(in->images, in->n_volumes, (size_t)g, in->line_weights);
+    auto s = pl.samples_all(in->images, in->n_volumes, (size_t)g, in->line_weights, sets_of(*in, (size_t)g),
+                            n_sets_of(*in, (size_t)g));
     size_t per = pl.nz * pl.table.nsamp;
     for (size_t q = 0; q < s.size(); ++q) put_cx(s[q], out + 2 * per * q);
   });

@@ -450,12 +450,12 @@ def grase_lines(train, ro, ny: int, nz: int) -> dict:
 
 
 def kspace_3d_observed(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition, train, ro,
-                       line_weights=None, phase=None, g: int = 0) -> np.ndarray:
+                       line_weights=None, phase=None, g: int = 0, shot_images=None) -> np.ndarray:
     """`kspace_3d_observed` (kspace3d.rs:439-456), FP64: complex128 [coil, p, ky, kx]."""
     from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
-                               None, keep)
+                               None, keep, shot_images)
     nx, ny, nz = acq_dims
     nc = max(acq.n_coils, 1)
     out = np.zeros(nc * nz * ny * nx, np.complex128)
@@ -465,13 +465,14 @@ def kspace_3d_observed(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_in
 
 
 def simulate_acquisition_3d(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition, train, ro,
-                            line_weights=None, phase=None, seed: int = 0, grappa_calibration=None, threads: int = 0):
+                            line_weights=None, phase=None, seed: int = 0, grappa_calibration=None, threads: int = 0,
+                            shot_images=None):
     """`simulate_acquisition_3d` (kspace3d.rs:549-589), FP64: (complex volumes [g, vox], mag, phase)."""
     import os
     from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
-                               grappa_calibration, keep)
+                               grappa_calibration, keep, shot_images)
     nvox = int(np.prod(acq_dims))
     vols = np.zeros(n_volumes * nvox, np.complex128)
     mag, ph = np.zeros(nvox * n_volumes, np.float32), np.zeros(nvox * n_volumes, np.float32)
@@ -506,12 +507,12 @@ def _kz_c(kz_opts, keep):
 
 
 def spiral_samples_3d(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition, train, ro,
-                      line_weights=None, phase=None, g: int = 0, kz_opts=None) -> np.ndarray:
+                      line_weights=None, phase=None, g: int = 0, kz_opts=None, shot_images=None) -> np.ndarray:
     """`SpiralPlan::samples_all` with the exact in-plane sum, FP64: complex128 [coil, partition, sample]."""
     from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
-                               None, keep)
+                               None, keep, shot_images)
     nz = acq_dims[2]
     tab = spiral_lines(train, ro, acq_dims[0], nz)
     nsamp = len(tab["k"])
@@ -524,13 +525,13 @@ def spiral_samples_3d(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inh
 
 def simulate_acquisition_3d_spiral(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, acq: Acquisition,
                                    train, ro, line_weights=None, phase=None, seed: int = 0, kz_opts=None,
-                                   threads: int = 0):
+                                   threads: int = 0, shot_images=None):
     """`spiral_volumes` (kspace3d.rs:1472-1569), FP64: (complex volumes [g, vox], mag, phase)."""
     import os
     from mrsim_acq_b200.kspace3d import acquisition_3d_input_c
     keep = _Keep()
     s = acquisition_3d_input_c(sim_dims, acq_dims, n_volumes, images, t2, t1, fmap, t_inhom, phase, line_weights,
-                               None, keep)
+                               None, keep, shot_images)
     nvox = int(np.prod(acq_dims))
     vols = np.zeros(n_volumes * nvox, np.complex128)
     mag, ph = np.zeros(nvox * n_volumes, np.float32), np.zeros(nvox * n_volumes, np.float32)

@@ -118,3 +118,50 @@ def test_refusals(gpu_ctx):
         run(ro=grase(2, 0.5, True))
     with pytest.raises(MrsimError, match="echo train length"):
         run(tr=K3.EchoTrain(etl=5, esp_ms=20.0, refocusing_deg=150.0, kz_segments=2))
+
+
+def moved_sets(images, nv, snx, sny, nz, g):
+    """Two shot sets of volume g: shot 1 sees the volume shifted by a voxel along x and scaled,
+    shots 0 and 1 see it scaled the other way (shot 1 takes the first set)."""
+    own = [im[g::nv].reshape(nz, sny, snx) for im in images]
+    a = [np.roll(v, 1, axis=2).ravel() * np.float32(1.1) for v in own]
+    b = [v.ravel() * np.float32(0.8) for v in own]
+    return [K3.ShotSet([1], a), K3.ShotSet([0, 1], b)]
+
+
+@pytest.mark.parametrize("name", ["class", "voxel", "grappa", "noise"])
+def test_shot_images_match_the_oracle(gpu_ctx, name):
+    """Per-shot images (`ShotSet`): volume 0 with two overlapping sets, volume 1 with none; the
+    observed k-space and the reconstructed volumes against the oracle."""
+    c = case(name)
+    snx, sny, nz = c["sim"]
+    sets = [moved_sets(c["images"], c["nv"], snx, sny, nz, 0), []]
+    args = (c["sim"], c["acqd"], c["nv"], c["images"], c["t2"], c["t1"], c["fmap"], c["ti"], c["acq"], c["tr"], c["ro"])
+    for g in range(c["nv"]):
+        got = K3.kspace_3d_observed(*args, line_weights=c["lw"], phase=c["phase"], g=g, ctx=gpu_ctx,
+                                    shot_images=sets)
+        want = O.kspace_3d_observed(*args, line_weights=c["lw"], phase=c["phase"], g=g, shot_images=sets)
+        assert rel_l2(got, want) <= 1e-5, (name, g)
+    mag, ph = K3.simulate_acquisition_3d(*args, line_weights=c["lw"], phase=c["phase"], seed=11, ctx=gpu_ctx,
+                                         shot_images=sets)
+    vols, _, _ = O.simulate_acquisition_3d(*args, line_weights=c["lw"], phase=c["phase"], seed=11, shot_images=sets)
+    z = mag.astype(np.float64) * np.exp(1j * ph.astype(np.float64))
+    assert rel_l2(z, vols.T.ravel()) <= 1e-5, name
+
+
+def test_shot_images_double_exactly_their_lines_on_the_device(gpu_ctx):
+    """Doubled images for shot 1 double exactly (bit for bit: a power-of-two scale commutes with
+    every rounding) the device's lines of shot 1 and leave the others unchanged."""
+    c = case("class")
+    snx, sny, nz = c["sim"]
+    args = (c["sim"], c["acqd"], c["nv"], c["images"], c["t2"], c["t1"], c["fmap"], c["ti"], c["acq"], c["tr"], c["ro"])
+    full = K3.kspace_3d_observed(*args, phase=c["phase"], g=0, ctx=gpu_ctx)
+    doubled = [2.0 * im[0::c["nv"]] for im in c["images"]]
+    moved = K3.kspace_3d_observed(*args, phase=c["phase"], g=0, ctx=gpu_ctx,
+                                  shot_images=[[K3.ShotSet([1], doubled)], []])
+    shot = K3.grase_lines(c["tr"], c["ro"], c["acqd"][1], nz).shot.reshape(nz, c["acqd"][1])
+    sel = np.broadcast_to((shot == 1)[None, :, :, None], full.shape)
+    assert np.array_equal(moved[sel], 2.0 * full[sel])
+    assert np.array_equal(moved[~sel], full[~sel])
+    with pytest.raises(MrsimError, match="a shot index beyond the train's"):
+        K3.kspace_3d_observed(*args, phase=c["phase"], g=0, ctx=gpu_ctx, shot_images=[[K3.ShotSet([99], doubled)], []])

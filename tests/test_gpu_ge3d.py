@@ -105,3 +105,29 @@ def test_ge3d_refusals(gpu_ctx):
     bad = lambda g: K3.GeVolume([vol(g).images[0], None], vol(g).weights)
     with pytest.raises(MrsimError, match="no image but a nonzero weight"):
         run(vol=bad)
+
+
+@pytest.mark.parametrize("name", ["class", "voxel", "unused", "grappa"])
+def test_ge3d_shot_images_match_the_oracle(gpu_ctx, name):
+    """`GeVolume::shot_images`: volume 0's shot 1 sees shifted images, shots 2 and 3 scaled ones
+    (a compartment the volume does not use has no set image either); the GRAPPA reference scan
+    takes none."""
+    c = case(name)
+    sim, acqd, nv, t2, fmap, ti, acq, tr, ro, vol = c["args"]
+    snx, sny, nz = sim
+
+    def with_sets(g):
+        v = vol(g)
+        if g != 0:
+            return v
+        own = [None if im is None else np.asarray(im).reshape(nz, sny, snx) for im in v.images]
+        a = [None if x is None else np.roll(x, 1, axis=1).ravel() * np.float32(1.2) for x in own]
+        b = [None if x is None else x.ravel() * np.float32(0.7) for x in own]
+        return K3.GeVolume(v.images, v.weights, [K3.ShotSet([1], a), K3.ShotSet([2, 3], b)])
+
+    args = (sim, acqd, nv, t2, fmap, ti, acq, tr, ro, with_sets)
+    got = K3.simulate_acquisition_3d_ge(*args, phase=c["phase"], seed=5, reference=c["ref"], ctx=gpu_ctx)
+    want, _ = O.simulate_acquisition_3d_ge(*args, phase=c["phase"], seed=5, reference=c["ref"])
+    for e, (mag, ph) in enumerate(got):
+        z = mag.astype(np.float64) * np.exp(1j * ph.astype(np.float64))
+        assert rel_l2(z, want[e].T.ravel()) <= 1e-5, (name, e)

@@ -133,3 +133,30 @@ def test_refusals(gpu_ctx):
         run(a, ro=spiral_ro(1.0, 2), tr=kz_train(4, kz, 130.0))
     with pytest.raises(MrsimError, match="at least as many coil rings"):
         run(a, ro=spiral_ro(1.0, 2), tr=kz_train(4, kz, 130.0), kzo=K3.KzOptions(coil_rows=1, calibration_images=c["images"]))
+
+
+@pytest.mark.parametrize("name", ["class", "voxel", "rings"])
+def test_spiral_shot_images_match_the_oracle(gpu_ctx, name):
+    """Per-shot images on the stack of spirals: volume 1's shot 1 sees shifted images, shots 2 and
+    3 scaled ones; samples and volumes against the oracle."""
+    c = case(name)
+    s, _, nz = c["sim"]
+    nv = c["nv"]
+
+    def sets(g):
+        own = [im[g::nv].reshape(nz, s, s) for im in c["images"]]
+        return [K3.ShotSet([1], [np.roll(x, 1, axis=2).ravel() * np.float32(1.1) for x in own]),
+                K3.ShotSet([2, 3], [x.ravel() * np.float32(0.75) for x in own])]
+
+    si = [[], sets(1)]
+    args = (c["sim"], c["acqd"], nv, c["images"], c["t2"], c["t1"], c["fmap"], c["ti"], c["acq"], c["tr"], c["ro"])
+    got = K3.spiral_samples_3d(*args, line_weights=c["lw"], phase=c["phase"], g=1, kz_opts=c["kzo"], ctx=gpu_ctx,
+                               shot_images=si)
+    want = O.spiral_samples_3d(*args, line_weights=c["lw"], phase=c["phase"], g=1, kz_opts=c["kzo"], shot_images=si)
+    assert rel_l2(got, want) <= 1e-5, name
+    mag, ph = K3.simulate_acquisition_3d(*args, line_weights=c["lw"], phase=c["phase"], seed=7, kz_opts=c["kzo"],
+                                         ctx=gpu_ctx, shot_images=si)
+    vols, _, _ = O.simulate_acquisition_3d_spiral(*args, line_weights=c["lw"], phase=c["phase"], seed=7,
+                                                  kz_opts=c["kzo"], shot_images=si)
+    z = mag.astype(np.float64) * np.exp(1j * ph.astype(np.float64))
+    assert rel_l2(z, vols.T.ravel()) <= 1e-5, name

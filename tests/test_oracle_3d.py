@@ -119,3 +119,36 @@ def test_refusals_name_the_input():
     with pytest.raises(RuntimeError, match="needs T1"):
         O.simulate_acquisition_3d([nx, ny, nz], [nx, ny, nz], 1, images, [T2.uniform(80.0)], None, fmap, None,
                                   Acquisition(), train(nz, 1, b=150.0), grase(1))
+
+
+def test_shot_images_double_exactly_their_lines():
+    """`shots_and_their_weights` (kspace3d.rs:1844-1901), the per-shot-images part: doubled images
+    for shot 1 of a two-segment GRASE train double exactly its lines (odd ky) at the observation
+    point and leave the others unchanged."""
+    nx = ny = 16
+    nz = 4
+    nvox = nx * ny * nz
+    vox = np.arange(nvox)
+    x, y = vox % nx, (vox // nx) % ny
+    img = np.where((x >= 5) & (x < 11) & (y >= 6) & (y < 10), 1.0 + 0.1 * x, 0.0).astype(np.float32)
+    fmap = np.zeros(nvox, np.float32)
+    acq = Acquisition(do_relaxation=False)
+    args = ([nx, ny, nz], [nx, ny, nz], 1, [img], [T2.uniform(80.0)], None, fmap, None, acq, train(nz, 1, b=180.0),
+            grase(2))
+    full = O.kspace_3d_observed(*args, phase=PhaseModel.none())[0]
+    moved = O.kspace_3d_observed(*args, phase=PhaseModel.none(),
+                                 shot_images=[[K3.ShotSet([1], [2.0 * img])]])[0]
+    odd = (np.arange(ny) % 2 == 1)[None, :, None]
+    assert np.all(np.abs(moved - 2.0 * full)[np.broadcast_to(odd, full.shape)] <= 1e-12)
+    assert np.array_equal(moved[np.broadcast_to(~odd, full.shape)], full[np.broadcast_to(~odd, full.shape)])
+
+
+def test_shot_images_refusals():
+    nx = ny = 8
+    nz = 4
+    nvox = nx * ny * nz
+    img = np.ones(nvox, np.float32)
+    args = ([nx, ny, nz], [nx, ny, nz], 1, [img], [T2.uniform(80.0)], None, np.zeros(nvox, np.float32), None,
+            Acquisition(do_relaxation=False), train(nz, 1, b=180.0), grase(2))
+    with pytest.raises(RuntimeError, match="a shot index beyond the train's 2"):
+        O.kspace_3d_observed(*args, shot_images=[[K3.ShotSet([2], [img])]])

@@ -149,3 +149,29 @@ def test_coil_rings_combine_to_the_single_ring_image():
     one, three = run(2, 1), run(6, 3)
     pk = np.abs(one).max()
     assert np.abs(one - three).max() <= 1e-9 * pk
+
+
+def test_spiral_shot_images_double_exactly_their_samples():
+    """`spiral_shots_select_exactly_their_samples` (kspace3d.rs:2103-2150), the shot-set part: with
+    3 interleaves x 2 kz segments, a set with doubled images for shot 4 (interleaf 2, kz segment
+    0) doubles exactly its own samples."""
+    n, nz, o, ncomp = 16, 4, 2, 2
+    s = n * o
+    images = blobs(s, s, nz, 1, ncomp)
+    fmap = spiral_fmap(s, s, nz)
+    t2 = [T2.uniform(80.0), T2.uniform(110.0)]
+    acq = Acquisition(do_relaxation=True, do_distortions=True, signal_scale=100.0)
+    tr = train(nz, 2, esp_ms=12.0, b=180.0)
+    ro = K3.SpiralReadout(3, 4.0, 0.01, 1.2, K3.KzSampling(1.0, 1))
+    args = ([s, s, nz], [n, n, nz], 1, images, t2, None, fmap, None, acq, tr, ro)
+    tab = O.spiral_lines(tr, ro, n, nz)
+    assert tab["n_shots"] == 6
+    base = O.spiral_samples_3d(*args, phase=PhaseModel.none())[0]
+    doubled = [2.0 * im for im in images]
+    moved = O.spiral_samples_3d(*args, phase=PhaseModel.none(), shot_images=[[K3.ShotSet([4], doubled)]])[0]
+    nsamp = base.shape[1]
+    ns = nsamp // 3
+    shot = (np.arange(nsamp)[None, :] // ns) * 2 + tab["kz_segment"][:, None]
+    f = np.where(shot == 4, 2.0, 1.0)
+    assert np.array_equal(moved, f * base)
+    assert np.count_nonzero(shot == 4) == ns * nz // 2
