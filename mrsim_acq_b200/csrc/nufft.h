@@ -51,11 +51,29 @@ template <class R>
 void nufft_type2(const NufftGridT<R>& g, const typename Vec2<R>::type* modes, int batch, size_t mode_stride,
                  const double* u, int npts, typename Vec2<R>::type* out, size_t out_stride,
                  typename Vec2<R>::type* work, int sign, const R* scale, cudaStream_t st);
-// Type 1 (nufft.rs:225-256): modes[b][m] = sum_j w[b][j] e^{sign i2pi (...)}.
+// The deterministic spread's fine-grid tiles and, per tile, the points whose kernel window can
+// reach it, in point order (CSR on the device, built on the host from the positions once per
+// point set).  A tile is 16 x 16 fine cells in 2D, 256 cells in 1D.
+constexpr int kSpreadTile = 16;
+constexpr int kSpreadTile1 = 256;
+struct NufftBins {
+  int tiles0 = 0, tiles1 = 0;
+  const int* start = nullptr;  // tiles0 * tiles1 + 1
+  const int* pts = nullptr;
+};
+struct DevArena;
+// 2D points u (npts x 2, period n per axis) on a fine grid of nf0 x nf1 cells, kernel width w
+NufftBins nufft_bins2(DevArena& A, int nf0, int nf1, int w, const double* u_host, int npts, cudaStream_t st);
+// 1D positions (cells, period n) on a fine grid of nf cells
+NufftBins nufft_bins1(DevArena& A, int nf, int w, const double* pos_host, int npos, cudaStream_t st);
+
+// Type 1 (nufft.rs:225-256): modes[b][m] = sum_j w[b][j] e^{sign i2pi (...)}.  The fine grid is
+// spread without atomics: each cell sums its points in point order (the reference's order), so
+// the result is the same on every run.  `bins` from nufft_bins2 over the same points.
 template <class R>
-void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const typename Vec2<R>::type* wts, int batch,
-                 size_t w_stride, typename Vec2<R>::type* modes, size_t mode_stride, typename Vec2<R>::type* work,
-                 int sign, cudaStream_t st);
+void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const NufftBins& bins,
+                 const typename Vec2<R>::type* wts, int batch, size_t w_stride, typename Vec2<R>::type* modes,
+                 size_t mode_stride, typename Vec2<R>::type* work, int sign, cudaStream_t st);
 
 // The 1D type-1 NUFFT (`Nufft1`, nufft.rs:25-112) in FP64: sources at `pos` (cells, period n),
 // outputs at integer frequencies k_lo .. k_lo + n_out, F[k] = sum_j w_j e^{+i2pi k pos_j / n}, for
@@ -66,8 +84,8 @@ struct Nufft1Grid {
   const double* corr;
   const double2* tw;
 };
-void nufft1_run(const Nufft1Grid& g, const double* pos, int npos, const double2* wts, int nw, double2* out,
-                double2* work, cudaStream_t st);
+void nufft1_run(const Nufft1Grid& g, const double* pos, int npos, const NufftBins& bins, const double2* wts, int nw,
+                double2* out, double2* work, cudaStream_t st);
 
 // The exact spiral sum (`spiral_kspace_exact`, spiral.rs:107-137) of one slice and coil.
 struct SpiralExactArgs {

@@ -1,7 +1,7 @@
 // nufft_kernels.cu — the 2D NUFFT pair of the stack-of-spirals path on the device (reference
 // `Nufft2`, nufft.rs:125-299): exponential-of-semicircle kernel exp(beta (sqrt(1 - z^2) - 1)),
 // beta = 2.30 w, w = ceil(-log10 tol) + 1 clamped to 2..16, oversampling 2, deapodization by the
-// kernel's sampled transform.  Type 1 spreads (FP32 atomics), type 2 interpolates; the fine-grid
+// kernel's sampled transform.  Type 1 spreads (tiles, in point order), type 2 interpolates; the fine-grid
 // FFT is a shared-memory radix-2 kernel (a direct DFT for lengths that are not powers of two).
 // Point positions and kernel offsets are formed in FP64 (the kernel is steep: an FP32 position
 // would cost ~1e-5 of relative accuracy); the taps and sums are FP32.
@@ -179,50 +179,102 @@ __global__ void interp_kernel(const NufftGridT<R> g, const typename Vec2<R>::typ
   }
 }
 
-// Type 1 spreading: grid += w_j * taps (atomics).
+// The wrapped offset of cell c from a window start a on a ring of n cells, in [0, n).
+__device__ __forceinline__ int ring_offset(int c, int a, int n) {
+  int d = c - a;
+  while (d < 0) d += n;
+  while (d >= n) d -= n;
+  return d;
+}
+
+constexpr int kSpreadChunk = 64;  // points whose taps a spread block holds at a time
+
+// Type 1 spreading without atomics: one block per 16 x 16 tile of the fine grid (one thread per
+// cell) and batch item.  The tile's points (nufft_bins2: every point whose window can reach the
+// tile, in point order) pass through shared memory in chunks with their taps; each thread adds
+// the contributions to its own cell point after point, cell += w_j (k0 k1) as the reference does
+// (nufft.rs:236-250), and stores the cell once.  The sum order is fixed, so the grid is the same
+// on every run; a window that wraps onto a cell twice (a fine grid narrower than the kernel) adds
+// both taps in tap order.
 template <class R>
-__global__ void spread_kernel(const NufftGridT<R> g, typename Vec2<R>::type* __restrict__ grid,
-                              const double* __restrict__ u, int npts, const typename Vec2<R>::type* __restrict__ wts,
-                              size_t grid_stride, size_t w_stride) {
+__global__ void __launch_bounds__(kSpreadTile * kSpreadTile)
+    spread_tile_kernel(const NufftGridT<R> g, typename Vec2<R>::type* __restrict__ grid, const double* __restrict__ u,
+                       const typename Vec2<R>::type* __restrict__ wts, size_t grid_stride, size_t w_stride,
+                       const NufftBins bins) {
   using V = typename Vec2<R>::type;
-  const int b = blockIdx.y;
-  V* G = grid + b * grid_stride;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npts; j += gridDim.x * blockDim.x) {
-    R k0[kWMax], k1[kWMax];
-    const int a0 = es_taps<R>(u[2 * j], g.nf0, g.w, g.beta, k0);
-    const int a1 = es_taps<R>(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
-    const V wv = wts[b * w_stride + j];
-    for (int i1 = 0; i1 < g.w; ++i1) {
-      const int c1 = wrap(a1 + i1, g.nf1);
-      R* row = reinterpret_cast<R*>(G + (size_t)g.nf0 * c1);
-      const R wr = wv.x * k1[i1], wi = wv.y * k1[i1];
-      for (int i0 = 0; i0 < g.w; ++i0) {
-        const int c0 = wrap(a0 + i0, g.nf0);
-        atomicAdd(row + 2 * c0, wr * k0[i0]);
-        atomicAdd(row + 2 * c0 + 1, wi * k0[i0]);
-      }
+  __shared__ R sk0[kSpreadChunk][kWMax], sk1[kSpreadChunk][kWMax];
+  __shared__ int sa0[kSpreadChunk], sa1[kSpreadChunk];
+  __shared__ V sw[kSpreadChunk];
+  const int b = blockIdx.y, tile = blockIdx.x;
+  const int c0 = (tile % bins.tiles0) * kSpreadTile + (int)threadIdx.x % kSpreadTile;
+  const int c1 = (tile / bins.tiles0) * kSpreadTile + (int)threadIdx.x / kSpreadTile;
+  const bool mine = c0 < g.nf0 && c1 < g.nf1;
+  const int w = g.w;
+  R re = 0, im = 0;
+  const int p0 = bins.start[tile], p1 = bins.start[tile + 1];
+  for (int base = p0; base < p1; base += kSpreadChunk) {
+    const int n = min(kSpreadChunk, p1 - base);
+    if ((int)threadIdx.x < n) {
+      const int t = threadIdx.x, j = bins.pts[base + t];
+      sa0[t] = es_taps<R>(u[2 * j], g.nf0, w, g.beta, sk0[t]);
+      sa1[t] = es_taps<R>(u[2 * j + 1], g.nf1, w, g.beta, sk1[t]);
+      sw[t] = wts[b * w_stride + j];
     }
+    __syncthreads();
+    if (mine)
+      for (int q = 0; q < n; ++q) {
+        const int d0 = ring_offset(c0, sa0[q], g.nf0);
+        if (d0 >= w) continue;
+        const int d1 = ring_offset(c1, sa1[q], g.nf1);
+        if (d1 >= w) continue;
+        const V wq = sw[q];
+        for (int i1 = d1; i1 < w; i1 += g.nf1)
+          for (int i0 = d0; i0 < w; i0 += g.nf0) {
+            const R v = sk0[q][i0] * sk1[q][i1];
+            re += wq.x * v;
+            im += wq.y * v;
+          }
+      }
+    __syncthreads();
   }
+  if (mine) grid[b * grid_stride + (size_t)c0 + (size_t)g.nf0 * c1] = mk2<R>(re, im);
 }
 
 // ---- the 1D type-1 NUFFT (`Nufft1`, nufft.rs:25-112), FP64 --------------------------------------
-// Spreading: one thread per source, every weight vector in turn (the kernel is evaluated once per
-// source, as the reference does); FP64 atomics on the fine grid of each weight vector.
-__global__ void spread1_kernel(const double* __restrict__ pos, int npos, const double2* __restrict__ wts, int nw,
-                               int nf, int w, double beta, double2* __restrict__ grid) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npos; j += gridDim.x * blockDim.x) {
-    double k[kWMax];
-    const int m0 = es_taps<double>(pos[j], nf, w, beta, k);  // fine position 2 pos on nf = 2n cells
-    for (int q = 0; q < nw; ++q) {
-      const double2 wv = wts[(size_t)q * npos + j];
-      double* g = reinterpret_cast<double*>(grid + (size_t)q * nf);
-      for (int i = 0; i < w; ++i) {
-        const int c = wrap(m0 + i, nf);
-        atomicAdd(g + 2 * c, wv.x * k[i]);
-        atomicAdd(g + 2 * c + 1, wv.y * k[i]);
-      }
+// Spreading without atomics: one block per 256-cell tile of the fine grid and weight vector, one
+// thread per cell; the tile's points (nufft_bins1, in point order) pass through shared memory with
+// their taps, and each cell adds g += w_j k_i point after point as the reference does
+// (nufft.rs:80-97).
+__global__ void __launch_bounds__(kSpreadTile1)
+    spread1_tile_kernel(const double* __restrict__ pos, const double2* __restrict__ wts, int npos, int nf, int w,
+                        double beta, double2* __restrict__ grid, const NufftBins bins) {
+  __shared__ double sk[kSpreadChunk][kWMax];
+  __shared__ int sm0[kSpreadChunk];
+  __shared__ double2 sw[kSpreadChunk];
+  const int q = blockIdx.y, tile = blockIdx.x;
+  const int c = tile * kSpreadTile1 + (int)threadIdx.x;
+  const bool mine = c < nf;
+  double re = 0.0, im = 0.0;
+  const int p0 = bins.start[tile], p1 = bins.start[tile + 1];
+  for (int base = p0; base < p1; base += kSpreadChunk) {
+    const int n = min(kSpreadChunk, p1 - base);
+    if ((int)threadIdx.x < n) {
+      const int t = threadIdx.x, j = bins.pts[base + t];
+      sm0[t] = es_taps<double>(pos[j], nf, w, beta, sk[t]);  // fine position 2 pos on nf = 2n cells
+      sw[t] = wts[(size_t)q * npos + j];
     }
+    __syncthreads();
+    if (mine)
+      for (int t = 0; t < n; ++t) {
+        const int d = ring_offset(c, sm0[t], nf);
+        for (int i = d; i < w; i += nf) {
+          re += sw[t].x * sk[t][i];
+          im += sw[t].y * sk[t][i];
+        }
+      }
+    __syncthreads();
   }
+  if (mine) grid[(size_t)q * nf + c] = make_double2(re, im);
 }
 
 __global__ void extract1_kernel(const double2* __restrict__ grid, int nf, int k_lo, int n_out,
@@ -393,14 +445,13 @@ void nufft_type2(const NufftGridT<R>& g, const typename Vec2<R>::type* modes, in
 }
 
 template <class R>
-void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const typename Vec2<R>::type* wts, int batch,
-                 size_t w_stride, typename Vec2<R>::type* modes, size_t mode_stride, typename Vec2<R>::type* work,
-                 int sign, cudaStream_t st) {
-  using V = typename Vec2<R>::type;
+void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const NufftBins& bins,
+                 const typename Vec2<R>::type* wts, int batch, size_t w_stride, typename Vec2<R>::type* modes,
+                 size_t mode_stride, typename Vec2<R>::type* work, int sign, cudaStream_t st) {
   const size_t gs = (size_t)g.nf0 * g.nf1;
-  cudaMemsetAsync(work, 0, gs * batch * sizeof(V), st);
-  dim3 sg(std::max(1, std::min((npts + 127) / 128, 4096)), batch);
-  spread_kernel<R><<<sg, 128, 0, st>>>(g, work, u, npts, wts, gs, w_stride);
+  // every cell of every tile is written (zero where no point reaches it)
+  dim3 sg(bins.tiles0 * bins.tiles1, batch);
+  spread_tile_kernel<R><<<sg, kSpreadTile * kSpreadTile, 0, st>>>(g, work, u, wts, gs, w_stride, bins);
   nufft_fft2(g, work, batch, sign, st);
   dim3 eg((g.m_out0 * g.m_out1 + 255) / 256, batch);
   extract_kernel<R><<<eg, 256, 0, st>>>(g, work, modes, gs, mode_stride);
@@ -410,18 +461,16 @@ template void nufft_type2<float>(const NufftGridT<float>&, const float2*, int, s
                                  size_t, float2*, int, const float*, cudaStream_t);
 template void nufft_type2<double>(const NufftGridT<double>&, const double2*, int, size_t, const double*, int, double2*,
                                   size_t, double2*, int, const double*, cudaStream_t);
-template void nufft_type1<float>(const NufftGridT<float>&, const double*, int, const float2*, int, size_t, float2*,
-                                 size_t, float2*, int, cudaStream_t);
-template void nufft_type1<double>(const NufftGridT<double>&, const double*, int, const double2*, int, size_t,
-                                  double2*, size_t, double2*, int, cudaStream_t);
+template void nufft_type1<float>(const NufftGridT<float>&, const double*, int, const NufftBins&, const float2*, int,
+                                 size_t, float2*, size_t, float2*, int, cudaStream_t);
+template void nufft_type1<double>(const NufftGridT<double>&, const double*, int, const NufftBins&, const double2*, int,
+                                  size_t, double2*, size_t, double2*, int, cudaStream_t);
 
 
-void nufft1_run(const Nufft1Grid& g, const double* pos, int npos, const double2* wts, int nw, double2* out,
-                double2* work, cudaStream_t st) {
-  cudaMemsetAsync(work, 0, (size_t)nw * g.nf * sizeof(double2), st);
-  if (npos > 0)
-    spread1_kernel<<<std::max(1, std::min((npos + 127) / 128, 4096)), 128, 0, st>>>(pos, npos, wts, nw, g.nf, g.w,
-                                                                                   g.beta, work);
+void nufft1_run(const Nufft1Grid& g, const double* pos, int npos, const NufftBins& bins, const double2* wts, int nw,
+                double2* out, double2* work, cudaStream_t st) {
+  // every cell of every tile is written (zero where no source reaches it)
+  spread1_tile_kernel<<<dim3(bins.tiles0, nw), kSpreadTile1, 0, st>>>(pos, wts, npos, g.nf, g.w, g.beta, work, bins);
   fft2<double2>(work, g.nf, 1, g.tw, g.tw, nw, 1, st);  // the inverse transform (e^{+i}) of each fine grid
   dim3 eg((g.n_out + 255) / 256, nw);
   extract1_kernel<<<eg, 256, 0, st>>>(work, g.nf, g.k_lo, g.n_out, g.corr, nw, out);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -84,6 +85,68 @@ NufftGridT<R> make_nufft(DevArena& A, int n0, int n1, int m_lo0, int m_lo1, int 
 template NufftGridT<float> make_nufft<float>(DevArena&, int, int, int, int, int, int, double, cudaStream_t);
 template NufftGridT<double> make_nufft<double>(DevArena&, int, int, int, int, int, int, double, cudaStream_t);
 
+// ---- bins of the deterministic spread ----------------------------------------------------------
+namespace {
+// The tiles of a fine ring of nf cells (tiles of `tile` cells) that the kernel window of a point
+// at period coordinate u can reach: the window's cells m0 .. m0 + w - 1 (m0 as the device forms
+// it), widened by a cell each side.  A non-finite position reaches none (its taps are zero).
+void window_tiles(double u, int nf, int w, int tile, std::vector<int>& out) {
+  out.clear();
+  if (!std::isfinite(u)) return;
+  const double half = 0.5 * w;
+  double p = std::fmod(2.0 * u, (double)nf);
+  if (p < 0.0) p += nf;
+  const long long m0 = (long long)std::floor(p - half) + 1;
+  for (long long m = m0 - 1; m <= m0 + w; ++m) {
+    const int c = (int)(((m % nf) + nf) % nf);
+    const int t = c / tile;
+    if (std::find(out.begin(), out.end(), t) == out.end()) out.push_back(t);
+  }
+}
+
+// CSR of per-tile point lists in point order (two passes: counts, then fill point by point).
+NufftBins upload_bins(DevArena& A, int tiles0, int tiles1, int npts, const std::function<void(int, std::vector<int>&)>& tiles_of,
+                      cudaStream_t st) {
+  const size_t nt = (size_t)tiles0 * tiles1;
+  std::vector<int> start(nt + 1, 0), tl;
+  for (int j = 0; j < npts; ++j) {
+    tiles_of(j, tl);
+    for (int t : tl) ++start[(size_t)t + 1];
+  }
+  for (size_t t = 0; t < nt; ++t) start[t + 1] += start[t];
+  std::vector<int> pts((size_t)start[nt]), cur(start.begin(), start.end() - 1);
+  for (int j = 0; j < npts; ++j) {
+    tiles_of(j, tl);
+    for (int t : tl) pts[(size_t)cur[(size_t)t]++] = j;
+  }
+  NufftBins b;
+  b.tiles0 = tiles0;
+  b.tiles1 = tiles1;
+  b.start = (const int*)A.upload(start.data(), start.size() * 4, st);
+  b.pts = (const int*)A.upload(pts.data(), std::max<size_t>(1, pts.size()) * 4, st);
+  return b;
+}
+}  // namespace
+
+NufftBins nufft_bins2(DevArena& A, int nf0, int nf1, int w, const double* u_host, int npts, cudaStream_t st) {
+  const int tiles0 = (nf0 + kSpreadTile - 1) / kSpreadTile, tiles1 = (nf1 + kSpreadTile - 1) / kSpreadTile;
+  std::vector<int> t0, t1;
+  return upload_bins(A, tiles0, tiles1, npts, [&](int j, std::vector<int>& out) {
+    window_tiles(u_host[2 * (size_t)j], nf0, w, kSpreadTile, t0);
+    window_tiles(u_host[2 * (size_t)j + 1], nf1, w, kSpreadTile, t1);
+    out.clear();
+    for (int b : t1)
+      for (int a : t0) out.push_back(a + tiles0 * b);
+  }, st);
+}
+
+NufftBins nufft_bins1(DevArena& A, int nf, int w, const double* pos_host, int npos, cudaStream_t st) {
+  const int tiles = (nf + kSpreadTile1 - 1) / kSpreadTile1;
+  return upload_bins(A, tiles, 1, npos, [&](int j, std::vector<int>& out) {
+    window_tiles(pos_host[j], nf, w, kSpreadTile1, out);
+  }, st);
+}
+
 // ---- the 1D type-1 NUFFT (`Nufft1::new` / `run`, nufft.rs:41-107) on host buffers, FP64 ---------
 void nufft1_host(mrsim_context* ctx, int n, int k_lo, int n_out, double tol, const double* pos, int npos,
                  const double* weights, int nw, double* out) {
@@ -106,7 +169,8 @@ void nufft1_host(mrsim_context* ctx, int n, int k_lo, int n_out, double tol, con
   const double2* dw = npos > 0 ? (const double2*)A.upload(weights, (size_t)nw * npos * 16, st) : nullptr;
   double2* dout = (double2*)A.alloc((size_t)nw * n_out * 16);
   double2* work = (double2*)A.alloc((size_t)nw * g.nf * 16);
-  nufft1_run(g, dp, npos, dw, nw, dout, work, st);
+  const NufftBins bins = nufft_bins1(A, g.nf, g.w, pos, npos, st);
+  nufft1_run(g, dp, npos, bins, dw, nw, dout, work, st);
   MRSIM_CUDA(cudaGetLastError());
   MRSIM_CUDA(cudaMemcpyAsync(out, dout, (size_t)nw * n_out * 16, cudaMemcpyDeviceToHost, st));
   MRSIM_CUDA(cudaStreamSynchronize(st));
@@ -135,7 +199,8 @@ void nufft2_host(mrsim_context* ctx, int type, int n0, int n1, int m_lo0, int m_
   } else {
     const float2* dw = (const float2*)A.upload(in, (size_t)npts * sizeof(float2), st);
     float2* dm = (float2*)A.alloc(nm * sizeof(float2));
-    nufft_type1<float>(g, du, npts, dw, 1, npts, dm, nm, work, sign, st);
+    const NufftBins bins = nufft_bins2(A, g.nf0, g.nf1, g.w, u, npts, st);
+    nufft_type1<float>(g, du, npts, bins, dw, 1, npts, dm, nm, work, sign, st);
     MRSIM_CUDA(cudaGetLastError());
     MRSIM_CUDA(cudaMemcpyAsync(out, dm, nm * sizeof(float2), cudaMemcpyDeviceToHost, st));
   }

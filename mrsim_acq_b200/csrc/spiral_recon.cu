@@ -281,6 +281,7 @@ SpiralRecon::SpiralRecon(mrsim_context* c, const double* k, int npts_, int n_, c
   tw_2n = (const double2*)upload_twiddles<double>(A, 2 * n, st);
   k_host.assign(k, k + 2 * (size_t)npts);
   d_k = (double*)A.upload(k, (size_t)npts * 2 * 8, st);
+  bins_k = nufft_bins2(A, g.nf0, g.nf1, g.w, k, npts, st);
   d_w = (double*)A.alloc((size_t)npts * 8);
   DevArena T;
   // Pipe-Menon (grid_recon.rs:54-66)
@@ -293,7 +294,7 @@ SpiralRecon::SpiralRecon(mrsim_context* c, const double* k, int npts_, int n_, c
     double2* work = (double2*)T.alloc((size_t)g.nf0 * g.nf1 * 16);
     for (int it = 0; it < kDcfIterations; ++it) {
       real_to_complex_kernel<<<grid1(npts), 256, 0, st>>>(d_w, 1.0, npts, wc);
-      nufft_type1<double>(g, d_k, npts, wc, 1, npts, img, (size_t)n * n, work, -1, st);
+      nufft_type1<double>(g, d_k, npts, bins_k, wc, 1, npts, img, (size_t)n * n, work, -1, st);
       nufft_type2<double>(g, img, 1, (size_t)n * n, d_k, npts, back, npts, work, 1, nullptr, st);
       pipe_menon_kernel<<<grid1(npts), 256, 0, st>>>(d_w, back, npts);
     }
@@ -341,7 +342,8 @@ SpiralRecon::SpiralRecon(mrsim_context* c, const double* k, int npts_, int n_, c
     real_to_complex_kernel<<<grid1(npts), 256, 0, st>>>(d_w, sc * sc, npts, wc);
     double2* tmodes = (double2*)T.alloc((size_t)m * m * 16);
     double2* work = (double2*)T.alloc((size_t)g2.nf0 * g2.nf1 * 16);
-    nufft_type1<double>(g2, du2, npts, wc, 1, npts, tmodes, (size_t)m * m, work, -1, st);
+    const NufftBins bins2 = nufft_bins2(T, g2.nf0, g2.nf1, g2.w, u2.data(), npts, st);
+    nufft_type1<double>(g2, du2, npts, bins2, wc, 1, npts, tmodes, (size_t)m * m, work, -1, st);
     d_tf = (double2*)A.alloc((size_t)m * m * 16);
     circulant_kernel<<<grid1((size_t)m * m), 256, 0, st>>>(tmodes, n, d_tf);
     fft_lines(d_tf, m, m, 1, m, (size_t)m * m, 1, tw_2n, -1, st);
@@ -436,7 +438,7 @@ void SpiralRecon::gridding(const double2* d_data, int batch, double2* d_out) {
   double2* wts = (double2*)T.alloc((size_t)batch * npts * 16);
   weight_samples_kernel<<<grid1(npts, batch), 256, 0, st>>>(d_data, nullptr, d_w, sc, npts, wts);
   double2* work = (double2*)T.alloc((size_t)batch * g.nf0 * g.nf1 * 16);
-  nufft_type1<double>(g, d_k, npts, wts, batch, npts, d_out, (size_t)n * n, work, -1, st);
+  nufft_type1<double>(g, d_k, npts, bins_k, wts, batch, npts, d_out, (size_t)n * n, work, -1, st);
   scale_kernel<<<grid1((size_t)batch * n * n), 256, 0, st>>>(d_out, (double)n * n, (size_t)batch * n * n, d_out);
   MRSIM_CUDA(cudaGetLastError());
   MRSIM_CUDA(cudaStreamSynchronize(st));  // T's buffers are freed on return
@@ -456,7 +458,7 @@ void SpiralRecon::images(const double2* d_data, int batch, double2* d_x) {
     double2* wts = (double2*)W.alloc((size_t)batch * npts * 16);
     weight_samples_kernel<<<grid1(npts, batch), 256, 0, st>>>(d_data, d_win, d_w, sc, npts, wts);
     double2* work = (double2*)W.alloc((size_t)batch * g.nf0 * g.nf1 * 16);
-    nufft_type1<double>(g, d_k, npts, wts, batch, npts, r, nn, work, -1, st);
+    nufft_type1<double>(g, d_k, npts, bins_k, wts, batch, npts, r, nn, work, -1, st);
     project(r, batch, st);
     MRSIM_CUDA(cudaStreamSynchronize(st));  // W's buffers are freed on return
   }

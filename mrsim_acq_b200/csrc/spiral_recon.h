@@ -28,6 +28,7 @@ struct SpiralRecon {
   int power_iterations = 0;
   DevArena A;
   NufftGridT<double> g{};
+  NufftBins bins_k;  // the trajectory's spread bins on g
   const double2* tw_n = nullptr;
   const double2* tw_2n = nullptr;
   double* d_k = nullptr;

@@ -92,11 +92,34 @@ def test_width_rule_follows_the_reference_gridding(gpu_ctx, tol):
         got = nu.type2(c, u, sign)
         ref = O.nufft2(2, n, lo, mo, tol, u, c, sign)
         direct = O.nufft2_direct(2, n, lo, mo, u, c, sign)
-        gap = rel_l2(ref, direct)
-        assert rel_l2(got, ref) <= max(1e-5, 1e-2 * gap)
+        # the gridding error itself is far above the FP32 arithmetic's: a fixed bound against the
+        # FP64 gridding shows the device reproduces it
+        assert rel_l2(ref, direct) > 100 * 2e-6 or tol < 1e-3
+        assert rel_l2(got, ref) <= 2e-6
         got1 = nu.type1(u, w, sign).ravel()
         ref1 = O.nufft2(1, n, lo, mo, tol, u, w, sign)
-        assert rel_l2(got1, ref1) <= max(1e-5, 1e-2 * rel_l2(ref1, O.nufft2_direct(1, n, lo, mo, u, w, sign)))
+        assert rel_l2(got1, ref1) <= 2e-6
+
+
+def test_type1_spreading_is_deterministic(gpu_ctx):
+    """Type 1 spreads without atomics (every fine cell sums its points in point order): the same
+    input gives the same bits, also with thousands of points crowding a few cells, where the order
+    of floating-point additions would otherwise vary from run to run; and the result still follows
+    the FP64 gridding."""
+    rng = np.random.default_rng(3)
+    n, lo, mo = [32, 32], [-16, -16], [32, 32]
+    u = np.concatenate([rng.normal(0.0, 0.4, (6000, 2)), rng.uniform(-16, 16, (2000, 2))])
+    w = rng.normal(size=8000) + 1j * rng.normal(size=8000)
+    nu = S.Nufft2(n, lo, mo, 1e-6, ctx=gpu_ctx)
+    a = nu.type1(u, w, -1)
+    for _ in range(3):
+        assert np.array_equal(nu.type1(u, w, -1), a)
+    assert rel_l2(a.ravel(), O.nufft2(1, n, lo, mo, 1e-6, u, w, -1)) <= 2e-6
+    pos = rng.normal(0.0, 0.7, 5000)
+    wts = [rng.normal(size=5000) + 1j * rng.normal(size=5000) for _ in range(2)]
+    f = S.Nufft1(64, -20, 41, 1e-12, ctx=gpu_ctx)
+    b = f.run(pos, wts)
+    assert np.array_equal(f.run(pos, wts), b)
 
 
 def test_pair_errors(gpu_ctx):
