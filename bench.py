@@ -277,37 +277,7 @@ def scale_measurements(args, ctx, stream):
                                  "stage_ms": dict(zip(STAGES, [round(float(v), 3) for v in st])),
                                  "note": "exact pair (per-coil kernels: a ring of 32 takes no coil-class path); "
                                          "the segmented path refuses this shape (more than 16 line groups)"}
-    # one volume of the stack of spirals
-    from mrsim_acq_b200 import kspace3d as K3
-    n, nzs = 64, 48
-    sg = n * o
-    kz = K3.KzSampling(0.75, 2)
-    lo = nzs - min(nzs, int(round(nzs * kz.partial_fourier)))
-    etl = sum(1 for p in range(nzs) if p >= lo and (p - nzs // 2) % kz.accel == 0)
-    train = K3.EchoTrain(etl=etl, esp_ms=12.0, refocusing_deg=180.0, kz_order=K3.KzOrder.Centric, kz_segments=1)
-    ro = K3.SpiralReadout(32, 8.192, 0.004, 1.2, kz)
-    vox = np.arange(sg * sg * nzs)
-    x, y, z = (vox % sg) / sg, ((vox // sg) % sg) / sg, (vox // (sg * sg)) / nzs
-    img = (np.exp(-((x - 0.5) ** 2 + (y - 0.47) ** 2) / 0.04) * (1.0 + 0.3 * np.sin(6.3 * z))).astype(np.float32)
-    fm = (80.0 * np.exp(-((x - 0.4) ** 2 + (y - 0.4) ** 2) / 0.02) - 80.0 * np.exp(-((x - 0.65) ** 2 + (y - 0.6) ** 2)
-                                                                                     / 0.015)).astype(np.float32)
-    acq3 = Acquisition(do_relaxation=True, do_distortions=True, n_coils=16, signal_scale=100.0)
-    args3 = ((sg, sg, nzs), (n, n, nzs), 1, [img], [T2.uniform(80.0)], [T2.uniform(1300.0)], fm, None, acq3, train, ro)
-    kzo = K3.KzOptions(coil_rows=2)
-    K3.spiral_samples_3d(*args3, kz_opts=kzo, ctx=ctx)  # warm
-    t0 = time.perf_counter()
-    reps = 2
-    for _ in range(reps):
-        smp3 = K3.spiral_samples_3d(*args3, kz_opts=kzo, ctx=ctx)
-    dt = (time.perf_counter() - t0) / reps
-    acquired = int(np.count_nonzero(np.abs(smp3).reshape(16, nzs, -1).sum(axis=2)[0]))
-    n_samp = 16 * acquired * smp3.shape[2]
-    out["stack_of_spirals"] = {"config": "64x64x48 on 128x128, 16 coils in 2 rings, 32 x 2048 samples at 4 us, "
-                                         "kz PF 6/8 R=2, +-80 Hz, 1 compartment, certified segmentation",
-                               "acquired_partitions": acquired, "samples_per_volume": n_samp,
-                               "seconds_per_volume": dt, "value": n_samp / dt, "unit": "samples/s",
-                               "timing": "host-buffer call (mrsim_spiral_samples_3d) by wall clock, host<->device "
-                                         "copies included"}
+    out["stack_of_spirals"] = spiral_measurement(ctx)
     # the plain single-shot case on the device (launch-bound: one unit)
     c1, acq1 = c1_inputs()
     op = EpiOperator(c1["sim_dims"], c1["acq_dims"], 1, c1["t2"], c1["fmap"], acq1, images=c1["images"],
@@ -320,6 +290,52 @@ def scale_measurements(args, ctx, stream):
                                 "value": smp1 / (tot / 20 * 1e-3), "unit": "samples/s",
                                 "note": "one unit: five launches of a few microseconds each"}
     return out
+
+
+def spiral_measurement(ctx, reps=2):
+    """One volume of the stack of spirals (64x64x48 on a 128x128 grid, 16 coils in 2 rings, 32
+    interleaves x 2048 samples at 4 us, kz partial Fourier 6/8 and R = 2, +-80 Hz): the forward
+    alone (`spiral_samples_3d`) and the whole acquisition with its reconstruction
+    (`simulate_acquisition_3d`: forward, noise, kz GRAPPA fill, POCS, gridding + CG per partition),
+    host-buffer calls by wall clock, host<->device copies included."""
+    from mrsim_acq_b200 import kspace3d as K3
+    from mrsim_acq_b200.api import T2, Acquisition
+    o, n, nzs = 2, 64, 48
+    sg = n * o
+    kz = K3.KzSampling(0.75, 2)
+    lo = nzs - min(nzs, int(round(nzs * kz.partial_fourier)))
+    etl = sum(1 for p in range(nzs) if p >= lo and (p - nzs // 2) % kz.accel == 0)
+    train = K3.EchoTrain(etl=etl, esp_ms=12.0, refocusing_deg=180.0, kz_order=K3.KzOrder.Centric, kz_segments=1)
+    ro = K3.SpiralReadout(32, 8.192, 0.004, 1.2, kz)
+    vox = np.arange(sg * sg * nzs)
+    x, y, z = (vox % sg) / sg, ((vox // sg) % sg) / sg, (vox // (sg * sg)) / nzs
+    img = (np.exp(-((x - 0.5) ** 2 + (y - 0.47) ** 2) / 0.04) * (1.0 + 0.3 * np.sin(6.3 * z))).astype(np.float32)
+    fm = (80.0 * np.exp(-((x - 0.4) ** 2 + (y - 0.4) ** 2) / 0.02) - 80.0 * np.exp(-((x - 0.65) ** 2 + (y - 0.6) ** 2)
+                                                                                     / 0.015)).astype(np.float32)
+    acq3 = Acquisition(do_relaxation=True, do_distortions=True, n_coils=16, signal_scale=100.0, noise_variance=1e-4)
+    args3 = ((sg, sg, nzs), (n, n, nzs), 1, [img], [T2.uniform(80.0)], [T2.uniform(1300.0)], fm, None, acq3, train, ro)
+    kzo = K3.KzOptions(coil_rows=2, calibration_images=[img], calibration_seed=3, pocs=True)
+    K3.spiral_samples_3d(*args3, kz_opts=kzo, ctx=ctx)  # warm
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        smp3 = K3.spiral_samples_3d(*args3, kz_opts=kzo, ctx=ctx)
+    dt = (time.perf_counter() - t0) / reps
+    acquired = int(np.count_nonzero(np.abs(smp3).reshape(16, nzs, -1).sum(axis=2)[0]))
+    n_samp = 16 * acquired * smp3.shape[2]
+    K3.simulate_acquisition_3d(*args3, seed=5, kz_opts=kzo, ctx=ctx)  # warm
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        K3.simulate_acquisition_3d(*args3, seed=5, kz_opts=kzo, ctx=ctx)
+    dt_full = (time.perf_counter() - t0) / reps
+    return {"config": "64x64x48 on 128x128, 16 coils in 2 rings, 32 x 2048 samples at 4 us, kz PF 6/8 R=2, +-80 Hz, "
+                      "1 compartment, certified segmentation",
+            "acquired_partitions": acquired, "samples_per_volume": n_samp,
+            "seconds_per_volume": dt, "value": n_samp / dt, "unit": "samples/s",
+            "acquisition_with_reconstruction_seconds_per_volume": dt_full,
+            "acquisition_with_reconstruction_samples_per_s": n_samp / dt_full,
+            "timing": "host-buffer calls (mrsim_spiral_samples_3d; mrsim_simulate_acquisition_3d_spiral with noise, "
+                      "kz GRAPPA fill, POCS and the per-partition gridding + CG reconstruction) by wall clock, "
+                      "host<->device copies included"}
 
 
 def spin_history_series():
@@ -682,6 +698,8 @@ def main():
     ap.add_argument("--spin-history-only", action="store_true",
                     help="run only the spin-history workload and print its line (profiling)")
     ap.add_argument("--spin-volumes", type=int, default=40, help="volumes of the spin-history series")
+    ap.add_argument("--spiral-only", action="store_true",
+                    help="run only the stack-of-spirals volume and print its line (profiling)")
     args = ap.parse_args()
     if args.volumes > 0:
         WORKLOAD["nv"] = args.volumes
@@ -692,6 +710,10 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
+        return
+    if args.spiral_only:
+        from mrsim_acq_b200 import api
+        print(json.dumps(spiral_measurement(api.Context(local_rank), reps=1)), flush=True)
         return
     if args.spin_history_only:
         import torch

@@ -53,8 +53,9 @@ void nufft_type2(const NufftGridT<R>& g, const typename Vec2<R>::type* modes, in
                  typename Vec2<R>::type* work, int sign, const R* scale, cudaStream_t st);
 // The deterministic spread's fine-grid tiles and, per tile, the points whose kernel window can
 // reach it, in point order (CSR on the device, built on the host from the positions once per
-// point set).  A tile is 16 x 16 fine cells in 2D, 256 cells in 1D.
-constexpr int kSpreadTile = 16;
+// point set).  A tile is 8 x 8 fine cells in 2D (a cell's scan covers (8 + w)^2 cells of
+// windows to use w^2; a 128 x 128 fine grid still gives 256 blocks), 256 cells in 1D.
+constexpr int kSpreadTile = 8;
 constexpr int kSpreadTile1 = 256;
 struct NufftBins {
   int tiles0 = 0, tiles1 = 0;

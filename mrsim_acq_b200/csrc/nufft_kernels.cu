@@ -37,6 +37,8 @@ __device__ __forceinline__ double2 mk2<double>(double a, double b) {
 __device__ __forceinline__ float es_exp(float x) { return __expf(x); }
 __device__ __forceinline__ double es_exp(double x) { return exp(x); }
 
+constexpr int kWMax = 16;
+
 // First fine cell and the w taps of coordinate u (period n) on a fine grid of nf = 2n cells.
 template <class R>
 __device__ __forceinline__ int es_taps(double u, int nf, int w, R beta, R* k) {
@@ -45,15 +47,14 @@ __device__ __forceinline__ int es_taps(double u, int nf, int w, R beta, R* k) {
   if (p < 0.0) p += nf;
   const int m0 = (int)floor(p - half) + 1;
   const R ih = (R)(1.0 / half);
-#pragma unroll 4
-  for (int i = 0; i < w; ++i) {
+#pragma unroll
+  for (int i = 0; i < kWMax; ++i) {
+    if (i >= w) break;
     const R z = (R)((double)(m0 + i) - p) * ih;
     k[i] = fabs(z) < (R)1 ? es_exp(beta * (sqrt((R)1 - z * z) - (R)1)) : (R)0;
   }
   return m0;
 }
-
-constexpr int kWMax = 16;
 
 template <class R>
 __global__ void place_kernel(const NufftGridT<R> g, const typename Vec2<R>::type* __restrict__ modes,
@@ -150,32 +151,75 @@ __global__ void dft_line_kernel(V* __restrict__ data, int n, size_t es, size_t l
   }
 }
 
-// Type 2: out[j] = sum over the w x w taps of grid, for each point of each batch item.
+constexpr int kBatchBlock = 4;  // batch items a type-1 or type-2 thread serves with one set of taps
+
+// Type 2: out[j] = sum over the w x w taps of grid, for each point of each batch item; a thread
+// serves one point for up to kBatchBlock batch items (blockIdx.y), forming the taps once.  The tap
+// loops run to the compile-time bound kWMax (guarded by w), so taps and column indices live in
+// registers; a window wraps at most once when the fine grid is at least 2 kWMax wide (else the
+// general modulo).
 template <class R>
-__global__ void interp_kernel(const NufftGridT<R> g, const typename Vec2<R>::type* __restrict__ grid,
-                              const double* __restrict__ u, int npts, typename Vec2<R>::type* __restrict__ out,
-                              size_t grid_stride, size_t out_stride) {
+__global__ void __launch_bounds__(128) interp_kernel(const NufftGridT<R> g, const typename Vec2<R>::type* __restrict__ grid,
+                                                     const double* __restrict__ u, int npts,
+                                                     typename Vec2<R>::type* __restrict__ out, size_t grid_stride,
+                                                     size_t out_stride, int batch) {
   using V = typename Vec2<R>::type;
-  const int b = blockIdx.y;
-  const V* G = grid + b * grid_stride;
+  const int b0 = blockIdx.y * kBatchBlock, nb = min(kBatchBlock, batch - b0);
+  const int w = g.w;
+  const bool wide = g.nf0 >= 2 * kWMax && g.nf1 >= 2 * kWMax;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npts; j += gridDim.x * blockDim.x) {
     R k0[kWMax], k1[kWMax];
-    const int a0 = es_taps<R>(u[2 * j], g.nf0, g.w, g.beta, k0);
-    const int a1 = es_taps<R>(u[2 * j + 1], g.nf1, g.w, g.beta, k1);
-    R re = 0, im = 0;
-    for (int i1 = 0; i1 < g.w; ++i1) {
-      const int c1 = wrap(a1 + i1, g.nf1);
-      const V* row = G + (size_t)g.nf0 * c1;
-      R rr = 0, ri = 0;
-      for (int i0 = 0; i0 < g.w; ++i0) {
-        const V v = __ldg(row + wrap(a0 + i0, g.nf0));
-        rr = fma(v.x, k0[i0], rr);
-        ri = fma(v.y, k0[i0], ri);
+    const int a0 = es_taps<R>(u[2 * j], g.nf0, w, g.beta, k0);
+    const int a1 = es_taps<R>(u[2 * j + 1], g.nf1, w, g.beta, k1);
+    int col[kWMax];
+#pragma unroll
+    for (int i0 = 0; i0 < kWMax; ++i0) {
+      int c = a0 + i0;
+      if (wide) {
+        c = c < 0 ? c + g.nf0 : c;
+        c = c >= g.nf0 ? c - g.nf0 : c;
+      } else {
+        c = wrap(c, g.nf0);
       }
-      re = fma(rr, k1[i1], re);
-      im = fma(ri, k1[i1], im);
+      col[i0] = c;
     }
-    out[b * out_stride + j] = mk2<R>(re, im);
+    R re[kBatchBlock], im[kBatchBlock];
+#pragma unroll
+    for (int q = 0; q < kBatchBlock; ++q) re[q] = im[q] = 0;
+#pragma unroll
+    for (int i1 = 0; i1 < kWMax; ++i1) {
+      if (i1 >= w) break;
+      int c1 = a1 + i1;
+      if (wide) {
+        c1 = c1 < 0 ? c1 + g.nf1 : c1;
+        c1 = c1 >= g.nf1 ? c1 - g.nf1 : c1;
+      } else {
+        c1 = wrap(c1, g.nf1);
+      }
+      const V* row = grid + (size_t)g.nf0 * c1;
+      R rr[kBatchBlock], ri[kBatchBlock];
+#pragma unroll
+      for (int q = 0; q < kBatchBlock; ++q) rr[q] = ri[q] = 0;
+#pragma unroll
+      for (int i0 = 0; i0 < kWMax; ++i0) {
+        if (i0 >= w) break;
+#pragma unroll
+        for (int q = 0; q < kBatchBlock; ++q)
+          if (q < nb) {
+            const V v = __ldg(row + (size_t)(b0 + q) * grid_stride + col[i0]);
+            rr[q] = fma(v.x, k0[i0], rr[q]);
+            ri[q] = fma(v.y, k0[i0], ri[q]);
+          }
+      }
+#pragma unroll
+      for (int q = 0; q < kBatchBlock; ++q) {
+        re[q] = fma(rr[q], k1[i1], re[q]);
+        im[q] = fma(ri[q], k1[i1], im[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kBatchBlock; ++q)
+      if (q < nb) out[(size_t)(b0 + q) * out_stride + j] = mk2<R>(re[q], im[q]);
   }
 }
 
@@ -189,8 +233,8 @@ __device__ __forceinline__ int ring_offset(int c, int a, int n) {
 
 constexpr int kSpreadChunk = 64;  // points whose taps a spread block holds at a time
 
-// Type 1 spreading without atomics: one block per 16 x 16 tile of the fine grid (one thread per
-// cell) and batch item.  The tile's points (nufft_bins2: every point whose window can reach the
+// Type 1 spreading without atomics: one block per 8 x 8 tile of the fine grid (one thread per
+// cell) and group of up to kBatchBlock batch items (the taps formed once for the group).  The tile's points (nufft_bins2: every point whose window can reach the
 // tile, in point order) pass through shared memory in chunks with their taps; each thread adds
 // the contributions to its own cell point after point, cell += w_j (k0 k1) as the reference does
 // (nufft.rs:236-250), and stores the cell once.  The sum order is fixed, so the grid is the same
@@ -200,17 +244,19 @@ template <class R>
 __global__ void __launch_bounds__(kSpreadTile * kSpreadTile)
     spread_tile_kernel(const NufftGridT<R> g, typename Vec2<R>::type* __restrict__ grid, const double* __restrict__ u,
                        const typename Vec2<R>::type* __restrict__ wts, size_t grid_stride, size_t w_stride,
-                       const NufftBins bins) {
+                       const NufftBins bins, int batch) {
   using V = typename Vec2<R>::type;
   __shared__ R sk0[kSpreadChunk][kWMax], sk1[kSpreadChunk][kWMax];
   __shared__ int sa0[kSpreadChunk], sa1[kSpreadChunk];
-  __shared__ V sw[kSpreadChunk];
-  const int b = blockIdx.y, tile = blockIdx.x;
+  __shared__ V sw[kBatchBlock][kSpreadChunk];
+  const int b0 = blockIdx.y * kBatchBlock, nb = min(kBatchBlock, batch - b0), tile = blockIdx.x;
   const int c0 = (tile % bins.tiles0) * kSpreadTile + (int)threadIdx.x % kSpreadTile;
   const int c1 = (tile / bins.tiles0) * kSpreadTile + (int)threadIdx.x / kSpreadTile;
   const bool mine = c0 < g.nf0 && c1 < g.nf1;
   const int w = g.w;
-  R re = 0, im = 0;
+  R re[kBatchBlock], im[kBatchBlock];
+#pragma unroll
+  for (int q = 0; q < kBatchBlock; ++q) re[q] = im[q] = 0;
   const int p0 = bins.start[tile], p1 = bins.start[tile + 1];
   for (int base = p0; base < p1; base += kSpreadChunk) {
     const int n = min(kSpreadChunk, p1 - base);
@@ -218,7 +264,9 @@ __global__ void __launch_bounds__(kSpreadTile * kSpreadTile)
       const int t = threadIdx.x, j = bins.pts[base + t];
       sa0[t] = es_taps<R>(u[2 * j], g.nf0, w, g.beta, sk0[t]);
       sa1[t] = es_taps<R>(u[2 * j + 1], g.nf1, w, g.beta, sk1[t]);
-      sw[t] = wts[b * w_stride + j];
+#pragma unroll
+      for (int q = 0; q < kBatchBlock; ++q)
+        if (q < nb) sw[q][t] = wts[(size_t)(b0 + q) * w_stride + j];
     }
     __syncthreads();
     if (mine)
@@ -227,17 +275,22 @@ __global__ void __launch_bounds__(kSpreadTile * kSpreadTile)
         if (d0 >= w) continue;
         const int d1 = ring_offset(c1, sa1[q], g.nf1);
         if (d1 >= w) continue;
-        const V wq = sw[q];
         for (int i1 = d1; i1 < w; i1 += g.nf1)
           for (int i0 = d0; i0 < w; i0 += g.nf0) {
             const R v = sk0[q][i0] * sk1[q][i1];
-            re += wq.x * v;
-            im += wq.y * v;
+#pragma unroll
+            for (int bq = 0; bq < kBatchBlock; ++bq) {
+              re[bq] += sw[bq][q].x * v;
+              im[bq] += sw[bq][q].y * v;
+            }
           }
       }
     __syncthreads();
   }
-  if (mine) grid[b * grid_stride + (size_t)c0 + (size_t)g.nf0 * c1] = mk2<R>(re, im);
+  if (mine)
+#pragma unroll
+    for (int q = 0; q < kBatchBlock; ++q)
+      if (q < nb) grid[(size_t)(b0 + q) * grid_stride + (size_t)c0 + (size_t)g.nf0 * c1] = mk2<R>(re[q], im[q]);
 }
 
 // ---- the 1D type-1 NUFFT (`Nufft1`, nufft.rs:25-112), FP64 --------------------------------------
@@ -440,8 +493,8 @@ void nufft_type2(const NufftGridT<R>& g, const typename Vec2<R>::type* modes, in
   dim3 pg((g.m_out0 * g.m_out1 + 255) / 256, batch);
   place_kernel<R><<<pg, 256, 0, st>>>(g, modes, work, batch, mode_stride, gs, scale);
   nufft_fft2(g, work, batch, sign, st);
-  dim3 ig(std::max(1, std::min((npts + 127) / 128, 4096)), batch);
-  interp_kernel<R><<<ig, 128, 0, st>>>(g, work, u, npts, out, gs, out_stride);
+  dim3 ig(std::max(1, std::min((npts + 127) / 128, 4096)), (batch + kBatchBlock - 1) / kBatchBlock);
+  interp_kernel<R><<<ig, 128, 0, st>>>(g, work, u, npts, out, gs, out_stride, batch);
 }
 
 template <class R>
@@ -450,8 +503,8 @@ void nufft_type1(const NufftGridT<R>& g, const double* u, int npts, const NufftB
                  size_t mode_stride, typename Vec2<R>::type* work, int sign, cudaStream_t st) {
   const size_t gs = (size_t)g.nf0 * g.nf1;
   // every cell of every tile is written (zero where no point reaches it)
-  dim3 sg(bins.tiles0 * bins.tiles1, batch);
-  spread_tile_kernel<R><<<sg, kSpreadTile * kSpreadTile, 0, st>>>(g, work, u, wts, gs, w_stride, bins);
+  dim3 sg(bins.tiles0 * bins.tiles1, (batch + kBatchBlock - 1) / kBatchBlock);
+  spread_tile_kernel<R><<<sg, kSpreadTile * kSpreadTile, 0, st>>>(g, work, u, wts, gs, w_stride, bins, batch);
   nufft_fft2(g, work, batch, sign, st);
   dim3 eg((g.m_out0 * g.m_out1 + 255) / 256, batch);
   extract_kernel<R><<<eg, 256, 0, st>>>(g, work, modes, gs, mode_stride);
