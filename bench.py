@@ -292,6 +292,50 @@ def scale_measurements(args, ctx, stream):
     return out
 
 
+def pipeline_measurement(ctx, inp, acq, cpu=True):
+    """The whole reference pipeline of the benchmark series through its reference-compatible entry
+    point (`simulate_acquisition_echoes`, kspace.rs:2152): per echo the exact forward, the receiver
+    noise, GRAPPA R = 2 fitted on the echo's first volume, the Hann window, the inverse DFT and the
+    Roemer combine, host buffers in and magnitude / phase out, by wall clock; beside it the FP64
+    oracle's pipeline (`acquire_volumes_complex`) on one volume of one echo on the host cores."""
+    from mrsim_acq_b200 import api
+    from mrsim_acq_b200.api import AcquisitionInput, PhaseModel
+    W = WORKLOAD
+    a = acq.replace(noise_variance=1.56)  # image SNR about 40 at the phantom's mean magnitude
+    ai = AcquisitionInput(inp["sim_dims"], inp["acq_dims"], inp["n_volumes"], inp["images"], inp["t2"], inp["fmap"],
+                          t_inhom=inp["t_inhom"], phase=PhaseModel.hbcd_like(), seed=9)
+    echoes = list(W["echoes"])
+    per_echo = [inp["images"]] * len(echoes)
+    api.simulate_acquisition_echoes(ai, per_echo, a, echoes, ctx=ctx)  # warm
+    t0 = time.perf_counter()
+    api.simulate_acquisition_echoes(ai, per_echo, a, echoes, ctx=ctx)
+    dt = time.perf_counter() - t0
+    nx, ny, nz = inp["acq_dims"]
+    nv = inp["n_volumes"]
+    voxels = nx * ny * nz * nv * len(echoes)
+    res = {"config": f"the benchmark series ({nv} volumes x {nz} slices x {len(echoes)} echoes, {W['n_coils']} coils, "
+                     "3 compartments) with noise variance 1.56, GRAPPA R=2 from each echo's first volume, Hann "
+                     "window, Roemer combine",
+           "seconds_per_series": dt, "value": voxels / dt, "unit": "reconstructed voxels/s",
+           "timing": "mrsim_simulate_acquisition_echoes with host buffers by wall clock (inputs up, magnitude and "
+                     "phase down)"}
+    if cpu:
+        import os
+        from oracle import oracle
+        snx, sny, _ = inp["sim_dims"]
+        one = [im[0::nv].copy() for im in inp["images"]]
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.acquire_volumes_complex(inp["sim_dims"], inp["acq_dims"], 1, one, inp["t2"], inp["fmap"],
+                                       a.replace(t_echo=echoes[0]), 9, 9, threads=threads, t_inhom=inp["t_inhom"],
+                                       phase=PhaseModel.hbcd_like())
+        ct = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": nx * ny * nz / ct, "unit": "reconstructed voxels/s", "cores": threads,
+                               "kind": "port", "sample": f"1 volume x {nz} slices x 1 echo, FP64 oracle pipeline "
+                                                         f"(GRAPPA fitted on that volume), {ct:.2f} s"}
+    return res
+
+
 def spiral_measurement(ctx, reps=2):
     """One volume of the stack of spirals (64x64x48 on a 128x128 grid, 16 coils in 2 rings, 32
     interleaves x 2048 samples at 4 us, kz partial Fourier 6/8 and R = 2, +-80 Hz): the forward
@@ -567,6 +611,7 @@ def run_ours(args, rank, world, local_rank):
     }
     if not args.no_scale and world == 1:
         res["scale"] = scale_measurements(args, ctx, stream)
+        res["pipeline"] = pipeline_measurement(ctx, inp, acq, cpu=not args.no_cpu_baseline)
         res["spin_history"] = spin_history_measurement(ctx, stream, cpu=not args.no_cpu_baseline)
         res["gpu_launches_spin_history"] = res["spin_history"]["launches"]
     if not args.no_segmented and world == 1:
