@@ -333,6 +333,17 @@ def pipeline_measurement(ctx, inp, acq, cpu=True):
         res["cpu_baseline"] = {"value": nx * ny * nz / ct, "unit": "reconstructed voxels/s", "cores": threads,
                                "kind": "port", "sample": f"1 volume x {nz} slices x 1 echo, FP64 oracle pipeline "
                                                          f"(GRAPPA fitted on that volume), {ct:.2f} s"}
+        # the reference's `kspace` build on the same sample: NUFFT y-stage, FFT x-stage and inverse
+        with oracle.kspace_build():
+            t0 = time.perf_counter()
+            oracle.acquire_volumes_complex(inp["sim_dims"], inp["acq_dims"], 1, one, inp["t2"], inp["fmap"],
+                                           a.replace(t_echo=echoes[0]), 9, 9, threads=threads,
+                                           t_inhom=inp["t_inhom"], phase=PhaseModel.hbcd_like())
+            kt = time.perf_counter() - t0
+        res["cpu_baseline_kspace_build"] = {"value": nx * ny * nz / kt, "unit": "reconstructed voxels/s",
+                                            "cores": threads, "kind": "port",
+                                            "sample": f"the same sample under the reference's `kspace` build "
+                                                      f"(NUFFT y-stage, FFT x-stage and inverse), {kt:.2f} s"}
     return res
 
 

@@ -246,13 +246,96 @@ bool eddy_enabled(const mrsim_acquisition& a, const mrsim_slice_input& inp) {
 // T2 accessors (`T2Slice` kspace.rs:380-386)
 inline double t2_value(const mrsim_t2& t, size_t i) { return t.is_map ? (double)t.map[i] : (double)t.value; }
 
+// ---- the reference's two builds ------------------------------------------------------------
+// 0: the default build (rotor y-stage, twiddle x-stage, direct inverse); 1: the `kspace` cargo
+// feature (NUFFT y-stage kspace.rs:769-833, FFT x-stage kspace.rs:1079-1123, `inverse_2d_fft`
+// kspace.rs:1385-1424).  rustfft's transforms are restated by fft1d (the same linear maps).
+int g_kspace_build = 0;
+
+void fft1d(std::vector<Cx>& a, int sign);
+
+// `Nufft1` nufft.rs:25-112, FP64: sources at positions (cells, period n), any number of weight
+// vectors, outputs at integer frequencies k_lo .. k_lo + n_out.
+struct Nufft1O {
+  size_t nf, w, n_out;
+  double beta;
+  int64_t k_lo;
+  std::vector<double> corr, kern;
+  Nufft1O(size_t n, int64_t k_lo_, size_t n_out_, double tol) : nf(2 * n), n_out(n_out_), k_lo(k_lo_) {
+    if (!(n_out > 0 && k_lo >= -(int64_t)n / 2 && k_lo + (int64_t)n_out - 1 <= (int64_t)n / 2))
+      throw Fail("output band must sit inside the coarse Nyquist band");
+    w = (size_t)std::min(16.0, std::max(2.0, std::ceil(-std::log10(tol)) + 1.0));
+    beta = 2.30 * (double)w;
+    const double half = (double)w / 2.0;
+    for (size_t j = 0; j < n_out; ++j) {  // `deapodization` nufft.rs:48-63
+      const double k = (double)(k_lo + (int64_t)j);
+      double s = psi(0.0);
+      for (double m = 1.0; m < half; m += 1.0) s += 2.0 * psi(m / half) * std::cos(TAU * k * m / (double)nf);
+      corr.push_back(1.0 / s);
+    }
+    kern.assign(w, 0.0);
+  }
+  double psi(double z) const { return std::fabs(z) < 1.0 ? std::exp(beta * (std::sqrt(1.0 - z * z) - 1.0)) : 0.0; }
+  static double rem_euclid(double x, double m) {
+    const double r = std::fmod(x, m);
+    return r < 0.0 ? r + std::fabs(m) : r;
+  }
+  // `Nufft1::run` nufft.rs:70-108
+  void run(const std::vector<double>& pos, const std::vector<std::vector<double>>& wre,
+           const std::vector<std::vector<double>>& wim, std::vector<std::vector<Cx>>& out) {
+    const size_t nw = wre.size();
+    const double half = (double)w / 2.0;
+    std::vector<std::vector<Cx>> grid(nw, std::vector<Cx>(nf, CZERO));
+    for (size_t j = 0; j < pos.size(); ++j) {
+      const double p = rem_euclid(2.0 * pos[j], (double)nf);
+      const int64_t m0 = (int64_t)std::floor(p - half) + 1;
+      for (size_t i = 0; i < w; ++i) kern[i] = psi(((double)m0 + (double)i - p) / half);
+      for (size_t q = 0; q < nw; ++q) {
+        const double wr = wre[q][j], wi = wim[q][j];
+        for (size_t i = 0; i < w; ++i) {
+          int64_t m = (m0 + (int64_t)i) % (int64_t)nf;
+          if (m < 0) m += (int64_t)nf;
+          grid[q][(size_t)m].re += wr * kern[i];
+          grid[q][(size_t)m].im += wi * kern[i];
+        }
+      }
+    }
+    out.assign(nw, std::vector<Cx>(n_out));
+    for (size_t q = 0; q < nw; ++q) {
+      fft1d(grid[q], +1);
+      for (size_t j = 0; j < n_out; ++j) {
+        int64_t bin = (k_lo + (int64_t)j) % (int64_t)nf;
+        if (bin < 0) bin += (int64_t)nf;
+        const Cx v = grid[q][(size_t)bin];
+        out[q][j] = {v.re * corr[j], v.im * corr[j]};
+      }
+    }
+  }
+};
+
 // ---- `XStage` (default build, twiddle tables) kspace.rs:1052-1140 ----
 struct XStage {
-  size_t snx, nx;
+  size_t snx, nx, xs_ = 0;
+  bool fft = false;
   std::vector<Cx> tw[2];
+  std::vector<Cx> ramp[2], centre;  // the `kspace` build (kspace.rs:1079-1096)
   XStage(size_t snx_, size_t nx_, size_t xs, size_t sxs, double xoff, double ghost) : snx(snx_), nx(nx_) {
     double c = (double)sxs + xoff;
     double gh[2] = {ghost, -ghost};
+    if (g_kspace_build) {
+      fft = true;
+      xs_ = xs;
+      for (int p = 0; p < 2; ++p)
+        for (size_t x = 0; x < snx; ++x) {
+          const double ph = TAU * gh[p] * ((double)x - c) / (double)snx;
+          ramp[p].push_back({std::cos(ph), std::sin(ph)});
+        }
+      for (size_t kxi = 0; kxi < nx; ++kxi) {
+        const double ph = -TAU * ((double)kxi - (double)xs) * c / (double)snx;
+        centre.push_back({std::cos(ph), std::sin(ph)});
+      }
+      return;
+    }
     for (int p = 0; p < 2; ++p) {
       tw[p].reserve(snx * nx);
       for (size_t kxi = 0; kxi < nx; ++kxi) {
@@ -266,6 +349,22 @@ struct XStage {
   }
   void run(const double* g_re, const double* g_im, double ghost_shift, Cx* out) const {
     int pol = ghost_shift < 0.0 ? 1 : 0;
+    if (fft) {  // `XStage::run` kspace.rs:1102-1115: ramp, inverse FFT of length snx, centre phase
+      std::vector<Cx> buf(snx);
+      for (size_t x = 0; x < snx; ++x) {
+        const double rr = ramp[pol][x].re, ri = ramp[pol][x].im;
+        buf[x] = {g_re[x] * rr - g_im[x] * ri, g_re[x] * ri + g_im[x] * rr};
+      }
+      fft1d(buf, +1);
+      for (size_t kxi = 0; kxi < nx; ++kxi) {
+        int64_t bin = ((int64_t)kxi - (int64_t)xs_) % (int64_t)snx;
+        if (bin < 0) bin += (int64_t)snx;
+        const double cr = centre[kxi].re, ci = centre[kxi].im;
+        const Cx v = buf[(size_t)bin];
+        out[kxi] = {v.re * cr - v.im * ci, v.re * ci + v.im * cr};
+      }
+      return;
+    }
     const std::vector<Cx>& t = tw[pol];
     for (size_t kxi = 0; kxi < nx; ++kxi) {
       const Cx* row = &t[snx * kxi];
@@ -360,6 +459,56 @@ std::vector<Cx> build_coil_kspace_timed(const mrsim_slice_input& inp, const mrsi
   std::vector<double> g_re(snx, 0.0), g_im(snx, 0.0);
   XStage xstage(snx, nx, xs, sxs, xoff, acq.ghost_offset);
 
+  // the `kspace` build's NUFFT y-stage (kspace.rs:769-833): with t affine in the line index per
+  // parity, every column's y-sum is one type-1 NUFFT of sources displaced by the fieldmap
+  std::vector<std::vector<Cx>> nufft_rows;  // [c][x + snx kyi]
+  bool have_rows = false;
+  if (g_kspace_build && !do_eddy && ny >= 3 && uniform) {
+    const double tau = (t_ms[2] - t_ms[0]) / 2.0;
+    const double t0 = t_ms[0];
+    const double delta = t_ms[1] - (tau + t0);
+    double tmax = 0.0;
+    for (size_t k = 0; k < ny; ++k) tmax = std::fmax(tmax, std::fabs(t_ms[k]));
+    tmax = std::fmax(tmax, 1e-300);
+    bool affine = true;
+    for (size_t k = 0; k < ny; ++k) {
+      const double pred = tau * (double)k + t0 + (k % 2 == 1 ? delta : 0.0);
+      affine = affine && std::fabs(t_ms[k] - pred) <= 1e-9 * tmax && timing.polarity[k] == (k % 2 == 1 ? -1 : 1);
+    }
+    if (affine) {
+      const double tau_s = tau / 1000.0, delta_s = delta / 1000.0;
+      const double t_centre = (tau * (double)ys + t0) / 1000.0;
+      Nufft1O nufft(sny, -(int64_t)ys, ny, 1e-13);
+      std::vector<double> pos(sny, 0.0);
+      std::vector<std::vector<double>> wre(2 * ncomp, std::vector<double>(sny, 0.0)),
+          wim(2 * ncomp, std::vector<double>(sny, 0.0));
+      std::vector<std::vector<Cx>> out;
+      nufft_rows.assign(ncomp, std::vector<Cx>(snx * ny, CZERO));
+      for (size_t x = 0; x < snx; ++x) {
+        for (size_t y = 0; y < sny; ++y) {
+          const size_t i = x + snx * y;
+          pos[y] = ((double)y - (double)sys - yoff) + (double)sny * tau_s * rate[i];
+          const double ph = phi0[i] + TAU * rate[i] * t_centre;
+          const double c0 = std::cos(ph), s0 = std::sin(ph);
+          const double phd = TAU * rate[i] * delta_s;
+          const double cd = std::cos(phd), sd = std::sin(phd);
+          const double c1 = c0 * cd - s0 * sd, s1 = c0 * sd + s0 * cd;
+          for (size_t c = 0; c < ncomp; ++c) {
+            const double a = amp[i] * (double)inp.compartments[c][i];
+            wre[2 * c][y] = a * c0;
+            wim[2 * c][y] = a * s0;
+            wre[2 * c + 1][y] = a * c1;
+            wim[2 * c + 1][y] = a * s1;
+          }
+        }
+        nufft.run(pos, wre, wim, out);
+        for (size_t c = 0; c < ncomp; ++c)
+          for (size_t kyi = 0; kyi < ny; ++kyi) nufft_rows[c][x + snx * kyi] = out[2 * c + (kyi % 2)][kyi];
+      }
+      have_rows = true;
+    }
+  }
+
   std::vector<Cx> kspace(nx * ny, CZERO);
   bool have_prev = false;
   size_t prev = 0;
@@ -368,7 +517,9 @@ std::vector<Cx> build_coil_kspace_timed(const mrsim_slice_input& inp, const mrsi
     if (!mask[nx * kyi]) continue;
     double t = t_ms[kyi] / 1000.0;
     double trf = trf_ms[kyi];
-    if (have_prev && since_anchor < REANCHOR) {
+    if (have_rows) {
+      // the NUFFT rows replace the rotor state (kspace.rs:848)
+    } else if (have_prev && since_anchor < REANCHOR) {
       size_t p = prev;
       size_t k0 = kyi - p, k1 = p % 2;
       double dt = t - t_ms[p] / 1000.0;
@@ -446,7 +597,14 @@ std::vector<Cx> build_coil_kspace_timed(const mrsim_slice_input& inp, const mrsi
     }
     std::fill(g_re.begin(), g_re.end(), 0.0);
     std::fill(g_im.begin(), g_im.end(), 0.0);
-    for (size_t y = 0; y < sny; ++y) {
+    if (have_rows) {  // kspace.rs:929-937
+      for (size_t c = 0; c < ncomp; ++c)
+        for (size_t x = 0; x < snx; ++x) {
+          g_re[x] += rel[c] * nufft_rows[c][x + snx * kyi].re;
+          g_im[x] += rel[c] * nufft_rows[c][x + snx * kyi].im;
+        }
+    }
+    for (size_t y = 0; y < sny && !have_rows; ++y) {
       size_t row = snx * y;
       double eyr = ey_re[y], eyi = ey_im[y];
       for (size_t x = 0; x < snx; ++x) {
@@ -642,6 +800,40 @@ std::vector<Cx> reference_coil_kspace(const mrsim_slice_input& inp, const mrsim_
     }
   }
   return kspace;
+}
+
+// ---- `inverse_2d_fft` kspace.rs:1385-1424 (the `kspace` build): pre-modulation, forward FFTs
+// along x then y (rustfft's e^{-i}, here fft1d), post-modulation with the constant phase ----
+std::vector<Cx> inverse_2d_fft(const std::vector<Cx>& k, size_t nx, size_t ny, size_t xs, size_t ys) {
+  const double nxf = (double)nx, nyf = (double)ny, xsf = (double)xs, ysf = (double)ys;
+  std::vector<Cx> buf(nx * ny);
+  for (size_t i = 0; i < nx * ny; ++i) {
+    const double kx = (double)(i % nx), ky = (double)(i / nx);
+    const double ph = TAU * (kx * xsf / nxf + ky * ysf / nyf);
+    const double c = std::cos(ph), sn = std::sin(ph);
+    buf[i] = {k[i].re * c - k[i].im * sn, k[i].re * sn + k[i].im * c};
+  }
+  std::vector<Cx> line(nx);
+  for (size_t ky = 0; ky < ny; ++ky) {
+    for (size_t x = 0; x < nx; ++x) line[x] = buf[ky * nx + x];
+    fft1d(line, -1);
+    for (size_t x = 0; x < nx; ++x) buf[ky * nx + x] = line[x];
+  }
+  std::vector<Cx> col(ny);
+  for (size_t kx = 0; kx < nx; ++kx) {
+    for (size_t y = 0; y < ny; ++y) col[y] = buf[y * nx + kx];
+    fft1d(col, -1);
+    for (size_t y = 0; y < ny; ++y) buf[y * nx + kx] = col[y];
+  }
+  const double const_ph = -TAU * (xsf * xsf / nxf + ysf * ysf / nyf);
+  std::vector<Cx> out(nx * ny);
+  for (size_t i = 0; i < nx * ny; ++i) {
+    const double x = (double)(i % nx), y = (double)(i / nx);
+    const double ph = TAU * (x * xsf / nxf + y * ysf / nyf) + const_ph;
+    const double c = std::cos(ph), sn = std::sin(ph);
+    out[i] = {buf[i].re * c - buf[i].im * sn, buf[i].re * sn + buf[i].im * c};
+  }
+  return out;
 }
 
 // ---- `inverse_2d` kspace.rs:1428-1453 ----
@@ -864,7 +1056,8 @@ SliceRecon reconstruct_coils_full(std::vector<std::vector<Cx>> coil_kspace, cons
   std::vector<Cx> wsum(nx * ny, CZERO);
   std::vector<double> ssum(nx * ny, 0.0);
   for (size_t coil = 0; coil < ncoils; ++coil) {
-    auto img = inverse_2d(coil_kspace[coil], nx, ny, xs, ys);
+    auto img = g_kspace_build ? inverse_2d_fft(coil_kspace[coil], nx, ny, xs, ys)
+                              : inverse_2d(coil_kspace[coil], nx, ny, xs, ys);
     for (size_t i = 0; i < nx * ny; ++i) {
       double s = R.sensitivities[coil][i];
       wsum[i] = cadd(wsum[i], cscale(img[i], s));
@@ -3601,6 +3794,16 @@ int64_t oracle_golden_output(int i, uint32_t* out, int64_t cap) {
   if (out && cap >= (int64_t)b.size()) memcpy(out, b.data(), b.size() * 4);
   return (int64_t)b.size();
 }
+
+// The reference's `kspace` build (1) or its default build (0) for every later oracle call.
+void oracle_set_kspace_build(int on) {
+  if ((on ? 1 : 0) != g_kspace_build) {  // the cached golden outputs belong to the other build
+    delete g_golden;
+    g_golden = nullptr;
+  }
+  g_kspace_build = on ? 1 : 0;
+}
+int oracle_kspace_build(void) { return g_kspace_build; }
 
 
 int oracle_nufft2(int32_t type, const int64_t* n, const int64_t* m_lo, const int64_t* m_out, double tol,

@@ -38,6 +38,8 @@ def lib():
         L.oracle_golden_name.restype = C.c_char_p
         L.oracle_golden_output.restype = C.c_int64
         L.oracle_golden_output.argtypes = [C.c_int, P(C.c_uint32), C.c_int64]
+        L.oracle_set_kspace_build.argtypes = [C.c_int]
+        L.oracle_kspace_build.restype = C.c_int
         L.oracle_build_coil_kspace.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), C.c_int64, C.c_int64,
                                                abi.c_f64p, abi.c_f64p, abi.c_f64p, P(C.c_int8), abi.c_f64p, abi.c_f64p]
         L.oracle_reference_coil_kspace.argtypes = [P(abi.SliceInput_), P(abi.Acquisition_), C.c_int64, C.c_int64,
@@ -112,16 +114,37 @@ def _check(status):
 
 
 # ---- golden record -----------------------------------------------------------------------------
-def golden_outputs() -> list[tuple[str, np.ndarray]]:
-    """The reference's golden record regenerated by the oracle: (name, uint32 bit patterns)."""
+def set_kspace_build(on: bool) -> None:
+    """Every later oracle call follows the reference's `kspace` build (NUFFT y-stage, FFT x-stage
+    and inverse; on) or its default build (off)."""
+    lib().oracle_set_kspace_build(1 if on else 0)
+
+
+class kspace_build:
+    """`with oracle.kspace_build(): ...` runs the block under the reference's `kspace` build."""
+
+    def __enter__(self):
+        set_kspace_build(True)
+
+    def __exit__(self, *exc):
+        set_kspace_build(False)
+
+
+def golden_outputs(kspace: bool = False) -> list[tuple[str, np.ndarray]]:
+    """The reference's golden record regenerated by the oracle: (name, uint32 bit patterns), of
+    the default build or (kspace=True) of the `kspace` build."""
     L = lib()
     out = []
-    for i in range(L.oracle_golden_count()):
-        name = L.oracle_golden_name(i).decode()
-        n = L.oracle_golden_output(i, None, 0)
-        buf = np.zeros(n, np.uint32)
-        L.oracle_golden_output(i, buf.ctypes.data_as(C.POINTER(C.c_uint32)), n)
-        out.append((name, buf))
+    set_kspace_build(kspace)
+    try:
+        for i in range(L.oracle_golden_count()):
+            name = L.oracle_golden_name(i).decode()
+            n = L.oracle_golden_output(i, None, 0)
+            buf = np.zeros(n, np.uint32)
+            L.oracle_golden_output(i, buf.ctypes.data_as(C.POINTER(C.c_uint32)), n)
+            out.append((name, buf))
+    finally:
+        set_kspace_build(False)
     return out
 
 

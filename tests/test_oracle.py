@@ -2,8 +2,9 @@
 
 - the 41 golden fixture files of the reference (tests/fixtures/p4_baseline/default), bit for bit;
 - the reference's second record, of its `kspace` build (tests/fixtures/p4_baseline/kspace): the
-  same 41 cases, equal to the `default` record except one f32 word in each of two files, so the
-  oracle (the `default` arithmetic) is within 1 ulp of that word and bit-exact elsewhere;
+  same 41 cases, equal to the `default` record except one f32 word in each of two files; the
+  oracle's default build is within 1 ulp of that word and bit-exact elsewhere, and the oracle's
+  `kspace` build (NUFFT y-stage, FFT x-stage, FFT inverse) reproduces it bit for bit;
 - `restructured_forward_matches_the_literal_sum` (kspace.rs:3362-3433): rotor path vs literal sum
   to 1e-10 of peak over 16 effects x 3 geometries;
 - `eddy_drive_some_reproduces_the_bvec_bval_product` (kspace.rs:3476-3504): 8 f64 bit patterns.
@@ -58,6 +59,20 @@ def test_oracle_is_within_one_ulp_of_the_kspace_record():
         d = np.abs(want.astype(np.int64) - bits.astype(np.int64))
         assert d.max() <= 1, name
         assert np.count_nonzero(d) <= 1, name
+
+
+def test_oracle_kspace_build_reproduces_the_kspace_record_bit_for_bit():
+    """The reference's `kspace` build restated (kspace.rs:769-833 NUFFT y-stage through `Nufft1`,
+    kspace.rs:1079-1123 FFT x-stage, kspace.rs:1385-1424 `inverse_2d_fft`): every word of the
+    `kspace` record, including the two where it differs from the default record."""
+    outs = oracle.golden_outputs(kspace=True)
+    assert len(outs) == 41
+    for name, bits in outs:
+        want = np.fromfile(GOLD_KSPACE / f"{name}.bin", dtype="<u4")
+        assert want.shape == bits.shape, name
+        diff = np.nonzero(want != bits)[0]
+        assert diff.size == 0, f"{name}: {diff.size} words differ"
+    assert oracle.lib().oracle_kspace_build() == 0  # the default build again afterwards
 
 
 def test_oracle_reproduces_the_golden_record_bit_for_bit():
