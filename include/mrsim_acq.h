@@ -325,7 +325,7 @@ int mrsim_epi_operator_adjoint_host(mrsim_epi_operator* op, const float* kspace,
 int mrsim_epi_operator_apply_host(mrsim_epi_operator* op, const float* const* images,
                                   float* kspace, float* comp_grad, float* fmap_grad,
                                   float* r2_grad);
-/* The time-segmented y-stages of the pair (the north star's tensor-core form of the exact DFT; no
+/* The time-segmented y-stages of the pair (a tensor-core form of the exact DFT; no
  * reference counterpart: the reference segments only the spiral forward, `tseg::plan`
  * tseg.rs:230-289 via spiral.rs:141-201).  precision 0 restores the exact per-line phasors;
  * 1 selects contractions in split f16 (hi + lo operands, three products, FP32 accumulation),
@@ -751,7 +751,8 @@ int mrsim_simulate_acquisition_3d_spiral(mrsim_context* ctx, const mrsim_acquisi
 /* `SpiralSegmentation` / `spiral_segmentation` (kspace3d.rs:860-870, 1441-1470): the certified
  * time segmentations a spiral series will use, per slice and mode (class first), or the error
  * naming the slice whose rate rectangle cannot be certified.  Images are not read.  With rows
- * NULL only *count is written. */
+ * NULL only *count is written.  Planned on the host (no context): the series plans with its fits
+ * on the device, which choose the same L and m; b_sum and the bound agree to ~1e-6 relative. */
 typedef struct mrsim_spiral_segmentation_row {
   int32_t z, voxel, l, m;
   double b_sum, bound;
@@ -812,6 +813,15 @@ typedef struct mrsim_tseg_info {
 int mrsim_tseg_plan(const double* tau_ms, int64_t n_tau, double t_ms, const double d[2],
                     const double f[2], int64_t l_capacity, double* tau_l, double* b,
                     mrsim_tseg_info* info);
+/* The same plan with every fit's per-sample work (right-hand sides over the rate grid, the
+ * factored least-squares solve, the residual) on the context's device in FP64; the Jacobi
+ * factorisation and the search over L and m stay on the host.  This is the planner the device
+ * forwards use.  Same L and m as mrsim_tseg_plan; b_sum and the bound agree to ~1e-6 relative
+ * and b to the conditioning of the truncated least-squares problem (CUDA's exp / sin / cos round
+ * differently from the host's in the last bit). */
+int mrsim_tseg_plan_device(mrsim_context* ctx, const double* tau_ms, int64_t n_tau, double t_ms,
+                           const double d[2], const double f[2], int64_t l_capacity, double* tau_l,
+                           double* b, mrsim_tseg_info* info);
 
 /* `epg_cpmg` (epg.rs:101-125): ln A_e for e = 1..n_echoes of a CPMG train. */
 int mrsim_epg_cpmg(int64_t n_echoes, double esp_ms, double refocusing_deg, double t1_ms,

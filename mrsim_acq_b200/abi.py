@@ -340,6 +340,8 @@ def _declare(lib):
                                               C.c_int64, c_f64p, c_f64p, C.POINTER(SpiralInfo_)]),
         "mrsim_tseg_plan": (C.c_int, [c_f64p, C.c_int64, C.c_double, c_f64p, c_f64p, C.c_int64, c_f64p, c_f64p,
                                       C.POINTER(TsegInfo_)]),
+        "mrsim_tseg_plan_device": (C.c_int, [P, c_f64p, C.c_int64, C.c_double, c_f64p, c_f64p, C.c_int64, c_f64p,
+                                             c_f64p, C.POINTER(TsegInfo_)]),
         "mrsim_epg_cpmg": (C.c_int, [C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double, c_f64p]),
         "mrsim_nufft_kernel_width": (C.c_int, [C.c_double]),
         "mrsim_nufft1": (C.c_int, [P, C.c_int64, C.c_int64, C.c_int64, C.c_double, c_f64p, C.c_int64, c_f64p,

@@ -876,15 +876,14 @@ int mrsim_spiral_trajectory(int64_t nx, int64_t ny, int64_t interleaves, double 
   });
 }
 
-int mrsim_tseg_plan(const double* tau_ms, int64_t n_tau, double t_ms, const double d[2], const double f[2],
-                    int64_t l_capacity, double* tau_l, double* b, mrsim_tseg_info* info) {
-  return guarded([&] {
+static void tseg_plan_out(mrsim::TsegDevice* dev, const double* tau_ms, int64_t n_tau, double t_ms, const double d[2],
+                          const double f[2], int64_t l_capacity, double* tau_l, double* b, mrsim_tseg_info* info) {
     need(d, "d");
     need(f, "f");
     need(info, "info");
     if (n_tau > 0) need(tau_ms, "tau_ms");
     std::vector<double> tau(tau_ms, tau_ms + std::max<int64_t>(0, n_tau));
-    mrsim::TsegPlan p = mrsim::tseg_plan(tau, t_ms, d, f);
+    mrsim::TsegPlan p = mrsim::tseg_plan(tau, t_ms, d, f, dev);
     info->l = p.l;
     info->m = p.m;
     info->b_sum = p.b_sum;
@@ -894,6 +893,18 @@ int mrsim_tseg_plan(const double* tau_ms, int64_t n_tau, double t_ms, const doub
     if (l_capacity < p.l) mrsim::fail("segment capacity below the plan's L");
     if (tau_l) std::memcpy(tau_l, p.tau_l.data(), p.tau_l.size() * 8);
     if (b) std::memcpy(b, p.b.data(), p.b.size() * 8);
+}
+
+int mrsim_tseg_plan(const double* tau_ms, int64_t n_tau, double t_ms, const double d[2], const double f[2],
+                    int64_t l_capacity, double* tau_l, double* b, mrsim_tseg_info* info) {
+  return guarded([&] { tseg_plan_out(nullptr, tau_ms, n_tau, t_ms, d, f, l_capacity, tau_l, b, info); });
+}
+
+int mrsim_tseg_plan_device(mrsim_context* ctx, const double* tau_ms, int64_t n_tau, double t_ms, const double d[2],
+                           const double f[2], int64_t l_capacity, double* tau_l, double* b, mrsim_tseg_info* info) {
+  return on_ctx(ctx, [&] {
+    mrsim::TsegDevice dev(ctx->stream);
+    tseg_plan_out(&dev, tau_ms, n_tau, t_ms, d, f, l_capacity, tau_l, b, info);
   });
 }
 

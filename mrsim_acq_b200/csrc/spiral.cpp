@@ -324,7 +324,11 @@ SegmentedInfo spiral_segmented_host(mrsim_context* ctx, const mrsim_slice_input&
     rate[i] = make_float2((float)(-d), (float)(kTau * s.rate[i] / 1000.0));
   }
   std::vector<double> tau(tau_ms, tau_ms + ntau);
-  TsegPlan plan = tseg_plan(tau, t_ms, rect_d, rect_f);
+  TsegPlan plan;
+  {
+    TsegDevice dev(st);
+    plan = tseg_plan(tau, t_ms, rect_d, rect_f, &dev);
+  }
   SegmentedInfo info;
   info.l = plan.l;
   info.m = plan.m;

@@ -13,11 +13,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -606,7 +610,8 @@ static void build_sources(SpiralPlan3& P, const mrsim_acquisition& acq) {
 }
 
 static SpiralPlan3 make_spiral_plan(const mrsim_acquisition_3d_input& in, const mrsim_acquisition& acq,
-                                    const mrsim_echo_train& train, const mrsim_spiral_readout& ro, int rows) {
+                                    const mrsim_echo_train& train, const mrsim_spiral_readout& ro, int rows,
+                                    cudaStream_t st) {
   SpiralPlan3 P;
   P.nc = (int)std::max<int64_t>(acq.n_coils, 1);
   if (P.nc > kMaxCoils) fail("more than 64 coils");
@@ -645,14 +650,68 @@ static SpiralPlan3 make_spiral_plan(const mrsim_acquisition_3d_input& in, const 
   P.modes = resolve_modes(in.t2, in.t1, in.t_inhom, P.ncomp, acq, train, P.nvox);
   for (auto& m : P.modes) (m.voxel ? P.any_voxel : P.any_class) = true;
   build_sources(P, acq);
-  // per-slice certified segmentations
   P.class_plan.resize(P.nz);
   P.voxel_plan.resize(P.nz);
+  // per-slice certified segmentations: each distinct rate rectangle planned once (slices that
+  // share one get the same plan bit for bit), the distinct ones on up to 16 host threads, each
+  // with its fits' per-sample work on the device on a stream of its own; the first failure in
+  // slice order is the one reported, as a sequential plan would report it
   std::vector<double> tau(P.table.traj.tau_ms);
+  std::vector<std::array<double, 4>> keys;
+  std::vector<int> cls_of(P.nz, -1), vox_of(P.nz, -1);
+  auto key_of = [&](const double d[2], const double f[2]) {
+    const std::array<double, 4> k{d[0], d[1], f[0], f[1]};
+    for (size_t i = 0; i < keys.size(); ++i)
+      if (keys[i] == k) return (int)i;
+    keys.push_back(k);
+    return (int)keys.size() - 1;
+  };
   for (const SliceRect& r : spiral_rects(in, acq, P.modes, P.plane, P.nz)) {
     const double zero[2] = {0.0, 0.0};
-    if (P.any_class) P.class_plan[r.z] = tseg_plan(tau, P.table.traj.readout_ms, zero, r.f);
-    if (r.has_d) P.voxel_plan[r.z] = tseg_plan(tau, P.table.traj.readout_ms, r.d, r.f);
+    if (P.any_class) cls_of[r.z] = key_of(zero, r.f);
+    if (r.has_d) vox_of[r.z] = key_of(r.d, r.f);
+  }
+  std::vector<TsegPlan> plans(keys.size());
+  std::vector<std::exception_ptr> errs(keys.size());
+  int dev_id = 0;
+  MRSIM_CUDA(cudaGetDevice(&dev_id));
+  std::atomic<int> next{0};
+  std::mutex setup_mu;
+  std::exception_ptr setup_err;  // a worker that could not set up its stream
+  auto worker = [&] {
+    cudaStream_t ws = nullptr;
+    try {
+      MRSIM_CUDA(cudaSetDevice(dev_id));
+      MRSIM_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
+      TsegDevice dev(ws);
+      for (int i; (i = next.fetch_add(1)) < (int)keys.size();) {
+        try {
+          const double d[2] = {keys[i][0], keys[i][1]}, f[2] = {keys[i][2], keys[i][3]};
+          plans[i] = tseg_plan(tau, P.table.traj.readout_ms, d, f, &dev);
+        } catch (...) {
+          errs[i] = std::current_exception();
+        }
+      }
+    } catch (...) {
+      std::lock_guard<std::mutex> lk(setup_mu);
+      if (!setup_err) setup_err = std::current_exception();
+    }
+    if (ws) cudaStreamDestroy(ws);
+  };
+  const int nt = (int)std::min<size_t>(keys.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  if (nt <= 1) {
+    worker();
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+  }
+  if (setup_err) std::rethrow_exception(setup_err);
+  for (auto& e : errs)
+    if (e) std::rethrow_exception(e);
+  for (int z = 0; z < P.nz; ++z) {
+    if (cls_of[z] >= 0) P.class_plan[z] = plans[cls_of[z]];
+    if (vox_of[z] >= 0) P.voxel_plan[z] = plans[vox_of[z]];
   }
   // the centred z-DFT kernel, the ring z profiles, the object phase, the half-cell phase
   const double zs = (double)(P.nz / 2);
@@ -1068,7 +1127,7 @@ void spiral3d_samples(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, 
                       int g, float* out) {
   cudaStream_t st = ctx->stream;
   const int rows = opts ? (int)opts->coil_rows : 1;
-  SpiralPlan3 P = make_spiral_plan(in, acq, train, ro, rows);
+  SpiralPlan3 P = make_spiral_plan(in, acq, train, ro, rows, st);
   if (g < 0 || g >= (int)in.n_volumes) fail("volume index out of range");
   DevArena A;
   SpiralInputs I = upload_spiral_inputs(A, P, in, in.images, (int)in.n_volumes, acq, st);
@@ -1091,7 +1150,7 @@ void spiral3d_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, 
                       uint64_t seed, float* mag, float* ph) {
   cudaStream_t st = ctx->stream;
   const int rows = opts ? (int)opts->coil_rows : 1;
-  SpiralPlan3 P = make_spiral_plan(in, acq, train, ro, rows);
+  SpiralPlan3 P = make_spiral_plan(in, acq, train, ro, rows, st);
   const int nv = (int)in.n_volumes, nz = P.nz, nc = P.nc, n = P.n, nsamp = P.nsamp;
   const double sigma = std::sqrt(acq.noise_variance / (double)((size_t)n * n));
   DevArena A;

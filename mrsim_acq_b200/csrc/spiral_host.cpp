@@ -200,7 +200,8 @@ struct FitOut {
 };
 
 // `fit` (tseg.rs:185-227): least-squares interpolators over the rate grid
-FitOut fit(const std::vector<double>& tau, double t, int l, const std::vector<std::pair<double, double>>& rates) {
+FitOut fit(const std::vector<double>& tau, double t, int l, const std::vector<std::pair<double, double>>& rates,
+           TsegDevice* dev) {
   FitOut o;
   o.tau_l.resize(l);
   for (int i = 0; i < l; ++i) o.tau_l[i] = l == 1 ? 0.0 : t * (double)i / (double)(l - 1);
@@ -216,6 +217,10 @@ FitOut fit(const std::vector<double>& tau, double t, int l, const std::vector<st
       cols[l + i][g + k] = c;
     }
   Lsq p = Lsq::make(cols);
+  if (dev) {  // the per-sample solve and residual on the device; b stays there until accepted
+    dev->fit(rates, cols, p.left, p.right, p.sig, l, &o.b_sum, &o.err);
+    return o;
+  }
   std::vector<double> y(2 * g);
   o.b.reserve(tau.size() * l * 2);
   for (double tj : tau) {
@@ -245,7 +250,8 @@ FitOut fit(const std::vector<double>& tau, double t, int l, const std::vector<st
 }
 }  // namespace
 
-TsegPlan tseg_plan(const std::vector<double>& tau, double t_ms, const double d[2], const double f[2]) {
+TsegPlan tseg_plan(const std::vector<double>& tau, double t_ms, const double d[2], const double f[2],
+                   TsegDevice* dev) {
   char buf[512];
   if (!(d[0] >= 0.0 && d[1] >= d[0] && f[1] >= f[0])) {
     std::snprintf(buf, sizeof buf, "rate rectangle RateRect { d: [%g, %g], f: [%g, %g] }", d[0], d[1], f[0], f[1]);
@@ -265,6 +271,7 @@ TsegPlan tseg_plan(const std::vector<double>& tau, double t_ms, const double d[2
     fail(buf);
   }
   int l = (int)std::ceil((t_ms / 1000.0) * (f[1] - f[0])) + 2;
+  if (dev) dev->set_times(tau);
   for (;;) {
     if (l > kLMax) {
       std::snprintf(buf, sizeof buf,
@@ -285,7 +292,7 @@ TsegPlan tseg_plan(const std::vector<double>& tau, double t_ms, const double d[2
       std::vector<std::pair<double, double>> rates;
       for (double dd : ds)
         for (double w : fs) rates.emplace_back(-dd, w);
-      FitOut o = fit(tau, t_ms, l, rates);
+      FitOut o = fit(tau, t_ms, l, rates, dev);
       const double rem = rem_total(m, o.b_sum);
       if (rem >= kRemainderTarget && m < kMMax) {
         ++m;
@@ -301,7 +308,10 @@ TsegPlan tseg_plan(const std::vector<double>& tau, double t_ms, const double d[2
         p.l = l;
         p.m = m;
         p.tau_l = o.tau_l;
-        p.b = o.b;
+        if (dev)
+          dev->fetch_b(p.b);
+        else
+          p.b = o.b;
         p.b_sum = o.b_sum;
         p.grid_err = o.err;
         p.bound = bound;

@@ -1,6 +1,9 @@
 // spiral_host.h — host plans of the stack-of-spirals path (see spiral_host.cpp).
 #pragma once
 
+#include <cuda_runtime.h>
+
+#include <utility>
 #include <vector>
 
 namespace mrsim {
@@ -25,7 +28,35 @@ struct TsegPlan {
   std::vector<double> b;      // [sample][segment] (re, im)
   double b_sum = 0, grid_err = 0, bound = 0;
 };
-TsegPlan tseg_plan(const std::vector<double>& tau, double t_ms, const double d[2], const double f[2]);
+
+// The per-sample half of every fit of a plan on the device (tseg_fit.cu, FP64): right-hand
+// sides, factored solve and residual for all sample times at once; the factorisation and the
+// search over L and m stay on the host.  One object serves the plans of one call on one stream.
+class TsegDevice {
+ public:
+  explicit TsegDevice(cudaStream_t st);
+  ~TsegDevice();
+  TsegDevice(const TsegDevice&) = delete;
+  TsegDevice& operator=(const TsegDevice&) = delete;
+  void set_times(const std::vector<double>& tau);
+  // one fit over the rate grid: the maxima b_sum and err; b stays on the device
+  void fit(const std::vector<std::pair<double, double>>& rates, const std::vector<std::vector<double>>& cols,
+           const std::vector<std::vector<double>>& left, const std::vector<std::vector<double>>& right,
+           const std::vector<double>& sig, int l, double* b_sum, double* err);
+  // the last fit's b, [sample][segment] (re, im)
+  void fetch_b(std::vector<double>& b) const;
+
+ private:
+  struct Bufs;
+  cudaStream_t st_;
+  Bufs* d_;
+  int n_tau_ = 0, l_ = 0;
+};
+
+// With `dev` the fits' per-sample work runs on the device (the product's path); without it on
+// the host (planning without a GPU, and the host reference of the device fit).
+TsegPlan tseg_plan(const std::vector<double>& tau, double t_ms, const double d[2], const double f[2],
+                   TsegDevice* dev = nullptr);
 
 // `epg_cpmg` epg.rs:101-125: ln A_e, e = 1..n_echoes.
 std::vector<double> epg_cpmg(int n_echoes, double esp_ms, double refocusing_deg, double t1_ms, double t2_ms);

@@ -779,6 +779,7 @@ TsPlan* ts_plan_build(const EpiOperator& op, int precision) {
   const int snx = op.snx, sny = op.sny, nx = op.nx, ny = op.ny, ncomp = op.ncomp;
   const mrsim_acquisition& acq = op.acq;
   cudaStream_t st = op.ctx->stream;
+  TsegDevice fitdev(st);  // the segmentation fits' per-sample work
 
   // coil classes (the geometry's bitwise-equal ey rows) plus the offset row
   std::vector<float> eyc((size_t)op.geo.ncls * sny);
@@ -889,7 +890,7 @@ TsPlan* ts_plan_build(const EpiOperator& op, int precision) {
       plan.bound = 0.0;
     } else {
       const double d[2] = {0.0, dhi - dlo}, f[2] = {fmin, fmax};
-      plan = tseg_plan(tau, Tms, d, f);
+      plan = tseg_plan(tau, Tms, d, f, &fitdev);
     }
     if (plan.l > kTsMaxL) fail("the segmented path supports at most 32 segments per group");
     G.L = plan.l;

@@ -79,11 +79,26 @@ def _pair(v) -> np.ndarray:
     return np.ascontiguousarray([float(v[0]), float(v[1])], dtype=np.float64)
 
 
-def tseg_plan(tau: np.ndarray, t_ms: float, rect: RateRect) -> TsegPlan:
+_TSEG_L_MAX = 64  # the planner refuses past 64 segments
+
+
+def tseg_plan(tau: np.ndarray, t_ms: float, rect: RateRect, ctx: Optional[Context] = None) -> TsegPlan:
+    """`tseg::plan`.  With `ctx` the fits' per-sample work runs on that context's device in FP64
+    (the planner the device forwards use: the same L and m, b_sum and bound to ~1e-6); without it
+    the whole plan runs on the host."""
     tau = np.ascontiguousarray(tau, dtype=np.float64)
     d, f = _pair(rect.d), _pair(rect.f)
     info = abi.TsegInfo_()
     tp = tau.ctypes.data_as(abi.c_f64p)
+    if ctx is not None:
+        tau_l = np.zeros(_TSEG_L_MAX)
+        b = np.zeros(len(tau) * _TSEG_L_MAX * 2)
+        check(lib().mrsim_tseg_plan_device(ctx.handle, tp, len(tau), t_ms, d.ctypes.data_as(abi.c_f64p),
+                                           f.ctypes.data_as(abi.c_f64p), _TSEG_L_MAX, tau_l.ctypes.data_as(abi.c_f64p),
+                                           b.ctypes.data_as(abi.c_f64p), C.byref(info)))
+        L = int(info.l)
+        return TsegPlan(L, int(info.m), tau_l[:L].copy(), b[:len(tau) * L * 2].view(np.complex128).reshape(len(tau), L),
+                        info.b_sum, info.grid_err, info.bound)
     check(lib().mrsim_tseg_plan(tp, len(tau), t_ms, d.ctypes.data_as(abi.c_f64p), f.ctypes.data_as(abi.c_f64p), 0,
                                 None, None, C.byref(info)))
     L = int(info.l)
