@@ -756,6 +756,9 @@ def main():
     ap.add_argument("--spin-volumes", type=int, default=40, help="volumes of the spin-history series")
     ap.add_argument("--spiral-only", action="store_true",
                     help="run only the stack-of-spirals volume and print its line (profiling)")
+    ap.add_argument("--pipeline-only", action="store_true",
+                    help="run only the whole-pipeline series (with --volumes: a smaller one) and print its line "
+                         "(profiling)")
     args = ap.parse_args()
     if args.volumes > 0:
         WORKLOAD["nv"] = args.volumes
@@ -770,6 +773,11 @@ def main():
     if args.spiral_only:
         from mrsim_acq_b200 import api
         print(json.dumps(spiral_measurement(api.Context(local_rank), reps=1)), flush=True)
+        return
+    if args.pipeline_only:
+        from mrsim_acq_b200 import api
+        print(json.dumps(pipeline_measurement(api.Context(local_rank), make_inputs(seed=1), make_acquisition(),
+                                              cpu=not args.no_cpu_baseline)), flush=True)
         return
     if args.spin_history_only:
         import torch

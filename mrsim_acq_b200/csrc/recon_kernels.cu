@@ -10,17 +10,12 @@
 
 #include <algorithm>
 
+#include "hermitian_solve.cuh"
 #include "recon_kernels.h"
 
 namespace mrsim {
 
 namespace {
-
-struct cd {
-  double re, im;
-};
-__device__ __forceinline__ cd cmul(cd a, cd b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
-__device__ __forceinline__ double cabs2(cd a) { return a.re * a.re + a.im * a.im; }
 
 // The source feature i of GRAPPA at readout kx: lines s0/s1, readout offsets -1/0/+1 (wrapped),
 // every coil; layout (line*3 + point)*nc + coil (`grappa_feature`, kspace.rs:1526-1538).
@@ -63,15 +58,8 @@ __global__ void grappa_normal_kernel(const GrappaSystem* __restrict__ sys) {
   S.work[(size_t)i * cols + j] = make_double2(ar, ai);
 }
 
-__device__ __forceinline__ cd recip(cd d) {
-  double m2 = d.re * d.re + d.im * d.im;
-  if (m2 < 1e-18) return {0.0, 0.0};
-  return {d.re / m2, -d.im / m2};
-}
-
-// One CTA per system: scale by the mean diagonal, add the Tikhonov term, pivoted Gaussian
-// elimination on [H | B] with every right-hand side at once (the pivots depend on H alone, so each
-// column of B sees the reference's sequence of operations), then back substitution per column.
+// One CTA per system: scale by the mean diagonal, add the Tikhonov term, then the pivoted
+// Gaussian elimination of [H | B] with every right-hand side at once (hermitian_solve.cuh).
 __global__ void __launch_bounds__(256) grappa_solve_kernel(const GrappaSystem* __restrict__ sys, double lambda) {
   const GrappaSystem& S = sys[blockIdx.x];
   const int nf = 6 * S.nc, nc = S.nc;
@@ -94,94 +82,15 @@ __global__ void __launch_bounds__(256) grappa_solve_kernel(const GrappaSystem* _
     return;
   }
   const double sc = s_scale;
-  for (int e = threadIdx.x; e < nf * cols; e += blockDim.x) {
+  for (int e = threadIdx.x; e < nf * cols; e += blockDim.x) {  // (scale, then add: two roundings)
     double2 v = W[e];
-    v.x *= sc;
-    v.y *= sc;
-    if (e / cols == e % cols) v.x += lambda;
+    v.x = __dmul_rn(v.x, sc);
+    v.y = __dmul_rn(v.y, sc);
+    if (e / cols == e % cols) v.x = __dadd_rn(v.x, lambda);
     W[e] = v;
   }
   __syncthreads();
-  double* fre = S.fscratch;
-  double* fim = S.fscratch + nf;
-  for (int col = 0; col < nf; ++col) {
-    // pivot: first row of largest |h[r][col]| among r >= col
-    double best = -1.0;
-    int bi = col;
-    for (int r = col + threadIdx.x; r < nf; r += blockDim.x) {
-      double2 h = W[(size_t)r * cols + col];
-      double m = sqrt(h.x * h.x + h.y * h.y);
-      if (m > best) {
-        best = m;
-        bi = r;
-      }
-    }
-    red_v[threadIdx.x] = best;
-    red_i[threadIdx.x] = bi;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double b = red_v[0];
-      int p = red_i[0];
-      for (int t = 1; t < blockDim.x; ++t)
-        if (red_v[t] > b || (red_v[t] == b && red_i[t] < p)) {
-          b = red_v[t];
-          p = red_i[t];
-        }
-      // the reference keeps `col` unless a later row is strictly larger
-      double2 hc = W[(size_t)col * cols + col];
-      if (!(b > sqrt(hc.x * hc.x + hc.y * hc.y))) p = col;
-      red_i[0] = p;
-    }
-    __syncthreads();
-    const int piv = red_i[0];
-    if (piv != col)
-      for (int c = threadIdx.x; c < cols; c += blockDim.x) {
-        double2 a = W[(size_t)col * cols + c];
-        W[(size_t)col * cols + c] = W[(size_t)piv * cols + c];
-        W[(size_t)piv * cols + c] = a;
-      }
-    __syncthreads();
-    const double2 dd = W[(size_t)col * cols + col];
-    const cd dinv = recip({dd.x, dd.y});
-    for (int r = col + 1 + threadIdx.x; r < nf; r += blockDim.x) {
-      double2 h = W[(size_t)r * cols + col];
-      cd f = cmul({h.x, h.y}, dinv);
-      fre[r] = f.re;
-      fim[r] = f.im;
-    }
-    __syncthreads();
-    const int rows = nf - col - 1, width = cols - col;
-    for (int e = threadIdx.x; e < rows * width; e += blockDim.x) {
-      const int r = col + 1 + e / width, c = col + e % width;
-      const double2 p = W[(size_t)col * cols + c];
-      cd s = cmul({fre[r], fim[r]}, {p.x, p.y});
-      double2 h = W[(size_t)r * cols + c];
-      h.x = h.x + (-s.re);
-      h.y = h.y + (-s.im);
-      W[(size_t)r * cols + c] = h;
-    }
-    __syncthreads();
-  }
-  // back substitution, one thread per right-hand side (output coil)
-  for (int co = threadIdx.x; co < nc; co += blockDim.x) {
-    double* xre = S.fscratch + 2 * nf + (size_t)co * 2 * nf;
-    double* xim = xre + nf;
-    for (int col = nf - 1; col >= 0; --col) {
-      double2 b = W[(size_t)col * cols + nf + co];
-      cd s = {b.x, b.y};
-      for (int c = col + 1; c < nf; ++c) {
-        double2 h = W[(size_t)col * cols + c];
-        cd t = cmul({h.x, h.y}, {xre[c], xim[c]});
-        s.re = s.re + (-t.re);
-        s.im = s.im + (-t.im);
-      }
-      double2 d = W[(size_t)col * cols + col];
-      cd x = cmul(s, recip({d.x, d.y}));
-      xre[col] = x.re;
-      xim[col] = x.im;
-    }
-    for (int f = 0; f < nf; ++f) S.weights[(size_t)co * nf + f] = make_float2((float)xre[f], (float)xim[f]);
-  }
+  hermitian_solve_block(W, nf, nc, S.fscratch, S.fscratch + nf, S.fscratch + 2 * nf, S.weights, red_v, red_i);
 }
 
 // GRAPPA apply: one thread per (missing line, kx, output coil) of one (unit, echo).

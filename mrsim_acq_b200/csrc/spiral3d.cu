@@ -8,7 +8,7 @@
 // segment), one batched type-2 NUFFT and one combination kernel give every element's samples;
 // one kernel forms the z-DFT with the rings' z profiles, echo amplitudes and line weights for
 // every coil; the noise runs on the (volume, partition, coil) streams; the kz GRAPPA kernel is
-// fitted once (normal equations accumulated in FP64 on the device, solved on the host) and
+// fitted once (normal equations accumulated and solved in FP64 on the device) and
 // applied by one kernel; the inverse z-DFT feeds the FP64 spiral reconstruction of every slice.
 #include <cuda_runtime.h>
 
@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "driver.h"
+#include "hermitian_solve.cuh"
 #include "host3d.h"
 #include "host_tables.h"
 #include "mrsim_internal.h"
@@ -292,6 +293,58 @@ __global__ void __launch_bounds__(256) kz_normal_kernel(const KzFitArgs a) {
   }
 }
 
+// The kz kernel's system (`KzGrappa::fit`, kspace3d.rs:1299-1362): the blocks' partial normal
+// equations summed in block order, scaled by nfeat / trace, the Tikhonov term added to the
+// diagonal, then every target coil's weights by pivoted elimination (hermitian_solve.cuh).  One
+// CTA; status 1 when the trace is not positive (an empty calibration).
+struct KzSolveArgs {
+  const double2* partial;  // [blocks][nfeat][ncol], ncol = nfeat + nc
+  double2* W;              // [nfeat][ncol]
+  double* scratch;         // 2 nfeat + nc * 2 nfeat
+  float2* out;             // [nc][nfeat]
+  int* status;
+  double lambda;
+  int blocks, nfeat, nc;
+};
+
+__global__ void __launch_bounds__(256) kz_solve_kernel(const KzSolveArgs a) {
+  __shared__ double red_v[256];
+  __shared__ int red_i[256];
+  __shared__ double s_scale;
+  __shared__ int s_bad;
+  const int nf = a.nfeat, ncol = nf + a.nc;
+  const size_t n_el = (size_t)nf * ncol;
+  for (size_t e = threadIdx.x; e < n_el; e += blockDim.x) {
+    double2 g = make_double2(0.0, 0.0);
+    for (int b = 0; b < a.blocks; ++b) {
+      const double2 p = a.partial[(size_t)b * n_el + e];
+      g.x = __dadd_rn(g.x, p.x);
+      g.y = __dadd_rn(g.y, p.y);
+    }
+    a.W[e] = g;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double trace = 0.0;
+    for (int i = 0; i < nf; ++i) trace = __dadd_rn(trace, a.W[(size_t)i * ncol + i].x);
+    s_bad = !(trace > 0.0);
+    s_scale = s_bad ? 0.0 : __ddiv_rn((double)nf, trace);
+    if (s_bad) *a.status = 1;
+  }
+  __syncthreads();
+  if (s_bad) return;
+  const double sc = s_scale;
+  for (size_t e = threadIdx.x; e < n_el; e += blockDim.x) {
+    double2 v = a.W[e];
+    v.x = __dmul_rn(v.x, sc);
+    v.y = __dmul_rn(v.y, sc);
+    if ((int)(e / ncol) == (int)(e % ncol)) v.x = __dadd_rn(v.x, a.lambda);
+    a.W[e] = v;
+  }
+  __syncthreads();
+  hermitian_solve_block(a.W, nf, a.nc, a.scratch, a.scratch + nf, a.scratch + 2 * nf, a.out, red_v, red_i);
+}
+
 struct KzFillJob {
   int p, nsrc, woff, pad;
   int src[kKzSources];
@@ -431,49 +484,6 @@ dim3 g3(size_t n, int y, int z) {
   return dim3((unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 1024)), (unsigned)y, (unsigned)z);
 }
 
-// `solve_hermitian` (kspace.rs:1455-1491): Gaussian elimination with partial pivoting, FP64.
-std::vector<double2> solve_hermitian_host(std::vector<std::vector<double2>> h, std::vector<double2> b) {
-  const size_t n = b.size();
-  auto mul = [](double2 a, double2 c) { return make_double2(a.x * c.x - a.y * c.y, a.x * c.y + a.y * c.x); };
-  auto recip = [](double2 d) {
-    const double m2 = d.x * d.x + d.y * d.y;
-    return m2 < 1e-18 ? make_double2(0.0, 0.0) : make_double2(d.x / m2, -d.y / m2);
-  };
-  auto absz = [](double2 d) { return std::sqrt(d.x * d.x + d.y * d.y); };
-  for (size_t col = 0; col < n; ++col) {
-    size_t piv = col;
-    double best = absz(h[col][col]);
-    for (size_t r = col + 1; r < n; ++r) {
-      const double m = absz(h[r][col]);
-      if (m > best) {
-        best = m;
-        piv = r;
-      }
-    }
-    std::swap(h[col], h[piv]);
-    std::swap(b[col], b[piv]);
-    const double2 dinv = recip(h[col][col]);
-    for (size_t r = col + 1; r < n; ++r) {
-      const double2 f = mul(h[r][col], dinv);
-      for (size_t c = col; c < n; ++c) {
-        const double2 s = mul(f, h[col][c]);
-        h[r][c] = make_double2(h[r][c].x - s.x, h[r][c].y - s.y);
-      }
-      const double2 sb = mul(f, b[col]);
-      b[r] = make_double2(b[r].x - sb.x, b[r].y - sb.y);
-    }
-  }
-  std::vector<double2> x(n, make_double2(0.0, 0.0));
-  for (size_t col = n; col-- > 0;) {
-    double2 s = b[col];
-    for (size_t c = col + 1; c < n; ++c) {
-      const double2 t = mul(h[col][c], x[c]);
-      s = make_double2(s.x - t.x, s.y - t.y);
-    }
-    x[col] = mul(s, recip(h[col][col]));
-  }
-  return x;
-}
 
 }  // namespace
 
@@ -1062,35 +1072,27 @@ static KzKernel kz_fit(mrsim_context* ctx, const Spiral3dTable& T, int accel, co
     const size_t smem = (size_t)16 * ncol * sizeof(double2);
     kz_normal_kernel<<<blocks, 256, smem, st>>>(a);
     MRSIM_CUDA(cudaGetLastError());
-    std::vector<double2> part((size_t)blocks * nfeat * ncol);
-    MRSIM_CUDA(cudaMemcpyAsync(part.data(), a.partial, part.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
-    MRSIM_CUDA(cudaStreamSynchronize(st));
-    std::vector<double2> G((size_t)nfeat * ncol, make_double2(0.0, 0.0));
-    for (int b = 0; b < blocks; ++b)
-      for (size_t e = 0; e < G.size(); ++e) {
-        G[e].x += part[(size_t)b * G.size() + e].x;
-        G[e].y += part[(size_t)b * G.size() + e].y;
-      }
-    double trace = 0.0;
-    for (int i = 0; i < nfeat; ++i) trace += G[(size_t)i * ncol + i].x;
-    if (!(trace > 0.0)) fail("the kz calibration acquisition is empty: its images give no signal");
-    const double s = (double)nfeat / trace;
-    std::vector<std::vector<double2>> aha(nfeat, std::vector<double2>(nfeat));
-    for (int i = 0; i < nfeat; ++i)
-      for (int j = 0; j < nfeat; ++j) {
-        const double2 v = G[(size_t)i * ncol + j];
-        aha[i][j] = make_double2(v.x * s, v.y * s);
-      }
-    for (int i = 0; i < nfeat; ++i) aha[i][i].x += kKzLambda;
+    KzSolveArgs sa;
+    sa.partial = a.partial;
+    sa.W = (double2*)A.alloc((size_t)nfeat * ncol * sizeof(double2));
+    sa.scratch = (double*)A.alloc((size_t)(2 * nfeat + nc * 2 * nfeat) * sizeof(double));
+    sa.out = (float2*)A.alloc((size_t)nc * nfeat * sizeof(float2));
+    sa.status = (int*)A.alloc(sizeof(int));
+    sa.lambda = kKzLambda;
+    sa.blocks = blocks;
+    sa.nfeat = nfeat;
+    sa.nc = nc;
+    MRSIM_CUDA(cudaMemsetAsync(sa.status, 0, sizeof(int), st));
+    kz_solve_kernel<<<1, 256, 0, st>>>(sa);
+    MRSIM_CUDA(cudaGetLastError());
+    int status = 0;
     const int woff = (int)K.w.size();
-    for (int qt = 0; qt < nc; ++qt) {
-      std::vector<double2> b(nfeat);
-      for (int i = 0; i < nfeat; ++i) {
-        const double2 v = G[(size_t)i * ncol + nfeat + qt];
-        b[i] = make_double2(v.x * s, v.y * s);
-      }
-      for (const double2& x : solve_hermitian_host(aha, b)) K.w.push_back(make_float2((float)x.x, (float)x.y));
-    }
+    K.w.resize(K.w.size() + (size_t)nc * nfeat);
+    MRSIM_CUDA(cudaMemcpyAsync(&status, sa.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MRSIM_CUDA(cudaMemcpyAsync(K.w.data() + woff, sa.out, (size_t)nc * nfeat * sizeof(float2), cudaMemcpyDeviceToHost,
+                               st));
+    MRSIM_CUDA(cudaStreamSynchronize(st));
+    if (status) fail("the kz calibration acquisition is empty: its images give no signal");
     K.where[key] = std::make_pair(woff, nsrc);
   }
   return K;

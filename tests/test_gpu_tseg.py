@@ -24,6 +24,7 @@ CASES = [  # (sample times, readout ms, d, f)
     (SPIRAL, 8.192, (0.01, 0.02), (-30.0, 50.0)),
     ((np.arange(200) + 0.5) * 0.02, 4.0, (0.1, 1.1), (-50.0, 50.0)),
     (np.arange(24) * 0.5, 11.5, (0.0, 0.02), (-40.0, 40.0)),  # an EPI echo's line times
+    (SPIRAL, 8.192, (0.0, 0.05), (-200.0, 200.0)),  # a wide rectangle: L = 24, a 29 x 29 rate grid
 ]
 
 
