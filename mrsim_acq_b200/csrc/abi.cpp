@@ -167,6 +167,9 @@ int mrsim_context_destroy(mrsim_context* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (auto& b : ctx->ws)
       if (b.p) cudaFree(b.p);
+    for (auto& e : ctx->slot_ev)
+      if (e) cudaEventDestroy(e);
+    if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
   });
@@ -351,6 +354,7 @@ int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisitio
         mrsim::fail(buf);
       }
     if (n_echoes <= 0) mrsim::fail("simulate_acquisition_echoes needs at least one echo");
+    mrsim::SeriesImageCache images;  // echoes given the same image arrays upload them once
     for (int64_t e = 0; e < n_echoes; ++e) {
       mrsim_acquisition acq_e = *acq;
       acq_e.t_echo = echo_times_ms[e];
@@ -366,7 +370,7 @@ int mrsim_simulate_acquisition_echoes(mrsim_context* ctx, const mrsim_acquisitio
       out.re = mag[e];
       out.im = phase[e];
       mrsim::acquire_series(ctx, *in, acq_e, &opts, in->seed, in->seed ^ mrsim::echo_salt((uint64_t)e),
-                            images_per_echo[e], out, true);
+                            images_per_echo[e], out, true, &images);
     }
   });
 }

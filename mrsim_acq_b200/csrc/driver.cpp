@@ -459,7 +459,7 @@ void upload_series_images(EpiOperator* op, const float* const* host_images) {
   const size_t per_comp = (size_t)op->nz * plane * op->nv;
   float* staging = (float*)workspace(op->ctx, 20, per_comp * op->ncomp * 4);
   for (int c = 0; c < op->ncomp; ++c)
-    MRSIM_CUDA(cudaMemcpyAsync(staging + (size_t)c * per_comp, host_images[c], per_comp * 4, cudaMemcpyHostToDevice, st));
+    copy_pageable_h2d(op->ctx, staging + (size_t)c * per_comp, host_images[c], per_comp * 4, st);
   launch_series_transpose(staging, op->d_images, op->ncomp, op->nv, op->nz, (int)plane, st);
 }
 

@@ -491,7 +491,7 @@ void grase_observed(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, co
   float2* k3 = (float2*)A.alloc((size_t)P.nc * P.nz * per * sizeof(float2));
   ShotVariants V = input_sets(A, P, in, g, g + 1, st);
   grase_kspace(P, I, acq, in.phase, d_lw, g, g + 1, P.mask, k3, st, &V);
-  MRSIM_CUDA(cudaMemcpyAsync(out, k3, (size_t)P.nc * P.nz * per * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  copy_pageable_d2h(ctx, out, k3, (size_t)P.nc * P.nz * per * sizeof(float2), st);
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -588,8 +588,8 @@ void grase_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, con
     MRSIM_CUDA(cudaGetLastError());
     MRSIM_CUDA(cudaStreamSynchronize(st));
   }
-  MRSIM_CUDA(cudaMemcpyAsync(mag, d_mag, per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
-  MRSIM_CUDA(cudaMemcpyAsync(ph, d_ph, per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+  copy_pageable_d2h(ctx, mag, d_mag, per * nz * nv * 4, st);
+  copy_pageable_d2h(ctx, ph, d_ph, per * nz * nv * 4, st);
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -869,8 +869,8 @@ void ge_acquire(mrsim_context* ctx, const mrsim_acquisition_ge_input& in, const 
     }
   }
   for (int e = 0; e < n_echoes; ++e) {
-    MRSIM_CUDA(cudaMemcpyAsync(mag[e], d_mag[e], per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
-    MRSIM_CUDA(cudaMemcpyAsync(ph[e], d_ph[e], per * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+    copy_pageable_d2h(ctx, mag[e], d_mag[e], per * nz * nv * 4, st);
+    copy_pageable_d2h(ctx, ph[e], d_ph[e], per * nz * nv * 4, st);
   }
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }

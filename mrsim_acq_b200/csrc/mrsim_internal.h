@@ -128,8 +128,9 @@ struct mrsim_context {
   std::mutex mu;
   // grow-only device workspaces keyed by role
   std::vector<mrsim::DeviceBuffer> ws;
-  void* host_pinned = nullptr;
+  void* host_pinned = nullptr;  // page-locked staging slots of the pageable copies (host_copy.cpp)
   size_t host_pinned_n = 0;
+  std::vector<cudaEvent_t> slot_ev;  // per slot: its last copy
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -137,6 +138,12 @@ namespace mrsim {
 
 // Workspace slot `slot` of at least `bytes` (grow-only, device memory of the context's device).
 void* workspace(mrsim_context* ctx, int slot, size_t bytes);
+
+// Large copies between pageable host memory and the device through the context's page-locked
+// slots, several host threads at once (host_copy.cpp).  The upload is ordered on `st` like a
+// cudaMemcpyAsync; the download returns when `dst` holds the data.
+void copy_pageable_h2d(mrsim_context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st);
+void copy_pageable_d2h(mrsim_context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 // ---- the forward/adjoint plan (epi_kernels.cu) -----------------------------------------------
 // The plan's tunables (0: the built-in choice), the space the autotuner searches: coil classes

@@ -483,7 +483,8 @@ void validate_t2_volumes(const char* what, const mrsim_t2* vols, int ncomp, size
 
 void acquire_series(mrsim_context* ctx, const mrsim_acquisition_input& in, const mrsim_acquisition& acq,
                     const mrsim_acquisition_options* opts_in, uint64_t excitation_seed, uint64_t receiver_seed,
-                    const float* const* images, mrsim_acquisition_output& out, bool mag_phase) {
+                    const float* const* images, mrsim_acquisition_output& out, bool mag_phase,
+                    SeriesImageCache* cache) {
   mrsim_acquisition_options dflt;
   std::memset(&dflt, 0, sizeof dflt);
   const mrsim_acquisition_options& opts = opts_in ? *opts_in : dflt;
@@ -533,13 +534,33 @@ void acquire_series(mrsim_context* ctx, const mrsim_acquisition_input& in, const
     captured.push_back((int)opts.kspace_slices[i]);
   }
   DevArena A;
-  // ---- inputs on the device
+  // ---- inputs on the device (kept in `cache` for a later call with the same arrays)
   const size_t per_comp = nvox_sim * nv;
-  float* staging = (float*)A.alloc(std::max<size_t>(1, per_comp * ncomp) * 4);
-  for (int c = 0; c < ncomp; ++c)
-    MRSIM_CUDA(cudaMemcpyAsync(staging + (size_t)c * per_comp, images[c], per_comp * 4, cudaMemcpyHostToDevice, st));
-  float* d_img = (float*)A.alloc(std::max<size_t>(1, per_comp * ncomp) * 4);
-  if (ncomp) launch_series_transpose(staging, d_img, ncomp, nv, nz, (int)plane, st);
+  const std::vector<const float*> img_from(images, images + (images ? ncomp : 0));
+  float* d_img = nullptr;
+  if (cache && cache->d_img && cache->from == img_from && cache->n == per_comp * ncomp) {
+    d_img = cache->d_img;
+  } else {
+    float* staging = (float*)A.alloc(std::max<size_t>(1, per_comp * ncomp) * 4);
+    for (int c = 0; c < ncomp; ++c) copy_pageable_h2d(ctx, staging + (size_t)c * per_comp, images[c], per_comp * 4, st);
+    if (cache) {
+      if (cache->d_img && cache->n < per_comp * ncomp) {
+        MRSIM_CUDA(cudaStreamSynchronize(st));
+        MRSIM_CUDA(cudaFree(cache->d_img));
+        cache->d_img = nullptr;
+      }
+      if (!cache->d_img) {
+        MRSIM_CUDA(cudaMalloc(&cache->d_img, std::max<size_t>(1, per_comp * ncomp) * 4));
+        cache->n = per_comp * ncomp;
+      }
+      cache->from = img_from;
+      cache->n = per_comp * ncomp;
+      d_img = cache->d_img;
+    } else {
+      d_img = (float*)A.alloc(std::max<size_t>(1, per_comp * ncomp) * 4);
+    }
+    if (ncomp) launch_series_transpose(staging, d_img, ncomp, nv, nz, (int)plane, st);
+  }
   float* d_fmap = (float*)A.upload(in.fmap, nvox_sim * 4, st);
   const bool uniform = uniform_relaxation(in.t2, in.t_inhom, ncomp);
   const bool maps = !uniform && acq.do_relaxation;
@@ -774,8 +795,8 @@ void acquire_series(mrsim_context* ctx, const mrsim_acquisition_input& in, const
     launch_series_output(comb, d_sigma, d_re, d_im, g0, g1, nv, nz, nx, ny, d_zmap, receiver_seed, st, mag_phase);
     MRSIM_CUDA(cudaStreamSynchronize(st));
   }
-  MRSIM_CUDA(cudaMemcpyAsync(out.re, d_re, nvox_acq * nv * 4, cudaMemcpyDeviceToHost, st));
-  MRSIM_CUDA(cudaMemcpyAsync(out.im, d_im, nvox_acq * nv * 4, cudaMemcpyDeviceToHost, st));
+  copy_pageable_d2h(ctx, out.re, d_re, nvox_acq * nv * 4, st);
+  copy_pageable_d2h(ctx, out.im, d_im, nvox_acq * nv * 4, st);
   if (nsl) {
     const size_t n = (size_t)nv * nsl * nc * per;
     if (cap_acq) MRSIM_CUDA(cudaMemcpyAsync(out.acquired, cap_acq, n * sizeof(float2), cudaMemcpyDeviceToHost, st));

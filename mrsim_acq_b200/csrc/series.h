@@ -29,9 +29,24 @@ void simulate_slice_full(mrsim_context* ctx, const mrsim_slice_input& inp, const
 // `acquire_volumes_complex` (kspace.rs:1851-2125) with explicit excitation and receiver seeds;
 // `images` overrides in.images (the echoes entry passes each echo's images).  mag_phase: out.re /
 // out.im receive the magnitude and phase (kspace.rs:1839-1846), split on the device.
+// The device copy of a series' images ([g][z][c][plane], transposed from the reference's
+// vox*nv + g), kept across the calls of one entry point that pass the same arrays (the echoes of
+// `simulate_acquisition_echoes` when their images are one set).
+struct SeriesImageCache {
+  std::vector<const float*> from;  // the host arrays the copy was made from
+  float* d_img = nullptr;
+  size_t n = 0;  // floats
+  SeriesImageCache() = default;
+  SeriesImageCache(const SeriesImageCache&) = delete;
+  SeriesImageCache& operator=(const SeriesImageCache&) = delete;
+  ~SeriesImageCache() {
+    if (d_img) cudaFree(d_img);
+  }
+};
 void acquire_series(mrsim_context* ctx, const mrsim_acquisition_input& in, const mrsim_acquisition& acq,
                     const mrsim_acquisition_options* opts, uint64_t excitation_seed, uint64_t receiver_seed,
-                    const float* const* images, mrsim_acquisition_output& out, bool mag_phase = false);
+                    const float* const* images, mrsim_acquisition_output& out, bool mag_phase = false,
+                    SeriesImageCache* cache = nullptr);
 
 // misc_kernels.cu: combined images -> (re, im) in the series layout vox*nv + g, plus the
 // image-space noise of `acquire_volumes_complex` (kspace.rs:2031-2052).

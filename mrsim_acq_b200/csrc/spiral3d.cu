@@ -1143,7 +1143,7 @@ void spiral3d_samples(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, 
   for (int h = 0; h < (int)in.n_volumes; ++h) (void)spiral_sets(A, P, in, h, st, false);  // every volume's sets checked
   const SpiralVariants V = spiral_sets(A, P, in, g, st);
   spiral_samples(P, I, g, d_lw, k, st, &V);
-  MRSIM_CUDA(cudaMemcpyAsync(out, k, (size_t)P.nc * P.nz * P.nsamp * sizeof(float2), cudaMemcpyDeviceToHost, st));
+  copy_pageable_d2h(ctx, out, k, (size_t)P.nc * P.nz * P.nsamp * sizeof(float2), st);
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -1252,8 +1252,8 @@ void spiral3d_acquire(mrsim_context* ctx, const mrsim_acquisition_3d_input& in, 
     MRSIM_CUDA(cudaGetLastError());
     MRSIM_CUDA(cudaStreamSynchronize(st));
   }
-  MRSIM_CUDA(cudaMemcpyAsync(mag, d_mag, nn * nz * nv * 4, cudaMemcpyDeviceToHost, st));
-  MRSIM_CUDA(cudaMemcpyAsync(ph, d_ph, nn * nz * nv * 4, cudaMemcpyDeviceToHost, st));
+  copy_pageable_d2h(ctx, mag, d_mag, nn * nz * nv * 4, st);
+  copy_pageable_d2h(ctx, ph, d_ph, nn * nz * nv * 4, st);
   MRSIM_CUDA(cudaStreamSynchronize(st));
 }
 
