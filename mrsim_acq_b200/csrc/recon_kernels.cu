@@ -147,15 +147,16 @@ __global__ void __launch_bounds__(256) recon_combine_kernel(const ReconJob* __re
       float hr = 0.f, hi = 0.f;
       if (y < ny) {
         const int yc = y - ys;
-        for (int ky = 0; ky < ny; ++ky) {
+        // m = (ky - ys) yc mod ny, stepped: the same table entries without a modulo per term
+        const int step = ((yc % ny) + ny) % ny;
+        int m = (((-ys * yc) % ny) + ny) % ny;
+        for (int ky = 0; ky < ny; ++ky, m = m + step >= ny ? m + step - ny : m + step) {
           float2 v = kq[(size_t)ky * nx + kx];
           if (J.window) {
             float w = J.window[(size_t)ky * nx + kx];
             v.x *= w;
             v.y *= w;
           }
-          int m = ((ky - ys) * yc) % ny;
-          m += m < 0 ? ny : 0;
           const float2 t = Ey[m];
           hr = hr + (v.x * t.x - v.y * t.y);
           hi = hi + (v.x * t.y + v.y * t.x);
@@ -174,10 +175,10 @@ __global__ void __launch_bounds__(256) recon_combine_kernel(const ReconJob* __re
       if (y >= ny) continue;
       const int xc = x - xs;
       float ir = 0.f, ii = 0.f;
-      for (int kx = 0; kx < nx; ++kx) {
+      const int step = ((xc % nx) + nx) % nx;
+      int m = (((-xs * xc) % nx) + nx) % nx;
+      for (int kx = 0; kx < nx; ++kx, m = m + step >= nx ? m + step - nx : m + step) {
         const float2 v = h[yy * nx + kx];
-        int m = ((kx - xs) * xc) % nx;
-        m += m < 0 ? nx : 0;
         const float2 t = Ex[m];
         ir = ir + (v.x * t.x - v.y * t.y);
         ii = ii + (v.x * t.y + v.y * t.x);
