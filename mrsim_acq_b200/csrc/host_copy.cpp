@@ -30,12 +30,28 @@ bool page_locked(const void* p) {
   return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
 }
 
-void ensure_slots(mrsim_context* ctx) {
-  if (ctx->host_pinned) return;
-  MRSIM_CUDA(cudaHostAlloc(&ctx->host_pinned, kSlots * kSlotBytes, cudaHostAllocPortable));
+// The context's slots, allocated on first use; false (and the direct copy) when page-locked
+// memory cannot be had.
+bool ensure_slots(mrsim_context* ctx) {
+  if (ctx->host_pinned) return true;
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, kSlots * kSlotBytes, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  std::vector<cudaEvent_t> ev(kSlots, nullptr);
+  for (auto& e : ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      for (auto& f : ev)
+        if (f) cudaEventDestroy(f);
+      cudaFreeHost(p);
+      return false;
+    }
+  ctx->host_pinned = p;
   ctx->host_pinned_n = kSlots * kSlotBytes;
-  ctx->slot_ev.resize(kSlots);
-  for (auto& e : ctx->slot_ev) MRSIM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  ctx->slot_ev = ev;
+  return true;
 }
 
 int threads_for(size_t bytes) {
@@ -72,11 +88,10 @@ void on_threads(mrsim_context* ctx, int nt, F&& f) {
 }  // namespace
 
 void copy_pageable_h2d(mrsim_context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
-  if (bytes < kDirectBelow || page_locked(src)) {
+  if (bytes < kDirectBelow || page_locked(src) || !ensure_slots(ctx)) {
     MRSIM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
     return;
   }
-  ensure_slots(ctx);
   const size_t chunks = (bytes + kSlotBytes - 1) / kSlotBytes;
   const int nt = threads_for(bytes);
   on_threads(ctx, nt, [&](int t) {
@@ -92,12 +107,11 @@ void copy_pageable_h2d(mrsim_context* ctx, void* dst, const void* src, size_t by
 }
 
 void copy_pageable_d2h(mrsim_context* ctx, void* dst, const void* src, size_t bytes, cudaStream_t st) {
-  if (bytes < kDirectBelow || page_locked(dst)) {
+  if (bytes < kDirectBelow || page_locked(dst) || !ensure_slots(ctx)) {
     MRSIM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
     MRSIM_CUDA(cudaStreamSynchronize(st));
     return;
   }
-  ensure_slots(ctx);
   const size_t chunks = (bytes + kSlotBytes - 1) / kSlotBytes;
   const int nt = threads_for(bytes);
   on_threads(ctx, nt, [&](int t) {

@@ -15,8 +15,7 @@
 //  - the sizes are capped (see the limits below); larger slices are rejected with an error;
 //  - the first call on a device resolves the arrays' device addresses with cudaGetSymbolAddress
 //    (with that device current) and caches them with the identity of the device's current CUDA
-//    context; a later call in another context (after cudaDeviceReset, say) resolves them again.
-//    Make the first call before any stream capture begins;
+//    context; a later call in another context (after cudaDeviceReset, say) resolves them again;
 //  - every call checks that its data pointers are device (or managed) memory of the current
 //    device, so a host pointer passed by mistake is an error, not a device fault;
 //  - each call waits for its stream before it returns (the host tables it stages must outlive
