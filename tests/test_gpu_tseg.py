@@ -25,6 +25,9 @@ CASES = [  # (sample times, readout ms, d, f)
     ((np.arange(200) + 0.5) * 0.02, 4.0, (0.1, 1.1), (-50.0, 50.0)),
     (np.arange(24) * 0.5, 11.5, (0.0, 0.02), (-40.0, 40.0)),  # an EPI echo's line times
     (SPIRAL, 8.192, (0.0, 0.05), (-200.0, 200.0)),  # a wide rectangle: L = 24, a 29 x 29 rate grid
+    # a long decay range: L = 48, a 44 x 44 rate grid, so 4 sample times per block, and 37 samples
+    # leave a partial last block
+    ((np.arange(37) + 0.5) * (8.192 / 37), 8.192, (0.0, 5.0), (-10.0, 10.0)),
 ]
 
 
@@ -60,7 +63,7 @@ def test_device_plan_matches_the_host_plan(case, gpu_ctx):
             assert np.abs(g.b @ segs - h.b @ segs).max() <= 1e-3 * h.bound + 1e-14
 
 
-@pytest.mark.parametrize("case", [1, 3])
+@pytest.mark.parametrize("case", [1, 3, 6])
 def test_device_plan_bound_holds_between_grid_points(case, gpu_ctx):
     tau, t, d, f = CASES[case]
     p = S.tseg_plan(tau, t, S.RateRect(d, f), ctx=gpu_ctx)
