@@ -248,7 +248,8 @@ def scale_measurements(args, ctx, stream):
     128 lines; the exact pair with the complex-image adjoint, device-timed) and one volume of the
     stack of spirals (64x64x48 on a 128x128 grid, 16 coils in 2 rings, 32 interleaves x 2048
     samples at 4 us, kz partial Fourier 6/8 and R = 2, +-80 Hz; the host-buffer call, transfers
-    included)."""
+    included); the precision-at-scale mixed batch (64/96/128 with 17/23/31 slices, one plan) and
+    its GRASE train (64x64x32, 4 shots, 150-degree refocusing)."""
     from mrsim_acq_b200.api import T2, Acquisition, EpiOperator, PhaseModel
     out = {}
     nx, o, nz, nv, nc = 128, 2, 60, 20, 3
@@ -278,6 +279,8 @@ def scale_measurements(args, ctx, stream):
                                  "note": "exact pair (per-coil kernels: a ring of 32 takes no coil-class path); "
                                          "the segmented path refuses this shape (more than 16 line groups)"}
     out["stack_of_spirals"] = spiral_measurement(ctx)
+    out["mixed_batch"] = mixed_batch_measurement(ctx, stream)
+    out["grase"] = grase_measurement(ctx)
     # the plain single-shot case on the device (launch-bound: one unit)
     c1, acq1 = c1_inputs()
     op = EpiOperator(c1["sim_dims"], c1["acq_dims"], 1, c1["t2"], c1["fmap"], acq1, images=c1["images"],
@@ -395,6 +398,83 @@ def spiral_measurement(ctx, reps=2):
             "timing": "host-buffer calls (mrsim_spiral_samples_3d; mrsim_simulate_acquisition_3d_spiral with noise, "
                       "kz GRAPPA fill, POCS and the per-partition gridding + CG reconstruction) by wall clock, "
                       "host<->device copies included"}
+
+
+def mixed_batch_measurement(ctx, stream, steps=3):
+    """The precision-at-scale configuration's mixed batch: scans of 64, 96 and 128 on 2x grids with
+    uneven slice counts 17, 23 and 31 (one volume each), 32 ring coils, 3 compartments, all lines,
+    TE 40 ms, as one plan (`mrsim_epi_batch`: each stage one launch over every unit of every
+    geometry); forward + complex-image adjoint, CUDA events on the context stream."""
+    import torch
+    from mrsim_acq_b200.api import T2, Acquisition, EpiBatch, PhaseModel
+    acq = Acquisition(n_coils=32, t_line=0.5, t_echo=40.0, ghost_offset=0.05, signal_scale=100.0)
+    series = []
+    for n, nz in ((64, 17), (96, 23), (128, 31)):
+        snx = 2 * n
+        ys, xs = np.meshgrid((np.arange(snx) + 0.5) / snx, (np.arange(snx) + 0.5) / snx, indexing="ij")
+        blob = np.exp(-((xs - 0.5) ** 2 + (ys - 0.48) ** 2) / 0.05).astype(np.float32)
+        zs = (1.0 + 0.3 * np.sin(np.arange(nz) / 7.0)).astype(np.float32)
+        imgs = [(blob[None] * np.float32(0.6 + 0.2 * c) * zs[:, None, None]).reshape(-1) for c in range(3)]
+        fmap = np.tile((60.0 * (blob - 0.5)).astype(np.float32).reshape(-1), nz)
+        series.append(dict(sim_dims=(snx, snx, nz), acq_dims=(n, n, nz), n_volumes=1, images=imgs, fmap=fmap,
+                           t2=[T2.uniform(80.0), T2.uniform(250.0), T2.uniform(30.0)],
+                           t_inhom=[T2.uniform(40.0), T2.uniform(60.0), T2.uniform(20.0)],
+                           phase=PhaseModel.hbcd_like(), seed=42))
+    b = EpiBatch(series, acq, echo_times_ms=[40.0], grads=0, ctx=ctx)
+    b.forward()
+    b.adjoint()
+    ctx.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        b.forward()
+        b.adjoint()
+    t1.record(stream)
+    t1.synchronize()
+    ctx.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    smp = b.samples
+    b.close()
+    return {"config": "scans 64/96/128 on 2x grids, 17/23/31 slices, 1 volume each, 32 ring coils, 3 compartments, "
+                      "64/96/128 lines, TE 40 ms, one plan", "units": 17 + 23 + 31, "samples_per_step": smp,
+            "ms_per_step": ms, "value": smp / (ms * 1e-3), "unit": "samples/s",
+            "timing": "forward + complex-image adjoint, CUDA events on the context stream, mean of 3 after a warm-up"}
+
+
+def grase_measurement(ctx):
+    """The precision-at-scale configuration's GRASE train: 64x64x32 on a 128x128 grid, 4 shots (4 ky
+    segments, one kz segment), echo spacing 20 ms, 150-degree refocusing (CPMG amplitudes from T1
+    and T2), 32 ring coils, 3 compartments, one volume: the host-buffer call
+    `simulate_acquisition_3d` (forward, noise, per-partition reconstruction), wall clock."""
+    from mrsim_acq_b200 import kspace3d as K3
+    from mrsim_acq_b200.api import T2, Acquisition, PhaseModel
+    n, o, nz = 64, 2, 32
+    sg = n * o
+    vox = np.arange(sg * sg * nz)
+    x, y, z = (vox % sg) / sg, ((vox // sg) % sg) / sg, (vox // (sg * sg)) / nz
+    imgs = [(np.exp(-((x - 0.5 - 0.05 * c) ** 2 + (y - 0.47) ** 2) / 0.04) * (1.0 + 0.3 * np.sin(6.3 * z))
+             ).astype(np.float32) for c in range(3)]
+    fm = (40.0 * np.exp(-((x - 0.4) ** 2 + (y - 0.4) ** 2) / 0.02)).astype(np.float32)
+    acq = Acquisition(do_relaxation=True, do_distortions=True, n_coils=32, signal_scale=100.0, noise_variance=1e-4)
+    tr = K3.EchoTrain(etl=nz, esp_ms=20.0, refocusing_deg=150.0, kz_order=K3.KzOrder.Centric, kz_segments=1,
+                      refocusing_time_ms=2.0)
+    ro = K3.GraseReadout(ky_segments=4, t_line_ms=0.5, reverse_phase=False)
+    args = ((sg, sg, nz), (n, n, nz), 1, imgs, [T2.uniform(80.0), T2.uniform(250.0), T2.uniform(30.0)],
+            [T2.uniform(1330.0), T2.uniform(4000.0), T2.uniform(900.0)], fm, None, acq, tr, ro)
+    K3.simulate_acquisition_3d(*args, phase=PhaseModel.none(), seed=5, ctx=ctx)  # warm
+    runs = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        K3.simulate_acquisition_3d(*args, phase=PhaseModel.none(), seed=5, ctx=ctx)
+        runs.append(time.perf_counter() - t0)
+    dt = float(np.median(runs))
+    smp = 32 * nz * n * n
+    return {"config": "GRASE 64x64x32 on 128x128, 4 shots, ESP 20 ms, 150-degree refocusing with T1, 32 ring coils, "
+                      "3 compartments, 1 volume", "samples_per_volume": smp, "seconds_per_volume": dt,
+            "seconds_per_volume_runs": [round(r, 4) for r in runs], "value": smp / dt, "unit": "samples/s",
+            "timing": "mrsim_simulate_acquisition_3d with host buffers by wall clock (forward, noise, reconstruction), "
+                      "median of 3 after a warm-up"}
 
 
 def spin_history_series():
@@ -760,6 +840,8 @@ def main():
     ap.add_argument("--spin-volumes", type=int, default=40, help="volumes of the spin-history series")
     ap.add_argument("--spiral-only", action="store_true",
                     help="run only the stack-of-spirals volume and print its line (profiling)")
+    ap.add_argument("--c5-only", action="store_true",
+                    help="run only the mixed-geometry batch and the GRASE train and print their line (profiling)")
     ap.add_argument("--pipeline-only", action="store_true",
                     help="run only the whole-pipeline series (with --volumes: a smaller one) and print its line "
                          "(profiling)")
@@ -777,6 +859,14 @@ def main():
     if args.spiral_only:
         from mrsim_acq_b200 import api
         print(json.dumps(spiral_measurement(api.Context(local_rank), reps=1)), flush=True)
+        return
+    if args.c5_only:
+        import torch
+        from mrsim_acq_b200 import api
+        ctx = api.Context(local_rank)
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        print(json.dumps({"mixed_batch": mixed_batch_measurement(ctx, stream), "grase": grase_measurement(ctx)}),
+              flush=True)
         return
     if args.pipeline_only:
         from mrsim_acq_b200 import api

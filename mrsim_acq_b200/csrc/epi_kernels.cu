@@ -1890,6 +1890,15 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
       p->xfft_e = (N0 % 32 == 0 && N0 <= 256) ? N0 / 32 : 0;
       for (int i = 0; i < n; ++i)
         if (hu[i].snx != N0) p->xfft_e = 0;
+      // without one warp width for every unit the shared-memory radix-2 FFT serves, which needs
+      // every row length to be a power of two (a batch mixing 128, 192 and 256 takes the DFT GEMM)
+      if (p->xfft_e == 0)
+        for (int i = 0; i < n; ++i) {
+          const int N = hu[i].snx;
+          if (!(N >= 8 && N <= kXfftMaxN && (N & (N - 1)) == 0)) p->xfft = false;
+        }
+    }
+    if (p->xfft) {
       std::vector<int4> ft;
       p->f_start.assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {

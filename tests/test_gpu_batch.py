@@ -2,7 +2,9 @@
 32 lines on 2x grids (the precision-at-scale configuration's 64/96/128 mix, scaled down) with
 uneven slice counts 3, 2 and 4, one launch per stage over every unit; every series' k-space and
 complex-image adjoint against the FP64 oracle (relative L2 <= 1e-5) and equal to the series run
-alone."""
+alone.  A second mix, scans of 32, 48 and 64 (rows of 64, 96 and 128 points: every one a warp-FFT
+width, but not one width, and 96 not a power of two), takes the DFT GEMM x-stage in the batch
+where each series alone takes its warp FFT."""
 import numpy as np
 import pytest
 
@@ -18,12 +20,16 @@ def rel_l2(a, b):
     return np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b))
 
 
-def test_mixed_geometry_batch_matches_the_oracle(gpu_ctx):
-    acq = Acquisition(n_coils=8, accel=2, partial_fourier=0.75, pf_mode=PartialFourierMode.Scanner, t_line=0.5,
+MIXES = [(((16, 3), (24, 2), (32, 4)), 8, 1e-6), (((32, 2), (48, 1), (64, 2)), 4, 5e-6)]
+
+
+@pytest.mark.parametrize("mix,coils,alone_tol", MIXES)
+def test_mixed_geometry_batch_matches_the_oracle(gpu_ctx, mix, coils, alone_tol):
+    acq = Acquisition(n_coils=coils, accel=2, partial_fourier=0.75, pf_mode=PartialFourierMode.Scanner, t_line=0.5,
                       t_echo=30.0, ghost_offset=0.05)
     tes = [30.0, 50.0]
     series = []
-    for n, nz in ((16, 3), (24, 2), (32, 4)):
+    for n, nz in mix:
         s = cases.series_case(nx=n, ny=n, nz=nz, o=2, nv=2, ncomp=3)
         s.update(phase=PhaseModel.hbcd_like(), seed=42)
         series.append(s)
@@ -44,7 +50,7 @@ def test_mixed_geometry_batch_matches_the_oracle(gpu_ctx):
                              echo_times_ms=tes, grads=0, ctx=gpu_ctx, **kw)
         alone = op.apply_host(None)
         op.close()
-        assert rel_l2(got["kspace"], alone["kspace"]) <= 1e-6, i
+        assert rel_l2(got["kspace"], alone["kspace"]) <= alone_tol, i
     b.close()
 
 
