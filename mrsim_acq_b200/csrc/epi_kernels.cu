@@ -1888,17 +1888,38 @@ EpiPlan* epi_plan_create(const UnitDesc* hu, int n, const StaticDesc* hs, int ns
     if (p->xfft) {
       const int N0 = hu[0].snx;
       p->xfft_e = (N0 % 32 == 0 && N0 <= 256) ? N0 / 32 : 0;
-      for (int i = 0; i < n; ++i)
+      bool all_warp = true;
+      for (int i = 0; i < n; ++i) {
         if (hu[i].snx != N0) p->xfft_e = 0;
-      // without one warp width for every unit the shared-memory radix-2 FFT serves, which needs
-      // every row length to be a power of two (a batch mixing 128, 192 and 256 takes the DFT GEMM)
+        all_warp = all_warp && hu[i].snx % 32 == 0 && hu[i].snx <= 256;
+      }
+      // every row a warp width but not one width (a batch of 128, 192 and 256): the warp FFT once
+      // per width over that width's tiles
+      if (p->xfft_e == 0 && all_warp) p->xfft_e = -1;
+      // otherwise the shared-memory radix-2 FFT serves, which needs every row length to be a power
+      // of two; failing that, the DFT GEMM
       if (p->xfft_e == 0)
         for (int i = 0; i < n; ++i) {
           const int N = hu[i].snx;
           if (!(N >= 8 && N <= kXfftMaxN && (N & (N - 1)) == 0)) p->xfft = false;
         }
     }
-    if (p->xfft) {
+    if (p->xfft && p->xfft_e < 0) {
+      // one list ordered by width, no per-unit ranges (such a plan runs whole)
+      std::vector<int4> ft;
+      for (int E = 1; E <= 8; ++E) {
+        p->fe_first[E] = (int)ft.size();
+        for (int i = 0; i < n; ++i) {
+          if (hu[i].snx != 32 * E) continue;
+          const int rows = hu[i].ncoils * hu[i].n_lines;
+          for (int r0 = 0; r0 < rows; r0 += 32) ft.push_back(make_int4(i, r0, std::min(32, rows - r0), 0));
+        }
+        p->fe_count[E] = (int)ft.size() - p->fe_first[E];
+      }
+      p->f_start.clear();
+      p->n_ftiles = (int)ft.size();
+      p->d_ftiles = (int4*)dev_upload(p, ft.data(), sizeof(int4) * ft.size());
+    } else if (p->xfft) {
       std::vector<int4> ft;
       p->f_start.assign(n + 1, 0);
       for (int i = 0; i < n; ++i) {
@@ -2105,6 +2126,33 @@ void launch_xstage(const EpiPlan* p, cudaStream_t st, int u0, int u1, bool adj) 
     }
 #undef MRSIM_XC
     MRSIM_CUDA(cudaGetLastError());
+    return;
+  }
+  if (p->xfft && p->xfft_e < 0) {
+    if (!(u0 == 0 && (u1 < 0 || u1 == p->n_units))) fail("a plan of mixed row widths runs its units whole");
+    for (int E = 1; E <= 8; ++E) {
+      if (p->fe_count[E] == 0) continue;
+      const int4* tiles = p->d_ftiles + p->fe_first[E];
+      const unsigned g = (unsigned)p->fe_count[E];
+#define MRSIM_XE(ADJ)                                                                               \
+  switch (E) {                                                                                      \
+    case 1: xfft_warp_kernel<1, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;           \
+    case 2: xfft_warp_kernel<2, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;           \
+    case 3: xfft_warp_kernel<3, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;           \
+    case 4: xfft_warp_kernel<4, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;           \
+    case 5: xfft_warp_kernel<5, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;           \
+    case 6: xfft_warp_kernel<6, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;           \
+    case 7: xfft_warp_kernel<7, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;           \
+    default: xfft_warp_kernel<8, ADJ, false><<<g, 256, 0, st>>>(p->d_units, tiles); break;          \
+  }
+      if (adj) {
+        MRSIM_XE(true)
+      } else {
+        MRSIM_XE(false)
+      }
+#undef MRSIM_XE
+      MRSIM_CUDA(cudaGetLastError());
+    }
     return;
   }
   if (p->xfft) {

@@ -172,7 +172,9 @@ struct EpiPlan {
   int n_atiles[4] = {0, 0, 0, 0};
   // x-stage as per-row FFTs (every unit has a power-of-two snx and FFT tables): tiles of rows
   bool xfft = false;
-  int xfft_e = 0;  // > 0: every unit has snx = 32 * xfft_e and the warp-per-row FFT runs
+  int xfft_e = 0;  // > 0: every unit has snx = 32 * xfft_e and the warp-per-row FFT runs; -1:
+                   // every snx is a warp width (32 E, E <= 8) but not one width: per-width launches
+  int fe_first[9] = {0}, fe_count[9] = {0};  // xfft_e == -1: the width-E tiles of d_ftiles
   // coil classes in the adjoint: the x-adjoint writes class rows (tiles of 4 lines x 8 coils) and
   // the y-adjoint combines 6 rows instead of 8 coils
   bool adj_cls = false;

@@ -3,8 +3,8 @@
 uneven slice counts 3, 2 and 4, one launch per stage over every unit; every series' k-space and
 complex-image adjoint against the FP64 oracle (relative L2 <= 1e-5) and equal to the series run
 alone.  A second mix, scans of 32, 48 and 64 (rows of 64, 96 and 128 points: every one a warp-FFT
-width, but not one width, and 96 not a power of two), takes the DFT GEMM x-stage in the batch
-where each series alone takes its warp FFT."""
+width, but not one width), runs the warp FFT once per width in the batch, as each series alone
+does."""
 import numpy as np
 import pytest
 
