@@ -824,8 +824,10 @@ __global__ void __launch_bounds__(128) yadjoint_kernel(const UnitDesc* __restric
       const int j = j0 + jj;
       const float* e = Lt + j * LF;
       const float thi = e[0], tlo = e[1], trf = e[2], tinh = e[3], tph = e[4];
+      // (Re, Im) pairs in packed f32x2 arithmetic: each lane rounds as the scalar product, sum and
+      // fused multiply-add do, so the sums are bitwise the scalar ones in half the issue slots
       float2 H[TY];
-      float hsr = 0.f, hsi = 0.f;
+      float2 hs = make_float2(0.f, 0.f);
 #pragma unroll
       for (int ty = 0; ty < TY; ++ty) H[ty] = make_float2(0.f, 0.f);
       const float2* hb = hbuf + (size_t)(buf * JC + jj) * ncoils * 128 + col;
@@ -833,17 +835,14 @@ __global__ void __launch_bounds__(128) yadjoint_kernel(const UnitDesc* __restric
       for (int q = 0; q < ncoils; ++q) {
         const float2 h = hb[q * 128];
         const float ex = Ex[q * 128 + col];
-        hsr += h.x;
-        hsi += h.y;
-        const float ur = ex * h.x, ui = ex * h.y;
+        hs = fadd2(hs, h);
+        const float2 uu = fmul2(dup2(ex), h);
         const float4 e4 = *reinterpret_cast<const float4*>(Ey + q * ROWS);
         const float ey[4] = {e4.x, e4.y, e4.z, e4.w};
 #pragma unroll
-        for (int ty = 0; ty < TY; ++ty) {
-          H[ty].x = fmaf(ey[ty], ur, H[ty].x);
-          H[ty].y = fmaf(ey[ty], ui, H[ty].y);
-        }
+        for (int ty = 0; ty < TY; ++ty) H[ty] = ffma2(dup2(ey[ty]), uu, H[ty]);
       }
+      const float hsr = hs.x, hsi = hs.y;
       const float4 b4 = *reinterpret_cast<const float4*>(Bt + j * ROWS);
       const float bt[4] = {b4.x, b4.y, b4.z, b4.w};
 #pragma unroll
