@@ -160,6 +160,20 @@ def test_tseg_bound_against_double_double(f):
     assert worst <= p.bound
 
 
+@pytest.mark.parametrize("tau,t", [([0.0], 0.0), ([0.5], 1.0), ([], 4.0), ([0.0, 0.0, 0.0], 0.0)])
+def test_tseg_degenerate_sample_sets(tau, t):
+    # one sample, none, or a readout of zero length (every node at 0: the truncated least squares
+    # drops the repeated columns) still give a certified plan of the right shape
+    p = S.tseg_plan(np.asarray(tau, np.float64), t, S.RateRect((0.0, 0.02), (-30.0, 30.0)))
+    assert p.bound < 1e-7 and p.l >= 2
+    assert p.b.shape == (len(tau), p.l)
+    for j, tj in enumerate(tau):
+        for d in (0.0, 0.01, 0.02):
+            for f in (-30.0, 0.0, 30.0):
+                z = -d + 1j * TAU * f / 1000.0
+                assert abs(np.exp(z * tj) - p.b[j] @ np.exp(z * p.tau_l)) <= p.bound
+
+
 def test_tseg_segment_count_rule():
     # L starts at ceil(T (f1 - f0)) + 2 (T in s) and only doubles
     tau = (np.arange(2048) + 0.5) * 0.004
